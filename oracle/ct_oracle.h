@@ -1,0 +1,125 @@
+/*
+ * ct_oracle.h -- CPU restatement of the reference CBCT reconstruction path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (gpu_b200/, include/)
+ * links, loads or calls this code.  Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg use it, and only as the checker.
+ *
+ * Each function restates one reference function or kernel of
+ * CBCT/CBCT_1024V_1024P_multiGPU_v6.3_20170823 (abbreviated V63/ below) as
+ * scalar C, with the same float operation order, so that it can be pinned
+ * bit-for-bit against the reference's own kernel sources compiled for the
+ * CPU (oracle/ref_harness.cpp -> oracle/_ref/libctref.so).
+ *
+ * Layouts (the reference's):
+ *   volume    f[k*M*N + j*M + i]      (V63/kernel_IterativeRecon_universal.cu:10)
+ *   view      p[row*R + col]          (V63/kernel_IterativeRecon_universal.cu:17)
+ *   sinogram  views stacked: p[view*R*Z_prj + row*R + col]
+ */
+#ifndef CT_ORACLE_H
+#define CT_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Scan description: the reference's compile-time constants
+ * (V63/main_recon.cu:54-111) as run-time fields. */
+typedef struct og_desc {
+    int   nx, ny, nz;        /* M, N, ZETA                                  */
+    int   nu, nv;            /* R (detector columns), Z_prj (rows)          */
+    int   nviews;            /* Nviews                                      */
+    float vx, vy, vz;        /* volumn_x, volumn_y, volumn_z                */
+    float du, dv;            /* detector pitch (Detector_pixel_x, both axes)*/
+    float dso, dod;          /* DSO, DOD (detector plane at x = DOD < 0)    */
+    float offset;            /* Offset (half-detector shift)                */
+    int   m_offset;          /* M_Offset                                    */
+    float us_rate;           /* degrees per view                            */
+    float initial_angle;     /* degrees                                     */
+    float shift_angle;       /* degrees                                     */
+} og_desc;
+
+/* Derived constants, computed with the reference's float/double steps. */
+typedef struct og_geom {
+    og_desc d;
+    float inv_vx, inv_vy, inv_vz;   /* inv_volumn_*  = (float)(1.0/v)      */
+    float bx, by, bz;               /* boundary_voxel_*                     */
+    float ymin, zmin;               /* Detector_Ymin, Detector_Zmin         */
+    float srcx, srcy, srcz;         /* Source_x/y/z                         */
+} og_geom;
+
+int  og_init(og_geom* g, const og_desc* d);
+/* Per-view angle.  fdk=0: SART/FP frame theta' = -(j*us+init+shift)*pi/180
+ * (V63/host_IterativeRecon_CBCT.c:34-41); fdk=1: +theta (V63/host_FDK.cpp:35-40). */
+void og_view_trig(const og_geom* g, int view, int fdk, float* s, float* c);
+
+/* ---- Siddon forward projector (V63/kernel_IterativeRecon_universal.cu:7-567) ---- */
+/* One ray.  Returns the ray sum; *len gets the summed chord length.  When
+ * nseg/hash are non-NULL they receive the segment count and an FNV-1a hash of
+ * the visited voxel index sequence.  entry64=1 computes the entry/exit alphas
+ * and the first plane indices in double (the engine's optional FP64 entry). */
+float og_fp_ray(const og_geom* g, const float* vol, float s, float c, int u, int v,
+                int entry64, float* len, int* nseg, uint64_t* hash);
+/* command 0: out = A f ; command 1: out = (b - A f)/len (SART correction). */
+void og_forward_view(const og_geom* g, const float* vol, float s, float c, int command,
+                     const float* b, float* out, int entry64);
+void og_forward_trace(const og_geom* g, const float* vol, float s, float c, int entry64,
+                      int* nseg, uint64_t* hash, float* len);
+/* The same traversal in double throughout: the FP64 oracle. */
+void og_forward_view_f64(const og_geom* g, const double* vol, double s, double c, double* out);
+
+/* ---- reference voxel-driven BP (V63/kernel_IterativeRecon_universal.cu:571-810) ---- */
+void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float beta,
+                        float s, float c, int command);
+
+/* ---- exact adjoint of og_fp_ray, by scattering each ray's segments ----
+ * acc[idx] += seg * y[ray]; lacc (optional) += seg, for segments whose length
+ * is above the reference BP's threshold vx*1e-6 when thresh=1. */
+void og_adjoint_view(const og_geom* g, const float* y, float s, float c, int thresh,
+                     double* acc, double* lacc);
+void og_adjoint_view_f64(const og_geom* g, const double* y, double s, double c, double* acc);
+/* FOV cylinder test of the reference BP (V63/...universal.cu:626-628): 1 = masked. */
+int  og_fov_masked(const og_geom* g, int i, int j);
+
+/* ---- SART pass drivers (V63/host_IterativeRecon_CBCT.c:1-67) ---- */
+/* reference semantics: FP command 1, then the reference BP command 1, per view */
+void og_sart_pass_ref(const og_geom* g, float* vol, const float* sino, float beta);
+/* engine semantics: the BP uses the FP's own chord lengths (matched adjoint) */
+void og_sart_pass_matched(const og_geom* g, float* vol, const float* sino, float beta);
+void og_sart_pass_f64(const og_geom* g, double* vol, const double* sino, double beta);
+
+/* ---- FGP TV prox, 7-array GPU form (V63/kernel_FGP_Denoise_GPUx7.cu:2-88,
+ *      driver V63/host_FGP_Denoise_GPUx7.c:1-111) ---- */
+void og_fgp(int M, int N, int Z, const float* f, float lambda, int iters, float* out);
+void og_fgp_f64(int M, int N, int Z, const double* f, double lambda, int iters, double* out);
+
+/* ---- objective (V63/kernel_tool_functions.cu:30-65, V63/host_tool_functions.cu:18-101) ---- */
+double og_tv_norm(int M, int N, int Z, const float* vol);
+double og_l2_norm(const float* a, const float* b, long long n);
+
+/* ---- FISTA outer step (V63/main_recon.cu:372-384) ---- */
+void og_fista_momentum(long long n, float* y, float* xprev, const float* x, float t_prev, float t_k);
+
+/* ---- FDK (V63/host_FDK.cpp, V63/FDK/kernel_FDK.cu, V63/FDK/FFT_1d_GPU.h:241-287) ---- */
+void og_fdk_weight(const og_geom* g, const float* in, float* out, int nviews);
+/* Spatial kernel equivalent to the reference's padded-DFT ramp: h[n+R-1], n in (-R,R). */
+void og_ramp_kernel(const og_geom* g, double* h);
+/* Ramp filtering of every row: direct linear convolution with og_ramp_kernel. */
+void og_ramp_filter(const og_geom* g, const float* in, float* out, int nrows);
+/* The reference's frequency-domain form evaluated by direct DFT (slow; small sizes). */
+void og_ramp_filter_dft(const og_geom* g, const float* in, float* out, int nrows);
+void og_fdk_bp_view(const og_geom* g, float* vol, const float* view, float s, float c);
+void og_fdk(const og_geom* g, const float* sino, float* vol);
+
+/* ---- seeded ellipsoid phantoms ---- */
+/* params: n x 10 doubles: cx,cy,cz, ax,ay,az, phi,theta,psi (rad), mu */
+void og_phantom_voxelize(const og_geom* g, const double* params, int n, float* vol);
+void og_phantom_project(const og_geom* g, const double* params, int n, double s, double c,
+                        float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,279 @@
+/*
+ * ref_harness.cpp -- runs the reference's own CUDA kernel sources on the CPU.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline, never the
+ * product).  The Makefile compiles this file with -DREF_DIR pointing at the
+ * reference's CBCT v6.3 snapshot; the reference sources are #included from
+ * where they lie and are not copied.  Output: oracle/_ref/libctref.so.
+ *
+ * CUDA keywords are defined away, threadIdx/blockIdx/blockDim/gridDim become
+ * thread-local variables that the launch loops below set, and the reference's
+ * compile-time geometry constants (V63/main_recon.cu:54-111) become mutable
+ * globals set by ref_set_geometry() with the same float/double steps.
+ */
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cstdint>
+using namespace std;
+
+struct ref_dim3 { unsigned x, y, z; };
+static thread_local ref_dim3 tl_threadIdx, tl_blockIdx, tl_blockDim, tl_gridDim;
+#define threadIdx tl_threadIdx
+#define blockIdx tl_blockIdx
+#define blockDim tl_blockDim
+#define gridDim tl_gridDim
+#define __global__
+#define __device__
+#define __host__
+#define __shared__
+static inline void __syncthreads() {}
+float sdata[1];   /* satisfies the never-called shared-memory reduction kernels */
+
+#define CT_style 0
+#define MAX_infi (1.0 / 0.0)
+
+/* geometry globals with the reference's names */
+static int M, N, ZETA, NO_X, NO_Y, NO_Z, NO_VOXEL, R, Z_prj, M_Offset, Nviews;
+static float DSO, DOD, Offset, Detector_pixel_x, Detector_Ymin, Detector_Zmin;
+static float volumn_x, inv_volumn_x, boundary_voxel_x;
+static float volumn_y, inv_volumn_y, boundary_voxel_y;
+static float volumn_z, inv_volumn_z, boundary_voxel_z;
+static float Source_x, Source_y, Source_z;
+static float us_rate, initialAngle, shiftAngle;
+static const float PI = 3.141592653589793f;
+
+#define REF_STR2(x) #x
+#define REF_STR(x) REF_STR2(x)
+#include REF_STR(REF_DIR/kernel_IterativeRecon_universal.cu)
+#include REF_STR(REF_DIR/kernel_FGP_Denoise_GPUx7.cu)
+#include REF_STR(REF_DIR/kernel_tool_functions.cu)
+#include REF_STR(REF_DIR/FDK/kernel_FDK.cu)
+#include REF_STR(REF_DIR/FDK/FFT1d.h)
+
+#include "ct_oracle.h"
+
+extern "C" {
+
+/* V63/main_recon.cu:60-111 with the constants taken from the description. */
+int ref_set_geometry(const og_desc* d)
+{
+    if (d->vy > 0.f && d->vy != d->vx) return -1;   /* the reference has one voxel pitch */
+    if (d->vz > 0.f && d->vz != d->vx) return -1;
+    if (d->dv > 0.f && d->dv != d->du) return -1;   /* and one detector pitch */
+    M = d->nx; N = d->ny; ZETA = d->nz;
+    NO_X = M; NO_Y = N; NO_Z = ZETA; NO_VOXEL = M * N * ZETA;
+    R = d->nu; Z_prj = d->nv; Nviews = d->nviews;
+    DSO = d->dso; DOD = d->dod; Offset = d->offset; M_Offset = d->m_offset;
+    Detector_pixel_x = d->du;
+    Detector_Ymin = -Detector_pixel_x * (float(R) / 2.0f - 0.5f) + Offset;
+    Detector_Zmin = -Detector_pixel_x * (float(Z_prj) / 2.0f - 0.5f);
+    volumn_x = d->vx;
+    inv_volumn_x = 1.0 / volumn_x;
+    boundary_voxel_x = -volumn_x * (float(M) / 2.0f + M_Offset);
+    volumn_y = volumn_x;
+    inv_volumn_y = 1.0 / volumn_y;
+    boundary_voxel_y = -volumn_y * (float(N) / 2.0f);
+    volumn_z = volumn_x;
+    inv_volumn_z = 1.0 / volumn_z;
+    boundary_voxel_z = -volumn_z * (float(ZETA) / 2.0f);
+    Source_x = DSO; Source_y = Offset; Source_z = 0;
+    us_rate = d->us_rate; initialAngle = d->initial_angle; shiftAngle = d->shift_angle;
+    return 0;
+}
+
+/* V63/host_IterativeRecon_CBCT.c:34-41 */
+void ref_view_trig(int j, int fdk, float* s_out, float* c_out)
+{
+    float t_theta = (float)(j * us_rate + initialAngle);
+    t_theta = (t_theta + shiftAngle) * PI / 180.0f;
+    if (!fdk) t_theta = -t_theta;
+    *s_out = sin(t_theta);
+    *c_out = cos(t_theta);
+}
+
+/* forward_ray_driven_3d_kernel_correction over grid (1, Z_prj) x block R */
+void ref_forward_view(const float* vol, float* out, const float* b, float s, float c, int command)
+{
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int v = 0; v < Z_prj; ++v) {
+        tl_blockDim = {(unsigned)R, 1, 1};
+        tl_gridDim = {1, (unsigned)Z_prj, 1};
+        for (int u = 0; u < R; ++u) {
+            tl_blockIdx = {0, (unsigned)v, 0};
+            tl_threadIdx = {(unsigned)u, 0, 0};
+            forward_ray_driven_3d_kernel_correction((float*)vol, out, (float*)b, s, c, command);
+        }
+    }
+}
+
+/* backprj_ray_driven_3d_kernel over grid (1, N, ZETA) x block M */
+void ref_backproject_view(float* vol, const float* corr, float beta, float s, float c, int command)
+{
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = 0; k < ZETA; ++k)
+        for (int j = 0; j < N; ++j) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            tl_gridDim = {1, (unsigned)N, (unsigned)ZETA};
+            for (int i = 0; i < M; ++i) {
+                tl_blockIdx = {0, (unsigned)j, (unsigned)k};
+                tl_threadIdx = {(unsigned)i, 0, 0};
+                backprj_ray_driven_3d_kernel(vol, (float*)corr, beta, s, c, command);
+            }
+        }
+}
+
+/* Reconstruction_3D_ray_driven_CBCT (V63/host_IterativeRecon_CBCT.c:1-67) for
+ * the views [v0, v0+nv): FP command 1 then BP command 1, strictly in order. */
+void ref_sart_views(float* vol, const float* sino, float beta, int v0, int nv)
+{
+    const long long P = (long long)R * Z_prj;
+    float* corr = (float*)malloc(sizeof(float) * P);
+    for (int j = v0; j < v0 + nv; ++j) {
+        float s, c;
+        ref_view_trig(j, 0, &s, &c);
+        ref_forward_view(vol, corr, sino + P * j, s, c, 1);
+        ref_backproject_view(vol, corr, beta, s, c, 1);
+    }
+    free(corr);
+}
+
+/* FGP_denoise_GPUx7_exact (V63/host_FGP_Denoise_GPUx7.c:1-111), in place */
+void ref_fgp(float* f, float lambda, int niter)
+{
+    const long long V = (long long)M * N * ZETA;
+    const long long nr = (long long)ZETA * N * (M + 1), ns = (long long)ZETA * (N + 1) * M,
+                    nt = (long long)(ZETA + 1) * N * M;
+    float* r = (float*)calloc(nr, 4); float* o = (float*)calloc(nr, 4);
+    float* s = (float*)calloc(ns, 4); float* p = (float*)calloc(ns, 4);
+    float* t = (float*)calloc(nt, 4); float* q = (float*)calloc(nt, 4);
+    float* L = (float*)calloc(V, 4);
+    float t_k_1 = 1.0f, t_k;
+    auto launch = [&](int which) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int z = 0; z < ZETA; ++z)
+            for (int y = 0; y < N; ++y) {
+                tl_blockDim = {(unsigned)M, 1, 1};
+                tl_gridDim = {(unsigned)N, (unsigned)ZETA, 1};
+                for (int x = 0; x < M; ++x) {
+                    tl_blockIdx = {(unsigned)y, (unsigned)z, 0};
+                    tl_threadIdx = {(unsigned)x, 0, 0};
+                    if (which == 0) FGP_operator_L_Pc(f, r, s, t, L, lambda);
+                    else if (which == 1) FGP_operator_LT_Pp(r, s, t, L, o, p, q, t_k_1, t_k, 1.0f / (lambda * 12.0f));
+                    else FGP_operator_L_Pc(f, o, p, q, L, lambda);
+                }
+            }
+    };
+    for (int i = 0; i < niter; ++i) {
+        t_k = (1.0f + sqrt(1.0f + 4.0f * t_k_1 * t_k_1)) / 2.0f;
+        launch(0);
+        launch(1);
+        t_k_1 = t_k;
+    }
+    launch(2);
+    memcpy(f, L, sizeof(float) * V);
+    free(r); free(o); free(s); free(p); free(t); free(q); free(L);
+}
+
+/* TV_norm_kernel into a zeroed buffer, summed in double (the reference's
+ * alternative CPU summation, V63/host_tool_functions.cu:81-87) */
+double ref_tv_norm(const float* vol)
+{
+    const long long V = (long long)M * N * ZETA;
+    float* tv = (float*)calloc(V, 4);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < ZETA; ++z)
+        for (int y = 0; y < N; ++y) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            for (int x = 0; x < M; ++x) {
+                tl_blockIdx = {0, (unsigned)y, (unsigned)z};
+                tl_threadIdx = {(unsigned)x, 0, 0};
+                TV_norm_kernel(tv, (float*)vol);
+            }
+        }
+    double acc = 0.0;
+    for (long long i = 0; i < V; ++i) acc += (double)tv[i];
+    free(tv);
+    return acc;
+}
+
+/* L2_norm_kernel over (nviews, Z_prj, R), summed in double (the reference's
+ * CPU summation, V63/host_tool_functions.cu:37-44); a is overwritten. */
+double ref_l2_norm(float* a, const float* b, int nviews)
+{
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int w = 0; w < nviews; ++w)
+        for (int v = 0; v < Z_prj; ++v) {
+            tl_blockDim = {(unsigned)R, 1, 1};
+            tl_gridDim = {1, (unsigned)Z_prj, (unsigned)nviews};
+            for (int u = 0; u < R; ++u) {
+                tl_blockIdx = {0, (unsigned)v, (unsigned)w};
+                tl_threadIdx = {(unsigned)u, 0, 0};
+                L2_norm_kernel(a, (float*)b);
+            }
+        }
+    double acc = 0.0;
+    const long long n = (long long)nviews * R * Z_prj;
+    for (long long i = 0; i < n; ++i) acc += (double)a[i];
+    return acc;
+}
+
+/* kernel_FDK_projection_adjust over (1, Z_prj, nviews) x R */
+void ref_fdk_weight(const float* in, float* out, int nviews)
+{
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int w = 0; w < nviews; ++w)
+        for (int v = 0; v < Z_prj; ++v) {
+            tl_blockDim = {(unsigned)R, 1, 1};
+            for (int u = 0; u < R; ++u) {
+                tl_blockIdx = {0, (unsigned)v, (unsigned)w};
+                tl_threadIdx = {(unsigned)u, 0, 0};
+                kernel_FDK_projection_adjust((float*)in, out);
+            }
+        }
+}
+
+/* RampFiltering_GPU (V63/FDK/FFT_1d_GPU.h:241-287) with the reference's own
+ * CPU mixed-radix FFT (V63/FDK/FFT1d.h) in place of cuFFT.  Serial: FFT1d.h
+ * keeps its state in file-scope statics. */
+void ref_ramp_filter(const float* in, float* out, int nrows)
+{
+    const int pad_size = R * 2;
+    float F_max = 1.0 / 2.0 / (Detector_pixel_x * DSO / (DSO - DOD));
+    float F_step = F_max / (pad_size / 2);
+    float* H = (float*)malloc(sizeof(float) * pad_size);
+    for (int i = 0; i < pad_size; i++) {
+        const int k = (i >= pad_size / 2) ? i - pad_size : i;
+        H[i] = abs(k) * F_step;
+        H[i] *= 0.5f;
+    }
+    complex<double>* x = new complex<double>[pad_size];
+    for (int r = 0; r < nrows; ++r) {
+        for (int i = 0; i < pad_size; ++i) x[i] = complex<double>(i < R ? in[(long long)r * R + i] : 0.0, 0.0);
+        FFT(x, pad_size, 1);
+        for (int i = 0; i < pad_size; ++i) x[i] *= (double)H[i];
+        FFT(x, pad_size, -1);          /* FLAG=-1 divides by n, like the reference's /pad_size */
+        for (int j = 0; j < R; ++j) out[(long long)r * R + j] = (float)x[j].real();
+    }
+    delete[] x;
+    free(H);
+}
+
+/* kernel_FDK_reconstruction over (1, N, ZETA) x M, one view */
+void ref_fdk_bp_view(float* vol, const float* proj, float s, float c)
+{
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < ZETA; ++k)
+        for (int j = 0; j < N; ++j) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            for (int i = 0; i < M; ++i) {
+                tl_blockIdx = {0, (unsigned)j, (unsigned)k};
+                tl_threadIdx = {(unsigned)i, 0, 0};
+                kernel_FDK_reconstruction(vol, (float*)proj, s, c);
+            }
+        }
+}
+
+}  /* extern "C" */
