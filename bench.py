@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""SART + FISTA + FGP-TV iterations/s on the 512^3 / 1024-view CBCT scan.
+
+One step = one outer iteration of the reference's FISTA loop
+(V63/main_recon.cu:344-430): a SART pass over all 1024 views (Siddon FP
+correction + gather BP update per view, in order), the FGP-TV prox with 20
+inner iterations, the FISTA momentum and the objective (a forward
+projection of all views plus the TV norm).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Each rank reconstructs its own copy of the scan (replicas: the path has no
+data exchange between scans), so ``value`` is the sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCAN = dict(nx=512, ny=512, nz=512, vx=0.5, nu=1024, nv=768, du=0.4, dso=1000.0, dod=-500.0, n_views=1024)
+BETA, LAMBDA_TV, FGP_ITERS = 0.8, 2e-4, 20
+METRIC = "SART-FISTA-TV iter/s & voxel-updates/s, 512^3 x 1024 views, mixed vs FP32, 1 B200"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--mixed", choices=["f16", "bf16"], default="f16")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def phantom_params(seed=2024):
+    """40 ellipsoids (semi-axes 3-100 mm, 0.005-0.04 /mm) + 200 spheres (r 1-3 mm, 0.05 /mm)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n1, n2 = 40, 200
+    p = np.zeros((n1 + n2, 10))
+    p[:n1, 0:2] = rng.uniform(-60, 60, (n1, 2))
+    p[:n1, 2] = rng.uniform(-60, 60, n1)
+    p[:n1, 3:6] = rng.uniform(3, 100, (n1, 3))
+    p[:n1, 6:9] = rng.uniform(0, 2 * np.pi, (n1, 3))
+    p[:n1, 9] = rng.uniform(0.005, 0.04, n1)
+    r = rng.uniform(1, 3, n2)
+    ang = rng.uniform(0, 2 * np.pi, n2)
+    rad = 100 * np.sqrt(rng.uniform(0, 1, n2))
+    p[n1:, 0], p[n1:, 1] = rad * np.cos(ang), rad * np.sin(ang)
+    p[n1:, 2] = rng.uniform(-90, 90, n2)
+    p[n1:, 3:6] = r[:, None]
+    p[n1:, 9] = 0.05
+    return p
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
+        if not self.rows:
+            return out
+        import statistics
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        out["sm_mhz"] = statistics.median(sm) if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        out["reasons"] = sorted(reasons)
+        return out
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the backprojector from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(steps_hint=1, budget_s=12.0):
+    """The reference's own kernels compiled for the CPU (oracle/_ref), timed on
+    this host's cores on a bounded sample of one iteration, scaled to a full
+    iteration: S views of the SART pass and of the objective forward
+    projection (x 1024/S), 2 of the 20 FGP inner iterations (x 10), TV norm."""
+    import numpy as np
+
+    from oracle import ctoracle
+    d = ctoracle.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["nu"], SCAN["nv"], SCAN["n_views"], SCAN["vx"],
+                           SCAN["du"], SCAN["dso"], SCAN["dod"])
+    ref = ctoracle.RefOracle(d)
+    rng = np.random.default_rng(0)
+    vol = rng.uniform(0.0, 0.02, ref.vol_shape).astype(np.float32)
+    nviews = SCAN["n_views"]
+    b_view = rng.uniform(0.0, 5.0, (1,) + ref.view_shape).astype(np.float32)
+    # calibrate on one SART view, then size the sample to the budget
+    ref._set()
+    out = vol.copy()
+    t0 = time.perf_counter()
+    s, c = ref.trig(0)
+    corr = np.zeros(ref.view_shape, np.float32)
+    ref.lib.ref_forward_view(out, corr, b_view[0].ctypes.data, s, c, 1)
+    ref.lib.ref_backproject_view(out, corr, BETA, s, c, 1)
+    t_one = time.perf_counter() - t0
+    s_views = max(1, min(64, int(0.4 * budget_s / max(t_one, 1e-3))))
+    stride = max(1, nviews // s_views)
+    views = list(range(0, nviews, stride))[:s_views]
+    t0 = time.perf_counter()
+    for j in views:
+        s, c = ref.trig(j)
+        corr = np.zeros(ref.view_shape, np.float32)
+        ref.lib.ref_forward_view(out, corr, b_view[0].ctypes.data, s, c, 1)
+        ref.lib.ref_backproject_view(out, corr, BETA, s, c, 1)
+    t_sart = (time.perf_counter() - t0) / len(views) * nviews
+    t0 = time.perf_counter()
+    for j in views:
+        s, c = ref.trig(j)
+        fp = np.zeros(ref.view_shape, np.float32)
+        ref.lib.ref_forward_view(out, fp, None, s, c, 0)
+    t_obj = (time.perf_counter() - t0) / len(views) * nviews
+    t0 = time.perf_counter()
+    ref.fgp(out, BETA * LAMBDA_TV, 2)
+    t_fgp = (time.perf_counter() - t0) * FGP_ITERS / 2.0
+    t0 = time.perf_counter()
+    ref.tv_norm(out)
+    t_tv = time.perf_counter() - t0
+    t_iter = t_sart + t_obj + t_fgp + t_tv
+    cores = os.cpu_count()
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    return {
+        "value": 1.0 / t_iter, "unit": "iter/s", "cores": cores, "kind": "reference",
+        "sample": (f"reference kernels compiled for the CPU (OpenMP, {cores} threads): SART on {len(views)} of "
+                   f"{nviews} views and the objective forward projection on the same views (scaled x{nviews}/"
+                   f"{len(views)}), 2 of {FGP_ITERS} FGP inner iterations (x{FGP_ITERS // 2}), TV norm; "
+                   f"512^3 volume, 1024x768 detector"),
+        "seconds_per_iter": t_iter,
+        "parts_s": {"sart": t_sart, "objective_fp": t_obj, "fgp": t_fgp, "tv": t_tv},
+    }
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    times = []
+    info = None
+    for it in range(args.warmup + args.steps):
+        info = cpu_baseline()
+        if it >= args.warmup:
+            times.append(info["seconds_per_iter"])
+    ms = 1000.0 * sum(times) / len(times)
+    value = 1000.0 / ms
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "SART+FISTA+FGP-TV (20 inner) iteration, 512^3 x 0.5 mm, 1024 views, "
+                               "1024x768 detector x 0.4 mm, DSO 1000 mm, DOD -500 mm", "l2": "inputs > L2"},
+        "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")} | {"value": value},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "voxel_updates_per_s": value * SCAN["nx"] * SCAN["ny"] * SCAN["nz"] * SCAN["n_views"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import gpu_b200
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    desc = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
+                              SCAN["dso"], SCAN["dod"], SCAN["n_views"])
+    geom = gpu_b200.Geometry(desc)
+    vshape, sshape = geom.vol_shape, (SCAN["n_views"],) + geom.view_shape
+    V = SCAN["nx"] * SCAN["ny"] * SCAN["nz"]
+    P = SCAN["nu"] * SCAN["nv"]
+
+    # synthetic scan: seeded phantom, its Siddon projections + 0.5% Gaussian noise
+    truth = torch.zeros(vshape, device=dev)
+    geom.phantom_voxelize(phantom_params(2024 + rank), truth)
+    sino32 = torch.zeros(sshape, device=dev)
+    geom.forward(truth, sino32)
+    gen = torch.Generator(device=dev).manual_seed(77 + rank)
+    sino32 += 0.005 * sino32.max() * torch.randn(sshape, device=dev, generator=gen)
+    del truth
+    mixed_dt = torch.float16 if args.mixed == "f16" else torch.bfloat16
+    mixed_code = gpu_b200.F16 if args.mixed == "f16" else gpu_b200.BF16
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    runs = {}
+    stream = torch.cuda.current_stream()
+    for mode, vdt, sdt in (("f32", gpu_b200.F32, torch.float32), ("mixed", mixed_code, mixed_dt)):
+        sino = sino32 if sdt == torch.float32 else sino32.to(sdt)
+        solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
+                                 objective=True, use_graph=True)
+        solver.set_sinogram(sino)
+        solver.set_volume(None)
+        for _ in range(args.warmup):
+            solver.iterate(1)
+        barrier()
+        clocks = ClockSampler(local)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        objs = []
+        for _ in range(args.steps):
+            objs.append(solver.iterate(1)[0].tolist())
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1) / args.steps
+        runs[mode] = {"ms": max_over_ranks(ms), "clocks": clocks.stop(), "objective_last": objs[-1]}
+        runs[mode]["solver"] = solver
+        runs[mode]["sino"] = sino
+
+    # end to end through the public API with host buffers: every step copies the
+    # measured sinogram in from pinned host memory, runs one iteration and reads
+    # the objective and the reconstructed volume back
+    mode = "mixed"
+    solver, sino = runs[mode]["solver"], runs[mode]["sino"]
+    h_sino = sino.cpu().pin_memory()
+    h_vol = torch.empty(vshape, dtype=mixed_dt).pin_memory()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sino.copy_(h_sino, non_blocking=True)
+        solver.iterate(1)
+        solver.get_volume(h_vol)
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    h2d = h_sino.numel() * h_sino.element_size()
+    d2h = h_vol.numel() * h_vol.element_size() + 3 * 8
+
+    # per-kernel durations of the SART projector kernels, from CUDA events the
+    # library records around each launch on this stream (32 views spread over the scan)
+    kern = {}
+    for mode in ("f32", "mixed"):
+        sino = runs[mode]["sino"]
+        vol = torch.zeros(vshape, device=dev, dtype=torch.float32 if mode == "f32" else mixed_dt)
+        geom.sart_views(vol, sino, BETA, 0, 4)                       # warm-up
+        fp_t = bp_t = 0.0
+        nt = 32
+        for j in range(nt):
+            f_ms, b_ms = geom.sart_views(vol, sino, BETA, (j * 97) % SCAN["n_views"], 1, timed=True)
+            fp_t += f_ms
+            bp_t += b_ms
+        kern[mode] = {"fp_ms": fp_t / nt, "bp_ms": bp_t / nt}
+        del vol
+
+    peak, peak_kind = measured_peak_hbm()
+    s_v = 2  # mixed storage bytes
+    bp_bytes = 2 * V * s_v + 4 * P            # BP with SART update, per view (algorithmic)
+    bp_ms = kern["mixed"]["bp_ms"]
+    achieved = bp_bytes / (bp_ms * 1e-3) / 1e9
+    traffic = profiled_traffic()
+
+    line = None
+    if rank == 0:
+        ms_mixed = runs["mixed"]["ms"]
+        ms_f32 = runs["f32"]["ms"]
+        value = world * 1000.0 / ms_mixed
+        # SART: FP + BP per view; FGP: inner steps + final; objective: FP, 2 reduce, TV, reduce
+        launches_per_step = 2 * SCAN["n_views"] + FGP_ITERS + 1 + 1 + 2 + 1 + 1
+        line = {
+            "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"{args.mixed} storage, f32 arithmetic", "data": "synthetic",
+            "config": {"workload": "SART+FISTA+FGP-TV (20 inner) iteration with objective, 512^3 x 0.5 mm, "
+                                   "1024 views, 1024x768 detector x 0.4 mm, DSO 1000 mm, DOD -500 mm",
+                       "phantom": "40 ellipsoids + 200 spheres (seeded), Siddon projections + 0.5% noise",
+                       "parallelism": f"replicas x{world}", "l2": "inputs > L2 (512 MB+ volume)"},
+            "voxel_updates_per_s": value * V * SCAN["n_views"],
+            "f32": {"iter_per_s": world * 1000.0 / ms_f32, "ms_per_step": ms_f32,
+                    "voxel_updates_per_s": world * 1000.0 / ms_f32 * V * SCAN["n_views"]},
+            "mixed_over_f32": ms_f32 / ms_mixed,
+            "objective_last": {"f32": runs["f32"]["objective_last"], "mixed": runs["mixed"]["objective_last"]},
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "iter/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": "k_backproject (SART update, f16 volume)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind,
+                         "traffic": (traffic or {}).get("bytes_per_launch"),
+                         "algorithmic_bytes_per_launch": bp_bytes,
+                         "launch_ms": bp_ms},
+            "kernels_ms": kern,
+            "clocks": runs["mixed"]["clocks"],
+            "clocks_f32": runs["f32"]["clocks"],
+            "gpu_launches": launches_per_step * args.steps,
+        }
+    for m in runs.values():
+        m["solver"].close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                cb = cpu_baseline()
+                line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            except Exception as e:  # the CPU leg must not hide the GPU result
+                line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,783 @@
+// api.cpp -- the C ABI: argument checks, drivers for the reference's call
+// sequence (SART pass, SART+FISTA+TV iteration, FDK, objective) and the
+// reference-compatible host entry points.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "ctr_internal.h"
+
+using namespace ctr;
+
+namespace {
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+inline Geometry* GE(const ctr_geometry* g) { return const_cast<Geometry*>(reinterpret_cast<const Geometry*>(g)); }
+
+ctr_status check_views(const Geometry* g, int v0, int n)
+{
+    if (v0 < 0 || n < 0 || (long long)v0 + n > g->desc.n_views)
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "view range [%d, %d) outside [0, %d)", v0, v0 + n, g->desc.n_views);
+    return CTR_OK;
+}
+
+ctr_status need(const void* p, const char* what)
+{
+    if (!p) return set_error(CTR_ERR_INVALID_ARGUMENT, "%s is NULL", what);
+    return CTR_OK;
+}
+
+ctr_status need_dtype(int dt, const char* what)
+{
+    if (!dtype_ok(dt)) return set_error(CTR_ERR_INVALID_ARGUMENT, "%s: unknown dtype %d", what, dt);
+    return CTR_OK;
+}
+
+// views per adjoint pass: bounded so the ray records stay under ~256 MB
+int adjoint_batch(const Geometry* g)
+{
+    long long b = (256LL << 20) / (8LL * g->npix());
+    if (b < 1) b = 1;
+    if (b > 32) b = 32;
+    return (int)b;
+}
+
+// forward over [v0, v0+n) in launches of at most 65535 views
+ctr_status forward_chunks(Geometry* g, FpArgs a, cudaStream_t st)
+{
+    const long long P = g->npix();
+    const int v0 = a.view0, n = a.nview;
+    for (int c = 0; c < n; c += 65535) {
+        FpArgs b = a;
+        b.view0 = v0 + c;
+        b.nview = std::min(65535, n - c);
+        if (a.out) b.out = (char*)a.out + (size_t)c * P * (a.kind == FP_SART ? sizeof(float2) : dtype_size(a.out_dtype));
+        if (a.b) b.b = (const char*)a.b + (size_t)c * P * dtype_size(a.b_dtype);
+        CTR_TRY(launch_forward(*g, b, st, nullptr));
+    }
+    return CTR_OK;
+}
+
+// SART pass: per view FP command 1 -> ray records, then BP command 1.
+// With ev (3 events per view) the launches are bracketed for timing.
+ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
+                      unsigned flags, uint32_t seed, int v0, int nv, cudaStream_t st, cudaEvent_t* ev)
+{
+    const long long P = g->npix();
+    CTR_TRY(ensure_rays(g, (size_t)P));
+    for (int j = v0; j < v0 + nv; ++j) {
+        if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0)], st));
+        FpArgs a{};
+        a.vol = vol; a.vol_dtype = vdt; a.view0 = j; a.nview = 1; a.kind = FP_SART;
+        a.out = g->d_rays; a.b = (const char*)sino + (size_t)j * P * dtype_size(sdt); a.b_dtype = sdt;
+        CTR_TRY(launch_forward(*g, a, st, nullptr));
+        if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0) + 1], st));
+        BpArgs b{};
+        b.vol = vol; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = j; b.nview = 1; b.sart = 1;
+        b.flags = flags; b.beta = beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j;
+        CTR_TRY(launch_backproject(*g, b, st));
+        if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0) + 2], st));
+    }
+    return CTR_OK;
+}
+
+ctr_status sart_pass(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
+                     unsigned flags, uint32_t seed, cudaStream_t st)
+{
+    return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, 0, g->desc.n_views, st, nullptr);
+}
+
+ctr_status objective_async(Geometry* g, const void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt,
+                           double* d_fid, double* d_tv, cudaStream_t st)
+{
+    const DevGeom& q = g->dg;
+    const size_t per_view = (size_t)((q.R + 31) / 32) * ((q.ZP + 3) / 4);
+    const size_t nblk = per_view * g->desc.n_views;
+    const size_t tvcap = 148 * 64;
+    CTR_TRY(ensure_partial(g, std::max(nblk, tvcap) + 2048));
+    if (d_fid) {
+        FpArgs a{};
+        a.vol = vol; a.vol_dtype = vdt; a.view0 = 0; a.nview = g->desc.n_views; a.kind = FP_OBJECTIVE;
+        a.b = sino; a.b_dtype = sdt; a.partial = g->d_partial;
+        const long long P = g->npix();
+        for (int c = 0; c < g->desc.n_views; c += 65535) {
+            FpArgs b = a;
+            b.view0 = c;
+            b.nview = std::min(65535, g->desc.n_views - c);
+            b.b = (const char*)sino + (size_t)c * P * dtype_size(sdt);
+            b.partial = g->d_partial + (size_t)c * per_view;
+            CTR_TRY(launch_forward(*g, b, st, nullptr));
+        }
+        CTR_TRY(launch_reduce(g->d_partial, nblk, d_fid, st));
+    }
+    if (d_tv) CTR_TRY(launch_tv(*g, vol, vdt, g->d_partial, tvcap, d_tv, st));
+    return CTR_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ projectors
+
+extern "C" ctr_status ctr_forward(const ctr_geometry* geom, const void* vol, ctr_dtype vdt, void* sino,
+                                  ctr_dtype sdt, int v0, int n, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    CTR_TRY(need_dtype(sdt, "sino_dtype"));
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, v0, n));
+    FpArgs a{};
+    a.vol = vol; a.vol_dtype = vdt; a.view0 = v0; a.nview = n; a.kind = FP_FORWARD; a.out = sino; a.out_dtype = sdt;
+    return forward_chunks(g, a, S(stream));
+}
+
+extern "C" ctr_status ctr_backproject(const ctr_geometry* geom, const float* sino, int v0, int n, void* vol,
+                                      ctr_dtype vdt, unsigned flags, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, v0, n));
+    cudaStream_t st = S(stream);
+    const long long P = g->npix();
+    const bool masked = (flags & CTR_BP_FOV_MASK) != 0;
+    const int batch = masked ? 1 : adjoint_batch(g);
+    if (n == 0) {
+        if (!(flags & CTR_BP_ACCUMULATE)) CTR_CUDA_TRY(cudaMemsetAsync(vol, 0, g->nvox() * dtype_size(vdt), st));
+        return CTR_OK;
+    }
+    CTR_TRY(ensure_rays(g, (size_t)P * batch));
+    for (int c = 0; c < n; c += batch) {
+        const int cnt = std::min(batch, n - c);
+        CTR_TRY(launch_ray_prep(*g, sino + (size_t)c * P, v0 + c, cnt, g->d_rays, st));
+        BpArgs b{};
+        b.vol = vol; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = v0 + c; b.nview = cnt; b.sart = 0;
+        b.flags = (flags & CTR_BP_FOV_MASK) | ((c > 0 || (flags & CTR_BP_ACCUMULATE)) ? CTR_BP_ACCUMULATE : 0u);
+        CTR_TRY(launch_backproject(*g, b, st));
+    }
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_sart_pass(const ctr_geometry* geom, void* vol, ctr_dtype vdt, const void* sino,
+                                    ctr_dtype sdt, float beta, unsigned flags, uint32_t seed, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    CTR_TRY(need_dtype(sdt, "sino_dtype"));
+    if (!std::isfinite(beta)) return set_error(CTR_ERR_INVALID_ARGUMENT, "beta must be finite");
+    return sart_pass(GE(geom), vol, vdt, sino, sdt, beta, flags, seed, S(stream));
+}
+
+extern "C" ctr_status ctr_sart_views(const ctr_geometry* geom, void* vol, ctr_dtype vdt, const void* sino,
+                                     ctr_dtype sdt, float beta, unsigned flags, uint32_t seed, int v0, int n,
+                                     float* fp_ms, float* bp_ms, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    CTR_TRY(need_dtype(sdt, "sino_dtype"));
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, v0, n));
+    if (!std::isfinite(beta)) return set_error(CTR_ERR_INVALID_ARGUMENT, "beta must be finite");
+    cudaStream_t st = S(stream);
+    if (!fp_ms && !bp_ms) return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, v0, n, st, nullptr);
+    std::vector<cudaEvent_t> ev(3 * (size_t)n, nullptr);
+    ctr_status r = CTR_OK;
+    for (auto& e : ev)
+        if (r == CTR_OK && cudaEventCreate(&e) != cudaSuccess) r = set_error(CTR_ERR_CUDA, "cudaEventCreate");
+    if (r == CTR_OK) r = sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, v0, n, st, ev.data());
+    if (r == CTR_OK && cudaStreamSynchronize(st) != cudaSuccess) r = set_error(CTR_ERR_CUDA, "cudaStreamSynchronize");
+    float tf = 0.f, tb = 0.f;
+    for (int j = 0; r == CTR_OK && j < n; ++j) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, ev[3 * j], ev[3 * j + 1]);
+        cudaEventElapsedTime(&b, ev[3 * j + 1], ev[3 * j + 2]);
+        tf += a;
+        tb += b;
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (fp_ms) *fp_ms = tf;
+    if (bp_ms) *bp_ms = tb;
+    return r;
+}
+
+extern "C" ctr_status ctr_forward_trace(const ctr_geometry* geom, const float* vol, int view, int* nseg,
+                                        uint64_t* hash, float* len, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(nseg, "nseg"));
+    CTR_TRY(need(hash, "hash"));
+    CTR_TRY(need(len, "len"));
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, view, 1));
+    FpArgs a{};
+    a.vol = vol; a.vol_dtype = CTR_F32; a.view0 = view; a.nview = 1; a.kind = FP_TRACE;
+    a.nseg = nseg; a.hash = hash; a.len = len;
+    return launch_forward(*g, a, S(stream), nullptr);
+}
+
+// ------------------------------------------------------------- TV and FISTA
+
+extern "C" ctr_status ctr_fgp_tv(const ctr_geometry* geom, void* vol, ctr_dtype dt, float lambda, int n_iter,
+                                 void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need_dtype(dt, "dtype"));
+    if (!(lambda > 0.f) || !std::isfinite(lambda)) return set_error(CTR_ERR_INVALID_ARGUMENT, "lambda must be positive");
+    if (n_iter < 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "n_iter must be >= 0");
+    return launch_fgp(*GE(geom), vol, dt, lambda, n_iter, nullptr, nullptr, 0.f, S(stream));
+}
+
+extern "C" ctr_status ctr_fista_momentum(const ctr_geometry* geom, void* y, void* xprev, const void* x,
+                                         ctr_dtype dt, float t_prev, float t_k, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(y, "y"));
+    CTR_TRY(need(xprev, "x_prev"));
+    CTR_TRY(need(x, "x"));
+    CTR_TRY(need_dtype(dt, "dtype"));
+    if (!(t_k != 0.f)) return set_error(CTR_ERR_INVALID_ARGUMENT, "t_k must be non-zero");
+    const float gam = (t_prev - 1.0f) / t_k;
+    return launch_momentum(*GE(geom), y, xprev, x, dt, gam, S(stream));
+}
+
+// ---------------------------------------------------------------- objective
+
+extern "C" ctr_status ctr_objective(const ctr_geometry* geom, const void* vol, ctr_dtype vdt, const void* sino,
+                                    ctr_dtype sdt, double* fid, double* tv, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    CTR_TRY(need_dtype(sdt, "sino_dtype"));
+    Geometry* g = GE(geom);
+    cudaStream_t st = S(stream);
+    CTR_TRY(objective_async(g, vol, vdt, sino, sdt, g->d_result, g->d_result + 1, st));
+    double h[2];
+    CTR_CUDA_TRY(cudaMemcpyAsync(h, g->d_result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTR_TRY(check_device_errors(g, st));
+    if (fid) *fid = h[0];
+    if (tv) *tv = h[1];
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_tv_norm(const ctr_geometry* geom, const void* vol, ctr_dtype dt, double* out, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(out, "out"));
+    CTR_TRY(need_dtype(dt, "dtype"));
+    Geometry* g = GE(geom);
+    cudaStream_t st = S(stream);
+    CTR_TRY(ensure_partial(g, 148 * 64 + 2048));
+    CTR_TRY(launch_tv(*g, vol, dt, g->d_partial, 148 * 64, g->d_result, st));
+    CTR_CUDA_TRY(cudaMemcpyAsync(out, g->d_result, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTR_CUDA_TRY(cudaStreamSynchronize(st));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_l2_norm(const float* a, const float* b, int64_t n, double* out, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(a, "a"));
+    CTR_TRY(need(b, "b"));
+    CTR_TRY(need(out, "out"));
+    if (n < 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "n < 0");
+    cudaStream_t st = S(stream);
+    double* buf = nullptr;
+    const size_t cap = 148 * 64;
+    CTR_CUDA_TRY(cudaMalloc(&buf, (cap + 2048 + 1) * sizeof(double)));
+    ctr_status s = launch_l2(a, b, n, buf, cap, buf + cap + 2048, st);
+    if (s == CTR_OK) {
+        cudaError_t e = cudaMemcpyAsync(out, buf + cap + 2048, sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) s = cuda_error(e, "ctr_l2_norm");
+    }
+    cudaFree(buf);
+    return s;
+}
+
+// --------------------------------------------------------------------- FDK
+
+extern "C" ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float* vol, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need(vol, "vol"));
+    return launch_fdk(*GE(geom), sino, vol, S(stream));
+}
+
+// -------------------------------------------------------------- dot product
+
+extern "C" ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, const float* y, int v0, int n,
+                                   double* ax_y, double* x_aty, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(x, "x"));
+    CTR_TRY(need(y, "y"));
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, v0, n));
+    cudaStream_t st = S(stream);
+    const long long P = g->npix(), V = g->nvox();
+    float* ax = nullptr;
+    float* aty = nullptr;
+    CTR_CUDA_TRY(cudaMalloc(&ax, sizeof(float) * (size_t)P * (n > 0 ? n : 1)));
+    ctr_status s = CTR_OK;
+    cudaError_t e = cudaMalloc(&aty, sizeof(float) * (size_t)V);
+    if (e != cudaSuccess) s = cuda_error(e, "cudaMalloc");
+    const size_t cap = 148 * 64;
+    if (s == CTR_OK) s = ensure_partial(g, cap + 2048);
+    if (s == CTR_OK) s = ctr_forward(geom, x, CTR_F32, ax, CTR_F32, v0, n, stream);
+    if (s == CTR_OK) s = ctr_backproject(geom, y, v0, n, aty, CTR_F32, 0, stream);
+    if (s == CTR_OK) s = launch_dot(ax, y, P * n, g->d_partial, cap, g->d_result, st);
+    if (s == CTR_OK) s = launch_dot(x, aty, V, g->d_partial, cap, g->d_result + 1, st);
+    double h[2] = {0, 0};
+    if (s == CTR_OK) {
+        e = cudaMemcpyAsync(h, g->d_result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) s = cuda_error(e, "cudaMemcpyAsync");
+    }
+    if (s == CTR_OK) s = check_device_errors(g, st);
+    cudaFree(ax);
+    cudaFree(aty);
+    if (s == CTR_OK) {
+        if (ax_y) *ax_y = h[0];
+        if (x_aty) *x_aty = h[1];
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- utilities
+
+extern "C" ctr_status ctr_convert(const void* src, ctr_dtype sdt, void* dst, ctr_dtype ddt, int64_t n, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(src, "src"));
+    CTR_TRY(need(dst, "dst"));
+    CTR_TRY(need_dtype(sdt, "src_dtype"));
+    CTR_TRY(need_dtype(ddt, "dst_dtype"));
+    if (n < 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "n < 0");
+    if (n == 0) return CTR_OK;
+    return launch_convert(src, sdt, dst, ddt, n, S(stream));
+}
+
+extern "C" ctr_status ctr_phantom_voxelize(const ctr_geometry* geom, const double* params, int n, float* vol,
+                                           void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    if (n < 0 || (n > 0 && !params)) return set_error(CTR_ERR_INVALID_ARGUMENT, "bad ellipsoid list");
+    for (int a = 0; a < n; ++a)
+        for (int b = 3; b < 6; ++b)
+            if (!(params[10 * a + b] > 0.0)) return set_error(CTR_ERR_INVALID_ARGUMENT, "ellipsoid %d: semi-axes must be > 0", a);
+    if (n == 0) return CTR_OK;
+    return launch_phantom(*GE(geom), params, n, vol, S(stream));
+}
+
+// ------------------------------------------------------------------ solver
+
+struct ctr_solver {
+    Geometry* g = nullptr;
+    ctr_dtype vdt = CTR_F32;
+    ctr_solver_params p{};
+    const void* sino = nullptr;
+    ctr_dtype sdt = CTR_F32;
+    void* y = nullptr;       // working volume: y_k, then x_k during an iteration
+    void* xprev = nullptr;   // x_(k-1); after an iteration with FISTA, x_k
+    float t = 1.0f;          // t_(k-1) of V63/main_recon.cu:177
+    int k = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double* d_obj = nullptr; // [2] fid, tv
+};
+
+extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt, const ctr_solver_params* p,
+                                        ctr_solver** out)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(p, "params"));
+    CTR_TRY(need(out, "out"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    *out = nullptr;
+    if (!std::isfinite(p->beta) || !std::isfinite(p->lambda_tv) || p->lambda_tv < 0.f || p->fgp_iters < 0)
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "bad solver parameters");
+    ctr_solver* s = new (std::nothrow) ctr_solver();
+    if (!s) return set_error(CTR_ERR_OUT_OF_MEMORY, "host allocation");
+    s->g = GE(geom);
+    s->vdt = vdt;
+    s->p = *p;
+    const size_t bytes = s->g->nvox() * dtype_size(vdt);
+    cudaError_t e;
+    if ((e = cudaMalloc(&s->y, bytes)) != cudaSuccess || (e = cudaMalloc(&s->xprev, bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_obj, 4 * sizeof(double))) != cudaSuccess || (e = cudaMemset(s->y, 0, bytes)) != cudaSuccess ||
+        (e = cudaMemset(s->xprev, 0, bytes)) != cudaSuccess) {
+        ctr_status st = cuda_error(e, "solver allocation");
+        ctr_solver_destroy(s);
+        return st;
+    }
+    *out = s;
+    return CTR_OK;
+}
+
+static void drop_graph(ctr_solver* s)
+{
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->exec = nullptr;
+    s->graph = nullptr;
+}
+
+extern "C" ctr_status ctr_solver_destroy(ctr_solver* s)
+{
+    if (!s) return CTR_OK;
+    drop_graph(s);
+    cudaFree(s->y);
+    cudaFree(s->xprev);
+    cudaFree(s->d_obj);
+    delete s;
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_solver_set_sinogram(ctr_solver* s, const void* sino, ctr_dtype sdt)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need_dtype(sdt, "sino_dtype"));
+    if (s->sino != sino || s->sdt != sdt) drop_graph(s);
+    s->sino = sino;
+    s->sdt = sdt;
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    cudaStream_t st = S(stream);
+    const size_t bytes = s->g->nvox() * dtype_size(s->vdt);
+    if (vol) {
+        CTR_CUDA_TRY(cudaMemcpyAsync(s->y, vol, bytes, cudaMemcpyDefault, st));
+        CTR_CUDA_TRY(cudaMemcpyAsync(s->xprev, vol, bytes, cudaMemcpyDefault, st));
+    } else {
+        CTR_CUDA_TRY(cudaMemsetAsync(s->y, 0, bytes, st));
+        CTR_CUDA_TRY(cudaMemsetAsync(s->xprev, 0, bytes, st));
+    }
+    s->t = 1.0f;
+    s->k = 0;
+    return CTR_OK;
+}
+
+// One SART pass, captured once as a CUDA graph (2 launches per view) and replayed.
+static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st)
+{
+    const bool stoch = (s->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
+    if (!s->p.use_graph || stoch)   // the seed changes every pass: issue directly
+        return sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st);
+    if (!s->exec) {
+        CTR_TRY(ensure_rays(s->g, (size_t)s->g->npix()));
+        cudaStream_t cs;
+        CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        ctr_status r = CTR_OK;
+        if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
+        if (r == CTR_OK) r = sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, cs);
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(cs, &gr);
+        if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
+        if (r == CTR_OK) {
+            e = cudaGraphInstantiate(&s->exec, gr, 0);
+            if (e != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
+        }
+        s->graph = gr;
+        cudaStreamDestroy(cs);
+        if (r != CTR_OK) { drop_graph(s); return r; }
+    }
+    CTR_CUDA_TRY(cudaGraphLaunch(s->exec, st));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    if (!s->sino) return set_error(CTR_ERR_INVALID_ARGUMENT, "no sinogram set");
+    if (n < 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "n < 0");
+    cudaStream_t st = S(stream);
+    Geometry* g = s->g;
+    for (int it = 0; it < n; ++it) {
+        // V63/main_recon.cu:344-386 (FISTA == 1) / :316-341 (FISTA == 0)
+        CTR_TRY(solver_sart(s, (uint32_t)(s->k + 1), st));
+        const float lam = s->p.beta * s->p.lambda_tv;     // lambda_denoise_TV = 2*lambda_TV/Lip
+        const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // :372
+        const float gam = (s->t - 1.0f) / t_k;
+        if (s->p.fista) {
+            if (s->p.lambda_tv > 0.f && s->p.fgp_iters >= 0)
+                CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, s->y, s->xprev, gam, st));
+            else
+                CTR_TRY(launch_momentum(*g, s->y, s->xprev, s->y, s->vdt, gam, st));
+            s->t = t_k;
+        } else if (s->p.lambda_tv > 0.f) {
+            CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, nullptr, nullptr, 0.f, st));
+        }
+        s->k++;
+        if (s->p.objective) {
+            const void* xk = s->p.fista ? s->xprev : s->y;
+            CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st));
+            if (obj_out) {
+                double h[2];
+                CTR_CUDA_TRY(cudaMemcpyAsync(h, s->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+                CTR_CUDA_TRY(cudaStreamSynchronize(st));
+                obj_out[3 * it + 0] = h[1];
+                obj_out[3 * it + 1] = h[0];
+                obj_out[3 * it + 2] = h[0] + 2.0 * (double)s->p.lambda_tv * h[1];   // :423
+            }
+        } else if (obj_out) {
+            obj_out[3 * it + 0] = obj_out[3 * it + 1] = obj_out[3 * it + 2] = NAN;
+        }
+    }
+    return check_device_errors(g, st);
+}
+
+extern "C" ctr_status ctr_solver_get_volume(ctr_solver* s, void* dst, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    CTR_TRY(need(dst, "dst"));
+    const void* xk = (s->p.fista && s->k > 0) ? s->xprev : s->y;
+    CTR_CUDA_TRY(cudaMemcpyAsync(dst, xk, s->g->nvox() * dtype_size(s->vdt), cudaMemcpyDefault, S(stream)));
+    CTR_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k)
+{
+    if (!s || !k) return set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument");
+    *k = s->k;
+    return CTR_OK;
+}
+
+static uint64_t geom_hash(const ctr_geometry_desc& d)
+{
+    uint64_t h = 1469598103934665603ULL;
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&d);
+    for (size_t i = 0; i < sizeof(d); ++i) h = (h ^ b[i]) * 1099511628211ULL;
+    return h;
+}
+
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, dtype;
+    uint64_t geom;
+    int32_t k, fista;
+    float t, pad;
+    uint64_t nvox;
+};
+
+extern "C" ctr_status ctr_solver_save(ctr_solver* s, const char* path, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    CTR_TRY(need(path, "path"));
+    const size_t bytes = s->g->nvox() * dtype_size(s->vdt);
+    std::vector<char> buf(2 * bytes);
+    CTR_CUDA_TRY(cudaMemcpyAsync(buf.data(), s->y, bytes, cudaMemcpyDeviceToHost, S(stream)));
+    CTR_CUDA_TRY(cudaMemcpyAsync(buf.data() + bytes, s->xprev, bytes, cudaMemcpyDeviceToHost, S(stream)));
+    CTR_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+    CkptHeader h{};
+    memcpy(h.magic, "CTRCKPT1", 8);
+    h.version = 1; h.dtype = s->vdt; h.geom = geom_hash(s->g->desc); h.k = s->k; h.fista = s->p.fista;
+    h.t = s->t; h.nvox = s->g->nvox();
+    FILE* f = fopen(path, "wb");
+    if (!f) return set_error(CTR_ERR_IO, "cannot open %s for writing", path);
+    const bool ok = fwrite(&h, sizeof(h), 1, f) == 1 && fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+    const bool closed = fclose(f) == 0;
+    if (!ok || !closed) return set_error(CTR_ERR_IO, "short write to %s", path);
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_solver_load(ctr_solver* s, const char* path, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    CTR_TRY(need(path, "path"));
+    FILE* f = fopen(path, "rb");
+    if (!f) return set_error(CTR_ERR_IO, "cannot open %s", path);
+    CkptHeader h{};
+    const size_t bytes = s->g->nvox() * dtype_size(s->vdt);
+    std::vector<char> buf(2 * bytes);
+    const bool ok = fread(&h, sizeof(h), 1, f) == 1 && fread(buf.data(), 1, buf.size(), f) == buf.size();
+    fclose(f);
+    if (!ok || memcmp(h.magic, "CTRCKPT1", 8) != 0) return set_error(CTR_ERR_IO, "%s is not a solver checkpoint", path);
+    if (h.geom != geom_hash(s->g->desc) || h.dtype != (uint32_t)s->vdt || h.nvox != (uint64_t)s->g->nvox())
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "checkpoint %s was written for another geometry or dtype", path);
+    CTR_CUDA_TRY(cudaMemcpyAsync(s->y, buf.data(), bytes, cudaMemcpyHostToDevice, S(stream)));
+    CTR_CUDA_TRY(cudaMemcpyAsync(s->xprev, buf.data() + bytes, bytes, cudaMemcpyHostToDevice, S(stream)));
+    CTR_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+    s->k = h.k;
+    s->t = h.t;
+    return CTR_OK;
+}
+
+// -------------------------------------------- reference-compatible entry points
+
+namespace {
+std::mutex g_default_mu;
+Geometry* g_default = nullptr;
+
+// device copy of a host or device buffer
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+ctr_status in_dev(DevBuf& b, const void* src, size_t bytes)
+{
+    CTR_CUDA_TRY(cudaMalloc(&b.p, bytes));
+    if (src) CTR_CUDA_TRY(cudaMemcpy(b.p, src, bytes, cudaMemcpyDefault));
+    return CTR_OK;
+}
+}  // namespace
+
+extern "C" ctr_status ctr_set_default_geometry(const ctr_geometry_desc* desc)
+{
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    ctr_geometry* g = nullptr;
+    CTR_TRY(ctr_geometry_create(desc, &g));
+    if (g_default) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(g_default));
+    g_default = GE(g);
+    return CTR_OK;
+}
+
+static Geometry* default_geom()
+{
+    if (!g_default) set_error(CTR_ERR_INVALID_ARGUMENT, "ctr_set_default_geometry() has not been called");
+    return g_default;
+}
+
+extern "C" void Forward_3D_ray_driven_siddon(float* h_volume, float* h_proj_data)
+{
+    clear_error();
+    Geometry* g = default_geom();
+    if (!g || !h_volume || !h_proj_data) { if (g) set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument"); return; }
+    const size_t vb = g->nvox() * 4, pb = (size_t)g->npix() * g->desc.n_views * 4;
+    DevBuf v, p;
+    if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, nullptr, pb) != CTR_OK) return;
+    ctr_geometry* gg = reinterpret_cast<ctr_geometry*>(g);
+    if (ctr_forward(gg, v.p, CTR_F32, p.p, CTR_F32, 0, g->desc.n_views, nullptr) != CTR_OK) return;
+    cudaError_t e = cudaMemcpy(h_proj_data, p.p, pb, cudaMemcpyDefault);
+    if (e != cudaSuccess) cuda_error(e, "Forward_3D_ray_driven_siddon");
+}
+
+extern "C" void Reconstruction_3D_ray_driven_CBCT(float* h_volume, float* h_proj_data, float beta)
+{
+    clear_error();
+    Geometry* g = default_geom();
+    if (!g || !h_volume || !h_proj_data) { if (g) set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument"); return; }
+    const size_t vb = g->nvox() * 4, pb = (size_t)g->npix() * g->desc.n_views * 4;
+    DevBuf v, p;
+    if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, h_proj_data, pb) != CTR_OK) return;
+    if (ctr_sart_pass(reinterpret_cast<ctr_geometry*>(g), v.p, CTR_F32, p.p, CTR_F32, beta, 0, 0, nullptr) != CTR_OK) return;
+    cudaError_t e = cudaMemcpy(h_volume, v.p, vb, cudaMemcpyDefault);
+    if (e != cudaSuccess) { cuda_error(e, "Reconstruction_3D_ray_driven_CBCT"); return; }
+    check_device_errors(g, nullptr);
+}
+
+extern "C" void CheckMatchedJointOperator(float* h_volume)
+{
+    clear_error();
+    Geometry* g = default_geom();
+    if (!g || !h_volume) { if (g) set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument"); return; }
+    const size_t vb = g->nvox() * 4, pb = (size_t)g->npix() * 4;
+    DevBuf v, p, bp;
+    if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, nullptr, pb) != CTR_OK || in_dev(bp, nullptr, vb) != CTR_OK) return;
+    ctr_geometry* gg = reinterpret_cast<ctr_geometry*>(g);
+    // view 0: y = A x (command 0), z = A^T y with the reference's masked command-0 BP
+    if (ctr_forward(gg, v.p, CTR_F32, p.p, CTR_F32, 0, 1, nullptr) != CTR_OK) return;
+    if (cudaMemset(bp.p, 0, vb) != cudaSuccess) return;
+    if (ctr_backproject(gg, (const float*)p.p, 0, 1, bp.p, CTR_F32, CTR_BP_FOV_MASK, nullptr) != CTR_OK) return;
+    std::vector<float> hy(g->npix()), hz(g->nvox());
+    if (cudaMemcpy(hy.data(), p.p, pb, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hz.data(), bp.p, vb, cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    double ip1 = 0.0, ip2 = 0.0;   // V63/host_IterativeRecon_CBCT.c:186-197
+    for (size_t i = 0; i < hy.size(); ++i) ip1 += (double)hy[i] * (double)hy[i];
+    for (size_t i = 0; i < hz.size(); ++i) ip2 += (double)h_volume[i] * (double)hz[i];
+    printf("The 1st inner product = %f\n", ip1);
+    printf("The 2nd inner product = %f\n", ip2);
+}
+
+extern "C" void FGP_denoise_GPUx7_exact(float* h_f, float lambda, int niter)
+{
+    clear_error();
+    Geometry* g = default_geom();
+    if (!g || !h_f) { if (g) set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument"); return; }
+    const size_t vb = g->nvox() * 4;
+    DevBuf v;
+    if (in_dev(v, h_f, vb) != CTR_OK) return;
+    if (ctr_fgp_tv(reinterpret_cast<ctr_geometry*>(g), v.p, CTR_F32, lambda, niter, nullptr) != CTR_OK) return;
+    cudaError_t e = cudaMemcpy(h_f, v.p, vb, cudaMemcpyDefault);
+    if (e != cudaSuccess) cuda_error(e, "FGP_denoise_GPUx7_exact");
+}
+
+extern "C" void Reconstruction_FDK(float* h_volume, float* h_proj)
+{
+    clear_error();
+    Geometry* g = default_geom();
+    if (!g || !h_volume || !h_proj) { if (g) set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument"); return; }
+    const size_t vb = g->nvox() * 4, pb = (size_t)g->npix() * g->desc.n_views * 4;
+    DevBuf v, p;
+    if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, h_proj, pb) != CTR_OK) return;
+    if (ctr_fdk(reinterpret_cast<ctr_geometry*>(g), (const float*)p.p, (float*)v.p, nullptr) != CTR_OK) return;
+    cudaError_t e = cudaMemcpy(h_volume, v.p, vb, cudaMemcpyDefault);
+    if (e != cudaSuccess) cuda_error(e, "Reconstruction_FDK");
+}
+
+extern "C" double L2_norm_gpu(float* d_a, float* d_b)
+{
+    clear_error();
+    Geometry* g = default_geom();
+    if (!g || !d_a || !d_b) { if (g) set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument"); return NAN; }
+    const size_t n = (size_t)g->npix() * g->desc.n_views;
+    DevBuf a, b;
+    if (in_dev(a, d_a, n * 4) != CTR_OK || in_dev(b, d_b, n * 4) != CTR_OK) return NAN;
+    double r = NAN;
+    if (ctr_l2_norm((const float*)a.p, (const float*)b.p, (int64_t)n, &r, nullptr) != CTR_OK) return NAN;
+    return r;
+}
+
+extern "C" double TV_norm_gpu(float* d_volume)
+{
+    clear_error();
+    Geometry* g = default_geom();
+    if (!g || !d_volume) { if (g) set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument"); return NAN; }
+    DevBuf v;
+    if (in_dev(v, d_volume, g->nvox() * 4) != CTR_OK) return NAN;
+    double r = NAN;
+    if (ctr_tv_norm(reinterpret_cast<ctr_geometry*>(g), v.p, CTR_F32, &r, nullptr) != CTR_OK) return NAN;
+    return r;
+}

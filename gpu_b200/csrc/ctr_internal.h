@@ -1,0 +1,137 @@
+// ctr_internal.h -- types shared by the host library and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/ctrecon.h"
+
+namespace ctr {
+
+// Geometry as the kernels see it (passed by value, lives in the constant bank).
+// Every float is derived on the host with the reference's float/double steps
+// (V63/main_recon.cu:60-111).
+struct DevGeom {
+    int M, N, Z;            // volume
+    int R, ZP;              // detector columns, rows
+    int nviews;
+    int max_steps;          // Siddon step bound nx+ny+nz+3
+    int entry64;            // FP64 ray-box entry/exit
+    float vx, vy, vz, inv_vx, inv_vy, inv_vz;
+    float bx, by, bz;       // boundary_voxel_*
+    float ymin, zmin;       // Detector_Ymin/Zmin
+    float du, dv, inv_du, inv_dv;
+    float dso, dod;
+    float srcx, srcy, srcz;
+    float thr_fp;           // volumn_z*1e-6f: FP zero-length threshold
+    float thr_bp;           // volumn_x*1e-6f: BP pair and sum thresholds
+    float fov_h_x, fov_h_y; // float(M)*0.5f-0.5f, float(N)*0.5f-0.5f
+    float fov_r2;           // (hx*vx)*hy*vy
+    float m_off;            // (float)M_Offset
+    float fdk_ang;          // us_rate*PI/180.0f        (V63/FDK/kernel_FDK.cu:117)
+    float fdk_usn;          // us_rate*Nviews in float  (same line)
+    const float* px;        // plane coordinates vx*n+bx for n = -1..M+1 at px[n+1]
+    const float* py;
+    const float* pz;
+    const float2* trig;     // [view] (sin, cos) of the FP/SART frame angle
+    const float2* trig_fdk; // [view] (sin, cos) of the FDK frame angle
+    const float4* colt;     // [view][u] (x1x, 1/dx, x1y, 1/dy), parallel axes encoded
+    const float2* rowt;     // [v] (x1z, 1/dz), parallel rows encoded
+    unsigned int* err;      // device error bits (ERR_*)
+};
+
+enum : unsigned { ERR_TRAVERSAL = 1u };
+
+struct Geometry {
+    ctr_geometry_desc desc{};
+    DevGeom dg{};
+    int device = 0;
+    std::vector<float> h_px, h_py, h_pz;
+    std::vector<float2> h_trig, h_trig_fdk;
+    // device allocations
+    void* d_tables = nullptr;  // px,py,pz,trig,trig_fdk,rowt
+    float4* d_colt = nullptr;
+    unsigned* d_err = nullptr;
+    // workspace
+    float2* d_rays = nullptr;  size_t rays_cap = 0;     // ray records (value, chord length)
+    double* d_partial = nullptr; size_t partial_cap = 0;
+    double* d_result = nullptr;                        // 8 doubles
+    void* d_fgp = nullptr; size_t fgp_bytes = 0;       // 9 dual arrays
+    float* d_fdk = nullptr; size_t fdk_cap = 0;
+    float* d_ramp = nullptr;                           // 2R-1 taps
+    long long nvox() const { return (long long)desc.nx * desc.ny * desc.nz; }
+    long long npix() const { return (long long)desc.nu * desc.nv; }
+};
+
+// error reporting (thread-local message)
+ctr_status set_error(ctr_status st, const char* fmt, ...);
+ctr_status cuda_error(cudaError_t e, const char* what);
+void clear_error();
+
+#define CTR_CUDA_TRY(call)                                         \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return ::ctr::cuda_error(e_, #call); \
+    } while (0)
+#define CTR_TRY(call)                          \
+    do {                                       \
+        ctr_status s_ = (call);                \
+        if (s_ != CTR_OK) return s_;           \
+    } while (0)
+
+inline size_t dtype_size(ctr_dtype t) { return t == CTR_F32 ? 4 : 2; }
+inline bool dtype_ok(int t) { return t == CTR_F32 || t == CTR_BF16 || t == CTR_F16; }
+
+// workspace helpers (geometry.cpp)
+ctr_status ensure_rays(Geometry* g, size_t n);
+ctr_status ensure_partial(Geometry* g, size_t n);
+ctr_status ensure_fgp(Geometry* g, size_t bytes);
+ctr_status check_device_errors(Geometry* g, cudaStream_t st);
+
+// ---- kernel launchers (implemented in the .cu files) ----
+enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3 };
+struct FpArgs {
+    const void* vol; ctr_dtype vol_dtype;
+    int view0, nview;
+    FpKind kind;
+    void* out; ctr_dtype out_dtype;       // FORWARD: sino; SART: float2 rays
+    const void* b; ctr_dtype b_dtype;     // SART/OBJECTIVE: measured sinogram (already offset to view0)
+    double* partial;                      // OBJECTIVE: one double per block
+    int* nseg; uint64_t* hash; float* len;  // TRACE
+};
+ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, size_t* nblocks_out);
+
+struct BpArgs {
+    void* vol; ctr_dtype vol_dtype;
+    const float2* rays;                   // [nview][ZP][R] (value, chord length)
+    int view0, nview;
+    int sart;                             // 1: SART update; 0: adjoint
+    unsigned flags;                       // CTR_BP_* / CTR_SART_*
+    float beta;
+    uint32_t seed;
+};
+ctr_status launch_backproject(const Geometry& g, const BpArgs& a, cudaStream_t st);
+ctr_status launch_ray_prep(const Geometry& g, const float* y, int view0, int nview, float2* rays,
+                           cudaStream_t st);
+
+ctr_status launch_reduce(const double* partial, size_t n, double* out, cudaStream_t st);
+ctr_status launch_dot(const float* a, const float* b, long long n, double* partial, size_t cap,
+                      double* out, cudaStream_t st);
+ctr_status launch_l2(const float* a, const float* b, long long n, double* partial, size_t cap,
+                     double* out, cudaStream_t st);
+ctr_status launch_tv(const Geometry& g, const void* vol, ctr_dtype dt, double* partial, size_t cap,
+                     double* out, cudaStream_t st);
+ctr_status launch_fgp(Geometry& g, void* vol, ctr_dtype dt, float lambda, int iters,
+                      void* fista_y, void* fista_xprev, float fista_gamma, cudaStream_t st);
+ctr_status launch_momentum(const Geometry& g, void* y, void* xprev, const void* x, ctr_dtype dt,
+                           float gam, cudaStream_t st);
+ctr_status launch_convert(const void* src, ctr_dtype sdt, void* dst, ctr_dtype ddt, long long n,
+                          cudaStream_t st);
+ctr_status launch_fdk(Geometry& g, const float* sino, float* vol, cudaStream_t st);
+ctr_status launch_phantom(const Geometry& g, const double* dparams, int n, float* vol,
+                          cudaStream_t st);
+
+}  // namespace ctr

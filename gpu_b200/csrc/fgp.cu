@@ -1,0 +1,299 @@
+// fgp.cu -- FGP total-variation prox, FISTA momentum, objective reductions.
+//
+// FGP restates FGP_denoise_GPUx7_exact (V63/host_FGP_Denoise_GPUx7.c:1-111)
+// and its kernels FGP_operator_L_Pc / FGP_operator_LT_Pp
+// (V63/kernel_FGP_Denoise_GPUx7.cu:2-88) with the same float operations, but
+// one kernel per inner iteration instead of two: each thread walks a z run of
+// one (x, y) column, evaluates L = f - lambda*div(r,s,t) at its voxel and at the
+// +x, +y, +z neighbours on the fly, and writes the projected, extrapolated
+// duals.  The extrapolated duals r,s,t are double-buffered (read A, write B),
+// so no thread reads a dual another thread has already advanced.  Per inner
+// iteration the kernel streams f and 6 duals in and 6 duals out: 13 volumes,
+// where the two-kernel form moves 18.
+//
+// Dual layout: volume-sized arrays; r[p] belongs to the edge (x, x+1) and is 0
+// at x = nx-1 (the reference's zero-padded d_r[x+1], V63/host_FGP_Denoise_
+// GPUx7.c:8-38); likewise s along y and t along z.
+#include "ctr_device.cuh"
+
+namespace ctr {
+
+static constexpr int FG_BX = 32, FG_BY = 8, FG_ZRUN = 32;
+
+template <typename T>
+__device__ __forceinline__ float fgp_L(const T* __restrict__ f, const T* __restrict__ r, const T* __restrict__ s,
+                                       const T* __restrict__ t, int x, int y, int z, long long p, int M, long long MN,
+                                       float lambda)
+{
+    const float rv = Store<T>::ld(r + p), rm = x > 0 ? Store<T>::ld(r + p - 1) : 0.0f;
+    const float sv = Store<T>::ld(s + p), sm = y > 0 ? Store<T>::ld(s + p - M) : 0.0f;
+    const float tv = Store<T>::ld(t + p), tm = z > 0 ? Store<T>::ld(t + p - MN) : 0.0f;
+    const float tl = fa(fa(fs(rv, rm), fs(sv, sm)), fs(tv, tm));       // L_Pc :14
+    return fs(Store<T>::ld(f + p), fm(lambda, tl));                    // :17
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FG_BX * FG_BY)
+k_fgp_step(int M, int N, int Z, const T* __restrict__ f, const T* __restrict__ rA, const T* __restrict__ sA,
+           const T* __restrict__ tA, T* __restrict__ rB, T* __restrict__ sB, T* __restrict__ tB, T* __restrict__ o,
+           T* __restrict__ pd, T* __restrict__ q, float lambda, float alpha12, float gam)
+{
+    const int x = blockIdx.x * FG_BX + threadIdx.x;
+    const int y = blockIdx.y * FG_BY + threadIdx.y;
+    const int z0 = blockIdx.z * FG_ZRUN;
+    if (x >= M || y >= N) return;
+    const long long MN = (long long)M * N;
+    const int z1 = min(z0 + FG_ZRUN, Z);
+    long long p = (long long)z0 * MN + (long long)y * M + x;
+    float Lc = fgp_L(f, rA, sA, tA, x, y, z0, p, M, MN, lambda);
+    for (int z = z0; z < z1; ++z, p += MN) {
+        const float Lz = (z < Z - 1) ? fgp_L(f, rA, sA, tA, x, y, z + 1, p + MN, M, MN, lambda) : 0.0f;
+        const float Lx = (x < M - 1) ? fgp_L(f, rA, sA, tA, x + 1, y, z, p + 1, M, MN, lambda) : 0.0f;
+        const float Ly = (y < N - 1) ? fgp_L(f, rA, sA, tA, x, y + 1, z, p + M, M, MN, lambda) : 0.0f;
+        // LT_Pp (V63/kernel_FGP_Denoise_GPUx7.cu:52-86)
+        float tr = Store<T>::ld(rA + p), ts = Store<T>::ld(sA + p), tt = Store<T>::ld(tA + p);
+        if (x < M - 1) tr = fa(tr, fm(alpha12, fs(Lc, Lx)));
+        if (y < N - 1) ts = fa(ts, fm(alpha12, fs(Lc, Ly)));
+        if (z < Z - 1) tt = fa(tt, fm(alpha12, fs(Lc, Lz)));
+        const float rst = __fsqrt_rn(fa(fa(fm(tr, tr), fm(ts, ts)), fm(tt, tt)));
+        const float den = fmaxf(1.0f, rst);
+        if (x < M - 1) {
+            const float on = fdv(tr, den);
+            Store<T>::st(rB + p, fa(on, fm(gam, fs(on, Store<T>::ldw(o + p)))));
+            Store<T>::st(o + p, on);
+        }
+        if (y < N - 1) {
+            const float pn = fdv(ts, den);
+            Store<T>::st(sB + p, fa(pn, fm(gam, fs(pn, Store<T>::ldw(pd + p)))));
+            Store<T>::st(pd + p, pn);
+        }
+        if (z < Z - 1) {
+            const float qn = fdv(tt, den);
+            Store<T>::st(tB + p, fa(qn, fm(gam, fs(qn, Store<T>::ldw(q + p)))));
+            Store<T>::st(q + p, qn);
+        }
+        Lc = Lz;
+    }
+}
+
+// x* = f - lambda*div(o,p,q) (the final L_Pc, V63/host_FGP_Denoise_GPUx7.c:83);
+// with FISTA fused: y = x* + gam*(x* - xprev), xprev = x* (V63/main_recon.cu:375-382).
+template <typename T, bool FISTA>
+__global__ void __launch_bounds__(256)
+k_fgp_final(int M, int N, int Z, T* __restrict__ vol, const T* __restrict__ o, const T* __restrict__ pd,
+            const T* __restrict__ q, float lambda, T* __restrict__ xprev, float gam)
+{
+    const long long MN = (long long)M * N;
+    const long long n = MN * Z;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % M);
+        const int y = (int)((p / M) % N);
+        const int z = (int)(p / MN);
+        const float xs = fgp_L<T>(vol, o, pd, q, x, y, z, p, M, MN, lambda);
+        if (FISTA) {
+            const float xp = Store<T>::ldw(xprev + p);
+            // the stored x_k is what the momentum step sees
+            T xs_t;
+            Store<T>::st(&xs_t, xs);
+            const float xk = Store<T>::ldw(&xs_t);
+            Store<T>::st(vol + p, fa(xk, fm(gam, fs(xk, xp))));
+            xprev[p] = xs_t;
+        } else {
+            Store<T>::st(vol + p, xs);
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_momentum(long long n, T* __restrict__ y, T* __restrict__ xprev, const T* __restrict__ x, float gam)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const float xv = Store<T>::ldw(x + p);
+        const float xp = Store<T>::ldw(xprev + p);
+        Store<T>::st(y + p, fa(xv, fm(gam, fs(xv, xp))));        // main_recon.cu:378
+        Store<T>::st(xprev + p, xv);                              // :380
+    }
+}
+
+static int grid_for(long long n, int threads)
+{
+    long long b = (n + threads - 1) / threads;
+    if (b > 148LL * 64) b = 148LL * 64;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// t_k = (1 + sqrt(1 + 4 t^2))/2 in float (V63/host_FGP_Denoise_GPUx7.c:161)
+static float next_t(float t) { return (1.0f + sqrtf(1.0f + 4.0f * t * t)) / 2.0f; }
+
+ctr_status launch_fgp(Geometry& G, void* vol, ctr_dtype dt, float lambda, int iters, void* fista_y,
+                      void* fista_xprev, float fista_gamma, cudaStream_t st)
+{
+    const int M = G.desc.nx, N = G.desc.ny, Z = G.desc.nz;
+    const long long V = G.nvox();
+    const size_t es = dtype_size(dt);
+    CTR_TRY(ensure_fgp(&G, 9 * (size_t)V * es));
+    CTR_CUDA_TRY(cudaMemsetAsync(G.d_fgp, 0, 9 * (size_t)V * es, st));
+    const float alpha12 = 1.0f / (lambda * 12.0f);                 // :166
+    dim3 blk(FG_BX, FG_BY), grd((M + FG_BX - 1) / FG_BX, (N + FG_BY - 1) / FG_BY, (Z + FG_ZRUN - 1) / FG_ZRUN);
+    CTR_DISPATCH_DTYPE(dt, T, {
+        T* base = (T*)G.d_fgp;
+        T* A[3] = {base, base + V, base + 2 * V};
+        T* B[3] = {base + 3 * V, base + 4 * V, base + 5 * V};
+        T* O[3] = {base + 6 * V, base + 7 * V, base + 8 * V};
+        float t_k_1 = 1.0f;
+        for (int it = 0; it < iters; ++it) {
+            const float t_k = next_t(t_k_1);
+            const float gam = (t_k_1 - 1.0f) / t_k;
+            k_fgp_step<T><<<grd, blk, 0, st>>>(M, N, Z, (const T*)vol, A[0], A[1], A[2], B[0], B[1], B[2], O[0], O[1],
+                                               O[2], lambda, alpha12, gam);
+            for (int a = 0; a < 3; ++a) { T* tmp = A[a]; A[a] = B[a]; B[a] = tmp; }
+            t_k_1 = t_k;
+        }
+        if (fista_y) {
+            if (fista_y != vol) return set_error(CTR_ERR_INVALID_ARGUMENT, "fused FISTA output must alias the volume");
+            k_fgp_final<T, true><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, O[0], O[1], O[2], lambda,
+                                                                    (T*)fista_xprev, fista_gamma);
+        } else {
+            k_fgp_final<T, false><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, O[0], O[1], O[2], lambda,
+                                                                     nullptr, 0.0f);
+        }
+    });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+ctr_status launch_momentum(const Geometry& G, void* y, void* xprev, const void* x, ctr_dtype dt, float gam,
+                           cudaStream_t st)
+{
+    const long long V = G.nvox();
+    CTR_DISPATCH_DTYPE(dt, T, { k_momentum<T><<<grid_for(V, 256), 256, 0, st>>>(V, (T*)y, (T*)xprev, (const T*)x, gam); });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+// ---------------------------------------------------------------- reductions
+
+// Sum of part[0..n) in a fixed order: block b sums the contiguous segment
+// [b*seg, (b+1)*seg) into out[b].  Repeated runs give identical bits.
+__global__ void __launch_bounds__(1024) k_reduce(const double* __restrict__ part, long long n, long long seg,
+                                                 double* __restrict__ out)
+{
+    __shared__ double sh[32];
+    const long long lo = blockIdx.x * seg, hi = min(n, lo + seg);
+    double v = 0.0;
+    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) v += part[i];
+    const double t = block_sum(v, sh);
+    if (threadIdx.x == 0) out[blockIdx.x] = t;
+}
+
+// Needs 1024 doubles of scratch after part[n].
+ctr_status launch_reduce(const double* partial, size_t n, double* out, cudaStream_t st)
+{
+    if (n > 16384) {
+        double* mid = const_cast<double*>(partial) + n;
+        const long long seg = ((long long)n + 1023) / 1024;
+        k_reduce<<<1024, 1024, 0, st>>>(partial, (long long)n, seg, mid);
+        k_reduce<<<1, 1024, 0, st>>>(mid, 1024, 1024, out);
+    } else {
+        k_reduce<<<1, 1024, 0, st>>>(partial, (long long)n, (long long)n, out);
+    }
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+template <int OP>   // 0: a*b, 1: (a-b)^2 in float
+__global__ void __launch_bounds__(256)
+k_pairsum(const float* __restrict__ a, const float* __restrict__ b, long long n, double* __restrict__ part)
+{
+    __shared__ double sh[8];
+    double v = 0.0;
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+        if (OP == 0) v += (double)a[i] * (double)b[i];
+        else {
+            const float e = fs(a[i], b[i]);
+            v += (double)fm(e, e);
+        }
+    }
+    const double t = block_sum(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+ctr_status launch_dot(const float* a, const float* b, long long n, double* partial, size_t cap, double* out,
+                      cudaStream_t st)
+{
+    int nb = grid_for(n, 256);
+    if ((size_t)nb > cap) nb = (int)cap;
+    k_pairsum<0><<<nb, 256, 0, st>>>(a, b, n, partial);
+    CTR_CUDA_TRY(cudaGetLastError());
+    return launch_reduce(partial, nb, out, st);
+}
+
+ctr_status launch_l2(const float* a, const float* b, long long n, double* partial, size_t cap, double* out,
+                     cudaStream_t st)
+{
+    int nb = grid_for(n, 256);
+    if ((size_t)nb > cap) nb = (int)cap;
+    k_pairsum<1><<<nb, 256, 0, st>>>(a, b, n, partial);
+    CTR_CUDA_TRY(cudaGetLastError());
+    return launch_reduce(partial, nb, out, st);
+}
+
+// TV_norm_kernel (V63/kernel_tool_functions.cu:39-65) with an FP64 block sum.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_tv(int M, int N, int Z, const T* __restrict__ d, double* __restrict__ part)
+{
+    __shared__ double sh[8];
+    const long long MN = (long long)M * N, n = MN * Z;
+    double acc = 0.0;
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+        const int x = (int)(i % M), y = (int)((i / M) % N), z = (int)(i / MN);
+        const float c = Store<T>::ld(d + i);
+        const float dj = x < M - 1 ? fs(c, Store<T>::ld(d + i + 1)) : 0.f;
+        const float dk = y < N - 1 ? fs(c, Store<T>::ld(d + i + M)) : 0.f;
+        const float dl = z < Z - 1 ? fs(c, Store<T>::ld(d + i + MN)) : 0.f;
+        float tv = 0.0f;
+        const bool bx = x < M - 1, by = y < N - 1, bz = z < Z - 1;
+        if (bx && by && bz) tv = __fsqrt_rn(fa(fa(fm(dj, dj), fm(dk, dk)), fm(dl, dl)));
+        else if (!bx && by && bz) tv = __fsqrt_rn(fa(fm(dk, dk), fm(dl, dl)));
+        else if (bx && !by && bz) tv = __fsqrt_rn(fa(fm(dj, dj), fm(dl, dl)));
+        else if (bx && by && !bz) tv = __fsqrt_rn(fa(fm(dj, dj), fm(dk, dk)));
+        else if (!bx && !by && bz) tv = fabsf(dl);
+        else if (!bx && by && !bz) tv = fabsf(dk);
+        else if (bx && !by && !bz) tv = fabsf(dj);
+        acc += (double)tv;
+    }
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+ctr_status launch_tv(const Geometry& G, const void* vol, ctr_dtype dt, double* partial, size_t cap, double* out,
+                     cudaStream_t st)
+{
+    const long long V = G.nvox();
+    int nb = grid_for(V, 256);
+    if ((size_t)nb > cap) nb = (int)cap;
+    CTR_DISPATCH_DTYPE(dt, T, { k_tv<T><<<nb, 256, 0, st>>>(G.desc.nx, G.desc.ny, G.desc.nz, (const T*)vol, partial); });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return launch_reduce(partial, nb, out, st);
+}
+
+template <typename S, typename D>
+__global__ void k_convert(const S* __restrict__ s, D* __restrict__ d, long long n)
+{
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+        Store<D>::st(d + i, Store<S>::ld(s + i));
+}
+
+ctr_status launch_convert(const void* src, ctr_dtype sdt, void* dst, ctr_dtype ddt, long long n, cudaStream_t st)
+{
+    const int nb = grid_for(n, 256);
+    CTR_DISPATCH_DTYPE(sdt, S, {
+        CTR_DISPATCH_DTYPE(ddt, D, { k_convert<S, D><<<nb, 256, 0, st>>>((const S*)src, (D*)dst, n); });
+    });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+}  // namespace ctr

@@ -1,0 +1,314 @@
+// fp.cu -- Siddon ray-driven forward projector for sm_100a.
+//
+// One ray per thread.  The traversal restates forward_ray_driven_3d_kernel_
+// correction (V63/kernel_IterativeRecon_universal.cu:7-567) with IEEE float
+// operations in the reference's order, so the voxel index sequence of every
+// ray and its float ray sum are bit-identical to the reference compiled for
+// the CPU.  Differences from the reference kernel are in organisation only:
+//   * the seven tie branches become "advance every axis whose next-plane
+//     alpha equals the minimum" (the same rule for non-NaN alphas), executed
+//     branch-free, which keeps the 32 lanes of a warp converged;
+//   * the plane coordinates volumn*n+boundary come from shared-memory tables;
+//   * the loop is bounded by nx+ny+nz+3 steps and reports ERR_TRAVERSAL;
+//   * the epilogue also writes the chord length of every ray (for the gather
+//     backprojector), or reduces the squared residual in FP64 (objective).
+#include "ctr_device.cuh"
+
+namespace ctr {
+
+static constexpr int FP_BX = 32;   // rays along a detector row per block
+static constexpr int FP_BY = 4;    // detector rows per block
+static constexpr int FP_THREADS = FP_BX * FP_BY;
+static constexpr uint64_t kFnvOffset = 1469598103934665603ULL;
+static constexpr uint64_t kFnvPrime = 1099511628211ULL;
+
+struct RayResult {
+    float sum, len, d12;
+    int nseg;
+    uint64_t hash;
+};
+
+// Floor of the position along an axis at parameter a, as a plane index
+// (the reference's floor((a*(x2-x1) + x1 - b)*inv_v)).
+__device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, float inv_v)
+{
+    return floorf(fm(fs(fa(fm(a, d), x1), b), inv_v));
+}
+
+template <typename VT, bool E64, bool TRACE>
+__device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
+                                            const float* __restrict__ PY, const float* __restrict__ PZ,
+                                            const VT* __restrict__ vol, float s, float c, int u, int v)
+{
+    const int M = g.M, N = g.N, Z = g.Z;
+    RayResult r;
+    r.sum = 0.f; r.len = 0.f; r.nseg = 0; r.hash = kFnvOffset;
+
+    // source X2 and detector pixel centre X1 (universal.cu:24-45)
+    const float x2x = fs(fm(g.srcx, c), fm(g.srcy, s));
+    const float x2y = fa(fm(g.srcx, s), fm(g.srcy, c));
+    const float x2z = g.srcz;
+    const float pu = fa(g.ymin, fm((float)u, g.du));
+    const float x1x = fs(fm(g.dod, c), fm(pu, s));
+    const float x1y = fa(fm(g.dod, s), fm(pu, c));
+    const float x1z = fa(g.zmin, fm((float)v, g.dv));
+    const float dx = fs(x2x, x1x), dy = fs(x2y, x1y), dz = fs(x2z, x1z);
+    const float ix = fdv(1.0f, dx), iy = fdv(1.0f, dy), iz = fdv(1.0f, dz);
+    r.d12 = __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));   // :290
+
+    // alpha_min / alpha_max (:77-104); PX[n+1] is plane n
+    float a0, a1;
+    a0 = fm(fs(PX[1], x1x), ix); a1 = fm(fs(PX[M + 1], x1x), ix);
+    const float axmin = fminf(a0, a1), axmax = fmaxf(a0, a1);
+    a0 = fm(fs(PY[1], x1y), iy); a1 = fm(fs(PY[N + 1], x1y), iy);
+    const float aymin = fminf(a0, a1), aymax = fmaxf(a0, a1);
+    a0 = fm(fs(PZ[1], x1z), iz); a1 = fm(fs(PZ[Z + 1], x1z), iz);
+    const float azmin = fminf(a0, a1), azmax = fmaxf(a0, a1);
+    float amin = fmaxf(fmaxf(axmin, aymin), fmaxf(aymin, azmin));
+    float amax = fminf(fminf(axmax, aymax), fminf(aymax, azmax));
+
+    int i_min, i_max, j_min, j_max, k_min, k_max;
+    bool hit;
+    const bool zpar = fabsf(fs(x1z, x2z)) < fm(g.vz, 1e-6f);
+    if (!E64) {
+        hit = !(amax <= amin);
+        if (!hit) return r;
+        // first/last plane index per axis (:113-209)
+        if (x1x < x2x) {
+            i_min = (amin == axmin) ? 1 : __float2int_rz(fa(pos_floor(amin, dx, x1x, g.bx, g.inv_vx), 1.0f));
+            i_max = (amax == axmax) ? M : __float2int_rz(pos_floor(amax, dx, x1x, g.bx, g.inv_vx));
+        } else {
+            i_max = (amin == axmin) ? M - 1 : __float2int_rz(pos_floor(amin, dx, x1x, g.bx, g.inv_vx));
+            i_min = (amax == axmax) ? 0 : __float2int_rz(fa(pos_floor(amax, dx, x1x, g.bx, g.inv_vx), 1.0f));
+        }
+        if (x1y < x2y) {
+            j_min = (amin == aymin) ? 1 : __float2int_rz(fa(pos_floor(amin, dy, x1y, g.by, g.inv_vy), 1.0f));
+            j_max = (amax == aymax) ? N : __float2int_rz(pos_floor(amax, dy, x1y, g.by, g.inv_vy));
+        } else {
+            j_max = (amin == aymin) ? N - 1 : __float2int_rz(pos_floor(amin, dy, x1y, g.by, g.inv_vy));
+            j_min = (amax == aymax) ? 0 : __float2int_rz(fa(pos_floor(amax, dy, x1y, g.by, g.inv_vy), 1.0f));
+        }
+        if (zpar) {
+            const float fz = floorf(fm(fs(x1z, g.bz), g.inv_vz));
+            k_min = __float2int_rz(fa(fz, 1.0f));
+            k_max = __float2int_rz(fz);
+        } else if (x1z < x2z) {
+            k_min = (amin == azmin) ? 1 : __float2int_rz(fa(pos_floor(amin, dz, x1z, g.bz, g.inv_vz), 1.0f));
+            k_max = (amax == azmax) ? Z : __float2int_rz(pos_floor(amax, dz, x1z, g.bz, g.inv_vz));
+        } else {
+            k_max = (amin == azmin) ? Z - 1 : __float2int_rz(pos_floor(amin, dz, x1z, g.bz, g.inv_vz));
+            k_min = (amax == azmax) ? 0 : __float2int_rz(fa(pos_floor(amax, dz, x1z, g.bz, g.inv_vz), 1.0f));
+        }
+    } else {
+        // FP64 ray-box entry/exit on the float positions; traversal stays float.
+        const double X1x = x1x, X1y = x1y, X1z = x1z;
+        const double Dx = (double)x2x - X1x, Dy = (double)x2y - X1y, Dz = (double)x2z - X1z;
+        const double Ix = 1.0 / Dx, Iy = 1.0 / Dy, Iz = 1.0 / Dz;
+        const double IVx = 1.0 / (double)g.vx, IVy = 1.0 / (double)g.vy, IVz = 1.0 / (double)g.vz;
+        double b0, b1;
+        b0 = ((double)PX[1] - X1x) * Ix; b1 = ((double)PX[M + 1] - X1x) * Ix;
+        const double Axmin = fmin(b0, b1), Axmax = fmax(b0, b1);
+        b0 = ((double)PY[1] - X1y) * Iy; b1 = ((double)PY[N + 1] - X1y) * Iy;
+        const double Aymin = fmin(b0, b1), Aymax = fmax(b0, b1);
+        b0 = ((double)PZ[1] - X1z) * Iz; b1 = ((double)PZ[Z + 1] - X1z) * Iz;
+        const double Azmin = fmin(b0, b1), Azmax = fmax(b0, b1);
+        const double Amin = fmax(fmax(Axmin, Aymin), Azmin);
+        const double Amax = fmin(fmin(Axmax, Aymax), Azmax);
+        hit = !(Amax <= Amin);
+        if (!hit) return r;
+        const double Bx = g.bx, By = g.by, Bz = g.bz;
+        if (x1x < x2x) {
+            i_min = (Amin == Axmin) ? 1 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amin, Dx), X1x), Bx), IVx)) + 1;
+            i_max = (Amax == Axmax) ? M : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amax, Dx), X1x), Bx), IVx));
+        } else {
+            i_max = (Amin == Axmin) ? M - 1 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amin, Dx), X1x), Bx), IVx));
+            i_min = (Amax == Axmax) ? 0 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amax, Dx), X1x), Bx), IVx)) + 1;
+        }
+        if (x1y < x2y) {
+            j_min = (Amin == Aymin) ? 1 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amin, Dy), X1y), By), IVy)) + 1;
+            j_max = (Amax == Aymax) ? N : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amax, Dy), X1y), By), IVy));
+        } else {
+            j_max = (Amin == Aymin) ? N - 1 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amin, Dy), X1y), By), IVy));
+            j_min = (Amax == Aymax) ? 0 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amax, Dy), X1y), By), IVy)) + 1;
+        }
+        if (zpar) {
+            k_min = (int)floor(__dmul_rn(__dsub_rn(X1z, Bz), IVz)) + 1;
+            k_max = (int)floor(__dmul_rn(__dsub_rn(X1z, Bz), IVz));
+        } else if (x1z < x2z) {
+            k_min = (Amin == Azmin) ? 1 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amin, Dz), X1z), Bz), IVz)) + 1;
+            k_max = (Amax == Azmax) ? Z : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amax, Dz), X1z), Bz), IVz));
+        } else {
+            k_max = (Amin == Azmin) ? Z - 1 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amin, Dz), X1z), Bz), IVz));
+            k_min = (Amax == Azmax) ? 0 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amax, Dz), X1z), Bz), IVz)) + 1;
+        }
+        amin = (float)Amin;
+        amax = (float)Amax;
+    }
+
+    // initial next-plane alphas (:218-266) and voxel indices (:271-284)
+    const float INF = __int_as_float(0x7f800000);
+    float ax, ay, az;
+    if (fabsf(fs(x1x, x2x)) < fm(g.vx, 1e-6f)) ax = INF;
+    else ax = fm(fs(fa(fm(g.vx, (float)(x1x < x2x ? i_min : i_max)), g.bx), x1x), ix);
+    if (fabsf(fs(x1y, x2y)) < fm(g.vy, 1e-6f)) ay = INF;
+    else ay = fm(fs(fa(fm(g.vy, (float)(x1y < x2y ? j_min : j_max)), g.by), x1y), iy);
+    if (zpar) az = INF;
+    else az = fm(fs(fa(fm(g.vz, (float)(x1z < x2z ? k_min : k_max)), g.bz), x1z), iz);
+    int vi = (x1x < x2x) ? i_min - 1 : i_max;
+    int vj = (x1y < x2y) ? j_min - 1 : j_max;
+    int vk = (x1z < x2z) ? k_min - 1 : k_max;
+    const int sx = (x1x < x2x) ? 1 : ((x1x > x2x) ? -1 : 0);
+    const int sy = (x1y < x2y) ? 1 : ((x1y > x2y) ? -1 : 0);
+    const int sz = (x1z < x2z) ? 1 : ((x1z > x2z) ? -1 : 0);
+    // PXo[vi] = plane index vi+1 (increasing) or vi (decreasing): the
+    // reference's next_alpha_index after the move.
+    const float* PXo = PX + 1 + (sx > 0);
+    const float* PYo = PY + 1 + (sy > 0);
+    const float* PZo = PZ + 1 + (sz > 0);
+    const int MN = M * N;
+    const int syM = sy * M, szMN = sz * MN;
+    int idx = vk * MN + vj * M + vi;
+    const float d12 = r.d12;
+    float ac = amin, sum = 0.f, len = 0.f;
+    int steps = 0;
+    // :297-551
+    while (fs(amax, ac) > 1e-16f) {
+        if ((unsigned)vi >= (unsigned)M || (unsigned)vj >= (unsigned)N || (unsigned)vk >= (unsigned)Z) break;
+        if (++steps > g.max_steps) {
+            atomicOr(g.err, ERR_TRAVERSAL);
+            break;
+        }
+        const float m = fminf(fminf(ax, ay), az);
+        const float seg = fm(d12, fs(m, ac));
+        const float f = Store<VT>::ld(vol + idx);
+        len = fa(len, seg);
+        sum = fa(sum, fm(seg, f));
+        if (TRACE) {
+            r.nseg++;
+            r.hash = (r.hash ^ (uint64_t)(uint32_t)idx) * kFnvPrime;
+        }
+        ac = m;
+        if (ax == m) { vi += sx; idx += sx; ax = fm(fs(PXo[vi], x1x), ix); }
+        if (ay == m) { vj += sy; idx += syM; ay = fm(fs(PYo[vj], x1y), iy); }
+        if (az == m) { vk += sz; idx += szMN; az = fm(fs(PZo[vk], x1z), iz); }
+    }
+    r.sum = sum;
+    r.len = len;
+    return r;
+}
+
+template <typename VT, int KIND, bool E64>
+__global__ void __launch_bounds__(FP_THREADS)
+k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
+          const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
+          uint64_t* __restrict__ hash, float* __restrict__ lens)
+{
+    extern __shared__ float sp[];
+    float* PX = sp;
+    float* PY = PX + (g.M + 3);
+    float* PZ = PY + (g.N + 3);
+    for (int t = threadIdx.x; t < g.M + 3; t += FP_THREADS) PX[t] = g.px[t];
+    for (int t = threadIdx.x; t < g.N + 3; t += FP_THREADS) PY[t] = g.py[t];
+    for (int t = threadIdx.x; t < g.Z + 3; t += FP_THREADS) PZ[t] = g.pz[t];
+    __syncthreads();
+
+    const int u = blockIdx.x * FP_BX + (threadIdx.x % FP_BX);
+    const int v = blockIdx.y * FP_BY + (threadIdx.x / FP_BX);
+    const int w = blockIdx.z;
+    const bool active = (u < g.R) && (v < g.ZP);
+    const long long P = (long long)g.R * g.ZP;
+    const long long p = (long long)w * P + (long long)v * g.R + u;
+    double e2 = 0.0;
+    if (active) {
+        const float2 sc = g.trig[view0 + w];
+        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE>(g, PX, PY, PZ, vol, sc.x, sc.y, u, v);
+        const bool zero = rr.len < g.thr_fp;                       // :554
+        if (KIND == FP_FORWARD) {
+            st_any(out, p, out_dt, zero ? 0.0f : rr.sum);
+        } else if (KIND == FP_SART) {
+            const float bv = ld_any(b, p, b_dt);
+            const float cv = zero ? 0.0f : fdv(fs(bv, rr.sum), rr.len);   // :562
+            ((float2*)out)[p] = make_float2(cv, rr.d12);
+        } else if (KIND == FP_OBJECTIVE) {
+            const float ax = zero ? 0.0f : rr.sum;
+            const float bv = ld_any(b, p, b_dt);
+            const float e = fs(ax, bv);
+            e2 = (double)fm(e, e);                                     // L2_norm_kernel, tool_functions.cu:35
+        } else {
+            nseg[p] = rr.nseg;
+            hash[p] = rr.hash;
+            lens[p] = rr.len;
+        }
+    }
+    if (KIND == FP_OBJECTIVE) {
+        __shared__ double sh[FP_THREADS / 32];
+        const double t = block_sum(e2, sh);
+        if (threadIdx.x == 0)
+            partial[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+template <typename VT, int KIND>
+static void launch_fp_t(const Geometry& G, const FpArgs& a, dim3 grid, size_t smem, cudaStream_t st)
+{
+    const VT* vol = (const VT*)a.vol;
+    if (G.dg.entry64)
+        k_forward<VT, KIND, true><<<grid, FP_THREADS, smem, st>>>(G.dg, vol, a.view0, a.out, a.out_dtype, a.b,
+                                                                 a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+    else
+        k_forward<VT, KIND, false><<<grid, FP_THREADS, smem, st>>>(G.dg, vol, a.view0, a.out, a.out_dtype, a.b,
+                                                                  a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+}
+
+ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, size_t* nblocks_out)
+{
+    const DevGeom& g = G.dg;
+    if (a.nview <= 0) return CTR_OK;
+    if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
+    dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + FP_BY - 1) / FP_BY, a.nview);
+    if (nblocks_out) *nblocks_out = (size_t)grid.x * grid.y * grid.z;
+    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 9);
+    CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
+        switch (a.kind) {
+        case FP_FORWARD: launch_fp_t<VT, FP_FORWARD>(G, a, grid, smem, st); break;
+        case FP_SART: launch_fp_t<VT, FP_SART>(G, a, grid, smem, st); break;
+        case FP_OBJECTIVE: launch_fp_t<VT, FP_OBJECTIVE>(G, a, grid, smem, st); break;
+        case FP_TRACE: launch_fp_t<VT, FP_TRACE>(G, a, grid, smem, st); break;
+        }
+    });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+// Ray records (value, chord length) for the adjoint: the chord length is the
+// forward projector's own d12 (:290) for every ray of views [view0, view0+nview).
+__global__ void k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, float2* __restrict__ rays)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y;
+    const int w = blockIdx.z;
+    if (u >= g.R) return;
+    const float2 sc = g.trig[view0 + w];
+    const float s = sc.x, c = sc.y;
+    const float x2x = fs(fm(g.srcx, c), fm(g.srcy, s));
+    const float x2y = fa(fm(g.srcx, s), fm(g.srcy, c));
+    const float pu = fa(g.ymin, fm((float)u, g.du));
+    const float x1x = fs(fm(g.dod, c), fm(pu, s));
+    const float x1y = fa(fm(g.dod, s), fm(pu, c));
+    const float x1z = fa(g.zmin, fm((float)v, g.dv));
+    const float dx = fs(x2x, x1x), dy = fs(x2y, x1y), dz = fs(g.srcz, x1z);
+    const float d12 = __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));
+    const long long p = ((long long)w * g.ZP + v) * g.R + u;
+    rays[p] = make_float2(y[p], d12);
+}
+
+ctr_status launch_ray_prep(const Geometry& G, const float* y, int view0, int nview, float2* rays, cudaStream_t st)
+{
+    if (nview <= 0) return CTR_OK;
+    dim3 grid((G.dg.R + 127) / 128, G.dg.ZP, nview);
+    k_ray_prep<<<grid, 128, 0, st>>>(G.dg, y, view0, rays);
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+}  // namespace ctr

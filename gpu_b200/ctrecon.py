@@ -1,0 +1,405 @@
+"""ctypes binding of ``libctrecon.so`` (``include/ctrecon.h``).
+
+The library is the product; this module only marshals arguments.  Device
+buffers are torch CUDA tensors (their ``data_ptr()``), streams are torch
+streams (``cuda_stream``); host buffers for the reference-compatible entry
+points are numpy arrays.  Every call checks the returned ``ctr_status`` and
+raises :class:`CtrError` with the library's message.
+
+The names of the reference's host functions are mirrored one to one at the
+bottom (``forward_3d_ray_driven_siddon`` ... ``tv_norm_gpu``) with the same
+argument meaning.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libctrecon.so")
+
+# ctr_status
+CTR_OK = 0
+STATUS_NAMES = {
+    0: "CTR_OK", 1: "CTR_ERR_INVALID_ARGUMENT", 2: "CTR_ERR_BAD_GEOMETRY", 3: "CTR_ERR_OUT_OF_MEMORY",
+    4: "CTR_ERR_CUDA", 5: "CTR_ERR_TRAVERSAL_BOUND", 6: "CTR_ERR_TIMEOUT", 7: "CTR_ERR_UNSUPPORTED",
+    8: "CTR_ERR_NO_DEVICE", 9: "CTR_ERR_IO",
+}
+# ctr_dtype
+F32, BF16, F16 = 0, 1, 2
+GEOM_ENTRY_F64 = 0x1
+BP_ACCUMULATE = 0x1
+BP_FOV_MASK = 0x2
+SART_STOCHASTIC_ROUND = 0x1
+
+# every symbol include/ctrecon.h declares
+EXPORTED = [
+    "ctr_geometry_create", "ctr_geometry_destroy", "ctr_geometry_view_trig", "ctr_forward",
+    "ctr_backproject", "ctr_sart_pass", "ctr_sart_views", "ctr_forward_trace", "ctr_fgp_tv", "ctr_fista_momentum",
+    "ctr_objective", "ctr_tv_norm", "ctr_l2_norm", "ctr_fdk", "ctr_dot_test", "ctr_solver_create",
+    "ctr_solver_destroy", "ctr_solver_set_sinogram", "ctr_solver_set_volume", "ctr_solver_iterate",
+    "ctr_solver_get_volume", "ctr_solver_iteration_count", "ctr_solver_save", "ctr_solver_load",
+    "ctr_last_error_string", "ctr_convert", "ctr_phantom_voxelize", "ctr_set_default_geometry",
+    "Forward_3D_ray_driven_siddon", "Reconstruction_3D_ray_driven_CBCT", "CheckMatchedJointOperator",
+    "FGP_denoise_GPUx7_exact", "Reconstruction_FDK", "L2_norm_gpu", "TV_norm_gpu",
+]
+
+
+class CtrError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class GeometryDesc(C.Structure):
+    """Mirror of ``ctr_geometry_desc``."""
+
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("vx", C.c_float), ("vy", C.c_float), ("vz", C.c_float),
+        ("nu", C.c_int), ("nv", C.c_int),
+        ("du", C.c_float), ("dv", C.c_float),
+        ("dso", C.c_float), ("dod", C.c_float), ("offset", C.c_float), ("m_offset", C.c_int),
+        ("n_views", C.c_int), ("us_rate", C.c_float), ("initial_angle", C.c_float),
+        ("shift_angle", C.c_float), ("flags", C.c_uint),
+    ]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [
+        ("beta", C.c_float), ("lambda_tv", C.c_float), ("fgp_iters", C.c_int), ("fista", C.c_int),
+        ("objective", C.c_int), ("use_graph", C.c_int), ("sart_flags", C.c_uint),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the in-tree ``libctrecon.so``; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: run `python gpu_b200/build.py` (the engine has no CPU fallback)")
+    lib = C.CDLL(path)
+    vp, i, f, d, u = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_uint
+    G = C.c_void_p
+    sig = {
+        "ctr_geometry_create": ([C.POINTER(GeometryDesc), C.POINTER(C.c_void_p)], i),
+        "ctr_geometry_destroy": ([G], i),
+        "ctr_geometry_view_trig": ([G, i, C.POINTER(f), C.POINTER(f)], i),
+        "ctr_forward": ([G, vp, i, vp, i, i, i, vp], i),
+        "ctr_backproject": ([G, vp, i, i, vp, i, u, vp], i),
+        "ctr_sart_pass": ([G, vp, i, vp, i, f, u, C.c_uint32, vp], i),
+        "ctr_sart_views": ([G, vp, i, vp, i, f, u, C.c_uint32, i, i, C.POINTER(f), C.POINTER(f), vp], i),
+        "ctr_forward_trace": ([G, vp, i, vp, vp, vp, vp], i),
+        "ctr_fgp_tv": ([G, vp, i, f, i, vp], i),
+        "ctr_fista_momentum": ([G, vp, vp, vp, i, f, f, vp], i),
+        "ctr_objective": ([G, vp, i, vp, i, C.POINTER(d), C.POINTER(d), vp], i),
+        "ctr_tv_norm": ([G, vp, i, C.POINTER(d), vp], i),
+        "ctr_l2_norm": ([vp, vp, C.c_int64, C.POINTER(d), vp], i),
+        "ctr_fdk": ([G, vp, vp, vp], i),
+        "ctr_dot_test": ([G, vp, vp, i, i, C.POINTER(d), C.POINTER(d), vp], i),
+        "ctr_solver_create": ([G, i, C.POINTER(SolverParams), C.POINTER(C.c_void_p)], i),
+        "ctr_solver_destroy": ([vp], i),
+        "ctr_solver_set_sinogram": ([vp, vp, i], i),
+        "ctr_solver_set_volume": ([vp, vp, vp], i),
+        "ctr_solver_iterate": ([vp, i, vp, vp], i),
+        "ctr_solver_get_volume": ([vp, vp, vp], i),
+        "ctr_solver_iteration_count": ([vp, C.POINTER(i)], i),
+        "ctr_solver_save": ([vp, C.c_char_p, vp], i),
+        "ctr_solver_load": ([vp, C.c_char_p, vp], i),
+        "ctr_last_error_string": ([], C.c_char_p),
+        "ctr_convert": ([vp, i, vp, i, C.c_int64, vp], i),
+        "ctr_phantom_voxelize": ([G, vp, i, vp, vp], i),
+        "ctr_set_default_geometry": ([C.POINTER(GeometryDesc)], i),
+        "Forward_3D_ray_driven_siddon": ([vp, vp], None),
+        "Reconstruction_3D_ray_driven_CBCT": ([vp, vp, f], None),
+        "CheckMatchedJointOperator": ([vp], None),
+        "FGP_denoise_GPUx7_exact": ([vp, f, i], None),
+        "Reconstruction_FDK": ([vp, vp], None),
+        "L2_norm_gpu": ([vp, vp], d),
+        "TV_norm_gpu": ([vp], d),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load_library().ctr_last_error_string().decode()
+
+
+def check(status):
+    if status != CTR_OK:
+        raise CtrError(status, last_error())
+
+
+def _ptr(t):
+    """Device (torch) or host (numpy) buffer address."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        if not t.is_contiguous():
+            raise ValueError("buffer must be contiguous")
+        return t.data_ptr()
+    if isinstance(t, np.ndarray):
+        if not t.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return t.ctypes.data
+    return int(t)
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def dtype_code(t) -> int:
+    import torch
+    dt = t.dtype
+    if dt == torch.float32:
+        return F32
+    if dt == torch.bfloat16:
+        return BF16
+    if dt == torch.float16:
+        return F16
+    raise TypeError(f"unsupported dtype {dt}")
+
+
+def make_desc(nx, ny, nz, vx, nu, nv, du, dso, dod, n_views, us_rate=None, initial_angle=0.0,
+              shift_angle=0.0, offset=0.0, m_offset=0, entry64=False, vy=0.0, vz=0.0, dv=0.0):
+    if us_rate is None:
+        us_rate = 360.0 / n_views
+    return GeometryDesc(nx, ny, nz, vx, vy, vz, nu, nv, du, dv, dso, dod, offset, m_offset, n_views,
+                        us_rate, initial_angle, shift_angle, GEOM_ENTRY_F64 if entry64 else 0)
+
+
+class Geometry:
+    """A scan geometry on the current CUDA device (``ctr_geometry``)."""
+
+    def __init__(self, desc: GeometryDesc):
+        self.lib = load_library()
+        self.desc = desc
+        h = C.c_void_p()
+        check(self.lib.ctr_geometry_create(C.byref(desc), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ctr_geometry_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # shapes
+    @property
+    def vol_shape(self):
+        return (self.desc.nz, self.desc.ny, self.desc.nx)
+
+    @property
+    def view_shape(self):
+        return (self.desc.nv, self.desc.nu)
+
+    @property
+    def n_views(self):
+        return self.desc.n_views
+
+    def view_trig(self, view):
+        s, c = C.c_float(), C.c_float()
+        check(self.lib.ctr_geometry_view_trig(self.h, view, C.byref(s), C.byref(c)))
+        return s.value, c.value
+
+    # operators (device tensors)
+    def forward(self, vol, sino, view_begin=0, view_count=None, stream=None):
+        n = self.n_views - view_begin if view_count is None else view_count
+        check(self.lib.ctr_forward(self.h, _ptr(vol), dtype_code(vol), _ptr(sino), dtype_code(sino),
+                                   view_begin, n, _stream(stream)))
+        return sino
+
+    def backproject(self, sino, vol, view_begin=0, view_count=None, flags=0, stream=None):
+        n = self.n_views - view_begin if view_count is None else view_count
+        check(self.lib.ctr_backproject(self.h, _ptr(sino), view_begin, n, _ptr(vol), dtype_code(vol), flags,
+                                       _stream(stream)))
+        return vol
+
+    def sart_pass(self, vol, sino, beta, flags=0, seed=0, stream=None):
+        check(self.lib.ctr_sart_pass(self.h, _ptr(vol), dtype_code(vol), _ptr(sino), dtype_code(sino), beta, flags,
+                                     seed, _stream(stream)))
+        return vol
+
+    def sart_views(self, vol, sino, beta, view_begin, view_count, flags=0, seed=0, timed=False, stream=None):
+        """SART over a view range; with timed=True returns (fp_ms, bp_ms) summed kernel times."""
+        fp, bp = C.c_float(), C.c_float()
+        check(self.lib.ctr_sart_views(self.h, _ptr(vol), dtype_code(vol), _ptr(sino), dtype_code(sino), beta, flags,
+                                      seed, view_begin, view_count, C.byref(fp) if timed else None,
+                                      C.byref(bp) if timed else None, _stream(stream)))
+        return (fp.value, bp.value) if timed else None
+
+    def forward_trace(self, vol, view, nseg, hsh, length, stream=None):
+        check(self.lib.ctr_forward_trace(self.h, _ptr(vol), view, _ptr(nseg), _ptr(hsh), _ptr(length),
+                                         _stream(stream)))
+
+    def fgp_tv(self, vol, lam, n_iter, stream=None):
+        check(self.lib.ctr_fgp_tv(self.h, _ptr(vol), dtype_code(vol), lam, n_iter, _stream(stream)))
+        return vol
+
+    def fista_momentum(self, y, x_prev, x, t_prev, t_k, stream=None):
+        check(self.lib.ctr_fista_momentum(self.h, _ptr(y), _ptr(x_prev), _ptr(x), dtype_code(y), t_prev, t_k,
+                                          _stream(stream)))
+
+    def objective(self, vol, sino, stream=None):
+        fid, tv = C.c_double(), C.c_double()
+        check(self.lib.ctr_objective(self.h, _ptr(vol), dtype_code(vol), _ptr(sino), dtype_code(sino),
+                                     C.byref(fid), C.byref(tv), _stream(stream)))
+        return fid.value, tv.value
+
+    def tv_norm(self, vol, stream=None):
+        tv = C.c_double()
+        check(self.lib.ctr_tv_norm(self.h, _ptr(vol), dtype_code(vol), C.byref(tv), _stream(stream)))
+        return tv.value
+
+    def fdk(self, sino, vol, stream=None):
+        check(self.lib.ctr_fdk(self.h, _ptr(sino), _ptr(vol), _stream(stream)))
+        return vol
+
+    def dot_test(self, x, y, view_begin=0, view_count=None, stream=None):
+        n = self.n_views - view_begin if view_count is None else view_count
+        a, b = C.c_double(), C.c_double()
+        check(self.lib.ctr_dot_test(self.h, _ptr(x), _ptr(y), view_begin, n, C.byref(a), C.byref(b),
+                                    _stream(stream)))
+        return a.value, b.value
+
+    def phantom_voxelize(self, params, vol, stream=None):
+        p = np.ascontiguousarray(params, np.float64)
+        check(self.lib.ctr_phantom_voxelize(self.h, p.ctypes.data, p.shape[0], _ptr(vol), _stream(stream)))
+        return vol
+
+
+def l2_norm(a, b, stream=None):
+    out = C.c_double()
+    check(load_library().ctr_l2_norm(_ptr(a), _ptr(b), a.numel(), C.byref(out), _stream(stream)))
+    return out.value
+
+
+def convert(src, dst, stream=None):
+    check(load_library().ctr_convert(_ptr(src), dtype_code(src), _ptr(dst), dtype_code(dst), src.numel(),
+                                     _stream(stream)))
+    return dst
+
+
+class Solver:
+    """SART + FISTA + FGP-TV outer loop on device buffers (``ctr_solver``)."""
+
+    def __init__(self, geom: Geometry, vol_dtype=F32, beta=0.8, lambda_tv=0.0, fgp_iters=20, fista=True,
+                 objective=True, use_graph=True, sart_flags=0):
+        self.geom = geom
+        self.lib = geom.lib
+        self.params = SolverParams(beta, lambda_tv, fgp_iters, int(fista), int(objective), int(use_graph),
+                                   sart_flags)
+        h = C.c_void_p()
+        check(self.lib.ctr_solver_create(geom.h, vol_dtype, C.byref(self.params), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ctr_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_sinogram(self, sino):
+        self._sino = sino  # keep the borrowed buffer alive
+        check(self.lib.ctr_solver_set_sinogram(self.h, _ptr(sino), dtype_code(sino)))
+
+    def set_volume(self, vol=None, stream=None):
+        check(self.lib.ctr_solver_set_volume(self.h, _ptr(vol), _stream(stream)))
+
+    def iterate(self, n, stream=None):
+        obj = np.zeros(3 * max(n, 1), np.float64)
+        check(self.lib.ctr_solver_iterate(self.h, n, obj.ctypes.data, _stream(stream)))
+        return obj[: 3 * n].reshape(n, 3)
+
+    def get_volume(self, out, stream=None):
+        check(self.lib.ctr_solver_get_volume(self.h, _ptr(out), _stream(stream)))
+        return out
+
+    @property
+    def iteration(self):
+        k = C.c_int()
+        check(self.lib.ctr_solver_iteration_count(self.h, C.byref(k)))
+        return k.value
+
+    def save(self, path, stream=None):
+        check(self.lib.ctr_solver_save(self.h, str(path).encode(), _stream(stream)))
+
+    def load(self, path, stream=None):
+        check(self.lib.ctr_solver_load(self.h, str(path).encode(), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# The reference's host entry points (V63/host_*.c[u|pp]), same names and
+# argument meaning; host numpy arrays are updated in place like the reference.
+# ---------------------------------------------------------------------------
+
+def set_default_geometry(desc: GeometryDesc):
+    check(load_library().ctr_set_default_geometry(C.byref(desc)))
+
+
+def _after_void():
+    msg = last_error()
+    if msg:
+        raise CtrError(-1, msg)
+
+
+def forward_3d_ray_driven_siddon(h_volume: np.ndarray, h_proj_data: np.ndarray):
+    load_library().Forward_3D_ray_driven_siddon(_ptr(h_volume), _ptr(h_proj_data))
+    _after_void()
+
+
+def reconstruction_3d_ray_driven_cbct(h_volume: np.ndarray, h_proj_data: np.ndarray, beta: float):
+    load_library().Reconstruction_3D_ray_driven_CBCT(_ptr(h_volume), _ptr(h_proj_data), beta)
+    _after_void()
+
+
+def check_matched_joint_operator(h_volume: np.ndarray):
+    load_library().CheckMatchedJointOperator(_ptr(h_volume))
+    _after_void()
+
+
+def fgp_denoise_gpux7_exact(h_f: np.ndarray, lam: float, n_iter: int):
+    load_library().FGP_denoise_GPUx7_exact(_ptr(h_f), lam, n_iter)
+    _after_void()
+
+
+def reconstruction_fdk(h_volume: np.ndarray, h_proj_data: np.ndarray):
+    load_library().Reconstruction_FDK(_ptr(h_volume), _ptr(h_proj_data))
+    _after_void()
+
+
+def l2_norm_gpu(a, b) -> float:
+    r = load_library().L2_norm_gpu(_ptr(a), _ptr(b))
+    _after_void()
+    return r
+
+
+def tv_norm_gpu(vol) -> float:
+    r = load_library().TV_norm_gpu(_ptr(vol))
+    _after_void()
+    return r

@@ -1,0 +1,260 @@
+/*
+ * ctrecon.h -- C ABI of the B200 cone-beam CT reconstruction engine.
+ *
+ * One process, one GPU.  Every entry point returns a ctr_status (0 = OK);
+ * ctr_last_error_string() gives the calling thread's last message.  Nothing
+ * in the library calls exit() or assert().
+ *
+ * Units: any consistent length unit (the reference uses metres, the scan
+ * descriptions used by the tests use millimetres).
+ *
+ * Layouts are the reference's:
+ *   volume    vol[k*nx*ny + j*nx + i]         (k = z slice, j = y row, i = x)
+ *   view      view[row*nu + col]              (row = detector z, col = detector u)
+ *   sinogram  views stacked: sino[view*nu*nv + row*nu + col]
+ *
+ * Native API: device pointers, an explicit CUDA stream (cudaStream_t passed
+ * as void*; NULL = the legacy default stream), asynchronous unless stated.
+ * Reference-compatible API (bottom of this file): the reference's host
+ * function names and signatures, host pointers, synchronous.
+ *
+ * Reference interface citations use CBCT/CBCT_1024V_1024P_multiGPU_v6.3_20170823/
+ * (abbreviated V63/).
+ */
+#ifndef CTRECON_H
+#define CTRECON_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTRECON_ABI_VERSION 1
+
+typedef enum ctr_status {
+    CTR_OK = 0,
+    CTR_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad dtype, bad view range      */
+    CTR_ERR_BAD_GEOMETRY = 2,     /* geometry description rejected                         */
+    CTR_ERR_OUT_OF_MEMORY = 3,    /* a device or host allocation failed                     */
+    CTR_ERR_CUDA = 4,             /* a CUDA runtime call failed (message has the CUDA text)  */
+    CTR_ERR_TRAVERSAL_BOUND = 5,  /* a ray took more than nx+ny+nz+3 Siddon steps            */
+    CTR_ERR_TIMEOUT = 6,          /* a device-side wait gave up                              */
+    CTR_ERR_UNSUPPORTED = 7,      /* combination not implemented                             */
+    CTR_ERR_NO_DEVICE = 8,        /* no CUDA device, or not an sm_100 device                 */
+    CTR_ERR_IO = 9                /* file could not be read or written                       */
+} ctr_status;
+
+/* storage type of a volume or sinogram buffer; arithmetic is always FP32
+ * (FP64 for the norm reductions) */
+typedef enum ctr_dtype { CTR_F32 = 0, CTR_BF16 = 1, CTR_F16 = 2 } ctr_dtype;
+
+/* Scan geometry: the reference's compile-time constants (V63/main_recon.cu:54-111)
+ * as a run-time description.  Circular orbit; source at (dso, offset, 0) and
+ * the detector plane at x = dod (< 0), both rotated by the view angle. */
+typedef struct ctr_geometry_desc {
+    int   nx, ny, nz;          /* M, N, ZETA: voxels                                   */
+    float vx, vy, vz;          /* voxel pitch (volumn_x/y/z); vy, vz <= 0 mean = vx     */
+    int   nu, nv;              /* R (detector columns), Z_prj (detector rows)           */
+    float du, dv;              /* detector pitch (Detector_pixel_x); dv <= 0 means = du */
+    float dso;                 /* DSO: source to isocentre                              */
+    float dod;                 /* DOD: detector plane position (negative)               */
+    float offset;              /* Offset: half-detector shift (source y and detector u) */
+    int   m_offset;            /* M_Offset: volume x shift in voxels                    */
+    int   n_views;             /* Nviews                                                */
+    float us_rate;             /* degrees between views                                 */
+    float initial_angle;       /* degrees                                               */
+    float shift_angle;         /* degrees                                               */
+    unsigned flags;            /* CTR_GEOM_* below                                      */
+} ctr_geometry_desc;
+
+/* Compute the ray-box entry/exit parameters and the first plane indices in
+ * FP64 (the traversal itself stays FP32). */
+#define CTR_GEOM_ENTRY_F64 0x1u
+
+typedef struct ctr_geometry ctr_geometry;
+
+/* Validate the description, derive the reference's float constants, and
+ * upload the per-view and per-plane tables to the current device.
+ * Replaces the compile-time globals of V63/main_recon.cu:60-111. */
+ctr_status ctr_geometry_create(const ctr_geometry_desc* desc, ctr_geometry** out);
+ctr_status ctr_geometry_destroy(ctr_geometry* geom);
+/* Per-view sin/cos of the FP frame angle -(j*us_rate+initial+shift)*pi/180
+ * (V63/host_IterativeRecon_CBCT.c:34-41), as the kernels use them. */
+ctr_status ctr_geometry_view_trig(const ctr_geometry* geom, int view, float* sin_out, float* cos_out);
+
+/* ---------------------------------------------------------------- projectors */
+
+/* sino[w] = A_(view_begin+w) vol for w < view_count (Siddon ray sums, command 0
+ * of V63/kernel_IterativeRecon_universal.cu:7-567).  Replaces the per-view
+ * launches of Forward_3D_ray_driven_siddon (V63/host_IterativeRecon_CBCT.c:70-128). */
+ctr_status ctr_forward(const ctr_geometry* geom, const void* vol, ctr_dtype vol_dtype,
+                       void* sino, ctr_dtype sino_dtype, int view_begin, int view_count,
+                       void* stream);
+
+/* Matched adjoint: vol = sum_w A_(view_begin+w)^T sino[w] (FP32 sino), with the
+ * forward projector's own Siddon chord lengths (gather form, no atomics).
+ * CTR_BP_ACCUMULATE adds into vol instead of overwriting; CTR_BP_FOV_MASK skips
+ * voxels outside the reconstruction cylinder and keeps the reference's
+ * thresholds, i.e. command 0 of backprj_ray_driven_3d_kernel
+ * (V63/kernel_IterativeRecon_universal.cu:571-810) as used by
+ * CheckMatchedJointOperator (V63/host_IterativeRecon_CBCT.c:131-204). */
+#define CTR_BP_ACCUMULATE 0x1u
+#define CTR_BP_FOV_MASK 0x2u
+ctr_status ctr_backproject(const ctr_geometry* geom, const float* sino, int view_begin,
+                           int view_count, void* vol, ctr_dtype vol_dtype, unsigned flags,
+                           void* stream);
+
+/* One SART pass over all views in order: per view, FP command 1 (correction
+ * (b - Af)/len) then BP command 1 (f += beta * sum(w c)/sum(w) inside the FOV
+ * cylinder).  Replaces Reconstruction_3D_ray_driven_CBCT
+ * (V63/host_IterativeRecon_CBCT.c:1-67) on device buffers.
+ * CTR_SART_STOCHASTIC_ROUND rounds BF16/F16 voxel updates stochastically. */
+#define CTR_SART_STOCHASTIC_ROUND 0x1u
+ctr_status ctr_sart_pass(const ctr_geometry* geom, void* vol, ctr_dtype vol_dtype,
+                         const void* sino, ctr_dtype sino_dtype, float beta, unsigned flags,
+                         uint32_t seed, void* stream);
+
+/* The SART pass restricted to views [view_begin, view_begin+view_count), in
+ * order.  When fp_ms / bp_ms are non-NULL the library records CUDA events
+ * around every forward and backprojection launch on the stream, synchronises,
+ * and returns the summed kernel times in milliseconds (profiling hook). */
+ctr_status ctr_sart_views(const ctr_geometry* geom, void* vol, ctr_dtype vol_dtype, const void* sino,
+                          ctr_dtype sino_dtype, float beta, unsigned flags, uint32_t seed,
+                          int view_begin, int view_count, float* fp_ms, float* bp_ms, void* stream);
+
+/* Trace one view: per ray, the number of Siddon segments, an FNV-1a hash of
+ * the visited voxel index sequence and the summed chord length.  For parity
+ * checks of the traversal (the voxel index set of every ray). */
+ctr_status ctr_forward_trace(const ctr_geometry* geom, const float* vol, int view, int* nseg,
+                             uint64_t* hash, float* len, void* stream);
+
+/* ----------------------------------------------------- TV prox and FISTA */
+
+/* In-place FGP TV prox: vol = argmin 0.5||x - vol||^2 + lambda TV_iso(x), n_iter
+ * Beck-Teboulle FGP steps with dual step 1/(12 lambda).  Replaces
+ * FGP_denoise_GPUx7_exact (V63/host_FGP_Denoise_GPUx7.c:1-111, kernels
+ * V63/kernel_FGP_Denoise_GPUx7.cu:2-88).  Workspace: 9 volume-sized dual arrays
+ * of vol_dtype, allocated on first use and kept with the geometry. */
+ctr_status ctr_fgp_tv(const ctr_geometry* geom, void* vol, ctr_dtype vol_dtype, float lambda,
+                      int n_iter, void* stream);
+
+/* FISTA outer step (V63/main_recon.cu:372-384):
+ *   y = x + (t_prev - 1)/t_k * (x - x_prev);  x_prev = x.
+ * y may alias x.  t_k = (1 + sqrt(1 + 4 t_prev^2))/2 is the caller's. */
+ctr_status ctr_fista_momentum(const ctr_geometry* geom, void* y, void* x_prev, const void* x,
+                              ctr_dtype dtype, float t_prev, float t_k, void* stream);
+
+/* ---------------------------------------------------------------- objective */
+
+/* sum over all views of (A vol - sino)^2 and the isotropic TV of vol, both
+ * reduced in FP64.  Synchronises the stream.  Replaces L2_norm_gpu and
+ * TV_norm_gpu (V63/host_tool_functions.cu:28-101) after the objective's
+ * Forward_3D_ray_driven_siddon (V63/main_recon.cu:401-417). */
+ctr_status ctr_objective(const ctr_geometry* geom, const void* vol, ctr_dtype vol_dtype,
+                         const void* sino, ctr_dtype sino_dtype, double* fidelity, double* tv,
+                         void* stream);
+/* TV_norm_gpu (V63/host_tool_functions.cu:61-101): FP64 sum of the per-voxel
+ * forward-difference TV terms.  Synchronises the stream. */
+ctr_status ctr_tv_norm(const ctr_geometry* geom, const void* vol, ctr_dtype dtype, double* tv,
+                       void* stream);
+/* L2_norm_gpu (V63/host_tool_functions.cu:28-58) without its in-place side
+ * effect: FP64 sum of float (a - b)^2 over n elements.  Synchronises. */
+ctr_status ctr_l2_norm(const float* a, const float* b, int64_t n, double* out, void* stream);
+
+/* --------------------------------------------------------------------- FDK */
+
+/* FDK: cosine pre-weight, spatial-domain ramp (the exact kernel of the
+ * reference's padded-DFT filter |k|*F_step*0.5 on a 2R grid), then voxel-driven
+ * bilinear backprojection in the +theta frame, accumulated into vol (FP32).
+ * Replaces Reconstruction_FDK (V63/host_FDK.cpp:4-57; kernels
+ * V63/FDK/kernel_FDK.cu:1-62; ramp V63/FDK/FFT_1d_GPU.h:241-287).
+ * Workspace: one FP32 sinogram copy, allocated per call. */
+ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float* vol, void* stream);
+
+/* ------------------------------------------------------------ dot product */
+
+/* <A x, y> and <x, A^T y> over views [view_begin, view_begin+view_count), FP64
+ * inner products of FP32 operators.  Synchronises.  The matched-adjoint
+ * check of CheckMatchedJointOperator (V63/host_IterativeRecon_CBCT.c:131-204). */
+ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, const float* y, int view_begin,
+                        int view_count, double* ax_dot_y, double* x_dot_aty, void* stream);
+
+/* ------------------------------------------------------- iterative solver */
+
+/* SART + FISTA + FGP-TV outer loop of V63/main_recon.cu:286-484 (FISTA == 1)
+ * on device buffers.  One iteration: x = SART(y); x = FGP(x, beta*lambda_tv);
+ * t_k = (1+sqrt(1+4 t^2))/2; y = x + (t-1)/t_k (x - x_prev); x_prev = x; and,
+ * when requested, the objective [TV, fidelity, fidelity + 2 lambda_tv TV]. */
+typedef struct ctr_solver_params {
+    float beta;            /* SART relaxation, the reference's 2/Lip_con               */
+    float lambda_tv;       /* lambda_TV; the FGP weight is beta*lambda_tv (main:162)     */
+    int   fgp_iters;       /* Niter_denoise (20)                                         */
+    int   fista;           /* 1: FISTA momentum (FISTA == 1); 0: SART + TV only          */
+    int   objective;       /* 1: evaluate the objective every iteration                  */
+    int   use_graph;       /* 1: capture one iteration as a CUDA graph and replay it     */
+    unsigned sart_flags;   /* CTR_SART_*                                                 */
+} ctr_solver_params;
+
+typedef struct ctr_solver ctr_solver;
+
+ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vol_dtype,
+                             const ctr_solver_params* params, ctr_solver** out);
+ctr_status ctr_solver_destroy(ctr_solver* s);
+/* Borrow the measured sinogram (device, n_views*nv*nu of sino_dtype); it must
+ * stay valid while the solver iterates. */
+ctr_status ctr_solver_set_sinogram(ctr_solver* s, const void* sino, ctr_dtype sino_dtype);
+/* Set the estimate (device, vol_dtype; NULL = zeros) and restart FISTA (t = 1). */
+ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void* stream);
+/* Run n outer iterations.  objective_out (host, may be NULL) receives 3 doubles
+ * per iteration: TV, fidelity, objective.  Synchronises the stream. */
+ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* objective_out, void* stream);
+/* Copy the current estimate x_k (vol_dtype) to dst (device or host). */
+ctr_status ctr_solver_get_volume(ctr_solver* s, void* dst, void* stream);
+ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k);
+/* Exact checkpoint of the FISTA state (x_k, y_k, t_k, k and a geometry hash),
+ * raw little-endian, and its restore. */
+ctr_status ctr_solver_save(ctr_solver* s, const char* path, void* stream);
+ctr_status ctr_solver_load(ctr_solver* s, const char* path, void* stream);
+
+/* ------------------------------------------------------------- utilities */
+
+/* Thread-local text of the last failure on this thread ("" if none). */
+const char* ctr_last_error_string(void);
+/* Convert between storage types on the device (n elements). */
+ctr_status ctr_convert(const void* src, ctr_dtype src_dtype, void* dst, ctr_dtype dst_dtype,
+                       int64_t n, void* stream);
+/* Add seeded ellipsoids to a device volume: params is n x 10 host doubles
+ * (cx,cy,cz, ax,ay,az, phi,theta,psi (z-x-z Euler, radians), attenuation). */
+ctr_status ctr_phantom_voxelize(const ctr_geometry* geom, const double* params, int n,
+                                float* vol, void* stream);
+
+/* ------------------------------------------- reference-compatible entry points */
+
+/* The reference's host functions keep their geometry in compile-time globals;
+ * these names take it from the default geometry set here.  All take host
+ * (pinned or pageable) or device pointers, copy in and out like the reference,
+ * and report failures through ctr_last_error_string(). */
+ctr_status ctr_set_default_geometry(const ctr_geometry_desc* desc);
+
+/* V63/host_IterativeRecon_CBCT.c:70-128: A x for all views into h_proj_data. */
+void Forward_3D_ray_driven_siddon(float* h_volume, float* h_proj_data);
+/* V63/host_IterativeRecon_CBCT.c:1-67: one SART pass, h_volume updated in place. */
+void Reconstruction_3D_ray_driven_CBCT(float* h_volume, float* h_proj_data, float beta_temp);
+/* V63/host_IterativeRecon_CBCT.c:131-204: prints <Ax,Ax> and <x,A^T A x> for view 0. */
+void CheckMatchedJointOperator(float* h_volume);
+/* V63/host_FGP_Denoise_GPUx7.c:1-111: TV prox of h_f_noise in place. */
+void FGP_denoise_GPUx7_exact(float* h_f_noise, float lambda, int Niter_denoise);
+/* V63/host_FDK.cpp:4-57: FDK of h_proj_data accumulated into h_volume. */
+void Reconstruction_FDK(float* h_volume, float* h_proj_data);
+/* V63/host_tool_functions.cu:28-58: sum over all views of (a-b)^2; unlike the
+ * reference, d_a is not overwritten. */
+double L2_norm_gpu(float* d_a, float* d_b);
+/* V63/host_tool_functions.cu:61-101 */
+double TV_norm_gpu(float* d_volume);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CTRECON_H */

@@ -1,0 +1,42 @@
+"""Small scan descriptions shared by the tests (sizes in millimetres).
+
+Each entry: nx, ny, nz, nu, nv, nviews, vx, du, dso, dod, and optional
+offset, m_offset, initial_angle, shift_angle.  The odd detector sizes put a
+detector column and row exactly on the central ray, so axis-parallel rays
+exist; the angle steps hit 0, 90, 180 and 270 degrees.
+"""
+
+SMALL = {
+    "cube16": dict(nx=16, ny=16, nz=16, nu=24, nv=20, nviews=12, vx=1.0, du=1.6, dso=1000.0, dod=-500.0),
+    "odd": dict(nx=12, ny=12, nz=12, nu=17, nv=13, nviews=8, vx=1.0, du=1.6, dso=1000.0, dod=-500.0),
+    "fine": dict(nx=20, ny=20, nz=20, nu=31, nv=9, nviews=16, vx=0.5, du=0.4, dso=1000.0, dod=-500.0),
+    "aniso": dict(nx=18, ny=14, nz=10, nu=27, nv=15, nviews=10, vx=1.0, du=1.6, dso=1000.0, dod=-500.0,
+                  offset=0.8, m_offset=1, initial_angle=3.5, shift_angle=1.25),
+}
+
+# the reference's sample configuration, scaled down in resolution only
+# (128^3, 1 mm voxels, 128^2 detector at 1.6 mm, 180 views over 360 degrees)
+CONFIG0 = dict(nx=128, ny=128, nz=128, nu=128, nv=128, nviews=180, vx=1.0, du=1.6, dso=1000.0, dod=-500.0)
+
+
+def og_desc(cfg):
+    from oracle.ctoracle import make_desc
+    return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["nu"], cfg["nv"], cfg["nviews"], cfg["vx"], cfg["du"],
+                     cfg["dso"], cfg["dod"], initial_angle=cfg.get("initial_angle", 0.0),
+                     shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
+                     m_offset=cfg.get("m_offset", 0))
+
+
+def og_desc_xyz(cfg):
+    """Oracle description with independent nx, ny, nz."""
+    d = og_desc(cfg)
+    d.nx, d.ny, d.nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    return d
+
+
+def ctr_desc(cfg, entry64=False):
+    from gpu_b200.ctrecon import make_desc
+    return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["vx"], cfg["nu"], cfg["nv"], cfg["du"], cfg["dso"],
+                     cfg["dod"], cfg["nviews"], initial_angle=cfg.get("initial_angle", 0.0),
+                     shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
+                     m_offset=cfg.get("m_offset", 0), entry64=entry64)
