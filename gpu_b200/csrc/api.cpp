@@ -38,7 +38,7 @@ ctr_status need_dtype(int dt, const char* what)
 // views per adjoint pass: bounded so the ray records stay under ~256 MB
 int adjoint_batch(const Geometry* g)
 {
-    long long b = (256LL << 20) / (8LL * g->npix());
+    long long b = (256LL << 20) / (16LL * g->npix());
     if (b < 1) b = 1;
     if (b > 32) b = 32;
     return (int)b;
@@ -66,7 +66,7 @@ ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, c
                       unsigned flags, uint32_t seed, int v0, int nv, cudaStream_t st, cudaEvent_t* ev)
 {
     const long long P = g->npix();
-    CTR_TRY(ensure_rays(g, (size_t)P));
+    CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
     for (int j = v0; j < v0 + nv; ++j) {
         if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0)], st));
         FpArgs a{};
@@ -154,10 +154,10 @@ extern "C" ctr_status ctr_backproject(const ctr_geometry* geom, const float* sin
         if (!(flags & CTR_BP_ACCUMULATE)) CTR_CUDA_TRY(cudaMemsetAsync(vol, 0, g->nvox() * dtype_size(vdt), st));
         return CTR_OK;
     }
-    CTR_TRY(ensure_rays(g, (size_t)P * batch));
+    CTR_TRY(ensure_rays(g, (size_t)P * batch * sizeof(float4)));
     for (int c = 0; c < n; c += batch) {
         const int cnt = std::min(batch, n - c);
-        CTR_TRY(launch_ray_prep(*g, sino + (size_t)c * P, v0 + c, cnt, g->d_rays, st));
+        CTR_TRY(launch_ray_prep(*g, sino + (size_t)c * P, v0 + c, cnt, (float4*)g->d_rays, st));
         BpArgs b{};
         b.vol = vol; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = v0 + c; b.nview = cnt; b.sart = 0;
         b.flags = (flags & CTR_BP_FOV_MASK) | ((c > 0 || (flags & CTR_BP_ACCUMULATE)) ? CTR_BP_ACCUMULATE : 0u);
@@ -500,7 +500,7 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st)
     if (!s->p.use_graph || stoch)   // the seed changes every pass: issue directly
         return sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st);
     if (!s->exec) {
-        CTR_TRY(ensure_rays(s->g, (size_t)s->g->npix()));
+        CTR_TRY(ensure_rays(s->g, (size_t)s->g->npix() * sizeof(float2)));
         cudaStream_t cs;
         CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);

@@ -26,11 +26,17 @@ static constexpr int BP_BY = 4;    // voxel rows along y per block
 static constexpr int BP_THREADS = BP_BX * BP_BY;
 static constexpr int BP_K = 4;     // z voxels per thread
 
-template <typename VT, bool SART, bool MASK, bool STOCH>
+// Ray records: REC = float2 (c, d12) for the SART update and the reference's
+// command-0 backprojection, whose chords are purely geometric like the
+// reference BP's; REC = float4 (y, d12, alpha_lo, alpha_hi) for the matched
+// adjoint, whose chords are clipped to the interval the forward traversal
+// covered (empty where the reference traversal drops a ray at a volume edge).
+template <typename VT, typename REC, bool SART, bool MASK, bool STOCH>
 __global__ void __launch_bounds__(BP_THREADS)
-k_backproject(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view0, int nview,
+k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ rays, int view0, int nview,
               int accumulate, float beta, uint32_t seed)
 {
+    constexpr bool WINDOW = sizeof(REC) == sizeof(float4) && !SART && !MASK;
     extern __shared__ float sp[];
     float* PX = sp;
     float* PY = PX + (g.M + 3);
@@ -111,7 +117,7 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ 
                 }
             }
             const float4* __restrict__ colt = g.colt + (long long)view * R;
-            const float2* __restrict__ rw = rays + (long long)w * R * ZP;
+            const REC* __restrict__ rw = rays + (long long)w * R * ZP;
             for (int uu = ulo; uu <= uhi; ++uu) {
                 const float4 ct = __ldg(colt + uu);
                 // xy entry/exit of this ray column through the voxel column
@@ -127,9 +133,13 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ 
                     for (int vv = vlo[kk]; vv <= vhi[kk]; ++vv) {
                         const float2 rt = RT[vv];
                         const float az0 = fm(fs(zl, rt.x), rt.y), az1 = fm(fs(zh, rt.x), rt.y);
-                        const float lo = fmaxf(a, fminf(az0, az1));
-                        const float hi = fminf(bb, fmaxf(az0, az1));
-                        const float2 rec = __ldg(rw + (long long)vv * R + uu);
+                        float lo = fmaxf(a, fminf(az0, az1));
+                        float hi = fminf(bb, fmaxf(az0, az1));
+                        const REC rec = __ldg(rw + (long long)vv * R + uu);
+                        if constexpr (WINDOW) {
+                            lo = fmaxf(lo, rec.z);
+                            hi = fminf(hi, rec.w);
+                        }
                         const float temp = fm(rec.y, fs(hi, lo));
                         if (SART || MASK) {
                             if (temp > g.thr_bp) {                        // :785-791
@@ -167,14 +177,14 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ 
     }
 }
 
-template <typename VT, bool SART, bool MASK, bool STOCH>
+template <typename VT, typename REC, bool SART, bool MASK, bool STOCH>
 static void launch_bp_t(const Geometry& G, const BpArgs& a, cudaStream_t st)
 {
     const DevGeom& g = G.dg;
     dim3 grid((g.M + BP_BX - 1) / BP_BX, (g.N + BP_BY - 1) / BP_BY, (g.Z + BP_K - 1) / BP_K);
     const size_t smem = sizeof(float) * (size_t)(g.M + 3 + g.N + 3 + ((g.Z + 3 + 1) & ~1)) + sizeof(float2) * g.ZP;
-    k_backproject<VT, SART, MASK, STOCH><<<grid, BP_THREADS, smem, st>>>(
-        g, (VT*)a.vol, a.rays, a.view0, a.nview, (a.flags & CTR_BP_ACCUMULATE) ? 1 : 0, a.beta, a.seed);
+    k_backproject<VT, REC, SART, MASK, STOCH><<<grid, BP_THREADS, smem, st>>>(
+        g, (VT*)a.vol, (const REC*)a.rays, a.view0, a.nview, (a.flags & CTR_BP_ACCUMULATE) ? 1 : 0, a.beta, a.seed);
 }
 
 ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t st)
@@ -184,11 +194,11 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
     if (smem > 48 * 1024) return set_error(CTR_ERR_UNSUPPORTED, "plane tables exceed 48 KB of shared memory");
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         if (a.sart) {
-            if (a.flags & CTR_SART_STOCHASTIC_ROUND) launch_bp_t<VT, true, true, true>(G, a, st);
-            else launch_bp_t<VT, true, true, false>(G, a, st);
+            if (a.flags & CTR_SART_STOCHASTIC_ROUND) launch_bp_t<VT, float2, true, true, true>(G, a, st);
+            else launch_bp_t<VT, float2, true, true, false>(G, a, st);
         } else {
-            if (a.flags & CTR_BP_FOV_MASK) launch_bp_t<VT, false, true, false>(G, a, st);
-            else launch_bp_t<VT, false, false, false>(G, a, st);
+            if (a.flags & CTR_BP_FOV_MASK) launch_bp_t<VT, float4, false, true, false>(G, a, st);
+            else launch_bp_t<VT, float4, false, false, false>(G, a, st);
         }
     });
     CTR_CUDA_TRY(cudaGetLastError());

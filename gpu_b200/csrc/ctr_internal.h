@@ -56,7 +56,7 @@ struct Geometry {
     float4* d_colt = nullptr;
     unsigned* d_err = nullptr;
     // workspace
-    float2* d_rays = nullptr;  size_t rays_cap = 0;     // ray records (value, chord length)
+    void* d_rays = nullptr;  size_t rays_cap = 0;       // ray records (float2 SART / float4 adjoint)
     double* d_partial = nullptr; size_t partial_cap = 0;
     double* d_result = nullptr;                        // 8 doubles
     void* d_fgp = nullptr; size_t fgp_bytes = 0;       // 9 dual arrays
@@ -86,7 +86,7 @@ inline size_t dtype_size(ctr_dtype t) { return t == CTR_F32 ? 4 : 2; }
 inline bool dtype_ok(int t) { return t == CTR_F32 || t == CTR_BF16 || t == CTR_F16; }
 
 // workspace helpers (geometry.cpp)
-ctr_status ensure_rays(Geometry* g, size_t n);
+ctr_status ensure_rays(Geometry* g, size_t bytes);
 ctr_status ensure_partial(Geometry* g, size_t n);
 ctr_status ensure_fgp(Geometry* g, size_t bytes);
 ctr_status check_device_errors(Geometry* g, cudaStream_t st);
@@ -106,7 +106,8 @@ ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, s
 
 struct BpArgs {
     void* vol; ctr_dtype vol_dtype;
-    const float2* rays;                   // [nview][ZP][R] (value, chord length)
+    const void* rays;                     // [nview][ZP][R]: float2 (c, d12) for SART,
+                                          // float4 (y, d12, alpha_lo, alpha_hi) for the adjoint
     int view0, nview;
     int sart;                             // 1: SART update; 0: adjoint
     unsigned flags;                       // CTR_BP_* / CTR_SART_*
@@ -114,7 +115,7 @@ struct BpArgs {
     uint32_t seed;
 };
 ctr_status launch_backproject(const Geometry& g, const BpArgs& a, cudaStream_t st);
-ctr_status launch_ray_prep(const Geometry& g, const float* y, int view0, int nview, float2* rays,
+ctr_status launch_ray_prep(const Geometry& g, const float* y, int view0, int nview, float4* rays,
                            cudaStream_t st);
 
 ctr_status launch_reduce(const double* partial, size_t n, double* out, cudaStream_t st);

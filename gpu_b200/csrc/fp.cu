@@ -24,6 +24,7 @@ static constexpr uint64_t kFnvPrime = 1099511628211ULL;
 
 struct RayResult {
     float sum, len, d12;
+    float a_lo, a_hi;   // alpha interval the traversal covered (empty when it dropped the ray)
     int nseg;
     uint64_t hash;
 };
@@ -35,7 +36,9 @@ __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, 
     return floorf(fm(fs(fa(fm(a, d), x1), b), inv_v));
 }
 
-template <typename VT, bool E64, bool TRACE>
+// LOAD=false walks the rays without reading the volume: it yields the chord
+// lengths' support (a_lo, a_hi) for the matched adjoint.
+template <typename VT, bool E64, bool TRACE, bool LOAD = true>
 __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
                                             const float* __restrict__ PY, const float* __restrict__ PZ,
                                             const VT* __restrict__ vol, float s, float c, int u, int v)
@@ -43,6 +46,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     const int M = g.M, N = g.N, Z = g.Z;
     RayResult r;
     r.sum = 0.f; r.len = 0.f; r.nseg = 0; r.hash = kFnvOffset;
+    r.a_lo = 1.0f; r.a_hi = 0.0f;
 
     // source X2 and detector pixel centre X1 (universal.cu:24-45)
     const float x2x = fs(fm(g.srcx, c), fm(g.srcy, s));
@@ -171,6 +175,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     const float d12 = r.d12;
     float ac = amin, sum = 0.f, len = 0.f;
     int steps = 0;
+    bool any = false;
     // :297-551
     while (fs(amax, ac) > 1e-16f) {
         if ((unsigned)vi >= (unsigned)M || (unsigned)vj >= (unsigned)N || (unsigned)vk >= (unsigned)Z) break;
@@ -180,9 +185,12 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
         }
         const float m = fminf(fminf(ax, ay), az);
         const float seg = fm(d12, fs(m, ac));
-        const float f = Store<VT>::ld(vol + idx);
         len = fa(len, seg);
-        sum = fa(sum, fm(seg, f));
+        if (LOAD) {
+            const float f = Store<VT>::ld(vol + idx);
+            sum = fa(sum, fm(seg, f));
+        }
+        any = true;
         if (TRACE) {
             r.nseg++;
             r.hash = (r.hash ^ (uint64_t)(uint32_t)idx) * kFnvPrime;
@@ -194,6 +202,10 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     }
     r.sum = sum;
     r.len = len;
+    if (any) {
+        r.a_lo = amin;
+        r.a_hi = ac;
+    }
     return r;
 }
 
@@ -280,33 +292,40 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
     return CTR_OK;
 }
 
-// Ray records (value, chord length) for the adjoint: the chord length is the
-// forward projector's own d12 (:290) for every ray of views [view0, view0+nview).
-__global__ void k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, float2* __restrict__ rays)
+// Ray records for the matched adjoint: (value, chord length d12 (:290), and
+// the alpha interval the forward traversal covers).  The interval is what
+// keeps the gather backprojector the exact adjoint where the reference
+// traversal drops or stops a ray at a volume edge.
+template <bool E64>
+__global__ void __launch_bounds__(FP_THREADS)
+k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, float4* __restrict__ rays)
 {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int v = blockIdx.y;
+    extern __shared__ float sp[];
+    float* PX = sp;
+    float* PY = PX + (g.M + 3);
+    float* PZ = PY + (g.N + 3);
+    for (int t = threadIdx.x; t < g.M + 3; t += FP_THREADS) PX[t] = g.px[t];
+    for (int t = threadIdx.x; t < g.N + 3; t += FP_THREADS) PY[t] = g.py[t];
+    for (int t = threadIdx.x; t < g.Z + 3; t += FP_THREADS) PZ[t] = g.pz[t];
+    __syncthreads();
+    const int u = blockIdx.x * FP_BX + (threadIdx.x % FP_BX);
+    const int v = blockIdx.y * FP_BY + (threadIdx.x / FP_BX);
     const int w = blockIdx.z;
-    if (u >= g.R) return;
+    if (u >= g.R || v >= g.ZP) return;
     const float2 sc = g.trig[view0 + w];
-    const float s = sc.x, c = sc.y;
-    const float x2x = fs(fm(g.srcx, c), fm(g.srcy, s));
-    const float x2y = fa(fm(g.srcx, s), fm(g.srcy, c));
-    const float pu = fa(g.ymin, fm((float)u, g.du));
-    const float x1x = fs(fm(g.dod, c), fm(pu, s));
-    const float x1y = fa(fm(g.dod, s), fm(pu, c));
-    const float x1z = fa(g.zmin, fm((float)v, g.dv));
-    const float dx = fs(x2x, x1x), dy = fs(x2y, x1y), dz = fs(g.srcz, x1z);
-    const float d12 = __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));
+    const RayResult rr = siddon<float, E64, false, false>(g, PX, PY, PZ, nullptr, sc.x, sc.y, u, v);
     const long long p = ((long long)w * g.ZP + v) * g.R + u;
-    rays[p] = make_float2(y[p], d12);
+    rays[p] = make_float4(y[p], rr.d12, rr.a_lo, rr.a_hi);
 }
 
-ctr_status launch_ray_prep(const Geometry& G, const float* y, int view0, int nview, float2* rays, cudaStream_t st)
+ctr_status launch_ray_prep(const Geometry& G, const float* y, int view0, int nview, float4* rays, cudaStream_t st)
 {
+    const DevGeom& g = G.dg;
     if (nview <= 0) return CTR_OK;
-    dim3 grid((G.dg.R + 127) / 128, G.dg.ZP, nview);
-    k_ray_prep<<<grid, 128, 0, st>>>(G.dg, y, view0, rays);
+    dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + FP_BY - 1) / FP_BY, nview);
+    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 9);
+    if (g.entry64) k_ray_prep<true><<<grid, FP_THREADS, smem, st>>>(g, y, view0, rays);
+    else k_ray_prep<false><<<grid, FP_THREADS, smem, st>>>(g, y, view0, rays);
     CTR_CUDA_TRY(cudaGetLastError());
     return CTR_OK;
 }

@@ -58,14 +58,14 @@ static int parallel_voxel(float x1, float b, float inv_v)
 
 static float plane(float v, int n, float b) { return v * (float)n + b; }
 
-ctr_status ensure_rays(Geometry* g, size_t n)
+ctr_status ensure_rays(Geometry* g, size_t bytes)
 {
-    if (n <= g->rays_cap) return CTR_OK;
+    if (bytes <= g->rays_cap) return CTR_OK;
     if (g->d_rays) cudaFree(g->d_rays);
     g->d_rays = nullptr;
     g->rays_cap = 0;
-    CTR_CUDA_TRY(cudaMalloc(&g->d_rays, n * sizeof(float2)));
-    g->rays_cap = n;
+    CTR_CUDA_TRY(cudaMalloc(&g->d_rays, bytes));
+    g->rays_cap = bytes;
     return CTR_OK;
 }
 

@@ -1016,3 +1016,140 @@ void og_phantom_project(const og_geom* g, const double* par, int n, double s, do
             out[(long long)v * R + u] = (float)acc;
         }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Gather SART backprojection with the projector's own alphas: the engine's  */
+/* SART update (reference BP semantics: MBR candidates, FOV mask, thresholds */
+/* of V63/kernel_IterativeRecon_universal.cu:626-807) with every alpha       */
+/* evaluated as the Siddon projector evaluates it.  Accumulates in float in  */
+/* the engine's pair order (detector column, then row).                      */
+/* ------------------------------------------------------------------------ */
+static void og_column_eff(const og_geom* g, float s, float c, int u, float* x1x_e, float* ix_e, float* x1y_e,
+                          float* iy_e)
+{
+    const float x2x = g->srcx * c - g->srcy * s, x2y = g->srcx * s + g->srcy * c;
+    const float pu = g->ymin + (float)u * g->d.du;
+    const float x1x = g->d.dod * c - pu * s, x1y = g->d.dod * s + pu * c;
+    if (fabsf(x1x - x2x) < g->d.vx * 1e-6f) {
+        const int iv = (int)floorf((x1x - g->bx) * g->inv_vx);
+        *x1x_e = og_plane(g->d.vx, iv, g->bx) + 0.5f * g->d.vx;
+        *ix_e = INFINITY;
+    } else {
+        *x1x_e = x1x;
+        *ix_e = 1.0f / (x2x - x1x);
+    }
+    if (fabsf(x1y - x2y) < g->d.vy * 1e-6f) {
+        const int jv = (int)floorf((x1y - g->by) * g->inv_vy);
+        *x1y_e = og_plane(g->d.vy, jv, g->by) + 0.5f * g->d.vy;
+        *iy_e = INFINITY;
+    } else {
+        *x1y_e = x1y;
+        *iy_e = 1.0f / (x2y - x1y);
+    }
+}
+
+static void og_row_eff(const og_geom* g, int v, float* x1z_e, float* iz_e)
+{
+    const float x1z = g->zmin + (float)v * g->d.dv, x2z = g->srcz;
+    if (fabsf(x1z - x2z) < g->d.vz * 1e-6f) {
+        const int kv = (int)floorf((x1z - g->bz) * g->inv_vz);
+        *x1z_e = og_plane(g->d.vz, kv, g->bz) + 0.5f * g->d.vz;
+        *iz_e = INFINITY;
+    } else {
+        *x1z_e = x1z;
+        *iz_e = 1.0f / (x2z - x1z);
+    }
+}
+
+static float og_ray_d12(const og_geom* g, float s, float c, int u, int v)
+{
+    const float x2x = g->srcx * c - g->srcy * s, x2y = g->srcx * s + g->srcy * c, x2z = g->srcz;
+    const float pu = g->ymin + (float)u * g->d.du;
+    const float x1x = g->d.dod * c - pu * s, x1y = g->d.dod * s + pu * c, x1z = g->zmin + (float)v * g->d.dv;
+    return sqrtf((x2x - x1x) * (x2x - x1x) + (x2y - x1y) * (x2y - x1y) + (x2z - x1z) * (x2z - x1z));
+}
+
+void og_backproject_gather(const og_geom* g, float* vol, const float* corr, float beta, float s, float c)
+{
+    const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->d.nv;
+    const float vx = g->d.vx, vy = g->d.vy, vz = g->d.vz;
+    const float DSO = g->d.dso, DOD = g->d.dod;
+    const float inv_du = 1.0f / g->d.du, inv_dv = 1.0f / g->d.dv;
+    float* col = (float*)malloc(sizeof(float) * 4 * R);
+    float* row = (float*)malloc(sizeof(float) * 2 * ZP);
+    float* d12 = (float*)malloc(sizeof(float) * R * ZP);
+    for (int u = 0; u < R; ++u) og_column_eff(g, s, c, u, &col[4 * u], &col[4 * u + 1], &col[4 * u + 2], &col[4 * u + 3]);
+    for (int v = 0; v < ZP; ++v) og_row_eff(g, v, &row[2 * v], &row[2 * v + 1]);
+    for (int v = 0; v < ZP; ++v)
+        for (int u = 0; u < R; ++u) d12[v * R + u] = og_ray_d12(g, s, c, u, v);
+    const float thr = vx * 1e-6f;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Z; ++k)
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < M; ++i) {
+                if (og_fov_masked(g, i, j)) continue;
+                const float cx = g->bx + vx * 0.5f + (float)i * vx;
+                const float cy = g->by + vy * 0.5f + (float)j * vy;
+                const float cz = g->bz + vz * 0.5f + (float)k * vz;
+                /* candidate rectangle of the reference BP (:639-706) */
+                float minY = INFINITY, minZ = INFINITY, maxY = -INFINITY, maxZ = -INFINITY;
+                for (int kk = 0; kk < 2; ++kk)
+                    for (int jj = 0; jj < 2; ++jj)
+                        for (int ii = 0; ii < 2; ++ii) {
+                            const float px = cx + (float)ii * vx - 0.5f * vx;
+                            const float py = cy + (float)jj * vy - 0.5f * vy;
+                            const float pz = cz + (float)kk * vz - 0.5f * vz;
+                            const float t = px * c + py * s, ss = -px * s + py * c;
+                            const float ou = (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
+                            const float oz = (t - DOD) / (DSO - t) * (pz - g->srcz) + pz;
+                            minY = fminf(minY, ou); maxY = fmaxf(maxY, ou);
+                            minZ = fminf(minZ, oz); maxZ = fmaxf(maxZ, oz);
+                        }
+                int u0 = (int)floorf((minY - g->ymin) * inv_du + 0.5f), u1 = (int)floorf((maxY - g->ymin) * inv_du + 0.5f);
+                int v0 = (int)floorf((minZ - g->zmin) * inv_dv + 0.5f), v1 = (int)floorf((maxZ - g->zmin) * inv_dv + 0.5f);
+                if ((u0 < 0 && u1 < 0) || (u0 > R - 1 && u1 > R - 1) || (v0 < 0 && v1 < 0) || (v0 > ZP - 1 && v1 > ZP - 1))
+                    continue;
+                /* widen by one row each side: the engine's row range is any superset */
+                v0 = v0 - 1 < 0 ? 0 : v0 - 1;
+                v1 = v1 + 1 > ZP - 1 ? ZP - 1 : v1 + 1;
+                u0 = u0 < 0 ? 0 : u0;
+                u1 = u1 > R - 1 ? R - 1 : u1;
+                const float xlo = og_plane(vx, i, g->bx), xhi = og_plane(vx, i + 1, g->bx);
+                const float ylo = og_plane(vy, j, g->by), yhi = og_plane(vy, j + 1, g->by);
+                const float zlo = og_plane(vz, k, g->bz), zhi = og_plane(vz, k + 1, g->bz);
+                float sw = 0.0f, sl = 0.0f;
+                for (int u = u0; u <= u1; ++u) {
+                    const float* ct = &col[4 * u];
+                    const float ax0 = (xlo - ct[0]) * ct[1], ax1 = (xhi - ct[0]) * ct[1];
+                    const float ay0 = (ylo - ct[2]) * ct[3], ay1 = (yhi - ct[2]) * ct[3];
+                    const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
+                    const float b = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+                    if (!(b > a)) continue;
+                    for (int v = v0; v <= v1; ++v) {
+                        const float az0 = (zlo - row[2 * v]) * row[2 * v + 1], az1 = (zhi - row[2 * v]) * row[2 * v + 1];
+                        const float lo = fmaxf(a, fminf(az0, az1)), hi = fminf(b, fmaxf(az0, az1));
+                        const float temp = d12[v * R + u] * (hi - lo);
+                        if (temp > thr) {
+                            sw = sw + temp * corr[v * R + u];
+                            sl = sl + temp;
+                        }
+                    }
+                }
+                const long long idx = (long long)M * N * k + (long long)M * j + i;
+                if (!(sl < thr)) vol[idx] = vol[idx] + beta * sw / sl;
+            }
+    free(col); free(row); free(d12);
+}
+
+void og_sart_pass_gather(const og_geom* g, float* vol, const float* sino, float beta)
+{
+    const long long P = (long long)g->d.nu * g->d.nv;
+    float* corr = (float*)malloc(sizeof(float) * P);
+    for (int j = 0; j < g->d.nviews; ++j) {
+        float s, c;
+        og_view_trig(g, j, 0, &s, &c);
+        og_forward_view(g, vol, s, c, 1, sino + P * j, corr, 0);
+        og_backproject_gather(g, vol, corr, beta, s, c);
+    }
+    free(corr);
+}

@@ -89,6 +89,11 @@ void og_sart_pass_ref(const og_geom* g, float* vol, const float* sino, float bet
 /* engine semantics: the BP uses the FP's own chord lengths (matched adjoint) */
 void og_sart_pass_matched(const og_geom* g, float* vol, const float* sino, float beta);
 void og_sart_pass_f64(const og_geom* g, double* vol, const double* sino, double beta);
+/* the engine's gather SART update: reference BP semantics (candidate
+ * rectangle, FOV mask, thresholds) with every alpha evaluated the Siddon
+ * projector's way, float sums in the engine's pair order */
+void og_backproject_gather(const og_geom* g, float* vol, const float* corr, float beta, float s, float c);
+void og_sart_pass_gather(const og_geom* g, float* vol, const float* sino, float beta);
 
 /* ---- FGP TV prox, 7-array GPU form (V63/kernel_FGP_Denoise_GPUx7.cu:2-88,
  *      driver V63/host_FGP_Denoise_GPUx7.c:1-111) ---- */

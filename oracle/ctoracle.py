@@ -90,6 +90,8 @@ class Oracle:
             "og_sart_pass_ref": [G, _f32p, _f32p, f],
             "og_sart_pass_matched": [G, _f32p, _f32p, f],
             "og_sart_pass_f64": [G, _f64p, _f64p, d],
+            "og_backproject_gather": [G, _f32p, _f32p, f, f, f],
+            "og_sart_pass_gather": [G, _f32p, _f32p, f],
             "og_fgp": [i, i, i, _f32p, f, i, _f32p],
             "og_fgp_f64": [i, i, i, _f64p, d, i, _f64p],
             "og_tv_norm": [i, i, i, _f32p],
@@ -199,6 +201,17 @@ class Oracle:
     def sart_pass_matched(self, vol, sino, beta):
         vol = np.ascontiguousarray(vol, np.float32).copy()
         self.lib.og_sart_pass_matched(self.gp, vol, np.ascontiguousarray(sino, np.float32), beta)
+        return vol
+
+    def backproject_gather(self, vol, corr, view, beta):
+        s, c = self.trig(view)
+        vol = np.ascontiguousarray(vol, np.float32).copy()
+        self.lib.og_backproject_gather(self.gp, vol, np.ascontiguousarray(corr, np.float32), beta, s, c)
+        return vol
+
+    def sart_pass_gather(self, vol, sino, beta):
+        vol = np.ascontiguousarray(vol, np.float32).copy()
+        self.lib.og_sart_pass_gather(self.gp, vol, np.ascontiguousarray(sino, np.float32), beta)
         return vol
 
     def sart_pass_f64(self, vol, sino, beta):
