@@ -38,7 +38,7 @@ ctr_status need_dtype(int dt, const char* what)
 // views per adjoint pass: bounded so the ray records stay under ~256 MB
 int adjoint_batch(const Geometry* g)
 {
-    long long b = (256LL << 20) / (16LL * g->npix());
+    long long b = (256LL << 20) / ((long long)sizeof(AdjRay) * g->npix());
     if (b < 1) b = 1;
     if (b > 32) b = 32;
     return (int)b;
@@ -154,10 +154,10 @@ extern "C" ctr_status ctr_backproject(const ctr_geometry* geom, const float* sin
         if (!(flags & CTR_BP_ACCUMULATE)) CTR_CUDA_TRY(cudaMemsetAsync(vol, 0, g->nvox() * dtype_size(vdt), st));
         return CTR_OK;
     }
-    CTR_TRY(ensure_rays(g, (size_t)P * batch * sizeof(float4)));
+    CTR_TRY(ensure_rays(g, (size_t)P * batch * sizeof(AdjRay)));
     for (int c = 0; c < n; c += batch) {
         const int cnt = std::min(batch, n - c);
-        CTR_TRY(launch_ray_prep(*g, sino + (size_t)c * P, v0 + c, cnt, (float4*)g->d_rays, st));
+        CTR_TRY(launch_ray_prep(*g, sino + (size_t)c * P, v0 + c, cnt, (AdjRay*)g->d_rays, st));
         BpArgs b{};
         b.vol = vol; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = v0 + c; b.nview = cnt; b.sart = 0;
         b.flags = (flags & CTR_BP_FOV_MASK) | ((c > 0 || (flags & CTR_BP_ACCUMULATE)) ? CTR_BP_ACCUMULATE : 0u);

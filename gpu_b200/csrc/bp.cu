@@ -1,22 +1,33 @@
-// bp.cu -- voxel-driven gather backprojector (matched adjoint and SART update).
+// bp.cu -- voxel-driven gather backprojectors (SART update, matched adjoint).
 //
-// Restates backprj_ray_driven_3d_kernel (V63/kernel_IterativeRecon_universal.cu:
-// 571-810): for each voxel, every detector pixel in the bounding rectangle of
-// its corner projections is a candidate ray, and the ray's chord through the
-// voxel is d12 * (min of exit alphas - max of entry alphas).
+// Both restate backprj_ray_driven_3d_kernel (V63/kernel_IterativeRecon_
+// universal.cu:571-810): for each voxel, every detector pixel in the bounding
+// rectangle of its corner projections is a candidate ray, and the ray's chord
+// through the voxel is d12 * (min of exit alphas - max of entry alphas).
 //
 // Where the reference recomputes each alpha as ((c +- v/2) - x1)/(x2 - x1),
-// this kernel evaluates the alphas exactly as the forward projector does,
+// these kernels evaluate the alphas exactly as the forward projector does,
 // (plane_n - x1) * (1/(x2 - x1)) with the projector's own x1, 1/(x2-x1) and
-// d12, so every (voxel, ray) chord equals the projector's Siddon segment
-// bit for bit and the adjoint is matched.  Two further changes:
-//   * the alphas of a ray split into an xy part, fixed by the detector column
-//     (x1x, x1y, 1/dx, 1/dy do not depend on the row), and a z part fixed by
-//     the row.  A thread owns K voxels of one z column: the column's
-//     detector-column range and its xy entry/exit interval per column are
-//     computed once and reused for all K voxels;
-//   * the adjoint accumulates several views per pass in registers, so the
-//     volume is read and written once per batch.
+// d12, so every (voxel, ray) chord is the projector's Siddon segment bit for
+// bit.  Organisation:
+//   * the alphas of a ray split into an xy part fixed by the detector column
+//     (x1x, x1y, 1/dx, 1/dy do not depend on the row) and a z part fixed by
+//     the row.  A thread owns BP_K voxels of one z column: the column's
+//     detector-column range and the xy entry/exit alphas per detector column
+//     are computed once and reused for all of them;
+//   * writes are coalesced: the 32 lanes of a warp own 32 consecutive x.
+//
+// k_backproject: the SART update (command 1) and the reference's command 0,
+// with the reference BP's geometric chords, FOV mask and thresholds.
+// k_adjoint: the exact adjoint of the forward projector.  Each ray record
+// carries the alpha interval, start voxel and parallel axes of the forward
+// traversal, and the chord of a voxel is taken over the traversal's own cell
+// intervals: the start cell opens at -inf, cells behind the start are never
+// visited, a parallel axis keeps its start cell.  That is what the reference
+// traversal does where its floor-based start index differs from the geometry
+// (rays through volume edges, nearly axis-parallel rays).  Several views are
+// accumulated per pass in FP64 registers (a float*float product is exact in
+// FP64), so the volume is read and written once per batch.
 #include "ctr_device.cuh"
 
 namespace ctr {
@@ -26,101 +37,114 @@ static constexpr int BP_BY = 4;    // voxel rows along y per block
 static constexpr int BP_THREADS = BP_BX * BP_BY;
 static constexpr int BP_K = 4;     // z voxels per thread
 
-// Ray records: REC = float2 (c, d12) for the SART update and the reference's
-// command-0 backprojection, whose chords are purely geometric like the
-// reference BP's; REC = float4 (y, d12, alpha_lo, alpha_hi) for the matched
-// adjoint, whose chords are clipped to the interval the forward traversal
-// covered (empty where the reference traversal drops a ray at a volume edge).
-template <typename VT, typename REC, bool SART, bool MASK, bool STOCH>
-__global__ void __launch_bounds__(BP_THREADS)
-k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ rays, int view0, int nview,
-              int accumulate, float beta, uint32_t seed)
-{
-    constexpr bool WINDOW = sizeof(REC) == sizeof(float4) && !SART && !MASK;
-    extern __shared__ float sp[];
-    float* PX = sp;
-    float* PY = PX + (g.M + 3);
-    float* PZ = PY + (g.N + 3);
-    float2* RT = reinterpret_cast<float2*>(PZ + ((g.Z + 3 + 1) & ~1));
-    for (int t = threadIdx.x; t < g.M + 3; t += BP_THREADS) PX[t] = g.px[t];
-    for (int t = threadIdx.x; t < g.N + 3; t += BP_THREADS) PY[t] = g.py[t];
-    for (int t = threadIdx.x; t < g.Z + 3; t += BP_THREADS) PZ[t] = g.pz[t];
-    for (int t = threadIdx.x; t < g.ZP; t += BP_THREADS) RT[t] = g.rowt[t];
-    __syncthreads();
+struct SharedTables {
+    float* PX;
+    float* PY;
+    float* PZ;
+    float2* RT;
+};
 
+__device__ __forceinline__ SharedTables load_tables(const DevGeom& g, float* sp)
+{
+    SharedTables t;
+    t.PX = sp;
+    t.PY = t.PX + (g.M + 3);
+    t.PZ = t.PY + (g.N + 3);
+    t.RT = reinterpret_cast<float2*>(t.PZ + ((g.Z + 3 + 1) & ~1));
+    for (int q = threadIdx.x; q < g.M + 3; q += BP_THREADS) t.PX[q] = g.px[q];
+    for (int q = threadIdx.x; q < g.N + 3; q += BP_THREADS) t.PY[q] = g.py[q];
+    for (int q = threadIdx.x; q < g.Z + 3; q += BP_THREADS) t.PZ[q] = g.pz[q];
+    for (int q = threadIdx.x; q < g.ZP; q += BP_THREADS) t.RT[q] = g.rowt[q];
+    __syncthreads();
+    return t;
+}
+
+// Candidate detector columns of voxel column (i, j) and candidate rows of
+// its BP_K voxels: the reference's bounding rectangle of the corner
+// projections (universal.cu:639-706).  u depends on the corner's x, y only;
+// the z projection scales by 1 + (t-DOD)/(DSO-t), bounded by its extremes
+// over the 4 xy corners.  Returns false when the column misses the detector.
+__device__ __forceinline__ bool candidate_rect(const DevGeom& g, const SharedTables& T, float cx, float cy, int k0,
+                                               float s, float c, int& ulo, int& uhi, int* vlo, int* vhi)
+{
+    float umin = __int_as_float(0x7f800000), umax = -umin, mlo = umin, mhi = -umin;
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {
+        const float pxc = fs(fa(cx, fm((float)(cc & 1), g.vx)), fm(0.5f, g.vx));
+        const float pyc = fs(fa(cy, fm((float)(cc >> 1), g.vy)), fm(0.5f, g.vy));
+        const float t = fa(fm(pxc, c), fm(pyc, s));
+        const float ss = fa(fm(-pxc, s), fm(pyc, c));
+        const float mt = fdv(fs(t, g.dod), fs(g.dso, t));
+        const float ou = fa(fm(mt, fs(ss, g.srcy)), ss);
+        umin = fminf(umin, ou); umax = fmaxf(umax, ou);
+        mlo = fminf(mlo, mt); mhi = fmaxf(mhi, mt);
+    }
+    ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
+    uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
+    if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) return false;
+    ulo = max(ulo, 0);
+    uhi = min(uhi, g.R - 1);
+#pragma unroll
+    for (int kk = 0; kk < BP_K; ++kk) {
+        const int k = k0 + kk;
+        vlo[kk] = 1; vhi[kk] = 0;
+        if (k < g.Z) {
+            const float z0 = T.PZ[k + 1], z1 = T.PZ[k + 2];
+            const float zlo = fs(z0, g.srcz), zhi = fs(z1, g.srcz);
+            const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
+            const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
+            const float zmn = fminf(fminf(a0, a1), fminf(b0, b1));
+            const float zmx = fmaxf(fmaxf(a0, a1), fmaxf(b0, b1));
+            const int lo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
+            const int hi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
+            if (!((lo < 0 && hi < 0) || (lo > g.ZP - 1 && hi > g.ZP - 1))) {
+                vlo[kk] = max(lo, 0);
+                vhi[kk] = min(hi, g.ZP - 1);
+            }
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ float rec_value(const float2& r) { return r.x; }
+__device__ __forceinline__ float rec_d12(const float2& r) { return r.y; }
+__device__ __forceinline__ float rec_value(const AdjRay& r) { return r.f.x; }
+__device__ __forceinline__ float rec_d12(const AdjRay& r) { return r.f.y; }
+
+// SART update (SART=true) or the reference's command 0 (SART=false).
+template <typename VT, typename REC, bool SART, bool STOCH>
+__global__ void __launch_bounds__(BP_THREADS)
+k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ rays, int view0, int accumulate,
+              float beta, uint32_t seed)
+{
+    extern __shared__ float sp[];
+    const SharedTables T = load_tables(g, sp);
     const int i = blockIdx.x * BP_BX + (threadIdx.x % BP_BX);
     const int j = blockIdx.y * BP_BY + (threadIdx.x / BP_BX);
     const int k0 = blockIdx.z * BP_K;
     if (i >= g.M || j >= g.N) return;
-    const int R = g.R, ZP = g.ZP;
+    const int R = g.R;
 
     // FOV cylinder (universal.cu:626-628)
-    bool masked = false;
-    if (MASK) {
-        const float ex = fs(fs((float)i, g.fov_h_x), g.m_off);
-        const float ey = fs((float)j, g.fov_h_y);
-        masked = fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2;
-    }
+    const float ex = fs(fs((float)i, g.fov_h_x), g.m_off);
+    const float ey = fs((float)j, g.fov_h_y);
+    const bool masked = fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2;
 
     float sw[BP_K], sl[BP_K];
 #pragma unroll
     for (int kk = 0; kk < BP_K; ++kk) { sw[kk] = 0.f; sl[kk] = 0.f; }
 
     if (!masked) {
-        // voxel centre (universal.cu:592-594) and its bounding planes
-        const float cx = fa(fa(g.bx, fm(g.vx, 0.5f)), fm((float)i, g.vx));
+        const float cx = fa(fa(g.bx, fm(g.vx, 0.5f)), fm((float)i, g.vx));   // :592-594
         const float cy = fa(fa(g.by, fm(g.vy, 0.5f)), fm((float)j, g.vy));
-        const float xlo = PX[i + 1], xhi = PX[i + 2];
-        const float ylo = PY[j + 1], yhi = PY[j + 2];
-        for (int w = 0; w < nview; ++w) {
-            const int view = view0 + w;
-            const float2 sc = g.trig[view];
-            const float s = sc.x, c = sc.y;
-            // corner projections onto the detector (universal.cu:639-683):
-            // u depends on the corner's x,y only; the z projection scales by
-            // 1 + (t-DOD)/(DSO-t), bounded by its extremes over the 4 corners.
-            float umin = __int_as_float(0x7f800000), umax = -umin, mlo = umin, mhi = -umin;
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                const float pxc = fs(fa(cx, fm((float)(cc & 1), g.vx)), fm(0.5f, g.vx));
-                const float pyc = fs(fa(cy, fm((float)(cc >> 1), g.vy)), fm(0.5f, g.vy));
-                const float t = fa(fm(pxc, c), fm(pyc, s));
-                const float ss = fa(fm(-pxc, s), fm(pyc, c));
-                const float mt = fdv(fs(t, g.dod), fs(g.dso, t));
-                const float ou = fa(fm(mt, fs(ss, g.srcy)), ss);
-                umin = fminf(umin, ou); umax = fmaxf(umax, ou);
-                mlo = fminf(mlo, mt); mhi = fmaxf(mhi, mt);
-            }
-            int ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
-            int uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
-            if ((ulo < 0 && uhi < 0) || (ulo > R - 1 && uhi > R - 1)) continue;
-            ulo = max(ulo, 0);
-            uhi = min(uhi, R - 1);
-            // detector-row range of each of the K voxels
-            int vlo[BP_K], vhi[BP_K];
-#pragma unroll
-            for (int kk = 0; kk < BP_K; ++kk) {
-                const int k = k0 + kk;
-                vlo[kk] = 1; vhi[kk] = 0;
-                if (k < g.Z) {
-                    const float zlo = fs(PZ[k + 1], g.srcz), zhi = fs(PZ[k + 2], g.srcz);
-                    const float a0 = fa(fm(mlo, zlo), PZ[k + 1]), a1 = fa(fm(mhi, zlo), PZ[k + 1]);
-                    const float b0 = fa(fm(mlo, zhi), PZ[k + 2]), b1 = fa(fm(mhi, zhi), PZ[k + 2]);
-                    const float zmn = fminf(fminf(a0, a1), fminf(b0, b1));
-                    const float zmx = fmaxf(fmaxf(a0, a1), fmaxf(b0, b1));
-                    int lo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
-                    int hi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
-                    if (!((lo < 0 && hi < 0) || (lo > ZP - 1 && hi > ZP - 1))) {
-                        vlo[kk] = max(lo, 0);
-                        vhi[kk] = min(hi, ZP - 1);
-                    }
-                }
-            }
-            const float4* __restrict__ colt = g.colt + (long long)view * R;
-            const REC* __restrict__ rw = rays + (long long)w * R * ZP;
+        const float xlo = T.PX[i + 1], xhi = T.PX[i + 2];
+        const float ylo = T.PY[j + 1], yhi = T.PY[j + 2];
+        const float2 sc = g.trig[view0];
+        int ulo, uhi, vlo[BP_K], vhi[BP_K];
+        if (candidate_rect(g, T, cx, cy, k0, sc.x, sc.y, ulo, uhi, vlo, vhi)) {
+            const float4* __restrict__ colt = g.colt + (long long)view0 * R;
             for (int uu = ulo; uu <= uhi; ++uu) {
                 const float4 ct = __ldg(colt + uu);
-                // xy entry/exit of this ray column through the voxel column
                 const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
                 const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
                 const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
@@ -129,25 +153,17 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
 #pragma unroll
                 for (int kk = 0; kk < BP_K; ++kk) {
                     const int kc = min(k0 + kk, g.Z - 1);
-                    const float zl = PZ[kc + 1], zh = PZ[kc + 2];
+                    const float zl = T.PZ[kc + 1], zh = T.PZ[kc + 2];
                     for (int vv = vlo[kk]; vv <= vhi[kk]; ++vv) {
-                        const float2 rt = RT[vv];
+                        const float2 rt = T.RT[vv];
                         const float az0 = fm(fs(zl, rt.x), rt.y), az1 = fm(fs(zh, rt.x), rt.y);
-                        float lo = fmaxf(a, fminf(az0, az1));
-                        float hi = fminf(bb, fmaxf(az0, az1));
-                        const REC rec = __ldg(rw + (long long)vv * R + uu);
-                        if constexpr (WINDOW) {
-                            lo = fmaxf(lo, rec.z);
-                            hi = fminf(hi, rec.w);
-                        }
-                        const float temp = fm(rec.y, fs(hi, lo));
-                        if (SART || MASK) {
-                            if (temp > g.thr_bp) {                        // :785-791
-                                sw[kk] = fa(sw[kk], fm(temp, rec.x));
-                                sl[kk] = fa(sl[kk], temp);
-                            }
-                        } else if (temp > 0.0f) {
-                            sw[kk] = __fmaf_rn(temp, rec.x, sw[kk]);
+                        const float lo = fmaxf(a, fminf(az0, az1));
+                        const float hi = fminf(bb, fmaxf(az0, az1));
+                        const REC rec = rays[(long long)vv * R + uu];
+                        const float temp = fm(rec_d12(rec), fs(hi, lo));
+                        if (temp > g.thr_bp) {                                 // :785-791
+                            sw[kk] = fa(sw[kk], fm(temp, rec_value(rec)));
+                            sl[kk] = fa(sl[kk], temp);
                         }
                     }
                 }
@@ -162,43 +178,132 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
         if (k >= g.Z) break;
         VT* p = vol + (long long)k * MN + (long long)j * g.M + i;
         if (SART) {
-            if (!(sl[kk] < g.thr_bp)) {                                  // :799-806
+            if (!(sl[kk] < g.thr_bp)) {                                         // :799-806
                 const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, sw[kk]), sl[kk]));
                 if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
                 else Store<VT>::st(p, nv);
             }
-        } else if (MASK) {
-            // reference command 0: assignment where the summed length passes
+        } else {
+            // command 0: assignment where the summed length passes
             if (!(sl[kk] < g.thr_bp)) Store<VT>::st(p, accumulate ? fa(Store<VT>::ldw(p), sw[kk]) : sw[kk]);
             else if (!accumulate) Store<VT>::st(p, 0.0f);
-        } else {
-            Store<VT>::st(p, accumulate ? fa(Store<VT>::ldw(p), sw[kk]) : sw[kk]);
         }
     }
 }
 
-template <typename VT, typename REC, bool SART, bool MASK, bool STOCH>
-static void launch_bp_t(const Geometry& G, const BpArgs& a, cudaStream_t st)
+// Interval of cell n along one axis under the forward traversal: geometric
+// [min(a0,a1), max(a0,a1)], opened at -inf for the start cell, empty behind
+// the start; for a parallel axis (-inf, +inf) at the start cell only.
+__device__ __forceinline__ bool traversal_cell(int n, int n0, bool par, float a0, float a1, float dirsign,
+                                               float& lo, float& hi)
 {
-    const DevGeom& g = G.dg;
-    dim3 grid((g.M + BP_BX - 1) / BP_BX, (g.N + BP_BY - 1) / BP_BY, (g.Z + BP_K - 1) / BP_K);
-    const size_t smem = sizeof(float) * (size_t)(g.M + 3 + g.N + 3 + ((g.Z + 3 + 1) & ~1)) + sizeof(float2) * g.ZP;
-    k_backproject<VT, REC, SART, MASK, STOCH><<<grid, BP_THREADS, smem, st>>>(
-        g, (VT*)a.vol, (const REC*)a.rays, a.view0, a.nview, (a.flags & CTR_BP_ACCUMULATE) ? 1 : 0, a.beta, a.seed);
+    const float INF = __int_as_float(0x7f800000);
+    if (par) {
+        lo = -INF;
+        hi = INF;
+        return n == n0;
+    }
+    const int d = n - n0;
+    if ((dirsign > 0.f && d < 0) || (dirsign < 0.f && d > 0)) return false;
+    lo = d == 0 ? -INF : fminf(a0, a1);
+    hi = fmaxf(a0, a1);
+    return true;
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(BP_THREADS)
+k_adjoint(const DevGeom g, VT* __restrict__ vol, const AdjRay* __restrict__ rays, int view0, int nview,
+          int accumulate)
+{
+    extern __shared__ float sp[];
+    const SharedTables T = load_tables(g, sp);
+    const int i = blockIdx.x * BP_BX + (threadIdx.x % BP_BX);
+    const int j = blockIdx.y * BP_BY + (threadIdx.x / BP_BX);
+    const int k0 = blockIdx.z * BP_K;
+    if (i >= g.M || j >= g.N) return;
+    const int R = g.R, ZP = g.ZP;
+    double acc[BP_K];
+#pragma unroll
+    for (int kk = 0; kk < BP_K; ++kk) acc[kk] = 0.0;
+    const float cx = fa(fa(g.bx, fm(g.vx, 0.5f)), fm((float)i, g.vx));
+    const float cy = fa(fa(g.by, fm(g.vy, 0.5f)), fm((float)j, g.vy));
+    const float xlo = T.PX[i + 1], xhi = T.PX[i + 2];
+    const float ylo = T.PY[j + 1], yhi = T.PY[j + 2];
+    for (int w = 0; w < nview; ++w) {
+        const int view = view0 + w;
+        const float2 sc = g.trig[view];
+        int ulo, uhi, vlo[BP_K], vhi[BP_K];
+        if (!candidate_rect(g, T, cx, cy, k0, sc.x, sc.y, ulo, uhi, vlo, vhi)) continue;
+        const float4* __restrict__ colt = g.colt + (long long)view * R;
+        const AdjRay* __restrict__ rw = rays + (long long)w * R * ZP;
+        for (int uu = ulo; uu <= uhi; ++uu) {
+            const float4 ct = __ldg(colt + uu);
+            const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+            const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+#pragma unroll
+            for (int kk = 0; kk < BP_K; ++kk) {
+                const int k = k0 + kk;
+                const int kc = min(k, g.Z - 1);
+                const float zl = T.PZ[kc + 1], zh = T.PZ[kc + 2];
+                for (int vv = vlo[kk]; vv <= vhi[kk]; ++vv) {
+                    const AdjRay rec = rw[(long long)vv * R + uu];
+                    const float2 rt = T.RT[vv];
+                    const float az0 = fm(fs(zl, rt.x), rt.y), az1 = fm(fs(zh, rt.x), rt.y);
+                    float exl, exh, eyl, eyh, ezl, ezh;
+                    if (!traversal_cell(i, rec.i.x, rec.i.w & 1, ax0, ax1, ct.y, exl, exh)) continue;
+                    if (!traversal_cell(j, rec.i.y, rec.i.w & 2, ay0, ay1, ct.w, eyl, eyh)) continue;
+                    if (!traversal_cell(k, rec.i.z, rec.i.w & 4, az0, az1, rt.y, ezl, ezh)) continue;
+                    const float lo = fmaxf(fmaxf(exl, eyl), fmaxf(ezl, rec.f.z));
+                    const float hi = fminf(fminf(exh, eyh), fminf(ezh, rec.f.w));
+                    const float temp = fm(rec.f.y, fs(hi, lo));
+                    const bool start = (i == rec.i.x) && (j == rec.i.y) && (k == rec.i.z);
+                    // the traversal's first segment may be a rounding-size negative length
+                    if (temp > 0.0f || (start && rec.f.z <= rec.f.w))
+                        acc[kk] = __fma_rn((double)temp, (double)rec.f.x, acc[kk]);
+                }
+            }
+        }
+    }
+    const long long MN = (long long)g.M * g.N;
+#pragma unroll
+    for (int kk = 0; kk < BP_K; ++kk) {
+        const int k = k0 + kk;
+        if (k >= g.Z) break;
+        VT* p = vol + (long long)k * MN + (long long)j * g.M + i;
+        const double v = accumulate ? (double)Store<VT>::ldw(p) + acc[kk] : acc[kk];
+        Store<VT>::st(p, (float)v);
+    }
+}
+
+static size_t bp_smem(const DevGeom& g)
+{
+    return sizeof(float) * (size_t)(g.M + 3 + g.N + 3 + ((g.Z + 3 + 1) & ~1)) + sizeof(float2) * g.ZP;
 }
 
 ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t st)
 {
+    const DevGeom& g = G.dg;
     if (a.nview <= 0) return CTR_OK;
-    const size_t smem = sizeof(float) * (size_t)(G.dg.M + G.dg.N + G.dg.Z + 10) + sizeof(float2) * G.dg.ZP;
+    const size_t smem = bp_smem(g);
     if (smem > 48 * 1024) return set_error(CTR_ERR_UNSUPPORTED, "plane tables exceed 48 KB of shared memory");
+    dim3 grid((g.M + BP_BX - 1) / BP_BX, (g.N + BP_BY - 1) / BP_BY, (g.Z + BP_K - 1) / BP_K);
+    const int acc = (a.flags & CTR_BP_ACCUMULATE) ? 1 : 0;
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         if (a.sart) {
-            if (a.flags & CTR_SART_STOCHASTIC_ROUND) launch_bp_t<VT, float2, true, true, true>(G, a, st);
-            else launch_bp_t<VT, float2, true, true, false>(G, a, st);
+            if (a.nview != 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART updates one view at a time");
+            if (a.flags & CTR_SART_STOCHASTIC_ROUND)
+                k_backproject<VT, float2, true, true><<<grid, BP_THREADS, smem, st>>>(
+                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed);
+            else
+                k_backproject<VT, float2, true, false><<<grid, BP_THREADS, smem, st>>>(
+                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed);
+        } else if (a.flags & CTR_BP_FOV_MASK) {
+            for (int w = 0; w < a.nview; ++w)
+                k_backproject<VT, AdjRay, false, false><<<grid, BP_THREADS, smem, st>>>(
+                    g, (VT*)a.vol, (const AdjRay*)a.rays + (size_t)w * G.npix(), a.view0 + w, (acc || w > 0) ? 1 : 0,
+                    0.f, 0u);
         } else {
-            if (a.flags & CTR_BP_FOV_MASK) launch_bp_t<VT, float4, false, true, false>(G, a, st);
-            else launch_bp_t<VT, float4, false, false, false>(G, a, st);
+            k_adjoint<VT><<<grid, BP_THREADS, smem, st>>>(g, (VT*)a.vol, (const AdjRay*)a.rays, a.view0, a.nview, acc);
         }
     });
     CTR_CUDA_TRY(cudaGetLastError());

@@ -56,7 +56,7 @@ struct Geometry {
     float4* d_colt = nullptr;
     unsigned* d_err = nullptr;
     // workspace
-    void* d_rays = nullptr;  size_t rays_cap = 0;       // ray records (float2 SART / float4 adjoint)
+    void* d_rays = nullptr;  size_t rays_cap = 0;       // ray records (float2 SART / AdjRay adjoint)
     double* d_partial = nullptr; size_t partial_cap = 0;
     double* d_result = nullptr;                        // 8 doubles
     void* d_fgp = nullptr; size_t fgp_bytes = 0;       // 9 dual arrays
@@ -106,8 +106,8 @@ ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, s
 
 struct BpArgs {
     void* vol; ctr_dtype vol_dtype;
-    const void* rays;                     // [nview][ZP][R]: float2 (c, d12) for SART,
-                                          // float4 (y, d12, alpha_lo, alpha_hi) for the adjoint
+    const void* rays;                     // [nview][ZP][R]: float2 (c, d12) for SART and the
+                                          // masked (reference command 0) form, AdjRay otherwise
     int view0, nview;
     int sart;                             // 1: SART update; 0: adjoint
     unsigned flags;                       // CTR_BP_* / CTR_SART_*
@@ -115,7 +115,13 @@ struct BpArgs {
     uint32_t seed;
 };
 ctr_status launch_backproject(const Geometry& g, const BpArgs& a, cudaStream_t st);
-ctr_status launch_ray_prep(const Geometry& g, const float* y, int view0, int nview, float4* rays,
+// Matched-adjoint ray record: f = (value, chord length d12, alpha_lo, alpha_hi),
+// i = (start voxel i, j, k, parallel-axis bits).
+struct __align__(16) AdjRay {
+    float4 f;
+    int4 i;
+};
+ctr_status launch_ray_prep(const Geometry& g, const float* y, int view0, int nview, AdjRay* rays,
                            cudaStream_t st);
 
 ctr_status launch_reduce(const double* partial, size_t n, double* out, cudaStream_t st);

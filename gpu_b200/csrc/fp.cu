@@ -25,6 +25,8 @@ static constexpr uint64_t kFnvPrime = 1099511628211ULL;
 struct RayResult {
     float sum, len, d12;
     float a_lo, a_hi;   // alpha interval the traversal covered (empty when it dropped the ray)
+    int vi0, vj0, vk0;  // voxel the traversal starts in
+    int par;            // axes the traversal treats as parallel (bit 0 x, 1 y, 2 z)
     int nseg;
     uint64_t hash;
 };
@@ -47,6 +49,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     RayResult r;
     r.sum = 0.f; r.len = 0.f; r.nseg = 0; r.hash = kFnvOffset;
     r.a_lo = 1.0f; r.a_hi = 0.0f;
+    r.vi0 = r.vj0 = r.vk0 = -1; r.par = 0;
 
     // source X2 and detector pixel centre X1 (universal.cu:24-45)
     const float x2x = fs(fm(g.srcx, c), fm(g.srcy, s));
@@ -161,6 +164,8 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     int vi = (x1x < x2x) ? i_min - 1 : i_max;
     int vj = (x1y < x2y) ? j_min - 1 : j_max;
     int vk = (x1z < x2z) ? k_min - 1 : k_max;
+    r.vi0 = vi; r.vj0 = vj; r.vk0 = vk;
+    r.par = (ax == INF ? 1 : 0) | (ay == INF ? 2 : 0) | (az == INF ? 4 : 0);
     const int sx = (x1x < x2x) ? 1 : ((x1x > x2x) ? -1 : 0);
     const int sy = (x1y < x2y) ? 1 : ((x1y > x2y) ? -1 : 0);
     const int sz = (x1z < x2z) ? 1 : ((x1z > x2z) ? -1 : 0);
@@ -292,13 +297,15 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
     return CTR_OK;
 }
 
-// Ray records for the matched adjoint: (value, chord length d12 (:290), and
-// the alpha interval the forward traversal covers).  The interval is what
-// keeps the gather backprojector the exact adjoint where the reference
-// traversal drops or stops a ray at a volume edge.
+// Ray records for the matched adjoint: the value, the chord length d12 (:290),
+// the alpha interval the forward traversal covers, the voxel it starts in and
+// the axes it treats as parallel.  With these the gather backprojector
+// reproduces the traversal's own cell intervals, so it stays the exact
+// adjoint where the reference traversal drops a ray at a volume edge or
+// starts a nearly axis-parallel ray one cell over.
 template <bool E64>
 __global__ void __launch_bounds__(FP_THREADS)
-k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, float4* __restrict__ rays)
+k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, AdjRay* __restrict__ rays)
 {
     extern __shared__ float sp[];
     float* PX = sp;
@@ -315,10 +322,13 @@ k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, float4* __re
     const float2 sc = g.trig[view0 + w];
     const RayResult rr = siddon<float, E64, false, false>(g, PX, PY, PZ, nullptr, sc.x, sc.y, u, v);
     const long long p = ((long long)w * g.ZP + v) * g.R + u;
-    rays[p] = make_float4(y[p], rr.d12, rr.a_lo, rr.a_hi);
+    AdjRay a;
+    a.f = make_float4(y[p], rr.d12, rr.a_lo, rr.a_hi);
+    a.i = make_int4(rr.vi0, rr.vj0, rr.vk0, rr.par);
+    rays[p] = a;
 }
 
-ctr_status launch_ray_prep(const Geometry& G, const float* y, int view0, int nview, float4* rays, cudaStream_t st)
+ctr_status launch_ray_prep(const Geometry& G, const float* y, int view0, int nview, AdjRay* rays, cudaStream_t st)
 {
     const DevGeom& g = G.dg;
     if (nview <= 0) return CTR_OK;

@@ -73,6 +73,8 @@ typedef struct {
     double* lacc;
     int nseg;
     uint64_t hash;
+    float a_lo, a_hi;         /* alpha interval the traversal covered       */
+    int vi0, vj0, vk0, par;   /* start voxel and parallel axes              */
 } og_visit;
 
 #define FNV_OFFSET 1469598103934665603ULL
@@ -216,6 +218,8 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
         int vi = (x1x < x2x) ? i_min - 1 : i_max;
         int vj = (x1y < x2y) ? j_min - 1 : j_max;
         int vk = (x1z < x2z) ? k_min - 1 : k_max;
+        vis->vi0 = vi; vis->vj0 = vj; vis->vk0 = vk;
+        vis->par = (ax == INFINITY ? 1 : 0) | (ay == INFINITY ? 2 : 0) | (az == INFINITY ? 4 : 0);
         /* direction per axis and the offset from the voxel index to the next
          * plane index: +1 when increasing, 0 when decreasing (the reference's
          * next_alpha_index = i+1 / i-1 with i tracking the plane). */
@@ -243,15 +247,17 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
             len = len + seg;
             if (vis->mode == 0) {
                 sum = sum + seg * vis->vol[idx];
-            } else {
+            } else if (vis->mode == 1) {
                 if (!vis->thresh || seg > vis->thr) {
                     vis->acc[idx] += (double)seg * (double)vis->y;
                     if (vis->lacc) vis->lacc[idx] += (double)seg;
                 }
             }
+            if (vis->nseg == 0) vis->a_lo = ac;
             vis->nseg++;
             vis->hash = (vis->hash ^ (uint64_t)(uint32_t)idx) * FNV_PRIME;
             ac = m;
+            vis->a_hi = ac;
             if (ax == m) { vi += sx; ax = (vx * (float)(vi + ox) + bx - x1x) * ix; }
             if (ay == m) { vj += sy; ay = (vy * (float)(vj + oy) + by - x1y) * iy; }
             if (az == m) { vk += sz; az = (vz * (float)(vk + oz) + bz - x1z) * iz; }
@@ -259,6 +265,28 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
     }
     *len_out = len;
     return sum;
+}
+
+void og_fp_window(const og_geom* g, float s, float c, int u, int v, int entry64, float* lo, float* hi)
+{
+    int st[4];
+    og_fp_start(g, s, c, u, v, entry64, lo, hi, st);
+}
+
+void og_fp_start(const og_geom* g, float s, float c, int u, int v, int entry64, float* lo, float* hi, int* start)
+{
+    og_visit vis;
+    memset(&vis, 0, sizeof(vis));
+    vis.mode = 2;
+    vis.hash = FNV_OFFSET;
+    vis.a_lo = 1.0f;
+    vis.a_hi = 0.0f;
+    vis.vi0 = vis.vj0 = vis.vk0 = -1;
+    float l;
+    og_traverse(g, s, c, u, v, entry64, &vis, &l);
+    *lo = vis.a_lo;
+    *hi = vis.a_hi;
+    start[0] = vis.vi0; start[1] = vis.vj0; start[2] = vis.vk0; start[3] = vis.par;
 }
 
 float og_fp_ray(const og_geom* g, const float* vol, float s, float c, int u, int v,

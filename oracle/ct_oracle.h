@@ -62,6 +62,11 @@ void og_view_trig(const og_geom* g, int view, int fdk, float* s, float* c);
  * and the first plane indices in double (the engine's optional FP64 entry). */
 float og_fp_ray(const og_geom* g, const float* vol, float s, float c, int u, int v,
                 int entry64, float* len, int* nseg, uint64_t* hash);
+/* The alpha interval [lo, hi] the traversal of ray (u, v) covers (lo > hi when
+ * it visits no voxel): the support of the engine's matched adjoint chords. */
+void og_fp_window(const og_geom* g, float s, float c, int u, int v, int entry64, float* lo, float* hi);
+/* ... and the voxel it starts in plus its parallel axes (start[0..2], start[3] bits x=1,y=2,z=4). */
+void og_fp_start(const og_geom* g, float s, float c, int u, int v, int entry64, float* lo, float* hi, int* start);
 /* command 0: out = A f ; command 1: out = (b - A f)/len (SART correction). */
 void og_forward_view(const og_geom* g, const float* vol, float s, float c, int command,
                      const float* b, float* out, int entry64);

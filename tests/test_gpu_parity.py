@@ -10,7 +10,7 @@ filter (FP32 convolution against the FP64 kernel), FP64 reductions.
 import numpy as np
 import pytest
 
-from scan_configs import CONFIG0, SMALL, ctr_desc, og_desc_xyz
+from scan_configs import CONFIG0, NO_ON_PLANE_RAYS, SMALL, ctr_desc, og_desc_xyz
 
 pytestmark = pytest.mark.gpu
 
@@ -93,17 +93,19 @@ def test_forward_config0_bit_exact(oracle_built):
 
 @pytest.mark.parametrize("name", sorted(SMALL))
 def test_adjoint_matches_scatter_of_projector(name, oracle_built):
-    """Gather BP == scatter of the projector's own segments (FP32 sums in another order)."""
+    """Gather adjoint == scatter of the projector's own segments: the same
+    chords, FP64 sums in another order, rounded once to float."""
     cfg = SMALL[name]
     g, o = pair(cfg, oracle_built)
     rng = np.random.default_rng(11)
     y = rng.standard_normal((cfg["nviews"],) + o.view_shape).astype(np.float32)
     vol = torch.zeros(o.vol_shape, device="cuda")
     g.backproject(dev(y), vol)
-    got = host(vol)
+    got = host(vol).astype(np.float64)
     ref = o.adjoint(y)
-    scale = np.abs(ref).max()
-    assert np.abs(got - ref).max() <= 2e-6 * scale * cfg["nviews"] ** 0.5
+    assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
+    # to float rounding, voxel by voxel
+    assert np.all(np.abs(got - ref) <= 1.2e-7 * np.abs(ref) + 1e-12 * np.abs(ref).max())
 
 
 @pytest.mark.parametrize("name", sorted(SMALL))
@@ -119,7 +121,7 @@ def test_dot_product(name, oracle_built):
         assert abs(a - b) <= 1e-6 * max(abs(a), abs(b)), (a, b)
 
 
-@pytest.mark.parametrize("name", sorted(SMALL))
+@pytest.mark.parametrize("name", NO_ON_PLANE_RAYS)
 def test_masked_adjoint_vs_reference_bp(name, oracle_built):
     """Reference command-0 BP semantics (FOV mask, thresholds) against the
     reference kernel's own alpha formula: equal up to alpha rounding."""
@@ -151,9 +153,33 @@ def test_sart_pass(name, oracle_built):
     got = host(vol)
     exact = o.sart_pass_gather(np.zeros_like(truth), b, 0.8)
     np.testing.assert_array_equal(bits(got), bits(exact))
-    ref = o.sart_pass_ref(np.zeros_like(truth), b, 0.8)
-    scale = np.abs(ref).max()
-    assert np.sqrt(np.mean((got - ref) ** 2)) <= 2e-3 * scale
+    if name in NO_ON_PLANE_RAYS:
+        ref = o.sart_pass_ref(np.zeros_like(truth), b, 0.8)
+        scale = np.abs(ref).max()
+        assert np.sqrt(np.mean((got - ref) ** 2)) <= 2e-3 * scale
+
+
+def test_reference_bp_drops_on_plane_rays(oracle_built):
+    """The reference BP evaluates 0/0 for a ray lying exactly on a voxel plane
+    and drops it, though its FP traverses it; the engine backprojects the
+    FP's own chord.  One-hot correction on the central ray of an odd detector."""
+    import gpu_b200
+    cfg = SMALL["odd"]
+    g, o = pair(cfg, oracle_built)
+    c = np.zeros(o.view_shape, np.float32)
+    c[cfg["nv"] // 2, cfg["nu"] // 2] = 1.0
+    ref = o.backproject_ref(np.zeros(o.vol_shape, np.float32), c, 0, 1.0, 0)
+    assert np.count_nonzero(ref) == 0
+    vol = torch.zeros(o.vol_shape, device="cuda")
+    g.backproject(dev(c[None]), vol, 0, 1, flags=gpu_b200.BP_FOV_MASK)
+    got = host(vol)
+    n_ref, _, _ = o.forward_trace(np.zeros(o.vol_shape, np.float32), 0)
+    assert n_ref[cfg["nv"] // 2, cfg["nu"] // 2] > 0
+    chords = o.adjoint_view(c, 0, thresh=True)          # the FP's segments of that ray
+    inside = ~o.fov_mask()[None, :, :]
+    expected = (chords * inside).astype(np.float32)
+    assert expected.sum() > 0
+    np.testing.assert_allclose(got, expected, rtol=1e-6, atol=1e-7)
 
 
 @pytest.mark.parametrize("name", sorted(SMALL))
