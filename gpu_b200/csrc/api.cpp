@@ -342,30 +342,40 @@ extern "C" ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, con
     Geometry* g = GE(geom);
     CTR_TRY(check_views(g, v0, n));
     cudaStream_t st = S(stream);
-    const long long P = g->npix(), V = g->nvox();
-    float* ax = nullptr;
-    float* aty = nullptr;
-    CTR_CUDA_TRY(cudaMalloc(&ax, sizeof(float) * (size_t)P * (n > 0 ? n : 1)));
-    ctr_status s = CTR_OK;
-    cudaError_t e = cudaMalloc(&aty, sizeof(float) * (size_t)V);
-    if (e != cudaSuccess) s = cuda_error(e, "cudaMalloc");
+    const long long V = g->nvox();
+    const DevGeom& q = g->dg;
+    const size_t per_view = (size_t)((q.R + 31) / 32) * ((q.ZP + 3) / 4);
+    const size_t nblk = per_view * (n > 0 ? n : 1);
     const size_t cap = 148 * 64;
-    if (s == CTR_OK) s = ensure_partial(g, cap + 2048);
-    if (s == CTR_OK) s = ctr_forward(geom, x, CTR_F32, ax, CTR_F32, v0, n, stream);
-    if (s == CTR_OK) s = ctr_backproject(geom, y, v0, n, aty, CTR_F32, 0, stream);
-    if (s == CTR_OK) s = launch_dot(ax, y, P * n, g->d_partial, cap, g->d_result, st);
+    CTR_TRY(ensure_partial(g, std::max(nblk, cap) + 2048));
+    // <A x, y>: the projector's segments, each ray summed in FP64
+    if (n > 0) {
+        FpArgs a{};
+        a.vol = x; a.vol_dtype = CTR_F32; a.view0 = v0; a.nview = n; a.kind = FP_DOT;
+        a.b = y; a.b_dtype = CTR_F32; a.partial = g->d_partial;
+        CTR_TRY(launch_forward(*g, a, st, nullptr));
+        CTR_TRY(launch_reduce(g->d_partial, nblk, g->d_result, st));
+    } else {
+        CTR_CUDA_TRY(cudaMemsetAsync(g->d_result, 0, sizeof(double), st));
+    }
+    double h0 = 0.0;
+    CTR_CUDA_TRY(cudaMemcpyAsync(&h0, g->d_result, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTR_CUDA_TRY(cudaStreamSynchronize(st));
+    // <x, A^T y>: the matched adjoint (FP64 accumulation, rounded to float per voxel)
+    float* aty = nullptr;
+    CTR_CUDA_TRY(cudaMalloc(&aty, sizeof(float) * (size_t)V));
+    ctr_status s = ctr_backproject(geom, y, v0, n, aty, CTR_F32, 0, stream);
     if (s == CTR_OK) s = launch_dot(x, aty, V, g->d_partial, cap, g->d_result + 1, st);
-    double h[2] = {0, 0};
+    double h1 = 0.0;
     if (s == CTR_OK) {
-        e = cudaMemcpyAsync(h, g->d_result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaMemcpyAsync(&h1, g->d_result + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
         if (e != cudaSuccess) s = cuda_error(e, "cudaMemcpyAsync");
     }
     if (s == CTR_OK) s = check_device_errors(g, st);
-    cudaFree(ax);
     cudaFree(aty);
     if (s == CTR_OK) {
-        if (ax_y) *ax_y = h[0];
-        if (x_aty) *x_aty = h[1];
+        if (ax_y) *ax_y = h0;
+        if (x_aty) *x_aty = h1;
     }
     return s;
 }

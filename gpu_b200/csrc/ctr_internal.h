@@ -92,14 +92,14 @@ ctr_status ensure_fgp(Geometry* g, size_t bytes);
 ctr_status check_device_errors(Geometry* g, cudaStream_t st);
 
 // ---- kernel launchers (implemented in the .cu files) ----
-enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3 };
+enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3, FP_DOT = 4 };
 struct FpArgs {
     const void* vol; ctr_dtype vol_dtype;
     int view0, nview;
     FpKind kind;
     void* out; ctr_dtype out_dtype;       // FORWARD: sino; SART: float2 rays
-    const void* b; ctr_dtype b_dtype;     // SART/OBJECTIVE: measured sinogram (already offset to view0)
-    double* partial;                      // OBJECTIVE: one double per block
+    const void* b; ctr_dtype b_dtype;     // SART/OBJECTIVE: measured sinogram; DOT: y (offset to view0)
+    double* partial;                      // OBJECTIVE/DOT: one double per block
     int* nseg; uint64_t* hash; float* len;  // TRACE
 };
 ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, size_t* nblocks_out);

@@ -24,6 +24,7 @@ static constexpr uint64_t kFnvPrime = 1099511628211ULL;
 
 struct RayResult {
     float sum, len, d12;
+    double dsum;        // the same segments summed in FP64 (ACC64 only)
     float a_lo, a_hi;   // alpha interval the traversal covered (empty when it dropped the ray)
     int vi0, vj0, vk0;  // voxel the traversal starts in
     int par;            // axes the traversal treats as parallel (bit 0 x, 1 y, 2 z)
@@ -40,14 +41,14 @@ __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, 
 
 // LOAD=false walks the rays without reading the volume: it yields the chord
 // lengths' support (a_lo, a_hi) for the matched adjoint.
-template <typename VT, bool E64, bool TRACE, bool LOAD = true>
+template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false>
 __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
                                             const float* __restrict__ PY, const float* __restrict__ PZ,
                                             const VT* __restrict__ vol, float s, float c, int u, int v)
 {
     const int M = g.M, N = g.N, Z = g.Z;
     RayResult r;
-    r.sum = 0.f; r.len = 0.f; r.nseg = 0; r.hash = kFnvOffset;
+    r.sum = 0.f; r.len = 0.f; r.dsum = 0.0; r.nseg = 0; r.hash = kFnvOffset;
     r.a_lo = 1.0f; r.a_hi = 0.0f;
     r.vi0 = r.vj0 = r.vk0 = -1; r.par = 0;
 
@@ -179,6 +180,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     int idx = vk * MN + vj * M + vi;
     const float d12 = r.d12;
     float ac = amin, sum = 0.f, len = 0.f;
+    double dsum = 0.0;
     int steps = 0;
     bool any = false;
     // :297-551
@@ -193,7 +195,8 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
         len = fa(len, seg);
         if (LOAD) {
             const float f = Store<VT>::ld(vol + idx);
-            sum = fa(sum, fm(seg, f));
+            if (ACC64) dsum = __fma_rn((double)seg, (double)f, dsum);
+            else sum = fa(sum, fm(seg, f));
         }
         any = true;
         if (TRACE) {
@@ -206,6 +209,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
         if (az == m) { vk += sz; idx += szMN; az = fm(fs(PZo[vk], x1z), iz); }
     }
     r.sum = sum;
+    r.dsum = dsum;
     r.len = len;
     if (any) {
         r.a_lo = amin;
@@ -238,7 +242,7 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     double e2 = 0.0;
     if (active) {
         const float2 sc = g.trig[view0 + w];
-        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE>(g, PX, PY, PZ, vol, sc.x, sc.y, u, v);
+        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT>(g, PX, PY, PZ, vol, sc.x, sc.y, u, v);
         const bool zero = rr.len < g.thr_fp;                       // :554
         if (KIND == FP_FORWARD) {
             st_any(out, p, out_dt, zero ? 0.0f : rr.sum);
@@ -251,13 +255,15 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
             const float bv = ld_any(b, p, b_dt);
             const float e = fs(ax, bv);
             e2 = (double)fm(e, e);                                     // L2_norm_kernel, tool_functions.cu:35
+        } else if (KIND == FP_DOT) {
+            e2 = zero ? 0.0 : rr.dsum * (double)ld_any(b, p, b_dt);   // <A x, y> with FP64 ray sums
         } else {
             nseg[p] = rr.nseg;
             hash[p] = rr.hash;
             lens[p] = rr.len;
         }
     }
-    if (KIND == FP_OBJECTIVE) {
+    if (KIND == FP_OBJECTIVE || KIND == FP_DOT) {
         __shared__ double sh[FP_THREADS / 32];
         const double t = block_sum(e2, sh);
         if (threadIdx.x == 0)
@@ -291,6 +297,7 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
         case FP_SART: launch_fp_t<VT, FP_SART>(G, a, grid, smem, st); break;
         case FP_OBJECTIVE: launch_fp_t<VT, FP_OBJECTIVE>(G, a, grid, smem, st); break;
         case FP_TRACE: launch_fp_t<VT, FP_TRACE>(G, a, grid, smem, st); break;
+        case FP_DOT: launch_fp_t<VT, FP_DOT>(G, a, grid, smem, st); break;
         }
     });
     CTR_CUDA_TRY(cudaGetLastError());

@@ -175,9 +175,11 @@ ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float* vol, void
 
 /* ------------------------------------------------------------ dot product */
 
-/* <A x, y> and <x, A^T y> over views [view_begin, view_begin+view_count), FP64
- * inner products of FP32 operators.  Synchronises.  The matched-adjoint
- * check of CheckMatchedJointOperator (V63/host_IterativeRecon_CBCT.c:131-204). */
+/* <A x, y> and <x, A^T y> over views [view_begin, view_begin+view_count):
+ * FP64 inner products; A x sums the projector's Siddon segments of each ray
+ * in FP64 and A^T y is the matched adjoint (FP64 accumulation, float result),
+ * so the two agree to float rounding of A^T y.  Synchronises.  The matched-
+ * adjoint check of CheckMatchedJointOperator (V63/host_IterativeRecon_CBCT.c:131-204). */
 ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, const float* y, int view_begin,
                         int view_count, double* ax_dot_y, double* x_dot_aty, void* stream);
 

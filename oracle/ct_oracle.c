@@ -755,9 +755,9 @@ void og_fgp_f64(int M, int N, int Z, const double* f, double lambda, int iters, 
  * sums the float terms in one 1024-thread block; here the sum is in double. */
 double og_tv_norm(int M, int N, int Z, const float* d)
 {
-    const long long MN = (long long)M * N;
-    double total = 0.0;
-#pragma omp parallel for collapse(2) reduction(+ : total) schedule(static)
+    const long long MN = (long long)M * N, V = MN * Z;
+    float* terms = (float*)malloc(sizeof(float) * V);
+#pragma omp parallel for collapse(2) schedule(static)
     for (int z = 0; z < Z; ++z)
         for (int y = 0; y < N; ++y)
             for (int x = 0; x < M; ++x) {
@@ -778,17 +778,20 @@ double og_tv_norm(int M, int N, int Z, const float* d)
                     tv = fabsf(d[i] - d[k]);
                 else if (x < M - 1 && y == N - 1 && z == Z - 1)
                     tv = fabsf(d[i] - d[j]);
-                total += (double)tv;
+                terms[i] = tv;
             }
+    double total = 0.0;                 /* index order, like the reference's CPU summation */
+    for (long long i = 0; i < V; ++i) total += (double)terms[i];
+    free(terms);
     return total;
 }
 
 /* L2_norm_kernel + summation (V63/kernel_tool_functions.cu:30-35,
- * V63/host_tool_functions.cu:18-25): sum of float (a-b)^2 terms, in double. */
+ * V63/host_tool_functions.cu:18-25): sum of float (a-b)^2 terms, in double,
+ * in index order. */
 double og_l2_norm(const float* a, const float* b, long long n)
 {
     double total = 0.0;
-#pragma omp parallel for reduction(+ : total) schedule(static)
     for (long long i = 0; i < n; ++i) {
         const float e = (a[i] - b[i]) * (a[i] - b[i]);
         total += (double)e;
