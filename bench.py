@@ -38,6 +38,8 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mixed", choices=["f16", "bf16"], default="f16")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-views", type=int, default=0,
+                   help="profiling mode: set up the scan, run a SART update of this many views, print timings, exit")
     return p.parse_args()
 
 
@@ -224,10 +226,34 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_views(args):
+    """A short run for ncu: the benchmark scan, then SART updates of a few
+    views (one forward + one backprojection launch each) in FP32 and FP16."""
+    import torch
+
+    import gpu_b200
+    desc = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
+                              SCAN["dso"], SCAN["dod"], SCAN["n_views"])
+    geom = gpu_b200.Geometry(desc)
+    truth = torch.zeros(geom.vol_shape, device="cuda")
+    geom.phantom_voxelize(phantom_params(2024), truth)
+    sino = torch.zeros((SCAN["n_views"],) + geom.view_shape, device="cuda")
+    geom.forward(truth, sino, 0, args.profile_views)
+    out = {}
+    for name, dt in (("f32", torch.float32), ("f16", torch.float16)):
+        vol = torch.zeros(geom.vol_shape, device="cuda", dtype=dt)
+        s = sino if dt == torch.float32 else sino.to(dt)
+        fp, bp = geom.sart_views(vol, s, BETA, 0, args.profile_views, timed=True)
+        out[name] = {"fp_ms_per_view": fp / args.profile_views, "bp_ms_per_view": bp / args.profile_views}
+    print(json.dumps({"profile_views": args.profile_views, **out}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_views:
+        return profile_views(args)
     import numpy as np
     import torch
     import torch.distributed as dist
