@@ -40,6 +40,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-views", type=int, default=0,
                    help="profiling mode: set up the scan, run a SART update of this many views, print timings, exit")
+    p.add_argument("--profile-iteration", action="store_true",
+                   help="with --profile-views: also run one FP16 solver iteration")
     return p.parse_args()
 
 
@@ -227,25 +229,40 @@ def run_reference(args):
 
 
 def profile_views(args):
-    """A short run for ncu: the benchmark scan, then SART updates of a few
-    views (one forward + one backprojection launch each) in FP32 and FP16."""
+    """A short run for ncu on the benchmark scan: SART updates of the first
+    --profile-views views (one forward + one backprojection launch each) in
+    FP32 and FP16, then, with --profile-iteration, one FP16 solver iteration.
+    Only the profiled views' sinogram is kept on the device unless the
+    iteration needs all of it."""
     import torch
 
     import gpu_b200
+    n = args.profile_views
     desc = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
                               SCAN["dso"], SCAN["dod"], SCAN["n_views"])
     geom = gpu_b200.Geometry(desc)
     truth = torch.zeros(geom.vol_shape, device="cuda")
     geom.phantom_voxelize(phantom_params(2024), truth)
-    sino = torch.zeros((SCAN["n_views"],) + geom.view_shape, device="cuda")
-    geom.forward(truth, sino, 0, args.profile_views)
+    nv = SCAN["n_views"] if args.profile_iteration else n
+    sino16 = torch.zeros((nv,) + geom.view_shape, device="cuda", dtype=torch.float16)
+    geom.forward(truth, sino16, 0, nv)
+    sino32 = sino16[:n].float()
     out = {}
-    for name, dt in (("f32", torch.float32), ("f16", torch.float16)):
-        vol = torch.zeros(geom.vol_shape, device="cuda", dtype=dt)
-        s = sino if dt == torch.float32 else sino.to(dt)
-        fp, bp = geom.sart_views(vol, s, BETA, 0, args.profile_views, timed=True)
-        out[name] = {"fp_ms_per_view": fp / args.profile_views, "bp_ms_per_view": bp / args.profile_views}
-    print(json.dumps({"profile_views": args.profile_views, **out}), flush=True)
+    for name, s in (("f32", sino32), ("f16", sino16)):
+        vol = torch.zeros(geom.vol_shape, device="cuda", dtype=s.dtype)
+        fp, bp = geom.sart_views(vol, s, BETA, 0, n, timed=True)
+        out[name] = {"fp_ms_per_view": fp / n, "bp_ms_per_view": bp / n}
+        del vol
+    del truth
+    if args.profile_iteration:
+        solver = gpu_b200.Solver(geom, gpu_b200.F16, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS)
+        solver.set_sinogram(sino16)
+        solver.set_volume(None)
+        t0 = time.perf_counter()
+        solver.iterate(1)
+        out["iteration_s"] = time.perf_counter() - t0
+        solver.close()
+    print(json.dumps({"profile_views": n, **out}), flush=True)
 
 
 def main():
