@@ -37,7 +37,7 @@ SART_STOCHASTIC_ROUND = 0x1
 # every symbol include/ctrecon.h declares
 EXPORTED = [
     "ctr_geometry_create", "ctr_geometry_destroy", "ctr_geometry_view_trig", "ctr_forward",
-    "ctr_backproject", "ctr_sart_pass", "ctr_sart_views", "ctr_forward_trace", "ctr_fgp_tv", "ctr_fista_momentum",
+    "ctr_backproject", "ctr_sart_pass", "ctr_sart_views", "ctr_sart_views_noalloc", "ctr_forward_trace", "ctr_fgp_tv", "ctr_fista_momentum",
     "ctr_objective", "ctr_tv_norm", "ctr_l2_norm", "ctr_fdk", "ctr_dot_test", "ctr_solver_create",
     "ctr_solver_destroy", "ctr_solver_set_sinogram", "ctr_solver_set_volume", "ctr_solver_iterate",
     "ctr_solver_get_volume", "ctr_solver_iteration_count", "ctr_solver_save", "ctr_solver_load",
@@ -95,6 +95,7 @@ def load_library(path: str = LIB_PATH):
         "ctr_backproject": ([G, vp, i, i, vp, i, u, vp], i),
         "ctr_sart_pass": ([G, vp, i, vp, i, f, u, C.c_uint32, vp], i),
         "ctr_sart_views": ([G, vp, i, vp, i, f, u, C.c_uint32, i, i, C.POINTER(f), C.POINTER(f), vp], i),
+        "ctr_sart_views_noalloc": ([G, vp, i, vp, i, f, u, C.c_uint32, i, i, vp], i),
         "ctr_forward_trace": ([G, vp, i, vp, vp, vp, vp], i),
         "ctr_fgp_tv": ([G, vp, i, f, i, vp], i),
         "ctr_fista_momentum": ([G, vp, vp, vp, i, f, f, vp], i),

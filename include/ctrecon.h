@@ -124,6 +124,20 @@ ctr_status ctr_sart_views(const ctr_geometry* geom, void* vol, ctr_dtype vol_dty
                           ctr_dtype sino_dtype, float beta, unsigned flags, uint32_t seed,
                           int view_begin, int view_count, float* fp_ms, float* bp_ms, void* stream);
 
+/* ctr_sart_views without any device allocation, for callers that cannot
+ * allocate while they reconstruct: a host whose memory pool has reserved the
+ * GPU up front, or a real-time loop that must not stall on cudaMalloc/cudaFree.
+ * No counterpart in the reference (its host functions cudaMalloc and cudaFree
+ * on every call).  The ray records live in a fixed 8 MiB device array inside
+ * the library, so the detector may have at most 1,048,576 pixels (larger ones
+ * are rejected with CTR_ERR_INVALID_ARGUMENT).  The geometry's device must be
+ * current.  The first call on a device looks the array up (no allocation);
+ * make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race. */
+ctr_status ctr_sart_views_noalloc(const ctr_geometry* geom, void* vol, ctr_dtype vol_dtype, const void* sino,
+                                  ctr_dtype sino_dtype, float beta, unsigned flags, uint32_t seed,
+                                  int view_begin, int view_count, void* stream);
+
 /* Trace one view: per ray, the number of Siddon segments, an FNV-1a hash of
  * the visited voxel index sequence and the summed chord length.  For parity
  * checks of the traversal (the voxel index set of every ray). */
