@@ -35,7 +35,7 @@ namespace ctr {
 static constexpr int BP_BX = 32;   // voxels along x per block (one warp row)
 static constexpr int BP_BY = 4;    // voxel rows along y per block
 static constexpr int BP_THREADS = BP_BX * BP_BY;
-static constexpr int BP_K = 4;     // z voxels per thread
+static constexpr int BP_K = 8;     // z voxels per thread
 
 struct SharedTables {
     float* PX;

@@ -48,3 +48,14 @@ def ctr_desc(cfg, entry64=False):
                      cfg["dod"], cfg["nviews"], initial_angle=cfg.get("initial_angle", 0.0),
                      shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
                      m_offset=cfg.get("m_offset", 0), entry64=entry64)
+
+# Differentiation scan: 256^3, 360 views, 384^2 detector.  "Config-0 geometry
+# scaled by 2" is read as the same physical extents at twice the sampling:
+# 0.5 mm voxels (128 mm FOV) and a 204.8 mm detector of 384 pixels.
+CONFIG2 = dict(nx=256, ny=256, nz=256, nu=384, nv=384, nviews=360, vx=0.5, du=204.8 / 384, dso=1000.0,
+               dod=-500.0)
+
+# Mixed-precision accuracy scan: small enough for the FP64 oracle, an angle
+# offset keeps views off the exact axes.
+MIXED = dict(nx=64, ny=64, nz=64, nu=96, nv=96, nviews=90, vx=2.0, du=3.2, dso=1000.0, dod=-500.0,
+             initial_angle=1.0)
