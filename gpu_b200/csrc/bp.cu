@@ -143,7 +143,19 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
         int ulo, uhi, vlo[BP_K], vhi[BP_K];
         if (candidate_rect(g, T, cx, cy, k0, sc.x, sc.y, ulo, uhi, vlo, vhi)) {
             const float4* __restrict__ colt = g.colt + (long long)view0 * R;
+            // the detector columns whose ray column crosses this voxel column
+            // form one run; find it first so that lanes loop over it in step
+            int ua = uhi + 1, ub = ulo - 1;
             for (int uu = ulo; uu <= uhi; ++uu) {
+                const float4 ct = __ldg(colt + uu);
+                const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+                const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+                if (fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)) > fmaxf(fminf(ax0, ax1), fminf(ay0, ay1))) {
+                    ua = min(ua, uu);
+                    ub = uu;
+                }
+            }
+            for (int uu = ua; uu <= ub; ++uu) {
                 const float4 ct = __ldg(colt + uu);
                 const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
                 const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);

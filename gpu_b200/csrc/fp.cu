@@ -41,10 +41,13 @@ __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, 
 
 // LOAD=false walks the rays without reading the volume: it yields the chord
 // lengths' support (a_lo, a_hi) for the matched adjoint.
+// PINF points at a shared +inf: the next-plane table of an axis the ray is
+// parallel to, so every axis can recompute its alpha unconditionally.
 template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false>
 __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
                                             const float* __restrict__ PY, const float* __restrict__ PZ,
-                                            const VT* __restrict__ vol, float s, float c, int u, int v)
+                                            const float* __restrict__ PINF, const VT* __restrict__ vol, float s,
+                                            float c, int u, int v)
 {
     const int M = g.M, N = g.N, Z = g.Z;
     RayResult r;
@@ -167,14 +170,20 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     int vk = (x1z < x2z) ? k_min - 1 : k_max;
     r.vi0 = vi; r.vj0 = vj; r.vk0 = vk;
     r.par = (ax == INF ? 1 : 0) | (ay == INF ? 2 : 0) | (az == INF ? 4 : 0);
-    const int sx = (x1x < x2x) ? 1 : ((x1x > x2x) ? -1 : 0);
-    const int sy = (x1y < x2y) ? 1 : ((x1y > x2y) ? -1 : 0);
-    const int sz = (x1z < x2z) ? 1 : ((x1z > x2z) ? -1 : 0);
-    // PXo[vi] = plane index vi+1 (increasing) or vi (decreasing): the
-    // reference's next_alpha_index after the move.
+    // Per axis: direction, and the table PXo with PXo[voxel] = the next plane
+    // after the move (the reference's next_alpha_index): plane vi+1 when
+    // increasing, vi when decreasing.  A parallel axis never moves and reads
+    // +inf through (x1 = 0, 1/d = 1).
+    int sx = (x1x < x2x) ? 1 : ((x1x > x2x) ? -1 : 0);
+    int sy = (x1y < x2y) ? 1 : ((x1y > x2y) ? -1 : 0);
+    int sz = (x1z < x2z) ? 1 : ((x1z > x2z) ? -1 : 0);
     const float* PXo = PX + 1 + (sx > 0);
     const float* PYo = PY + 1 + (sy > 0);
     const float* PZo = PZ + 1 + (sz > 0);
+    float ex1x = x1x, eix = ix, ex1y = x1y, eiy = iy, ex1z = x1z, eiz = iz;
+    if (ax == INF) { sx = 0; PXo = PINF - vi; ex1x = 0.f; eix = 1.f; }
+    if (ay == INF) { sy = 0; PYo = PINF - vj; ex1y = 0.f; eiy = 1.f; }
+    if (az == INF) { sz = 0; PZo = PINF - vk; ex1z = 0.f; eiz = 1.f; }
     const int MN = M * N;
     const int syM = sy * M, szMN = sz * MN;
     int idx = vk * MN + vj * M + vi;
@@ -183,7 +192,9 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     double dsum = 0.0;
     int steps = 0;
     bool any = false;
-    // :297-551
+    // :297-551.  Branch-free step: every axis re-evaluates its next-plane
+    // alpha from its (possibly unchanged) index, which reproduces the current
+    // value bit for bit when the axis did not move.
     while (fs(amax, ac) > 1e-16f) {
         if ((unsigned)vi >= (unsigned)M || (unsigned)vj >= (unsigned)N || (unsigned)vk >= (unsigned)Z) break;
         if (++steps > g.max_steps) {
@@ -204,9 +215,14 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
             r.hash = (r.hash ^ (uint64_t)(uint32_t)idx) * kFnvPrime;
         }
         ac = m;
-        if (ax == m) { vi += sx; idx += sx; ax = fm(fs(PXo[vi], x1x), ix); }
-        if (ay == m) { vj += sy; idx += syM; ay = fm(fs(PYo[vj], x1y), iy); }
-        if (az == m) { vk += sz; idx += szMN; az = fm(fs(PZo[vk], x1z), iz); }
+        const int mx = (ax == m) ? 1 : 0, my = (ay == m) ? 1 : 0, mz = (az == m) ? 1 : 0;
+        vi += mx * sx;
+        vj += my * sy;
+        vk += mz * sz;
+        idx += mx * sx + my * syM + mz * szMN;
+        ax = fm(fs(PXo[vi], ex1x), eix);
+        ay = fm(fs(PYo[vj], ex1y), eiy);
+        az = fm(fs(PZo[vk], ex1z), eiz);
     }
     r.sum = sum;
     r.dsum = dsum;
@@ -228,9 +244,11 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     float* PX = sp;
     float* PY = PX + (g.M + 3);
     float* PZ = PY + (g.N + 3);
+    float* PINF = PZ + (g.Z + 3);
     for (int t = threadIdx.x; t < g.M + 3; t += FP_THREADS) PX[t] = g.px[t];
     for (int t = threadIdx.x; t < g.N + 3; t += FP_THREADS) PY[t] = g.py[t];
     for (int t = threadIdx.x; t < g.Z + 3; t += FP_THREADS) PZ[t] = g.pz[t];
+    if (threadIdx.x == 0) PINF[0] = __int_as_float(0x7f800000);
     __syncthreads();
 
     const int u = blockIdx.x * FP_BX + (threadIdx.x % FP_BX);
@@ -242,7 +260,7 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     double e2 = 0.0;
     if (active) {
         const float2 sc = g.trig[view0 + w];
-        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT>(g, PX, PY, PZ, vol, sc.x, sc.y, u, v);
+        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT>(g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v);
         const bool zero = rr.len < g.thr_fp;                       // :554
         if (KIND == FP_FORWARD) {
             st_any(out, p, out_dt, zero ? 0.0f : rr.sum);
@@ -290,7 +308,7 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
     if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
     dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + FP_BY - 1) / FP_BY, a.nview);
     if (nblocks_out) *nblocks_out = (size_t)grid.x * grid.y * grid.z;
-    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 9);
+    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 10);
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         switch (a.kind) {
         case FP_FORWARD: launch_fp_t<VT, FP_FORWARD>(G, a, grid, smem, st); break;
@@ -318,16 +336,18 @@ k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, AdjRay* __re
     float* PX = sp;
     float* PY = PX + (g.M + 3);
     float* PZ = PY + (g.N + 3);
+    float* PINF = PZ + (g.Z + 3);
     for (int t = threadIdx.x; t < g.M + 3; t += FP_THREADS) PX[t] = g.px[t];
     for (int t = threadIdx.x; t < g.N + 3; t += FP_THREADS) PY[t] = g.py[t];
     for (int t = threadIdx.x; t < g.Z + 3; t += FP_THREADS) PZ[t] = g.pz[t];
+    if (threadIdx.x == 0) PINF[0] = __int_as_float(0x7f800000);
     __syncthreads();
     const int u = blockIdx.x * FP_BX + (threadIdx.x % FP_BX);
     const int v = blockIdx.y * FP_BY + (threadIdx.x / FP_BX);
     const int w = blockIdx.z;
     if (u >= g.R || v >= g.ZP) return;
     const float2 sc = g.trig[view0 + w];
-    const RayResult rr = siddon<float, E64, false, false>(g, PX, PY, PZ, nullptr, sc.x, sc.y, u, v);
+    const RayResult rr = siddon<float, E64, false, false>(g, PX, PY, PZ, PINF, nullptr, sc.x, sc.y, u, v);
     const long long p = ((long long)w * g.ZP + v) * g.R + u;
     AdjRay a;
     a.f = make_float4(y[p], rr.d12, rr.a_lo, rr.a_hi);
@@ -340,7 +360,7 @@ ctr_status launch_ray_prep(const Geometry& G, const float* y, int view0, int nvi
     const DevGeom& g = G.dg;
     if (nview <= 0) return CTR_OK;
     dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + FP_BY - 1) / FP_BY, nview);
-    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 9);
+    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 10);
     if (g.entry64) k_ray_prep<true><<<grid, FP_THREADS, smem, st>>>(g, y, view0, rays);
     else k_ray_prep<false><<<grid, FP_THREADS, smem, st>>>(g, y, view0, rays);
     CTR_CUDA_TRY(cudaGetLastError());
