@@ -44,6 +44,8 @@ EXPORTED = [
     "ctr_last_error_string", "ctr_convert", "ctr_phantom_voxelize", "ctr_set_default_geometry",
     "Forward_3D_ray_driven_siddon", "Reconstruction_3D_ray_driven_CBCT", "CheckMatchedJointOperator",
     "FGP_denoise_GPUx7_exact", "Reconstruction_FDK", "L2_norm_gpu", "TV_norm_gpu",
+    "ctr_io_view_filename", "ctr_io_recon_filename", "ctr_io_objective_filename", "ctr_io_write_raw",
+    "ctr_io_read_raw", "ctr_io_read_views", "ctr_io_write_views",
 ]
 
 
@@ -124,6 +126,13 @@ def load_library(path: str = LIB_PATH):
         "Reconstruction_FDK": ([vp, vp], None),
         "L2_norm_gpu": ([vp, vp], d),
         "TV_norm_gpu": ([vp], d),
+        "ctr_io_view_filename": ([C.c_char_p, C.c_size_t, i, f, f, i, i], i),
+        "ctr_io_recon_filename": ([C.c_char_p, C.c_size_t, C.c_char_p, i, i, i, f, i, f, f, f, f, f, i], i),
+        "ctr_io_objective_filename": ([C.c_char_p, C.c_size_t, C.c_char_p, i, f, f, f, f], i),
+        "ctr_io_write_raw": ([C.c_char_p, vp, C.c_size_t], i),
+        "ctr_io_read_raw": ([C.c_char_p, vp, C.c_size_t, C.c_size_t], i),
+        "ctr_io_read_views": ([C.c_char_p, i, i, i, f, f, i, i, vp], i),
+        "ctr_io_write_views": ([C.c_char_p, i, i, i, f, f, i, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -352,6 +361,55 @@ class Solver:
 
     def load(self, path, stream=None):
         check(self.lib.ctr_solver_load(self.h, str(path).encode(), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# The reference driver's file formats
+# ---------------------------------------------------------------------------
+
+def view_filename(view, us_rate, initial_angle=0.0, tomo=0, n_views=0):
+    buf = C.create_string_buffer(64)
+    check(load_library().ctr_io_view_filename(buf, 64, view, us_rate, initial_angle, tomo, n_views))
+    return buf.value.decode()
+
+
+def recon_filename(object_name, nx, ny, nz, voxel_um, n_views, initial_angle, end_angle, lambda_tv, lambda_l1,
+                   lip, iteration=-1):
+    buf = C.create_string_buffer(512)
+    check(load_library().ctr_io_recon_filename(buf, 512, object_name.encode(), nx, ny, nz, voxel_um, n_views,
+                                               initial_angle, end_angle, lambda_tv, lambda_l1, lip, iteration))
+    return buf.value.decode()
+
+
+def objective_filename(object_name, n_views, initial_angle, end_angle, lambda_tv, lip):
+    buf = C.create_string_buffer(512)
+    check(load_library().ctr_io_objective_filename(buf, 512, object_name.encode(), n_views, initial_angle,
+                                                   end_angle, lambda_tv, lip))
+    return buf.value.decode()
+
+
+def write_raw(path, arr):
+    a = np.ascontiguousarray(arr)
+    check(load_library().ctr_io_write_raw(str(path).encode(), a.ctypes.data, a.nbytes))
+
+
+def read_raw(path, shape, dtype=np.float32, offset=0):
+    a = np.empty(shape, dtype)
+    check(load_library().ctr_io_read_raw(str(path).encode(), a.ctypes.data, a.nbytes, offset))
+    return a
+
+
+def write_views(directory, proj, us_rate, initial_angle=0.0, tomo=0):
+    p = np.ascontiguousarray(proj, np.float32)
+    check(load_library().ctr_io_write_views(str(directory).encode(), p.shape[2], p.shape[1], p.shape[0], us_rate,
+                                            initial_angle, tomo, p.ctypes.data))
+
+
+def read_views(directory, nu, nv, n_views, us_rate, initial_angle=0.0, tomo=0, row_offset=0):
+    p = np.empty((n_views, nv, nu), np.float32)
+    check(load_library().ctr_io_read_views(str(directory).encode(), nu, nv, n_views, us_rate, initial_angle, tomo,
+                                           row_offset, p.ctypes.data))
+    return p
 
 
 # ---------------------------------------------------------------------------

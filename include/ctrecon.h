@@ -246,6 +246,32 @@ ctr_status ctr_convert(const void* src, ctr_dtype src_dtype, void* dst, ctr_dtyp
 ctr_status ctr_phantom_voxelize(const ctr_geometry* geom, const double* params, int n,
                                 float* vol, void* stream);
 
+/* ------------------------------------------------------------- file formats */
+
+/* The reference driver's files (V63/main_recon.cu:197-266, 434-477), host only.
+ * View files hold one view as raw little-endian float [nv][nu]; volumes are raw
+ * float [nz][ny][nx]; the objective file holds 3 doubles per iteration. */
+/* "View_%.02f.dat" for view j, with the reference's angle rule (tomosynthesis
+ * split at n_views/2, negative angles + 360), V63/main_recon.cu:203-212. */
+ctr_status ctr_io_view_filename(char* out, size_t n, int view, float us_rate, float initial_angle, int tomo,
+                                int n_views);
+/* The reconstruction file names of V63/main_recon.cu:438 (iteration < 0) and
+ * :452 (numbered copy); voxel_um is the voxel pitch in micrometres. */
+ctr_status ctr_io_recon_filename(char* out, size_t n, const char* object, int nx, int ny, int nz, float voxel_um,
+                                 int n_views, float initial_angle, float end_angle, float lambda_tv,
+                                 float lambda_l1, float lip, int iteration);
+/* object_func_<...>.bin of V63/main_recon.cu:468. */
+ctr_status ctr_io_objective_filename(char* out, size_t n, const char* object, int n_views, float initial_angle,
+                                     float end_angle, float lambda_tv, float lip);
+ctr_status ctr_io_write_raw(const char* path, const void* data, size_t bytes);
+ctr_status ctr_io_read_raw(const char* path, void* data, size_t bytes, size_t offset);
+/* All views from dir/View_<angle>.dat into h_proj [n_views][nv][nu], skipping
+ * row_offset rows at the start of each file (the reference's fseek, :221). */
+ctr_status ctr_io_read_views(const char* dir, int nu, int nv, int n_views, float us_rate, float initial_angle,
+                             int tomo, int row_offset, float* h_proj);
+ctr_status ctr_io_write_views(const char* dir, int nu, int nv, int n_views, float us_rate, float initial_angle,
+                              int tomo, const float* h_proj);
+
 /* ------------------------------------------- reference-compatible entry points */
 
 /* The reference's host functions keep their geometry in compile-time globals;
