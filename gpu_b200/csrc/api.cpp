@@ -63,7 +63,8 @@ ctr_status forward_chunks(Geometry* g, FpArgs a, cudaStream_t st)
 // SART pass: per view FP command 1 -> ray records, then BP command 1.
 // With ev (3 events per view) the launches are bracketed for timing.
 ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
-                      unsigned flags, uint32_t seed, int v0, int nv, cudaStream_t st, cudaEvent_t* ev)
+                      unsigned flags, uint32_t seed, int v0, int nv, cudaStream_t st, cudaEvent_t* ev,
+                      const uint32_t* pass_seed = nullptr)
 {
     const long long P = g->npix();
     CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
@@ -76,7 +77,7 @@ ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, c
         if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0) + 1], st));
         BpArgs b{};
         b.vol = vol; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = j; b.nview = 1; b.sart = 1;
-        b.flags = flags; b.beta = beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j;
+        b.flags = flags; b.beta = beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j; b.pass_seed = pass_seed;
         CTR_TRY(launch_backproject(*g, b, st));
         if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0) + 2], st));
     }
@@ -84,9 +85,9 @@ ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, c
 }
 
 ctr_status sart_pass(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
-                     unsigned flags, uint32_t seed, cudaStream_t st)
+                     unsigned flags, uint32_t seed, cudaStream_t st, const uint32_t* pass_seed = nullptr)
 {
-    return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, 0, g->desc.n_views, st, nullptr);
+    return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, 0, g->desc.n_views, st, nullptr, pass_seed);
 }
 
 ctr_status objective_async(Geometry* g, const void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt,
@@ -422,6 +423,7 @@ struct ctr_solver {
     int k = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    const void* graph_rays = nullptr;   // the ray workspace the graph was captured with
     double* d_obj = nullptr; // [2] fid, tv
 };
 
@@ -509,6 +511,7 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st)
     const bool stoch = (s->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
     if (!s->p.use_graph || stoch)   // the seed changes every pass: issue directly
         return sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st);
+    if (s->exec && s->graph_rays != s->g->d_rays) drop_graph(s);   // workspace grown by another call
     if (!s->exec) {
         CTR_TRY(ensure_rays(s->g, (size_t)s->g->npix() * sizeof(float2)));
         cudaStream_t cs;
@@ -525,6 +528,7 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st)
             if (e != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
         }
         s->graph = gr;
+        s->graph_rays = s->g->d_rays;
         cudaStreamDestroy(cs);
         if (r != CTR_OK) { drop_graph(s); return r; }
     }
@@ -652,6 +656,233 @@ extern "C" ctr_status ctr_solver_load(ctr_solver* s, const char* path, void* str
     s->k = h.k;
     s->t = h.t;
     return CTR_OK;
+}
+
+// ------------------------------------------------------------ batched scans
+
+// Workspace a solver's iteration needs, allocated before graph capture.
+static ctr_status solver_reserve(ctr_solver* s)
+{
+    Geometry* g = s->g;
+    CTR_TRY(ensure_rays(g, (size_t)g->npix() * sizeof(float2)));
+    if (s->p.lambda_tv > 0.f) CTR_TRY(ensure_fgp(g, 9 * (size_t)g->nvox() * dtype_size(s->vdt)));
+    const DevGeom& q = g->dg;
+    const size_t nblk = (size_t)((q.R + 31) / 32) * ((q.ZP + 3) / 4) * g->desc.n_views;
+    CTR_TRY(ensure_partial(g, std::max(nblk, (size_t)148 * 64) + 2048));
+    return CTR_OK;
+}
+
+// One outer iteration of V63/main_recon.cu:344-430 for one scan on stream st;
+// the FISTA factor and the stochastic-rounding seed of the pass are read from
+// device memory so the launches can be replayed.
+static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_dev, const uint32_t* seed_dev)
+{
+    Geometry* g = s->g;
+    CTR_TRY(sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, st, seed_dev));
+    const float lam = s->p.beta * s->p.lambda_tv;
+    if (s->p.fista) {
+        if (s->p.lambda_tv > 0.f)
+            CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, s->y, s->xprev, 0.f, st, gam_dev));
+        else
+            CTR_TRY(launch_momentum(*g, s->y, s->xprev, s->y, s->vdt, 0.f, st, gam_dev));
+    } else if (s->p.lambda_tv > 0.f) {
+        CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, nullptr, nullptr, 0.f, st));
+    }
+    if (s->p.objective) {
+        const void* xk = s->p.fista ? s->xprev : s->y;
+        CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st));
+    }
+    return CTR_OK;
+}
+
+struct ctr_batch {
+    std::vector<ctr_solver*> scans;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> joins;
+    cudaEvent_t fork = nullptr;
+    float* d_gam = nullptr;                 // per scan FISTA factor of the coming iteration
+    uint32_t* d_seed = nullptr;             // per scan stochastic-rounding seed of the coming pass
+    std::vector<float> h_gam;
+    std::vector<uint32_t> h_seed;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> ws;            // workspaces the graph was captured with, 3 per scan
+};
+
+static std::vector<const void*> batch_workspaces(const ctr_batch* b)
+{
+    std::vector<const void*> w;
+    for (const auto* s : b->scans) {
+        w.push_back(s->g->d_rays);
+        w.push_back(s->g->d_partial);
+        w.push_back(s->g->d_fgp);
+    }
+    return w;
+}
+
+static void batch_drop_graph(ctr_batch* b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+extern "C" ctr_status ctr_batch_destroy(ctr_batch* b)
+{
+    if (!b) return CTR_OK;
+    batch_drop_graph(b);
+    for (auto* s : b->scans) ctr_solver_destroy(s);
+    for (auto st : b->streams) if (st) cudaStreamDestroy(st);
+    for (auto e : b->joins) if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    cudaFree(b->d_gam);
+    cudaFree(b->d_seed);
+    delete b;
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_batch_create(const ctr_geometry* const* geoms, int n, ctr_dtype vdt,
+                                       const ctr_solver_params* p, ctr_batch** out)
+{
+    clear_error();
+    CTR_TRY(need(geoms, "geometries"));
+    CTR_TRY(need(p, "params"));
+    CTR_TRY(need(out, "out"));
+    *out = nullptr;
+    if (n <= 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "need at least one scan");
+    for (int i = 0; i < n; ++i) {
+        if (!geoms[i]) return set_error(CTR_ERR_INVALID_ARGUMENT, "geometry %d is NULL", i);
+        for (int j = 0; j < i; ++j)
+            if (geoms[j] == geoms[i])
+                return set_error(CTR_ERR_INVALID_ARGUMENT, "scans %d and %d share a geometry (workspaces would race)", j, i);
+    }
+    ctr_batch* b = new (std::nothrow) ctr_batch();
+    if (!b) return set_error(CTR_ERR_OUT_OF_MEMORY, "host allocation");
+    ctr_status st = CTR_OK;
+    for (int i = 0; i < n && st == CTR_OK; ++i) {
+        ctr_solver* s = nullptr;
+        st = ctr_solver_create(geoms[i], vdt, p, &s);
+        if (st == CTR_OK) b->scans.push_back(s);
+        cudaStream_t cs = nullptr;
+        cudaEvent_t ev = nullptr;
+        if (st == CTR_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+            st = set_error(CTR_ERR_CUDA, "cudaStreamCreate");
+        b->streams.push_back(cs);
+        if (st == CTR_OK && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            st = set_error(CTR_ERR_CUDA, "cudaEventCreate");
+        b->joins.push_back(ev);
+    }
+    if (st == CTR_OK && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+        st = set_error(CTR_ERR_CUDA, "cudaEventCreate");
+    if (st == CTR_OK && (cudaMalloc(&b->d_gam, sizeof(float) * n) != cudaSuccess ||
+                         cudaMalloc(&b->d_seed, sizeof(uint32_t) * n) != cudaSuccess))
+        st = set_error(CTR_ERR_OUT_OF_MEMORY, "cudaMalloc");
+    b->h_gam.assign(n, 0.f);
+    b->h_seed.assign(n, 0u);
+    if (st != CTR_OK) {
+        ctr_batch_destroy(b);
+        return st;
+    }
+    *out = b;
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_batch_set_sinogram(ctr_batch* b, int scan, const void* sino, ctr_dtype sdt)
+{
+    clear_error();
+    CTR_TRY(need(b, "batch"));
+    if (scan < 0 || scan >= (int)b->scans.size()) return set_error(CTR_ERR_INVALID_ARGUMENT, "scan %d out of range", scan);
+    const void* old = b->scans[scan]->sino;
+    CTR_TRY(ctr_solver_set_sinogram(b->scans[scan], sino, sdt));
+    if (old != sino) batch_drop_graph(b);
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_batch_reset(ctr_batch* b, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(b, "batch"));
+    for (auto* s : b->scans) CTR_TRY(ctr_solver_set_volume(s, nullptr, stream));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* obj_out, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(b, "batch"));
+    if (n < 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "n < 0");
+    const int ns = (int)b->scans.size();
+    for (int i = 0; i < ns; ++i)
+        if (!b->scans[i]->sino) return set_error(CTR_ERR_INVALID_ARGUMENT, "scan %d has no sinogram", i);
+    cudaStream_t st = S(stream);
+    if (b->exec && b->ws != batch_workspaces(b)) batch_drop_graph(b);   // grown by another call
+    if (!b->exec) {
+        for (auto* s : b->scans) CTR_TRY(solver_reserve(s));
+        CTR_CUDA_TRY(cudaDeviceSynchronize());
+        cudaStream_t cs;
+        CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        ctr_status r = CTR_OK;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
+        if (r == CTR_OK && (e = cudaEventRecord(b->fork, cs)) != cudaSuccess) r = cuda_error(e, "cudaEventRecord");
+        for (int i = 0; i < ns && r == CTR_OK; ++i) {
+            if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
+            r = solver_issue(b->scans[i], b->streams[i], b->d_gam + i, b->d_seed + i);
+            if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
+            if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
+        }
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(cs, &gr);
+        if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
+        if (r == CTR_OK && (e = cudaGraphInstantiate(&b->exec, gr, 0)) != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
+        b->graph = gr;
+        b->ws = batch_workspaces(b);
+        cudaStreamDestroy(cs);
+        if (r != CTR_OK) { batch_drop_graph(b); return r; }
+    }
+    for (int it = 0; it < n; ++it) {
+        for (int i = 0; i < ns; ++i) {
+            ctr_solver* s = b->scans[i];
+            const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // V63/main_recon.cu:372
+            b->h_gam[i] = (s->t - 1.0f) / t_k;
+            b->h_seed[i] = (uint32_t)(s->k + 1);   // the single-scan solver's seed of this pass
+        }
+        CTR_CUDA_TRY(cudaMemcpyAsync(b->d_gam, b->h_gam.data(), sizeof(float) * ns, cudaMemcpyHostToDevice, st));
+        CTR_CUDA_TRY(cudaMemcpyAsync(b->d_seed, b->h_seed.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice, st));
+        CTR_CUDA_TRY(cudaGraphLaunch(b->exec, st));
+        for (auto* s : b->scans) {
+            if (s->p.fista) s->t = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;
+            s->k++;
+        }
+        if (obj_out) {
+            std::vector<double> h(2 * (size_t)ns);
+            for (int i = 0; i < ns; ++i)
+                CTR_CUDA_TRY(cudaMemcpyAsync(&h[2 * i], b->scans[i]->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CTR_CUDA_TRY(cudaStreamSynchronize(st));
+            for (int i = 0; i < ns; ++i) {
+                const ctr_solver* s = b->scans[i];
+                double* o = obj_out + ((size_t)i * n + it) * 3;
+                if (s->p.objective) {
+                    o[0] = h[2 * i + 1];
+                    o[1] = h[2 * i];
+                    o[2] = h[2 * i] + 2.0 * (double)s->p.lambda_tv * h[2 * i + 1];
+                } else {
+                    o[0] = o[1] = o[2] = NAN;
+                }
+            }
+        }
+    }
+    for (auto* s : b->scans) CTR_TRY(check_device_errors(s->g, st));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_batch_get_volume(ctr_batch* b, int scan, void* dst, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(b, "batch"));
+    if (scan < 0 || scan >= (int)b->scans.size()) return set_error(CTR_ERR_INVALID_ARGUMENT, "scan %d out of range", scan);
+    return ctr_solver_get_volume(b->scans[scan], dst, stream);
 }
 
 // -------------------------------------------- reference-compatible entry points

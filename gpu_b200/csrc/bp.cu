@@ -115,8 +115,9 @@ __device__ __forceinline__ float rec_d12(const AdjRay& r) { return r.f.y; }
 template <typename VT, typename REC, bool SART, bool STOCH>
 __global__ void __launch_bounds__(BP_THREADS)
 k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ rays, int view0, int accumulate,
-              float beta, uint32_t seed)
+              float beta, uint32_t seed, const uint32_t* __restrict__ pass_seed)
 {
+    if (STOCH && pass_seed) seed = *pass_seed * 0x9E3779B9u + (uint32_t)view0;
     extern __shared__ float sp[];
     const SharedTables T = load_tables(g, sp);
     const int i = blockIdx.x * BP_BX + (threadIdx.x % BP_BX);
@@ -305,15 +306,15 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
             if (a.nview != 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART updates one view at a time");
             if (a.flags & CTR_SART_STOCHASTIC_ROUND)
                 k_backproject<VT, float2, true, true><<<grid, BP_THREADS, smem, st>>>(
-                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed);
+                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, a.pass_seed);
             else
                 k_backproject<VT, float2, true, false><<<grid, BP_THREADS, smem, st>>>(
-                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed);
+                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, nullptr);
         } else if (a.flags & CTR_BP_FOV_MASK) {
             for (int w = 0; w < a.nview; ++w)
                 k_backproject<VT, AdjRay, false, false><<<grid, BP_THREADS, smem, st>>>(
                     g, (VT*)a.vol, (const AdjRay*)a.rays + (size_t)w * G.npix(), a.view0 + w, (acc || w > 0) ? 1 : 0,
-                    0.f, 0u);
+                    0.f, 0u, nullptr);
         } else {
             k_adjoint<VT><<<grid, BP_THREADS, smem, st>>>(g, (VT*)a.vol, (const AdjRay*)a.rays, a.view0, a.nview, acc);
         }

@@ -112,7 +112,8 @@ struct BpArgs {
     int sart;                             // 1: SART update; 0: adjoint
     unsigned flags;                       // CTR_BP_* / CTR_SART_*
     float beta;
-    uint32_t seed;
+    uint32_t seed;                        // stochastic rounding: per-view seed
+    const uint32_t* pass_seed = nullptr;  // if set, the seed is *pass_seed * 0x9E3779B9 + view (device)
 };
 ctr_status launch_backproject(const Geometry& g, const BpArgs& a, cudaStream_t st);
 // Matched-adjoint ray record: f = (value, chord length d12, alpha_lo, alpha_hi),
@@ -131,10 +132,13 @@ ctr_status launch_l2(const float* a, const float* b, long long n, double* partia
                      double* out, cudaStream_t st);
 ctr_status launch_tv(const Geometry& g, const void* vol, ctr_dtype dt, double* partial, size_t cap,
                      double* out, cudaStream_t st);
+// gamma_dev (optional): read the FISTA factor (t_prev-1)/t_k from device
+// memory instead of the argument, so a captured graph can be replayed.
 ctr_status launch_fgp(Geometry& g, void* vol, ctr_dtype dt, float lambda, int iters,
-                      void* fista_y, void* fista_xprev, float fista_gamma, cudaStream_t st);
+                      void* fista_y, void* fista_xprev, float fista_gamma, cudaStream_t st,
+                      const float* gamma_dev = nullptr);
 ctr_status launch_momentum(const Geometry& g, void* y, void* xprev, const void* x, ctr_dtype dt,
-                           float gam, cudaStream_t st);
+                           float gam, cudaStream_t st, const float* gamma_dev = nullptr);
 ctr_status launch_convert(const void* src, ctr_dtype sdt, void* dst, ctr_dtype ddt, long long n,
                           cudaStream_t st);
 ctr_status launch_fdk(Geometry& g, const float* sino, float* vol, cudaStream_t st);

@@ -81,8 +81,9 @@ k_fgp_step(int M, int N, int Z, const T* __restrict__ f, const T* __restrict__ r
 template <typename T, bool FISTA>
 __global__ void __launch_bounds__(256)
 k_fgp_final(int M, int N, int Z, T* __restrict__ vol, const T* __restrict__ o, const T* __restrict__ pd,
-            const T* __restrict__ q, float lambda, T* __restrict__ xprev, float gam)
+            const T* __restrict__ q, float lambda, T* __restrict__ xprev, float gam, const float* __restrict__ gam_dev)
 {
+    if (FISTA && gam_dev) gam = *gam_dev;
     const long long MN = (long long)M * N;
     const long long n = MN * Z;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
@@ -106,8 +107,10 @@ k_fgp_final(int M, int N, int Z, T* __restrict__ vol, const T* __restrict__ o, c
 
 template <typename T>
 __global__ void __launch_bounds__(256)
-k_momentum(long long n, T* __restrict__ y, T* __restrict__ xprev, const T* __restrict__ x, float gam)
+k_momentum(long long n, T* __restrict__ y, T* __restrict__ xprev, const T* __restrict__ x, float gam,
+           const float* __restrict__ gam_dev)
 {
+    if (gam_dev) gam = *gam_dev;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         const float xv = Store<T>::ldw(x + p);
         const float xp = Store<T>::ldw(xprev + p);
@@ -127,7 +130,7 @@ static int grid_for(long long n, int threads)
 static float next_t(float t) { return (1.0f + sqrtf(1.0f + 4.0f * t * t)) / 2.0f; }
 
 ctr_status launch_fgp(Geometry& G, void* vol, ctr_dtype dt, float lambda, int iters, void* fista_y,
-                      void* fista_xprev, float fista_gamma, cudaStream_t st)
+                      void* fista_xprev, float fista_gamma, cudaStream_t st, const float* gamma_dev)
 {
     const int M = G.desc.nx, N = G.desc.ny, Z = G.desc.nz;
     const long long V = G.nvox();
@@ -153,10 +156,10 @@ ctr_status launch_fgp(Geometry& G, void* vol, ctr_dtype dt, float lambda, int it
         if (fista_y) {
             if (fista_y != vol) return set_error(CTR_ERR_INVALID_ARGUMENT, "fused FISTA output must alias the volume");
             k_fgp_final<T, true><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, O[0], O[1], O[2], lambda,
-                                                                    (T*)fista_xprev, fista_gamma);
+                                                                    (T*)fista_xprev, fista_gamma, gamma_dev);
         } else {
             k_fgp_final<T, false><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, O[0], O[1], O[2], lambda,
-                                                                     nullptr, 0.0f);
+                                                                     nullptr, 0.0f, nullptr);
         }
     });
     CTR_CUDA_TRY(cudaGetLastError());
@@ -164,10 +167,12 @@ ctr_status launch_fgp(Geometry& G, void* vol, ctr_dtype dt, float lambda, int it
 }
 
 ctr_status launch_momentum(const Geometry& G, void* y, void* xprev, const void* x, ctr_dtype dt, float gam,
-                           cudaStream_t st)
+                           cudaStream_t st, const float* gamma_dev)
 {
     const long long V = G.nvox();
-    CTR_DISPATCH_DTYPE(dt, T, { k_momentum<T><<<grid_for(V, 256), 256, 0, st>>>(V, (T*)y, (T*)xprev, (const T*)x, gam); });
+    CTR_DISPATCH_DTYPE(dt, T, {
+        k_momentum<T><<<grid_for(V, 256), 256, 0, st>>>(V, (T*)y, (T*)xprev, (const T*)x, gam, gamma_dev);
+    });
     CTR_CUDA_TRY(cudaGetLastError());
     return CTR_OK;
 }

@@ -46,6 +46,8 @@ EXPORTED = [
     "FGP_denoise_GPUx7_exact", "Reconstruction_FDK", "L2_norm_gpu", "TV_norm_gpu",
     "ctr_io_view_filename", "ctr_io_recon_filename", "ctr_io_objective_filename", "ctr_io_write_raw",
     "ctr_io_read_raw", "ctr_io_read_views", "ctr_io_write_views",
+    "ctr_batch_create", "ctr_batch_destroy", "ctr_batch_set_sinogram", "ctr_batch_reset", "ctr_batch_iterate",
+    "ctr_batch_get_volume",
 ]
 
 
@@ -133,6 +135,12 @@ def load_library(path: str = LIB_PATH):
         "ctr_io_read_raw": ([C.c_char_p, vp, C.c_size_t, C.c_size_t], i),
         "ctr_io_read_views": ([C.c_char_p, i, i, i, f, f, i, i, vp], i),
         "ctr_io_write_views": ([C.c_char_p, i, i, i, f, f, i, vp], i),
+        "ctr_batch_create": ([C.POINTER(C.c_void_p), i, i, C.POINTER(SolverParams), C.POINTER(C.c_void_p)], i),
+        "ctr_batch_destroy": ([vp], i),
+        "ctr_batch_set_sinogram": ([vp, i, vp, i], i),
+        "ctr_batch_reset": ([vp, vp], i),
+        "ctr_batch_iterate": ([vp, i, vp, vp], i),
+        "ctr_batch_get_volume": ([vp, i, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -361,6 +369,48 @@ class Solver:
 
     def load(self, path, stream=None):
         check(self.lib.ctr_solver_load(self.h, str(path).encode(), _stream(stream)))
+
+
+class Batch:
+    """Many scans iterated together, one CUDA graph launch per iteration (``ctr_batch``)."""
+
+    def __init__(self, geoms, vol_dtype=F32, beta=0.8, lambda_tv=0.0, fgp_iters=20, fista=True, objective=True,
+                 sart_flags=0):
+        self.geoms = list(geoms)
+        self.lib = load_library()
+        self.params = SolverParams(beta, lambda_tv, fgp_iters, int(fista), int(objective), 1, sart_flags)
+        arr = (C.c_void_p * len(self.geoms))(*[g.h.value for g in self.geoms])
+        h = C.c_void_p()
+        check(self.lib.ctr_batch_create(arr, len(self.geoms), vol_dtype, C.byref(self.params), C.byref(h)))
+        self.h = h
+        self._sinos = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ctr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_sinogram(self, scan, sino):
+        self._sinos[scan] = sino
+        check(self.lib.ctr_batch_set_sinogram(self.h, scan, _ptr(sino), dtype_code(sino)))
+
+    def reset(self, stream=None):
+        check(self.lib.ctr_batch_reset(self.h, _stream(stream)))
+
+    def iterate(self, n, stream=None):
+        obj = np.zeros(len(self.geoms) * max(n, 1) * 3, np.float64)
+        check(self.lib.ctr_batch_iterate(self.h, n, obj.ctypes.data, _stream(stream)))
+        return obj[: len(self.geoms) * n * 3].reshape(len(self.geoms), n, 3)
+
+    def get_volume(self, scan, out, stream=None):
+        check(self.lib.ctr_batch_get_volume(self.h, scan, _ptr(out), _stream(stream)))
+        return out
 
 
 # ---------------------------------------------------------------------------

@@ -234,6 +234,28 @@ ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k);
 ctr_status ctr_solver_save(ctr_solver* s, const char* path, void* stream);
 ctr_status ctr_solver_load(ctr_solver* s, const char* path, void* stream);
 
+/* ------------------------------------------------------------ batched scans */
+
+/* Many independent scans of uneven sizes iterated together: one CUDA graph
+ * launch runs one outer iteration (SART pass, FGP-TV, FISTA, objective) of
+ * every scan, the scans as parallel branches.  Each scan needs its own
+ * geometry handle (workspaces are per geometry).  Per-iteration scalars (the
+ * FISTA factor, the stochastic-rounding seed of the pass) are read from device
+ * memory, so every scan's result is bit-identical to ctr_solver_iterate on the
+ * same inputs.  No counterpart in the reference, which reconstructs one scan
+ * per process. */
+typedef struct ctr_batch ctr_batch;
+ctr_status ctr_batch_create(const ctr_geometry* const* geoms, int n_scans, ctr_dtype vol_dtype,
+                            const ctr_solver_params* params, ctr_batch** out);
+ctr_status ctr_batch_destroy(ctr_batch* b);
+ctr_status ctr_batch_set_sinogram(ctr_batch* b, int scan, const void* sino, ctr_dtype sino_dtype);
+/* zero every estimate and restart FISTA */
+ctr_status ctr_batch_reset(ctr_batch* b, void* stream);
+/* n iterations of every scan; objective_out (host, may be NULL) receives
+ * [scan][iteration][TV, fidelity, objective].  Synchronises. */
+ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* objective_out, void* stream);
+ctr_status ctr_batch_get_volume(ctr_batch* b, int scan, void* dst, void* stream);
+
 /* ------------------------------------------------------------- utilities */
 
 /* Thread-local text of the last failure on this thread ("" if none). */
