@@ -42,9 +42,12 @@ def parse():
                    help="profiling mode: set up the scan, run a SART update of this many views, print timings, exit")
     p.add_argument("--profile-iteration", action="store_true",
                    help="with --profile-views: also run one FP16 solver iteration")
+    p.add_argument("--profile-tune", action="store_true",
+                   help="with --profile-views: also print the tuner's time for every launch shape")
     p.add_argument("--workload", choices=["scan512", "batched"], default="scan512",
                    help="scan512: the 512^3 / 1024-view scan (default); batched: 48 uneven scans in one graph")
     p.add_argument("--scans", type=int, default=48, help="batched: number of scans")
+    p.add_argument("--no-tune", action="store_true", help="batched: keep the default launch shapes")
     p.add_argument("--no-sr", action="store_true", help="batched: BF16 updates rounded to nearest instead of "
                                                         "stochastically")
     return p.parse_args()
@@ -253,6 +256,10 @@ def profile_views(args):
     geom.forward(truth, sino16, 0, nv)
     sino32 = sino16[:n].float()
     out = {}
+    if args.profile_tune:
+        out["tune_f16"] = geom.autotune(gpu_b200.F16, n_views=4)
+        out["tune_f32"] = geom.autotune(gpu_b200.F32, n_views=4)
+        geom.set_shapes(1, 1)
     for name, s in (("f32", sino32), ("f16", sino16)):
         vol = torch.zeros(geom.vol_shape, device="cuda", dtype=s.dtype)
         fp, bp = geom.sart_views(vol, s, BETA, 0, n, timed=True)
@@ -323,6 +330,8 @@ def run_batched(args):
         geoms.append(g)
         sinos.append(sino.to(torch.bfloat16))
         del truth, sino
+        if not args.no_tune:
+            g.autotune(gpu_b200.BF16, n_views=2)
     flags = 0 if args.no_sr else gpu_b200.SART_STOCHASTIC_ROUND
     batch = gpu_b200.Batch(geoms, gpu_b200.BF16, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS,
                            sart_flags=flags)
@@ -371,6 +380,7 @@ def run_batched(args):
         "iter_per_s": 1000.0 / ms,
         "rel_rmse_vs_f32": {"max": max(errs), "median": sorted(errs)[len(errs) // 2]},
         "clocks": clk, "gpu_launches": launches,
+        "launch_shapes": [g.shapes() for g in geoms],
     }
     batch.close()
     print(json.dumps(line), flush=True)
@@ -427,7 +437,9 @@ def main():
 
     runs = {}
     stream = torch.cuda.current_stream()
+    tuned = {}
     for mode, vdt, sdt in (("f32", gpu_b200.F32, torch.float32), ("mixed", mixed_code, mixed_dt)):
+        tuned[mode] = geom.autotune(vdt, n_views=4)      # launch shapes; results do not depend on them
         sino = sino32 if sdt == torch.float32 else sino32.to(sdt)
         solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
                                  objective=True, use_graph=True)
@@ -454,6 +466,7 @@ def main():
     # measured sinogram in from pinned host memory, runs one iteration and reads
     # the objective and the reconstructed volume back
     mode = "mixed"
+    geom.set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
     solver, sino = runs[mode]["solver"], runs[mode]["sino"]
     h_sino = sino.cpu().pin_memory()
     h_vol = torch.empty(vshape, dtype=mixed_dt).pin_memory()
@@ -474,6 +487,7 @@ def main():
     # library records around each launch on this stream (32 views spread over the scan)
     kern = {}
     for mode in ("f32", "mixed"):
+        geom.set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
         sino = runs[mode]["sino"]
         vol = torch.zeros(vshape, device=dev, dtype=torch.float32 if mode == "f32" else mixed_dt)
         geom.sart_views(vol, sino, BETA, 0, 4)                       # warm-up
@@ -522,6 +536,7 @@ def main():
                          "algorithmic_bytes_per_launch": bp_bytes,
                          "launch_ms": bp_ms},
             "kernels_ms": kern,
+            "launch_shapes": tuned,
             "clocks": runs["mixed"]["clocks"],
             "clocks_f32": runs["f32"]["clocks"],
             "gpu_launches": launches_per_step * args.steps,

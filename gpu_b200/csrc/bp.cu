@@ -204,6 +204,173 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
     }
 }
 
+// SART update by voxel-column walk.  A thread owns a run of up to zl voxels
+// of one (i, j) column: the column's xy work -- FOV test, detector-column
+// bounds from the corner projections, the run of detector columns whose
+// rays cross the column and their xy entry/exit alphas -- is done once and
+// kept in registers while the thread walks down its voxels; per voxel only
+// the candidate detector rows and the z alphas of each (column, row) pair
+// remain.  Every voxel sums its rays in the same order as k_backproject
+// (detector column ascending, then row ascending) with the same
+// arithmetic, so the two give bit-identical volumes.
+constexpr int WALK_RUN = 4;   // detector columns of the run kept in registers
+
+template <typename VT, bool STOCH, int BY>
+__global__ void __launch_bounds__(32 * BY)
+k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
+            uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
+{
+    extern __shared__ float sp[];
+    float* PX = sp;
+    float* PY = PX + (g.M + 3);
+    float* PZ = PY + (g.N + 3);
+    float2* RT = reinterpret_cast<float2*>(PZ + ((g.Z + 3 + 1) & ~1));
+    for (int q = threadIdx.x; q < g.M + 3; q += 32 * BY) PX[q] = g.px[q];
+    for (int q = threadIdx.x; q < g.N + 3; q += 32 * BY) PY[q] = g.py[q];
+    for (int q = threadIdx.x; q < g.Z + 3; q += 32 * BY) PZ[q] = g.pz[q];
+    for (int q = threadIdx.x; q < g.ZP; q += 32 * BY) RT[q] = g.rowt[q];
+    __syncthreads();
+    if (STOCH && pass_seed) seed = *pass_seed * 0x9E3779B9u + (uint32_t)view;
+
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * BY + (threadIdx.x >> 5);
+    if (i >= g.M || j >= g.N) return;
+    const int kb = blockIdx.z * zl, ke = min(g.Z, kb + zl);
+
+    // FOV cylinder (universal.cu:626-628): masked voxels keep their value
+    const float ex = fs(fs((float)i, g.fov_h_x), g.m_off);
+    const float ey = fs((float)j, g.fov_h_y);
+    if (fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2) return;
+
+    const float cx = fa(fa(g.bx, fm(g.vx, 0.5f)), fm((float)i, g.vx));   // :592-594
+    const float cy = fa(fa(g.by, fm(g.vy, 0.5f)), fm((float)j, g.vy));
+    const float xlo = PX[i + 1], xhi = PX[i + 2];
+    const float ylo = PY[j + 1], yhi = PY[j + 2];
+    const float2 sc = g.trig[view];
+    const float s = sc.x, c = sc.y;
+
+    // detector-column bounds of the corner projections (universal.cu:639-706)
+    float umin = __int_as_float(0x7f800000), umax = -umin, mlo = umin, mhi = -umin;
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {
+        const float pxc = fs(fa(cx, fm((float)(cc & 1), g.vx)), fm(0.5f, g.vx));
+        const float pyc = fs(fa(cy, fm((float)(cc >> 1), g.vy)), fm(0.5f, g.vy));
+        const float t = fa(fm(pxc, c), fm(pyc, s));
+        const float ss = fa(fm(-pxc, s), fm(pyc, c));
+        const float mt = fdv(fs(t, g.dod), fs(g.dso, t));
+        const float ou = fa(fm(mt, fs(ss, g.srcy)), ss);
+        umin = fminf(umin, ou); umax = fmaxf(umax, ou);
+        mlo = fminf(mlo, mt); mhi = fmaxf(mhi, mt);
+    }
+    int ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
+    int uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
+    if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) return;
+    ulo = max(ulo, 0);
+    uhi = min(uhi, g.R - 1);
+
+    // the run of detector columns whose ray column crosses this voxel column
+    const float4* __restrict__ colt = g.colt + (long long)view * g.R;
+    int ua = uhi + 1, ub = ulo - 1;
+    for (int uu = ulo; uu <= uhi; ++uu) {
+        const float4 ct = __ldg(colt + uu);
+        const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+        const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+        if (fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)) > fmaxf(fminf(ax0, ax1), fminf(ay0, ay1))) {
+            ua = min(ua, uu);
+            ub = uu;
+        }
+    }
+    if (ua > ub) return;
+    float ra[WALK_RUN], rb[WALK_RUN];
+#pragma unroll
+    for (int q = 0; q < WALK_RUN; ++q) {
+        ra[q] = 0.f; rb[q] = 0.f;
+        if (ua + q <= ub) {
+            const float4 ct = __ldg(colt + ua + q);
+            const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+            const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+            ra[q] = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
+            rb[q] = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+        }
+    }
+
+    const int R = g.R;
+    const long long MN = (long long)g.M * g.N;
+    for (int k = kb; k < ke; ++k) {
+        // candidate detector rows of voxel k
+        const float z0 = PZ[k + 1], z1 = PZ[k + 2];
+        const float zlo = fs(z0, g.srcz), zhi = fs(z1, g.srcz);
+        const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
+        const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
+        const float zmn = fminf(fminf(a0, a1), fminf(b0, b1));
+        const float zmx = fmaxf(fmaxf(a0, a1), fmaxf(b0, b1));
+        int vlo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
+        int vhi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
+        if ((vlo < 0 && vhi < 0) || (vlo > g.ZP - 1 && vhi > g.ZP - 1)) continue;
+        vlo = max(vlo, 0);
+        vhi = min(vhi, g.ZP - 1);
+        float sw = 0.f, sl = 0.f;
+        auto pairs = [&](int uu, float a, float bb) {
+            if (!(bb > a)) return;
+            for (int vv = vlo; vv <= vhi; ++vv) {
+                const float2 rt = RT[vv];
+                const float az0 = fm(fs(z0, rt.x), rt.y), az1 = fm(fs(z1, rt.x), rt.y);
+                const float lo = fmaxf(a, fminf(az0, az1));
+                const float hi = fminf(bb, fmaxf(az0, az1));
+                const float2 rec = __ldg(rays + (long long)vv * R + uu);
+                const float temp = fm(rec.y, fs(hi, lo));
+                if (temp > g.thr_bp) {                                         // :785-791
+                    sw = fa(sw, fm(temp, rec.x));
+                    sl = fa(sl, temp);
+                }
+            }
+        };
+#pragma unroll
+        for (int q = 0; q < WALK_RUN; ++q)
+            if (ua + q <= ub) pairs(ua + q, ra[q], rb[q]);
+        for (int uu = ua + WALK_RUN; uu <= ub; ++uu) {
+            const float4 ct = __ldg(colt + uu);
+            const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+            const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+            pairs(uu, fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)));
+        }
+        if (!(sl < g.thr_bp)) {                                                // :799-806
+            VT* p = vol + (long long)k * MN + (long long)j * g.M + i;
+            const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, sw), sl));
+            if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
+            else Store<VT>::st(p, nv);
+        }
+    }
+}
+
+// SART backprojector launch shapes the tuner chooses from: voxel rows per
+// block and the longest z run per thread (shortened for small volumes so
+// that the grid still fills the GPU).
+struct BpShape { int rows, zl; };
+static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8}, {4, 32}, {2, 32}, {8, 32}, {4, 128}, {2, 8}};
+
+template <typename VT, bool STOCH>
+static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStream_t st, size_t smem)
+{
+    const DevGeom& g = G.dg;
+    const BpShape sh = kBpShapes[(G.bp_shape >= 0 && G.bp_shape < BP_SHAPES) ? G.bp_shape : 1];
+    int zl = sh.zl;
+    const long long cols = (long long)g.M * g.N;
+    while (zl > 1 && cols * ((g.Z + zl - 1) / zl) < 148LL * 2048 * 4) zl >>= 1;
+    const dim3 grid((g.M + 31) / 32, (g.N + sh.rows - 1) / sh.rows, (g.Z + zl - 1) / zl);
+    if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
+    const float2* rays = (const float2*)a.rays;
+    switch (sh.rows) {
+    case 2: k_sart_walk<VT, STOCH, 2><<<grid, 64, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                  a.pass_seed, zl); break;
+    case 8: k_sart_walk<VT, STOCH, 8><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                   a.pass_seed, zl); break;
+    default: k_sart_walk<VT, STOCH, 4><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                    a.pass_seed, zl); break;
+    }
+    return CTR_OK;
+}
+
 // Interval of cell n along one axis under the forward traversal: geometric
 // [min(a0,a1), max(a0,a1)], opened at -inf for the start cell, empty behind
 // the start; for a parallel axis (-inf, +inf) at the start cell only.
@@ -304,12 +471,18 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         if (a.sart) {
             if (a.nview != 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART updates one view at a time");
-            if (a.flags & CTR_SART_STOCHASTIC_ROUND)
-                k_backproject<VT, float2, true, true><<<grid, BP_THREADS, smem, st>>>(
-                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, a.pass_seed);
-            else
-                k_backproject<VT, float2, true, false><<<grid, BP_THREADS, smem, st>>>(
-                    g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, nullptr);
+            if (G.bp_shape < 0) {   // the fixed-shape kernel: 8 voxels of a column per thread
+                if (a.flags & CTR_SART_STOCHASTIC_ROUND)
+                    k_backproject<VT, float2, true, true><<<grid, BP_THREADS, smem, st>>>(
+                        g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, a.pass_seed);
+                else
+                    k_backproject<VT, float2, true, false><<<grid, BP_THREADS, smem, st>>>(
+                        g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, nullptr);
+            } else if (a.flags & CTR_SART_STOCHASTIC_ROUND) {
+                CTR_TRY((launch_sart_walk<VT, true>(G, a, st, smem)));
+            } else {
+                CTR_TRY((launch_sart_walk<VT, false>(G, a, st, smem)));
+            }
         } else if (a.flags & CTR_BP_FOV_MASK) {
             for (int w = 0; w < a.nview; ++w)
                 k_backproject<VT, AdjRay, false, false><<<grid, BP_THREADS, smem, st>>>(

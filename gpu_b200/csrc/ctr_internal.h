@@ -44,6 +44,8 @@ struct DevGeom {
 };
 
 enum : unsigned { ERR_TRAVERSAL = 1u };
+constexpr int FP_SHAPES = 3;
+constexpr int BP_SHAPES = 6;
 
 struct Geometry {
     ctr_geometry_desc desc{};
@@ -62,6 +64,9 @@ struct Geometry {
     void* d_fgp = nullptr; size_t fgp_bytes = 0;       // 9 dual arrays
     float* d_fdk = nullptr; size_t fdk_cap = 0;
     float* d_ramp = nullptr;                           // 2R-1 taps
+    // launch shapes (indices into the tuner's tables; results do not depend on them)
+    int fp_shape = 1;                                  // FP rows per block: {2, 4, 8}
+    int bp_shape = 1;                                  // SART BP: see kBpShapes in bp.cu
     long long nvox() const { return (long long)desc.nx * desc.ny * desc.nz; }
     long long npix() const { return (long long)desc.nu * desc.nv; }
 };

@@ -9,7 +9,14 @@
 //     alpha equals the minimum" (the same rule for non-NaN alphas), executed
 //     branch-free, which keeps the 32 lanes of a warp converged;
 //   * the plane coordinates volumn*n+boundary come from shared-memory tables;
-//   * the loop is bounded by nx+ny+nz+3 steps and reports ERR_TRAVERSAL;
+//   * the loop also ends when a voxel index leaves the volume.  Every step
+//     moves at least one index one voxel in its fixed direction (the minimum
+//     of non-NaN alphas equals one of them; all-NaN alphas end the loop), so
+//     a ray takes at most nx+ny+nz+1 steps: the reference's endless loop on
+//     NaN alphas cannot occur;
+//   * blocks are issued centre-out over the detector, so the long rays
+//     through the middle of the volume start first and the last wave holds
+//     short ones;
 //   * the epilogue also writes the chord length of every ray (for the gather
 //     backprojector), or reduces the squared residual in FP64 (objective).
 #include "ctr_device.cuh"
@@ -17,8 +24,16 @@
 namespace ctr {
 
 static constexpr int FP_BX = 32;   // rays along a detector row per block
-static constexpr int FP_BY = 4;    // detector rows per block
+static constexpr int FP_BY = 4;    // detector rows per block of the fixed-shape kernels
 static constexpr int FP_THREADS = FP_BX * FP_BY;
+
+// Tile t of n in centre-out order: c, c+1, c-1, c+2, c-2, ... (c = (n-1)/2),
+// a bijection of [0, n).
+__device__ __forceinline__ int centre_out(int t, int n)
+{
+    const int c = (n - 1) >> 1, d = (t + 1) >> 1;
+    return (t & 1) ? c + d : c - d;
+}
 static constexpr uint64_t kFnvOffset = 1469598103934665603ULL;
 static constexpr uint64_t kFnvPrime = 1099511628211ULL;
 
@@ -190,17 +205,13 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     const float d12 = r.d12;
     float ac = amin, sum = 0.f, len = 0.f;
     double dsum = 0.0;
-    int steps = 0;
     bool any = false;
     // :297-551.  Branch-free step: every axis re-evaluates its next-plane
     // alpha from its (possibly unchanged) index, which reproduces the current
     // value bit for bit when the axis did not move.
-    while (fs(amax, ac) > 1e-16f) {
-        if ((unsigned)vi >= (unsigned)M || (unsigned)vj >= (unsigned)N || (unsigned)vk >= (unsigned)Z) break;
-        if (++steps > g.max_steps) {
-            atomicOr(g.err, ERR_TRAVERSAL);
-            break;
-        }
+    bool go = (fs(amax, ac) > 1e-16f) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
+              ((unsigned)vk < (unsigned)Z);
+    while (go) {
         const float m = fminf(fminf(ax, ay), az);
         const float seg = fm(d12, fs(m, ac));
         len = fa(len, seg);
@@ -223,6 +234,8 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
         ax = fm(fs(PXo[vi], ex1x), eix);
         ay = fm(fs(PYo[vj], ex1y), eiy);
         az = fm(fs(PZo[vk], ex1z), eiz);
+        go = (fs(amax, ac) > 1e-16f) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
+             ((unsigned)vk < (unsigned)Z);
     }
     r.sum = sum;
     r.dsum = dsum;
@@ -234,25 +247,30 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     return r;
 }
 
-template <typename VT, int KIND, bool E64>
-__global__ void __launch_bounds__(FP_THREADS)
+// BY detector rows of 32 rays per block.  The partial sums of the objective
+// and the dot product are per tile (tile_x, tile_y, view), so their order
+// does not depend on the issue order.
+template <typename VT, int KIND, bool E64, int BY>
+__global__ void __launch_bounds__(FP_BX * BY)
 k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
           const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
           uint64_t* __restrict__ hash, float* __restrict__ lens)
 {
+    constexpr int NT = FP_BX * BY;
     extern __shared__ float sp[];
     float* PX = sp;
     float* PY = PX + (g.M + 3);
     float* PZ = PY + (g.N + 3);
     float* PINF = PZ + (g.Z + 3);
-    for (int t = threadIdx.x; t < g.M + 3; t += FP_THREADS) PX[t] = g.px[t];
-    for (int t = threadIdx.x; t < g.N + 3; t += FP_THREADS) PY[t] = g.py[t];
-    for (int t = threadIdx.x; t < g.Z + 3; t += FP_THREADS) PZ[t] = g.pz[t];
+    for (int t = threadIdx.x; t < g.M + 3; t += NT) PX[t] = g.px[t];
+    for (int t = threadIdx.x; t < g.N + 3; t += NT) PY[t] = g.py[t];
+    for (int t = threadIdx.x; t < g.Z + 3; t += NT) PZ[t] = g.pz[t];
     if (threadIdx.x == 0) PINF[0] = __int_as_float(0x7f800000);
     __syncthreads();
 
-    const int u = blockIdx.x * FP_BX + (threadIdx.x % FP_BX);
-    const int v = blockIdx.y * FP_BY + (threadIdx.x / FP_BX);
+    const int tx = centre_out(blockIdx.x, gridDim.x), ty = centre_out(blockIdx.y, gridDim.y);
+    const int u = tx * FP_BX + (threadIdx.x % FP_BX);
+    const int v = ty * BY + (threadIdx.x / FP_BX);
     const int w = blockIdx.z;
     const bool active = (u < g.R) && (v < g.ZP);
     const long long P = (long long)g.R * g.ZP;
@@ -282,40 +300,57 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
         }
     }
     if (KIND == FP_OBJECTIVE || KIND == FP_DOT) {
-        __shared__ double sh[FP_THREADS / 32];
+        __shared__ double sh[BY];
         const double t = block_sum(e2, sh);
-        if (threadIdx.x == 0)
-            partial[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+        if (threadIdx.x == 0) partial[((size_t)blockIdx.z * gridDim.y + ty) * gridDim.x + tx] = t;
     }
 }
 
-template <typename VT, int KIND>
-static void launch_fp_t(const Geometry& G, const FpArgs& a, dim3 grid, size_t smem, cudaStream_t st)
+template <typename VT, int KIND, int BY>
+static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
+    const DevGeom& g = G.dg;
+    const dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + BY - 1) / BY, nview);
     const VT* vol = (const VT*)a.vol;
-    if (G.dg.entry64)
-        k_forward<VT, KIND, true><<<grid, FP_THREADS, smem, st>>>(G.dg, vol, a.view0, a.out, a.out_dtype, a.b,
-                                                                 a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+    if (g.entry64)
+        k_forward<VT, KIND, true, BY><<<grid, FP_BX * BY, smem, st>>>(g, vol, a.view0, a.out, a.out_dtype, a.b,
+                                                                     a.b_dtype, a.partial, a.nseg, a.hash, a.len);
     else
-        k_forward<VT, KIND, false><<<grid, FP_THREADS, smem, st>>>(G.dg, vol, a.view0, a.out, a.out_dtype, a.b,
-                                                                  a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+        k_forward<VT, KIND, false, BY><<<grid, FP_BX * BY, smem, st>>>(g, vol, a.view0, a.out, a.out_dtype, a.b,
+                                                                      a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+}
+
+// Rows per block of the projector shapes the tuner chooses from.
+static constexpr int kFpShapeRows[FP_SHAPES] = {2, 4, 8};
+
+template <typename VT, int KIND>
+static void launch_fp_shape(const Geometry& G, const FpArgs& a, size_t smem, cudaStream_t st)
+{
+    switch (G.fp_shape) {
+    case 0: launch_fp_t<VT, KIND, 2>(G, a, a.nview, smem, st); break;
+    case 2: launch_fp_t<VT, KIND, 8>(G, a, a.nview, smem, st); break;
+    default: launch_fp_t<VT, KIND, 4>(G, a, a.nview, smem, st); break;
+    }
 }
 
 ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, size_t* nblocks_out)
 {
+    static_assert(kFpShapeRows[1] == FP_BY, "shape 1 is the fixed shape");
     const DevGeom& g = G.dg;
     if (a.nview <= 0) return CTR_OK;
     if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
-    dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + FP_BY - 1) / FP_BY, a.nview);
-    if (nblocks_out) *nblocks_out = (size_t)grid.x * grid.y * grid.z;
+    // reductions keep the fixed shape: their partial sums, and so the
+    // rounding of the totals, do not depend on the tuned shape
+    if (nblocks_out)
+        *nblocks_out = (size_t)((g.R + FP_BX - 1) / FP_BX) * ((g.ZP + FP_BY - 1) / FP_BY) * a.nview;
     const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 10);
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         switch (a.kind) {
-        case FP_FORWARD: launch_fp_t<VT, FP_FORWARD>(G, a, grid, smem, st); break;
-        case FP_SART: launch_fp_t<VT, FP_SART>(G, a, grid, smem, st); break;
-        case FP_OBJECTIVE: launch_fp_t<VT, FP_OBJECTIVE>(G, a, grid, smem, st); break;
-        case FP_TRACE: launch_fp_t<VT, FP_TRACE>(G, a, grid, smem, st); break;
-        case FP_DOT: launch_fp_t<VT, FP_DOT>(G, a, grid, smem, st); break;
+        case FP_FORWARD: launch_fp_shape<VT, FP_FORWARD>(G, a, smem, st); break;
+        case FP_SART: launch_fp_shape<VT, FP_SART>(G, a, smem, st); break;
+        case FP_OBJECTIVE: launch_fp_t<VT, FP_OBJECTIVE, FP_BY>(G, a, a.nview, smem, st); break;
+        case FP_TRACE: launch_fp_t<VT, FP_TRACE, FP_BY>(G, a, a.nview, smem, st); break;
+        case FP_DOT: launch_fp_t<VT, FP_DOT, FP_BY>(G, a, a.nview, smem, st); break;
         }
     });
     CTR_CUDA_TRY(cudaGetLastError());

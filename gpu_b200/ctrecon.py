@@ -47,7 +47,7 @@ EXPORTED = [
     "ctr_io_view_filename", "ctr_io_recon_filename", "ctr_io_objective_filename", "ctr_io_write_raw",
     "ctr_io_read_raw", "ctr_io_read_views", "ctr_io_write_views",
     "ctr_batch_create", "ctr_batch_destroy", "ctr_batch_set_sinogram", "ctr_batch_reset", "ctr_batch_iterate",
-    "ctr_batch_get_volume",
+    "ctr_batch_get_volume", "ctr_geometry_set_shapes", "ctr_geometry_get_shapes", "ctr_geometry_autotune",
 ]
 
 
@@ -135,6 +135,9 @@ def load_library(path: str = LIB_PATH):
         "ctr_io_read_raw": ([C.c_char_p, vp, C.c_size_t, C.c_size_t], i),
         "ctr_io_read_views": ([C.c_char_p, i, i, i, f, f, i, i, vp], i),
         "ctr_io_write_views": ([C.c_char_p, i, i, i, f, f, i, vp], i),
+        "ctr_geometry_set_shapes": ([G, i, i], i),
+        "ctr_geometry_get_shapes": ([G, C.POINTER(i), C.POINTER(i)], i),
+        "ctr_geometry_autotune": ([G, i, i, C.POINTER(f), C.POINTER(f), vp], i),
         "ctr_batch_create": ([C.POINTER(C.c_void_p), i, i, C.POINTER(SolverParams), C.POINTER(C.c_void_p)], i),
         "ctr_batch_destroy": ([vp], i),
         "ctr_batch_set_sinogram": ([vp, i, vp, i], i),
@@ -304,6 +307,28 @@ class Geometry:
         p = np.ascontiguousarray(params, np.float64)
         check(self.lib.ctr_phantom_voxelize(self.h, p.ctypes.data, p.shape[0], _ptr(vol), _stream(stream)))
         return vol
+
+    FP_SHAPES = 3
+    BP_SHAPES = 6
+
+    def set_shapes(self, fp_shape, bp_shape):
+        """Launch shapes of the SART projectors (``ctr_geometry_set_shapes``)."""
+        check(self.lib.ctr_geometry_set_shapes(self.h, fp_shape, bp_shape))
+
+    def shapes(self):
+        a, b = C.c_int(), C.c_int()
+        check(self.lib.ctr_geometry_get_shapes(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, vol_dtype=F32, n_views=4, stream=None):
+        """Time every projector shape on n_views views and keep the fastest;
+        returns {"fp_ms": [...], "bp_ms": {shape: ms}, "fp_shape": s, "bp_shape": s}."""
+        fp = (C.c_float * self.FP_SHAPES)()
+        bp = (C.c_float * (self.BP_SHAPES + 1))()
+        check(self.lib.ctr_geometry_autotune(self.h, vol_dtype, n_views, fp, bp, _stream(stream)))
+        f, b = self.shapes()
+        return {"fp_ms": list(fp), "bp_ms": {s - 1: bp[s] for s in range(self.BP_SHAPES + 1)}, "fp_shape": f,
+                "bp_shape": b}
 
 
 def l2_norm(a, b, stream=None):

@@ -84,6 +84,22 @@ ctr_status ctr_geometry_destroy(ctr_geometry* geom);
  * (V63/host_IterativeRecon_CBCT.c:34-41), as the kernels use them. */
 ctr_status ctr_geometry_view_trig(const ctr_geometry* geom, int view, float* sin_out, float* cos_out);
 
+/* Launch shapes of the SART projectors.  fp_shape 0..2: 32 x {2, 4, 8} rays
+ * per block.  bp_shape -1: the fixed-shape backprojector (8 voxels of a
+ * column per thread); 0..5: the column walk with (voxel rows per block, z
+ * run) = (4,8) (4,32) (2,32) (8,32) (4,128) (2,8).  Results never depend on
+ * the shape.  Defaults: fp_shape 1, bp_shape 1.  Not thread-safe against
+ * launches on the same geometry. */
+ctr_status ctr_geometry_set_shapes(ctr_geometry* geom, int fp_shape, int bp_shape);
+ctr_status ctr_geometry_get_shapes(const ctr_geometry* geom, int* fp_shape, int* bp_shape);
+/* Time every shape on n_views views spread over the scan (SART forward
+ * projection, then SART backprojection into a scratch volume of vol_dtype)
+ * and keep the fastest.  fp_ms[3] and bp_ms[7] (may be NULL) receive the mean
+ * milliseconds per view of each shape; bp_ms[0] is bp_shape -1.  Allocates a
+ * scratch volume and one sinogram view; synchronises the stream. */
+ctr_status ctr_geometry_autotune(ctr_geometry* geom, ctr_dtype vol_dtype, int n_views, float* fp_ms, float* bp_ms,
+                                 void* stream);
+
 /* ---------------------------------------------------------------- projectors */
 
 /* sino[w] = A_(view_begin+w) vol for w < view_count (Siddon ray sums, command 0
