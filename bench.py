@@ -262,7 +262,7 @@ def profile_views(args):
         geom.set_shapes(1, 1)
     for name, s in (("f32", sino32), ("f16", sino16)):
         vol = torch.zeros(geom.vol_shape, device="cuda", dtype=s.dtype)
-        fp, bp = geom.sart_views(vol, s, BETA, 0, n, timed=True)
+        fp, bp = geom.sart_views(vol, s, BETA, 0, n, flags=gpu_b200.SART_TILED, timed=True)
         out[name] = {"fp_ms_per_view": fp / n, "bp_ms_per_view": bp / n}
         del vol
     del truth
@@ -490,11 +490,12 @@ def main():
         geom.set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
         sino = runs[mode]["sino"]
         vol = torch.zeros(vshape, device=dev, dtype=torch.float32 if mode == "f32" else mixed_dt)
-        geom.sart_views(vol, sino, BETA, 0, 4)                       # warm-up
+        tl = gpu_b200.SART_TILED                                      # the solver's layout
+        geom.sart_views(vol, sino, BETA, 0, 4, flags=tl)              # warm-up
         fp_t = bp_t = 0.0
         nt = 32
         for j in range(nt):
-            f_ms, b_ms = geom.sart_views(vol, sino, BETA, (j * 97) % SCAN["n_views"], 1, timed=True)
+            f_ms, b_ms = geom.sart_views(vol, sino, BETA, (j * 97) % SCAN["n_views"], 1, flags=tl, timed=True)
             fp_t += f_ms
             bp_t += b_ms
         kern[mode] = {"fp_ms": fp_t / nt, "bp_ms": bp_t / nt}
@@ -529,7 +530,7 @@ def main():
             "objective_last": {"f32": runs["f32"]["objective_last"], "mixed": runs["mixed"]["objective_last"]},
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "iter/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "kernel": "k_backproject (SART update, f16 volume)",
+            "roofline": {"bound": "hbm", "kernel": "k_sart_walk (SART update, f16 volume, tiled layout)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind,
                          "traffic": (traffic or {}).get("bytes_per_launch"),

@@ -62,36 +62,45 @@ ctr_status forward_chunks(Geometry* g, FpArgs a, cudaStream_t st)
 
 // SART pass: per view FP command 1 -> ray records, then BP command 1.
 // With ev (3 events per view) the launches are bracketed for timing.
+// With tiled (a scratch of tiled_count elements) the views run on an 8x8-tiled
+// copy of the volume, copied in before and out after; the result is the same.
 ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
                       unsigned flags, uint32_t seed, int v0, int nv, cudaStream_t st, cudaEvent_t* ev,
-                      const uint32_t* pass_seed = nullptr)
+                      const uint32_t* pass_seed = nullptr, void* tiled = nullptr)
 {
     const long long P = g->npix();
     CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
+    void* pv = tiled ? tiled : vol;
+    if (tiled) CTR_TRY(launch_tiling(*g, vol, tiled, vdt, true, st));
     for (int j = v0; j < v0 + nv; ++j) {
         if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0)], st));
         FpArgs a{};
-        a.vol = vol; a.vol_dtype = vdt; a.view0 = j; a.nview = 1; a.kind = FP_SART;
+        a.vol = pv; a.vol_dtype = vdt; a.view0 = j; a.nview = 1; a.kind = FP_SART; a.tiled = tiled != nullptr;
         a.out = g->d_rays; a.b = (const char*)sino + (size_t)j * P * dtype_size(sdt); a.b_dtype = sdt;
         CTR_TRY(launch_forward(*g, a, st, nullptr));
         if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0) + 1], st));
         BpArgs b{};
-        b.vol = vol; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = j; b.nview = 1; b.sart = 1;
+        b.vol = pv; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = j; b.nview = 1; b.sart = 1;
         b.flags = flags; b.beta = beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j; b.pass_seed = pass_seed;
+        b.tiled = tiled != nullptr;
         CTR_TRY(launch_backproject(*g, b, st));
         if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0) + 2], st));
     }
+    if (tiled) CTR_TRY(launch_tiling(*g, tiled, vol, vdt, false, st));
     return CTR_OK;
 }
 
 ctr_status sart_pass(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
-                     unsigned flags, uint32_t seed, cudaStream_t st, const uint32_t* pass_seed = nullptr)
+                     unsigned flags, uint32_t seed, cudaStream_t st, const uint32_t* pass_seed = nullptr,
+                     void* tiled = nullptr)
 {
-    return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, 0, g->desc.n_views, st, nullptr, pass_seed);
+    return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, 0, g->desc.n_views, st, nullptr, pass_seed, tiled);
 }
 
+// Fidelity ||A x - b||^2 (per-block FP64 partials, two-level reduction) and TV
+// of x.  With tiled, the projection reads an 8x8-tiled copy of x made there.
 ctr_status objective_async(Geometry* g, const void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt,
-                           double* d_fid, double* d_tv, cudaStream_t st)
+                           double* d_fid, double* d_tv, cudaStream_t st, void* tiled = nullptr)
 {
     const DevGeom& q = g->dg;
     const size_t per_view = (size_t)((q.R + 31) / 32) * ((q.ZP + 3) / 4);
@@ -99,8 +108,10 @@ ctr_status objective_async(Geometry* g, const void* vol, ctr_dtype vdt, const vo
     const size_t tvcap = 148 * 64;
     CTR_TRY(ensure_partial(g, std::max(nblk, tvcap) + 2048));
     if (d_fid) {
+        if (tiled) CTR_TRY(launch_tiling(*g, vol, tiled, vdt, true, st));
         FpArgs a{};
-        a.vol = vol; a.vol_dtype = vdt; a.view0 = 0; a.nview = g->desc.n_views; a.kind = FP_OBJECTIVE;
+        a.vol = tiled ? tiled : vol; a.vol_dtype = vdt; a.view0 = 0; a.nview = g->desc.n_views;
+        a.kind = FP_OBJECTIVE; a.tiled = tiled != nullptr;
         a.b = sino; a.b_dtype = sdt; a.partial = g->d_partial;
         const long long P = g->npix();
         for (int c = 0; c < g->desc.n_views; c += 65535) {
@@ -177,7 +188,13 @@ extern "C" ctr_status ctr_sart_pass(const ctr_geometry* geom, void* vol, ctr_dty
     CTR_TRY(need_dtype(vdt, "vol_dtype"));
     CTR_TRY(need_dtype(sdt, "sino_dtype"));
     if (!std::isfinite(beta)) return set_error(CTR_ERR_INVALID_ARGUMENT, "beta must be finite");
-    return sart_pass(GE(geom), vol, vdt, sino, sdt, beta, flags, seed, S(stream));
+    Geometry* g = GE(geom);
+    void* tiled = nullptr;
+    if (flags & CTR_SART_TILED) {
+        CTR_TRY(ensure_tiled(g, (size_t)tiled_count(g->dg) * dtype_size(vdt)));
+        tiled = g->d_tiled;
+    }
+    return sart_pass(g, vol, vdt, sino, sdt, beta, flags, seed, S(stream), nullptr, tiled);
 }
 
 extern "C" ctr_status ctr_sart_views(const ctr_geometry* geom, void* vol, ctr_dtype vdt, const void* sino,
@@ -194,12 +211,18 @@ extern "C" ctr_status ctr_sart_views(const ctr_geometry* geom, void* vol, ctr_dt
     CTR_TRY(check_views(g, v0, n));
     if (!std::isfinite(beta)) return set_error(CTR_ERR_INVALID_ARGUMENT, "beta must be finite");
     cudaStream_t st = S(stream);
-    if (!fp_ms && !bp_ms) return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, v0, n, st, nullptr);
+    void* tiled = nullptr;
+    if (flags & CTR_SART_TILED) {
+        CTR_TRY(ensure_tiled(g, (size_t)tiled_count(g->dg) * dtype_size(vdt)));
+        tiled = g->d_tiled;
+    }
+    if (!fp_ms && !bp_ms)
+        return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, v0, n, st, nullptr, nullptr, tiled);
     std::vector<cudaEvent_t> ev(3 * (size_t)n, nullptr);
     ctr_status r = CTR_OK;
     for (auto& e : ev)
         if (r == CTR_OK && cudaEventCreate(&e) != cudaSuccess) r = set_error(CTR_ERR_CUDA, "cudaEventCreate");
-    if (r == CTR_OK) r = sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, v0, n, st, ev.data());
+    if (r == CTR_OK) r = sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, v0, n, st, ev.data(), nullptr, tiled);
     if (r == CTR_OK && cudaStreamSynchronize(st) != cudaSuccess) r = set_error(CTR_ERR_CUDA, "cudaStreamSynchronize");
     float tf = 0.f, tb = 0.f;
     for (int j = 0; r == CTR_OK && j < n; ++j) {
@@ -419,6 +442,7 @@ struct ctr_solver {
     ctr_dtype sdt = CTR_F32;
     void* y = nullptr;       // working volume: y_k, then x_k during an iteration
     void* xprev = nullptr;   // x_(k-1); after an iteration with FISTA, x_k
+    void* yt = nullptr;      // 8x8-tiled scratch copy for the projections
     float t = 1.0f;          // t_(k-1) of V63/main_recon.cu:177
     int k = 0;
     cudaGraph_t graph = nullptr;
@@ -446,6 +470,7 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
     const size_t bytes = s->g->nvox() * dtype_size(vdt);
     cudaError_t e;
     if ((e = cudaMalloc(&s->y, bytes)) != cudaSuccess || (e = cudaMalloc(&s->xprev, bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&s->yt, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess ||
         (e = cudaMalloc(&s->d_obj, 4 * sizeof(double))) != cudaSuccess || (e = cudaMemset(s->y, 0, bytes)) != cudaSuccess ||
         (e = cudaMemset(s->xprev, 0, bytes)) != cudaSuccess) {
         ctr_status st = cuda_error(e, "solver allocation");
@@ -470,6 +495,7 @@ extern "C" ctr_status ctr_solver_destroy(ctr_solver* s)
     drop_graph(s);
     cudaFree(s->y);
     cudaFree(s->xprev);
+    cudaFree(s->yt);
     cudaFree(s->d_obj);
     delete s;
     return CTR_OK;
@@ -510,7 +536,7 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st)
 {
     const bool stoch = (s->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
     if (!s->p.use_graph || stoch)   // the seed changes every pass: issue directly
-        return sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st);
+        return sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st, nullptr, s->yt);
     if (s->exec && s->graph_rays != s->g->d_rays) drop_graph(s);   // workspace grown by another call
     if (!s->exec) {
         CTR_TRY(ensure_rays(s->g, (size_t)s->g->npix() * sizeof(float2)));
@@ -519,7 +545,8 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st)
         cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         ctr_status r = CTR_OK;
         if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
-        if (r == CTR_OK) r = sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, cs);
+        if (r == CTR_OK)
+            r = sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, cs, nullptr, s->yt);
         cudaGraph_t gr = nullptr;
         e = cudaStreamEndCapture(cs, &gr);
         if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
@@ -562,7 +589,7 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
         s->k++;
         if (s->p.objective) {
             const void* xk = s->p.fista ? s->xprev : s->y;
-            CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st));
+            CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
             if (obj_out) {
                 double h[2];
                 CTR_CUDA_TRY(cudaMemcpyAsync(h, s->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -678,7 +705,7 @@ static ctr_status solver_reserve(ctr_solver* s)
 static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_dev, const uint32_t* seed_dev)
 {
     Geometry* g = s->g;
-    CTR_TRY(sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, st, seed_dev));
+    CTR_TRY(sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, st, seed_dev, s->yt));
     const float lam = s->p.beta * s->p.lambda_tv;
     if (s->p.fista) {
         if (s->p.lambda_tv > 0.f)
@@ -690,7 +717,7 @@ static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_
     }
     if (s->p.objective) {
         const void* xk = s->p.fista ? s->xprev : s->y;
-        CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st));
+        CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
     }
     return CTR_OK;
 }

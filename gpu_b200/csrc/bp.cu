@@ -204,6 +204,28 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
     }
 }
 
+// z alphas of every (cell k, detector row v) pair, ordered: the values the
+// gather backprojectors otherwise compute per pair from the row table,
+// (plane - x1z) * (1/dz) for the cell's two planes.
+__global__ void k_zcell(const DevGeom g, float2* __restrict__ zcell)
+{
+    const long long n = (long long)g.Z * g.ZP;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / g.ZP), v = (int)(t % g.ZP);
+        const float2 rt = g.rowt[v];
+        const float az0 = fm(fs(g.pz[k + 1], rt.x), rt.y), az1 = fm(fs(g.pz[k + 2], rt.x), rt.y);
+        zcell[t] = make_float2(fminf(az0, az1), fmaxf(az0, az1));
+    }
+}
+
+ctr_status launch_zcell(const Geometry& G, float2* zcell, cudaStream_t st)
+{
+    const long long n = (long long)G.dg.Z * G.dg.ZP;
+    k_zcell<<<(int)std::min<long long>((n + 255) / 256, 148LL * 64), 256, 0, st>>>(G.dg, zcell);
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
 // SART update by voxel-column walk.  A thread owns a run of up to zl voxels
 // of one (i, j) column: the column's xy work -- FOV test, detector-column
 // bounds from the corner projections, the run of detector columns whose
@@ -215,7 +237,7 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
 // arithmetic, so the two give bit-identical volumes.
 constexpr int WALK_RUN = 4;   // detector columns of the run kept in registers
 
-template <typename VT, bool STOCH, int BY>
+template <typename VT, bool STOCH, int BY, int UNR, bool TL>
 __global__ void __launch_bounds__(32 * BY)
 k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
             uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
@@ -310,20 +332,29 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         vlo = max(vlo, 0);
         vhi = min(vhi, g.ZP - 1);
         float sw = 0.f, sl = 0.f;
+        const float2* __restrict__ zrow = g.zcell + (long long)k * g.ZP;
+        auto pair = [&](float a, float bb, float2 zc, float2 rec) {
+            const float lo = fmaxf(a, zc.x);
+            const float hi = fminf(bb, zc.y);
+            const float temp = fm(rec.y, fs(hi, lo));
+            if (temp > g.thr_bp) {                                             // :785-791
+                sw = fa(sw, fm(temp, rec.x));
+                sl = fa(sl, temp);
+            }
+        };
         auto pairs = [&](int uu, float a, float bb) {
             if (!(bb > a)) return;
-            for (int vv = vlo; vv <= vhi; ++vv) {
-                const float2 rt = RT[vv];
-                const float az0 = fm(fs(z0, rt.x), rt.y), az1 = fm(fs(z1, rt.x), rt.y);
-                const float lo = fmaxf(a, fminf(az0, az1));
-                const float hi = fminf(bb, fmaxf(az0, az1));
-                const float2 rec = __ldg(rays + (long long)vv * R + uu);
-                const float temp = fm(rec.y, fs(hi, lo));
-                if (temp > g.thr_bp) {                                         // :785-791
-                    sw = fa(sw, fm(temp, rec.x));
-                    sl = fa(sl, temp);
+            int vv = vlo;
+            if (UNR == 2) {   // both rows' loads first, then the pairs in row order
+                for (; vv < vhi; vv += 2) {
+                    const float2 z0c = __ldg(zrow + vv), z1c = __ldg(zrow + vv + 1);
+                    const float2 r0 = __ldg(rays + (long long)vv * R + uu);
+                    const float2 r1 = __ldg(rays + (long long)(vv + 1) * R + uu);
+                    pair(a, bb, z0c, r0);
+                    pair(a, bb, z1c, r1);
                 }
             }
+            for (; vv <= vhi; ++vv) pair(a, bb, __ldg(zrow + vv), __ldg(rays + (long long)vv * R + uu));
         };
 #pragma unroll
         for (int q = 0; q < WALK_RUN; ++q)
@@ -335,7 +366,7 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
             pairs(uu, fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)));
         }
         if (!(sl < g.thr_bp)) {                                                // :799-806
-            VT* p = vol + (long long)k * MN + (long long)j * g.M + i;
+            VT* p = vol + (TL ? (long long)tile_index(g, i, j, k) : (long long)k * MN + (long long)j * g.M + i);
             const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, sw), sl));
             if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
             else Store<VT>::st(p, nv);
@@ -343,31 +374,66 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
     }
 }
 
+// Linear <-> 8x8-tiled copies of a volume (same storage type).  One thread
+// per tiled element; padding elements are written as zero.
+template <typename T, bool TO_TILED>
+__global__ void k_tiling(const DevGeom g, const T* __restrict__ src, T* __restrict__ dst)
+{
+    const long long n = tiled_count(g);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int w = (int)(t & 63);
+        const long long tile = t >> 6;
+        const int tx = (int)(tile % g.Mt);
+        const long long r = tile / g.Mt;
+        const int ty = (int)(r % g.Nt);
+        const int k = (int)(r / g.Nt);
+        const int i = tx * 8 + (w & 7), j = ty * 8 + (w >> 3);
+        const bool in = i < g.M && j < g.N;
+        const long long lin = ((long long)k * g.N + j) * g.M + i;
+        if (TO_TILED) dst[t] = in ? src[lin] : T(0.0f);
+        else if (in) dst[lin] = src[t];
+    }
+}
+
+ctr_status launch_tiling(const Geometry& G, const void* src, void* dst, ctr_dtype dt, bool to_tiled, cudaStream_t st)
+{
+    const long long n = tiled_count(G.dg);
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 32);
+    CTR_DISPATCH_DTYPE(dt, T, {
+        if (to_tiled) k_tiling<T, true><<<blocks, 256, 0, st>>>(G.dg, (const T*)src, (T*)dst);
+        else k_tiling<T, false><<<blocks, 256, 0, st>>>(G.dg, (const T*)src, (T*)dst);
+    });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
 // SART backprojector launch shapes the tuner chooses from: voxel rows per
 // block and the longest z run per thread (shortened for small volumes so
 // that the grid still fills the GPU).
-struct BpShape { int rows, zl; };
-static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8}, {4, 32}, {2, 32}, {8, 32}, {4, 128}, {2, 8}};
+struct BpShape { int rows, zl, unroll; };
+static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8, 1}, {4, 32, 1}, {4, 32, 2}, {8, 32, 1}, {4, 128, 1},
+                                                 {4, 128, 2}};
 
-template <typename VT, bool STOCH>
+template <typename VT, bool STOCH, bool TL>
 static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStream_t st, size_t smem)
 {
     const DevGeom& g = G.dg;
     const BpShape sh = kBpShapes[(G.bp_shape >= 0 && G.bp_shape < BP_SHAPES) ? G.bp_shape : 1];
     int zl = sh.zl;
     const long long cols = (long long)g.M * g.N;
-    while (zl > 1 && cols * ((g.Z + zl - 1) / zl) < 148LL * 2048 * 4) zl >>= 1;
+    while (zl > 1 && cols * ((g.Z + zl - 1) / zl) < 148LL * 2048) zl >>= 1;   // about two waves at least
     const dim3 grid((g.M + 31) / 32, (g.N + sh.rows - 1) / sh.rows, (g.Z + zl - 1) / zl);
     if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
     const float2* rays = (const float2*)a.rays;
-    switch (sh.rows) {
-    case 2: k_sart_walk<VT, STOCH, 2><<<grid, 64, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                                  a.pass_seed, zl); break;
-    case 8: k_sart_walk<VT, STOCH, 8><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                                   a.pass_seed, zl); break;
-    default: k_sart_walk<VT, STOCH, 4><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                                    a.pass_seed, zl); break;
-    }
+    if (sh.rows == 8)
+        k_sart_walk<VT, STOCH, 8, 1, TL><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                  a.pass_seed, zl);
+    else if (sh.unroll == 2)
+        k_sart_walk<VT, STOCH, 4, 2, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                  a.pass_seed, zl);
+    else
+        k_sart_walk<VT, STOCH, 4, 1, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                  a.pass_seed, zl);
     return CTR_OK;
 }
 
@@ -471,7 +537,10 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         if (a.sart) {
             if (a.nview != 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART updates one view at a time");
-            if (G.bp_shape < 0) {   // the fixed-shape kernel: 8 voxels of a column per thread
+            if (a.tiled) {
+                if (a.flags & CTR_SART_STOCHASTIC_ROUND) CTR_TRY((launch_sart_walk<VT, true, true>(G, a, st, smem)));
+                else CTR_TRY((launch_sart_walk<VT, false, true>(G, a, st, smem)));
+            } else if (G.bp_shape < 0) {   // the fixed-shape kernel: 8 voxels of a column per thread
                 if (a.flags & CTR_SART_STOCHASTIC_ROUND)
                     k_backproject<VT, float2, true, true><<<grid, BP_THREADS, smem, st>>>(
                         g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, a.pass_seed);
@@ -479,9 +548,9 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
                     k_backproject<VT, float2, true, false><<<grid, BP_THREADS, smem, st>>>(
                         g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, nullptr);
             } else if (a.flags & CTR_SART_STOCHASTIC_ROUND) {
-                CTR_TRY((launch_sart_walk<VT, true>(G, a, st, smem)));
+                CTR_TRY((launch_sart_walk<VT, true, false>(G, a, st, smem)));
             } else {
-                CTR_TRY((launch_sart_walk<VT, false>(G, a, st, smem)));
+                CTR_TRY((launch_sart_walk<VT, false, false>(G, a, st, smem)));
             }
         } else if (a.flags & CTR_BP_FOV_MASK) {
             for (int w = 0; w < a.nview; ++w)

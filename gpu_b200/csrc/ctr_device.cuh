@@ -98,6 +98,12 @@ __device__ __forceinline__ double block_sum(double v, double* sh)
     return r;
 }
 
+// Index of voxel (i, j, k) in the 8x8-tiled layout.
+__device__ __forceinline__ int tile_index(const DevGeom& g, int i, int j, int k)
+{
+    return (((k * g.Nt) + (j >> 3)) * g.Mt + (i >> 3)) * 64 + ((j & 7) << 3) + (i & 7);
+}
+
 // Dispatch a runtime ctr_dtype to a storage type.
 #define CTR_DISPATCH_DTYPE(dt, T, ...)                      \
     switch (dt) {                                           \

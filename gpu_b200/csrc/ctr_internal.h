@@ -19,6 +19,7 @@ struct DevGeom {
     int R, ZP;              // detector columns, rows
     int nviews;
     int max_steps;          // Siddon step bound nx+ny+nz+3
+    int Mt, Nt;             // 8x8 (x, y) tiles per row / column of the tiled layout
     int entry64;            // FP64 ray-box entry/exit
     float vx, vy, vz, inv_vx, inv_vy, inv_vz;
     float bx, by, bz;       // boundary_voxel_*
@@ -40,11 +41,12 @@ struct DevGeom {
     const float2* trig_fdk; // [view] (sin, cos) of the FDK frame angle
     const float4* colt;     // [view][u] (x1x, 1/dx, x1y, 1/dy), parallel axes encoded
     const float2* rowt;     // [v] (x1z, 1/dz), parallel rows encoded
+    const float2* zcell;    // [k][v] (min, max) of the z alphas of cell k's planes for row v
     unsigned int* err;      // device error bits (ERR_*)
 };
 
 enum : unsigned { ERR_TRAVERSAL = 1u };
-constexpr int FP_SHAPES = 3;
+constexpr int FP_SHAPES = 7;
 constexpr int BP_SHAPES = 6;
 
 struct Geometry {
@@ -56,6 +58,7 @@ struct Geometry {
     // device allocations
     void* d_tables = nullptr;  // px,py,pz,trig,trig_fdk,rowt
     float4* d_colt = nullptr;
+    float2* d_zcell = nullptr;
     unsigned* d_err = nullptr;
     // workspace
     void* d_rays = nullptr;  size_t rays_cap = 0;       // ray records (float2 SART / AdjRay adjoint)
@@ -63,9 +66,10 @@ struct Geometry {
     double* d_result = nullptr;                        // 8 doubles
     void* d_fgp = nullptr; size_t fgp_bytes = 0;       // 9 dual arrays
     float* d_fdk = nullptr; size_t fdk_cap = 0;
+    void* d_tiled = nullptr; size_t tiled_bytes = 0;   // tiled copy for CTR_SART_TILED
     float* d_ramp = nullptr;                           // 2R-1 taps
     // launch shapes (indices into the tuner's tables; results do not depend on them)
-    int fp_shape = 1;                                  // FP rows per block: {2, 4, 8}
+    int fp_shape = 1;                                  // FP: see kFpShapes in fp.cu
     int bp_shape = 1;                                  // SART BP: see kBpShapes in bp.cu
     long long nvox() const { return (long long)desc.nx * desc.ny * desc.nz; }
     long long npix() const { return (long long)desc.nu * desc.nv; }
@@ -94,6 +98,7 @@ inline bool dtype_ok(int t) { return t == CTR_F32 || t == CTR_BF16 || t == CTR_F
 ctr_status ensure_rays(Geometry* g, size_t bytes);
 ctr_status ensure_partial(Geometry* g, size_t n);
 ctr_status ensure_fgp(Geometry* g, size_t bytes);
+ctr_status ensure_tiled(Geometry* g, size_t bytes);
 ctr_status check_device_errors(Geometry* g, cudaStream_t st);
 
 // ---- kernel launchers (implemented in the .cu files) ----
@@ -106,6 +111,7 @@ struct FpArgs {
     const void* b; ctr_dtype b_dtype;     // SART/OBJECTIVE: measured sinogram; DOT: y (offset to view0)
     double* partial;                      // OBJECTIVE/DOT: one double per block
     int* nseg; uint64_t* hash; float* len;  // TRACE
+    int tiled = 0;                        // vol in the 8x8-tiled layout (FORWARD, SART, OBJECTIVE)
 };
 ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, size_t* nblocks_out);
 
@@ -119,8 +125,18 @@ struct BpArgs {
     float beta;
     uint32_t seed;                        // stochastic rounding: per-view seed
     const uint32_t* pass_seed = nullptr;  // if set, the seed is *pass_seed * 0x9E3779B9 + view (device)
+    int tiled = 0;                        // vol in the 8x8-tiled layout (SART only)
 };
 ctr_status launch_backproject(const Geometry& g, const BpArgs& a, cudaStream_t st);
+// The tiled volume layout of the solver's projections: 8x8 tiles in (x, y),
+// tile-major within a z slice, so the 32 rays of a warp, which lie side by
+// side across the beam, touch a few 128-byte lines instead of one per ray.
+// Voxels of the padding (x >= nx or y >= ny in the last tiles) are never read
+// or written by the projectors.
+__host__ __device__ inline long long tiled_count(const DevGeom& g) { return (long long)g.Z * g.Nt * g.Mt * 64; }
+ctr_status launch_tiling(const Geometry& g, const void* src, void* dst, ctr_dtype dt, bool to_tiled, cudaStream_t st);
+// fills dg.zcell (view-independent: the rows' z and the source height do not turn)
+ctr_status launch_zcell(const Geometry& g, float2* zcell, cudaStream_t st);
 // Matched-adjoint ray record: f = (value, chord length d12, alpha_lo, alpha_hi),
 // i = (start voxel i, j, k, parallel-axis bits).
 struct __align__(16) AdjRay {

@@ -47,6 +47,20 @@ struct RayResult {
     uint64_t hash;
 };
 
+// Shared plane tables with one padding entry before and after each table,
+// then the +inf slot: 1 + (M+3) + 2 + (N+3) + 2 + (Z+3) + 1 + 1 floats.
+__device__ __forceinline__ void plane_tables_layout(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
+                                                    float*& PINF)
+{
+    PX = sp + 1;
+    PY = PX + (g.M + 3) + 2;
+    PZ = PY + (g.N + 3) + 2;
+    PINF = PZ + (g.Z + 3) + 1;
+    for (int t = threadIdx.x; t < g.M + g.N + g.Z + 16; t += blockDim.x) sp[t] = 0.f;
+    __syncthreads();
+}
+static size_t plane_tables_bytes(const DevGeom& g) { return sizeof(float) * (size_t)(g.M + g.N + g.Z + 16); }
+
 // Floor of the position along an axis at parameter a, as a plane index
 // (the reference's floor((a*(x2-x1) + x1 - b)*inv_v)).
 __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, float inv_v)
@@ -58,7 +72,17 @@ __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, 
 // lengths' support (a_lo, a_hi) for the matched adjoint.
 // PINF points at a shared +inf: the next-plane table of an axis the ray is
 // parallel to, so every axis can recompute its alpha unconditionally.
-template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false>
+// CPM (bit 0 x, 1 y, 2 z): axes whose next plane is computed as
+// volumn*n + boundary from a float plane counter instead of read from the
+// shared table -- the same two roundings as the table entries, so the same
+// alphas; it trades shared-memory traffic for arithmetic.  CPM == 8: every
+// axis keeps the plane after its next one loaded ahead, so no shared-memory
+// read sits between choosing a step and the next alpha.  The tables carry a
+// padding entry at each end for those reads one plane past the volume.
+// The voxel value loaded in a step is accumulated in the next step, so the
+// load's latency overlaps the following traversal step; the sum is the same
+// sequence of roundings.
+template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false, int CPM = 0, bool TL = false>
 __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
                                             const float* __restrict__ PY, const float* __restrict__ PZ,
                                             const float* __restrict__ PINF, const VT* __restrict__ vol, float s,
@@ -196,15 +220,29 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     const float* PYo = PY + 1 + (sy > 0);
     const float* PZo = PZ + 1 + (sz > 0);
     float ex1x = x1x, eix = ix, ex1y = x1y, eiy = iy, ex1z = x1z, eiz = iz;
-    if (ax == INF) { sx = 0; PXo = PINF - vi; ex1x = 0.f; eix = 1.f; }
-    if (ay == INF) { sy = 0; PYo = PINF - vj; ex1y = 0.f; eiy = 1.f; }
-    if (az == INF) { sz = 0; PZo = PINF - vk; ex1z = 0.f; eiz = 1.f; }
+    // computed planes: counter fn = index of the next plane, plane = v*fn + b;
+    // a parallel axis uses v = 0, b = +inf
+    float fnx = (float)(vi + (sx > 0)), fny = (float)(vj + (sy > 0)), fnz = (float)(vk + (sz > 0));
+    float vxe = g.vx, bxe = g.bx, vye = g.vy, bye = g.by, vze = g.vz, bze = g.bz;
+    if (ax == INF) { sx = 0; PXo = PINF - vi; ex1x = 0.f; eix = 1.f; vxe = 0.f; bxe = INF; }
+    if (ay == INF) { sy = 0; PYo = PINF - vj; ex1y = 0.f; eiy = 1.f; vye = 0.f; bye = INF; }
+    if (az == INF) { sz = 0; PZo = PINF - vk; ex1z = 0.f; eiz = 1.f; vze = 0.f; bze = INF; }
+    const float fsx = (float)sx, fsy = (float)sy, fsz = (float)sz;
+    // prefetch mode: current next-plane coordinate and the one after it
+    float cxp = 0.f, nxp = 0.f, cyp = 0.f, nyp = 0.f, czp = 0.f, nzp = 0.f;
+    if (CPM == 8) {
+        const int ci = min(max(vi, -1), M), cj = min(max(vj, -1), N), ck = min(max(vk, -1), Z);
+        cxp = PXo[ci]; nxp = PXo[ci + sx];
+        cyp = PYo[cj]; nyp = PYo[cj + sy];
+        czp = PZo[ck]; nzp = PZo[ck + sz];
+    }
     const int MN = M * N;
     const int syM = sy * M, szMN = sz * MN;
-    int idx = vk * MN + vj * M + vi;
+    int idx = TL ? tile_index(g, vi, vj, vk) : vk * MN + vj * M + vi;
     const float d12 = r.d12;
     float ac = amin, sum = 0.f, len = 0.f;
     double dsum = 0.0;
+    float seg_p = 0.f, f_p = 0.f;   // the previous step's segment and voxel value
     bool any = false;
     // :297-551.  Branch-free step: every axis re-evaluates its next-plane
     // alpha from its (possibly unchanged) index, which reproduces the current
@@ -217,8 +255,10 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
         len = fa(len, seg);
         if (LOAD) {
             const float f = Store<VT>::ld(vol + idx);
-            if (ACC64) dsum = __fma_rn((double)seg, (double)f, dsum);
-            else sum = fa(sum, fm(seg, f));
+            if (ACC64) dsum = __fma_rn((double)seg_p, (double)f_p, dsum);   // +0 on the first step
+            else sum = fa(sum, fm(seg_p, f_p));
+            seg_p = seg;
+            f_p = f;
         }
         any = true;
         if (TRACE) {
@@ -230,12 +270,44 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
         vi += mx * sx;
         vj += my * sy;
         vk += mz * sz;
-        idx += mx * sx + my * syM + mz * szMN;
-        ax = fm(fs(PXo[vi], ex1x), eix);
-        ay = fm(fs(PYo[vj], ex1y), eiy);
-        az = fm(fs(PZo[vk], ex1z), eiz);
+        if (TL) idx = tile_index(g, vi, vj, vk);
+        else idx += mx * sx + my * syM + mz * szMN;
+        if (CPM == 8) {
+            cxp = mx ? nxp : cxp;
+            cyp = my ? nyp : cyp;
+            czp = mz ? nzp : czp;
+            ax = fm(fs(cxp, ex1x), eix);
+            ay = fm(fs(cyp, ex1y), eiy);
+            az = fm(fs(czp, ex1z), eiz);
+            nxp = PXo[vi + sx];   // in [-2, M+1]: padded
+            nyp = PYo[vj + sy];
+            nzp = PZo[vk + sz];
+        } else {
+            if (CPM & 1) {
+                fnx = fa(fnx, mx ? fsx : 0.f);
+                ax = fm(fs(fa(fm(vxe, fnx), bxe), ex1x), eix);
+            } else {
+                ax = fm(fs(PXo[vi], ex1x), eix);
+            }
+            if (CPM & 2) {
+                fny = fa(fny, my ? fsy : 0.f);
+                ay = fm(fs(fa(fm(vye, fny), bye), ex1y), eiy);
+            } else {
+                ay = fm(fs(PYo[vj], ex1y), eiy);
+            }
+            if (CPM & 4) {
+                fnz = fa(fnz, mz ? fsz : 0.f);
+                az = fm(fs(fa(fm(vze, fnz), bze), ex1z), eiz);
+            } else {
+                az = fm(fs(PZo[vk], ex1z), eiz);
+            }
+        }
         go = (fs(amax, ac) > 1e-16f) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
              ((unsigned)vk < (unsigned)Z);
+    }
+    if (LOAD && any) {
+        if (ACC64) dsum = __fma_rn((double)seg_p, (double)f_p, dsum);
+        else sum = fa(sum, fm(seg_p, f_p));
     }
     r.sum = sum;
     r.dsum = dsum;
@@ -250,7 +322,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
 // BY detector rows of 32 rays per block.  The partial sums of the objective
 // and the dot product are per tile (tile_x, tile_y, view), so their order
 // does not depend on the issue order.
-template <typename VT, int KIND, bool E64, int BY>
+template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false>
 __global__ void __launch_bounds__(FP_BX * BY)
 k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
           const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
@@ -258,10 +330,11 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
 {
     constexpr int NT = FP_BX * BY;
     extern __shared__ float sp[];
-    float* PX = sp;
-    float* PY = PX + (g.M + 3);
-    float* PZ = PY + (g.N + 3);
-    float* PINF = PZ + (g.Z + 3);
+    float* PX;
+    float* PY;
+    float* PZ;
+    float* PINF;
+    plane_tables_layout(g, sp, PX, PY, PZ, PINF);
     for (int t = threadIdx.x; t < g.M + 3; t += NT) PX[t] = g.px[t];
     for (int t = threadIdx.x; t < g.N + 3; t += NT) PY[t] = g.py[t];
     for (int t = threadIdx.x; t < g.Z + 3; t += NT) PZ[t] = g.pz[t];
@@ -278,7 +351,8 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     double e2 = 0.0;
     if (active) {
         const float2 sc = g.trig[view0 + w];
-        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT>(g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v);
+        const RayResult rr =
+            siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL>(g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v);
         const bool zero = rr.len < g.thr_fp;                       // :554
         if (KIND == FP_FORWARD) {
             st_any(out, p, out_dt, zero ? 0.0f : rr.sum);
@@ -306,44 +380,63 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     }
 }
 
-template <typename VT, int KIND, int BY>
-static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
+template <typename VT, int KIND, int BY, int CPM, bool TL>
+static void launch_fp_tl(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
     const DevGeom& g = G.dg;
     const dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + BY - 1) / BY, nview);
     const VT* vol = (const VT*)a.vol;
     if (g.entry64)
-        k_forward<VT, KIND, true, BY><<<grid, FP_BX * BY, smem, st>>>(g, vol, a.view0, a.out, a.out_dtype, a.b,
-                                                                     a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+        k_forward<VT, KIND, true, BY, CPM, TL><<<grid, FP_BX * BY, smem, st>>>(
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len);
     else
-        k_forward<VT, KIND, false, BY><<<grid, FP_BX * BY, smem, st>>>(g, vol, a.view0, a.out, a.out_dtype, a.b,
-                                                                      a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+        k_forward<VT, KIND, false, BY, CPM, TL><<<grid, FP_BX * BY, smem, st>>>(
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len);
 }
 
-// Rows per block of the projector shapes the tuner chooses from.
-static constexpr int kFpShapeRows[FP_SHAPES] = {2, 4, 8};
+template <typename VT, int KIND, int BY, int CPM = 0>
+static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
+{
+    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE) {
+        if (a.tiled) {
+            launch_fp_tl<VT, KIND, BY, CPM, true>(G, a, nview, smem, st);
+            return;
+        }
+    }
+    launch_fp_tl<VT, KIND, BY, CPM, false>(G, a, nview, smem, st);
+}
+
+// Projector shapes the tuner chooses from: (rows per block, computed-plane axes).
+struct FpShape { int rows, cpm; };
+static constexpr FpShape kFpShapes[FP_SHAPES] = {{2, 0}, {4, 0}, {8, 0}, {4, 4}, {4, 7}, {4, 8}, {8, 8}};
 
 template <typename VT, int KIND>
 static void launch_fp_shape(const Geometry& G, const FpArgs& a, size_t smem, cudaStream_t st)
 {
     switch (G.fp_shape) {
-    case 0: launch_fp_t<VT, KIND, 2>(G, a, a.nview, smem, st); break;
-    case 2: launch_fp_t<VT, KIND, 8>(G, a, a.nview, smem, st); break;
-    default: launch_fp_t<VT, KIND, 4>(G, a, a.nview, smem, st); break;
+    case 0: launch_fp_t<VT, KIND, 2, 0>(G, a, a.nview, smem, st); break;
+    case 2: launch_fp_t<VT, KIND, 8, 0>(G, a, a.nview, smem, st); break;
+    case 3: launch_fp_t<VT, KIND, 4, 4>(G, a, a.nview, smem, st); break;
+    case 4: launch_fp_t<VT, KIND, 4, 7>(G, a, a.nview, smem, st); break;
+    case 5: launch_fp_t<VT, KIND, 4, 8>(G, a, a.nview, smem, st); break;
+    case 6: launch_fp_t<VT, KIND, 8, 8>(G, a, a.nview, smem, st); break;
+    default: launch_fp_t<VT, KIND, 4, 0>(G, a, a.nview, smem, st); break;
     }
 }
 
 ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, size_t* nblocks_out)
 {
-    static_assert(kFpShapeRows[1] == FP_BY, "shape 1 is the fixed shape");
+    static_assert(kFpShapes[1].rows == FP_BY && kFpShapes[1].cpm == 0, "shape 1 is the fixed shape");
     const DevGeom& g = G.dg;
     if (a.nview <= 0) return CTR_OK;
     if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
+    if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE)
+        return set_error(CTR_ERR_UNSUPPORTED, "the tiled layout is for SART and objective projections");
     // reductions keep the fixed shape: their partial sums, and so the
     // rounding of the totals, do not depend on the tuned shape
     if (nblocks_out)
         *nblocks_out = (size_t)((g.R + FP_BX - 1) / FP_BX) * ((g.ZP + FP_BY - 1) / FP_BY) * a.nview;
-    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 10);
+    const size_t smem = plane_tables_bytes(g);
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         switch (a.kind) {
         case FP_FORWARD: launch_fp_shape<VT, FP_FORWARD>(G, a, smem, st); break;
@@ -368,10 +461,11 @@ __global__ void __launch_bounds__(FP_THREADS)
 k_ray_prep(const DevGeom g, const float* __restrict__ y, int view0, AdjRay* __restrict__ rays)
 {
     extern __shared__ float sp[];
-    float* PX = sp;
-    float* PY = PX + (g.M + 3);
-    float* PZ = PY + (g.N + 3);
-    float* PINF = PZ + (g.Z + 3);
+    float* PX;
+    float* PY;
+    float* PZ;
+    float* PINF;
+    plane_tables_layout(g, sp, PX, PY, PZ, PINF);
     for (int t = threadIdx.x; t < g.M + 3; t += FP_THREADS) PX[t] = g.px[t];
     for (int t = threadIdx.x; t < g.N + 3; t += FP_THREADS) PY[t] = g.py[t];
     for (int t = threadIdx.x; t < g.Z + 3; t += FP_THREADS) PZ[t] = g.pz[t];
@@ -395,7 +489,7 @@ ctr_status launch_ray_prep(const Geometry& G, const float* y, int view0, int nvi
     const DevGeom& g = G.dg;
     if (nview <= 0) return CTR_OK;
     dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + FP_BY - 1) / FP_BY, nview);
-    const size_t smem = sizeof(float) * (size_t)(g.M + g.N + g.Z + 10);
+    const size_t smem = plane_tables_bytes(g);
     if (g.entry64) k_ray_prep<true><<<grid, FP_THREADS, smem, st>>>(g, y, view0, rays);
     else k_ray_prep<false><<<grid, FP_THREADS, smem, st>>>(g, y, view0, rays);
     CTR_CUDA_TRY(cudaGetLastError());

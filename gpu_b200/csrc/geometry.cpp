@@ -91,6 +91,17 @@ ctr_status ensure_fgp(Geometry* g, size_t bytes)
     return CTR_OK;
 }
 
+ctr_status ensure_tiled(Geometry* g, size_t bytes)
+{
+    if (bytes <= g->tiled_bytes) return CTR_OK;
+    if (g->d_tiled) cudaFree(g->d_tiled);
+    g->d_tiled = nullptr;
+    g->tiled_bytes = 0;
+    CTR_CUDA_TRY(cudaMalloc(&g->d_tiled, bytes));
+    g->tiled_bytes = bytes;
+    return CTR_OK;
+}
+
 ctr_status check_device_errors(Geometry* g, cudaStream_t st)
 {
     unsigned h = 0;
@@ -110,7 +121,7 @@ static ctr_status validate(const ctr_geometry_desc* d)
     if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0 || d->nu <= 0 || d->nv <= 0 || d->n_views <= 0)
         return set_error(CTR_ERR_BAD_GEOMETRY, "sizes must be positive (nx=%d ny=%d nz=%d nu=%d nv=%d views=%d)",
                          d->nx, d->ny, d->nz, d->nu, d->nv, d->n_views);
-    const double vox = (double)d->nx * d->ny * d->nz;
+    const double vox = (double)((d->nx + 7) / 8 * 8) * ((d->ny + 7) / 8 * 8) * d->nz;   // tiled layout
     if (vox > 2147483647.0)
         return set_error(CTR_ERR_BAD_GEOMETRY, "volume of %.0f voxels exceeds the 2^31-1 index range", vox);
     if ((double)d->nu * d->nv > 2147483647.0)
@@ -158,6 +169,8 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     DevGeom& q = g->dg;
     q.M = d.nx; q.N = d.ny; q.Z = d.nz; q.R = d.nu; q.ZP = d.nv; q.nviews = d.n_views;
     q.max_steps = d.nx + d.ny + d.nz + 3;
+    q.Mt = (d.nx + 7) / 8;
+    q.Nt = (d.ny + 7) / 8;
     q.entry64 = (d.flags & CTR_GEOM_ENTRY_F64) ? 1 : 0;
     q.vx = d.vx; q.vy = d.vy; q.vz = d.vz;
     // inv_volumn_x = 1.0/volumn_x (double division stored as float), main_recon.cu:88
@@ -286,6 +299,13 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     q.rowt = (const float2*)(base + o_row);
     q.colt = g->d_colt;
     q.err = g->d_err;
+    if ((e = cudaMalloc(&g->d_zcell, sizeof(float2) * (size_t)d.nz * d.nv)) != cudaSuccess) {
+        st = cuda_error(e, "cudaMalloc(zcell)");
+        goto fail;
+    }
+    if ((st = launch_zcell(*g, g->d_zcell, 0)) != CTR_OK) goto fail;
+    if ((e = cudaStreamSynchronize(0)) != cudaSuccess) { st = cuda_error(e, "zcell"); goto fail; }
+    q.zcell = g->d_zcell;
     *out = reinterpret_cast<ctr_geometry*>(g);
     return CTR_OK;
 fail:
@@ -299,12 +319,14 @@ extern "C" ctr_status ctr_geometry_destroy(ctr_geometry* geom)
     Geometry* g = reinterpret_cast<Geometry*>(geom);
     cudaFree(g->d_tables);
     cudaFree(g->d_colt);
+    cudaFree(g->d_zcell);
     cudaFree(g->d_err);
     cudaFree(g->d_rays);
     cudaFree(g->d_partial);
     cudaFree(g->d_result);
     cudaFree(g->d_fgp);
     cudaFree(g->d_fdk);
+    cudaFree(g->d_tiled);
     cudaFree(g->d_ramp);
     delete g;
     return CTR_OK;

@@ -33,6 +33,7 @@ GEOM_ENTRY_F64 = 0x1
 BP_ACCUMULATE = 0x1
 BP_FOV_MASK = 0x2
 SART_STOCHASTIC_ROUND = 0x1
+SART_TILED = 0x2
 
 # every symbol include/ctrecon.h declares
 EXPORTED = [
@@ -308,7 +309,7 @@ class Geometry:
         check(self.lib.ctr_phantom_voxelize(self.h, p.ctypes.data, p.shape[0], _ptr(vol), _stream(stream)))
         return vol
 
-    FP_SHAPES = 3
+    FP_SHAPES = 7
     BP_SHAPES = 6
 
     def set_shapes(self, fp_shape, bp_shape):

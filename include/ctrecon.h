@@ -84,18 +84,21 @@ ctr_status ctr_geometry_destroy(ctr_geometry* geom);
  * (V63/host_IterativeRecon_CBCT.c:34-41), as the kernels use them. */
 ctr_status ctr_geometry_view_trig(const ctr_geometry* geom, int view, float* sin_out, float* cos_out);
 
-/* Launch shapes of the SART projectors.  fp_shape 0..2: 32 x {2, 4, 8} rays
- * per block.  bp_shape -1: the fixed-shape backprojector (8 voxels of a
+/* Launch shapes of the SART projectors.  fp_shape 0..6: (rows of 32 rays per
+ * block, plane coordinates) = (2, table) (4, table) (8, table) (4, z computed)
+ * (4, xyz computed) (4, table read one plane ahead) (8, read ahead).  bp_shape -1: the fixed-shape backprojector (8 voxels of a
  * column per thread); 0..5: the column walk with (voxel rows per block, z
- * run) = (4,8) (4,32) (2,32) (8,32) (4,128) (2,8).  Results never depend on
+ * run, detector rows per load batch) = (4,8,1) (4,32,1) (4,32,2) (8,32,1)
+ * (4,128,1) (4,128,2).  Results never depend on
  * the shape.  Defaults: fp_shape 1, bp_shape 1.  Not thread-safe against
  * launches on the same geometry. */
 ctr_status ctr_geometry_set_shapes(ctr_geometry* geom, int fp_shape, int bp_shape);
 ctr_status ctr_geometry_get_shapes(const ctr_geometry* geom, int* fp_shape, int* bp_shape);
 /* Time every shape on n_views views spread over the scan (SART forward
- * projection, then SART backprojection into a scratch volume of vol_dtype)
- * and keep the fastest.  fp_ms[3] and bp_ms[7] (may be NULL) receive the mean
- * milliseconds per view of each shape; bp_ms[0] is bp_shape -1.  Allocates a
+ * projection, then SART backprojection into a scratch volume of vol_dtype in
+ * the tiled layout the solver projects) and keep the fastest.  fp_ms[7] and
+ * bp_ms[7] (may be NULL) receive the mean milliseconds per view of each
+ * shape; bp_ms[0] is bp_shape -1 on the linear layout (reported, not chosen).  Allocates a
  * scratch volume and one sinogram view; synchronises the stream. */
 ctr_status ctr_geometry_autotune(ctr_geometry* geom, ctr_dtype vol_dtype, int n_views, float* fp_ms, float* bp_ms,
                                  void* stream);
@@ -126,8 +129,12 @@ ctr_status ctr_backproject(const ctr_geometry* geom, const float* sino, int view
  * (b - Af)/len) then BP command 1 (f += beta * sum(w c)/sum(w) inside the FOV
  * cylinder).  Replaces Reconstruction_3D_ray_driven_CBCT
  * (V63/host_IterativeRecon_CBCT.c:1-67) on device buffers.
- * CTR_SART_STOCHASTIC_ROUND rounds BF16/F16 voxel updates stochastically. */
+ * CTR_SART_STOCHASTIC_ROUND rounds BF16/F16 voxel updates stochastically.
+ * CTR_SART_TILED runs the views on an 8x8-tiled copy of the volume (a
+ * geometry workspace, copied in before and out after): the same result,
+ * fewer cache lines per projector load.  The solver always does this. */
 #define CTR_SART_STOCHASTIC_ROUND 0x1u
+#define CTR_SART_TILED 0x2u
 ctr_status ctr_sart_pass(const ctr_geometry* geom, void* vol, ctr_dtype vol_dtype,
                          const void* sino, ctr_dtype sino_dtype, float beta, unsigned flags,
                          uint32_t seed, void* stream);

@@ -1,6 +1,7 @@
 """Launch shapes of the SART projectors and their tuner: every forward
 projector shape and every backprojector shape (the fixed-shape kernel and
-the column walks) gives bit-identical projections and SART passes."""
+the column walks), on the linear and on the 8x8-tiled volume layout, gives
+bit-identical projections and SART passes."""
 import numpy as np
 import pytest
 
@@ -39,15 +40,16 @@ def test_every_shape_gives_the_same_result(name, dtype, oracle_built):
             assert g.shapes() == (fs, bs)
             fp = torch.zeros_like(b)
             g.forward(x0, fp)
-            x = torch.zeros(g.vol_shape, device="cuda", dtype=tdt)
-            g.sart_pass(x, b, 0.8, flags=flags, seed=7)
-            g.sart_pass(x, b, 0.8, flags=flags, seed=8)
-            if ref_fp is None:
-                ref_fp, ref_sart = bits(fp), bits(x)
-                assert np.any(ref_sart != 0)
-            else:
-                np.testing.assert_array_equal(bits(fp), ref_fp, err_msg=f"fp shape {fs}")
-                np.testing.assert_array_equal(bits(x), ref_sart, err_msg=f"shapes {fs} {bs}")
+            for tiled in (0, gpu_b200.SART_TILED):
+                x = torch.zeros(g.vol_shape, device="cuda", dtype=tdt)
+                g.sart_pass(x, b, 0.8, flags=flags | tiled, seed=7)
+                g.sart_pass(x, b, 0.8, flags=flags | tiled, seed=8)
+                if ref_fp is None:
+                    ref_fp, ref_sart = bits(fp), bits(x)
+                    assert np.any(ref_sart != 0)
+                else:
+                    np.testing.assert_array_equal(bits(fp), ref_fp, err_msg=f"fp shape {fs}")
+                    np.testing.assert_array_equal(bits(x), ref_sart, err_msg=f"shapes {fs} {bs} tiled {tiled}")
 
 
 def test_autotune_picks_a_valid_shape():
@@ -59,6 +61,6 @@ def test_autotune_picks_a_valid_shape():
     assert r["fp_ms"][r["fp_shape"]] == min(r["fp_ms"])
     assert r["bp_ms"][r["bp_shape"]] == min(r["bp_ms"].values())
     with pytest.raises(gpu_b200.CtrError):
-        g.set_shapes(3, 0)
+        g.set_shapes(g.FP_SHAPES, 0)
     with pytest.raises(gpu_b200.CtrError):
         g.set_shapes(0, -2)
