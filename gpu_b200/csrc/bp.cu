@@ -237,8 +237,8 @@ ctr_status launch_zcell(const Geometry& G, float2* zcell, cudaStream_t st)
 // arithmetic, so the two give bit-identical volumes.
 constexpr int WALK_RUN = 4;   // detector columns of the run kept in registers
 
-template <typename VT, bool STOCH, int BY, int UNR, bool TL>
-__global__ void __launch_bounds__(32 * BY)
+template <typename VT, bool STOCH, int BY, int MINB, bool TL>
+__global__ void __launch_bounds__(32 * BY, MINB)
 k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
             uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
 {
@@ -318,14 +318,24 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
 
     const int R = g.R;
     const long long MN = (long long)g.M * g.N;
+    // projections of the lower plane of voxel kb; each voxel's upper plane is
+    // the next voxel's lower one, so its pair is carried (min and max of
+    // four finite values do not depend on the grouping)
+    float cmn, cmx;
+    {
+        const float z0 = PZ[kb + 1], zlo = fs(z0, g.srcz);
+        const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
+        cmn = fminf(a0, a1);
+        cmx = fmaxf(a0, a1);
+    }
     for (int k = kb; k < ke; ++k) {
         // candidate detector rows of voxel k
-        const float z0 = PZ[k + 1], z1 = PZ[k + 2];
-        const float zlo = fs(z0, g.srcz), zhi = fs(z1, g.srcz);
-        const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
+        const float z1 = PZ[k + 2], zhi = fs(z1, g.srcz);
         const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
-        const float zmn = fminf(fminf(a0, a1), fminf(b0, b1));
-        const float zmx = fmaxf(fmaxf(a0, a1), fmaxf(b0, b1));
+        const float bmn = fminf(b0, b1), bmx = fmaxf(b0, b1);
+        const float zmn = fminf(cmn, bmn), zmx = fmaxf(cmx, bmx);
+        cmn = bmn;
+        cmx = bmx;
         int vlo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
         int vhi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
         if ((vlo < 0 && vhi < 0) || (vlo > g.ZP - 1 && vhi > g.ZP - 1)) continue;
@@ -344,17 +354,7 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         };
         auto pairs = [&](int uu, float a, float bb) {
             if (!(bb > a)) return;
-            int vv = vlo;
-            if (UNR == 2) {   // both rows' loads first, then the pairs in row order
-                for (; vv < vhi; vv += 2) {
-                    const float2 z0c = __ldg(zrow + vv), z1c = __ldg(zrow + vv + 1);
-                    const float2 r0 = __ldg(rays + (long long)vv * R + uu);
-                    const float2 r1 = __ldg(rays + (long long)(vv + 1) * R + uu);
-                    pair(a, bb, z0c, r0);
-                    pair(a, bb, z1c, r1);
-                }
-            }
-            for (; vv <= vhi; ++vv) pair(a, bb, __ldg(zrow + vv), __ldg(rays + (long long)vv * R + uu));
+            for (int vv = vlo; vv <= vhi; ++vv) pair(a, bb, __ldg(zrow + vv), __ldg(rays + (long long)vv * R + uu));
         };
 #pragma unroll
         for (int q = 0; q < WALK_RUN; ++q)
@@ -408,11 +408,12 @@ ctr_status launch_tiling(const Geometry& G, const void* src, void* dst, ctr_dtyp
 }
 
 // SART backprojector launch shapes the tuner chooses from: voxel rows per
-// block and the longest z run per thread (shortened for small volumes so
-// that the grid still fills the GPU).
-struct BpShape { int rows, zl, unroll; };
-static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8, 1}, {4, 32, 1}, {4, 32, 2}, {8, 32, 1}, {4, 128, 1},
-                                                 {4, 128, 2}};
+// block, the longest z run per thread (shortened for small volumes so that
+// the grid still fills the GPU) and the blocks per SM the registers are
+// capped for.
+struct BpShape { int rows, zl, minb; };
+static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8, 8}, {4, 32, 8}, {4, 32, 10}, {8, 32, 4}, {4, 128, 8},
+                                                 {4, 128, 10}};
 
 template <typename VT, bool STOCH, bool TL>
 static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStream_t st, size_t smem)
@@ -426,13 +427,13 @@ static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStrea
     if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
     const float2* rays = (const float2*)a.rays;
     if (sh.rows == 8)
-        k_sart_walk<VT, STOCH, 8, 1, TL><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+        k_sart_walk<VT, STOCH, 8, 4, TL><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
                                                                   a.pass_seed, zl);
-    else if (sh.unroll == 2)
-        k_sart_walk<VT, STOCH, 4, 2, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                                  a.pass_seed, zl);
+    else if (sh.minb == 10)
+        k_sart_walk<VT, STOCH, 4, 10, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                   a.pass_seed, zl);
     else
-        k_sart_walk<VT, STOCH, 4, 1, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+        k_sart_walk<VT, STOCH, 4, 8, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
                                                                   a.pass_seed, zl);
     return CTR_OK;
 }

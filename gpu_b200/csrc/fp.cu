@@ -322,8 +322,8 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
 // BY detector rows of 32 rays per block.  The partial sums of the objective
 // and the dot product are per tile (tile_x, tile_y, view), so their order
 // does not depend on the issue order.
-template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false>
-__global__ void __launch_bounds__(FP_BX * BY)
+template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false, int MINB = 1>
+__global__ void __launch_bounds__(FP_BX * BY, MINB)
 k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
           const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
           uint64_t* __restrict__ hash, float* __restrict__ lens)
@@ -380,47 +380,50 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     }
 }
 
-template <typename VT, int KIND, int BY, int CPM, bool TL>
+template <typename VT, int KIND, int BY, int CPM, bool TL, int MINB>
 static void launch_fp_tl(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
     const DevGeom& g = G.dg;
     const dim3 grid((g.R + FP_BX - 1) / FP_BX, (g.ZP + BY - 1) / BY, nview);
     const VT* vol = (const VT*)a.vol;
     if (g.entry64)
-        k_forward<VT, KIND, true, BY, CPM, TL><<<grid, FP_BX * BY, smem, st>>>(
+        k_forward<VT, KIND, true, BY, CPM, TL, MINB><<<grid, FP_BX * BY, smem, st>>>(
             g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len);
     else
-        k_forward<VT, KIND, false, BY, CPM, TL><<<grid, FP_BX * BY, smem, st>>>(
+        k_forward<VT, KIND, false, BY, CPM, TL, MINB><<<grid, FP_BX * BY, smem, st>>>(
             g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len);
 }
 
-template <typename VT, int KIND, int BY, int CPM = 0>
+template <typename VT, int KIND, int BY, int CPM = 0, int MINB = 1>
 static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
     if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE) {
         if (a.tiled) {
-            launch_fp_tl<VT, KIND, BY, CPM, true>(G, a, nview, smem, st);
+            launch_fp_tl<VT, KIND, BY, CPM, true, MINB>(G, a, nview, smem, st);
             return;
         }
     }
-    launch_fp_tl<VT, KIND, BY, CPM, false>(G, a, nview, smem, st);
+    launch_fp_tl<VT, KIND, BY, CPM, false, MINB>(G, a, nview, smem, st);
 }
 
-// Projector shapes the tuner chooses from: (rows per block, computed-plane axes).
-struct FpShape { int rows, cpm; };
-static constexpr FpShape kFpShapes[FP_SHAPES] = {{2, 0}, {4, 0}, {8, 0}, {4, 4}, {4, 7}, {4, 8}, {8, 8}};
+// Projector shapes the tuner chooses from: (rows per block, plane mode --
+// 0 table, 7 computed, 8 table read ahead --, blocks per SM the registers
+// are capped for).
+struct FpShape { int rows, cpm, minb; };
+static constexpr FpShape kFpShapes[FP_SHAPES] = {{2, 0, 1}, {4, 0, 1}, {8, 0, 1}, {4, 0, 16},
+                                                 {4, 0, 12}, {4, 8, 1}, {4, 7, 1}};
 
 template <typename VT, int KIND>
 static void launch_fp_shape(const Geometry& G, const FpArgs& a, size_t smem, cudaStream_t st)
 {
     switch (G.fp_shape) {
-    case 0: launch_fp_t<VT, KIND, 2, 0>(G, a, a.nview, smem, st); break;
-    case 2: launch_fp_t<VT, KIND, 8, 0>(G, a, a.nview, smem, st); break;
-    case 3: launch_fp_t<VT, KIND, 4, 4>(G, a, a.nview, smem, st); break;
-    case 4: launch_fp_t<VT, KIND, 4, 7>(G, a, a.nview, smem, st); break;
-    case 5: launch_fp_t<VT, KIND, 4, 8>(G, a, a.nview, smem, st); break;
-    case 6: launch_fp_t<VT, KIND, 8, 8>(G, a, a.nview, smem, st); break;
-    default: launch_fp_t<VT, KIND, 4, 0>(G, a, a.nview, smem, st); break;
+    case 0: launch_fp_t<VT, KIND, 2, 0, 1>(G, a, a.nview, smem, st); break;
+    case 2: launch_fp_t<VT, KIND, 8, 0, 1>(G, a, a.nview, smem, st); break;
+    case 3: launch_fp_t<VT, KIND, 4, 0, 16>(G, a, a.nview, smem, st); break;
+    case 4: launch_fp_t<VT, KIND, 4, 0, 12>(G, a, a.nview, smem, st); break;
+    case 5: launch_fp_t<VT, KIND, 4, 8, 1>(G, a, a.nview, smem, st); break;
+    case 6: launch_fp_t<VT, KIND, 4, 7, 1>(G, a, a.nview, smem, st); break;
+    default: launch_fp_t<VT, KIND, 4, 0, 1>(G, a, a.nview, smem, st); break;
     }
 }
 
