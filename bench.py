@@ -44,8 +44,9 @@ def parse():
                    help="with --profile-views: also run one FP16 solver iteration")
     p.add_argument("--profile-tune", action="store_true",
                    help="with --profile-views: also print the tuner's time for every launch shape")
-    p.add_argument("--workload", choices=["scan512", "batched"], default="scan512",
-                   help="scan512: the 512^3 / 1024-view scan (default); batched: 48 uneven scans in one graph")
+    p.add_argument("--workload", choices=["scan512", "batched", "large"], default="scan512",
+                   help="scan512: the 512^3 / 1024-view scan (default); batched: 48 uneven scans in one graph; "
+                        "large: 1024^3 / 1024 views / 1024^2 detector in FP32, BF16 and FP16")
     p.add_argument("--scans", type=int, default=48, help="batched: number of scans")
     p.add_argument("--no-tune", action="store_true", help="batched: keep the default launch shapes")
     p.add_argument("--no-sr", action="store_true", help="batched: BF16 updates rounded to nearest instead of "
@@ -366,7 +367,7 @@ def run_batched(args):
         s32.get_volume(want)
         s32.close()
         errs.append(float(torch.sqrt(torch.mean((got.float() - want) ** 2)) / want.abs().max().clamp_min(1e-30)))
-    launches = sum(2 * sp["n_views"] + FGP_ITERS + 1 + 1 + 2 + 1 + 1 for sp in specs) * iters
+    launches = sum(2 + 2 * sp["n_views"] + FGP_ITERS + 1 + 1 + 1 + 2 + 1 + 1 for sp in specs) * iters
     line = {
         "metric": "batched SART-FISTA-TV voxel-updates/s", "value": updates * 1000.0 / ms,
         "unit": "voxel-updates/s", "n_gpus": 1, "steps": iters, "warmup": args.warmup, "ms_per_step": ms,
@@ -386,6 +387,88 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+LARGE = dict(nx=1024, ny=1024, nz=1024, vx=0.25, nu=1024, nv=1024, du=0.3, dso=1000.0, dod=-500.0, n_views=1024)
+
+
+def run_large(args):
+    """1024^3 (0.25 mm) / 1024 views / 1024x1024 detector (0.3 mm): iterations/s
+    of FP32, BF16 and FP16 storage on a seeded 100-ellipsoid phantom, and the
+    RMSE and maximum error of the BF16/FP16 reconstructions against the FP32
+    one after the same iterations (relative to the phantom's maximum)."""
+    import numpy as np
+    import torch
+
+    import gpu_b200
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = LARGE
+    geom = gpu_b200.Geometry(gpu_b200.make_desc(L["nx"], L["ny"], L["nz"], L["vx"], L["nu"], L["nv"], L["du"],
+                                                L["dso"], L["dod"], L["n_views"]))
+    rng = np.random.default_rng(1024)
+    k = 100
+    ph = np.zeros((k, 10))
+    r = 40.0 * np.cbrt(rng.uniform(0, 1, k))
+    d = rng.normal(size=(k, 3))
+    ph[:, 0:3] = r[:, None] * d / np.linalg.norm(d, axis=1, keepdims=True)
+    ph[:, 3:6] = rng.uniform(5.0, 40.0, (k, 3))
+    ph[:, 6:9] = rng.uniform(0, 2 * np.pi, (k, 3))
+    ph[:, 9] = rng.uniform(0.01, 0.03, k)
+    truth = torch.zeros(geom.vol_shape, device=dev)
+    geom.phantom_voxelize(ph, truth)
+    mu_max = float(truth.max())
+    sino32 = torch.zeros((L["n_views"],) + geom.view_shape, device=dev)
+    geom.forward(truth, sino32)
+    del truth
+    stream = torch.cuda.current_stream()
+    out = {}
+    vols = {}
+    for mode, vdt, tdt in (("f32", gpu_b200.F32, torch.float32), ("bf16", gpu_b200.BF16, torch.bfloat16),
+                           ("f16", gpu_b200.F16, torch.float16)):
+        sino = sino32 if tdt == torch.float32 else sino32.to(tdt)
+        tuned = geom.autotune(vdt, n_views=2)
+        flags = gpu_b200.SART_STOCHASTIC_ROUND if mode == "bf16" else 0
+        solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, sart_flags=flags)
+        solver.set_sinogram(sino)
+        solver.set_volume(None)
+        for _ in range(args.warmup):
+            solver.iterate(1)
+        solver.set_volume(None)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.iterate(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        vol = torch.zeros(geom.vol_shape, device=dev, dtype=tdt)
+        solver.get_volume(vol)
+        solver.close()
+        vols[mode] = vol
+        out[mode] = {"ms_per_step": ms, "iter_per_s": 1000.0 / ms, "clocks": clocks.stop(),
+                     "launch_shapes": [tuned["fp_shape"], tuned["bp_shape"]],
+                     "voxel_updates_per_s": 1000.0 / ms * L["nx"] * L["ny"] * L["nz"] * L["n_views"]}
+        if sino is not sino32:
+            del sino
+    ref = vols["f32"]
+    for mode in ("bf16", "f16"):
+        dlt = vols[mode].float() - ref
+        out[mode]["rmse_vs_f32"] = float(torch.sqrt(torch.mean(dlt * dlt))) / mu_max
+        out[mode]["max_err_vs_f32"] = float(dlt.abs().max()) / mu_max
+        out[mode]["speedup_vs_f32"] = out["f32"]["ms_per_step"] / out[mode]["ms_per_step"]
+    line = {"metric": "SART-FISTA-TV iter/s, 1024^3 x 1024 views, BF16/FP16 vs FP32", "value": out["bf16"]["iter_per_s"],
+            "unit": "iter/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["bf16"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 storage (stochastic rounding), f32 arithmetic", "data": "synthetic",
+            "config": {"workload": "1024^3 x 0.25 mm, 1024 views, 1024x1024 detector x 0.3 mm, DSO 1000 mm, "
+                                   "DOD -500 mm, 100 seeded ellipsoids, noiseless Siddon sinogram",
+                       "l2": "inputs > L2"},
+            "modes": out, "phantom_max": mu_max}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -394,6 +477,8 @@ def main():
         return profile_views(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "large":
+        return run_large(args)
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -501,6 +586,47 @@ def main():
         kern[mode] = {"fp_ms": fp_t / nt, "bp_ms": bp_t / nt}
         del vol
 
+    # the iteration without the objective (the reference's loop evaluates it
+    # every iteration, so the headline keeps it)
+    geom.set_shapes(tuned["mixed"]["fp_shape"], tuned["mixed"]["bp_shape"])
+    noobj = gpu_b200.Solver(geom, mixed_code, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
+                            objective=False, use_graph=True)
+    noobj.set_sinogram(runs["mixed"]["sino"])
+    noobj.set_volume(None)
+    noobj.iterate(1)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    noobj.iterate(args.steps)
+    e1.record(stream)
+    barrier()
+    noobj_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    noobj.close()
+
+    # ray-voxel intersections of one pass over all views (Siddon segments of
+    # every ray, counted once per geometry); an iteration visits each of them
+    # three times: SART forward projection, SART backprojection, objective
+    nseg = torch.empty(sshape[1:], device=dev, dtype=torch.int32)
+    hsh = torch.empty(sshape[1:], device=dev, dtype=torch.int64)
+    lng = torch.empty(sshape[1:], device=dev, dtype=torch.float32)
+    zero = torch.zeros(vshape, device=dev)
+    segs = torch.zeros((), device=dev, dtype=torch.int64)
+    for j in range(SCAN["n_views"]):
+        geom.forward_trace(zero, j, nseg, hsh, lng)
+        segs += nseg.sum(dtype=torch.int64)
+    segs_per_pass = int(segs.item())
+    del nseg, hsh, lng
+
+    # FDK of the same scan (FP32), reported beside the iterative numbers
+    geom.fdk(sino32, zero)
+    barrier()
+    e0.record(stream)
+    geom.fdk(sino32, zero)
+    e1.record(stream)
+    barrier()
+    fdk_ms = max_over_ranks(e0.elapsed_time(e1))
+    del zero
+
     peak, peak_kind = measured_peak_hbm()
     s_v = 2  # mixed storage bytes
     bp_bytes = 2 * V * s_v + 4 * P            # BP with SART update, per view (algorithmic)
@@ -513,8 +639,9 @@ def main():
         ms_mixed = runs["mixed"]["ms"]
         ms_f32 = runs["f32"]["ms"]
         value = world * 1000.0 / ms_mixed
-        # SART: FP + BP per view; FGP: inner steps + final; objective: FP, 2 reduce, TV, reduce
-        launches_per_step = 2 * SCAN["n_views"] + FGP_ITERS + 1 + 1 + 2 + 1 + 1
+        # SART: tile, FP + BP per view, untile; FGP: inner steps + final;
+        # objective: tile, FP, 2 reduce, TV, reduce
+        launches_per_step = 2 + 2 * SCAN["n_views"] + FGP_ITERS + 1 + 1 + 1 + 2 + 1 + 1
         line = {
             "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
@@ -524,6 +651,10 @@ def main():
                        "phantom": "40 ellipsoids + 200 spheres (seeded), Siddon projections + 0.5% noise",
                        "parallelism": f"replicas x{world}", "l2": "inputs > L2 (512 MB+ volume)"},
             "voxel_updates_per_s": value * V * SCAN["n_views"],
+            "ray_voxel_intersections_per_s": value * 3 * segs_per_pass,
+            "ray_voxel_intersections_per_pass": segs_per_pass,
+            "ms_per_step_without_objective": noobj_ms,
+            "fdk_ms": fdk_ms,
             "f32": {"iter_per_s": world * 1000.0 / ms_f32, "ms_per_step": ms_f32,
                     "voxel_updates_per_s": world * 1000.0 / ms_f32 * V * SCAN["n_views"]},
             "mixed_over_f32": ms_f32 / ms_mixed,
