@@ -20,6 +20,7 @@ struct DevGeom {
     int nviews;
     int max_steps;          // Siddon step bound nx+ny+nz+3
     int Mt, Nt;             // 8x8 (x, y) tiles per row / column of the tiled layout
+    int fast_exit;          // every alpha inside the volume >= 1e-6: the Siddon loop test is one comparison
     int entry64;            // FP64 ray-box entry/exit
     float vx, vy, vz, inv_vx, inv_vy, inv_vz;
     float bx, by, bz;       // boundary_voxel_*

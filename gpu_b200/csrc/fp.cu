@@ -13,7 +13,8 @@
 //     moves at least one index one voxel in its fixed direction (the minimum
 //     of non-NaN alphas equals one of them; all-NaN alphas end the loop), so
 //     a ray takes at most nx+ny+nz+1 steps: the reference's endless loop on
-//     NaN alphas cannot occur;
+//     NaN alphas cannot occur.  After the first step the whole test is one
+//     comparison of alpha against a per-ray limit (see the loop);
 //   * blocks are issued centre-out over the detector, so the long rays
 //     through the middle of the volume start first and the last wave holds
 //     short ones;
@@ -244,6 +245,21 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     double dsum = 0.0;
     float seg_p = 0.f, f_p = 0.f;   // the previous step's segment and voxel value
     bool any = false;
+    // Loop condition after the first step.  Every next-plane alpha is at
+    // least ac and grows along its axis, so an index leaves the volume
+    // exactly when ac reaches the alpha of that axis's last plane in index
+    // space (aex*: the next plane of the last voxel); and when every alpha of
+    // the volume is >= 1e-6 (geometry flag fast_exit), amax - ac > 1e-16 is
+    // ac < amax (distinct floats >= 2^-28 differ by more than 2^-51).  The
+    // first step keeps the reference's own test, which also covers a start
+    // voxel whose next plane lies behind the entry point.
+    float alim = amax;
+    if (g.fast_exit) {
+        const float aex = sx > 0 ? fm(fs(PXo[M - 1], ex1x), eix) : (sx < 0 ? fm(fs(PXo[0], ex1x), eix) : INF);
+        const float aey = sy > 0 ? fm(fs(PYo[N - 1], ex1y), eiy) : (sy < 0 ? fm(fs(PYo[0], ex1y), eiy) : INF);
+        const float aez = sz > 0 ? fm(fs(PZo[Z - 1], ex1z), eiz) : (sz < 0 ? fm(fs(PZo[0], ex1z), eiz) : INF);
+        alim = fminf(amax, fminf(aex, fminf(aey, aez)));
+    }
     // :297-551.  Branch-free step: every axis re-evaluates its next-plane
     // alpha from its (possibly unchanged) index, which reproduces the current
     // value bit for bit when the axis did not move.
@@ -302,8 +318,9 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
                 az = fm(fs(PZo[vk], ex1z), eiz);
             }
         }
-        go = (fs(amax, ac) > 1e-16f) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
-             ((unsigned)vk < (unsigned)Z);
+        if (g.fast_exit) go = ac < alim;
+        else go = (fs(amax, ac) > 1e-16f) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
+                  ((unsigned)vk < (unsigned)Z);
     }
     if (LOAD && any) {
         if (ACC64) dsum = __fma_rn((double)seg_p, (double)f_p, dsum);

@@ -134,8 +134,8 @@ static ctr_status validate(const ctr_geometry_desc* d)
         !std::isfinite(d->offset))
         return set_error(CTR_ERR_BAD_GEOMETRY, "angles and offset must be finite");
     // the volume must sit strictly between source and detector planes along every view
-    const double half_diag = 0.5 * std::sqrt((double)d->nx * d->vx * d->nx * d->vx +
-                                             (double)d->ny * d->vx * d->ny * d->vx) +
+    const double vy = d->vy > 0.f ? d->vy : d->vx;
+    const double half_diag = 0.5 * std::sqrt((double)d->nx * d->vx * d->nx * d->vx + (double)d->ny * vy * d->ny * vy) +
                              std::fabs((double)d->m_offset * d->vx);
     if (half_diag >= d->dso || half_diag >= -d->dod)
         return set_error(CTR_ERR_BAD_GEOMETRY, "volume (half-diagonal %.4g) reaches the source or detector", half_diag);
@@ -171,6 +171,13 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     q.max_steps = d.nx + d.ny + d.nz + 3;
     q.Mt = (d.nx + 7) / 8;
     q.Nt = (d.ny + 7) / 8;
+    {
+        // alpha of a point = its distance from the detector plane / (DSO - DOD);
+        // the volume's nearest point is at least -DOD - (half-diagonal) away
+        const double half_diag = 0.5 * std::sqrt((double)d.nx * d.vx * d.nx * d.vx + (double)d.ny * d.vy * d.ny * d.vy) +
+                                 std::fabs((double)d.m_offset * d.vx);
+        q.fast_exit = ((-(double)d.dod - half_diag) / ((double)d.dso - (double)d.dod) >= 1e-6) ? 1 : 0;
+    }
     q.entry64 = (d.flags & CTR_GEOM_ENTRY_F64) ? 1 : 0;
     q.vx = d.vx; q.vy = d.vy; q.vz = d.vz;
     // inv_volumn_x = 1.0/volumn_x (double division stored as float), main_recon.cu:88

@@ -16,6 +16,12 @@ SMALL = {
                       initial_angle=1.5),
 }
 
+# The volume within 1e-3 mm of the detector plane: alphas inside the volume
+# below 1e-6, where the projector keeps the reference's loop test as written
+# instead of the single-comparison form.
+NEAR_DETECTOR = dict(nx=16, ny=16, nz=16, nu=48, nv=40, nviews=12, vx=1.0, du=0.4, dso=1000.0, dod=-11.3147,
+                     initial_angle=7.0)
+
 # Scans with no ray lying exactly on a voxel plane.  On such a ray the
 # reference BP evaluates 0/0 and drops the ray while the reference FP keeps it
 # (V63/kernel_IterativeRecon_universal.cu:760-765 versus :218-266), so

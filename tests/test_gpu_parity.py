@@ -10,7 +10,9 @@ filter (FP32 convolution against the FP64 kernel), FP64 reductions.
 import numpy as np
 import pytest
 
-from scan_configs import CONFIG0, NO_ON_PLANE_RAYS, SMALL, ctr_desc, og_desc_xyz
+from scan_configs import CONFIG0, NEAR_DETECTOR, NO_ON_PLANE_RAYS, SMALL, ctr_desc, og_desc_xyz
+
+FP_CASES = dict(SMALL, near_detector=NEAR_DETECTOR)
 
 pytestmark = pytest.mark.gpu
 
@@ -44,9 +46,9 @@ def host(t):
     return t.float().cpu().numpy()
 
 
-@pytest.mark.parametrize("name", sorted(SMALL))
+@pytest.mark.parametrize("name", sorted(FP_CASES))
 def test_forward_bit_exact(name, oracle_built):
-    cfg = SMALL[name]
+    cfg = FP_CASES[name]
     g, o = pair(cfg, oracle_built)
     rng = np.random.default_rng(7)
     vol = rng.uniform(0, 1, o.vol_shape).astype(np.float32)
@@ -57,11 +59,11 @@ def test_forward_bit_exact(name, oracle_built):
         np.testing.assert_array_equal(bits(out[j]), bits(o.forward_view(vol, j, 0)), err_msg=f"view {j}")
 
 
-@pytest.mark.parametrize("name", sorted(SMALL))
+@pytest.mark.parametrize("name", sorted(FP_CASES))
 @pytest.mark.parametrize("entry64", [False, True])
 def test_traversal_index_sets(name, entry64, oracle_built):
     """Every ray visits the same voxel index sequence as the restated reference."""
-    cfg = SMALL[name]
+    cfg = FP_CASES[name]
     g, o = pair(cfg, oracle_built, entry64)
     vol = np.zeros(o.vol_shape, np.float32)
     P = o.view_shape
