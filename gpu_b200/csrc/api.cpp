@@ -64,10 +64,16 @@ ctr_status forward_chunks(Geometry* g, FpArgs a, cudaStream_t st)
 // With ev (3 events per view) the launches are bracketed for timing.
 // With tiled (a scratch of tiled_count elements) the views run on an 8x8-tiled
 // copy of the volume, copied in before and out after; the result is the same.
+// With obj_tiled (a tiled volume) each view's forward projection also writes
+// the objective partials of that volume, [view][row][u/32] into obj_partial:
+// the objective's projection rides on the SART traversal.
 ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
                       unsigned flags, uint32_t seed, int v0, int nv, cudaStream_t st, cudaEvent_t* ev,
-                      const uint32_t* pass_seed = nullptr, void* tiled = nullptr)
+                      const uint32_t* pass_seed = nullptr, void* tiled = nullptr, const void* obj_tiled = nullptr,
+                      double* obj_partial = nullptr)
 {
+    if (obj_tiled && (!tiled || !obj_partial)) return set_error(CTR_ERR_INVALID_ARGUMENT, "fused objective needs tiled");
+    const size_t per_view = objective_partials_per_view(g->dg);
     const long long P = g->npix();
     CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
     void* pv = tiled ? tiled : vol;
@@ -77,6 +83,11 @@ ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, c
         FpArgs a{};
         a.vol = pv; a.vol_dtype = vdt; a.view0 = j; a.nview = 1; a.kind = FP_SART; a.tiled = tiled != nullptr;
         a.out = g->d_rays; a.b = (const char*)sino + (size_t)j * P * dtype_size(sdt); a.b_dtype = sdt;
+        if (obj_tiled) {
+            a.kind = FP_SART_OBJ;
+            a.vol2 = obj_tiled;
+            a.partial = obj_partial + (size_t)j * per_view;
+        }
         CTR_TRY(launch_forward(*g, a, st, nullptr));
         if (ev) CTR_CUDA_TRY(cudaEventRecord(ev[3 * (j - v0) + 1], st));
         BpArgs b{};
@@ -92,18 +103,20 @@ ctr_status sart_views(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, c
 
 ctr_status sart_pass(Geometry* g, void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt, float beta,
                      unsigned flags, uint32_t seed, cudaStream_t st, const uint32_t* pass_seed = nullptr,
-                     void* tiled = nullptr)
+                     void* tiled = nullptr, const void* obj_tiled = nullptr, double* obj_partial = nullptr)
 {
-    return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, 0, g->desc.n_views, st, nullptr, pass_seed, tiled);
+    return sart_views(g, vol, vdt, sino, sdt, beta, flags, seed, 0, g->desc.n_views, st, nullptr, pass_seed, tiled,
+                      obj_tiled, obj_partial);
 }
 
-// Fidelity ||A x - b||^2 (per-block FP64 partials, two-level reduction) and TV
-// of x.  With tiled, the projection reads an 8x8-tiled copy of x made there.
+// Fidelity ||A x - b||^2 (FP64 partials per warp of 32 rays, summed in index
+// order by a two-level reduction) and TV of x.  With tiled, the projection
+// reads an 8x8-tiled copy of x made there.
 ctr_status objective_async(Geometry* g, const void* vol, ctr_dtype vdt, const void* sino, ctr_dtype sdt,
                            double* d_fid, double* d_tv, cudaStream_t st, void* tiled = nullptr)
 {
     const DevGeom& q = g->dg;
-    const size_t per_view = (size_t)((q.R + 31) / 32) * ((q.ZP + 3) / 4);
+    const size_t per_view = objective_partials_per_view(q);
     const size_t nblk = per_view * g->desc.n_views;
     const size_t tvcap = 148 * 64;
     CTR_TRY(ensure_partial(g, std::max(nblk, tvcap) + 2048));
@@ -443,11 +456,12 @@ struct ctr_solver {
     void* y = nullptr;       // working volume: y_k, then x_k during an iteration
     void* xprev = nullptr;   // x_(k-1); after an iteration with FISTA, x_k
     void* yt = nullptr;      // 8x8-tiled scratch copy for the projections
+    void* xt = nullptr;      // 8x8-tiled copy of x_(k-1) for the objective fused into the SART pass
     float t = 1.0f;          // t_(k-1) of V63/main_recon.cu:177
     int k = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    const void* graph_rays = nullptr;   // the ray workspace the graph was captured with
+    cudaGraph_t graph[2] = {nullptr, nullptr};        // SART pass: plain, with the fused objective
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    const void* graph_ws[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // workspaces captured with
     double* d_obj = nullptr; // [2] fid, tv
 };
 
@@ -471,6 +485,7 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
     cudaError_t e;
     if ((e = cudaMalloc(&s->y, bytes)) != cudaSuccess || (e = cudaMalloc(&s->xprev, bytes)) != cudaSuccess ||
         (e = cudaMalloc(&s->yt, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess ||
+        (e = cudaMalloc(&s->xt, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess ||
         (e = cudaMalloc(&s->d_obj, 4 * sizeof(double))) != cudaSuccess || (e = cudaMemset(s->y, 0, bytes)) != cudaSuccess ||
         (e = cudaMemset(s->xprev, 0, bytes)) != cudaSuccess) {
         ctr_status st = cuda_error(e, "solver allocation");
@@ -483,10 +498,12 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
 
 static void drop_graph(ctr_solver* s)
 {
-    if (s->exec) cudaGraphExecDestroy(s->exec);
-    if (s->graph) cudaGraphDestroy(s->graph);
-    s->exec = nullptr;
-    s->graph = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        if (s->exec[i]) cudaGraphExecDestroy(s->exec[i]);
+        if (s->graph[i]) cudaGraphDestroy(s->graph[i]);
+        s->exec[i] = nullptr;
+        s->graph[i] = nullptr;
+    }
 }
 
 extern "C" ctr_status ctr_solver_destroy(ctr_solver* s)
@@ -496,6 +513,7 @@ extern "C" ctr_status ctr_solver_destroy(ctr_solver* s)
     cudaFree(s->y);
     cudaFree(s->xprev);
     cudaFree(s->yt);
+    cudaFree(s->xt);
     cudaFree(s->d_obj);
     delete s;
     return CTR_OK;
@@ -531,35 +549,67 @@ extern "C" ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void
     return CTR_OK;
 }
 
-// One SART pass, captured once as a CUDA graph (2 launches per view) and replayed.
-static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st)
+// One SART pass (fused: also the objective partials of xt), captured once per
+// form as a CUDA graph (2 launches per view) and replayed.
+static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st, bool fused)
 {
+    Geometry* g = s->g;
+    const void* xt = fused ? s->xt : nullptr;
+    CTR_TRY(ensure_rays(g, (size_t)g->npix() * sizeof(float2)));
+    if (fused) CTR_TRY(ensure_partial(g, objective_partials_per_view(g->dg) * g->desc.n_views + 2048));
+    double* part = fused ? g->d_partial : nullptr;
     const bool stoch = (s->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
     if (!s->p.use_graph || stoch)   // the seed changes every pass: issue directly
-        return sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st, nullptr, s->yt);
-    if (s->exec && s->graph_rays != s->g->d_rays) drop_graph(s);   // workspace grown by another call
-    if (!s->exec) {
-        CTR_TRY(ensure_rays(s->g, (size_t)s->g->npix() * sizeof(float2)));
+        return sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st, nullptr, s->yt, xt,
+                         part);
+    const int gi = fused ? 1 : 0;
+    if (s->exec[gi] && (s->graph_ws[gi][0] != g->d_rays || s->graph_ws[gi][1] != part)) {
+        cudaGraphExecDestroy(s->exec[gi]);   // a workspace was reallocated by another call
+        cudaGraphDestroy(s->graph[gi]);
+        s->exec[gi] = nullptr;
+        s->graph[gi] = nullptr;
+    }
+    if (!s->exec[gi]) {
         cudaStream_t cs;
         CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         ctr_status r = CTR_OK;
         if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
         if (r == CTR_OK)
-            r = sart_pass(s->g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, cs, nullptr, s->yt);
+            r = sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, cs, nullptr, s->yt, xt,
+                          part);
         cudaGraph_t gr = nullptr;
         e = cudaStreamEndCapture(cs, &gr);
         if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
         if (r == CTR_OK) {
-            e = cudaGraphInstantiate(&s->exec, gr, 0);
+            e = cudaGraphInstantiate(&s->exec[gi], gr, 0);
             if (e != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
         }
-        s->graph = gr;
-        s->graph_rays = s->g->d_rays;
+        s->graph[gi] = gr;
+        s->graph_ws[gi][0] = g->d_rays;
+        s->graph_ws[gi][1] = part;
         cudaStreamDestroy(cs);
-        if (r != CTR_OK) { drop_graph(s); return r; }
+        if (r != CTR_OK) {
+            if (s->exec[gi]) cudaGraphExecDestroy(s->exec[gi]);
+            if (s->graph[gi]) cudaGraphDestroy(s->graph[gi]);
+            s->exec[gi] = nullptr;
+            s->graph[gi] = nullptr;
+            return r;
+        }
     }
-    CTR_CUDA_TRY(cudaGraphLaunch(s->exec, st));
+    CTR_CUDA_TRY(cudaGraphLaunch(s->exec[gi], st));
+    return CTR_OK;
+}
+
+static ctr_status store_objective(ctr_solver* s, double* obj_out, int it, cudaStream_t st)
+{
+    if (!obj_out) return CTR_OK;
+    double h[2];
+    CTR_CUDA_TRY(cudaMemcpyAsync(h, s->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CTR_CUDA_TRY(cudaStreamSynchronize(st));
+    obj_out[3 * it + 0] = h[1];
+    obj_out[3 * it + 1] = h[0];
+    obj_out[3 * it + 2] = h[0] + 2.0 * (double)s->p.lambda_tv * h[1];   // V63/main_recon.cu:423
     return CTR_OK;
 }
 
@@ -572,8 +622,22 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
     cudaStream_t st = S(stream);
     Geometry* g = s->g;
     for (int it = 0; it < n; ++it) {
+        // The objective of x_(k-1), the previous iteration's result (V63/main_recon.cu:390-430),
+        // is projected in this iteration's SART traversal: x_(k-1) is xprev with
+        // FISTA and the volume the pass starts from without.  The first
+        // iteration of a call and the last x_k use the separate projection.
+        const bool fused = s->p.objective && it > 0;
+        if (fused) {
+            const void* xk1 = s->p.fista ? s->xprev : s->y;
+            CTR_TRY(launch_tiling(*g, xk1, s->xt, s->vdt, true, st));
+            CTR_TRY(objective_async(g, xk1, s->vdt, s->sino, s->sdt, nullptr, s->d_obj + 1, st));   // TV
+        }
         // V63/main_recon.cu:344-386 (FISTA == 1) / :316-341 (FISTA == 0)
-        CTR_TRY(solver_sart(s, (uint32_t)(s->k + 1), st));
+        CTR_TRY(solver_sart(s, (uint32_t)(s->k + 1), st, fused));
+        if (fused) {
+            CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
+            CTR_TRY(store_objective(s, obj_out, it - 1, st));
+        }
         const float lam = s->p.beta * s->p.lambda_tv;     // lambda_denoise_TV = 2*lambda_TV/Lip
         const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // :372
         const float gam = (s->t - 1.0f) / t_k;
@@ -587,18 +651,11 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
             CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, nullptr, nullptr, 0.f, st));
         }
         s->k++;
-        if (s->p.objective) {
+        if (s->p.objective && it == n - 1) {
             const void* xk = s->p.fista ? s->xprev : s->y;
             CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
-            if (obj_out) {
-                double h[2];
-                CTR_CUDA_TRY(cudaMemcpyAsync(h, s->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-                CTR_CUDA_TRY(cudaStreamSynchronize(st));
-                obj_out[3 * it + 0] = h[1];
-                obj_out[3 * it + 1] = h[0];
-                obj_out[3 * it + 2] = h[0] + 2.0 * (double)s->p.lambda_tv * h[1];   // :423
-            }
-        } else if (obj_out) {
+            CTR_TRY(store_objective(s, obj_out, it, st));
+        } else if (!s->p.objective && obj_out) {
             obj_out[3 * it + 0] = obj_out[3 * it + 1] = obj_out[3 * it + 2] = NAN;
         }
     }
@@ -693,8 +750,7 @@ static ctr_status solver_reserve(ctr_solver* s)
     Geometry* g = s->g;
     CTR_TRY(ensure_rays(g, (size_t)g->npix() * sizeof(float2)));
     if (s->p.lambda_tv > 0.f) CTR_TRY(ensure_fgp(g, 9 * (size_t)g->nvox() * dtype_size(s->vdt)));
-    const DevGeom& q = g->dg;
-    const size_t nblk = (size_t)((q.R + 31) / 32) * ((q.ZP + 3) / 4) * g->desc.n_views;
+    const size_t nblk = objective_partials_per_view(g->dg) * g->desc.n_views;
     CTR_TRY(ensure_partial(g, std::max(nblk, (size_t)148 * 64) + 2048));
     return CTR_OK;
 }

@@ -328,7 +328,11 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         cmn = fminf(a0, a1);
         cmx = fmaxf(a0, a1);
     }
-    for (int k = kb; k < ke; ++k) {
+    // voxel and z-cell row addresses advance by a constant per z step
+    const long long vstep = TL ? 64LL * g.Mt * g.Nt : MN;
+    VT* pv = vol + (TL ? (long long)tile_index(g, i, j, kb) : (long long)kb * MN + (long long)j * g.M + i);
+    const float2* __restrict__ zrow = g.zcell + (long long)kb * g.ZP;
+    for (int k = kb; k < ke; ++k, pv += vstep, zrow += g.ZP) {
         // candidate detector rows of voxel k
         const float z1 = PZ[k + 2], zhi = fs(z1, g.srcz);
         const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
@@ -342,7 +346,6 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         vlo = max(vlo, 0);
         vhi = min(vhi, g.ZP - 1);
         float sw = 0.f, sl = 0.f;
-        const float2* __restrict__ zrow = g.zcell + (long long)k * g.ZP;
         auto pair = [&](float a, float bb, float2 zc, float2 rec) {
             const float lo = fmaxf(a, zc.x);
             const float hi = fminf(bb, zc.y);
@@ -366,7 +369,7 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
             pairs(uu, fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)));
         }
         if (!(sl < g.thr_bp)) {                                                // :799-806
-            VT* p = vol + (TL ? (long long)tile_index(g, i, j, k) : (long long)k * MN + (long long)j * g.M + i);
+            VT* p = pv;
             const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, sw), sl));
             if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
             else Store<VT>::st(p, nv);

@@ -103,18 +103,24 @@ ctr_status ensure_tiled(Geometry* g, size_t bytes);
 ctr_status check_device_errors(Geometry* g, cudaStream_t st);
 
 // ---- kernel launchers (implemented in the .cu files) ----
-enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3, FP_DOT = 4 };
+// FP_SART_OBJ: the SART correction of vol and, in the same traversal, the
+// objective residual (A vol2 - b)^2 of a second volume.
+enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3, FP_DOT = 4, FP_SART_OBJ = 5 };
 struct FpArgs {
     const void* vol; ctr_dtype vol_dtype;
     int view0, nview;
     FpKind kind;
     void* out; ctr_dtype out_dtype;       // FORWARD: sino; SART: float2 rays
     const void* b; ctr_dtype b_dtype;     // SART/OBJECTIVE: measured sinogram; DOT: y (offset to view0)
-    double* partial;                      // OBJECTIVE/DOT: one double per block
+    double* partial;                      // OBJECTIVE, SART_OBJ: one double per warp (32 rays of a row),
+                                          // [view - view0][v][u/32]; DOT: one per block
+    const void* vol2 = nullptr;           // SART_OBJ: the volume of the objective (same dtype, layout)
     int* nseg; uint64_t* hash; float* len;  // TRACE
     int tiled = 0;                        // vol in the 8x8-tiled layout (FORWARD, SART, OBJECTIVE)
 };
 ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, size_t* nblocks_out);
+// objective partials per view: one per warp of 32 rays
+inline size_t objective_partials_per_view(const DevGeom& g) { return (size_t)g.ZP * ((g.R + 31) / 32); }
 
 struct BpArgs {
     void* vol; ctr_dtype vol_dtype;

@@ -40,6 +40,7 @@ static constexpr uint64_t kFnvPrime = 1099511628211ULL;
 
 struct RayResult {
     float sum, len, d12;
+    float sum2;         // the same segments over a second volume (DUAL only)
     double dsum;        // the same segments summed in FP64 (ACC64 only)
     float a_lo, a_hi;   // alpha interval the traversal covered (empty when it dropped the ray)
     int vi0, vj0, vk0;  // voxel the traversal starts in
@@ -83,15 +84,16 @@ __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, 
 // The voxel value loaded in a step is accumulated in the next step, so the
 // load's latency overlaps the following traversal step; the sum is the same
 // sequence of roundings.
-template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false, int CPM = 0, bool TL = false>
+template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false, int CPM = 0, bool TL = false,
+          bool DUAL = false>
 __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
                                             const float* __restrict__ PY, const float* __restrict__ PZ,
                                             const float* __restrict__ PINF, const VT* __restrict__ vol, float s,
-                                            float c, int u, int v)
+                                            float c, int u, int v, const VT* __restrict__ vol2 = nullptr)
 {
     const int M = g.M, N = g.N, Z = g.Z;
     RayResult r;
-    r.sum = 0.f; r.len = 0.f; r.dsum = 0.0; r.nseg = 0; r.hash = kFnvOffset;
+    r.sum = 0.f; r.sum2 = 0.f; r.len = 0.f; r.dsum = 0.0; r.nseg = 0; r.hash = kFnvOffset;
     r.a_lo = 1.0f; r.a_hi = 0.0f;
     r.vi0 = r.vj0 = r.vk0 = -1; r.par = 0;
 
@@ -244,6 +246,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     float ac = amin, sum = 0.f, len = 0.f;
     double dsum = 0.0;
     float seg_p = 0.f, f_p = 0.f;   // the previous step's segment and voxel value
+    float sum2 = 0.f, f2_p = 0.f;
     bool any = false;
     // Loop condition after the first step.  Every next-plane alpha is at
     // least ac and grows along its axis, so an index leaves the volume
@@ -273,6 +276,11 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
             const float f = Store<VT>::ld(vol + idx);
             if (ACC64) dsum = __fma_rn((double)seg_p, (double)f_p, dsum);   // +0 on the first step
             else sum = fa(sum, fm(seg_p, f_p));
+            if (DUAL) {
+                const float f2 = Store<VT>::ld(vol2 + idx);
+                sum2 = fa(sum2, fm(seg_p, f2_p));
+                f2_p = f2;
+            }
             seg_p = seg;
             f_p = f;
         }
@@ -325,8 +333,10 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     if (LOAD && any) {
         if (ACC64) dsum = __fma_rn((double)seg_p, (double)f_p, dsum);
         else sum = fa(sum, fm(seg_p, f_p));
+        if (DUAL) sum2 = fa(sum2, fm(seg_p, f2_p));
     }
     r.sum = sum;
+    r.sum2 = sum2;
     r.dsum = dsum;
     r.len = len;
     if (any) {
@@ -336,14 +346,16 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     return r;
 }
 
-// BY detector rows of 32 rays per block.  The partial sums of the objective
-// and the dot product are per tile (tile_x, tile_y, view), so their order
-// does not depend on the issue order.
+// BY detector rows of 32 rays per block.  The objective's partial sums are
+// one per warp (the 32 rays of one detector row segment, a fixed shuffle
+// tree), stored by (view, row, segment), so the totals do not depend on the
+// launch shape or the issue order; the dot product's are per block of the
+// fixed 32x4 shape.
 template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false, int MINB = 1>
 __global__ void __launch_bounds__(FP_BX * BY, MINB)
 k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
           const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
-          uint64_t* __restrict__ hash, float* __restrict__ lens)
+          uint64_t* __restrict__ hash, float* __restrict__ lens, const VT* __restrict__ vol2)
 {
     constexpr int NT = FP_BX * BY;
     extern __shared__ float sp[];
@@ -368,15 +380,19 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     double e2 = 0.0;
     if (active) {
         const float2 sc = g.trig[view0 + w];
-        const RayResult rr =
-            siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL>(g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v);
+        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, KIND == FP_SART_OBJ>(
+            g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v, vol2);
         const bool zero = rr.len < g.thr_fp;                       // :554
         if (KIND == FP_FORWARD) {
             st_any(out, p, out_dt, zero ? 0.0f : rr.sum);
-        } else if (KIND == FP_SART) {
+        } else if (KIND == FP_SART || KIND == FP_SART_OBJ) {
             const float bv = ld_any(b, p, b_dt);
             const float cv = zero ? 0.0f : fdv(fs(bv, rr.sum), rr.len);   // :562
             ((float2*)out)[p] = make_float2(cv, rr.d12);
+            if (KIND == FP_SART_OBJ) {
+                const float e = fs(zero ? 0.0f : rr.sum2, bv);
+                e2 = (double)fm(e, e);                                 // L2_norm_kernel, tool_functions.cu:35
+            }
         } else if (KIND == FP_OBJECTIVE) {
             const float ax = zero ? 0.0f : rr.sum;
             const float bv = ld_any(b, p, b_dt);
@@ -390,7 +406,11 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
             lens[p] = rr.len;
         }
     }
-    if (KIND == FP_OBJECTIVE || KIND == FP_DOT) {
+    if (KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ) {
+        double t = e2;
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if ((threadIdx.x & 31) == 0 && v < g.ZP) partial[((size_t)w * g.ZP + v) * gridDim.x + tx] = t;
+    } else if (KIND == FP_DOT) {
         __shared__ double sh[BY];
         const double t = block_sum(e2, sh);
         if (threadIdx.x == 0) partial[((size_t)blockIdx.z * gridDim.y + ty) * gridDim.x + tx] = t;
@@ -405,16 +425,16 @@ static void launch_fp_tl(const Geometry& G, const FpArgs& a, int nview, size_t s
     const VT* vol = (const VT*)a.vol;
     if (g.entry64)
         k_forward<VT, KIND, true, BY, CPM, TL, MINB><<<grid, FP_BX * BY, smem, st>>>(
-            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2);
     else
         k_forward<VT, KIND, false, BY, CPM, TL, MINB><<<grid, FP_BX * BY, smem, st>>>(
-            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len);
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2);
 }
 
 template <typename VT, int KIND, int BY, int CPM = 0, int MINB = 1>
 static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
-    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE) {
+    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ) {
         if (a.tiled) {
             launch_fp_tl<VT, KIND, BY, CPM, true, MINB>(G, a, nview, smem, st);
             return;
@@ -450,18 +470,22 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
     const DevGeom& g = G.dg;
     if (a.nview <= 0) return CTR_OK;
     if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
-    if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE)
+    if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE && a.kind != FP_SART_OBJ)
         return set_error(CTR_ERR_UNSUPPORTED, "the tiled layout is for SART and objective projections");
-    // reductions keep the fixed shape: their partial sums, and so the
-    // rounding of the totals, do not depend on the tuned shape
+    if (a.kind == FP_SART_OBJ && !a.vol2) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART_OBJ needs vol2");
+    // the dot product keeps the fixed shape: its block partial sums, and so
+    // the rounding of the total, do not depend on the tuned shape
     if (nblocks_out)
-        *nblocks_out = (size_t)((g.R + FP_BX - 1) / FP_BX) * ((g.ZP + FP_BY - 1) / FP_BY) * a.nview;
+        *nblocks_out = (a.kind == FP_OBJECTIVE || a.kind == FP_SART_OBJ)
+                           ? objective_partials_per_view(g) * a.nview
+                           : (size_t)((g.R + FP_BX - 1) / FP_BX) * ((g.ZP + FP_BY - 1) / FP_BY) * a.nview;
     const size_t smem = plane_tables_bytes(g);
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         switch (a.kind) {
         case FP_FORWARD: launch_fp_shape<VT, FP_FORWARD>(G, a, smem, st); break;
         case FP_SART: launch_fp_shape<VT, FP_SART>(G, a, smem, st); break;
-        case FP_OBJECTIVE: launch_fp_t<VT, FP_OBJECTIVE, FP_BY>(G, a, a.nview, smem, st); break;
+        case FP_OBJECTIVE: launch_fp_shape<VT, FP_OBJECTIVE>(G, a, smem, st); break;
+        case FP_SART_OBJ: launch_fp_shape<VT, FP_SART_OBJ>(G, a, smem, st); break;
         case FP_TRACE: launch_fp_t<VT, FP_TRACE, FP_BY>(G, a, a.nview, smem, st); break;
         case FP_DOT: launch_fp_t<VT, FP_DOT, FP_BY>(G, a, a.nview, smem, st); break;
         }
