@@ -463,6 +463,13 @@ struct ctr_solver {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     const void* graph_ws[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // workspaces captured with
     double* d_obj = nullptr; // [2] fid, tv
+    // Objective history on the device, row k-1 = (fidelity, TV) of x_k.  The
+    // objective of the latest x_k is "pending" until the next SART pass
+    // projects it in the same traversal, or until someone asks for it.
+    double* d_hist = nullptr;
+    int hist_cap = 0;
+    std::vector<unsigned char> hist_valid;
+    bool obj_pending = false;
 };
 
 extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt, const ctr_solver_params* p,
@@ -515,9 +522,12 @@ extern "C" ctr_status ctr_solver_destroy(ctr_solver* s)
     cudaFree(s->yt);
     cudaFree(s->xt);
     cudaFree(s->d_obj);
+    cudaFree(s->d_hist);
     delete s;
     return CTR_OK;
 }
+
+static ctr_status flush_objective(ctr_solver* s, cudaStream_t st);
 
 extern "C" ctr_status ctr_solver_set_sinogram(ctr_solver* s, const void* sino, ctr_dtype sdt)
 {
@@ -525,7 +535,10 @@ extern "C" ctr_status ctr_solver_set_sinogram(ctr_solver* s, const void* sino, c
     CTR_TRY(need(s, "solver"));
     CTR_TRY(need(sino, "sino"));
     CTR_TRY(need_dtype(sdt, "sino_dtype"));
-    if (s->sino != sino || s->sdt != sdt) drop_graph(s);
+    if (s->sino != sino || s->sdt != sdt) {
+        CTR_TRY(flush_objective(s, nullptr));   // the pending objective belongs to the old sinogram
+        drop_graph(s);
+    }
     s->sino = sino;
     s->sdt = sdt;
     return CTR_OK;
@@ -546,6 +559,8 @@ extern "C" ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void
     }
     s->t = 1.0f;
     s->k = 0;
+    s->obj_pending = false;
+    s->hist_valid.clear();
     return CTR_OK;
 }
 
@@ -601,15 +616,62 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st, boo
     return CTR_OK;
 }
 
-static ctr_status store_objective(ctr_solver* s, double* obj_out, int it, cudaStream_t st)
+// history rows for iterations 1..k (allocated outside any capture)
+static ctr_status hist_reserve(ctr_solver* s, int k, cudaStream_t st)
 {
-    if (!obj_out) return CTR_OK;
-    double h[2];
-    CTR_CUDA_TRY(cudaMemcpyAsync(h, s->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if ((int)s->hist_valid.size() < k) s->hist_valid.resize(k, 0);
+    if (k <= s->hist_cap) return CTR_OK;
+    const int cap = std::max(k, 2 * s->hist_cap + 16);
+    double* d = nullptr;
+    CTR_CUDA_TRY(cudaMalloc(&d, sizeof(double) * 2 * cap));
+    if (s->d_hist) {
+        cudaError_t e = cudaMemcpyAsync(d, s->d_hist, sizeof(double) * 2 * s->hist_cap, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) { cudaFree(d); return cuda_error(e, "objective history"); }
+        cudaFree(s->d_hist);
+    }
+    s->d_hist = d;
+    s->hist_cap = cap;
+    return CTR_OK;
+}
+
+// d_obj (fid, tv) -> history row of iteration k
+static ctr_status hist_store(ctr_solver* s, int k, cudaStream_t st)
+{
+    CTR_CUDA_TRY(cudaMemcpyAsync(s->d_hist + 2 * (size_t)(k - 1), s->d_obj, 2 * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st));
+    s->hist_valid[k - 1] = 1;
+    return CTR_OK;
+}
+
+// the pending objective of the current x_k, by its own projection
+static ctr_status flush_objective(ctr_solver* s, cudaStream_t st)
+{
+    if (!s->obj_pending) return CTR_OK;
+    const void* xk = s->p.fista ? s->xprev : s->y;
+    CTR_TRY(hist_reserve(s, s->k, st));
+    CTR_TRY(objective_async(s->g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
+    CTR_TRY(hist_store(s, s->k, st));
+    s->obj_pending = false;
+    return CTR_OK;
+}
+
+// history rows of iterations first..first+count-1 as [TV, fidelity, objective]
+static ctr_status read_history(ctr_solver* s, int first, int count, double* out, cudaStream_t st)
+{
+    std::vector<double> h(2 * (size_t)count);
+    CTR_CUDA_TRY(cudaMemcpyAsync(h.data(), s->d_hist + 2 * (size_t)(first - 1), sizeof(double) * 2 * count,
+                                 cudaMemcpyDeviceToHost, st));
     CTR_CUDA_TRY(cudaStreamSynchronize(st));
-    obj_out[3 * it + 0] = h[1];
-    obj_out[3 * it + 1] = h[0];
-    obj_out[3 * it + 2] = h[0] + 2.0 * (double)s->p.lambda_tv * h[1];   // V63/main_recon.cu:423
+    for (int i = 0; i < count; ++i) {
+        if (!s->hist_valid[first - 1 + i]) {
+            out[3 * i + 0] = out[3 * i + 1] = out[3 * i + 2] = NAN;
+            continue;
+        }
+        out[3 * i + 0] = h[2 * i + 1];
+        out[3 * i + 1] = h[2 * i];
+        out[3 * i + 2] = h[2 * i] + 2.0 * (double)s->p.lambda_tv * h[2 * i + 1];   // V63/main_recon.cu:423
+    }
     return CTR_OK;
 }
 
@@ -621,12 +683,13 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
     if (n < 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "n < 0");
     cudaStream_t st = S(stream);
     Geometry* g = s->g;
+    const int k0 = s->k;
+    CTR_TRY(hist_reserve(s, k0 + n, st));
     for (int it = 0; it < n; ++it) {
         // The objective of x_(k-1), the previous iteration's result (V63/main_recon.cu:390-430),
         // is projected in this iteration's SART traversal: x_(k-1) is xprev with
-        // FISTA and the volume the pass starts from without.  The first
-        // iteration of a call and the last x_k use the separate projection.
-        const bool fused = s->p.objective && it > 0;
+        // FISTA and the volume the pass starts from without.
+        const bool fused = s->obj_pending;
         if (fused) {
             const void* xk1 = s->p.fista ? s->xprev : s->y;
             CTR_TRY(launch_tiling(*g, xk1, s->xt, s->vdt, true, st));
@@ -636,7 +699,8 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
         CTR_TRY(solver_sart(s, (uint32_t)(s->k + 1), st, fused));
         if (fused) {
             CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
-            CTR_TRY(store_objective(s, obj_out, it - 1, st));
+            CTR_TRY(hist_store(s, s->k, st));
+            s->obj_pending = false;
         }
         const float lam = s->p.beta * s->p.lambda_tv;     // lambda_denoise_TV = 2*lambda_TV/Lip
         const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // :372
@@ -651,15 +715,27 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
             CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, nullptr, nullptr, 0.f, st));
         }
         s->k++;
-        if (s->p.objective && it == n - 1) {
-            const void* xk = s->p.fista ? s->xprev : s->y;
-            CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
-            CTR_TRY(store_objective(s, obj_out, it, st));
-        } else if (!s->p.objective && obj_out) {
-            obj_out[3 * it + 0] = obj_out[3 * it + 1] = obj_out[3 * it + 2] = NAN;
-        }
+        s->obj_pending = s->p.objective != 0;
+    }
+    if (obj_out && n > 0) {
+        CTR_TRY(flush_objective(s, st));
+        CTR_TRY(read_history(s, k0 + 1, n, obj_out, st));
     }
     return check_device_errors(g, st);
+}
+
+extern "C" ctr_status ctr_solver_objectives(ctr_solver* s, int first, int count, double* out, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    CTR_TRY(need(out, "out"));
+    if (first < 1 || count < 0 || first + count - 1 > s->k)
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "iterations %d..%d not run (k = %d)", first, first + count - 1, s->k);
+    if (count == 0) return CTR_OK;
+    cudaStream_t st = S(stream);
+    CTR_TRY(hist_reserve(s, s->k, st));
+    if (first + count - 1 == s->k) CTR_TRY(flush_objective(s, st));
+    return read_history(s, first, count, out, st);
 }
 
 extern "C" ctr_status ctr_solver_get_volume(ctr_solver* s, void* dst, void* stream)
@@ -739,6 +815,8 @@ extern "C" ctr_status ctr_solver_load(ctr_solver* s, const char* path, void* str
     CTR_CUDA_TRY(cudaStreamSynchronize(S(stream)));
     s->k = h.k;
     s->t = h.t;
+    s->obj_pending = false;                       // objectives before the checkpoint are not known here
+    s->hist_valid.assign((size_t)std::max(h.k, 0), 0);
     return CTR_OK;
 }
 

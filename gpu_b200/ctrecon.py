@@ -49,6 +49,7 @@ EXPORTED = [
     "ctr_io_read_raw", "ctr_io_read_views", "ctr_io_write_views",
     "ctr_batch_create", "ctr_batch_destroy", "ctr_batch_set_sinogram", "ctr_batch_reset", "ctr_batch_iterate",
     "ctr_batch_get_volume", "ctr_geometry_set_shapes", "ctr_geometry_get_shapes", "ctr_geometry_autotune",
+    "ctr_solver_objectives",
 ]
 
 
@@ -136,6 +137,7 @@ def load_library(path: str = LIB_PATH):
         "ctr_io_read_raw": ([C.c_char_p, vp, C.c_size_t, C.c_size_t], i),
         "ctr_io_read_views": ([C.c_char_p, i, i, i, f, f, i, i, vp], i),
         "ctr_io_write_views": ([C.c_char_p, i, i, i, f, f, i, vp], i),
+        "ctr_solver_objectives": ([vp, i, i, vp, vp], i),
         "ctr_geometry_set_shapes": ([G, i, i], i),
         "ctr_geometry_get_shapes": ([G, C.POINTER(i), C.POINTER(i)], i),
         "ctr_geometry_autotune": ([G, i, i, C.POINTER(f), C.POINTER(f), vp], i),
@@ -375,10 +377,22 @@ class Solver:
     def set_volume(self, vol=None, stream=None):
         check(self.lib.ctr_solver_set_volume(self.h, _ptr(vol), _stream(stream)))
 
-    def iterate(self, n, stream=None):
+    def iterate(self, n, stream=None, objectives=True):
+        """n iterations; returns their [TV, fidelity, objective] rows, or None
+        with objectives=False (the last objective is then projected inside the
+        next call's first SART pass, or by ``objectives()``)."""
+        if not objectives:
+            check(self.lib.ctr_solver_iterate(self.h, n, None, _stream(stream)))
+            return None
         obj = np.zeros(3 * max(n, 1), np.float64)
         check(self.lib.ctr_solver_iterate(self.h, n, obj.ctypes.data, _stream(stream)))
         return obj[: 3 * n].reshape(n, 3)
+
+    def objectives(self, first, count, stream=None):
+        """Objective history rows of iterations first..first+count-1 (1-based)."""
+        obj = np.zeros(3 * max(count, 1), np.float64)
+        check(self.lib.ctr_solver_objectives(self.h, first, count, obj.ctypes.data, _stream(stream)))
+        return obj[: 3 * count].reshape(count, 3)
 
     def get_volume(self, out, stream=None):
         check(self.lib.ctr_solver_get_volume(self.h, _ptr(out), _stream(stream)))

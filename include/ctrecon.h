@@ -253,6 +253,13 @@ ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* objective_out, void*
 /* Copy the current estimate x_k (vol_dtype) to dst (device or host). */
 ctr_status ctr_solver_get_volume(ctr_solver* s, void* dst, void* stream);
 ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k);
+/* Objective history [TV, fidelity, objective] of iterations first..first+count-1
+ * (1-based, at most the iterations run).  With objective_out == NULL,
+ * ctr_solver_iterate leaves the objective of its last x_k pending and projects
+ * it inside the next call's first SART traversal; asking for it here
+ * projects it at once.  Rows the solver never evaluated (before a checkpoint
+ * load) are NaN.  Synchronises. */
+ctr_status ctr_solver_objectives(ctr_solver* s, int first, int count, double* out, void* stream);
 /* Exact checkpoint of the FISTA state (x_k, y_k, t_k, k and a geometry hash),
  * raw little-endian, and its restore. */
 ctr_status ctr_solver_save(ctr_solver* s, const char* path, void* stream);

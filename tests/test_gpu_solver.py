@@ -120,13 +120,21 @@ def test_fused_objective_equals_separate(fista, oracle_built):
     b = torch.from_numpy(np.stack([o.forward_view(truth, j, 0) for j in range(cfg["nviews"])])).cuda()
     g = gpu_b200.Geometry(ctr_desc(cfg))
     runs = []
-    for calls in ([3], [1, 1, 1]):
+    for calls in ([3], [1, 1, 1], "deferred"):
         s = gpu_b200.Solver(g, gpu_b200.F32, beta=0.8, lambda_tv=0.05, fgp_iters=4, fista=fista)
         s.set_sinogram(b)
         s.set_volume(None)
-        objs = np.concatenate([s.iterate(c) for c in calls])
+        if calls == "deferred":   # objectives left pending, projected in the next call, read at the end
+            for _ in range(3):
+                assert s.iterate(1, objectives=False) is None
+            objs = s.objectives(1, 3)
+        else:
+            objs = np.concatenate([s.iterate(c) for c in calls])
         out = torch.zeros(o.vol_shape, device="cuda")
         s.get_volume(out)
         runs.append((objs, bits(out.cpu().numpy())))
-    np.testing.assert_array_equal(runs[0][1], runs[1][1])
-    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    for r in runs[1:]:
+        np.testing.assert_array_equal(runs[0][1], r[1])
+        np.testing.assert_array_equal(runs[0][0], r[0])
+    with pytest.raises(gpu_b200.CtrError):
+        s.objectives(1, 4)
