@@ -827,7 +827,7 @@ static ctr_status solver_reserve(ctr_solver* s)
 {
     Geometry* g = s->g;
     CTR_TRY(ensure_rays(g, (size_t)g->npix() * sizeof(float2)));
-    if (s->p.lambda_tv > 0.f) CTR_TRY(ensure_fgp(g, 9 * (size_t)g->nvox() * dtype_size(s->vdt)));
+    if (s->p.lambda_tv > 0.f) CTR_TRY(ensure_fgp(g, fgp_workspace_bytes(g->nvox(), s->vdt)));
     const size_t nblk = objective_partials_per_view(g->dg) * g->desc.n_views;
     CTR_TRY(ensure_partial(g, std::max(nblk, (size_t)148 * 64) + 2048));
     return CTR_OK;

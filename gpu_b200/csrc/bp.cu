@@ -237,7 +237,7 @@ ctr_status launch_zcell(const Geometry& G, float2* zcell, cudaStream_t st)
 // arithmetic, so the two give bit-identical volumes.
 constexpr int WALK_RUN = 4;   // detector columns of the run kept in registers
 
-template <typename VT, bool STOCH, int BY, int MINB, bool TL>
+template <typename VT, bool STOCH, int BY, int MINB, bool TL, int UNR>
 __global__ void __launch_bounds__(32 * BY, MINB)
 k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
             uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
@@ -357,7 +357,17 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         };
         auto pairs = [&](int uu, float a, float bb) {
             if (!(bb > a)) return;
-            for (int vv = vlo; vv <= vhi; ++vv) pair(a, bb, __ldg(zrow + vv), __ldg(rays + (long long)vv * R + uu));
+            int vv = vlo;
+            if (UNR == 2) {   // two rows' loads in flight, then their pairs in row order
+                for (; vv < vhi; vv += 2) {
+                    const float2 z0c = __ldg(zrow + vv), z1c = __ldg(zrow + vv + 1);
+                    const float2 r0 = __ldg(rays + (long long)vv * R + uu);
+                    const float2 r1 = __ldg(rays + (long long)(vv + 1) * R + uu);
+                    pair(a, bb, z0c, r0);
+                    pair(a, bb, z1c, r1);
+                }
+            }
+            for (; vv <= vhi; ++vv) pair(a, bb, __ldg(zrow + vv), __ldg(rays + (long long)vv * R + uu));
         };
 #pragma unroll
         for (int q = 0; q < WALK_RUN; ++q)
@@ -414,9 +424,9 @@ ctr_status launch_tiling(const Geometry& G, const void* src, void* dst, ctr_dtyp
 // block, the longest z run per thread (shortened for small volumes so that
 // the grid still fills the GPU) and the blocks per SM the registers are
 // capped for.
-struct BpShape { int rows, zl, minb; };
-static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8, 8}, {4, 32, 8}, {4, 32, 10}, {8, 32, 4}, {4, 128, 8},
-                                                 {4, 128, 10}};
+struct BpShape { int rows, zl, minb, unroll; };
+static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8, 8, 1}, {4, 32, 8, 1}, {4, 32, 8, 2}, {8, 32, 4, 1},
+                                                 {4, 128, 8, 1}, {4, 32, 10, 1}};
 
 template <typename VT, bool STOCH, bool TL>
 static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStream_t st, size_t smem)
@@ -430,14 +440,17 @@ static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStrea
     if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
     const float2* rays = (const float2*)a.rays;
     if (sh.rows == 8)
-        k_sart_walk<VT, STOCH, 8, 4, TL><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                                  a.pass_seed, zl);
+        k_sart_walk<VT, STOCH, 8, 4, TL, 1><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                     a.pass_seed, zl);
     else if (sh.minb == 10)
-        k_sart_walk<VT, STOCH, 4, 10, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                                   a.pass_seed, zl);
+        k_sart_walk<VT, STOCH, 4, 10, TL, 1><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                      a.pass_seed, zl);
+    else if (sh.unroll == 2)
+        k_sart_walk<VT, STOCH, 4, 8, TL, 2><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                     a.pass_seed, zl);
     else
-        k_sart_walk<VT, STOCH, 4, 8, TL><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                                  a.pass_seed, zl);
+        k_sart_walk<VT, STOCH, 4, 8, TL, 1><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                     a.pass_seed, zl);
     return CTR_OK;
 }
 

@@ -99,6 +99,8 @@ inline bool dtype_ok(int t) { return t == CTR_F32 || t == CTR_BF16 || t == CTR_F
 ctr_status ensure_rays(Geometry* g, size_t bytes);
 ctr_status ensure_partial(Geometry* g, size_t n);
 ctr_status ensure_fgp(Geometry* g, size_t bytes);
+// FGP workspace: six duals in the storage type and L in FP32
+inline size_t fgp_workspace_bytes(long long V, ctr_dtype dt) { return (size_t)V * (6 * dtype_size(dt) + 4); }
 ctr_status ensure_tiled(Geometry* g, size_t bytes);
 ctr_status check_device_errors(Geometry* g, cudaStream_t st);
 

@@ -2,14 +2,8 @@
 //
 // FGP restates FGP_denoise_GPUx7_exact (V63/host_FGP_Denoise_GPUx7.c:1-111)
 // and its kernels FGP_operator_L_Pc / FGP_operator_LT_Pp
-// (V63/kernel_FGP_Denoise_GPUx7.cu:2-88) with the same float operations, but
-// one kernel per inner iteration instead of two: each thread walks a z run of
-// one (x, y) column, evaluates L = f - lambda*div(r,s,t) at its voxel and at the
-// +x, +y, +z neighbours on the fly, and writes the projected, extrapolated
-// duals.  The extrapolated duals r,s,t are double-buffered (read A, write B),
-// so no thread reads a dual another thread has already advanced.  Per inner
-// iteration the kernel streams f and 6 duals in and 6 duals out: 13 volumes,
-// where the two-kernel form moves 18.
+// (V63/kernel_FGP_Denoise_GPUx7.cu:2-88) with the same float operations.  The
+// duals are stored in the volume's storage type; L stays FP32.
 //
 // Dual layout: volume-sized arrays; r[p] belongs to the edge (x, x+1) and is 0
 // at x = nx-1 (the reference's zero-padded d_r[x+1], V63/host_FGP_Denoise_
@@ -18,7 +12,7 @@
 
 namespace ctr {
 
-static constexpr int FG_BX = 32, FG_BY = 8, FG_ZRUN = 32;
+static constexpr int FG_BX = 32, FG_BY = 8;
 
 template <typename T>
 __device__ __forceinline__ float fgp_L(const T* __restrict__ f, const T* __restrict__ r, const T* __restrict__ s,
@@ -32,70 +26,62 @@ __device__ __forceinline__ float fgp_L(const T* __restrict__ f, const T* __restr
     return fs(Store<T>::ld(f + p), fm(lambda, tl));                    // :17
 }
 
-// One inner iteration.  A block owns a 32x8 (x, y) tile and walks a z run;
-// L = f - lambda*div(r,s,t) of the next slice, tile plus its +x column and +y
-// row, goes to shared memory once, so each L is evaluated ~1.16 times instead
-// of four (own voxel, -x, -y and -z neighbours).
+// One inner iteration in two passes, as the reference's x7 form: k_fgp_L
+// writes L = f - lambda*div(r,s,t) (FP32, as the reference keeps it) for every
+// voxel; k_fgp_dual reads L at the voxel and its +x, +y, +z neighbours and
+// updates the voxel's own duals in place (no voxel reads another's duals in
+// this pass, so no double buffer is needed).  One thread per voxel, a 3-D
+// grid of 32x8 tiles: both passes stream at close to the copy bandwidth.
 template <typename T>
 __global__ void __launch_bounds__(FG_BX * FG_BY)
-k_fgp_step(int M, int N, int Z, const T* __restrict__ f, const T* __restrict__ rA, const T* __restrict__ sA,
-           const T* __restrict__ tA, T* __restrict__ rB, T* __restrict__ sB, T* __restrict__ tB, T* __restrict__ o,
-           T* __restrict__ pd, T* __restrict__ q, float lambda, float alpha12, float gam)
+k_fgp_L(int M, int N, int Z, const T* __restrict__ f, const T* __restrict__ r, const T* __restrict__ s,
+        const T* __restrict__ t, float* __restrict__ L, float lambda)
 {
-    __shared__ float Ls[2][FG_BY + 1][FG_BX + 1];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x = blockIdx.x * FG_BX + tx;
-    const int y = blockIdx.y * FG_BY + ty;
-    const int z0 = blockIdx.z * FG_ZRUN;
-    const int z1 = min(z0 + FG_ZRUN, Z);
-    const bool own = x < M && y < N;
+    const int x = blockIdx.x * FG_BX + threadIdx.x;
+    const int y = blockIdx.y * FG_BY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= M || y >= N) return;
     const long long MN = (long long)M * N;
-    // halo: warp 0 computes the +y row (x of its lane), warp 1 lanes 0..7 the +x column
-    const int hx = ty == 0 ? x : (ty == 1 && tx < FG_BY ? blockIdx.x * FG_BX + FG_BX : -1);
-    const int hy = ty == 0 ? blockIdx.y * FG_BY + FG_BY : (ty == 1 && tx < FG_BY ? blockIdx.y * FG_BY + tx : -1);
-    const bool halo = hx >= 0 && hx < M && hy < N;
-    const int hsx = ty == 0 ? tx : FG_BX, hsy = ty == 0 ? FG_BY : tx;
-    auto slice = [&](int z, int b) {   // L of slice z into Ls[b]
-        if (own) Ls[b][ty][tx] = fgp_L(f, rA, sA, tA, x, y, z, (long long)z * MN + (long long)y * M + x, M, MN, lambda);
-        if (halo)
-            Ls[b][hsy][hsx] = fgp_L(f, rA, sA, tA, hx, hy, z, (long long)z * MN + (long long)hy * M + hx, M, MN, lambda);
-    };
-    if (z0 < z1) slice(z0, 0);
-    int cur = 0;
-    long long p = (long long)z0 * MN + (long long)y * M + x;
-    for (int z = z0; z < z1; ++z, p += MN) {
-        if (z < Z - 1) slice(z + 1, cur ^ 1);
-        __syncthreads();
-        if (own) {
-            const float Lc = Ls[cur][ty][tx];
-            const float Lz = (z < Z - 1) ? Ls[cur ^ 1][ty][tx] : 0.0f;
-            const float Lx = (x < M - 1) ? Ls[cur][ty][tx + 1] : 0.0f;
-            const float Ly = (y < N - 1) ? Ls[cur][ty + 1][tx] : 0.0f;
-            // LT_Pp (V63/kernel_FGP_Denoise_GPUx7.cu:52-86)
-            float tr = Store<T>::ld(rA + p), ts = Store<T>::ld(sA + p), tt = Store<T>::ld(tA + p);
-            if (x < M - 1) tr = fa(tr, fm(alpha12, fs(Lc, Lx)));
-            if (y < N - 1) ts = fa(ts, fm(alpha12, fs(Lc, Ly)));
-            if (z < Z - 1) tt = fa(tt, fm(alpha12, fs(Lc, Lz)));
-            const float rst = __fsqrt_rn(fa(fa(fm(tr, tr), fm(ts, ts)), fm(tt, tt)));
-            const float den = fmaxf(1.0f, rst);
-            if (x < M - 1) {
-                const float on = fdv(tr, den);
-                Store<T>::st(rB + p, fa(on, fm(gam, fs(on, Store<T>::ldw(o + p)))));
-                Store<T>::st(o + p, on);
-            }
-            if (y < N - 1) {
-                const float pn = fdv(ts, den);
-                Store<T>::st(sB + p, fa(pn, fm(gam, fs(pn, Store<T>::ldw(pd + p)))));
-                Store<T>::st(pd + p, pn);
-            }
-            if (z < Z - 1) {
-                const float qn = fdv(tt, den);
-                Store<T>::st(tB + p, fa(qn, fm(gam, fs(qn, Store<T>::ldw(q + p)))));
-                Store<T>::st(q + p, qn);
-            }
-        }
-        __syncthreads();
-        cur ^= 1;
+    const long long p = (long long)z * MN + (long long)y * M + x;
+    L[p] = fgp_L(f, r, s, t, x, y, z, p, M, MN, lambda);                 // L_Pc, GPUx7.cu:2-24
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FG_BX * FG_BY)
+k_fgp_dual(int M, int N, int Z, const float* __restrict__ L, T* __restrict__ r, T* __restrict__ s,
+           T* __restrict__ t, T* __restrict__ o, T* __restrict__ pd, T* __restrict__ q, float alpha12, float gam)
+{
+    const int x = blockIdx.x * FG_BX + threadIdx.x;
+    const int y = blockIdx.y * FG_BY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= M || y >= N) return;
+    const long long MN = (long long)M * N;
+    const long long p = (long long)z * MN + (long long)y * M + x;
+    const float Lc = __ldg(L + p);
+    const float Lx = (x < M - 1) ? __ldg(L + p + 1) : 0.0f;
+    const float Ly = (y < N - 1) ? __ldg(L + p + M) : 0.0f;
+    const float Lz = (z < Z - 1) ? __ldg(L + p + MN) : 0.0f;
+    // LT_Pp (V63/kernel_FGP_Denoise_GPUx7.cu:52-86)
+    float tr = Store<T>::ldw(r + p), ts = Store<T>::ldw(s + p), tt = Store<T>::ldw(t + p);
+    if (x < M - 1) tr = fa(tr, fm(alpha12, fs(Lc, Lx)));
+    if (y < N - 1) ts = fa(ts, fm(alpha12, fs(Lc, Ly)));
+    if (z < Z - 1) tt = fa(tt, fm(alpha12, fs(Lc, Lz)));
+    const float rst = __fsqrt_rn(fa(fa(fm(tr, tr), fm(ts, ts)), fm(tt, tt)));
+    const float den = fmaxf(1.0f, rst);
+    if (x < M - 1) {
+        const float on = fdv(tr, den);
+        Store<T>::st(r + p, fa(on, fm(gam, fs(on, Store<T>::ldw(o + p)))));
+        Store<T>::st(o + p, on);
+    }
+    if (y < N - 1) {
+        const float pn = fdv(ts, den);
+        Store<T>::st(s + p, fa(pn, fm(gam, fs(pn, Store<T>::ldw(pd + p)))));
+        Store<T>::st(pd + p, pn);
+    }
+    if (z < Z - 1) {
+        const float qn = fdv(tt, den);
+        Store<T>::st(t + p, fa(qn, fm(gam, fs(qn, Store<T>::ldw(q + p)))));
+        Store<T>::st(q + p, qn);
     }
 }
 
@@ -158,30 +144,28 @@ ctr_status launch_fgp(Geometry& G, void* vol, ctr_dtype dt, float lambda, int it
     const int M = G.desc.nx, N = G.desc.ny, Z = G.desc.nz;
     const long long V = G.nvox();
     const size_t es = dtype_size(dt);
-    CTR_TRY(ensure_fgp(&G, 9 * (size_t)V * es));
-    CTR_CUDA_TRY(cudaMemsetAsync(G.d_fgp, 0, 9 * (size_t)V * es, st));
+    CTR_TRY(ensure_fgp(&G, fgp_workspace_bytes(V, dt)));
+    CTR_CUDA_TRY(cudaMemsetAsync(G.d_fgp, 0, 6 * (size_t)V * es, st));
     const float alpha12 = 1.0f / (lambda * 12.0f);                 // :166
-    dim3 blk(FG_BX, FG_BY), grd((M + FG_BX - 1) / FG_BX, (N + FG_BY - 1) / FG_BY, (Z + FG_ZRUN - 1) / FG_ZRUN);
+    const dim3 blk(FG_BX, FG_BY), grd((M + FG_BX - 1) / FG_BX, (N + FG_BY - 1) / FG_BY, Z);
     CTR_DISPATCH_DTYPE(dt, T, {
         T* base = (T*)G.d_fgp;
-        T* A[3] = {base, base + V, base + 2 * V};
-        T* B[3] = {base + 3 * V, base + 4 * V, base + 5 * V};
-        T* O[3] = {base + 6 * V, base + 7 * V, base + 8 * V};
+        T* D[6] = {base, base + V, base + 2 * V, base + 3 * V, base + 4 * V, base + 5 * V};   // r s t o p q
+        float* L = (float*)((char*)G.d_fgp + 6 * (size_t)V * es);
         float t_k_1 = 1.0f;
         for (int it = 0; it < iters; ++it) {
             const float t_k = next_t(t_k_1);
             const float gam = (t_k_1 - 1.0f) / t_k;
-            k_fgp_step<T><<<grd, blk, 0, st>>>(M, N, Z, (const T*)vol, A[0], A[1], A[2], B[0], B[1], B[2], O[0], O[1],
-                                               O[2], lambda, alpha12, gam);
-            for (int a = 0; a < 3; ++a) { T* tmp = A[a]; A[a] = B[a]; B[a] = tmp; }
+            k_fgp_L<T><<<grd, blk, 0, st>>>(M, N, Z, (const T*)vol, D[0], D[1], D[2], L, lambda);
+            k_fgp_dual<T><<<grd, blk, 0, st>>>(M, N, Z, L, D[0], D[1], D[2], D[3], D[4], D[5], alpha12, gam);
             t_k_1 = t_k;
         }
         if (fista_y) {
             if (fista_y != vol) return set_error(CTR_ERR_INVALID_ARGUMENT, "fused FISTA output must alias the volume");
-            k_fgp_final<T, true><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, O[0], O[1], O[2], lambda,
+            k_fgp_final<T, true><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, D[3], D[4], D[5], lambda,
                                                                     (T*)fista_xprev, fista_gamma, gamma_dev);
         } else {
-            k_fgp_final<T, false><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, O[0], O[1], O[2], lambda,
+            k_fgp_final<T, false><<<grid_for(V, 256), 256, 0, st>>>(M, N, Z, (T*)vol, D[3], D[4], D[5], lambda,
                                                                      nullptr, 0.0f, nullptr);
         }
     });

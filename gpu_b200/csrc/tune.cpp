@@ -1,10 +1,11 @@
 // tune.cpp -- launch shapes of the SART projectors and their tuner.
 //
 // The forward projector runs 32 x {2, 4, 8} rays per block, with plane
-// coordinates read from shared memory or computed; the SART
-// backprojector runs either the fixed-shape kernel (8 voxels of a column per
-// thread) or the column walk with {4, 8} voxel rows per block, a z run of
-// {8, 32, 128} voxels and registers capped or not for 10 blocks per SM.  Every shape computes each ray and each voxel with
+// coordinates read from shared memory or computed; the SART backprojector
+// runs either the fixed-shape kernel (8 voxels of a column per thread) or the
+// column walk with {4, 8} voxel rows per block, a z run of {8, 32, 128}
+// voxels, registers capped for 8 or 10 blocks per SM, and one or two detector
+// rows per batch of loads.  Every shape computes each ray and each voxel with
 // the same operations in the same order, so the shape changes the speed and
 // never the result.  ctr_geometry_autotune times each shape on a few views
 // spread over the scan and keeps the fastest, on the tiled layout the solver

@@ -89,8 +89,9 @@ ctr_status ctr_geometry_view_trig(const ctr_geometry* geom, int view, float* sin
  * (2, table, -) (4, table, -) (8, table, -) (4, table, 16) (4, table, 12)
  * (4, table read one plane ahead, -) (4, computed, -).  bp_shape -1: the fixed-shape backprojector (8 voxels of a
  * column per thread); 0..5: the column walk with (voxel rows per block, z
- * run, blocks per SM the registers are capped for) = (4,8,8) (4,32,8)
- * (4,32,10) (8,32,4) (4,128,8) (4,128,10).  Results never depend on
+ * run, blocks per SM the registers are capped for, detector rows loaded
+ * together) = (4,8,8,1) (4,32,8,1) (4,32,8,2) (8,32,4,1) (4,128,8,1)
+ * (4,32,10,1).  Results never depend on
  * the shape.  Defaults: fp_shape 1, bp_shape 1.  Not thread-safe against
  * launches on the same geometry. */
 ctr_status ctr_geometry_set_shapes(ctr_geometry* geom, int fp_shape, int bp_shape);
