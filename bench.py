@@ -370,7 +370,11 @@ def run_batched(args):
         s32.get_volume(want)
         s32.close()
         errs.append(float(torch.sqrt(torch.mean((got.float() - want) ** 2)) / want.abs().max().clamp_min(1e-30)))
-    launches = sum(2 + 2 * sp["n_views"] + FGP_ITERS + 1 + 1 + 1 + 2 + 1 + 1 for sp in specs) * iters
+    # per scan and step: tile, FP + BP per view, untile, FGP (2 per inner step
+    # + final); from the second step the previous objective fused (tile, TV +
+    # reduce, 2-level reduce); after the last step the objective (tile, FP,
+    # 2 reduce, TV, reduce)
+    launches = sum((2 + 2 * sp["n_views"] + 2 * FGP_ITERS + 1) * iters + 5 * (iters - 1) + 6 for sp in specs)
     line = {
         "metric": "batched SART-FISTA-TV voxel-updates/s", "value": updates * 1000.0 / ms,
         "unit": "voxel-updates/s", "n_gpus": 1, "steps": iters, "warmup": args.warmup, "ms_per_step": ms,
@@ -645,11 +649,11 @@ def main():
         ms_mixed = runs["mixed"]["ms"]
         ms_f32 = runs["f32"]["ms"]
         value = world * 1000.0 / ms_mixed
-        # every step: SART (tile, FP + BP per view, untile), FGP (inner steps +
-        # final); objective of steps 1..K-1 fused into the next SART pass (tile
+        # every step: SART (tile, FP + BP per view, untile), FGP (2 per inner
+        # step + final); objective of steps 1..K-1 fused into the next SART pass (tile
         # x, TV + reduce, 2-level reduce of the partials); of step K separate
         # (tile, FP, 2 reduce, TV, reduce)
-        launches_per_step = 2 + 2 * SCAN["n_views"] + FGP_ITERS + 1
+        launches_per_step = 2 + 2 * SCAN["n_views"] + 2 * FGP_ITERS + 1
         launches_total = launches_per_step * args.steps + 5 * (args.steps - 1) + 6
         line = {
             "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,

@@ -833,13 +833,24 @@ static ctr_status solver_reserve(ctr_solver* s)
     return CTR_OK;
 }
 
-// One outer iteration of V63/main_recon.cu:344-430 for one scan on stream st;
+// One outer iteration of V63/main_recon.cu:344-386 for one scan on stream st;
 // the FISTA factor and the stochastic-rounding seed of the pass are read from
-// device memory so the launches can be replayed.
-static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_dev, const uint32_t* seed_dev)
+// device memory so the launches can be replayed.  fused: the SART traversal
+// also projects the objective of x_(k-1) (into d_obj), as ctr_solver_iterate
+// does from the second iteration of a call on.
+static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_dev, const uint32_t* seed_dev,
+                               bool fused)
 {
     Geometry* g = s->g;
-    CTR_TRY(sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, st, seed_dev, s->yt));
+    if (fused) {
+        const void* xk1 = s->p.fista ? s->xprev : s->y;
+        CTR_TRY(launch_tiling(*g, xk1, s->xt, s->vdt, true, st));
+        CTR_TRY(objective_async(g, xk1, s->vdt, s->sino, s->sdt, nullptr, s->d_obj + 1, st));   // TV
+    }
+    CTR_TRY(sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, st, seed_dev, s->yt,
+                      fused ? s->xt : nullptr, fused ? g->d_partial : nullptr));
+    if (fused)
+        CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
     const float lam = s->p.beta * s->p.lambda_tv;
     if (s->p.fista) {
         if (s->p.lambda_tv > 0.f)
@@ -848,10 +859,6 @@ static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_
             CTR_TRY(launch_momentum(*g, s->y, s->xprev, s->y, s->vdt, 0.f, st, gam_dev));
     } else if (s->p.lambda_tv > 0.f) {
         CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, nullptr, nullptr, 0.f, st));
-    }
-    if (s->p.objective) {
-        const void* xk = s->p.fista ? s->xprev : s->y;
-        CTR_TRY(objective_async(g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
     }
     return CTR_OK;
 }
@@ -865,9 +872,10 @@ struct ctr_batch {
     uint32_t* d_seed = nullptr;             // per scan stochastic-rounding seed of the coming pass
     std::vector<float> h_gam;
     std::vector<uint32_t> h_seed;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    std::vector<const void*> ws;            // workspaces the graph was captured with, 3 per scan
+    // one iteration of every scan: [0] plain, [1] with the previous objective fused
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    std::vector<const void*> ws[2];         // workspaces each graph was captured with, 3 per scan
 };
 
 static std::vector<const void*> batch_workspaces(const ctr_batch* b)
@@ -881,12 +889,43 @@ static std::vector<const void*> batch_workspaces(const ctr_batch* b)
     return w;
 }
 
-static void batch_drop_graph(ctr_batch* b)
+static void batch_drop_graph(ctr_batch* b, int which = -1)
 {
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        if (which >= 0 && which != i) continue;
+        if (b->exec[i]) cudaGraphExecDestroy(b->exec[i]);
+        if (b->graph[i]) cudaGraphDestroy(b->graph[i]);
+        b->exec[i] = nullptr;
+        b->graph[i] = nullptr;
+    }
+}
+
+static ctr_status batch_capture(ctr_batch* b, int gi)
+{
+    const int ns = (int)b->scans.size();
+    for (auto* s : b->scans) CTR_TRY(solver_reserve(s));
+    CTR_CUDA_TRY(cudaDeviceSynchronize());
+    cudaStream_t cs;
+    CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    ctr_status r = CTR_OK;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
+    if (r == CTR_OK && (e = cudaEventRecord(b->fork, cs)) != cudaSuccess) r = cuda_error(e, "cudaEventRecord");
+    for (int i = 0; i < ns && r == CTR_OK; ++i) {
+        if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
+        r = solver_issue(b->scans[i], b->streams[i], b->d_gam + i, b->d_seed + i, gi == 1);
+        if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
+        if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
+    }
+    cudaGraph_t gr = nullptr;
+    e = cudaStreamEndCapture(cs, &gr);
+    if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
+    if (r == CTR_OK && (e = cudaGraphInstantiate(&b->exec[gi], gr, 0)) != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
+    b->graph[gi] = gr;
+    b->ws[gi] = batch_workspaces(b);
+    cudaStreamDestroy(cs);
+    if (r != CTR_OK) batch_drop_graph(b, gi);
+    return r;
 }
 
 extern "C" ctr_status ctr_batch_destroy(ctr_batch* b)
@@ -977,32 +1016,28 @@ extern "C" ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* obj_out, vo
     for (int i = 0; i < ns; ++i)
         if (!b->scans[i]->sino) return set_error(CTR_ERR_INVALID_ARGUMENT, "scan %d has no sinogram", i);
     cudaStream_t st = S(stream);
-    if (b->exec && b->ws != batch_workspaces(b)) batch_drop_graph(b);   // grown by another call
-    if (!b->exec) {
-        for (auto* s : b->scans) CTR_TRY(solver_reserve(s));
-        CTR_CUDA_TRY(cudaDeviceSynchronize());
-        cudaStream_t cs;
-        CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        ctr_status r = CTR_OK;
-        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
-        if (r == CTR_OK && (e = cudaEventRecord(b->fork, cs)) != cudaSuccess) r = cuda_error(e, "cudaEventRecord");
-        for (int i = 0; i < ns && r == CTR_OK; ++i) {
-            if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
-            r = solver_issue(b->scans[i], b->streams[i], b->d_gam + i, b->d_seed + i);
-            if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
-            if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
+    const bool objective = b->scans[0]->p.objective != 0;
+    // the objective of iteration it is projected in iteration it+1's SART
+    // traversal (graph 1); the last one of the call separately
+    auto obj_rows = [&](int it) -> ctr_status {
+        if (!obj_out) return CTR_OK;
+        std::vector<double> h(2 * (size_t)ns);
+        for (int i = 0; i < ns; ++i)
+            CTR_CUDA_TRY(cudaMemcpyAsync(&h[2 * i], b->scans[i]->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CTR_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int i = 0; i < ns; ++i) {
+            const ctr_solver* s = b->scans[i];
+            double* o = obj_out + ((size_t)i * n + it) * 3;
+            o[0] = h[2 * i + 1];
+            o[1] = h[2 * i];
+            o[2] = h[2 * i] + 2.0 * (double)s->p.lambda_tv * h[2 * i + 1];   // V63/main_recon.cu:423
         }
-        cudaGraph_t gr = nullptr;
-        e = cudaStreamEndCapture(cs, &gr);
-        if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
-        if (r == CTR_OK && (e = cudaGraphInstantiate(&b->exec, gr, 0)) != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
-        b->graph = gr;
-        b->ws = batch_workspaces(b);
-        cudaStreamDestroy(cs);
-        if (r != CTR_OK) { batch_drop_graph(b); return r; }
-    }
+        return CTR_OK;
+    };
     for (int it = 0; it < n; ++it) {
+        const int gi = (objective && it > 0) ? 1 : 0;
+        if (b->exec[gi] && b->ws[gi] != batch_workspaces(b)) batch_drop_graph(b, gi);   // grown by another call
+        if (!b->exec[gi]) CTR_TRY(batch_capture(b, gi));
         for (int i = 0; i < ns; ++i) {
             ctr_solver* s = b->scans[i];
             const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // V63/main_recon.cu:372
@@ -1011,27 +1046,22 @@ extern "C" ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* obj_out, vo
         }
         CTR_CUDA_TRY(cudaMemcpyAsync(b->d_gam, b->h_gam.data(), sizeof(float) * ns, cudaMemcpyHostToDevice, st));
         CTR_CUDA_TRY(cudaMemcpyAsync(b->d_seed, b->h_seed.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice, st));
-        CTR_CUDA_TRY(cudaGraphLaunch(b->exec, st));
+        CTR_CUDA_TRY(cudaGraphLaunch(b->exec[gi], st));
         for (auto* s : b->scans) {
             if (s->p.fista) s->t = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;
             s->k++;
         }
-        if (obj_out) {
-            std::vector<double> h(2 * (size_t)ns);
-            for (int i = 0; i < ns; ++i)
-                CTR_CUDA_TRY(cudaMemcpyAsync(&h[2 * i], b->scans[i]->d_obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-            CTR_CUDA_TRY(cudaStreamSynchronize(st));
-            for (int i = 0; i < ns; ++i) {
-                const ctr_solver* s = b->scans[i];
-                double* o = obj_out + ((size_t)i * n + it) * 3;
-                if (s->p.objective) {
-                    o[0] = h[2 * i + 1];
-                    o[1] = h[2 * i];
-                    o[2] = h[2 * i] + 2.0 * (double)s->p.lambda_tv * h[2 * i + 1];
-                } else {
-                    o[0] = o[1] = o[2] = NAN;
-                }
+        if (gi == 1) CTR_TRY(obj_rows(it - 1));
+    }
+    if (n > 0) {
+        if (objective) {
+            for (auto* s : b->scans) {
+                const void* xk = s->p.fista ? s->xprev : s->y;
+                CTR_TRY(objective_async(s->g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
             }
+            CTR_TRY(obj_rows(n - 1));
+        } else if (obj_out) {
+            for (size_t i = 0; i < (size_t)ns * n * 3; ++i) obj_out[i] = NAN;
         }
     }
     for (auto* s : b->scans) CTR_TRY(check_device_errors(s->g, st));
