@@ -364,6 +364,7 @@ extern "C" ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float
     CTR_TRY(need(geom, "geometry"));
     CTR_TRY(need(sino, "sino"));
     CTR_TRY(need(vol, "vol"));
+    if (GE(geom)->dg.ct_style != 0) return set_error(CTR_ERR_UNSUPPORTED, "FDK is for the cone-beam geometry");
     return launch_fdk(*GE(geom), sino, vol, S(stream));
 }
 

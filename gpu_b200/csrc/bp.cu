@@ -74,11 +74,13 @@ __device__ __forceinline__ bool candidate_rect(const DevGeom& g, const SharedTab
         const float pyc = fs(fa(cy, fm((float)(cc >> 1), g.vy)), fm(0.5f, g.vy));
         const float t = fa(fm(pxc, c), fm(pyc, s));
         const float ss = fa(fm(-pxc, s), fm(pyc, c));
-        const float mt = fdv(fs(t, g.dod), fs(g.dso, t));
+        // magnification of the corner (universal.cu:655-670); a parallel beam has none
+        const float mt = g.ct_style == 2 ? 0.0f : fdv(fs(t, g.dod), fs(g.dso, t));
         const float ou = fa(fm(mt, fs(ss, g.srcy)), ss);
         umin = fminf(umin, ou); umax = fmaxf(umax, ou);
         mlo = fminf(mlo, mt); mhi = fmaxf(mhi, mt);
     }
+    if (g.ct_style != 0) { mlo = 0.0f; mhi = 0.0f; }   // rays parallel to the xy plane: rows in the voxel's z span
     ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
     uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
     if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) return false;
@@ -279,11 +281,13 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         const float pyc = fs(fa(cy, fm((float)(cc >> 1), g.vy)), fm(0.5f, g.vy));
         const float t = fa(fm(pxc, c), fm(pyc, s));
         const float ss = fa(fm(-pxc, s), fm(pyc, c));
-        const float mt = fdv(fs(t, g.dod), fs(g.dso, t));
+        // magnification of the corner (universal.cu:655-670); a parallel beam has none
+        const float mt = g.ct_style == 2 ? 0.0f : fdv(fs(t, g.dod), fs(g.dso, t));
         const float ou = fa(fm(mt, fs(ss, g.srcy)), ss);
         umin = fminf(umin, ou); umax = fmaxf(umax, ou);
         mlo = fminf(mlo, mt); mhi = fmaxf(mhi, mt);
     }
+    if (g.ct_style != 0) { mlo = 0.0f; mhi = 0.0f; }   // rays parallel to the xy plane: rows in the voxel's z span
     int ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
     int uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
     if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) return;

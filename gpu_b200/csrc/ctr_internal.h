@@ -22,6 +22,7 @@ struct DevGeom {
     int Mt, Nt;             // 8x8 (x, y) tiles per row / column of the tiled layout
     int fast_exit;          // every alpha inside the volume >= 1e-6: the Siddon loop test is one comparison
     int entry64;            // FP64 ray-box entry/exit
+    int ct_style;           // 0 cone beam, 1 multi-slice fan beam, 2 parallel beam (the reference's CT_style)
     float vx, vy, vz, inv_vx, inv_vy, inv_vz;
     float bx, by, bz;       // boundary_voxel_*
     float ymin, zmin;       // Detector_Ymin/Zmin

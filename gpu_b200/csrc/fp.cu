@@ -97,14 +97,17 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     r.a_lo = 1.0f; r.a_hi = 0.0f;
     r.vi0 = r.vj0 = r.vk0 = -1; r.par = 0;
 
-    // source X2 and detector pixel centre X1 (universal.cu:24-45)
-    const float x2x = fs(fm(g.srcx, c), fm(g.srcy, s));
-    const float x2y = fa(fm(g.srcx, s), fm(g.srcy, c));
-    const float x2z = g.srcz;
+    // source X2 and detector pixel centre X1 (universal.cu:21-45): one
+    // source (cone beam), the source at the row's height (multi-slice fan
+    // beam), or a source opposite each pixel (parallel beam)
     const float pu = fa(g.ymin, fm((float)u, g.du));
+    const float sy_ = g.ct_style == 2 ? pu : g.srcy;
+    const float x2x = fs(fm(g.srcx, c), fm(sy_, s));
+    const float x2y = fa(fm(g.srcx, s), fm(sy_, c));
     const float x1x = fs(fm(g.dod, c), fm(pu, s));
     const float x1y = fa(fm(g.dod, s), fm(pu, c));
     const float x1z = fa(g.zmin, fm((float)v, g.dv));
+    const float x2z = g.ct_style == 0 ? g.srcz : x1z;
     const float dx = fs(x2x, x1x), dy = fs(x2y, x1y), dz = fs(x2z, x1z);
     const float ix = fdv(1.0f, dx), iy = fdv(1.0f, dy), iz = fdv(1.0f, dz);
     r.d12 = __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));   // :290

@@ -139,6 +139,8 @@ static ctr_status validate(const ctr_geometry_desc* d)
                              std::fabs((double)d->m_offset * d->vx);
     if (half_diag >= d->dso || half_diag >= -d->dod)
         return set_error(CTR_ERR_BAD_GEOMETRY, "volume (half-diagonal %.4g) reaches the source or detector", half_diag);
+    if ((d->flags & CTR_GEOM_FAN_SLICES) && (d->flags & CTR_GEOM_PARALLEL))
+        return set_error(CTR_ERR_BAD_GEOMETRY, "CTR_GEOM_FAN_SLICES and CTR_GEOM_PARALLEL exclude each other");
     if (d->nx > 65535 || d->ny > 65535 * 8 || d->nz > 65535 || d->nv > 65535 * 4)
         return set_error(CTR_ERR_BAD_GEOMETRY, "dimension exceeds the launch limits");
     return CTR_OK;
@@ -179,6 +181,7 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
         q.fast_exit = ((-(double)d.dod - half_diag) / ((double)d.dso - (double)d.dod) >= 1e-6) ? 1 : 0;
     }
     q.entry64 = (d.flags & CTR_GEOM_ENTRY_F64) ? 1 : 0;
+    q.ct_style = (d.flags & CTR_GEOM_FAN_SLICES) ? 1 : ((d.flags & CTR_GEOM_PARALLEL) ? 2 : 0);
     q.vx = d.vx; q.vy = d.vy; q.vz = d.vz;
     // inv_volumn_x = 1.0/volumn_x (double division stored as float), main_recon.cu:88
     q.inv_vx = (float)(1.0 / (double)d.vx);
@@ -229,10 +232,11 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     std::vector<float4> colt((size_t)d.n_views * d.nu);
     for (int j = 0; j < d.n_views; ++j) {
         const float s = g->h_trig[j].x, c = g->h_trig[j].y;
-        const float x2x = q.srcx * c - q.srcy * s;
-        const float x2y = q.srcx * s + q.srcy * c;
         for (int u = 0; u < d.nu; ++u) {
             const float pu = q.ymin + (float)u * q.du;
+            const float sy = q.ct_style == 2 ? pu : q.srcy;   // parallel beam: a source per column
+            const float x2x = q.srcx * c - sy * s;
+            const float x2y = q.srcx * s + sy * c;
             const float x1x = q.dod * c - pu * s;
             const float x1y = q.dod * s + pu * c;
             float4 e;
@@ -259,7 +263,7 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     std::vector<float2> rowt(d.nv);
     for (int v = 0; v < d.nv; ++v) {
         const float x1z = q.zmin + (float)v * q.dv;
-        const float x2z = q.srcz;
+        const float x2z = q.ct_style == 0 ? q.srcz : x1z;   // fan slices, parallel beam: rows parallel to xy
         if (std::fabs(x1z - x2z) < q.vz * 1e-6f) {
             const int kv = parallel_voxel(x1z, q.bz, q.inv_vz);
             rowt[v].x = plane(q.vz, kv, q.bz) + 0.5f * q.vz;

@@ -32,6 +32,8 @@ F32, BF16, F16 = 0, 1, 2
 GEOM_ENTRY_F64 = 0x1
 BP_ACCUMULATE = 0x1
 BP_FOV_MASK = 0x2
+GEOM_FAN_SLICES = 0x2
+GEOM_PARALLEL = 0x4
 SART_STOCHASTIC_ROUND = 0x1
 SART_TILED = 0x2
 
@@ -200,11 +202,17 @@ def dtype_code(t) -> int:
 
 
 def make_desc(nx, ny, nz, vx, nu, nv, du, dso, dod, n_views, us_rate=None, initial_angle=0.0,
-              shift_angle=0.0, offset=0.0, m_offset=0, entry64=False, vy=0.0, vz=0.0, dv=0.0):
+              shift_angle=0.0, offset=0.0, m_offset=0, entry64=False, vy=0.0, vz=0.0, dv=0.0, ct_style=0):
+    """ct_style: 0 cone beam, 1 multi-slice fan beam, 2 parallel beam (the
+    reference's CT_style); styles 1 and 2 default vz to the detector pitch, as
+    the reference does."""
     if us_rate is None:
         us_rate = 360.0 / n_views
+    if ct_style and not vz:
+        vz = du
+    flags = (GEOM_ENTRY_F64 if entry64 else 0) | {0: 0, 1: GEOM_FAN_SLICES, 2: GEOM_PARALLEL}[ct_style]
     return GeometryDesc(nx, ny, nz, vx, vy, vz, nu, nv, du, dv, dso, dod, offset, m_offset, n_views,
-                        us_rate, initial_angle, shift_angle, GEOM_ENTRY_F64 if entry64 else 0)
+                        us_rate, initial_angle, shift_angle, flags)
 
 
 class Geometry:

@@ -72,6 +72,14 @@ typedef struct ctr_geometry_desc {
 /* Compute the ray-box entry/exit parameters and the first plane indices in
  * FP64 (the traversal itself stays FP32). */
 #define CTR_GEOM_ENTRY_F64 0x1u
+/* Scanner geometry, the reference's CT_style (V63/main_recon.cu:29): cone
+ * beam by default; CTR_GEOM_FAN_SLICES (CT_style 1): a fan beam per detector
+ * row, the source at the row's height; CTR_GEOM_PARALLEL (CT_style 2): a
+ * parallel beam, every ray perpendicular to the detector.  In both the rays
+ * are parallel to the xy plane, and the reference sets vz to the detector
+ * pitch.  FDK supports the cone beam only. */
+#define CTR_GEOM_FAN_SLICES 0x2u
+#define CTR_GEOM_PARALLEL 0x4u
 
 typedef struct ctr_geometry ctr_geometry;
 

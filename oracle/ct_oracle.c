@@ -50,6 +50,18 @@ int og_init(og_geom* g, const og_desc* d)
     return 0;
 }
 
+void og_source(const og_geom* g, float s, float c, int u, int v, float* x2x, float* x2y, float* x2z)
+{
+    if (g->d.ct_style == 2) {                                    /* :34-37 */
+        *x2x = g->srcx * c - (g->ymin + (float)u * g->d.du) * s;
+        *x2y = g->srcx * s + (g->ymin + (float)u * g->d.du) * c;
+    } else {                                                     /* :23-24, :29-30 */
+        *x2x = g->srcx * c - g->srcy * s;
+        *x2y = g->srcx * s + g->srcy * c;
+    }
+    *x2z = g->d.ct_style == 0 ? g->srcz : g->zmin + (float)v * g->d.dv;   /* :25, :31, :38 */
+}
+
 /* V63/host_IterativeRecon_CBCT.c:34-41 (SART/FP) and V63/host_FDK.cpp:35-40 (FDK) */
 void og_view_trig(const og_geom* g, int view, int fdk, float* s, float* c)
 {
@@ -91,10 +103,9 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
     const float vx = g->d.vx, vy = g->d.vy, vz = g->d.vz;
     const float bx = g->bx, by = g->by, bz = g->bz;
 
-    /* source (X2) and detector pixel centre (X1), :24-45 (CT_style 0) */
-    const float x2x = g->srcx * c - g->srcy * s;
-    const float x2y = g->srcx * s + g->srcy * c;
-    const float x2z = g->srcz;
+    /* source (X2) and detector pixel centre (X1), :21-45 */
+    float x2x, x2y, x2z;
+    og_source(g, s, c, u, v, &x2x, &x2y, &x2z);
     const float x1x = g->d.dod * c - (g->ymin + (float)u * g->d.du) * s;
     const float x1y = g->d.dod * s + (g->ymin + (float)u * g->d.du) * c;
     const float x1z = g->zmin + (float)v * g->d.dv;
@@ -340,7 +351,7 @@ void og_forward_trace(const og_geom* g, const float* vol, float s, float c, int 
 /* FP64 oracle: the same Siddon traversal, every quantity in double.        */
 /* ------------------------------------------------------------------------ */
 typedef struct {
-    int M, N, Z;
+    int M, N, Z, ct_style;
     double vx, vy, vz, bx, by, bz, ymin, zmin, du, dv, dso, dod, srcx, srcy, srcz;
 } og_geom64;
 
@@ -357,6 +368,15 @@ static void og_geom_to64(const og_geom* g, og_geom64* h)
     h->zmin = -h->dv * ((double)e->nv / 2.0 - 0.5);
     h->dso = e->dso; h->dod = e->dod;
     h->srcx = e->dso; h->srcy = e->offset; h->srcz = 0.0;
+    h->ct_style = e->ct_style;
+}
+
+static void og_source64(const og_geom64* h, double s, double c, int u, int v, double x2[3])
+{
+    const double pu = h->ymin + u * h->du;
+    x2[0] = h->ct_style == 2 ? h->srcx * c - pu * s : h->srcx * c - h->srcy * s;
+    x2[1] = h->ct_style == 2 ? h->srcx * s + pu * c : h->srcx * s + h->srcy * c;
+    x2[2] = h->ct_style == 0 ? h->srcz : h->zmin + v * h->dv;
 }
 
 typedef void (*og_visit64_fn)(void* ctx, long long idx, double seg);
@@ -365,7 +385,9 @@ static double og_traverse64(const og_geom64* h, double s, double c, int u, int v
                             og_visit64_fn fn, void* ctx, const double* vol, double* len_out)
 {
     const int M = h->M, N = h->N, Z = h->Z;
-    const double x2x = h->srcx * c - h->srcy * s, x2y = h->srcx * s + h->srcy * c, x2z = h->srcz;
+    double X2[3];
+    og_source64(h, s, c, u, v, X2);
+    const double x2x = X2[0], x2y = X2[1], x2z = X2[2];
     const double pu = h->ymin + u * h->du;
     const double x1x = h->dod * c - pu * s, x1y = h->dod * s + pu * c, x1z = h->zmin + v * h->dv;
     const double dx = x2x - x1x, dy = x2y - x1y, dz = x2z - x1z;
@@ -507,8 +529,17 @@ void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float b
                                 const float pz = cz + (float)kk * vz - 0.5f * vz;
                                 const float t = px * c + py * s;
                                 const float ss = -px * s + py * c;
-                                const float ou = (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
-                                const float oz = (t - DOD) / (DSO - t) * (pz - g->srcz) + pz;
+                                float ou, oz;                                 /* :655-670 */
+                                if (g->d.ct_style == 0) {
+                                    ou = (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
+                                    oz = (t - DOD) / (DSO - t) * (pz - g->srcz) + pz;
+                                } else if (g->d.ct_style == 1) {
+                                    ou = (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
+                                    oz = cz;
+                                } else {
+                                    ou = ss;
+                                    oz = cz;
+                                }
                                 minY = fminf(minY, ou); maxY = fmaxf(maxY, ou);
                                 minZ = fminf(minZ, oz); maxZ = fmaxf(maxZ, oz);
                             }
@@ -522,14 +553,18 @@ void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float b
                         if (maxYi >= R - 1) maxYi = R - 1;
                         if (minZi <= 0) minZi = 0;
                         if (maxZi >= ZP - 1) maxZi = ZP - 1;
-                        const float sx = g->srcx * c - g->srcy * s;           /* :711-713 */
-                        const float sy = g->srcx * s + g->srcy * c;
-                        const float sz = g->srcz;
+                        float sx = g->srcx * c - g->srcy * s;                 /* :711-726 */
+                        float sy = g->srcx * s + g->srcy * c;
+                        const float sz = g->d.ct_style == 0 ? g->srcz : cz;
                         for (int jr = minZi; jr <= maxZi; ++jr)
                             for (int ir = minYi; ir <= maxYi; ++ir) {
                                 const float qx = DOD * c - (g->ymin + (float)ir * g->d.du) * s;   /* :733-735 */
                                 const float qy = DOD * s + (g->ymin + (float)ir * g->d.du) * c;
                                 const float qz = g->zmin + (float)jr * g->d.dv;
+                                if (g->d.ct_style == 2) {                                         /* :737-742 */
+                                    sx = g->srcx * c - (g->ymin + (float)ir * g->d.du) * s;
+                                    sy = g->srcx * s + (g->ymin + (float)ir * g->d.du) * c;
+                                }
                                 const float ax0 = ((cx - 0.5f * vx) - qx) / (sx - qx);   /* :760-765 */
                                 const float ax1 = ((cx + 0.5f * vx) - qx) / (sx - qx);
                                 const float ay0 = ((cy - 0.5f * vy) - qy) / (sy - qy);
@@ -1017,7 +1052,8 @@ void og_phantom_project(const og_geom* g, const double* par, int n, double s, do
 #pragma omp parallel for schedule(static)
     for (int v = 0; v < ZP; ++v)
         for (int u = 0; u < R; ++u) {
-            const double x2[3] = {h.srcx * c - h.srcy * s, h.srcx * s + h.srcy * c, h.srcz};
+            double x2[3];
+            og_source64(&h, s, c, u, v, x2);
             const double pu = h.ymin + u * h.du;
             const double x1[3] = {h.dod * c - pu * s, h.dod * s + pu * c, h.zmin + v * h.dv};
             const double D[3] = {x2[0] - x1[0], x2[1] - x1[1], x2[2] - x1[2]};
@@ -1058,7 +1094,8 @@ void og_phantom_project(const og_geom* g, const double* par, int n, double s, do
 static void og_column_eff(const og_geom* g, float s, float c, int u, float* x1x_e, float* ix_e, float* x1y_e,
                           float* iy_e)
 {
-    const float x2x = g->srcx * c - g->srcy * s, x2y = g->srcx * s + g->srcy * c;
+    float x2x, x2y, x2z;
+    og_source(g, s, c, u, 0, &x2x, &x2y, &x2z);
     const float pu = g->ymin + (float)u * g->d.du;
     const float x1x = g->d.dod * c - pu * s, x1y = g->d.dod * s + pu * c;
     if (fabsf(x1x - x2x) < g->d.vx * 1e-6f) {
@@ -1081,7 +1118,7 @@ static void og_column_eff(const og_geom* g, float s, float c, int u, float* x1x_
 
 static void og_row_eff(const og_geom* g, int v, float* x1z_e, float* iz_e)
 {
-    const float x1z = g->zmin + (float)v * g->d.dv, x2z = g->srcz;
+    const float x1z = g->zmin + (float)v * g->d.dv, x2z = g->d.ct_style == 0 ? g->srcz : x1z;
     if (fabsf(x1z - x2z) < g->d.vz * 1e-6f) {
         const int kv = (int)floorf((x1z - g->bz) * g->inv_vz);
         *x1z_e = og_plane(g->d.vz, kv, g->bz) + 0.5f * g->d.vz;
@@ -1094,7 +1131,8 @@ static void og_row_eff(const og_geom* g, int v, float* x1z_e, float* iz_e)
 
 static float og_ray_d12(const og_geom* g, float s, float c, int u, int v)
 {
-    const float x2x = g->srcx * c - g->srcy * s, x2y = g->srcx * s + g->srcy * c, x2z = g->srcz;
+    float x2x, x2y, x2z;
+    og_source(g, s, c, u, v, &x2x, &x2y, &x2z);
     const float pu = g->ymin + (float)u * g->d.du;
     const float x1x = g->d.dod * c - pu * s, x1y = g->d.dod * s + pu * c, x1z = g->zmin + (float)v * g->d.dv;
     return sqrtf((x2x - x1x) * (x2x - x1x) + (x2y - x1y) * (x2y - x1y) + (x2z - x1z) * (x2z - x1z));
@@ -1131,8 +1169,8 @@ void og_backproject_gather(const og_geom* g, float* vol, const float* corr, floa
                             const float py = cy + (float)jj * vy - 0.5f * vy;
                             const float pz = cz + (float)kk * vz - 0.5f * vz;
                             const float t = px * c + py * s, ss = -px * s + py * c;
-                            const float ou = (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
-                            const float oz = (t - DOD) / (DSO - t) * (pz - g->srcz) + pz;
+                            const float ou = g->d.ct_style == 2 ? ss : (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
+                            const float oz = g->d.ct_style == 0 ? (t - DOD) / (DSO - t) * (pz - g->srcz) + pz : cz;
                             minY = fminf(minY, ou); maxY = fmaxf(maxY, ou);
                             minZ = fminf(minZ, oz); maxZ = fmaxf(maxZ, oz);
                         }

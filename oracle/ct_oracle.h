@@ -39,6 +39,8 @@ typedef struct og_desc {
     float us_rate;           /* degrees per view                            */
     float initial_angle;     /* degrees                                     */
     float shift_angle;       /* degrees                                     */
+    int   ct_style;          /* CT_style: 0 cone beam, 1 multi-slice fan     */
+                             /* beam, 2 parallel beam (V63/main_recon.cu:29) */
 } og_desc;
 
 /* Derived constants, computed with the reference's float/double steps. */
@@ -51,6 +53,10 @@ typedef struct og_geom {
 } og_geom;
 
 int  og_init(og_geom* g, const og_desc* d);
+/* Source (X2) of the ray through detector pixel (u, v) at a view, per
+ * CT_style (V63/kernel_IterativeRecon_universal.cu:21-39): one source (0);
+ * the source at the row's height (1); a source per pixel, opposite it (2). */
+void og_source(const og_geom* g, float s, float c, int u, int v, float* x2x, float* x2y, float* x2z);
 /* Per-view angle.  fdk=0: SART/FP frame theta' = -(j*us+init+shift)*pi/180
  * (V63/host_IterativeRecon_CBCT.c:34-41); fdk=1: +theta (V63/host_FDK.cpp:35-40). */
 void og_view_trig(const og_geom* g, int view, int fdk, float* s, float* c);

@@ -16,6 +16,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libctoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libctref.so")
+# the reference fixes CT_style at compile time: one build per style
+REF_SO_STYLE = {0: REF_SO, 1: os.path.join(HERE, "_ref", "libctref_fbct.so"),
+                2: os.path.join(HERE, "_ref", "libctref_pbct.so")}
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -34,6 +37,7 @@ class OgDesc(C.Structure):
         ("dso", C.c_float), ("dod", C.c_float),
         ("offset", C.c_float), ("m_offset", C.c_int),
         ("us_rate", C.c_float), ("initial_angle", C.c_float), ("shift_angle", C.c_float),
+        ("ct_style", C.c_int),
     ]
 
 
@@ -48,11 +52,15 @@ class OgGeom(C.Structure):
 
 
 def make_desc(nx, ny, nz, nu, nv, nviews, vx, du, dso, dod, us_rate=None,
-              initial_angle=0.0, shift_angle=0.0, offset=0.0, m_offset=0):
+              initial_angle=0.0, shift_angle=0.0, offset=0.0, m_offset=0, ct_style=0, vz=None):
+    """ct_style 1 and 2 take the reference's z pitch, volumn_z = Detector_pixel_x
+    (V63/main_recon.cu:96), unless vz is given."""
     if us_rate is None:
         us_rate = 360.0 / nviews
-    return OgDesc(nx, ny, nz, nu, nv, nviews, vx, vx, vx, du, du, dso, dod,
-                  offset, m_offset, us_rate, initial_angle, shift_angle)
+    if vz is None:
+        vz = vx if ct_style == 0 else du
+    return OgDesc(nx, ny, nz, nu, nv, nviews, vx, vx, vz, du, du, dso, dod,
+                  offset, m_offset, us_rate, initial_angle, shift_angle, ct_style)
 
 
 def build():
@@ -296,9 +304,10 @@ class RefOracle:
     """The reference's own kernels compiled for the CPU (``_ref/libctref.so``)."""
 
     def __init__(self, desc: OgDesc):
-        if not os.path.exists(REF_SO):
-            raise FileNotFoundError(REF_SO)
-        self.lib = lib = C.CDLL(REF_SO)
+        so = REF_SO_STYLE[desc.ct_style]
+        if not os.path.exists(so):
+            raise FileNotFoundError(so)
+        self.lib = lib = C.CDLL(so)
         self.desc = desc
         f, i = C.c_float, C.c_int
         sig = {

@@ -32,7 +32,9 @@ static thread_local ref_dim3 tl_threadIdx, tl_blockIdx, tl_blockDim, tl_gridDim;
 static inline void __syncthreads() {}
 float sdata[1];   /* satisfies the never-called shared-memory reduction kernels */
 
-#define CT_style 0
+#ifndef CT_style
+#define CT_style 0   /* the Makefile builds one library per style */
+#endif
 #define MAX_infi (1.0 / 0.0)
 
 /* geometry globals with the reference's names */
@@ -61,7 +63,10 @@ extern "C" {
 int ref_set_geometry(const og_desc* d)
 {
     if (d->vy > 0.f && d->vy != d->vx) return -1;   /* the reference has one voxel pitch */
-    if (d->vz > 0.f && d->vz != d->vx) return -1;
+    /* volumn_z = (CT_style == 0) ? volumn_x : Detector_pixel_x (V63/main_recon.cu:96) */
+    const float vz_ref = CT_style == 0 ? d->vx : d->du;
+    if (d->ct_style != CT_style) return -1;
+    if (d->vz > 0.f && d->vz != vz_ref) return -1;
     if (d->dv > 0.f && d->dv != d->du) return -1;   /* and one detector pitch */
     M = d->nx; N = d->ny; ZETA = d->nz;
     NO_X = M; NO_Y = N; NO_Z = ZETA; NO_VOXEL = M * N * ZETA;
@@ -76,7 +81,7 @@ int ref_set_geometry(const og_desc* d)
     volumn_y = volumn_x;
     inv_volumn_y = 1.0 / volumn_y;
     boundary_voxel_y = -volumn_y * (float(N) / 2.0f);
-    volumn_z = volumn_x;
+    volumn_z = CT_style == 0 ? volumn_x : Detector_pixel_x;
     inv_volumn_z = 1.0 / volumn_z;
     boundary_voxel_z = -volumn_z * (float(ZETA) / 2.0f);
     Source_x = DSO; Source_y = Offset; Source_z = 0;

@@ -1,9 +1,10 @@
 """Generate tests/golden/*.npz from the reference's own kernels.
 
 Runs the reference's CUDA kernel sources compiled for the CPU
-(oracle/_ref/libctref.so, built by `make -C oracle` from the reference
-checkout) on seeded inputs for the small scans of tests/scan_configs.py and
-stores inputs and outputs.  The fixtures pin the C restatement in
+(oracle/_ref/libctref*.so, one per CT_style, built by `make -C oracle` from
+the reference checkout) on seeded inputs for the small scans of
+tests/scan_configs.py (cone beam, and the fan-slice and parallel geometries)
+and stores inputs and outputs.  The fixtures pin the C restatement in
 oracle/ct_oracle.c where the reference checkout is absent.
 
     python tests/golden/make_golden.py
@@ -19,12 +20,13 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 from oracle import ctoracle  # noqa: E402
-from scan_configs import SMALL, og_desc  # noqa: E402
+from scan_configs import SMALL, STYLES, og_desc  # noqa: E402
 
 
 def main():
     ctoracle.build()
-    for name, cfg in SMALL.items():
+    for name, cfg in list(SMALL.items()) + list(STYLES.items()):
+        cone = cfg.get("ct_style", 0) == 0
         if cfg["nx"] != cfg["ny"] or cfg["ny"] != cfg["nz"]:
             d = og_desc(cfg)
             d.nx, d.ny, d.nz = cfg["nx"], cfg["ny"], cfg["nz"]
@@ -45,11 +47,13 @@ def main():
         fgp = ref.fgp(vol, 0.01, 5)
         tv = ref.tv_norm(vol)
         l2 = ref.l2_norm(fp0, b)
-        fdkw = ref.fdk_weight(b)
-        ramp = ref.ramp_filter(fdkw[:2])
-        fdkbp = np.zeros_like(vol)
-        for j in range(min(nv, 4)):
-            fdkbp = ref.fdk_bp_view(fdkbp, ramp[0] if j % 2 == 0 else ramp[1], j)
+        fdkw = ramp = fdkbp = np.zeros(0, np.float32)   # FDK is the cone beam's only
+        if cone:
+            fdkw = ref.fdk_weight(b)
+            ramp = ref.ramp_filter(fdkw[:2])
+            fdkbp = np.zeros_like(vol)
+            for j in range(min(nv, 4)):
+                fdkbp = ref.fdk_bp_view(fdkbp, ramp[0] if j % 2 == 0 else ramp[1], j)
         np.savez_compressed(
             os.path.join(HERE, f"{name}.npz"),
             vol=vol, b=b, fp0=fp0, fp1=fp1, bp_views=np.array(bpv), corr=corr, bp1=bp1, bp0=bp0, sart=sart,

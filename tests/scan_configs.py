@@ -33,12 +33,26 @@ NO_ON_PLANE_RAYS = ["cube16", "fine_even"]
 CONFIG0 = dict(nx=128, ny=128, nz=128, nu=128, nv=128, nviews=180, vx=1.0, du=1.6, dso=1000.0, dod=-500.0)
 
 
+# The reference's other scanner geometries (CT_style 1 and 2), z pitch equal
+# to the detector pitch as the reference sets it; odd and even detectors.
+STYLES = {
+    "fan_slices": dict(nx=16, ny=16, nz=12, nu=24, nv=12, nviews=12, vx=1.0, du=1.2, dso=1000.0, dod=-500.0,
+                       ct_style=1),
+    "fan_slices_odd": dict(nx=12, ny=12, nz=9, nu=17, nv=9, nviews=8, vx=1.0, du=1.6, dso=1000.0, dod=-500.0,
+                           initial_angle=3.5, ct_style=1),
+    "parallel": dict(nx=16, ny=16, nz=12, nu=24, nv=12, nviews=12, vx=1.0, du=1.2, dso=1000.0, dod=-500.0,
+                     ct_style=2),
+    "parallel_odd": dict(nx=12, ny=12, nz=9, nu=17, nv=9, nviews=8, vx=1.0, du=1.6, dso=1000.0, dod=-500.0,
+                         initial_angle=3.5, ct_style=2),
+}
+
+
 def og_desc(cfg):
     from oracle.ctoracle import make_desc
     return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["nu"], cfg["nv"], cfg["nviews"], cfg["vx"], cfg["du"],
                      cfg["dso"], cfg["dod"], initial_angle=cfg.get("initial_angle", 0.0),
                      shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
-                     m_offset=cfg.get("m_offset", 0))
+                     m_offset=cfg.get("m_offset", 0), ct_style=cfg.get("ct_style", 0))
 
 
 def og_desc_xyz(cfg):
@@ -53,7 +67,7 @@ def ctr_desc(cfg, entry64=False):
     return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["vx"], cfg["nu"], cfg["nv"], cfg["du"], cfg["dso"],
                      cfg["dod"], cfg["nviews"], initial_angle=cfg.get("initial_angle", 0.0),
                      shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
-                     m_offset=cfg.get("m_offset", 0), entry64=entry64)
+                     m_offset=cfg.get("m_offset", 0), entry64=entry64, ct_style=cfg.get("ct_style", 0))
 
 # Differentiation scan: 256^3, 360 views, 384^2 detector.  "Config-0 geometry
 # scaled by 2" is read as the same physical extents at twice the sampling:

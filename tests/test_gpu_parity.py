@@ -10,9 +10,12 @@ filter (FP32 convolution against the FP64 kernel), FP64 reductions.
 import numpy as np
 import pytest
 
-from scan_configs import CONFIG0, NEAR_DETECTOR, NO_ON_PLANE_RAYS, SMALL, ctr_desc, og_desc_xyz
+from scan_configs import CONFIG0, NEAR_DETECTOR, NO_ON_PLANE_RAYS, SMALL, STYLES, ctr_desc, og_desc_xyz
 
-FP_CASES = dict(SMALL, near_detector=NEAR_DETECTOR)
+FP_CASES = dict(SMALL, near_detector=NEAR_DETECTOR, **STYLES)
+BP_CASES = dict(SMALL, **STYLES)
+# the fan-slice scan has no ray on a voxel plane either (its rows sit at voxel centres)
+NO_ON_PLANE = NO_ON_PLANE_RAYS + ["fan_slices"]
 
 pytestmark = pytest.mark.gpu
 
@@ -93,11 +96,11 @@ def test_forward_config0_bit_exact(oracle_built):
         np.testing.assert_array_equal(bits(out[j]), bits(o.forward_view(vol, j, 0)), err_msg=f"view {j}")
 
 
-@pytest.mark.parametrize("name", sorted(SMALL))
+@pytest.mark.parametrize("name", sorted(BP_CASES))
 def test_adjoint_matches_scatter_of_projector(name, oracle_built):
     """Gather adjoint == scatter of the projector's own segments: the same
     chords, FP64 sums in another order, rounded once to float."""
-    cfg = SMALL[name]
+    cfg = BP_CASES[name]
     g, o = pair(cfg, oracle_built)
     rng = np.random.default_rng(11)
     y = rng.standard_normal((cfg["nviews"],) + o.view_shape).astype(np.float32)
@@ -110,11 +113,11 @@ def test_adjoint_matches_scatter_of_projector(name, oracle_built):
     assert np.all(np.abs(got - ref) <= 1.2e-7 * np.abs(ref) + 1e-12 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("name", sorted(SMALL))
+@pytest.mark.parametrize("name", sorted(BP_CASES))
 def test_dot_product(name, oracle_built):
     """<Ax, y> = <x, A^T y> to 1e-6 relative on 16 seeded pairs (x uniform over
     all voxels, y normal over all detector bins)."""
-    cfg = SMALL[name]
+    cfg = BP_CASES[name]
     g, o = pair(cfg, oracle_built)
     rng = np.random.default_rng(5)
     for _ in range(16):
@@ -145,11 +148,11 @@ def test_masked_adjoint_vs_reference_bp(name, oracle_built):
         assert np.abs(got - ref).max() <= 2e-3 * scale
 
 
-@pytest.mark.parametrize("name", sorted(SMALL))
+@pytest.mark.parametrize("name", sorted(BP_CASES))
 def test_sart_pass(name, oracle_built):
     """The SART pass equals the restated engine algorithm bit for bit, and the
     reference's own BP (its alpha formula) to alpha rounding."""
-    cfg = SMALL[name]
+    cfg = BP_CASES[name]
     g, o = pair(cfg, oracle_built)
     rng = np.random.default_rng(17)
     truth = rng.uniform(0, 0.05, o.vol_shape).astype(np.float32)
@@ -159,7 +162,7 @@ def test_sart_pass(name, oracle_built):
     got = host(vol)
     exact = o.sart_pass_gather(np.zeros_like(truth), b, 0.8)
     np.testing.assert_array_equal(bits(got), bits(exact))
-    if name in NO_ON_PLANE_RAYS:
+    if name in NO_ON_PLANE:
         ref = o.sart_pass_ref(np.zeros_like(truth), b, 0.8)
         scale = np.abs(ref).max()
         assert np.sqrt(np.mean((got - ref) ** 2)) <= 2e-3 * scale

@@ -5,7 +5,9 @@ bit-identical projections and SART passes."""
 import numpy as np
 import pytest
 
-from scan_configs import SMALL, ctr_desc, og_desc_xyz
+from scan_configs import SMALL, STYLES, ctr_desc, og_desc_xyz
+
+CASES = dict(SMALL, **STYLES)
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -21,11 +23,11 @@ def bits(t):
     return t.float().cpu().numpy().view(np.uint32)
 
 
-@pytest.mark.parametrize("name", ["cube16", "odd", "aniso", "fine_even"])
+@pytest.mark.parametrize("name", ["cube16", "odd", "aniso", "fine_even", "fan_slices_odd", "parallel"])
 @pytest.mark.parametrize("dtype", ["f32", "bf16_sr"])
 def test_every_shape_gives_the_same_result(name, dtype, oracle_built):
     import gpu_b200
-    cfg = SMALL[name]
+    cfg = CASES[name]
     o = oracle_built.Oracle(og_desc_xyz(cfg))
     truth = o.phantom(np.array([[0, 0, 0, 5, 4, 3, 0.3, 0.2, 0.1, 0.02], [1.5, -1, 0.5, 2, 2, 2, 0, 0, 0, 0.03]]))
     b = torch.from_numpy(np.stack([o.forward_view(truth, j, 0) for j in range(cfg["nviews"])])).cuda()

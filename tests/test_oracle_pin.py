@@ -1,7 +1,8 @@
 """Pin the C restatement (oracle/ct_oracle.c) to the reference.
 
 The golden fixtures were produced by the reference's own kernel sources
-compiled for the CPU (tests/golden/make_golden.py).  The restatement must
+compiled for the CPU (tests/golden/make_golden.py), for the cone beam and
+the reference's fan-slice and parallel-beam geometries (CT_style 1, 2).  The restatement must
 reproduce them bit for bit: Siddon FP (command 0 and the SART correction),
 the voxel-driven BP (command 0 and the SART update), a whole SART pass, FGP,
 the TV and L2 norms, and the FDK weight / ramp / backprojection.
@@ -11,7 +12,9 @@ import os
 import numpy as np
 import pytest
 
-from scan_configs import SMALL, og_desc_xyz
+from scan_configs import SMALL, STYLES, og_desc_xyz
+
+CASES = dict(SMALL, **STYLES)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -24,10 +27,10 @@ def load(name):
     return dict(np.load(os.path.join(HERE, "golden", f"{name}.npz")))
 
 
-@pytest.fixture(params=sorted(SMALL))
+@pytest.fixture(params=sorted(CASES))
 def case(request, oracle_built):
     name = request.param
-    cfg = SMALL[name]
+    cfg = CASES[name]
     o = oracle_built.Oracle(og_desc_xyz(cfg))
     return name, cfg, o, load(name)
 
@@ -62,6 +65,8 @@ def test_fgp_and_norms_bit_exact(case):
 
 def test_fdk_stages(case):
     _, cfg, o, g = case
+    if cfg.get("ct_style", 0):
+        pytest.skip("FDK is the cone beam's only")
     np.testing.assert_array_equal(bits(o.fdk_weight(g["b"])), bits(g["fdkw"]))
     ramp = o.ramp_filter(g["fdkw"][:2])
     # the reference filters with a double-precision FFT; the restatement convolves
@@ -75,11 +80,12 @@ def test_fdk_stages(case):
     np.testing.assert_array_equal(bits(fdkbp), bits(g["fdkbp"]))
 
 
-def test_against_reference_build_directly(oracle_built):
+@pytest.mark.parametrize("name", ["odd", "fan_slices_odd", "parallel_odd"])
+def test_against_reference_build_directly(name, oracle_built):
     """When the reference checkout was compiled here, compare on fresh seeds too."""
-    if not os.path.exists(oracle_built.REF_SO):
+    cfg = CASES[name]
+    if not os.path.exists(oracle_built.REF_SO_STYLE[cfg.get("ct_style", 0)]):
         pytest.skip("oracle/_ref not built (no reference checkout)")
-    cfg = SMALL["odd"]
     d = og_desc_xyz(cfg)
     o, r = oracle_built.Oracle(d), oracle_built.RefOracle(d)
     rng = np.random.default_rng(99)
