@@ -47,7 +47,34 @@ int og_init(og_geom* g, const og_desc* d)
     g->srcx = e->dso;
     g->srcy = e->offset;
     g->srcz = 0.0f;
+    g->rows = e->nv;
+    if (e->ct_style == 3) {
+        /* the automatic source distribution of T42/main_recon.cu:76-108: the
+         * first source sees the volume's bottom face from the detector's
+         * bottom row, the last its top face from the top row */
+        const int K = e->n_sources;
+        if (K < 1 || e->dv != e->du || e->vz != e->vx) return -1;
+        g->rows = e->nv * K;
+        g->zmax = +e->du * ((float)e->nv / 2.0f - 0.5f);                  /* :93 */
+        if (K == 1) {                                                     /* :97-100 */
+            g->zsrc0 = 0.0f;
+            g->zsrc_dz = 0.0f;
+        } else {
+            const float bzu = -e->vz * ((float)e->nz / 2.0f) + (float)e->nz * e->vz;   /* :76 */
+            const float zsmax = (bzu - g->zmax) * (e->dso - e->dod) / e->dso + g->zmax; /* :105 */
+            g->zsrc0 = (g->bz - g->zmin) * (e->dso - e->dod) / e->dso + g->zmin;       /* :106 */
+            g->zsrc_dz = (zsmax - g->zsrc0) / (float)(K - 1);                          /* :107 */
+        }
+    } else if (e->ct_style < 0 || e->ct_style > 3) {
+        return -1;
+    }
     return 0;
+}
+
+float og_row_z(const og_geom* g, int v)
+{
+    const int vr = g->d.ct_style == 3 ? v % g->d.nv : v;
+    return g->zmin + (float)vr * g->d.dv;
 }
 
 void og_source(const og_geom* g, float s, float c, int u, int v, float* x2x, float* x2y, float* x2z)
@@ -59,7 +86,10 @@ void og_source(const og_geom* g, float s, float c, int u, int v, float* x2x, flo
         *x2x = g->srcx * c - g->srcy * s;
         *x2y = g->srcx * s + g->srcy * c;
     }
-    *x2z = g->d.ct_style == 0 ? g->srcz : g->zmin + (float)v * g->d.dv;   /* :25, :31, :38 */
+    if (g->d.ct_style == 3)
+        *x2z = g->zsrc0 + (float)(v / g->d.nv) * g->zsrc_dz;      /* T42/...TBCT_voxel.cu:33 */
+    else
+        *x2z = g->d.ct_style == 0 ? g->srcz : g->zmin + (float)v * g->d.dv;   /* :25, :31, :38 */
 }
 
 /* V63/host_IterativeRecon_CBCT.c:34-41 (SART/FP) and V63/host_FDK.cpp:35-40 (FDK) */
@@ -108,7 +138,12 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
     og_source(g, s, c, u, v, &x2x, &x2y, &x2z);
     const float x1x = g->d.dod * c - (g->ymin + (float)u * g->d.du) * s;
     const float x1y = g->d.dod * s + (g->ymin + (float)u * g->d.du) * c;
-    const float x1z = g->zmin + (float)v * g->d.dv;
+    const float x1z = og_row_z(g, v);
+    /* T42's traversal (T42/...TBCT_voxel.cu:1-544) differs in two places:
+     * no special k range for rays parallel to the z planes (:171) and the
+     * loop test alpha_max - alpha_c > 1e-6f (:282) */
+    const int tb = g->d.ct_style == 3;
+    const int zpar_k = !tb && fabsf(x1z - x2z) < g->d.vz * 1e-6f;
 
     const float ix = 1.0f / (x2x - x1x);   /* :48-50 */
     const float iy = 1.0f / (x2y - x1y);
@@ -151,7 +186,7 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
                 j_max = (amin == aymin) ? N - 1 : (int)floorf((amin * (x2y - x1y) + x1y - by) * g->inv_vy);
                 j_min = (amax == aymax) ? 0 : (int)(floorf((amax * (x2y - x1y) + x1y - by) * g->inv_vy) + 1.0f);
             }
-            if (fabsf(x1z - x2z) < vz * 1e-6f) {
+            if (zpar_k) {
                 k_min = (int)(floorf((x1z - bz) * g->inv_vz) + 1.0f);
                 k_max = (int)floorf((x1z - bz) * g->inv_vz);
             } else if (x1z < x2z) {
@@ -195,7 +230,7 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
                 j_max = (Amin == Aymin) ? N - 1 : (int)floor((Amin * Dy + X1y - By) * IVy);
                 j_min = (Amax == Aymax) ? 0 : (int)floor((Amax * Dy + X1y - By) * IVy) + 1;
             }
-            if (fabsf(x1z - x2z) < vz * 1e-6f) {
+            if (zpar_k) {
                 k_min = (int)floor((X1z - Bz) * IVz) + 1;
                 k_max = (int)floor((X1z - Bz) * IVz);
             } else if (x1z < x2z) {
@@ -249,7 +284,8 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
          * is the same rule for all non-NaN alphas. */
         const int maxsteps = M + N + Z + 3;
         int steps = 0;
-        while (amax - ac > 1e-16f) {
+        const float eps = tb ? 1e-6f : 1e-16f;
+        while (amax - ac > eps) {
             if (vi > M - 1 || vi < 0 || vj > N - 1 || vj < 0 || vk > Z - 1 || vk < 0) break;
             if (++steps > maxsteps) break;   /* unreachable for finite alphas */
             const float m = fminf(fminf(ax, ay), az);
@@ -320,7 +356,7 @@ float og_fp_ray(const og_geom* g, const float* vol, float s, float c, int u, int
 void og_forward_view(const og_geom* g, const float* vol, float s, float c, int command,
                      const float* b, float* out, int entry64)
 {
-    const int R = g->d.nu, ZP = g->d.nv;
+    const int R = g->d.nu, ZP = g->rows;
     const float thr = g->d.vz * 1e-6f;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int v = 0; v < ZP; ++v) {
@@ -338,7 +374,7 @@ void og_forward_view(const og_geom* g, const float* vol, float s, float c, int c
 void og_forward_trace(const og_geom* g, const float* vol, float s, float c, int entry64,
                       int* nseg, uint64_t* hash, float* len)
 {
-    const int R = g->d.nu, ZP = g->d.nv;
+    const int R = g->d.nu, ZP = g->rows;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int v = 0; v < ZP; ++v)
         for (int u = 0; u < R; ++u) {
@@ -351,8 +387,8 @@ void og_forward_trace(const og_geom* g, const float* vol, float s, float c, int 
 /* FP64 oracle: the same Siddon traversal, every quantity in double.        */
 /* ------------------------------------------------------------------------ */
 typedef struct {
-    int M, N, Z, ct_style;
-    double vx, vy, vz, bx, by, bz, ymin, zmin, du, dv, dso, dod, srcx, srcy, srcz;
+    int M, N, Z, ct_style, nv;
+    double vx, vy, vz, bx, by, bz, ymin, zmin, du, dv, dso, dod, srcx, srcy, srcz, zsrc0, zsrc_dz;
 } og_geom64;
 
 static void og_geom_to64(const og_geom* g, og_geom64* h)
@@ -369,6 +405,15 @@ static void og_geom_to64(const og_geom* g, og_geom64* h)
     h->dso = e->dso; h->dod = e->dod;
     h->srcx = e->dso; h->srcy = e->offset; h->srcz = 0.0;
     h->ct_style = e->ct_style;
+    h->nv = e->nv;
+    h->zsrc0 = h->zsrc_dz = 0.0;
+    if (e->ct_style == 3 && e->n_sources > 1) {   /* T42/main_recon.cu:104-107 in double */
+        const double zmax = h->dv * ((double)e->nv / 2.0 - 0.5), zmin = -zmax;
+        const double bzu = h->bz + (double)e->nz * h->vz;
+        const double zsmax = (bzu - zmax) * (h->dso - h->dod) / h->dso + zmax;
+        h->zsrc0 = (h->bz - zmin) * (h->dso - h->dod) / h->dso + zmin;
+        h->zsrc_dz = (zsmax - h->zsrc0) / (double)(e->n_sources - 1);
+    }
 }
 
 static void og_source64(const og_geom64* h, double s, double c, int u, int v, double x2[3])
@@ -376,7 +421,8 @@ static void og_source64(const og_geom64* h, double s, double c, int u, int v, do
     const double pu = h->ymin + u * h->du;
     x2[0] = h->ct_style == 2 ? h->srcx * c - pu * s : h->srcx * c - h->srcy * s;
     x2[1] = h->ct_style == 2 ? h->srcx * s + pu * c : h->srcx * s + h->srcy * c;
-    x2[2] = h->ct_style == 0 ? h->srcz : h->zmin + v * h->dv;
+    x2[2] = h->ct_style == 3 ? h->zsrc0 + (double)(v / h->nv) * h->zsrc_dz
+                             : (h->ct_style == 0 ? h->srcz : h->zmin + v * h->dv);
 }
 
 typedef void (*og_visit64_fn)(void* ctx, long long idx, double seg);
@@ -389,7 +435,8 @@ static double og_traverse64(const og_geom64* h, double s, double c, int u, int v
     og_source64(h, s, c, u, v, X2);
     const double x2x = X2[0], x2y = X2[1], x2z = X2[2];
     const double pu = h->ymin + u * h->du;
-    const double x1x = h->dod * c - pu * s, x1y = h->dod * s + pu * c, x1z = h->zmin + v * h->dv;
+    const int vr = h->ct_style == 3 ? v % h->nv : v;
+    const double x1x = h->dod * c - pu * s, x1y = h->dod * s + pu * c, x1z = h->zmin + vr * h->dv;
     const double dx = x2x - x1x, dy = x2y - x1y, dz = x2z - x1z;
     const double P0[3] = {h->bx, h->by, h->bz};
     const double Vv[3] = {h->vx, h->vy, h->vz};
@@ -462,7 +509,7 @@ void og_forward_view_f64(const og_geom* g, const double* vol, double s, double c
 {
     og_geom64 h;
     og_geom_to64(g, &h);
-    const int R = g->d.nu, ZP = g->d.nv;
+    const int R = g->d.nu, ZP = g->rows;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int v = 0; v < ZP; ++v)
         for (int u = 0; u < R; ++u) {
@@ -482,7 +529,7 @@ void og_adjoint_view_f64(const og_geom* g, const double* y, double s, double c, 
 {
     og_geom64 h;
     og_geom_to64(g, &h);
-    const int R = g->d.nu, ZP = g->d.nv;
+    const int R = g->d.nu, ZP = g->rows;
     for (int v = 0; v < ZP; ++v)
         for (int u = 0; u < R; ++u) {
             og_sc64 q = {acc, y[v * R + u]};
@@ -503,9 +550,104 @@ int og_fov_masked(const og_geom* g, int i, int j)
     return ex * vx * ex * vx + ey * vy * ey * vy >= hx * vx * hy * vy;   /* :626-628 */
 }
 
+/* TBCT backprojection and update, T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:
+ * backprj_ray_driven_3d_kernel (:546-763) accumulates, per voxel and source,
+ * the chord-weighted corrections and chord lengths of the source's rays into
+ * two zeroed volumes by atomicAdd; update (:765-775) then adds
+ * beta*sum/length where the summed length exceeds volumn_x*1e-3 (a double
+ * comparison).  Sources are added in ascending order here. */
+static void og_backproject_ref_tbct(const og_geom* g, float* vol, const float* corr, float beta, float s, float c)
+{
+    const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->d.nv, K = g->d.n_sources;
+    const float vx = g->d.vx, vy = g->d.vy, vz = g->d.vz;
+    const float DSO = g->d.dso, DOD = g->d.dod, du = g->d.du;
+    const float inv_dp = 1.0f / du;                                      /* :592 */
+    const double thr_upd = (double)vx * 1e-3;                            /* :772 */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Z; ++k)
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < M; ++i) {
+                const long long idx = (long long)M * N * k + (long long)M * j + i;
+                float WS = 0.0f, L = 0.0f;                               /* the zeroed sums */
+                if (!og_fov_masked(g, i, j)) {                           /* :600-608 */
+                    const float cx = g->bx + vx * (0.5f + (float)i);    /* :568-570 */
+                    const float cy = g->by + vy * (0.5f + (float)j);
+                    const float cz = g->bz + vz * (0.5f + (float)k);
+                    const float sx = g->srcx * c - g->srcy * s;          /* :613-614 */
+                    const float sy = g->srcx * s + g->srcy * c;
+                    const float tc = cx * c + cy * s;                    /* :620 */
+                    const float upper = (cz + vz - g->zmin) * (DSO - DOD) / (tc - DOD) + g->zmin;   /* :623 */
+                    const float lower = (cz - vz - g->zmax) * (DSO - DOD) / (tc - DOD) + g->zmax;   /* :624 */
+                    for (int src = 0; src < K; ++src) {
+                        const float sz = g->zsrc0 + (float)src * g->zsrc_dz;                      /* :615 */
+                        if (sz < lower || sz > upper) continue;                                    /* :626-627 */
+                        float minY = INFINITY, minZ = INFINITY, maxY = -INFINITY, maxZ = -INFINITY;
+                        for (int kk = 0; kk < 2; ++kk)                                             /* :631-655 */
+                            for (int jj = 0; jj < 2; ++jj)
+                                for (int ii = 0; ii < 2; ++ii) {
+                                    const float px = cx + (float)ii * vx - 0.5f * vx;
+                                    const float py = cy + (float)jj * vy - 0.5f * vy;
+                                    const float pz = cz + (float)kk * vz - 0.5f * vz;
+                                    const float t = px * c + py * s;
+                                    const float ss = -px * s + py * c;
+                                    const float ou = (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
+                                    const float oz = (t - DOD) / (DSO - t) * (pz - sz) + pz;
+                                    minY = fminf(minY, ou); maxY = fmaxf(maxY, ou);
+                                    minZ = fminf(minZ, oz); maxZ = fmaxf(maxZ, oz);
+                                }
+                        int minYi = (int)floorf((minY - g->ymin) * inv_dp + 0.5f);               /* :659-662 */
+                        int maxYi = (int)floorf((maxY - g->ymin) * inv_dp + 0.5f);
+                        int minZi = (int)floorf((minZ - g->zmin) * inv_dp + 0.5f);
+                        int maxZi = (int)floorf((maxZ - g->zmin) * inv_dp + 0.5f);
+                        float sw = 0.0f, sl = 0.0f;
+                        if (!(((minYi < 0) && (maxYi < 0)) || (minYi > R - 1 && maxYi > R - 1) ||  /* :668 */
+                              ((minZi < 0) && (maxZi < 0)) || ((minZi > ZP - 1) && (maxZi > ZP - 1)))) {
+                            if (minYi <= 0) minYi = 0;                                              /* :678-685 */
+                            if (maxYi >= R - 1) maxYi = R - 1;
+                            if (minZi <= 0) minZi = 0;
+                            if (maxZi >= ZP - 1) maxZi = ZP - 1;
+                            for (int jr = minZi; jr <= maxZi; ++jr)                                 /* :689-750 */
+                                for (int ir = minYi; ir <= maxYi; ++ir) {
+                                    const float qx = DOD * c - (g->ymin + (float)ir * du) * s;
+                                    const float qy = DOD * s + (g->ymin + (float)ir * du) * c;
+                                    const float qz = g->zmin + (float)jr * du;
+                                    const float ax0 = ((cx - 0.5f * vx) - qx) / (sx - qx);
+                                    const float ax1 = ((cx + 0.5f * vx) - qx) / (sx - qx);
+                                    const float ay0 = ((cy - 0.5f * vy) - qy) / (sy - qy);
+                                    const float ay1 = ((cy + 0.5f * vy) - qy) / (sy - qy);
+                                    const float az0 = ((cz - 0.5f * vz) - qz) / (sz - qz);
+                                    const float az1 = ((cz + 0.5f * vz) - qz) / (sz - qz);
+                                    float tx = fminf(ax0, ax1), ty = fminf(ay0, ay1), tz = fminf(az0, az1);
+                                    const float amin = fmaxf(fmaxf(tx, ty), fmaxf(ty, tz));
+                                    tx = fmaxf(ax0, ax1); ty = fmaxf(ay0, ay1); tz = fmaxf(az0, az1);
+                                    const float amax = fminf(fminf(tx, ty), fminf(ty, tz));
+                                    if (amax - amin > 0) {
+                                        const float d12 = sqrtf((sx - qx) * (sx - qx) + (sy - qy) * (sy - qy) +
+                                                                (sz - qz) * (sz - qz));
+                                        const float temp = d12 * (amax - amin);
+                                        if (temp > vx * 1e-6f) {
+                                            sw = sw + temp * corr[(long long)R * ZP * src + (long long)R * jr + ir];
+                                            sl = sl + temp;
+                                        }
+                                    }
+                                }
+                        }
+                        WS = WS + sw;                                                               /* :754-755 */
+                        L = L + sl;
+                    }
+                }
+                if ((double)L > thr_upd) vol[idx] += beta * WS / L;                                 /* :772-773 */
+            }
+}
+
 void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float beta,
                         float s, float c, int command)
 {
+    if (g->d.ct_style == 3) {
+        (void)command;
+        og_backproject_ref_tbct(g, vol, corr, beta, s, c);
+        return;
+    }
     const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->d.nv;
     const float vx = g->d.vx, vy = g->d.vy, vz = g->d.vz;
     const float DSO = g->d.dso, DOD = g->d.dod;
@@ -599,7 +741,7 @@ void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float b
 void og_adjoint_view(const og_geom* g, const float* y, float s, float c, int thresh,
                      double* acc, double* lacc)
 {
-    const int R = g->d.nu, ZP = g->d.nv;
+    const int R = g->d.nu, ZP = g->rows;
     for (int v = 0; v < ZP; ++v)
         for (int u = 0; u < R; ++u) {
             og_visit vis;
@@ -620,7 +762,7 @@ void og_adjoint_view(const og_geom* g, const float* y, float s, float c, int thr
 /* ------------------------------------------------------------------------ */
 void og_sart_pass_ref(const og_geom* g, float* vol, const float* sino, float beta)
 {
-    const long long P = (long long)g->d.nu * g->d.nv;
+    const long long P = (long long)g->d.nu * g->rows;
     float* corr = (float*)malloc(sizeof(float) * P);
     for (int j = 0; j < g->d.nviews; ++j) {
         float s, c;
@@ -633,7 +775,7 @@ void og_sart_pass_ref(const og_geom* g, float* vol, const float* sino, float bet
 
 void og_sart_pass_matched(const og_geom* g, float* vol, const float* sino, float beta)
 {
-    const long long P = (long long)g->d.nu * g->d.nv;
+    const long long P = (long long)g->d.nu * g->rows;
     const long long V = (long long)g->d.nx * g->d.ny * g->d.nz;
     const int M = g->d.nx, N = g->d.ny;
     const float thr = g->d.vx * 1e-6f;
@@ -670,7 +812,7 @@ void og_sart_pass_f64(const og_geom* g, double* vol, const double* sino, double 
 {
     og_geom64 h;
     og_geom_to64(g, &h);
-    const int R = g->d.nu, ZP = g->d.nv, M = g->d.nx, N = g->d.ny;
+    const int R = g->d.nu, ZP = g->rows, M = g->d.nx, N = g->d.ny;
     const long long P = (long long)R * ZP;
     const long long V = (long long)g->d.nx * g->d.ny * g->d.nz;
     const double thr = (double)g->d.vx * 1e-6;
@@ -1048,14 +1190,15 @@ void og_phantom_project(const og_geom* g, const double* par, int n, double s, do
 {
     og_geom64 h;
     og_geom_to64(g, &h);
-    const int R = g->d.nu, ZP = g->d.nv;
+    const int R = g->d.nu, ZP = g->rows;
 #pragma omp parallel for schedule(static)
     for (int v = 0; v < ZP; ++v)
         for (int u = 0; u < R; ++u) {
             double x2[3];
             og_source64(&h, s, c, u, v, x2);
             const double pu = h.ymin + u * h.du;
-            const double x1[3] = {h.dod * c - pu * s, h.dod * s + pu * c, h.zmin + v * h.dv};
+            const int vr = h.ct_style == 3 ? v % h.nv : v;
+            const double x1[3] = {h.dod * c - pu * s, h.dod * s + pu * c, h.zmin + vr * h.dv};
             const double D[3] = {x2[0] - x1[0], x2[1] - x1[1], x2[2] - x1[2]};
             const double dl = sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]);
             double acc = 0.0;
@@ -1118,7 +1261,9 @@ static void og_column_eff(const og_geom* g, float s, float c, int u, float* x1x_
 
 static void og_row_eff(const og_geom* g, int v, float* x1z_e, float* iz_e)
 {
-    const float x1z = g->zmin + (float)v * g->d.dv, x2z = g->d.ct_style == 0 ? g->srcz : x1z;
+    float x2x, x2y, x2z;
+    og_source(g, 0.0f, 1.0f, 0, v, &x2x, &x2y, &x2z);
+    const float x1z = og_row_z(g, v);
     if (fabsf(x1z - x2z) < g->d.vz * 1e-6f) {
         const int kv = (int)floorf((x1z - g->bz) * g->inv_vz);
         *x1z_e = og_plane(g->d.vz, kv, g->bz) + 0.5f * g->d.vz;
@@ -1134,13 +1279,116 @@ static float og_ray_d12(const og_geom* g, float s, float c, int u, int v)
     float x2x, x2y, x2z;
     og_source(g, s, c, u, v, &x2x, &x2y, &x2z);
     const float pu = g->ymin + (float)u * g->d.du;
-    const float x1x = g->d.dod * c - pu * s, x1y = g->d.dod * s + pu * c, x1z = g->zmin + (float)v * g->d.dv;
+    const float x1x = g->d.dod * c - pu * s, x1y = g->d.dod * s + pu * c, x1z = og_row_z(g, v);
     return sqrtf((x2x - x1x) * (x2x - x1x) + (x2y - x1y) * (x2y - x1y) + (x2z - x1z) * (x2z - x1z));
+}
+
+/* The engine's TBCT SART update: the TBCT semantics (FOV mask, the
+ * per-voxel source exclusion of T42/...TBCT_voxel.cu:620-627 evaluated as
+ * there, a source's rays summed apart and the sources added in ascending
+ * order, pair threshold vx*1e-6f, update where the summed length exceeds
+ * vx*1e-3 in double, :772) with the projector's own chords; a source's pairs
+ * in the engine's order (detector column, then row). */
+static void og_backproject_gather_tbct(const og_geom* g, float* vol, const float* corr, float beta, float s, float c)
+{
+    const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->d.nv, K = g->d.n_sources;
+    const int ROWS = g->rows;
+    const float vx = g->d.vx, vy = g->d.vy, vz = g->d.vz;
+    const float DSO = g->d.dso, DOD = g->d.dod;
+    const float inv_du = 1.0f / g->d.du, inv_dv = 1.0f / g->d.dv;
+    float* col = (float*)malloc(sizeof(float) * 4 * R);
+    float* row = (float*)malloc(sizeof(float) * 2 * ROWS);
+    float* d12 = (float*)malloc(sizeof(float) * R * ROWS);
+    for (int u = 0; u < R; ++u) og_column_eff(g, s, c, u, &col[4 * u], &col[4 * u + 1], &col[4 * u + 2], &col[4 * u + 3]);
+    for (int v = 0; v < ROWS; ++v) og_row_eff(g, v, &row[2 * v], &row[2 * v + 1]);
+    for (int v = 0; v < ROWS; ++v)
+        for (int u = 0; u < R; ++u) d12[v * R + u] = og_ray_d12(g, s, c, u, v);
+    const float thr = vx * 1e-6f;
+    const double thr_upd = (double)vx * 1e-3;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Z; ++k)
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < M; ++i) {
+                if (og_fov_masked(g, i, j)) continue;
+                /* source exclusion, with the reference's voxel centre */
+                const float cxr = g->bx + vx * (0.5f + (float)i), cyr = g->by + vy * (0.5f + (float)j);
+                const float czr = g->bz + vz * (0.5f + (float)k);
+                const float tc = cxr * c + cyr * s;
+                const float upper = (czr + vz - g->zmin) * (DSO - DOD) / (tc - DOD) + g->zmin;
+                const float lower = (czr - vz - g->zmax) * (DSO - DOD) / (tc - DOD) + g->zmax;
+                /* candidate columns and, per source, rows: bounding rectangles of the corner
+                 * projections, rows widened by one each side (any superset gives the same sums) */
+                const float cx = g->bx + vx * 0.5f + (float)i * vx;
+                const float cy = g->by + vy * 0.5f + (float)j * vy;
+                const float cz = g->bz + vz * 0.5f + (float)k * vz;
+                float minY = INFINITY, maxY = -INFINITY;
+                for (int jj = 0; jj < 2; ++jj)
+                    for (int ii = 0; ii < 2; ++ii) {
+                        const float px = cx + (float)ii * vx - 0.5f * vx, py = cy + (float)jj * vy - 0.5f * vy;
+                        const float t = px * c + py * s, ss = -px * s + py * c;
+                        const float ou = (t - DOD) / (DSO - t) * (ss - g->srcy) + ss;
+                        minY = fminf(minY, ou); maxY = fmaxf(maxY, ou);
+                    }
+                int u0 = (int)floorf((minY - g->ymin) * inv_du + 0.5f), u1 = (int)floorf((maxY - g->ymin) * inv_du + 0.5f);
+                if ((u0 < 0 && u1 < 0) || (u0 > R - 1 && u1 > R - 1)) continue;
+                u0 = u0 < 0 ? 0 : u0;
+                u1 = u1 > R - 1 ? R - 1 : u1;
+                const float xlo = og_plane(vx, i, g->bx), xhi = og_plane(vx, i + 1, g->bx);
+                const float ylo = og_plane(vy, j, g->by), yhi = og_plane(vy, j + 1, g->by);
+                const float zlo = og_plane(vz, k, g->bz), zhi = og_plane(vz, k + 1, g->bz);
+                float WS = 0.0f, L = 0.0f;
+                for (int src = 0; src < K; ++src) {
+                    const float sz = g->zsrc0 + (float)src * g->zsrc_dz;
+                    if (sz < lower || sz > upper) continue;
+                    float minZ = INFINITY, maxZ = -INFINITY;
+                    for (int kk = 0; kk < 2; ++kk)
+                        for (int jj = 0; jj < 2; ++jj)
+                            for (int ii = 0; ii < 2; ++ii) {
+                                const float px = cx + (float)ii * vx - 0.5f * vx, py = cy + (float)jj * vy - 0.5f * vy;
+                                const float pz = cz + (float)kk * vz - 0.5f * vz;
+                                const float t = px * c + py * s;
+                                const float oz = (t - DOD) / (DSO - t) * (pz - sz) + pz;
+                                minZ = fminf(minZ, oz); maxZ = fmaxf(maxZ, oz);
+                            }
+                    int v0 = (int)floorf((minZ - g->zmin) * inv_dv + 0.5f), v1 = (int)floorf((maxZ - g->zmin) * inv_dv + 0.5f);
+                    if ((v0 < 0 && v1 < 0) || (v0 > ZP - 1 && v1 > ZP - 1)) continue;
+                    v0 = v0 - 1 < 0 ? 0 : v0 - 1;
+                    v1 = v1 + 1 > ZP - 1 ? ZP - 1 : v1 + 1;
+                    float sw = 0.0f, sl = 0.0f;
+                    for (int u = u0; u <= u1; ++u) {
+                        const float* ct = &col[4 * u];
+                        const float ax0 = (xlo - ct[0]) * ct[1], ax1 = (xhi - ct[0]) * ct[1];
+                        const float ay0 = (ylo - ct[2]) * ct[3], ay1 = (yhi - ct[2]) * ct[3];
+                        const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
+                        const float b = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+                        if (!(b > a)) continue;
+                        for (int vr = v0; vr <= v1; ++vr) {
+                            const int v = src * ZP + vr;
+                            const float az0 = (zlo - row[2 * v]) * row[2 * v + 1], az1 = (zhi - row[2 * v]) * row[2 * v + 1];
+                            const float lo = fmaxf(a, fminf(az0, az1)), hi = fminf(b, fmaxf(az0, az1));
+                            const float temp = d12[v * R + u] * (hi - lo);
+                            if (temp > thr) {
+                                sw = sw + temp * corr[v * R + u];
+                                sl = sl + temp;
+                            }
+                        }
+                    }
+                    WS = WS + sw;
+                    L = L + sl;
+                }
+                const long long idx = (long long)M * N * k + (long long)M * j + i;
+                if ((double)L > thr_upd) vol[idx] = vol[idx] + beta * WS / L;
+            }
+    free(col); free(row); free(d12);
 }
 
 void og_backproject_gather(const og_geom* g, float* vol, const float* corr, float beta, float s, float c)
 {
-    const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->d.nv;
+    if (g->d.ct_style == 3) {
+        og_backproject_gather_tbct(g, vol, corr, beta, s, c);
+        return;
+    }
+    const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->rows;
     const float vx = g->d.vx, vy = g->d.vy, vz = g->d.vz;
     const float DSO = g->d.dso, DOD = g->d.dod;
     const float inv_du = 1.0f / g->d.du, inv_dv = 1.0f / g->d.dv;
@@ -1212,7 +1460,7 @@ void og_backproject_gather(const og_geom* g, float* vol, const float* corr, floa
 
 void og_sart_pass_gather(const og_geom* g, float* vol, const float* sino, float beta)
 {
-    const long long P = (long long)g->d.nu * g->d.nv;
+    const long long P = (long long)g->d.nu * g->rows;
     float* corr = (float*)malloc(sizeof(float) * P);
     for (int j = 0; j < g->d.nviews; ++j) {
         float s, c;

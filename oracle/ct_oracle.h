@@ -15,6 +15,13 @@
  *   volume    f[k*M*N + j*M + i]      (V63/kernel_IterativeRecon_universal.cu:10)
  *   view      p[row*R + col]          (V63/kernel_IterativeRecon_universal.cu:17)
  *   sinogram  views stacked: p[view*R*Z_prj + row*R + col]
+ *
+ * ct_style 3 restates the tetrahedron-beam program TBCT/TBCT_1024V_1024P_
+ * v4.2_20171012 (abbreviated T42/): N_source sources stacked along z share
+ * the orbit, each with its own band of Z_prj detector rows, so one view is
+ * p[src*R*Z_prj + row*R + col] (T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:27)
+ * and every function below that loops over "rows" takes the N_source*Z_prj
+ * rows of og_geom.rows, row r belonging to source r / Z_prj.
  */
 #ifndef CT_ORACLE_H
 #define CT_ORACLE_H
@@ -41,6 +48,9 @@ typedef struct og_desc {
     float shift_angle;       /* degrees                                     */
     int   ct_style;          /* CT_style: 0 cone beam, 1 multi-slice fan     */
                              /* beam, 2 parallel beam (V63/main_recon.cu:29) */
+                             /* 3: tetrahedron beam (TBCT v4.2, below)       */
+    int   n_sources;         /* ct_style 3: N_source, sources along z, each  */
+                             /* with its own band of nv detector rows        */
 } og_desc;
 
 /* Derived constants, computed with the reference's float/double steps. */
@@ -50,16 +60,24 @@ typedef struct og_geom {
     float bx, by, bz;               /* boundary_voxel_*                     */
     float ymin, zmin;               /* Detector_Ymin, Detector_Zmin         */
     float srcx, srcy, srcz;         /* Source_x/y/z                         */
+    float zmax;                     /* Detector_Zmax (T42/main_recon.cu:91)   */
+    float zsrc0, zsrc_dz;           /* Source_z_min, Source_interval (:95-108) */
+    int   rows;                     /* detector rows of one view: nv, or     */
+                                    /* nv * n_sources for ct_style 3          */
 } og_geom;
 
 int  og_init(og_geom* g, const og_desc* d);
 /* Source (X2) of the ray through detector pixel (u, v) at a view, per
  * CT_style (V63/kernel_IterativeRecon_universal.cu:21-39): one source (0);
- * the source at the row's height (1); a source per pixel, opposite it (2). */
+ * the source at the row's height (1); a source per pixel, opposite it (2);
+ * source v / Z_prj of the stack (3, T42/...TBCT_voxel.cu:30-33). */
 void og_source(const og_geom* g, float s, float c, int u, int v, float* x2x, float* x2y, float* x2z);
 /* Per-view angle.  fdk=0: SART/FP frame theta' = -(j*us+init+shift)*pi/180
  * (V63/host_IterativeRecon_CBCT.c:34-41); fdk=1: +theta (V63/host_FDK.cpp:35-40). */
 void og_view_trig(const og_geom* g, int view, int fdk, float* s, float* c);
+/* z of the centre of detector row v (V63/...universal.cu:40; row v % Z_prj
+ * of its source's band for ct_style 3, T42/...TBCT_voxel.cu:40). */
+float og_row_z(const og_geom* g, int v);
 
 /* ---- Siddon forward projector (V63/kernel_IterativeRecon_universal.cu:7-567) ---- */
 /* One ray.  Returns the ray sum; *len gets the summed chord length.  When
@@ -81,7 +99,11 @@ void og_forward_trace(const og_geom* g, const float* vol, float s, float c, int 
 /* The same traversal in double throughout: the FP64 oracle. */
 void og_forward_view_f64(const og_geom* g, const double* vol, double s, double c, double* out);
 
-/* ---- reference voxel-driven BP (V63/kernel_IterativeRecon_universal.cu:571-810) ---- */
+/* ---- reference voxel-driven BP (V63/kernel_IterativeRecon_universal.cu:571-810) ----
+ * ct_style 3: the TBCT backprojection and update (T42/voxel/kernel_
+ * IterativeRecon_TBCT_voxel.cu:546-775), which has no command 0: the view's
+ * SART update whatever command is, its per-source sums added in ascending
+ * source order (one of the orders the reference's atomicAdd can take). */
 void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float beta,
                         float s, float c, int command);
 

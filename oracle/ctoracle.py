@@ -17,8 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libctoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libctref.so")
 # the reference fixes CT_style at compile time: one build per style
+# (3: the tetrahedron-beam program's kernels)
 REF_SO_STYLE = {0: REF_SO, 1: os.path.join(HERE, "_ref", "libctref_fbct.so"),
-                2: os.path.join(HERE, "_ref", "libctref_pbct.so")}
+                2: os.path.join(HERE, "_ref", "libctref_pbct.so"), 3: os.path.join(HERE, "_ref", "libctref_tbct.so")}
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -37,7 +38,7 @@ class OgDesc(C.Structure):
         ("dso", C.c_float), ("dod", C.c_float),
         ("offset", C.c_float), ("m_offset", C.c_int),
         ("us_rate", C.c_float), ("initial_angle", C.c_float), ("shift_angle", C.c_float),
-        ("ct_style", C.c_int),
+        ("ct_style", C.c_int), ("n_sources", C.c_int),
     ]
 
 
@@ -48,19 +49,23 @@ class OgGeom(C.Structure):
         ("bx", C.c_float), ("by", C.c_float), ("bz", C.c_float),
         ("ymin", C.c_float), ("zmin", C.c_float),
         ("srcx", C.c_float), ("srcy", C.c_float), ("srcz", C.c_float),
+        ("zmax", C.c_float), ("zsrc0", C.c_float), ("zsrc_dz", C.c_float), ("rows", C.c_int),
     ]
 
 
 def make_desc(nx, ny, nz, nu, nv, nviews, vx, du, dso, dod, us_rate=None,
-              initial_angle=0.0, shift_angle=0.0, offset=0.0, m_offset=0, ct_style=0, vz=None):
+              initial_angle=0.0, shift_angle=0.0, offset=0.0, m_offset=0, ct_style=0, vz=None,
+              n_sources=0):
     """ct_style 1 and 2 take the reference's z pitch, volumn_z = Detector_pixel_x
-    (V63/main_recon.cu:96), unless vz is given."""
+    (V63/main_recon.cu:96), unless vz is given.  ct_style 3 is the tetrahedron
+    beam with n_sources sources, nv detector rows each (volumn_z = volumn_x)."""
     if us_rate is None:
         us_rate = 360.0 / nviews
     if vz is None:
-        vz = vx if ct_style == 0 else du
+        vz = du if ct_style in (1, 2) else vx
     return OgDesc(nx, ny, nz, nu, nv, nviews, vx, vx, vz, du, du, dso, dod,
-                  offset, m_offset, us_rate, initial_angle, shift_angle, ct_style)
+                  offset, m_offset, us_rate, initial_angle, shift_angle, ct_style,
+                  n_sources if ct_style == 3 else 0)
 
 
 def build():
@@ -128,7 +133,8 @@ class Oracle:
 
     @property
     def view_shape(self):
-        return (self.desc.nv, self.desc.nu)
+        """(rows, columns) of one view: N_source bands of Z_prj rows for ct_style 3."""
+        return (self.g.rows, self.desc.nu)
 
     def trig(self, view, fdk=False):
         s, c = C.c_float(), C.c_float()
@@ -324,9 +330,11 @@ class RefOracle:
             "ref_fdk_bp_view": [_f32p, _f32p, f, f],
         }
         for name, args in sig.items():
-            getattr(lib, name).argtypes = args
-        lib.ref_tv_norm.restype = C.c_double
-        lib.ref_l2_norm.restype = C.c_double
+            if hasattr(lib, name):   # the tetrahedron-beam build has the projectors only
+                getattr(lib, name).argtypes = args
+        for name in ("ref_tv_norm", "ref_l2_norm"):
+            if hasattr(lib, name):
+                getattr(lib, name).restype = C.c_double
         self._set()
 
     def _set(self):
@@ -340,7 +348,8 @@ class RefOracle:
 
     @property
     def view_shape(self):
-        return (self.desc.nv, self.desc.nu)
+        d = self.desc
+        return (d.nv * (d.n_sources if d.ct_style == 3 else 1), d.nu)
 
     def trig(self, view, fdk=False):
         s, c = C.c_float(), C.c_float()

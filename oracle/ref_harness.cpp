@@ -10,6 +10,13 @@
  * thread-local variables that the launch loops below set, and the reference's
  * compile-time geometry constants (V63/main_recon.cu:54-111) become mutable
  * globals set by ref_set_geometry() with the same float/double steps.
+ *
+ * With -DREF_TBCT the same harness runs the tetrahedron-beam program's
+ * projector, backprojector and update kernels instead
+ * (TBCT/TBCT_1024V_1024P_v4.2_20171012/voxel/kernel_IterativeRecon_TBCT_voxel.cu,
+ * abbreviated T42/, read from REF_TBCT_DIR; output oracle/_ref/libctref_tbct.so).
+ * Its atomicAdd becomes a plain add: a voxel's sources are launched in
+ * ascending order by one thread.
  */
 #include <cmath>
 #include <complex>
@@ -49,11 +56,24 @@ static const float PI = 3.141592653589793f;
 
 #define REF_STR2(x) #x
 #define REF_STR(x) REF_STR2(x)
+#ifdef REF_TBCT
+/* T42/main_recon.cu:76-108 */
+static float boundary_voxel_z_upper, Detector_Zmax, Source_z_min, Source_interval;
+static int N_source;
+static inline float atomicAdd(float* p, float v)
+{
+    const float o = *p;
+    *p = o + v;
+    return o;
+}
+#include REF_STR(REF_TBCT_DIR/voxel/kernel_IterativeRecon_TBCT_voxel.cu)
+#else
 #include REF_STR(REF_DIR/kernel_IterativeRecon_universal.cu)
 #include REF_STR(REF_DIR/kernel_FGP_Denoise_GPUx7.cu)
 #include REF_STR(REF_DIR/kernel_tool_functions.cu)
 #include REF_STR(REF_DIR/FDK/kernel_FDK.cu)
 #include REF_STR(REF_DIR/FDK/FFT1d.h)
+#endif
 
 #include "ct_oracle.h"
 
@@ -63,9 +83,14 @@ extern "C" {
 int ref_set_geometry(const og_desc* d)
 {
     if (d->vy > 0.f && d->vy != d->vx) return -1;   /* the reference has one voxel pitch */
-    /* volumn_z = (CT_style == 0) ? volumn_x : Detector_pixel_x (V63/main_recon.cu:96) */
+    /* volumn_z = (CT_style == 0) ? volumn_x : Detector_pixel_x (V63/main_recon.cu:96);
+     * T42/main_recon.cu:73 volumn_z = volumn_x */
     const float vz_ref = CT_style == 0 ? d->vx : d->du;
+#ifdef REF_TBCT
+    if (d->ct_style != 3 || d->n_sources < 1) return -1;
+#else
     if (d->ct_style != CT_style) return -1;
+#endif
     if (d->vz > 0.f && d->vz != vz_ref) return -1;
     if (d->dv > 0.f && d->dv != d->du) return -1;   /* and one detector pitch */
     M = d->nx; N = d->ny; ZETA = d->nz;
@@ -86,6 +111,20 @@ int ref_set_geometry(const og_desc* d)
     boundary_voxel_z = -volumn_z * (float(ZETA) / 2.0f);
     Source_x = DSO; Source_y = Offset; Source_z = 0;
     us_rate = d->us_rate; initialAngle = d->initial_angle; shiftAngle = d->shift_angle;
+#ifdef REF_TBCT
+    /* T42/main_recon.cu:76, :93, :96-108 */
+    boundary_voxel_z_upper = -volumn_z * (float(ZETA) / 2.0f) + ZETA * volumn_z;
+    Detector_Zmax = +Detector_pixel_x * ((Z_prj) / 2.0f - 0.5f);
+    N_source = d->n_sources;
+    if (N_source == 1) {
+        Source_z_min = 0.0f;
+        Source_interval = 0.0f;
+    } else {
+        const float Source_z_max = (boundary_voxel_z_upper - Detector_Zmax) * (DSO - DOD) / DSO + Detector_Zmax;
+        Source_z_min = (boundary_voxel_z - Detector_Zmin) * (DSO - DOD) / DSO + Detector_Zmin;
+        Source_interval = (Source_z_max - Source_z_min) / (N_source - 1);
+    }
+#endif
     return 0;
 }
 
@@ -99,6 +138,75 @@ void ref_view_trig(int j, int fdk, float* s_out, float* c_out)
     *c_out = cos(t_theta);
 }
 
+#ifdef REF_TBCT
+/* forward_ray_driven_3d_kernel_correction over grid (1, Z_prj, N_source) x block R
+ * (T42/voxel/host_IterativeRecon_TBCT_voxel.c:48-49, one block row per launch here) */
+void ref_forward_view(const float* vol, float* out, const float* b, float s, float c, int command)
+{
+#pragma omp parallel for collapse(2) schedule(dynamic, 1)
+    for (int src = 0; src < N_source; ++src)
+        for (int v = 0; v < Z_prj; ++v) {
+            tl_blockDim = {(unsigned)R, 1, 1};
+            tl_gridDim = {1, (unsigned)Z_prj, (unsigned)N_source};
+            for (int u = 0; u < R; ++u) {
+                tl_blockIdx = {0, (unsigned)v, (unsigned)src};
+                tl_threadIdx = {(unsigned)u, 0, 0};
+                forward_ray_driven_3d_kernel_correction((float*)vol, out, (float*)b, s, c, (float)command);
+            }
+        }
+}
+
+/* The TBCT SART update of one view (T42/voxel/host_IterativeRecon_TBCT_voxel.c:67-75):
+ * zeroed weighted-sum and length volumes, backprj_ray_driven_3d_kernel over
+ * every voxel and source (sources of a voxel in ascending order), then
+ * update.  The kernel has no command: command is ignored. */
+void ref_backproject_view(float* vol, const float* corr, float beta, float s, float c, int command)
+{
+    (void)command;
+    const long long V = (long long)M * N * ZETA;
+    float* ws = (float*)calloc(V, sizeof(float));
+    float* len = (float*)calloc(V, sizeof(float));
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = 0; k < ZETA; ++k)
+        for (int j = 0; j < N; ++j) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            tl_gridDim = {(unsigned)N, (unsigned)ZETA, (unsigned)N_source};
+            for (int src = 0; src < N_source; ++src)
+                for (int i = 0; i < M; ++i) {
+                    tl_blockIdx = {(unsigned)j, (unsigned)k, (unsigned)src};
+                    tl_threadIdx = {(unsigned)i, 0, 0};
+                    backprj_ray_driven_3d_kernel(ws, len, (float*)corr, s, c);
+                }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < ZETA; ++k)
+        for (int j = 0; j < N; ++j) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            for (int i = 0; i < M; ++i) {
+                tl_blockIdx = {(unsigned)j, (unsigned)k, 0};
+                tl_threadIdx = {(unsigned)i, 0, 0};
+                update(vol, ws, len, beta);
+            }
+        }
+    free(ws);
+    free(len);
+}
+
+/* Reconstruction_3D_ray_driven_TBCT (T42/voxel/host_IterativeRecon_TBCT_voxel.c:1-92)
+ * for the views [v0, v0+nv) */
+void ref_sart_views(float* vol, const float* sino, float beta, int v0, int nv)
+{
+    const long long P = (long long)R * Z_prj * N_source;
+    float* corr = (float*)malloc(sizeof(float) * P);
+    for (int j = v0; j < v0 + nv; ++j) {
+        float s, c;
+        ref_view_trig(j, 0, &s, &c);
+        ref_forward_view(vol, corr, sino + P * j, s, c, 1);
+        ref_backproject_view(vol, corr, beta, s, c, 1);
+    }
+    free(corr);
+}
+#else
 /* forward_ray_driven_3d_kernel_correction over grid (1, Z_prj) x block R */
 void ref_forward_view(const float* vol, float* out, const float* b, float s, float c, int command)
 {
@@ -280,5 +388,7 @@ void ref_fdk_bp_view(float* vol, const float* proj, float s, float c)
             }
         }
 }
+
+#endif  /* REF_TBCT */
 
 }  /* extern "C" */

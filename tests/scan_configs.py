@@ -46,13 +46,34 @@ STYLES = {
                          initial_angle=3.5, ct_style=2),
 }
 
+# The tetrahedron-beam program (TBCT v4.2): n_sources sources stacked along z,
+# placed by the reference's automatic distribution, nv detector rows each.
+# Magnification 2 as in its sample configuration (DSO = -DOD); adjacent
+# sources' bands overlap in the volume.  "tbct_one": a single source at z = 0
+# and an odd row count, so the central row's rays lie in a z plane;
+# "tbct_odd": odd sizes, detector offset, M_Offset and shift angle.
+TBCT = {
+    "tbct": dict(nx=16, ny=16, nz=16, nu=32, nv=4, nviews=12, vx=1.0, du=1.2, dso=40.0, dod=-40.0,
+                 ct_style=3, n_sources=8),
+    "tbct_odd": dict(nx=15, ny=17, nz=13, nu=31, nv=3, nviews=8, vx=1.0, du=1.1, dso=50.0, dod=-30.0,
+                     offset=0.7, m_offset=1, shift_angle=3.0, ct_style=3, n_sources=3),
+    "tbct_one": dict(nx=16, ny=16, nz=16, nu=33, nv=5, nviews=8, vx=1.0, du=1.2, dso=40.0, dod=-40.0,
+                     ct_style=3, n_sources=1),
+}
+
 
 def og_desc(cfg):
     from oracle.ctoracle import make_desc
     return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["nu"], cfg["nv"], cfg["nviews"], cfg["vx"], cfg["du"],
                      cfg["dso"], cfg["dod"], initial_angle=cfg.get("initial_angle", 0.0),
                      shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
-                     m_offset=cfg.get("m_offset", 0), ct_style=cfg.get("ct_style", 0))
+                     m_offset=cfg.get("m_offset", 0), ct_style=cfg.get("ct_style", 0),
+                     n_sources=cfg.get("n_sources", 0))
+
+
+def view_rows(cfg):
+    """Detector rows of one view: every source's band for the tetrahedron beam."""
+    return cfg["nv"] * (cfg.get("n_sources", 1) if cfg.get("ct_style", 0) == 3 else 1)
 
 
 def og_desc_xyz(cfg):
@@ -67,7 +88,8 @@ def ctr_desc(cfg, entry64=False):
     return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["vx"], cfg["nu"], cfg["nv"], cfg["du"], cfg["dso"],
                      cfg["dod"], cfg["nviews"], initial_angle=cfg.get("initial_angle", 0.0),
                      shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
-                     m_offset=cfg.get("m_offset", 0), entry64=entry64, ct_style=cfg.get("ct_style", 0))
+                     m_offset=cfg.get("m_offset", 0), entry64=entry64, ct_style=cfg.get("ct_style", 0),
+                     n_sources=cfg.get("n_sources", 0))
 
 # Differentiation scan: 256^3, 360 views, 384^2 detector.  "Config-0 geometry
 # scaled by 2" is read as the same physical extents at twice the sampling:

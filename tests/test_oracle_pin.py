@@ -1,20 +1,22 @@
 """Pin the C restatement (oracle/ct_oracle.c) to the reference.
 
 The golden fixtures were produced by the reference's own kernel sources
-compiled for the CPU (tests/golden/make_golden.py), for the cone beam and
-the reference's fan-slice and parallel-beam geometries (CT_style 1, 2).  The restatement must
-reproduce them bit for bit: Siddon FP (command 0 and the SART correction),
-the voxel-driven BP (command 0 and the SART update), a whole SART pass, FGP,
-the TV and L2 norms, and the FDK weight / ramp / backprojection.
+compiled for the CPU (tests/golden/make_golden.py), for the cone beam, the
+reference's fan-slice and parallel-beam geometries (CT_style 1, 2) and its
+tetrahedron-beam program.  The restatement must reproduce them bit for bit:
+Siddon FP (command 0 and the SART correction), the voxel-driven BP (command
+0 and the SART update), a whole SART pass, FGP, the TV and L2 norms, and the
+FDK weight / ramp / backprojection (the tetrahedron beam: FP, its
+backprojection + update and its SART pass).
 """
 import os
 
 import numpy as np
 import pytest
 
-from scan_configs import SMALL, STYLES, og_desc_xyz
+from scan_configs import SMALL, STYLES, TBCT, og_desc_xyz
 
-CASES = dict(SMALL, **STYLES)
+CASES = dict(SMALL, **STYLES, **TBCT)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -43,9 +45,11 @@ def test_forward_bit_exact(case):
 
 
 def test_backproject_bit_exact(case):
-    _, _, o, g = case
+    _, cfg, o, g = case
     for a, j in enumerate(g["bp_views"]):
         np.testing.assert_array_equal(bits(o.backproject_ref(g["vol"], g["corr"][a], int(j), 0.8, 1)), bits(g["bp1"][a]))
+        if cfg.get("ct_style", 0) == 3:
+            continue   # the tetrahedron-beam backprojector has no command 0
         z = np.zeros_like(g["vol"])
         np.testing.assert_array_equal(bits(o.backproject_ref(z, g["corr"][a], int(j), 1.0, 0)), bits(g["bp0"][a]))
 
@@ -57,7 +61,9 @@ def test_sart_pass_bit_exact(case):
 
 
 def test_fgp_and_norms_bit_exact(case):
-    _, _, o, g = case
+    _, cfg, o, g = case
+    if cfg.get("ct_style", 0) == 3:
+        pytest.skip("the tetrahedron-beam program shares the cone-beam program's FGP")
     np.testing.assert_array_equal(bits(o.fgp(g["vol"], float(g["fgp_lambda"]), int(g["fgp_iters"]))), bits(g["fgp"]))
     assert o.tv_norm(g["vol"]) == float(g["tv"])
     assert o.l2_norm(g["fp0"], g["b"]) == float(g["l2"])
@@ -80,7 +86,7 @@ def test_fdk_stages(case):
     np.testing.assert_array_equal(bits(fdkbp), bits(g["fdkbp"]))
 
 
-@pytest.mark.parametrize("name", ["odd", "fan_slices_odd", "parallel_odd"])
+@pytest.mark.parametrize("name", ["odd", "fan_slices_odd", "parallel_odd", "tbct_odd"])
 def test_against_reference_build_directly(name, oracle_built):
     """When the reference checkout was compiled here, compare on fresh seeds too."""
     cfg = CASES[name]
