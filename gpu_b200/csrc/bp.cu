@@ -63,9 +63,12 @@ __device__ __forceinline__ SharedTables load_tables(const DevGeom& g, float* sp)
 // its BP_K voxels: the reference's bounding rectangle of the corner
 // projections (universal.cu:639-706).  u depends on the corner's x, y only;
 // the z projection scales by 1 + (t-DOD)/(DSO-t), bounded by its extremes
-// over the 4 xy corners.  Returns false when the column misses the detector.
+// over the 4 xy corners.  The rows are those of the band of nvr rows from
+// row0 seen from a source at height zs (one band for every style but the
+// tetrahedron beam).  Returns false when the column misses the detector.
 __device__ __forceinline__ bool candidate_rect(const DevGeom& g, const SharedTables& T, float cx, float cy, int k0,
-                                               float s, float c, int& ulo, int& uhi, int* vlo, int* vhi)
+                                               float s, float c, float zs, int row0, int& ulo, int& uhi, int* vlo,
+                                               int* vhi)
 {
     float umin = __int_as_float(0x7f800000), umax = -umin, mlo = umin, mhi = -umin;
 #pragma unroll
@@ -80,7 +83,8 @@ __device__ __forceinline__ bool candidate_rect(const DevGeom& g, const SharedTab
         umin = fminf(umin, ou); umax = fmaxf(umax, ou);
         mlo = fminf(mlo, mt); mhi = fmaxf(mhi, mt);
     }
-    if (g.ct_style != 0) { mlo = 0.0f; mhi = 0.0f; }   // rays parallel to the xy plane: rows in the voxel's z span
+    // rays parallel to the xy plane: rows in the voxel's z span
+    if (g.ct_style == 1 || g.ct_style == 2) { mlo = 0.0f; mhi = 0.0f; }
     ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
     uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
     if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) return false;
@@ -92,16 +96,16 @@ __device__ __forceinline__ bool candidate_rect(const DevGeom& g, const SharedTab
         vlo[kk] = 1; vhi[kk] = 0;
         if (k < g.Z) {
             const float z0 = T.PZ[k + 1], z1 = T.PZ[k + 2];
-            const float zlo = fs(z0, g.srcz), zhi = fs(z1, g.srcz);
+            const float zlo = fs(z0, zs), zhi = fs(z1, zs);
             const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
             const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
             const float zmn = fminf(fminf(a0, a1), fminf(b0, b1));
             const float zmx = fmaxf(fmaxf(a0, a1), fmaxf(b0, b1));
             const int lo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
             const int hi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
-            if (!((lo < 0 && hi < 0) || (lo > g.ZP - 1 && hi > g.ZP - 1))) {
-                vlo[kk] = max(lo, 0);
-                vhi[kk] = min(hi, g.ZP - 1);
+            if (!((lo < 0 && hi < 0) || (lo > g.nvr - 1 && hi > g.nvr - 1))) {
+                vlo[kk] = row0 + max(lo, 0);
+                vhi[kk] = row0 + min(hi, g.nvr - 1);
             }
         }
     }
@@ -144,7 +148,7 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
         const float ylo = T.PY[j + 1], yhi = T.PY[j + 2];
         const float2 sc = g.trig[view0];
         int ulo, uhi, vlo[BP_K], vhi[BP_K];
-        if (candidate_rect(g, T, cx, cy, k0, sc.x, sc.y, ulo, uhi, vlo, vhi)) {
+        if (candidate_rect(g, T, cx, cy, k0, sc.x, sc.y, g.srcz, 0, ulo, uhi, vlo, vhi)) {
             const float4* __restrict__ colt = g.colt + (long long)view0 * R;
             // the detector columns whose ray column crosses this voxel column
             // form one run; find it first so that lanes loop over it in step
@@ -237,9 +241,16 @@ ctr_status launch_zcell(const Geometry& G, float2* zcell, cudaStream_t st)
 // remain.  Every voxel sums its rays in the same order as k_backproject
 // (detector column ascending, then row ascending) with the same
 // arithmetic, so the two give bit-identical volumes.
+//
+// TB: the tetrahedron beam (T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:
+// 546-775).  Per voxel, the sources whose band can see it
+// (source_lower <= z_src <= source_upper, evaluated as T42 does at :620-627)
+// each contribute the sums over their own rows (column, then row, as
+// above); the sources are added in ascending order, and the update applies
+// where the summed length exceeds vx*1e-3 (:772).
 constexpr int WALK_RUN = 4;   // detector columns of the run kept in registers
 
-template <typename VT, bool STOCH, int BY, int MINB, bool TL, int UNR>
+template <typename VT, bool STOCH, int BY, int MINB, bool TL, int UNR, bool TB>
 __global__ void __launch_bounds__(32 * BY, MINB)
 k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
             uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
@@ -287,7 +298,8 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         umin = fminf(umin, ou); umax = fmaxf(umax, ou);
         mlo = fminf(mlo, mt); mhi = fmaxf(mhi, mt);
     }
-    if (g.ct_style != 0) { mlo = 0.0f; mhi = 0.0f; }   // rays parallel to the xy plane: rows in the voxel's z span
+    // rays parallel to the xy plane: rows in the voxel's z span
+    if (g.ct_style == 1 || g.ct_style == 2) { mlo = 0.0f; mhi = 0.0f; }
     int ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
     int uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
     if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) return;
@@ -325,30 +337,26 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
     // projections of the lower plane of voxel kb; each voxel's upper plane is
     // the next voxel's lower one, so its pair is carried (min and max of
     // four finite values do not depend on the grouping)
-    float cmn, cmx;
-    {
+    float cmn = 0.f, cmx = 0.f;
+    if (!TB) {
         const float z0 = PZ[kb + 1], zlo = fs(z0, g.srcz);
         const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
         cmn = fminf(a0, a1);
         cmx = fmaxf(a0, a1);
+    }
+    // TB: the depth of the column centre as T42 evaluates it (:568-569, :620)
+    float tden = 0.f;
+    if (TB) {
+        const float cxr = fa(g.bx, fm(g.vx, fa(0.5f, (float)i)));
+        const float cyr = fa(g.by, fm(g.vy, fa(0.5f, (float)j)));
+        tden = fs(fa(fm(cxr, c), fm(cyr, s)), g.dod);
     }
     // voxel and z-cell row addresses advance by a constant per z step
     const long long vstep = TL ? 64LL * g.Mt * g.Nt : MN;
     VT* pv = vol + (TL ? (long long)tile_index(g, i, j, kb) : (long long)kb * MN + (long long)j * g.M + i);
     const float2* __restrict__ zrow = g.zcell + (long long)kb * g.ZP;
     for (int k = kb; k < ke; ++k, pv += vstep, zrow += g.ZP) {
-        // candidate detector rows of voxel k
-        const float z1 = PZ[k + 2], zhi = fs(z1, g.srcz);
-        const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
-        const float bmn = fminf(b0, b1), bmx = fmaxf(b0, b1);
-        const float zmn = fminf(cmn, bmn), zmx = fmaxf(cmx, bmx);
-        cmn = bmn;
-        cmx = bmx;
-        int vlo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
-        int vhi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
-        if ((vlo < 0 && vhi < 0) || (vlo > g.ZP - 1 && vhi > g.ZP - 1)) continue;
-        vlo = max(vlo, 0);
-        vhi = min(vhi, g.ZP - 1);
+        int vlo = 0, vhi = -1;   // candidate rows (absolute row indices)
         float sw = 0.f, sl = 0.f;
         auto pair = [&](float a, float bb, float2 zc, float2 rec) {
             const float lo = fmaxf(a, zc.x);
@@ -373,20 +381,85 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
             }
             for (; vv <= vhi; ++vv) pair(a, bb, __ldg(zrow + vv), __ldg(rays + (long long)vv * R + uu));
         };
+        auto all_pairs = [&]() {
 #pragma unroll
-        for (int q = 0; q < WALK_RUN; ++q)
-            if (ua + q <= ub) pairs(ua + q, ra[q], rb[q]);
-        for (int uu = ua + WALK_RUN; uu <= ub; ++uu) {
-            const float4 ct = __ldg(colt + uu);
-            const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
-            const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
-            pairs(uu, fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)));
-        }
-        if (!(sl < g.thr_bp)) {                                                // :799-806
-            VT* p = pv;
-            const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, sw), sl));
-            if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
-            else Store<VT>::st(p, nv);
+            for (int q = 0; q < WALK_RUN; ++q)
+                if (ua + q <= ub) pairs(ua + q, ra[q], rb[q]);
+            for (int uu = ua + WALK_RUN; uu <= ub; ++uu) {
+                const float4 ct = __ldg(colt + uu);
+                const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+                const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+                pairs(uu, fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)));
+            }
+        };
+        // candidate rows of the band [row0, row0 + nvr) seen from height zs
+        // through the cell between planes z0 and z1
+        auto band_rows = [&](float z0, float z1, float zs, int row0) -> bool {
+            const float zlo = fs(z0, zs), zhi = fs(z1, zs);
+            const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
+            const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
+            const float zmn = fminf(fminf(a0, a1), fminf(b0, b1)), zmx = fmaxf(fmaxf(a0, a1), fmaxf(b0, b1));
+            int lo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
+            int hi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
+            if ((lo < 0 && hi < 0) || (lo > g.nvr - 1 && hi > g.nvr - 1)) return false;
+            vlo = row0 + max(lo, 0);
+            vhi = row0 + min(hi, g.nvr - 1);
+            return true;
+        };
+        if (!TB) {
+            // candidate detector rows of voxel k
+            const float z1 = PZ[k + 2], zhi = fs(z1, g.srcz);
+            const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
+            const float bmn = fminf(b0, b1), bmx = fmaxf(b0, b1);
+            const float zmn = fminf(cmn, bmn), zmx = fmaxf(cmx, bmx);
+            cmn = bmn;
+            cmx = bmx;
+            vlo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
+            vhi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
+            if ((vlo < 0 && vhi < 0) || (vlo > g.ZP - 1 && vhi > g.ZP - 1)) continue;
+            vlo = max(vlo, 0);
+            vhi = min(vhi, g.ZP - 1);
+            all_pairs();
+            if (!(sl < g.thr_bp)) {                                            // :799-806
+                VT* p = pv;
+                const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, sw), sl));
+                if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
+                else Store<VT>::st(p, nv);
+            }
+        } else {
+            // the sources T42 keeps for this voxel (:620-627): source_lower <= z <= source_upper
+            const float czr = fa(g.bz, fm(g.vz, fa(0.5f, (float)k)));
+            const float upper = fa(fdv(fm(fs(fa(czr, g.vz), g.zmin), g.dsod), tden), g.zmin);
+            const float lower = fa(fdv(fm(fs(fs(czr, g.vz), g.zmax), g.dsod), tden), g.zmax);
+            auto zsrc = [&](int q) { return fa(g.zsrc0, fm((float)q, g.zsrc_dz)); };
+            // the source heights increase with the index (zsrc_dz > 0), so the
+            // kept sources are one range [s0, s1]: estimated by division, then
+            // settled by T42's own comparisons
+            int s0 = 0, s1 = g.nsrc - 1;
+            if (g.nsrc > 1) {
+                s0 = (int)fminf(fmaxf(ceilf(fdv(fs(lower, g.zsrc0), g.zsrc_dz)), 0.f), (float)g.nsrc);
+                s1 = (int)fminf(fmaxf(floorf(fdv(fs(upper, g.zsrc0), g.zsrc_dz)), -1.f), (float)(g.nsrc - 1));
+            }
+            while (s0 > 0 && !(zsrc(s0 - 1) < lower)) --s0;
+            while (s0 < g.nsrc && zsrc(s0) < lower) ++s0;
+            while (s1 < g.nsrc - 1 && !(zsrc(s1 + 1) > upper)) ++s1;
+            while (s1 >= 0 && zsrc(s1) > upper) --s1;
+            const float z0 = PZ[k + 1], z1 = PZ[k + 2];
+            float WS = 0.f, L = 0.f;
+            for (int q = s0; q <= s1; ++q) {
+                if (!band_rows(z0, z1, zsrc(q), q * g.nvr)) continue;
+                sw = 0.f;
+                sl = 0.f;
+                all_pairs();
+                WS = fa(WS, sw);                                               // :754-755
+                L = fa(L, sl);
+            }
+            if (L > g.thr_upd) {                                               // :772-773
+                VT* p = pv;
+                const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, WS), L));
+                if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
+                else Store<VT>::st(p, nv);
+            }
         }
     }
 }
@@ -432,7 +505,7 @@ struct BpShape { int rows, zl, minb, unroll; };
 static constexpr BpShape kBpShapes[BP_SHAPES] = {{4, 8, 8, 1}, {4, 32, 8, 1}, {4, 32, 8, 2}, {8, 32, 4, 1},
                                                  {4, 128, 8, 1}, {4, 32, 10, 1}};
 
-template <typename VT, bool STOCH, bool TL>
+template <typename VT, bool STOCH, bool TL, bool TB>
 static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStream_t st, size_t smem)
 {
     const DevGeom& g = G.dg;
@@ -444,16 +517,16 @@ static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStrea
     if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
     const float2* rays = (const float2*)a.rays;
     if (sh.rows == 8)
-        k_sart_walk<VT, STOCH, 8, 4, TL, 1><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+        k_sart_walk<VT, STOCH, 8, 4, TL, 1, TB><<<grid, 256, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
                                                                      a.pass_seed, zl);
     else if (sh.minb == 10)
-        k_sart_walk<VT, STOCH, 4, 10, TL, 1><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+        k_sart_walk<VT, STOCH, 4, 10, TL, 1, TB><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
                                                                       a.pass_seed, zl);
     else if (sh.unroll == 2)
-        k_sart_walk<VT, STOCH, 4, 8, TL, 2><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+        k_sart_walk<VT, STOCH, 4, 8, TL, 2, TB><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
                                                                      a.pass_seed, zl);
     else
-        k_sart_walk<VT, STOCH, 4, 8, TL, 1><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+        k_sart_walk<VT, STOCH, 4, 8, TL, 1, TB><<<grid, 128, smem, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
                                                                      a.pass_seed, zl);
     return CTR_OK;
 }
@@ -496,11 +569,17 @@ k_adjoint(const DevGeom g, VT* __restrict__ vol, const AdjRay* __restrict__ rays
     const float cy = fa(fa(g.by, fm(g.vy, 0.5f)), fm((float)j, g.vy));
     const float xlo = T.PX[i + 1], xhi = T.PX[i + 2];
     const float ylo = T.PY[j + 1], yhi = T.PY[j + 2];
-    for (int w = 0; w < nview; ++w) {
+    for (int w = 0; w < nview; ++w)
+    for (int src = 0; src < g.nsrc; ++src) {   // each source's band of rows (one band but for TBCT)
         const int view = view0 + w;
         const float2 sc = g.trig[view];
+        const float zs = g.ct_style == 3 ? fa(g.zsrc0, fm((float)src, g.zsrc_dz)) : g.srcz;
         int ulo, uhi, vlo[BP_K], vhi[BP_K];
-        if (!candidate_rect(g, T, cx, cy, k0, sc.x, sc.y, ulo, uhi, vlo, vhi)) continue;
+        if (!candidate_rect(g, T, cx, cy, k0, sc.x, sc.y, zs, src * g.nvr, ulo, uhi, vlo, vhi)) break;
+        bool rows = false;
+#pragma unroll
+        for (int kk = 0; kk < BP_K; ++kk) rows |= vlo[kk] <= vhi[kk];
+        if (!rows) continue;
         const float4* __restrict__ colt = g.colt + (long long)view * R;
         const AdjRay* __restrict__ rw = rays + (long long)w * R * ZP;
         for (int uu = ulo; uu <= uhi; ++uu) {
@@ -558,9 +637,19 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         if (a.sart) {
             if (a.nview != 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART updates one view at a time");
-            if (a.tiled) {
-                if (a.flags & CTR_SART_STOCHASTIC_ROUND) CTR_TRY((launch_sart_walk<VT, true, true>(G, a, st, smem)));
-                else CTR_TRY((launch_sart_walk<VT, false, true>(G, a, st, smem)));
+            const bool sr = (a.flags & CTR_SART_STOCHASTIC_ROUND) != 0;
+            if (g.ct_style == 3) {   // the tetrahedron beam: column walks only (bp_shape -1 runs walk shape 1)
+                if (a.tiled) {
+                    if (sr) CTR_TRY((launch_sart_walk<VT, true, true, true>(G, a, st, smem)));
+                    else CTR_TRY((launch_sart_walk<VT, false, true, true>(G, a, st, smem)));
+                } else if (sr) {
+                    CTR_TRY((launch_sart_walk<VT, true, false, true>(G, a, st, smem)));
+                } else {
+                    CTR_TRY((launch_sart_walk<VT, false, false, true>(G, a, st, smem)));
+                }
+            } else if (a.tiled) {
+                if (sr) CTR_TRY((launch_sart_walk<VT, true, true, false>(G, a, st, smem)));
+                else CTR_TRY((launch_sart_walk<VT, false, true, false>(G, a, st, smem)));
             } else if (G.bp_shape < 0) {   // the fixed-shape kernel: 8 voxels of a column per thread
                 if (a.flags & CTR_SART_STOCHASTIC_ROUND)
                     k_backproject<VT, float2, true, true><<<grid, BP_THREADS, smem, st>>>(
@@ -568,12 +657,14 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
                 else
                     k_backproject<VT, float2, true, false><<<grid, BP_THREADS, smem, st>>>(
                         g, (VT*)a.vol, (const float2*)a.rays, a.view0, 0, a.beta, a.seed, nullptr);
-            } else if (a.flags & CTR_SART_STOCHASTIC_ROUND) {
-                CTR_TRY((launch_sart_walk<VT, true, false>(G, a, st, smem)));
+            } else if (sr) {
+                CTR_TRY((launch_sart_walk<VT, true, false, false>(G, a, st, smem)));
             } else {
-                CTR_TRY((launch_sart_walk<VT, false, false>(G, a, st, smem)));
+                CTR_TRY((launch_sart_walk<VT, false, false, false>(G, a, st, smem)));
             }
         } else if (a.flags & CTR_BP_FOV_MASK) {
+            if (g.ct_style == 3)
+                return set_error(CTR_ERR_UNSUPPORTED, "CTR_BP_FOV_MASK: the tetrahedron-beam backprojector has no command 0");
             for (int w = 0; w < a.nview; ++w)
                 k_backproject<VT, AdjRay, false, false><<<grid, BP_THREADS, smem, st>>>(
                     g, (VT*)a.vol, (const AdjRay*)a.rays + (size_t)w * G.npix(), a.view0 + w, (acc || w > 0) ? 1 : 0,

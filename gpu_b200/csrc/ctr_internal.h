@@ -16,19 +16,27 @@ namespace ctr {
 // (V63/main_recon.cu:60-111).
 struct DevGeom {
     int M, N, Z;            // volume
-    int R, ZP;              // detector columns, rows
+    int R, ZP;              // detector columns, rows of a view (all sources' bands for TBCT)
     int nviews;
     int max_steps;          // Siddon step bound nx+ny+nz+3
     int Mt, Nt;             // 8x8 (x, y) tiles per row / column of the tiled layout
     int fast_exit;          // every alpha inside the volume >= 1e-6: the Siddon loop test is one comparison
     int entry64;            // FP64 ray-box entry/exit
-    int ct_style;           // 0 cone beam, 1 multi-slice fan beam, 2 parallel beam (the reference's CT_style)
+    int ct_style;           // 0 cone beam, 1 multi-slice fan beam, 2 parallel beam (the reference's CT_style),
+                            // 3 tetrahedron beam (CTR_GEOM_TBCT)
+    int nvr;                // detector rows of one source's band (= ZP unless TBCT)
+    int nsrc;               // sources (1 unless TBCT)
     float vx, vy, vz, inv_vx, inv_vy, inv_vz;
     float bx, by, bz;       // boundary_voxel_*
     float ymin, zmin;       // Detector_Ymin/Zmin
     float du, dv, inv_du, inv_dv;
     float dso, dod;
     float srcx, srcy, srcz;
+    float zmax;             // TBCT: Detector_Zmax (T42/main_recon.cu:93)
+    float zsrc0, zsrc_dz;   // TBCT: Source_z_min, Source_interval (T42/main_recon.cu:96-108)
+    float dsod;             // DSO - DOD in float
+    float loop_eps;         // Siddon loop test alpha_max - alpha_c > loop_eps: 1e-16f, TBCT 1e-6f
+    float thr_upd;          // TBCT update threshold: L > thr_upd <=> (double)L > (double)vx*1e-3
     float thr_fp;           // volumn_z*1e-6f: FP zero-length threshold
     float thr_bp;           // volumn_x*1e-6f: BP pair and sum thresholds
     float fov_h_x, fov_h_y; // float(M)*0.5f-0.5f, float(N)*0.5f-0.5f
@@ -42,7 +50,7 @@ struct DevGeom {
     const float2* trig;     // [view] (sin, cos) of the FP/SART frame angle
     const float2* trig_fdk; // [view] (sin, cos) of the FDK frame angle
     const float4* colt;     // [view][u] (x1x, 1/dx, x1y, 1/dy), parallel axes encoded
-    const float2* rowt;     // [v] (x1z, 1/dz), parallel rows encoded
+    const float2* rowt;     // [v] (x1z, 1/dz) of every row of a view, parallel rows encoded
     const float2* zcell;    // [k][v] (min, max) of the z alphas of cell k's planes for row v
     unsigned int* err;      // device error bits (ERR_*)
 };
@@ -74,7 +82,7 @@ struct Geometry {
     int fp_shape = 1;                                  // FP: see kFpShapes in fp.cu
     int bp_shape = 1;                                  // SART BP: see kBpShapes in bp.cu
     long long nvox() const { return (long long)desc.nx * desc.ny * desc.nz; }
-    long long npix() const { return (long long)desc.nu * desc.nv; }
+    long long npix() const { return (long long)dg.R * dg.ZP; }
 };
 
 // error reporting (thread-local message)

@@ -99,15 +99,17 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
 
     // source X2 and detector pixel centre X1 (universal.cu:21-45): one
     // source (cone beam), the source at the row's height (multi-slice fan
-    // beam), or a source opposite each pixel (parallel beam)
+    // beam), or a source opposite each pixel (parallel beam); the tetrahedron
+    // beam's row v is row v % nvr of source v / nvr's band (T42/...TBCT_voxel.cu:23-40)
     const float pu = fa(g.ymin, fm((float)u, g.du));
     const float sy_ = g.ct_style == 2 ? pu : g.srcy;
     const float x2x = fs(fm(g.srcx, c), fm(sy_, s));
     const float x2y = fa(fm(g.srcx, s), fm(sy_, c));
     const float x1x = fs(fm(g.dod, c), fm(pu, s));
     const float x1y = fa(fm(g.dod, s), fm(pu, c));
-    const float x1z = fa(g.zmin, fm((float)v, g.dv));
-    const float x2z = g.ct_style == 0 ? g.srcz : x1z;
+    const int src = g.ct_style == 3 ? v / g.nvr : 0;
+    const float x1z = fa(g.zmin, fm((float)(v - src * g.nvr), g.dv));
+    const float x2z = g.ct_style == 3 ? fa(g.zsrc0, fm((float)src, g.zsrc_dz)) : (g.ct_style == 0 ? g.srcz : x1z);
     const float dx = fs(x2x, x1x), dy = fs(x2y, x1y), dz = fs(x2z, x1z);
     const float ix = fdv(1.0f, dx), iy = fdv(1.0f, dy), iz = fdv(1.0f, dz);
     r.d12 = __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));   // :290
@@ -126,6 +128,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     int i_min, i_max, j_min, j_max, k_min, k_max;
     bool hit;
     const bool zpar = fabsf(fs(x1z, x2z)) < fm(g.vz, 1e-6f);
+    const bool zpar_k = zpar && g.ct_style != 3;   // T42 has no z-parallel k range (T42/...TBCT_voxel.cu:171)
     if (!E64) {
         hit = !(amax <= amin);
         if (!hit) return r;
@@ -144,7 +147,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
             j_max = (amin == aymin) ? N - 1 : __float2int_rz(pos_floor(amin, dy, x1y, g.by, g.inv_vy));
             j_min = (amax == aymax) ? 0 : __float2int_rz(fa(pos_floor(amax, dy, x1y, g.by, g.inv_vy), 1.0f));
         }
-        if (zpar) {
+        if (zpar_k) {
             const float fz = floorf(fm(fs(x1z, g.bz), g.inv_vz));
             k_min = __float2int_rz(fa(fz, 1.0f));
             k_max = __float2int_rz(fz);
@@ -187,7 +190,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
             j_max = (Amin == Aymin) ? N - 1 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amin, Dy), X1y), By), IVy));
             j_min = (Amax == Aymax) ? 0 : (int)floor(__dmul_rn(__dsub_rn(__dadd_rn(__dmul_rn(Amax, Dy), X1y), By), IVy)) + 1;
         }
-        if (zpar) {
+        if (zpar_k) {
             k_min = (int)floor(__dmul_rn(__dsub_rn(X1z, Bz), IVz)) + 1;
             k_max = (int)floor(__dmul_rn(__dsub_rn(X1z, Bz), IVz));
         } else if (x1z < x2z) {
@@ -255,7 +258,8 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     // least ac and grows along its axis, so an index leaves the volume
     // exactly when ac reaches the alpha of that axis's last plane in index
     // space (aex*: the next plane of the last voxel); and when every alpha of
-    // the volume is >= 1e-6 (geometry flag fast_exit), amax - ac > 1e-16 is
+    // the volume is >= 1e-6 (geometry flag fast_exit, never set for the
+    // tetrahedron beam's test against 1e-6), amax - ac > 1e-16 is
     // ac < amax (distinct floats >= 2^-28 differ by more than 2^-51).  The
     // first step keeps the reference's own test, which also covers a start
     // voxel whose next plane lies behind the entry point.
@@ -269,7 +273,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     // :297-551.  Branch-free step: every axis re-evaluates its next-plane
     // alpha from its (possibly unchanged) index, which reproduces the current
     // value bit for bit when the axis did not move.
-    bool go = (fs(amax, ac) > 1e-16f) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
+    bool go = (fs(amax, ac) > g.loop_eps) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
               ((unsigned)vk < (unsigned)Z);
     while (go) {
         const float m = fminf(fminf(ax, ay), az);
@@ -330,7 +334,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
             }
         }
         if (g.fast_exit) go = ac < alim;
-        else go = (fs(amax, ac) > 1e-16f) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
+        else go = (fs(amax, ac) > g.loop_eps) & ((unsigned)vi < (unsigned)M) & ((unsigned)vj < (unsigned)N) &
                   ((unsigned)vk < (unsigned)Z);
     }
     if (LOAD && any) {

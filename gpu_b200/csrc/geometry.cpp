@@ -124,7 +124,10 @@ static ctr_status validate(const ctr_geometry_desc* d)
     const double vox = (double)((d->nx + 7) / 8 * 8) * ((d->ny + 7) / 8 * 8) * d->nz;   // tiled layout
     if (vox > 2147483647.0)
         return set_error(CTR_ERR_BAD_GEOMETRY, "volume of %.0f voxels exceeds the 2^31-1 index range", vox);
-    if ((double)d->nu * d->nv > 2147483647.0)
+    const bool tbct = (d->flags & CTR_GEOM_TBCT) != 0;
+    if (tbct && d->n_sources < 1) return set_error(CTR_ERR_BAD_GEOMETRY, "CTR_GEOM_TBCT needs n_sources >= 1");
+    const double rows = (double)d->nv * (tbct ? d->n_sources : 1);
+    if ((double)d->nu * rows > 2147483647.0)
         return set_error(CTR_ERR_BAD_GEOMETRY, "detector too large");
     if (!(d->vx > 0.f) || !(d->du > 0.f) || !std::isfinite(d->vx) || !std::isfinite(d->du))
         return set_error(CTR_ERR_BAD_GEOMETRY, "voxel and detector pitch must be positive and finite");
@@ -139,9 +142,13 @@ static ctr_status validate(const ctr_geometry_desc* d)
                              std::fabs((double)d->m_offset * d->vx);
     if (half_diag >= d->dso || half_diag >= -d->dod)
         return set_error(CTR_ERR_BAD_GEOMETRY, "volume (half-diagonal %.4g) reaches the source or detector", half_diag);
-    if ((d->flags & CTR_GEOM_FAN_SLICES) && (d->flags & CTR_GEOM_PARALLEL))
-        return set_error(CTR_ERR_BAD_GEOMETRY, "CTR_GEOM_FAN_SLICES and CTR_GEOM_PARALLEL exclude each other");
-    if (d->nx > 65535 || d->ny > 65535 * 8 || d->nz > 65535 || d->nv > 65535 * 4)
+    const int styles = ((d->flags & CTR_GEOM_FAN_SLICES) ? 1 : 0) + ((d->flags & CTR_GEOM_PARALLEL) ? 1 : 0) +
+                       (tbct ? 1 : 0);
+    if (styles > 1)
+        return set_error(CTR_ERR_BAD_GEOMETRY, "CTR_GEOM_FAN_SLICES, CTR_GEOM_PARALLEL and CTR_GEOM_TBCT exclude each other");
+    if (tbct && ((d->vz > 0.f && d->vz != d->vx) || (d->dv > 0.f && d->dv != d->du)))
+        return set_error(CTR_ERR_BAD_GEOMETRY, "CTR_GEOM_TBCT needs vz = vx and dv = du (the reference's single pitches)");
+    if (d->nx > 65535 || d->ny > 65535 * 8 || d->nz > 65535 || rows > 65535.0 * 4)
         return set_error(CTR_ERR_BAD_GEOMETRY, "dimension exceeds the launch limits");
     return CTR_OK;
 }
@@ -169,7 +176,12 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     cudaGetDevice(&g->device);
 
     DevGeom& q = g->dg;
-    q.M = d.nx; q.N = d.ny; q.Z = d.nz; q.R = d.nu; q.ZP = d.nv; q.nviews = d.n_views;
+    const bool tbct = (d.flags & CTR_GEOM_TBCT) != 0;
+    if (!tbct) d.n_sources = 0;
+    g->desc.n_sources = d.n_sources;
+    q.nsrc = tbct ? d.n_sources : 1;
+    q.nvr = d.nv;
+    q.M = d.nx; q.N = d.ny; q.Z = d.nz; q.R = d.nu; q.ZP = d.nv * q.nsrc; q.nviews = d.n_views;
     q.max_steps = d.nx + d.ny + d.nz + 3;
     q.Mt = (d.nx + 7) / 8;
     q.Nt = (d.ny + 7) / 8;
@@ -178,10 +190,12 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
         // the volume's nearest point is at least -DOD - (half-diagonal) away
         const double half_diag = 0.5 * std::sqrt((double)d.nx * d.vx * d.nx * d.vx + (double)d.ny * d.vy * d.ny * d.vy) +
                                  std::fabs((double)d.m_offset * d.vx);
-        q.fast_exit = ((-(double)d.dod - half_diag) / ((double)d.dso - (double)d.dod) >= 1e-6) ? 1 : 0;
+        // (the tetrahedron beam's loop test, alpha_max - alpha_c > 1e-6f, has no one-comparison form)
+        q.fast_exit = (!tbct && (-(double)d.dod - half_diag) / ((double)d.dso - (double)d.dod) >= 1e-6) ? 1 : 0;
     }
     q.entry64 = (d.flags & CTR_GEOM_ENTRY_F64) ? 1 : 0;
-    q.ct_style = (d.flags & CTR_GEOM_FAN_SLICES) ? 1 : ((d.flags & CTR_GEOM_PARALLEL) ? 2 : 0);
+    q.ct_style = tbct ? 3 : ((d.flags & CTR_GEOM_FAN_SLICES) ? 1 : ((d.flags & CTR_GEOM_PARALLEL) ? 2 : 0));
+    q.loop_eps = tbct ? 1e-6f : 1e-16f;   // T42/...TBCT_voxel.cu:282, V63/...universal.cu:291
     q.vx = d.vx; q.vy = d.vy; q.vz = d.vz;
     // inv_volumn_x = 1.0/volumn_x (double division stored as float), main_recon.cu:88
     q.inv_vx = (float)(1.0 / (double)d.vx);
@@ -199,6 +213,29 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     q.inv_dv = 1.0f / d.dv;
     q.dso = d.dso; q.dod = d.dod;
     q.srcx = d.dso; q.srcy = d.offset; q.srcz = 0.0f;   // main_recon.cu:101-103
+    q.dsod = d.dso - d.dod;
+    q.zmax = +d.du * ((float)d.nv / 2.0f - 0.5f);        // T42/main_recon.cu:93
+    q.zsrc0 = 0.0f;
+    q.zsrc_dz = 0.0f;
+    if (tbct && d.n_sources > 1) {                        // T42/main_recon.cu:76, :104-107
+        const float bzu = -d.vz * ((float)d.nz / 2.0f) + (float)d.nz * d.vz;
+        const float zsmax = (bzu - q.zmax) * (d.dso - d.dod) / d.dso + q.zmax;
+        q.zsrc0 = (q.bz - q.zmin) * (d.dso - d.dod) / d.dso + q.zmin;
+        q.zsrc_dz = (zsmax - q.zsrc0) / (float)(d.n_sources - 1);
+        if (!(q.zsrc_dz > 0.f)) {
+            delete g;
+            return set_error(CTR_ERR_BAD_GEOMETRY, "CTR_GEOM_TBCT: the source spacing is not positive "
+                                                   "(detector band taller than the magnified volume)");
+        }
+    }
+    {
+        // T42/...TBCT_voxel.cu:772 compares the float sum with the double
+        // volumn_x*1e-3: the same as comparing with the largest float <= it
+        const double t = (double)d.vx * 1e-3;
+        float f = (float)t;
+        if ((double)f > t) f = std::nextafter(f, -INFINITY);
+        q.thr_upd = f;
+    }
     q.thr_fp = d.vz * 1e-6f;       // universal.cu:554
     q.thr_bp = d.vx * 1e-6f;       // universal.cu:785,799
     q.fov_h_x = (float)d.nx * 0.5f - 0.5f;
@@ -260,10 +297,12 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
         }
     }
     // BP row table: x1z and 1/(x2z-x1z) per detector row, same encoding.
-    std::vector<float2> rowt(d.nv);
-    for (int v = 0; v < d.nv; ++v) {
-        const float x1z = q.zmin + (float)v * q.dv;
-        const float x2z = q.ct_style == 0 ? q.srcz : x1z;   // fan slices, parallel beam: rows parallel to xy
+    std::vector<float2> rowt(q.ZP);
+    for (int v = 0; v < q.ZP; ++v) {
+        const int src = v / q.nvr, vr = v - src * q.nvr;
+        const float x1z = q.zmin + (float)vr * q.dv;
+        // fan slices, parallel beam: rows parallel to xy; tetrahedron beam: the band's source
+        const float x2z = q.ct_style == 3 ? q.zsrc0 + (float)src * q.zsrc_dz : (q.ct_style == 0 ? q.srcz : x1z);
         if (std::fabs(x1z - x2z) < q.vz * 1e-6f) {
             const int kv = parallel_voxel(x1z, q.bz, q.inv_vz);
             rowt[v].x = plane(q.vz, kv, q.bz) + 0.5f * q.vz;
@@ -279,7 +318,7 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t o_px = 0, o_py = o_px + al(n_px * 4), o_pz = o_py + al(n_py * 4),
                  o_tr = o_pz + al(n_pz * 4), o_tf = o_tr + al(d.n_views * 8),
-                 o_row = o_tf + al(d.n_views * 8), total = o_row + al(d.nv * 8);
+                 o_row = o_tf + al(d.n_views * 8), total = o_row + al((size_t)q.ZP * 8);
     ctr_status st = CTR_OK;
     char* base = nullptr;
     cudaError_t e;
@@ -290,7 +329,7 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
         (e = cudaMemcpy(base + o_pz, g->h_pz.data(), n_pz * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(base + o_tr, g->h_trig.data(), d.n_views * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(base + o_tf, g->h_trig_fdk.data(), d.n_views * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(base + o_row, rowt.data(), d.nv * 8, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        (e = cudaMemcpy(base + o_row, rowt.data(), (size_t)q.ZP * 8, cudaMemcpyHostToDevice)) != cudaSuccess) {
         st = cuda_error(e, "cudaMemcpy(tables)");
         goto fail;
     }
@@ -310,7 +349,7 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     q.rowt = (const float2*)(base + o_row);
     q.colt = g->d_colt;
     q.err = g->d_err;
-    if ((e = cudaMalloc(&g->d_zcell, sizeof(float2) * (size_t)d.nz * d.nv)) != cudaSuccess) {
+    if ((e = cudaMalloc(&g->d_zcell, sizeof(float2) * (size_t)d.nz * q.ZP)) != cudaSuccess) {
         st = cuda_error(e, "cudaMalloc(zcell)");
         goto fail;
     }

@@ -34,6 +34,7 @@ BP_ACCUMULATE = 0x1
 BP_FOV_MASK = 0x2
 GEOM_FAN_SLICES = 0x2
 GEOM_PARALLEL = 0x4
+GEOM_TBCT = 0x8
 SART_STOCHASTIC_ROUND = 0x1
 SART_TILED = 0x2
 
@@ -71,7 +72,7 @@ class GeometryDesc(C.Structure):
         ("du", C.c_float), ("dv", C.c_float),
         ("dso", C.c_float), ("dod", C.c_float), ("offset", C.c_float), ("m_offset", C.c_int),
         ("n_views", C.c_int), ("us_rate", C.c_float), ("initial_angle", C.c_float),
-        ("shift_angle", C.c_float), ("flags", C.c_uint),
+        ("shift_angle", C.c_float), ("flags", C.c_uint), ("n_sources", C.c_int),
     ]
 
 
@@ -202,17 +203,19 @@ def dtype_code(t) -> int:
 
 
 def make_desc(nx, ny, nz, vx, nu, nv, du, dso, dod, n_views, us_rate=None, initial_angle=0.0,
-              shift_angle=0.0, offset=0.0, m_offset=0, entry64=False, vy=0.0, vz=0.0, dv=0.0, ct_style=0):
+              shift_angle=0.0, offset=0.0, m_offset=0, entry64=False, vy=0.0, vz=0.0, dv=0.0, ct_style=0,
+              n_sources=0):
     """ct_style: 0 cone beam, 1 multi-slice fan beam, 2 parallel beam (the
     reference's CT_style); styles 1 and 2 default vz to the detector pitch, as
-    the reference does."""
+    the reference does.  ct_style 3: the tetrahedron beam with n_sources
+    sources, nv detector rows each (a view has n_sources * nv rows)."""
     if us_rate is None:
         us_rate = 360.0 / n_views
-    if ct_style and not vz:
+    if ct_style in (1, 2) and not vz:
         vz = du
-    flags = (GEOM_ENTRY_F64 if entry64 else 0) | {0: 0, 1: GEOM_FAN_SLICES, 2: GEOM_PARALLEL}[ct_style]
+    flags = (GEOM_ENTRY_F64 if entry64 else 0) | {0: 0, 1: GEOM_FAN_SLICES, 2: GEOM_PARALLEL, 3: GEOM_TBCT}[ct_style]
     return GeometryDesc(nx, ny, nz, vx, vy, vz, nu, nv, du, dv, dso, dod, offset, m_offset, n_views,
-                        us_rate, initial_angle, shift_angle, flags)
+                        us_rate, initial_angle, shift_angle, flags, n_sources if ct_style == 3 else 0)
 
 
 class Geometry:
@@ -243,7 +246,9 @@ class Geometry:
 
     @property
     def view_shape(self):
-        return (self.desc.nv, self.desc.nu)
+        """(rows, columns) of one view; the tetrahedron beam's rows are all its sources' bands."""
+        d = self.desc
+        return (d.nv * (d.n_sources if d.flags & GEOM_TBCT else 1), d.nu)
 
     @property
     def n_views(self):

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CTRECON_ABI_VERSION 1
+#define CTRECON_ABI_VERSION 2
 
 typedef enum ctr_status {
     CTR_OK = 0,
@@ -67,6 +67,7 @@ typedef struct ctr_geometry_desc {
     float initial_angle;       /* degrees                                               */
     float shift_angle;         /* degrees                                               */
     unsigned flags;            /* CTR_GEOM_* below                                      */
+    int   n_sources;           /* CTR_GEOM_TBCT: N_source (>= 1); ignored otherwise     */
 } ctr_geometry_desc;
 
 /* Compute the ray-box entry/exit parameters and the first plane indices in
@@ -80,6 +81,21 @@ typedef struct ctr_geometry_desc {
  * pitch.  FDK supports the cone beam only. */
 #define CTR_GEOM_FAN_SLICES 0x2u
 #define CTR_GEOM_PARALLEL 0x4u
+/* Tetrahedron-beam CT (TBCT/TBCT_1024V_1024P_v4.2_20171012, abbreviated
+ * T42/): n_sources sources stacked along z on the orbit, placed as the
+ * reference places them (T42/main_recon.cu:95-108: the first source sees the
+ * volume's bottom face from the detector's bottom row, the last its top face
+ * from the top row), each with its own band of nv detector rows.  A view is
+ * n_sources bands of nv rows, view[(src*nv + row)*nu + col]
+ * (T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:27): every "row" count of
+ * this API is n_sources*nv.  The projector is T42's (its loop test
+ * alpha_max - alpha_c > 1e-6f and k range); the SART update is T42's
+ * backprojection + update (a voxel's rays summed per source, sources whose
+ * band cannot see the voxel skipped, update where the summed length exceeds
+ * vx*1e-3) with the projector's chords.  Requires vz = vx and dv = du (the
+ * reference's single pitches).  Not with CTR_GEOM_FAN_SLICES/PARALLEL, FDK or
+ * CTR_BP_FOV_MASK (T42's backprojector has no command 0). */
+#define CTR_GEOM_TBCT 0x8u
 
 typedef struct ctr_geometry ctr_geometry;
 

@@ -10,12 +10,13 @@ filter (FP32 convolution against the FP64 kernel), FP64 reductions.
 import numpy as np
 import pytest
 
-from scan_configs import CONFIG0, NEAR_DETECTOR, NO_ON_PLANE_RAYS, SMALL, STYLES, ctr_desc, og_desc_xyz
+from scan_configs import CONFIG0, NEAR_DETECTOR, NO_ON_PLANE_RAYS, SMALL, STYLES, TBCT, ctr_desc, og_desc_xyz
 
-FP_CASES = dict(SMALL, near_detector=NEAR_DETECTOR, **STYLES)
-BP_CASES = dict(SMALL, **STYLES)
-# the fan-slice scan has no ray on a voxel plane either (its rows sit at voxel centres)
-NO_ON_PLANE = NO_ON_PLANE_RAYS + ["fan_slices"]
+FP_CASES = dict(SMALL, near_detector=NEAR_DETECTOR, **STYLES, **TBCT)
+BP_CASES = dict(SMALL, **STYLES, **TBCT)
+# the fan-slice scan has no ray on a voxel plane either (its rows sit at voxel
+# centres), nor have the even and the offset tetrahedron-beam scans
+NO_ON_PLANE = NO_ON_PLANE_RAYS + ["fan_slices", "tbct", "tbct_odd"]
 
 pytestmark = pytest.mark.gpu
 
@@ -148,10 +149,22 @@ def test_masked_adjoint_vs_reference_bp(name, oracle_built):
         assert np.abs(got - ref).max() <= 2e-3 * scale
 
 
+def test_tbct_has_no_masked_command0(oracle_built):
+    """The tetrahedron-beam backprojector has no command 0: refused."""
+    import gpu_b200
+    cfg = TBCT["tbct"]
+    g, o = pair(cfg, oracle_built)
+    c = torch.zeros((1,) + o.view_shape, device="cuda")
+    vol = torch.zeros(o.vol_shape, device="cuda")
+    with pytest.raises(gpu_b200.CtrError):
+        g.backproject(c, vol, 0, 1, flags=gpu_b200.BP_FOV_MASK)
+
+
 @pytest.mark.parametrize("name", sorted(BP_CASES))
 def test_sart_pass(name, oracle_built):
     """The SART pass equals the restated engine algorithm bit for bit, and the
-    reference's own BP (its alpha formula) to alpha rounding."""
+    reference's own BP (its alpha formula) to alpha rounding (for the
+    tetrahedron beam: its backprojection and update)."""
     cfg = BP_CASES[name]
     g, o = pair(cfg, oracle_built)
     rng = np.random.default_rng(17)

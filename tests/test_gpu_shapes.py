@@ -5,9 +5,9 @@ bit-identical projections and SART passes."""
 import numpy as np
 import pytest
 
-from scan_configs import SMALL, STYLES, ctr_desc, og_desc_xyz
+from scan_configs import SMALL, STYLES, TBCT, ctr_desc, og_desc_xyz
 
-CASES = dict(SMALL, **STYLES)
+CASES = dict(SMALL, **STYLES, **TBCT)
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -23,7 +23,8 @@ def bits(t):
     return t.float().cpu().numpy().view(np.uint32)
 
 
-@pytest.mark.parametrize("name", ["cube16", "odd", "aniso", "fine_even", "fan_slices_odd", "parallel"])
+@pytest.mark.parametrize("name", ["cube16", "odd", "aniso", "fine_even", "fan_slices_odd", "parallel", "tbct",
+                                  "tbct_odd"])
 @pytest.mark.parametrize("dtype", ["f32", "bf16_sr"])
 def test_every_shape_gives_the_same_result(name, dtype, oracle_built):
     import gpu_b200

@@ -3,7 +3,9 @@ against the same call sequence composed from oracle functions."""
 import numpy as np
 import pytest
 
-from scan_configs import SMALL, ctr_desc, og_desc_xyz
+from scan_configs import SMALL, TBCT, ctr_desc, og_desc_xyz
+
+SOLVER_CASES = dict(SMALL, **TBCT)
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -38,11 +40,11 @@ def oracle_fista(o, b, beta, lam_tv, fgp_iters, n_iter):
     return xprev, np.array(objs)
 
 
-@pytest.mark.parametrize("name", ["cube16", "aniso"])
+@pytest.mark.parametrize("name", ["cube16", "aniso", "tbct"])
 @pytest.mark.parametrize("graph", [True, False])
 def test_solver_matches_oracle_sequence(name, graph, oracle_built):
     import gpu_b200
-    cfg = SMALL[name]
+    cfg = SOLVER_CASES[name]
     o = oracle_built.Oracle(og_desc_xyz(cfg))
     g = gpu_b200.Geometry(ctr_desc(cfg))
     params = np.array([[0, 0, 0, 5, 4, 3, 0.3, 0.2, 0.1, 0.02], [1.5, -1, 0.5, 2, 2, 2, 0, 0, 0, 0.03]])
