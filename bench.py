@@ -44,9 +44,10 @@ def parse():
                    help="with --profile-views: also run two FP16 solver iterations (the second in steady state)")
     p.add_argument("--profile-tune", action="store_true",
                    help="with --profile-views: also print the tuner's time for every launch shape")
-    p.add_argument("--workload", choices=["scan512", "batched", "large"], default="scan512",
+    p.add_argument("--workload", choices=["scan512", "batched", "large", "tbct"], default="scan512",
                    help="scan512: the 512^3 / 1024-view scan (default); batched: 48 uneven scans in one graph; "
-                        "large: 1024^3 / 1024 views / 1024^2 detector in FP32, BF16 and FP16")
+                        "large: 1024^3 / 1024 views / 1024^2 detector in FP32, BF16 and FP16; tbct: the "
+                        "tetrahedron-beam program's scan (512^3, 64 sources x 16 rows x 1024, 360 views)")
     p.add_argument("--scans", type=int, default=48, help="batched: number of scans")
     p.add_argument("--no-tune", action="store_true", help="batched: keep the default launch shapes")
     p.add_argument("--no-sr", action="store_true", help="batched: BF16 updates rounded to nearest instead of "
@@ -247,12 +248,19 @@ def profile_views(args):
 
     import gpu_b200
     n = args.profile_views
-    desc = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
-                              SCAN["dso"], SCAN["dod"], SCAN["n_views"])
-    geom = gpu_b200.Geometry(desc)
+    tbct = args.workload == "tbct"
+    if tbct:     # the tetrahedron-beam scan: its geometry, phantom and relaxation
+        geom, ph = tbct_geometry(0)
+        n_views, beta, lam = TBCT_SCAN["n_views"], TBCT_BETA, 0.0
+    else:
+        geom = gpu_b200.Geometry(gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"],
+                                                    SCAN["nv"], SCAN["du"], SCAN["dso"], SCAN["dod"],
+                                                    SCAN["n_views"]))
+        ph = phantom_params(2024)
+        n_views, beta, lam = SCAN["n_views"], BETA, LAMBDA_TV
     truth = torch.zeros(geom.vol_shape, device="cuda")
-    geom.phantom_voxelize(phantom_params(2024), truth)
-    nv = SCAN["n_views"] if args.profile_iteration else n
+    geom.phantom_voxelize(ph, truth)
+    nv = n_views if args.profile_iteration else n
     sino16 = torch.zeros((nv,) + geom.view_shape, device="cuda", dtype=torch.float16)
     geom.forward(truth, sino16, 0, nv)
     sino32 = sino16[:n].float()
@@ -263,12 +271,12 @@ def profile_views(args):
         geom.set_shapes(1, 1)
     for name, s in (("f32", sino32), ("f16", sino16)):
         vol = torch.zeros(geom.vol_shape, device="cuda", dtype=s.dtype)
-        fp, bp = geom.sart_views(vol, s, BETA, 0, n, flags=gpu_b200.SART_TILED, timed=True)
+        fp, bp = geom.sart_views(vol, s, beta, 0, n, flags=gpu_b200.SART_TILED, timed=True)
         out[name] = {"fp_ms_per_view": fp / n, "bp_ms_per_view": bp / n}
         del vol
     del truth
     if args.profile_iteration:
-        solver = gpu_b200.Solver(geom, gpu_b200.F16, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS)
+        solver = gpu_b200.Solver(geom, gpu_b200.F16, beta=beta, lambda_tv=lam, fgp_iters=FGP_ITERS)
         solver.set_sinogram(sino16)
         solver.set_volume(None)
         t0 = time.perf_counter()
@@ -278,7 +286,7 @@ def profile_views(args):
         out["iteration_s"] = time.perf_counter() - t1
         out["first_iteration_s"] = t1 - t0
         solver.close()
-    print(json.dumps({"profile_views": n, **out}), flush=True)
+    print(json.dumps({"profile_views": n, "workload": "tbct" if tbct else "scan512", **out}), flush=True)
 
 
 def batched_scans(n, seed=4):
@@ -476,6 +484,211 @@ def run_large(args):
     print(json.dumps(line), flush=True)
 
 
+# The tetrahedron-beam program's own configuration (T42/main_recon.cu:41-120)
+# in millimetres: 512^3 voxels of 0.1 mm, 64 sources stacked along z, each
+# with a band of 16 detector rows x 1024 columns of 0.12 mm, DSO 200 mm,
+# DOD -200 mm, 360 views 1 degree apart; relaxation 2/Lip_con = 2/32 and
+# lambda_TV = 0 (SART + FISTA, no TV prox), the objective every iteration.
+TBCT_SCAN = dict(nx=512, ny=512, nz=512, vx=0.1, nu=1024, nv=16, n_sources=64, du=0.12, dso=200.0, dod=-200.0,
+                 n_views=360, us_rate=1.0)
+TBCT_BETA = 2.0 / 32.0
+
+
+def tbct_geometry(seed):
+    """The tetrahedron-beam geometry on the current device and its phantom:
+    the 512^3 scan's ellipsoids scaled to the 51.2 mm volume (attenuation
+    scaled up alike)."""
+    import gpu_b200
+    T = TBCT_SCAN
+    desc = gpu_b200.make_desc(T["nx"], T["ny"], T["nz"], T["vx"], T["nu"], T["nv"], T["du"], T["dso"], T["dod"],
+                              T["n_views"], us_rate=T["us_rate"], ct_style=3, n_sources=T["n_sources"])
+    ph = phantom_params(2024 + seed)
+    ph[:, 0:6] *= 0.2
+    ph[:, 9] *= 5.0
+    return gpu_b200.Geometry(desc), ph
+
+
+def tbct_desc_oracle():
+    from oracle import ctoracle
+    T = TBCT_SCAN
+    return ctoracle.make_desc(T["nx"], T["ny"], T["nz"], T["nu"], T["nv"], T["n_views"], T["vx"], T["du"], T["dso"],
+                              T["dod"], us_rate=T["us_rate"], ct_style=3, n_sources=T["n_sources"])
+
+
+def cpu_baseline_tbct(budget_s=20.0):
+    """The tetrahedron-beam program's kernels compiled for the CPU
+    (oracle/_ref/libctref_tbct.so) on this host's cores, on a bounded sample
+    of one iteration scaled to a full one: S views of the SART pass (forward
+    projection of all 64 sources' rays, backprojection, update) and of the
+    objective's forward projection (x 360/S).  The FISTA step and the norms
+    are host loops over the volume and are left out (a few hundred ms)."""
+    import numpy as np
+
+    from oracle import ctoracle
+    ref = ctoracle.RefOracle(tbct_desc_oracle())
+    nviews = TBCT_SCAN["n_views"]
+    rng = np.random.default_rng(0)
+    vol = rng.uniform(0.0, 0.02, ref.vol_shape).astype(np.float32)
+    b_view = rng.uniform(0.0, 1.0, ref.view_shape).astype(np.float32)
+    ref._set()
+
+    def sart_view(j):
+        s, c = ref.trig(j)
+        corr = np.zeros(ref.view_shape, np.float32)
+        ref.lib.ref_forward_view(vol, corr, b_view.ctypes.data, s, c, 1)
+        ref.lib.ref_backproject_view(vol, corr, TBCT_BETA, s, c, 1)
+
+    # the first sampled view also sizes the sample to the budget
+    t0 = time.perf_counter()
+    sart_view(nviews // 2)
+    t_one = time.perf_counter() - t0
+    s_views = max(1, min(16, int(0.8 * budget_s / max(t_one, 1e-3))))
+    views = [nviews // 2] + [int((q + 0.5) * nviews / s_views) for q in range(1, s_views)]
+    t0 = time.perf_counter()
+    for j in views[1:]:
+        sart_view(j)
+    t_sart = (time.perf_counter() - t0 + t_one) / len(views) * nviews
+    t0 = time.perf_counter()
+    for j in views:
+        s, c = ref.trig(j)
+        fp = np.zeros(ref.view_shape, np.float32)
+        ref.lib.ref_forward_view(vol, fp, None, s, c, 0)
+    t_obj = (time.perf_counter() - t0) / len(views) * nviews
+    t_iter = t_sart + t_obj
+    cores = os.cpu_count()
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    return {
+        "value": 1.0 / t_iter, "unit": "iter/s", "cores": cores, "kind": "reference",
+        "sample": (f"the tetrahedron-beam program's kernels compiled for the CPU (OpenMP, {cores} threads): SART on "
+                   f"{len(views)} of {nviews} views and the objective forward projection on the same views (scaled "
+                   f"x{nviews}/{len(views)}); 512^3 volume, 64 sources x 16 x 1024 detector"),
+        "seconds_per_iter": t_iter, "parts_s": {"sart": t_sart, "objective_fp": t_obj},
+    }
+
+
+def run_tbct(args):
+    """The tetrahedron-beam scan: SART + FISTA iterations/s (FP32 and FP16
+    storage) with the objective, end to end with host buffers, the SART
+    update kernel against the HBM roofline, and the CPU reference beside it."""
+    import torch
+
+    import gpu_b200
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    T = TBCT_SCAN
+    geom, ph = tbct_geometry(rank)
+    vshape, sshape = geom.vol_shape, (T["n_views"],) + geom.view_shape
+    V = T["nx"] * T["ny"] * T["nz"]
+    P = geom.view_shape[0] * geom.view_shape[1]
+    truth = torch.zeros(vshape, device=dev)
+    geom.phantom_voxelize(ph, truth)
+    sino32 = torch.zeros(sshape, device=dev)
+    geom.forward(truth, sino32)
+    gen = torch.Generator(device=dev).manual_seed(77 + rank)
+    sino32 += 0.005 * sino32.max() * torch.randn(sshape, device=dev, generator=gen)
+    del truth
+    stream = torch.cuda.current_stream()
+    runs, tuned = {}, {}
+    for mode, vdt, sdt in (("f32", gpu_b200.F32, torch.float32), ("f16", gpu_b200.F16, torch.float16)):
+        tuned[mode] = geom.autotune(vdt, n_views=4)
+        sino = sino32 if sdt == torch.float32 else sino32.to(sdt)
+        solver = gpu_b200.Solver(geom, vdt, beta=TBCT_BETA, lambda_tv=0.0, fgp_iters=0, fista=True,
+                                 objective=True, use_graph=True)
+        solver.set_sinogram(sino)
+        solver.set_volume(None)
+        solver.iterate(args.warmup)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        objs = solver.iterate(args.steps).tolist()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        runs[mode] = {"ms": e0.elapsed_time(e1) / args.steps, "clocks": clocks.stop(), "objective_last": objs[-1],
+                      "solver": solver, "sino": sino}
+
+    # end to end with host buffers (FP16 storage): sinogram in, one iteration,
+    # volume out, every step; the objectives read at the end
+    geom.set_shapes(tuned["f16"]["fp_shape"], tuned["f16"]["bp_shape"])
+    solver, sino = runs["f16"]["solver"], runs["f16"]["sino"]
+    h_sino = sino.cpu().pin_memory()
+    h_vol = torch.empty(vshape, dtype=torch.float16).pin_memory()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    k0 = solver.iteration
+    for _ in range(args.steps):
+        sino.copy_(h_sino, non_blocking=True)
+        solver.iterate(1, objectives=False)
+        solver.get_volume(h_vol)
+    solver.objectives(k0 + 1, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    h2d = h_sino.numel() * h_sino.element_size()
+    d2h = h_vol.numel() * h_vol.element_size() + 3 * 8
+
+    # per-kernel times of the SART projectors (32 views spread over the scan)
+    kern = {}
+    for mode in ("f32", "f16"):
+        geom.set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
+        vol = torch.zeros(vshape, device=dev, dtype=torch.float32 if mode == "f32" else torch.float16)
+        geom.sart_views(vol, runs[mode]["sino"], TBCT_BETA, 0, 4, flags=gpu_b200.SART_TILED)
+        fp_t = bp_t = 0.0
+        nt = 32
+        for j in range(nt):
+            f_ms, b_ms = geom.sart_views(vol, runs[mode]["sino"], TBCT_BETA, (j * 97) % T["n_views"], 1,
+                                         flags=gpu_b200.SART_TILED, timed=True)
+            fp_t += f_ms
+            bp_t += b_ms
+        kern[mode] = {"fp_ms": fp_t / nt, "bp_ms": bp_t / nt}
+        del vol
+    for m in runs.values():
+        m["solver"].close()
+
+    peak, peak_kind = measured_peak_hbm()
+    bp_bytes = 2 * V * 2 + 8 * P            # SART update of one view, FP16 volume: volume in + out, float2 rays in
+    achieved = bp_bytes / (kern["f16"]["bp_ms"] * 1e-3) / 1e9
+    value = 1000.0 / runs["f16"]["ms"]
+    line = {
+        "metric": "TBCT SART-FISTA iter/s & voxel-updates/s, 512^3 x 360 views x 64 sources, FP16 vs FP32, 1 B200",
+        "value": value, "unit": "iter/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": runs["f16"]["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f16 storage, f32 arithmetic", "data": "synthetic",
+        "config": {"workload": "tetrahedron-beam SART+FISTA iteration with objective (lambda_TV 0), 512^3 x 0.1 mm, "
+                               "360 views, 64 sources x 16 rows x 1024 columns x 0.12 mm, DSO 200 mm, DOD -200 mm",
+                   "phantom": "40 ellipsoids + 200 spheres (seeded, scaled to the volume), Siddon projections "
+                              "+ 0.5% noise", "l2": "inputs > L2 (1.5 GB sinogram)"},
+        "voxel_updates_per_s": value * V * T["n_views"],
+        "f32": {"iter_per_s": 1000.0 / runs["f32"]["ms"], "ms_per_step": runs["f32"]["ms"],
+                "voxel_updates_per_s": 1000.0 / runs["f32"]["ms"] * V * T["n_views"]},
+        "f16_over_f32": runs["f32"]["ms"] / runs["f16"]["ms"],
+        "objective_last": {m: runs[m]["objective_last"] for m in runs},
+        "e2e": {"value": 1000.0 / e2e_ms, "unit": "iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": "k_sart_walk, tetrahedron beam (SART update, f16 volume, tiled)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": bp_bytes,
+                     "launch_ms": kern["f16"]["bp_ms"]},
+        "kernels_ms": kern, "launch_shapes": tuned, "clocks": runs["f16"]["clocks"],
+        "clocks_f32": runs["f32"]["clocks"],
+        # per step: tile, FP + BP per view, untile, FISTA momentum; objectives fused as in the 512^3 scan
+        "gpu_launches": (2 + 2 * T["n_views"] + 1) * args.steps + 5 * (args.steps - 1) + 6,
+    }
+    if not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline_tbct()
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            line["cpu_baseline_parts_s"] = cb["parts_s"]
+        except Exception as e:  # the CPU leg must not hide the GPU result
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -486,6 +699,8 @@ def main():
         return run_batched(args)
     if args.workload == "large":
         return run_large(args)
+    if args.workload == "tbct":
+        return run_tbct(args)
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -639,7 +854,7 @@ def main():
 
     peak, peak_kind = measured_peak_hbm()
     s_v = 2  # mixed storage bytes
-    bp_bytes = 2 * V * s_v + 4 * P            # BP with SART update, per view (algorithmic)
+    bp_bytes = 2 * V * s_v + 8 * P            # BP with SART update, per view: volume in + out, float2 rays in
     bp_ms = kern["mixed"]["bp_ms"]
     achieved = bp_bytes / (bp_ms * 1e-3) / 1e9
     traffic = profiled_traffic()

@@ -351,6 +351,12 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         const float cyr = fa(g.by, fm(g.vy, fa(0.5f, (float)j)));
         tden = fs(fa(fm(cxr, c), fm(cyr, s)), g.dod);
     }
+    // TB: the range [s0, s1] of sources kept for the current voxel.  Both
+    // bounds only grow with k (source_lower and source_upper grow with the
+    // voxel's height), so after an estimate at the first voxel each voxel
+    // settles them with a comparison or two.
+    int s0 = 0, s1 = -1;
+    bool s_est = TB;
     // voxel and z-cell row addresses advance by a constant per z step
     const long long vstep = TL ? 64LL * g.Mt * g.Nt : MN;
     VT* pv = vol + (TL ? (long long)tile_index(g, i, j, kb) : (long long)kb * MN + (long long)j * g.M + i);
@@ -433,12 +439,17 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
             const float lower = fa(fdv(fm(fs(fs(czr, g.vz), g.zmax), g.dsod), tden), g.zmax);
             auto zsrc = [&](int q) { return fa(g.zsrc0, fm((float)q, g.zsrc_dz)); };
             // the source heights increase with the index (zsrc_dz > 0), so the
-            // kept sources are one range [s0, s1]: estimated by division, then
-            // settled by T42's own comparisons
-            int s0 = 0, s1 = g.nsrc - 1;
-            if (g.nsrc > 1) {
-                s0 = (int)fminf(fmaxf(ceilf(fdv(fs(lower, g.zsrc0), g.zsrc_dz)), 0.f), (float)g.nsrc);
-                s1 = (int)fminf(fmaxf(floorf(fdv(fs(upper, g.zsrc0), g.zsrc_dz)), -1.f), (float)(g.nsrc - 1));
+            // kept sources are one range [s0, s1]: estimated by division at the
+            // first voxel, then settled by T42's own comparisons
+            if (s_est) {
+                s_est = false;
+                s0 = 0;
+                s1 = g.nsrc - 1;
+                if (g.nsrc > 1) {
+                    s0 = (int)fminf(fmaxf(ceilf(__fdividef(fs(lower, g.zsrc0), g.zsrc_dz)), 0.f), (float)g.nsrc);
+                    s1 = (int)fminf(fmaxf(floorf(__fdividef(fs(upper, g.zsrc0), g.zsrc_dz)), -1.f),
+                                    (float)(g.nsrc - 1));
+                }
             }
             while (s0 > 0 && !(zsrc(s0 - 1) < lower)) --s0;
             while (s0 < g.nsrc && zsrc(s0) < lower) ++s0;
