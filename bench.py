@@ -141,13 +141,29 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """Per-launch DRAM bytes of the backprojector from the committed ncu summary."""
+def profiled_traffic(name="roofline_traffic.json"):
+    """Per-launch DRAM bytes and warp instructions of the backprojector from
+    the committed ncu summary."""
     try:
-        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
             return json.load(f)
     except (OSError, ValueError):
         return None
+
+
+def issue_roofline(traffic, launch_ms, sm_mhz, dev):
+    """The bound that applies to the projectors: warp instructions issued per
+    second (the launch's instruction count from the ncu capture over its live
+    CUDA-event duration) against the issue peak, one warp instruction per
+    cycle on each of the 4 schedulers of every SM at the sampled SM clock."""
+    import torch
+    if not traffic or "warp_instructions_per_launch" not in traffic or not sm_mhz:
+        return None
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    achieved = traffic["warp_instructions_per_launch"] / (launch_ms * 1e-3) / 1e9
+    peak = sms * 4 * sm_mhz * 1e6 / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "G warp-instructions/s", "frac": achieved / peak,
+            "instructions_per_launch": traffic["warp_instructions_per_launch"], "sms": sms, "sm_mhz": sm_mhz}
 
 
 def cpu_baseline(steps_hint=1, budget_s=12.0):
@@ -654,6 +670,7 @@ def run_tbct(args):
     peak, peak_kind = measured_peak_hbm()
     bp_bytes = 2 * V * 2 + 8 * P            # SART update of one view, FP16 volume: volume in + out, float2 rays in
     achieved = bp_bytes / (kern["f16"]["bp_ms"] * 1e-3) / 1e9
+    traffic = profiled_traffic("roofline_traffic_tbct.json")
     value = 1000.0 / runs["f16"]["ms"]
     line = {
         "metric": "TBCT SART-FISTA iter/s & voxel-updates/s, 512^3 x 360 views x 64 sources, FP16 vs FP32, 1 B200",
@@ -672,8 +689,9 @@ def run_tbct(args):
         "e2e": {"value": 1000.0 / e2e_ms, "unit": "iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": "k_sart_walk, tetrahedron beam (SART update, f16 volume, tiled)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": bp_bytes,
-                     "launch_ms": kern["f16"]["bp_ms"]},
+                     "peak_kind": peak_kind, "traffic": (traffic or {}).get("bytes_per_launch"),
+                     "algorithmic_bytes_per_launch": bp_bytes, "launch_ms": kern["f16"]["bp_ms"],
+                     "issue": issue_roofline(traffic, kern["f16"]["bp_ms"], runs["f16"]["clocks"]["sm_mhz"], dev)},
         "kernels_ms": kern, "launch_shapes": tuned, "clocks": runs["f16"]["clocks"],
         "clocks_f32": runs["f32"]["clocks"],
         # per step: tile, FP + BP per view, untile, FISTA momentum; objectives fused as in the 512^3 scan
@@ -894,7 +912,8 @@ def main():
                          "peak_kind": peak_kind,
                          "traffic": (traffic or {}).get("bytes_per_launch"),
                          "algorithmic_bytes_per_launch": bp_bytes,
-                         "launch_ms": bp_ms},
+                         "launch_ms": bp_ms,
+                         "issue": issue_roofline(traffic, bp_ms, runs["mixed"]["clocks"]["sm_mhz"], dev)},
             "kernels_ms": kern,
             "launch_shapes": tuned,
             "clocks": runs["mixed"]["clocks"],
