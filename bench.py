@@ -59,6 +59,34 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+# Replicas: every rank reconstructs its own scan (seeded by its rank); the
+# only collectives are the barriers around the timed regions and the maximum
+# of the per-rank times.  NCCL on the GPUs; the same calls run over gloo on
+# the CPU in the tests.
+def init_replicas(world, backend="nccl", timeout_s=600):
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+
+
+def max_over_ranks(x, world, device):
+    """The largest of the ranks' values of x (a time in ms): the job's time."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(ms_max, world):
+    """Whole-job iterations/s: every rank completes one iteration per step,
+    the job's step time is the slowest rank's."""
+    return world * 1000.0 / ms_max
+
+
 def phantom_params(seed=2024):
     """40 ellipsoids (semi-axes 3-100 mm, 0.005-0.04 /mm) + 200 spheres (r 1-3 mm, 0.05 /mm)."""
     import numpy as np
@@ -726,9 +754,7 @@ def main():
     import gpu_b200
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    init_replicas(world, "nccl")
     dev = torch.device("cuda", local)
     desc = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
                               SCAN["dso"], SCAN["dod"], SCAN["n_views"])
@@ -753,12 +779,8 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def job_ms(x):
+        return max_over_ranks(x, world, dev)
 
     runs = {}
     stream = torch.cuda.current_stream()
@@ -782,7 +804,7 @@ def main():
         e1.record(stream)
         barrier()
         ms = e0.elapsed_time(e1) / args.steps
-        runs[mode] = {"ms": max_over_ranks(ms), "clocks": clocks.stop(), "objective_last": objs[-1]}
+        runs[mode] = {"ms": job_ms(ms), "clocks": clocks.stop(), "objective_last": objs[-1]}
         runs[mode]["solver"] = solver
         runs[mode]["sino"] = sino
 
@@ -807,7 +829,7 @@ def main():
     e2e_objs = solver.objectives(k0 + 1, args.steps)
     e1.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    e2e_ms = job_ms(e0.elapsed_time(e1) / args.steps)
     h2d = h_sino.numel() * h_sino.element_size()
     d2h = h_vol.numel() * h_vol.element_size() + 3 * 8
 
@@ -843,7 +865,7 @@ def main():
     noobj.iterate(args.steps)
     e1.record(stream)
     barrier()
-    noobj_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    noobj_ms = job_ms(e0.elapsed_time(e1) / args.steps)
     noobj.close()
 
     # ray-voxel intersections of one pass over all views (Siddon segments of
@@ -867,7 +889,7 @@ def main():
     geom.fdk(sino32, zero)
     e1.record(stream)
     barrier()
-    fdk_ms = max_over_ranks(e0.elapsed_time(e1))
+    fdk_ms = job_ms(e0.elapsed_time(e1))
     del zero
 
     peak, peak_kind = measured_peak_hbm()
@@ -881,7 +903,7 @@ def main():
     if rank == 0:
         ms_mixed = runs["mixed"]["ms"]
         ms_f32 = runs["f32"]["ms"]
-        value = world * 1000.0 / ms_mixed
+        value = job_rate(ms_mixed, world)
         # every step: SART (tile, FP + BP per view, untile), FGP (2 per inner
         # step + final); objective of steps 1..K-1 fused into the next SART pass (tile
         # x, TV + reduce, 2-level reduce of the partials); of step K separate
@@ -901,11 +923,11 @@ def main():
             "ray_voxel_intersections_per_pass": segs_per_pass,
             "ms_per_step_without_objective": noobj_ms,
             "fdk_ms": fdk_ms,
-            "f32": {"iter_per_s": world * 1000.0 / ms_f32, "ms_per_step": ms_f32,
-                    "voxel_updates_per_s": world * 1000.0 / ms_f32 * V * SCAN["n_views"]},
+            "f32": {"iter_per_s": job_rate(ms_f32, world), "ms_per_step": ms_f32,
+                    "voxel_updates_per_s": job_rate(ms_f32, world) * V * SCAN["n_views"]},
             "mixed_over_f32": ms_f32 / ms_mixed,
             "objective_last": {"f32": runs["f32"]["objective_last"], "mixed": runs["mixed"]["objective_last"]},
-            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "iter/s", "h2d_bytes_per_step": h2d,
+            "e2e": {"value": job_rate(e2e_ms, world), "unit": "iter/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": "k_sart_walk (SART update, f16 volume, tiled layout)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
