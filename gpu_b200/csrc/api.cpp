@@ -368,6 +368,19 @@ extern "C" ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float
     return launch_fdk(*GE(geom), sino, vol, S(stream));
 }
 
+extern "C" ctr_status ctr_fdk_backproject(const ctr_geometry* geom, const float* filtered, int v0, int n, float* vol,
+                                          void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(filtered, "filtered"));
+    CTR_TRY(need(vol, "vol"));
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, v0, n));
+    if (g->dg.ct_style != 0) return set_error(CTR_ERR_UNSUPPORTED, "FDK is for the cone-beam geometry");
+    return launch_fdk_bp(*g, filtered, v0, n, vol, S(stream));
+}
+
 // -------------------------------------------------------------- dot product
 
 extern "C" ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, const float* y, int v0, int n,

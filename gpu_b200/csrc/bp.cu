@@ -675,7 +675,8 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
             }
         } else if (a.flags & CTR_BP_FOV_MASK) {
             if (g.ct_style == 3)
-                return set_error(CTR_ERR_UNSUPPORTED, "CTR_BP_FOV_MASK: the tetrahedron-beam backprojector has no command 0");
+                return set_error(CTR_ERR_UNSUPPORTED, "CTR_BP_FOV_MASK (command 0): not defined for the tetrahedron "
+                                                      "beam, whose backprojector has no command argument");
             for (int w = 0; w < a.nview; ++w)
                 k_backproject<VT, AdjRay, false, false><<<grid, BP_THREADS, smem, st>>>(
                     g, (VT*)a.vol, (const AdjRay*)a.rays + (size_t)w * G.npix(), a.view0 + w, (acc || w > 0) ? 1 : 0,

@@ -44,6 +44,7 @@ struct DevGeom {
     float m_off;            // (float)M_Offset
     float fdk_ang;          // us_rate*PI/180.0f        (V63/FDK/kernel_FDK.cu:117)
     float fdk_usn;          // us_rate*Nviews in float  (same line)
+    int fdk_full;           // fdk_usn == 360: the FP64 factor 360.0/fdk_usn is exactly 1
     const float* px;        // plane coordinates vx*n+bx for n = -1..M+1 at px[n+1]
     const float* py;
     const float* pz;
@@ -181,6 +182,8 @@ ctr_status launch_momentum(const Geometry& g, void* y, void* xprev, const void* 
 ctr_status launch_convert(const void* src, ctr_dtype sdt, void* dst, ctr_dtype ddt, long long n,
                           cudaStream_t st);
 ctr_status launch_fdk(Geometry& g, const float* sino, float* vol, cudaStream_t st);
+// the backprojection stage: vol += views [view0, view0+nview) of the filtered sinogram (fsino[0] = view0)
+ctr_status launch_fdk_bp(const Geometry& g, const float* fsino, int view0, int nview, float* vol, cudaStream_t st);
 ctr_status launch_phantom(const Geometry& g, const double* dparams, int n, float* vol,
                           cudaStream_t st);
 

@@ -146,7 +146,10 @@ k_fdk_bp(const DevGeom g, float* __restrict__ vol, const float* __restrict__ pro
             }
             // vol += temp1*temp2*(us_rate*PI/180.0f)*360.0/(us_rate*Nviews)  (float*float*float, then double)
             const float fprod = fm(fm(temp1, temp2), g.fdk_ang);
-            const double dv = __ddiv_rn(__dmul_rn((double)fprod, 360.0), (double)g.fdk_usn);
+            // a full circle (us_rate*Nviews == 360): (double)fprod*360.0 is exact (24 + 6
+            // significant bits) and dividing it by 360 gives fprod back, exactly
+            const double dv = g.fdk_full ? (double)fprod
+                                         : __ddiv_rn(__dmul_rn((double)fprod, 360.0), (double)g.fdk_usn);
             acc[kk] = (float)__dadd_rn((double)acc[kk], dv);
         }
     }
@@ -214,10 +217,18 @@ ctr_status launch_fdk(Geometry& G, const float* sino, float* vol, cudaStream_t s
         dim3 grd((g.R + RP_COLS - 1) / RP_COLS, (unsigned)((cnt + RP_ROWS - 1) / RP_ROWS));
         k_ramp<<<grd, 128, 0, st>>>(wsino + r0 * g.R, fsino + r0 * g.R, G.d_ramp, g.R, cnt);
     }
+    CTR_CUDA_TRY(cudaGetLastError());
+    return launch_fdk_bp(G, fsino, 0, nv, vol, st);
+}
+
+ctr_status launch_fdk_bp(const Geometry& G, const float* fsino, int view0, int nview, float* vol, cudaStream_t st)
+{
+    const DevGeom& g = G.dg;
+    const long long P = G.npix();
     dim3 grd((g.M + FB_BX - 1) / FB_BX, (g.N + FB_BY - 1) / FB_BY, (g.Z + FB_K - 1) / FB_K);
     const int VB = 32;
-    for (int v0 = 0; v0 < nv; v0 += VB)
-        k_fdk_bp<<<grd, FB_BX * FB_BY, 0, st>>>(g, vol, fsino + (size_t)P * v0, v0, std::min(VB, nv - v0));
+    for (int w = 0; w < nview; w += VB)
+        k_fdk_bp<<<grd, FB_BX * FB_BY, 0, st>>>(g, vol, fsino + (size_t)P * w, view0 + w, std::min(VB, nview - w));
     CTR_CUDA_TRY(cudaGetLastError());
     return CTR_OK;
 }

@@ -244,6 +244,7 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     q.m_off = (float)d.m_offset;
     q.fdk_ang = d.us_rate * kPi / 180.0f;
     q.fdk_usn = d.us_rate * (float)d.n_views;
+    q.fdk_full = q.fdk_usn == 360.0f ? 1 : 0;
 
     // plane tables: px[n+1] = volumn_x*n + boundary_voxel_x, n = -1..M+1
     g->h_px.resize(d.nx + 3);

@@ -42,7 +42,7 @@ SART_TILED = 0x2
 EXPORTED = [
     "ctr_geometry_create", "ctr_geometry_destroy", "ctr_geometry_view_trig", "ctr_forward",
     "ctr_backproject", "ctr_sart_pass", "ctr_sart_views", "ctr_sart_views_noalloc", "ctr_forward_trace", "ctr_fgp_tv", "ctr_fista_momentum",
-    "ctr_objective", "ctr_tv_norm", "ctr_l2_norm", "ctr_fdk", "ctr_dot_test", "ctr_solver_create",
+    "ctr_objective", "ctr_tv_norm", "ctr_l2_norm", "ctr_fdk", "ctr_fdk_backproject", "ctr_dot_test", "ctr_solver_create",
     "ctr_solver_destroy", "ctr_solver_set_sinogram", "ctr_solver_set_volume", "ctr_solver_iterate",
     "ctr_solver_get_volume", "ctr_solver_iteration_count", "ctr_solver_save", "ctr_solver_load",
     "ctr_last_error_string", "ctr_convert", "ctr_phantom_voxelize", "ctr_set_default_geometry",
@@ -112,6 +112,7 @@ def load_library(path: str = LIB_PATH):
         "ctr_tv_norm": ([G, vp, i, C.POINTER(d), vp], i),
         "ctr_l2_norm": ([vp, vp, C.c_int64, C.POINTER(d), vp], i),
         "ctr_fdk": ([G, vp, vp, vp], i),
+        "ctr_fdk_backproject": ([G, vp, i, i, vp, vp], i),
         "ctr_dot_test": ([G, vp, vp, i, i, C.POINTER(d), C.POINTER(d), vp], i),
         "ctr_solver_create": ([G, i, C.POINTER(SolverParams), C.POINTER(C.c_void_p)], i),
         "ctr_solver_destroy": ([vp], i),
@@ -310,6 +311,12 @@ class Geometry:
 
     def fdk(self, sino, vol, stream=None):
         check(self.lib.ctr_fdk(self.h, _ptr(sino), _ptr(vol), _stream(stream)))
+        return vol
+
+    def fdk_backproject(self, filtered, vol, view_begin=0, view_count=None, stream=None):
+        """vol += FDK backprojection of weighted, filtered views (FP32)."""
+        n = self.n_views - view_begin if view_count is None else view_count
+        check(self.lib.ctr_fdk_backproject(self.h, _ptr(filtered), view_begin, n, _ptr(vol), _stream(stream)))
         return vol
 
     def dot_test(self, x, y, view_begin=0, view_count=None, stream=None):

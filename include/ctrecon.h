@@ -94,7 +94,8 @@ typedef struct ctr_geometry_desc {
  * band cannot see the voxel skipped, update where the summed length exceeds
  * vx*1e-3) with the projector's chords.  Requires vz = vx and dv = du (the
  * reference's single pitches).  Not with CTR_GEOM_FAN_SLICES/PARALLEL, FDK or
- * CTR_BP_FOV_MASK (T42's backprojector has no command 0). */
+ * CTR_BP_FOV_MASK (V63's command 0; T42's backprojector has no command
+ * argument). */
 #define CTR_GEOM_TBCT 0x8u
 
 typedef struct ctr_geometry ctr_geometry;
@@ -235,6 +236,14 @@ ctr_status ctr_l2_norm(const float* a, const float* b, int64_t n, double* out, v
  * V63/FDK/kernel_FDK.cu:1-62; ramp V63/FDK/FFT_1d_GPU.h:241-287).
  * Workspace: one FP32 sinogram copy, allocated per call. */
 ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float* vol, void* stream);
+/* The backprojection stage of FDK alone: vol += the bilinear voxel-driven
+ * backprojection of the already weighted and filtered views
+ * [view_begin, view_begin+view_count) (filtered[w] is view view_begin+w,
+ * FP32), view by view in order, each view's update rounded as the
+ * reference's kernel_FDK_reconstruction (V63/FDK/kernel_FDK.cu:16-62) rounds
+ * it, the per-view launch loop of V63/host_FDK.cpp:33-50.  No workspace. */
+ctr_status ctr_fdk_backproject(const ctr_geometry* geom, const float* filtered, int view_begin, int view_count,
+                               float* vol, void* stream);
 
 /* ------------------------------------------------------------ dot product */
 

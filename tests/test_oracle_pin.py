@@ -49,7 +49,7 @@ def test_backproject_bit_exact(case):
     for a, j in enumerate(g["bp_views"]):
         np.testing.assert_array_equal(bits(o.backproject_ref(g["vol"], g["corr"][a], int(j), 0.8, 1)), bits(g["bp1"][a]))
         if cfg.get("ct_style", 0) == 3:
-            continue   # the tetrahedron-beam backprojector has no command 0
+            continue   # the tetrahedron-beam backprojector has no command argument
         z = np.zeros_like(g["vol"])
         np.testing.assert_array_equal(bits(o.backproject_ref(z, g["corr"][a], int(j), 1.0, 0)), bits(g["bp0"][a]))
 
