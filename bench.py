@@ -42,6 +42,9 @@ def parse():
                    help="profiling mode: set up the scan, run a SART update of this many views, print timings, exit")
     p.add_argument("--profile-iteration", action="store_true",
                    help="with --profile-views: also run two FP16 solver iterations (the second in steady state)")
+    p.add_argument("--profile-fdk", type=int, default=0,
+                   help="profiling mode: FDK of the 512^3 scan restricted to this many views (weighting, ramp "
+                        "and backprojection), print timings, exit")
     p.add_argument("--profile-tune", action="store_true",
                    help="with --profile-views: also print the tuner's time for every launch shape")
     p.add_argument("--workload", choices=["scan512", "batched", "large", "tbct"], default="scan512",
@@ -280,6 +283,40 @@ def run_reference(args):
         "voxel_updates_per_s": value * SCAN["nx"] * SCAN["ny"] * SCAN["nz"] * SCAN["n_views"],
     }
     print(json.dumps(line), flush=True)
+
+
+def profile_fdk(args):
+    """A short run for ncu: FDK on the 512^3 scan's geometry restricted to the
+    first --profile-fdk views of its 1024 (same angles, the full-circle
+    scale factor): cosine weight + ramp of those views through ctr_fdk on a
+    geometry of that many views, and the backprojection of the filtered
+    views through ctr_fdk_backproject on the 1024-view geometry, twice."""
+    import torch
+
+    import gpu_b200
+    n = args.profile_fdk
+    S = SCAN
+    geom = gpu_b200.Geometry(gpu_b200.make_desc(S["nx"], S["ny"], S["nz"], S["vx"], S["nu"], S["nv"], S["du"],
+                                                S["dso"], S["dod"], S["n_views"]))
+    small = gpu_b200.Geometry(gpu_b200.make_desc(S["nx"], S["ny"], S["nz"], S["vx"], S["nu"], S["nv"], S["du"],
+                                                 S["dso"], S["dod"], n, us_rate=360.0 / S["n_views"]))
+    truth = torch.zeros(geom.vol_shape, device="cuda")
+    geom.phantom_voxelize(phantom_params(2024), truth)
+    sino = torch.zeros((n,) + geom.view_shape, device="cuda")
+    geom.forward(truth, sino, 0, n)
+    vol = torch.zeros(geom.vol_shape, device="cuda")
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    small.fdk(sino, vol)                            # weighting, ramp, backprojection of n views
+    e[1].record()
+    filt = sino.clone()                             # any FP32 views serve for timing the backprojection
+    e[2].record()
+    geom.fdk_backproject(filt, vol, 0, n)
+    geom.fdk_backproject(filt, vol, 0, n)
+    e[3].record()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_fdk": n, "fdk_small_ms": e[0].elapsed_time(e[1]),
+                      "backprojection_ms_per_view": e[2].elapsed_time(e[3]) / (2 * n)}), flush=True)
 
 
 def profile_views(args):
@@ -741,6 +778,8 @@ def main():
         return run_reference(args)
     if args.profile_views:
         return profile_views(args)
+    if args.profile_fdk:
+        return profile_fdk(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "large":

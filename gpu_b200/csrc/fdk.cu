@@ -94,6 +94,24 @@ k_ramp(const float* __restrict__ in, float* __restrict__ out, const float* __res
 }
 
 static constexpr int FB_BX = 32, FB_BY = 4, FB_K = 4;
+
+// floor(x) and (int)floor(x) for 0 <= x < 2^22 without conversion
+// instructions (the backprojection is bound by the pipe that executes them):
+// adding 1.5*2^23 rounds x to an integer m held in the low mantissa bits, and
+// m - 1 when m > x.  Both results are exact, so they equal the reference's
+// an = floor(ksi) and (float)an.
+__device__ __forceinline__ float floor_small(float x, int& n)
+{
+    const float C = 12582912.0f;   // 1.5 * 2^23
+    const float t = __fadd_rn(x, C);
+    float r = __fsub_rn(t, C);
+    n = __float_as_int(t) - 0x4B400000;
+    if (r > x) {
+        r = __fsub_rn(r, 1.0f);
+        n -= 1;
+    }
+    return r;
+}
 __global__ void __launch_bounds__(FB_BX * FB_BY)
 k_fdk_bp(const DevGeom g, float* __restrict__ vol, const float* __restrict__ proj, int view0, int nview)
 {
@@ -130,10 +148,9 @@ k_fdk_bp(const DevGeom g, float* __restrict__ vol, const float* __restrict__ pro
             ksi = fdv(fs(fdv(fm(ksi, fs(DSO, DOD)), DSO), g.zmin), g.dv);
             float temp2;
             if ((0 <= ksi) && (fa(ksi, 1.0f) < (float)ZP) && (0 <= p) && (fa(p, 1.0f) < (float)R)) {
-                const int an = (int)floorf(ksi);
-                const float an0 = fs(ksi, (float)an);
-                const int bn = (int)floorf(p);
-                const float bn0 = fs(p, (float)bn);
+                int an, bn;
+                const float an0 = fs(ksi, floor_small(ksi, an));   // ksi - an, an = floor(ksi)
+                const float bn0 = fs(p, floor_small(p, bn));
                 const float* q0 = pv + (long long)R * an + bn;
                 const float* q1 = q0 + R;
                 const float t00 = fm(fm(fs(1.0f, an0), fs(1.0f, bn0)), __ldg(q0));
@@ -146,11 +163,17 @@ k_fdk_bp(const DevGeom g, float* __restrict__ vol, const float* __restrict__ pro
             }
             // vol += temp1*temp2*(us_rate*PI/180.0f)*360.0/(us_rate*Nviews)  (float*float*float, then double)
             const float fprod = fm(fm(temp1, temp2), g.fdk_ang);
-            // a full circle (us_rate*Nviews == 360): (double)fprod*360.0 is exact (24 + 6
-            // significant bits) and dividing it by 360 gives fprod back, exactly
-            const double dv = g.fdk_full ? (double)fprod
-                                         : __ddiv_rn(__dmul_rn((double)fprod, 360.0), (double)g.fdk_usn);
-            acc[kk] = (float)__dadd_rn((double)acc[kk], dv);
+            if (g.fdk_full) {
+                // a full circle (us_rate*Nviews == 360): (double)fprod*360.0 is exact
+                // (24 + 6 significant bits) and dividing it by 360 gives fprod back; and
+                // the FP64 sum of two floats rounded to float is their float sum (when
+                // the FP64 sum is inexact the smaller term is below 2^-28 of the larger,
+                // far under half a float ulp), so the update is one float add
+                acc[kk] = fa(acc[kk], fprod);
+            } else {
+                const double dv = __ddiv_rn(__dmul_rn((double)fprod, 360.0), (double)g.fdk_usn);
+                acc[kk] = (float)__dadd_rn((double)acc[kk], dv);
+            }
         }
     }
 #pragma unroll
