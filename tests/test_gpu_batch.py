@@ -5,7 +5,9 @@ on the same inputs, which is itself pinned to the oracle's call sequence."""
 import numpy as np
 import pytest
 
-from scan_configs import SMALL, ctr_desc, og_desc_xyz
+from scan_configs import SMALL, TBCT, ctr_desc, og_desc_xyz
+
+SCANS = dict(SMALL, **TBCT)
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -22,8 +24,8 @@ PHANTOM = np.array([[0, 0, 0, 5, 4, 3, 0.3, 0.2, 0.1, 0.02], [1.5, -1, 0.5, 2, 2
 
 def scans(oracle_mod):
     out = []
-    for name in ["cube16", "odd", "fine", "aniso", "fine_even"]:
-        cfg = SMALL[name]
+    for name in ["cube16", "odd", "fine", "aniso", "fine_even", "tbct"]:   # a tetrahedron-beam scan among them
+        cfg = SCANS[name]
         o = oracle_mod.Oracle(og_desc_xyz(cfg))
         b = np.stack([o.forward_view(o.phantom(PHANTOM), j, 0) for j in range(cfg["nviews"])])
         out.append((cfg, torch.from_numpy(b).cuda()))
