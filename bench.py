@@ -907,6 +907,31 @@ def main():
     noobj_ms = job_ms(e0.elapsed_time(e1) / args.steps)
     noobj.close()
 
+    # the reference backprojector's arithmetic (CTR_SART_REFERENCE_BP: the
+    # SART pass equals the reference's bit for bit), FP32 as the reference
+    geom.set_shapes(tuned["f32"]["fp_shape"], tuned["f32"]["bp_shape"])
+    refbp = gpu_b200.Solver(geom, gpu_b200.F32, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
+                            objective=True, use_graph=True, sart_flags=gpu_b200.SART_REFERENCE_BP)
+    refbp.set_sinogram(runs["f32"]["sino"])
+    refbp.set_volume(None)
+    refbp.iterate(1)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    refbp.iterate(args.steps)
+    e1.record(stream)
+    barrier()
+    refbp_ms = job_ms(e0.elapsed_time(e1) / args.steps)
+    refbp.close()
+    vtmp = torch.zeros(vshape, device=dev)
+    geom.sart_views(vtmp, runs["f32"]["sino"], BETA, 0, 4, flags=gpu_b200.SART_TILED | gpu_b200.SART_REFERENCE_BP)
+    rb_bp = 0.0
+    for j in range(32):
+        _, b_ms = geom.sart_views(vtmp, runs["f32"]["sino"], BETA, (j * 97) % SCAN["n_views"], 1,
+                                     flags=gpu_b200.SART_TILED | gpu_b200.SART_REFERENCE_BP, timed=True)
+        rb_bp += b_ms
+    del vtmp
+
     # ray-voxel intersections of one pass over all views (Siddon segments of
     # every ray, counted once per geometry); an iteration visits each of them
     # three times: SART forward projection, SART backprojection, objective
@@ -961,6 +986,10 @@ def main():
             "ray_voxel_intersections_per_s": value * 3 * segs_per_pass,
             "ray_voxel_intersections_per_pass": segs_per_pass,
             "ms_per_step_without_objective": noobj_ms,
+            "reference_bp_f32": {"iter_per_s": job_rate(refbp_ms, world), "ms_per_step": refbp_ms,
+                                 "bp_ms_per_view": rb_bp / 32,
+                                 "note": "CTR_SART_REFERENCE_BP: the reference backprojector's arithmetic, "
+                                         "SART pass bit-exact with the reference"},
             "fdk_ms": fdk_ms,
             "f32": {"iter_per_s": job_rate(ms_f32, world), "ms_per_step": ms_f32,
                     "voxel_updates_per_s": job_rate(ms_f32, world) * V * SCAN["n_views"]},

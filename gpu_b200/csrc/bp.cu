@@ -649,7 +649,9 @@ ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t s
         if (a.sart) {
             if (a.nview != 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART updates one view at a time");
             const bool sr = (a.flags & CTR_SART_STOCHASTIC_ROUND) != 0;
-            if (g.ct_style == 3) {   // the tetrahedron beam: column walks only (bp_shape -1 runs walk shape 1)
+            if (a.flags & CTR_SART_REFERENCE_BP) {   // the reference backprojector's arithmetic (bp_ref.cu)
+                CTR_TRY(launch_sart_ref(G, a, st));
+            } else if (g.ct_style == 3) {   // the tetrahedron beam: column walks only (bp_shape -1 runs walk shape 1)
                 if (a.tiled) {
                     if (sr) CTR_TRY((launch_sart_walk<VT, true, true, true>(G, a, st, smem)));
                     else CTR_TRY((launch_sart_walk<VT, false, true, true>(G, a, st, smem)));

@@ -53,6 +53,7 @@ struct DevGeom {
     const float4* colt;     // [view][u] (x1x, 1/dx, x1y, 1/dy), parallel axes encoded
     const float2* rowt;     // [v] (x1z, 1/dz) of every row of a view, parallel rows encoded
     const float2* zcell;    // [k][v] (min, max) of the z alphas of cell k's planes for row v
+    const float2* zref;     // [k][v] (min, max) of the reference backprojector's z alphas (CTR_SART_REFERENCE_BP)
     unsigned int* err;      // device error bits (ERR_*)
 };
 
@@ -70,6 +71,7 @@ struct Geometry {
     void* d_tables = nullptr;  // px,py,pz,trig,trig_fdk,rowt
     float4* d_colt = nullptr;
     float2* d_zcell = nullptr;
+    float2* d_zref = nullptr;
     unsigned* d_err = nullptr;
     // workspace
     void* d_rays = nullptr;  size_t rays_cap = 0;       // ray records (float2 SART / AdjRay adjoint)
@@ -156,6 +158,9 @@ __host__ __device__ inline long long tiled_count(const DevGeom& g) { return (lon
 ctr_status launch_tiling(const Geometry& g, const void* src, void* dst, ctr_dtype dt, bool to_tiled, cudaStream_t st);
 // fills dg.zcell (view-independent: the rows' z and the source height do not turn)
 ctr_status launch_zcell(const Geometry& g, float2* zcell, cudaStream_t st);
+// the reference backprojector's z alphas per (cell, row), and its SART update (bp_ref.cu)
+ctr_status launch_zref(const Geometry& g, float2* zref, cudaStream_t st);
+ctr_status launch_sart_ref(const Geometry& g, const BpArgs& a, cudaStream_t st);
 // Matched-adjoint ray record: f = (value, chord length d12, alpha_lo, alpha_hi),
 // i = (start voxel i, j, k, parallel-axis bits).
 struct __align__(16) AdjRay {

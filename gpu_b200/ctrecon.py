@@ -37,6 +37,7 @@ GEOM_PARALLEL = 0x4
 GEOM_TBCT = 0x8
 SART_STOCHASTIC_ROUND = 0x1
 SART_TILED = 0x2
+SART_REFERENCE_BP = 0x4
 
 # every symbol include/ctrecon.h declares
 EXPORTED = [

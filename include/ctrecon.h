@@ -162,6 +162,17 @@ ctr_status ctr_backproject(const ctr_geometry* geom, const float* sino, int view
  * fewer cache lines per projector load.  The solver always does this. */
 #define CTR_SART_STOCHASTIC_ROUND 0x1u
 #define CTR_SART_TILED 0x2u
+/* CTR_SART_REFERENCE_BP: the backprojection with the reference kernel's own
+ * arithmetic (backprj_ray_driven_3d_kernel command 1,
+ * V63/kernel_IterativeRecon_universal.cu:571-810: the bounding rectangle of
+ * the voxel's corner projections, the slab alphas by division, the pixels
+ * row by row, "f += 0" where the summed length is below vx*1e-6), so that a
+ * FP32 SART pass equals the reference's bit for bit (CT_style 0, 1, 2; not
+ * the tetrahedron beam).  Default (flag clear): the gather backprojector with
+ * the forward projector's own chords, the exact transpose of the projector,
+ * which differs from the reference's alphas in rounding (and keeps the rays
+ * lying on a voxel plane that the reference's 0/0 drops). */
+#define CTR_SART_REFERENCE_BP 0x4u
 ctr_status ctr_sart_pass(const ctr_geometry* geom, void* vol, ctr_dtype vol_dtype,
                          const void* sino, ctr_dtype sino_dtype, float beta, unsigned flags,
                          uint32_t seed, void* stream);

@@ -102,3 +102,23 @@ def test_dot_product_full_size(cfg, oracle_built):
         y = torch.randn((4,) + g.view_shape, device="cuda", generator=gen)
         a, b = g.dot_test(x, y, v0, 4)
         assert abs(a - b) <= 1e-6 * max(abs(a), abs(b)), (a, b)
+
+
+def test_sart_view_reference_backprojector_full_size(oracle_built):
+    """CTR_SART_REFERENCE_BP at full size: one SART view from a non-zero volume
+    equals the reference's backprojection arithmetic (the C restatement pinned
+    to the reference's kernels) bit for bit."""
+    import gpu_b200
+    g, o, vol = scan(SCAN, oracle_built)
+    h = vol.cpu().numpy()
+    j = 701
+    b = torch.zeros((SCAN["nviews"],) + g.view_shape, device="cuda")
+    g.forward(vol * 1.05, b[j:j + 1], j, 1)
+    x = vol.clone()
+    g.sart_views(x, b, 0.8, j, 1, flags=gpu_b200.SART_REFERENCE_BP)
+    corr = o.forward_view(h, j, 1, b[j].cpu().numpy())
+    want = o.backproject_ref(h, corr, j, 0.8, 1)
+    got = x.cpu().numpy()
+    assert np.count_nonzero(got != h) > 0.05 * h.size
+    np.testing.assert_array_equal(bits(got), bits(want))
+
