@@ -55,7 +55,7 @@ ctr_status launch_zref(const Geometry& G, float2* zref, cudaStream_t st)
     return CTR_OK;
 }
 
-constexpr int REF_COLS = 8;   // rectangle columns whose x-y alphas a thread keeps in registers
+constexpr int REF_COLS = 4;   // rectangle columns whose x-y alphas a thread keeps in registers
 
 template <typename VT>
 __device__ __forceinline__ void plus_zero(VT* p)
@@ -64,7 +64,8 @@ __device__ __forceinline__ void plus_zero(VT* p)
     if (__float_as_uint(Store<VT>::ldw(p)) == 0x80000000u) Store<VT>::st(p, 0.0f);
 }
 
-template <typename VT, bool STOCH, int BY, int MINB, bool TL>
+// CONE: CT_style 0 (the source's height fixed; d12 from the ray record)
+template <typename VT, bool STOCH, int BY, int MINB, bool TL, bool CONE>
 __global__ void __launch_bounds__(32 * BY, MINB)
 k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
            uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
@@ -94,18 +95,23 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
     const float DSO = g.dso, DOD = g.dod;
 
     // corner projections (:639-678): u per corner, and the z magnification
-    float mg[4];
-    float minY = __int_as_float(0x7f800000), maxY = -minY;
+    // (t-DOD)/(DSO-t) of the corners, of which the z projections
+    // m*(pz - srcz) + pz take their extremes at the extreme m (rounding is
+    // monotone), so 4 of the 8 vertices give the rectangle's rows
+    float mlo = __int_as_float(0x7f800000), mhi = -mlo;
+    float minY = mlo, maxY = mhi;
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) {
         const float px = fs(fa(cx, fm((float)(cc & 1), g.vx)), fm(0.5f, g.vx));
         const float py = fs(fa(cy, fm((float)(cc >> 1), g.vy)), fm(0.5f, g.vy));
         const float t = fa(fm(px, c), fm(py, s));
         const float ss = fa(fm(-px, s), fm(py, c));
-        mg[cc] = fdv(fs(t, DOD), fs(DSO, t));
-        const float ou = g.ct_style == 2 ? ss : fa(fm(mg[cc], fs(ss, g.srcy)), ss);
+        const float mg = fdv(fs(t, DOD), fs(DSO, t));
+        const float ou = g.ct_style == 2 ? ss : fa(fm(mg, fs(ss, g.srcy)), ss);
         minY = fminf(minY, ou);
         maxY = fmaxf(maxY, ou);
+        mlo = fminf(mlo, mg);
+        mhi = fmaxf(mhi, mg);
     }
     int minYi = __float2int_rd(fa(fm(fs(minY, g.ymin), g.inv_du), 0.5f));   // :680-681
     int maxYi = __float2int_rd(fa(fm(fs(maxY, g.ymin), g.inv_du), 0.5f));
@@ -129,7 +135,7 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
         const float ay0 = fdv(fs(ylo, qy), fs(sy, qy)), ay1 = fdv(fs(yhi, qy), fs(sy, qy));
         lo = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
         hi = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
-        q2 = fa(fm(fs(sx, qx), fs(sx, qx)), fm(fs(sy, qy), fs(sy, qy)));
+        if (!CONE) q2 = fa(fm(fs(sx, qx), fs(sx, qx)), fm(fs(sy, qy), fs(sy, qy)));
     };
     float clo[REF_COLS], chi[REF_COLS], cq2[REF_COLS];
     unsigned live = 0;
@@ -149,19 +155,17 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
         const float cz = fa(fa(g.bz, fm(g.vz, 0.5f)), fm((float)k, g.vz));
         // detector rows of the rectangle (:655-683)
         float minZ, maxZ;
-        if (g.ct_style == 0) {
+        if (CONE) {
             minZ = __int_as_float(0x7f800000);
             maxZ = -minZ;
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk) {
                 const float pz = fs(fa(cz, fm((float)kk, g.vz)), fm(0.5f, g.vz));
                 const float dz = fs(pz, g.srcz);
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) {
-                    const float oz = fa(fm(mg[cc], dz), pz);
-                    minZ = fminf(minZ, oz);
-                    maxZ = fmaxf(maxZ, oz);
-                }
+                const float a0 = fa(fm(dz >= 0.f ? mlo : mhi, dz), pz);   // the smallest of the 4 corners
+                const float a1 = fa(fm(dz >= 0.f ? mhi : mlo, dz), pz);   // and the largest
+                minZ = fminf(minZ, a0);
+                maxZ = fmaxf(maxZ, a1);
             }
         } else {
             minZ = cz;
@@ -179,7 +183,7 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
                 const float dl = fs(amax, amin);
                 if (dl > 0.f) {                                              // :780
                     // cone beam: the projector's d12; fan slices / parallel beam: source at the voxel's height
-                    const float d12 = g.ct_style == 0 ? rec.y : __fsqrt_rn(fa(q2, fm(qzd, qzd)));
+                    const float d12 = CONE ? rec.y : __fsqrt_rn(fa(q2, fm(qzd, qzd)));
                     const float temp = fm(d12, dl);
                     if (temp > g.thr_bp) {                                   // :785-791
                         sw = fa(sw, fm(temp, rec.x));
@@ -189,7 +193,7 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
             };
             for (int jr = minZi; jr <= maxZi; ++jr) {
                 const float2 zc = __ldg(zr + jr);
-                const float qzd = fs(cz, fa(g.zmin, fm((float)jr, g.dv)));      // sz - qz for sz = cz
+                const float qzd = CONE ? 0.f : fs(cz, fa(g.zmin, fm((float)jr, g.dv)));   // sz - qz, sz = cz
                 const float2* __restrict__ rrow = rays + (long long)jr * R + minYi;
 #pragma unroll
                 for (int q = 0; q < REF_COLS; ++q)
@@ -226,12 +230,21 @@ ctr_status launch_sart_ref_t(const Geometry& G, const BpArgs& a, cudaStream_t st
     const dim3 grid((g.M + 31) / 32, (g.N + rows - 1) / rows, (g.Z + zl - 1) / zl);
     if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
     const float2* rays = (const float2*)a.rays;
-    if (rows == 8)
-        k_sart_ref<VT, STOCH, 8, 2, TL><<<grid, 256, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                              a.pass_seed, zl);
-    else
-        k_sart_ref<VT, STOCH, 4, 4, TL><<<grid, 128, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
-                                                              a.pass_seed, zl);
+    const bool cone = g.ct_style == 0;
+    if (rows == 8) {
+        if (cone)
+            k_sart_ref<VT, STOCH, 8, 4, TL, true><<<grid, 256, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                        a.pass_seed, zl);
+        else
+            k_sart_ref<VT, STOCH, 8, 4, TL, false><<<grid, 256, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                         a.pass_seed, zl);
+    } else if (cone) {
+        k_sart_ref<VT, STOCH, 4, 8, TL, true><<<grid, 128, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                    a.pass_seed, zl);
+    } else {
+        k_sart_ref<VT, STOCH, 4, 8, TL, false><<<grid, 128, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                     a.pass_seed, zl);
+    }
     return CTR_OK;
 }
 
