@@ -380,7 +380,10 @@ ctr_status ctr_set_default_geometry(const ctr_geometry_desc* desc);
 
 /* V63/host_IterativeRecon_CBCT.c:70-128: A x for all views into h_proj_data. */
 void Forward_3D_ray_driven_siddon(float* h_volume, float* h_proj_data);
-/* V63/host_IterativeRecon_CBCT.c:1-67: one SART pass, h_volume updated in place. */
+/* V63/host_IterativeRecon_CBCT.c:1-67: one SART pass, h_volume updated in place,
+ * with the reference backprojector's arithmetic (CTR_SART_REFERENCE_BP), so
+ * the result is the reference's bit for bit; for a tetrahedron-beam geometry,
+ * Reconstruction_3D_ray_driven_TBCT's backprojection and update. */
 void Reconstruction_3D_ray_driven_CBCT(float* h_volume, float* h_proj_data, float beta_temp);
 /* V63/host_IterativeRecon_CBCT.c:131-204: prints <Ax,Ax> and <x,A^T A x> for view 0. */
 void CheckMatchedJointOperator(float* h_volume);
