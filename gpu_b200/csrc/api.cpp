@@ -1149,8 +1149,9 @@ extern "C" void Reconstruction_3D_ray_driven_CBCT(float* h_volume, float* h_proj
     DevBuf v, p;
     if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, h_proj_data, pb) != CTR_OK) return;
     // the reference's own backprojection arithmetic: the drop-in returns the reference's numbers
-    const unsigned fl = g->dg.ct_style == 3 ? 0u : CTR_SART_REFERENCE_BP;
-    if (ctr_sart_pass(reinterpret_cast<ctr_geometry*>(g), v.p, CTR_F32, p.p, CTR_F32, beta, fl, 0, nullptr) != CTR_OK) return;
+    if (ctr_sart_pass(reinterpret_cast<ctr_geometry*>(g), v.p, CTR_F32, p.p, CTR_F32, beta, CTR_SART_REFERENCE_BP, 0,
+                      nullptr) != CTR_OK)
+        return;
     cudaError_t e = cudaMemcpy(h_volume, v.p, vb, cudaMemcpyDefault);
     if (e != cudaSuccess) { cuda_error(e, "Reconstruction_3D_ray_driven_CBCT"); return; }
     check_device_errors(g, nullptr);

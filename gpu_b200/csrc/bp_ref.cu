@@ -32,15 +32,19 @@
 namespace ctr {
 
 // zref[k][v] = (min, max) of the reference's z alphas of cell k for detector
-// row v (universal.cu:717-718 with :592-594 and :711-735).
+// row v (universal.cu:717-718 with :592-594 and :711-735; for the tetrahedron
+// beam T42/...TBCT_voxel.cu:717-718 with its voxel centre :568-570 and row v's
+// source, :615).
 __global__ void k_zref(const DevGeom g, float2* __restrict__ zref)
 {
     const long long n = (long long)g.Z * g.ZP;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t / g.ZP), v = (int)(t % g.ZP);
-        const float cz = fa(fa(g.bz, fm(g.vz, 0.5f)), fm((float)k, g.vz));
-        const float qz = fa(g.zmin, fm((float)v, g.dv));
-        const float sz = g.ct_style == 0 ? g.srcz : cz;
+        const int src = v / g.nvr;
+        const float cz = g.ct_style == 3 ? fa(g.bz, fm(g.vz, fa(0.5f, (float)k)))
+                                         : fa(fa(g.bz, fm(g.vz, 0.5f)), fm((float)k, g.vz));
+        const float qz = fa(g.zmin, fm((float)(v - src * g.nvr), g.dv));
+        const float sz = g.ct_style == 3 ? fa(g.zsrc0, fm((float)src, g.zsrc_dz)) : (g.ct_style == 0 ? g.srcz : cz);
         const float az0 = fdv(fs(fs(cz, fm(0.5f, g.vz)), qz), fs(sz, qz));
         const float az1 = fdv(fs(fa(cz, fm(0.5f, g.vz)), qz), fs(sz, qz));
         zref[t] = make_float2(fminf(az0, az1), fmaxf(az0, az1));
@@ -215,6 +219,161 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
     }
 }
 
+// The tetrahedron beam (T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:546-775):
+// per voxel (T42's centre, boundary + v*(0.5 + index)), the sources that pass
+// its source_lower/source_upper test (:620-627), each with the bounding
+// rectangle of the voxel's corners projected from that source (:631-685), its
+// pixels row by row, column by column, the slab alphas by division
+// (:713-731), chords above vx*1e-6 (:733-747); the sources' sums added in
+// ascending order (one of the orders of the reference's atomicAdd), and
+// f += beta*sum/length where the length exceeds vx*1e-3 (:772-773), nothing
+// otherwise.  The same regroupings as k_sart_ref; the chord length is the
+// projector's (source and pixel are the projector's endpoints).
+template <typename VT, bool STOCH, int BY, int MINB, bool TL>
+__global__ void __launch_bounds__(32 * BY, MINB)
+k_sart_ref_tb(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
+              uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
+{
+    if (STOCH && pass_seed) seed = *pass_seed * 0x9E3779B9u + (uint32_t)view;
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * BY + (threadIdx.x >> 5);
+    if (i >= g.M || j >= g.N) return;
+    const int kb = blockIdx.z * zl, ke = min(g.Z, kb + zl);
+    const long long MN = (long long)g.M * g.N;
+    const long long vstep = TL ? 64LL * g.Mt * g.Nt : MN;
+
+    const float ex = fs(fs((float)i, g.fov_h_x), g.m_off);                   // :600-602
+    const float ey = fs((float)j, g.fov_h_y);
+    if (fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2) return;
+
+    const float cx = fa(g.bx, fm(g.vx, fa(0.5f, (float)i)));                 // :568-569
+    const float cy = fa(g.by, fm(g.vy, fa(0.5f, (float)j)));
+    const float2 sc = g.trig[view];
+    const float s = sc.x, c = sc.y;
+    const float DSO = g.dso, DOD = g.dod;
+    const float tden = fs(fa(fm(cx, c), fm(cy, s)), DOD);                    // :620, t - DOD
+
+    float mlo = __int_as_float(0x7f800000), mhi = -mlo;
+    float minY = mlo, maxY = mhi;
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {                                          // :631-655
+        const float px = fs(fa(cx, fm((float)(cc & 1), g.vx)), fm(0.5f, g.vx));
+        const float py = fs(fa(cy, fm((float)(cc >> 1), g.vy)), fm(0.5f, g.vy));
+        const float t = fa(fm(px, c), fm(py, s));
+        const float ss = fa(fm(-px, s), fm(py, c));
+        const float mg = fdv(fs(t, DOD), fs(DSO, t));
+        const float ou = fa(fm(mg, fs(ss, g.srcy)), ss);
+        minY = fminf(minY, ou);
+        maxY = fmaxf(maxY, ou);
+        mlo = fminf(mlo, mg);
+        mhi = fmaxf(mhi, mg);
+    }
+    int minYi = __float2int_rd(fa(fm(fs(minY, g.ymin), g.inv_du), 0.5f));   // :659-660
+    int maxYi = __float2int_rd(fa(fm(fs(maxY, g.ymin), g.inv_du), 0.5f));
+    if ((minYi < 0 && maxYi < 0) || (minYi > g.R - 1 && maxYi > g.R - 1)) return;   // :668: nothing added
+    minYi = max(minYi, 0);
+    maxYi = min(maxYi, g.R - 1);
+
+    const float sx = fs(fm(g.srcx, c), fm(g.srcy, s));                      // :613-614
+    const float sy = fa(fm(g.srcx, s), fm(g.srcy, c));
+    const float xlo = fs(cx, fm(0.5f, g.vx)), xhi = fa(cx, fm(0.5f, g.vx));
+    const float ylo = fs(cy, fm(0.5f, g.vy)), yhi = fa(cy, fm(0.5f, g.vy));
+    auto column = [&](int ir, float& lo, float& hi) {                        // :693-731
+        const float pu = fa(g.ymin, fm((float)ir, g.du));
+        const float qx = fs(fm(DOD, c), fm(pu, s));
+        const float qy = fa(fm(DOD, s), fm(pu, c));
+        const float ax0 = fdv(fs(xlo, qx), fs(sx, qx)), ax1 = fdv(fs(xhi, qx), fs(sx, qx));
+        const float ay0 = fdv(fs(ylo, qy), fs(sy, qy)), ay1 = fdv(fs(yhi, qy), fs(sy, qy));
+        lo = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
+        hi = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+    };
+    float clo[REF_COLS], chi[REF_COLS];
+    unsigned live = 0;
+    const int ncol = maxYi - minYi + 1;
+#pragma unroll
+    for (int q = 0; q < REF_COLS; ++q) {
+        clo[q] = 0.f; chi[q] = 0.f;
+        if (q < ncol) {
+            column(minYi + q, clo[q], chi[q]);
+            if (chi[q] > clo[q]) live |= 1u << q;
+        }
+    }
+
+    const int R = g.R, nv = g.nvr;
+    auto zsrc = [&](int q) { return fa(g.zsrc0, fm((float)q, g.zsrc_dz)); };
+    int s0 = 0, s1 = -1;
+    bool s_est = true;
+    VT* pv = vol + (TL ? (long long)tile_index(g, i, j, kb) : (long long)kb * MN + (long long)j * g.M + i);
+    for (int k = kb; k < ke; ++k, pv += vstep) {
+        const float cz = fa(g.bz, fm(g.vz, fa(0.5f, (float)k)));           // :570
+        const float upper = fa(fdv(fm(fs(fa(cz, g.vz), g.zmin), g.dsod), tden), g.zmin);   // :623
+        const float lower = fa(fdv(fm(fs(fs(cz, g.vz), g.zmax), g.dsod), tden), g.zmax);   // :624
+        if (s_est) {   // the kept sources: one range growing with k (see k_sart_walk's TB form)
+            s_est = false;
+            s0 = 0;
+            s1 = g.nsrc - 1;
+            if (g.nsrc > 1) {
+                s0 = (int)fminf(fmaxf(ceilf(__fdividef(fs(lower, g.zsrc0), g.zsrc_dz)), 0.f), (float)g.nsrc);
+                s1 = (int)fminf(fmaxf(floorf(__fdividef(fs(upper, g.zsrc0), g.zsrc_dz)), -1.f), (float)(g.nsrc - 1));
+            }
+        }
+        while (s0 > 0 && !(zsrc(s0 - 1) < lower)) --s0;
+        while (s0 < g.nsrc && zsrc(s0) < lower) ++s0;
+        while (s1 < g.nsrc - 1 && !(zsrc(s1 + 1) > upper)) ++s1;
+        while (s1 >= 0 && zsrc(s1) > upper) --s1;
+        const float2* __restrict__ zr = g.zref + (long long)k * g.ZP;
+        float WS = 0.f, L = 0.f;
+        for (int sq = s0; sq <= s1; ++sq) {
+            const float zs = zsrc(sq);
+            // rows of the rectangle projected from this source (:649, :661-662)
+            float minZ = __int_as_float(0x7f800000), maxZ = -minZ;
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {
+                const float pz = fs(fa(cz, fm((float)kk, g.vz)), fm(0.5f, g.vz));
+                const float dz = fs(pz, zs);
+                minZ = fminf(minZ, fa(fm(dz >= 0.f ? mlo : mhi, dz), pz));
+                maxZ = fmaxf(maxZ, fa(fm(dz >= 0.f ? mhi : mlo, dz), pz));
+            }
+            int minZi = __float2int_rd(fa(fm(fs(minZ, g.zmin), g.inv_du), 0.5f));
+            int maxZi = __float2int_rd(fa(fm(fs(maxZ, g.zmin), g.inv_du), 0.5f));
+            float sw = 0.f, sl = 0.f;
+            if (!((minZi < 0 && maxZi < 0) || (minZi > nv - 1 && maxZi > nv - 1))) {
+                minZi = max(minZi, 0);
+                maxZi = min(maxZi, nv - 1);
+                for (int jr = sq * nv + minZi; jr <= sq * nv + maxZi; ++jr) {
+                    const float2 zc = __ldg(zr + jr);
+                    const float2* __restrict__ rrow = rays + (long long)jr * R + minYi;
+                    auto pair = [&](float lo, float hi, float2 rec) {
+                        const float dl = fs(fminf(hi, zc.y), fmaxf(lo, zc.x));
+                        if (dl > 0.f) {                                          // :733
+                            const float temp = fm(rec.y, dl);
+                            if (temp > g.thr_bp) {                              // :738-744
+                                sw = fa(sw, fm(temp, rec.x));
+                                sl = fa(sl, temp);
+                            }
+                        }
+                    };
+#pragma unroll
+                    for (int q = 0; q < REF_COLS; ++q)
+                        if (live & (1u << q)) pair(clo[q], chi[q], __ldg(rrow + q));
+                    for (int q = REF_COLS; q < ncol; ++q) {
+                        float lo, hi;
+                        column(minYi + q, lo, hi);
+                        if (hi > lo) pair(lo, hi, __ldg(rrow + q));
+                    }
+                }
+            }
+            WS = fa(WS, sw);                                                    // :754-755
+            L = fa(L, sl);
+        }
+        if (L > g.thr_upd) {                                                    // :772-773
+            const float nvl = fa(Store<VT>::ldw(pv), fdv(fm(beta, WS), L));
+            if (STOCH) st_sr<VT>(pv, nvl, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
+            else Store<VT>::st(pv, nvl);
+        }
+    }
+}
+
 // launch shapes: the column walk's table (rows per block, z run, register cap)
 template <typename VT, bool STOCH, bool TL>
 ctr_status launch_sart_ref_t(const Geometry& G, const BpArgs& a, cudaStream_t st)
@@ -231,7 +390,14 @@ ctr_status launch_sart_ref_t(const Geometry& G, const BpArgs& a, cudaStream_t st
     if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
     const float2* rays = (const float2*)a.rays;
     const bool cone = g.ct_style == 0;
-    if (rows == 8) {
+    if (g.ct_style == 3) {
+        if (rows == 8)
+            k_sart_ref_tb<VT, STOCH, 8, 4, TL><<<grid, 256, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                      a.pass_seed, zl);
+        else
+            k_sart_ref_tb<VT, STOCH, 4, 8, TL><<<grid, 128, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
+                                                                      a.pass_seed, zl);
+    } else if (rows == 8) {
         if (cone)
             k_sart_ref<VT, STOCH, 8, 4, TL, true><<<grid, 256, 0, st>>>(g, (VT*)a.vol, rays, a.view0, a.beta, a.seed,
                                                                         a.pass_seed, zl);
@@ -250,8 +416,6 @@ ctr_status launch_sart_ref_t(const Geometry& G, const BpArgs& a, cudaStream_t st
 
 ctr_status launch_sart_ref(const Geometry& G, const BpArgs& a, cudaStream_t st)
 {
-    if (G.dg.ct_style == 3)
-        return set_error(CTR_ERR_UNSUPPORTED, "CTR_SART_REFERENCE_BP: not for the tetrahedron beam");
     const bool sr = (a.flags & CTR_SART_STOCHASTIC_ROUND) != 0;
     CTR_DISPATCH_DTYPE(a.vol_dtype, VT, {
         if (a.tiled) {

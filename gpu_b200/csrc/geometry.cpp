@@ -355,14 +355,12 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
         goto fail;
     }
     if ((st = launch_zcell(*g, g->d_zcell, 0)) != CTR_OK) goto fail;
-    if (q.ct_style != 3) {
-        if ((e = cudaMalloc(&g->d_zref, sizeof(float2) * (size_t)d.nz * q.ZP)) != cudaSuccess) {
-            st = cuda_error(e, "cudaMalloc(zref)");
-            goto fail;
-        }
-        if ((st = launch_zref(*g, g->d_zref, 0)) != CTR_OK) goto fail;
-        q.zref = g->d_zref;
+    if ((e = cudaMalloc(&g->d_zref, sizeof(float2) * (size_t)d.nz * q.ZP)) != cudaSuccess) {
+        st = cuda_error(e, "cudaMalloc(zref)");
+        goto fail;
     }
+    if ((st = launch_zref(*g, g->d_zref, 0)) != CTR_OK) goto fail;
+    q.zref = g->d_zref;
     if ((e = cudaStreamSynchronize(0)) != cudaSuccess) { st = cuda_error(e, "zcell"); goto fail; }
     q.zcell = g->d_zcell;
     *out = reinterpret_cast<ctr_geometry*>(g);

@@ -167,8 +167,10 @@ ctr_status ctr_backproject(const ctr_geometry* geom, const float* sino, int view
  * V63/kernel_IterativeRecon_universal.cu:571-810: the bounding rectangle of
  * the voxel's corner projections, the slab alphas by division, the pixels
  * row by row, "f += 0" where the summed length is below vx*1e-6), so that a
- * FP32 SART pass equals the reference's bit for bit (CT_style 0, 1, 2; not
- * the tetrahedron beam).  Default (flag clear): the gather backprojector with
+ * FP32 SART pass equals the reference's bit for bit (CT_style 0, 1, 2; for
+ * CTR_GEOM_TBCT the tetrahedron-beam program's backprojection and update,
+ * T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:546-775, its sources added in
+ * ascending order).  Default (flag clear): the gather backprojector with
  * the forward projector's own chords, the exact transpose of the projector,
  * which differs from the reference's alphas in rounding (and keeps the rays
  * lying on a voxel plane that the reference's 0/0 drops). */
@@ -382,8 +384,9 @@ ctr_status ctr_set_default_geometry(const ctr_geometry_desc* desc);
 void Forward_3D_ray_driven_siddon(float* h_volume, float* h_proj_data);
 /* V63/host_IterativeRecon_CBCT.c:1-67: one SART pass, h_volume updated in place,
  * with the reference backprojector's arithmetic (CTR_SART_REFERENCE_BP), so
- * the result is the reference's bit for bit; for a tetrahedron-beam geometry,
- * Reconstruction_3D_ray_driven_TBCT's backprojection and update. */
+ * the result is the reference's bit for bit; for a tetrahedron-beam geometry
+ * that of Reconstruction_3D_ray_driven_TBCT
+ * (TBCT/TBCT_1024V_1024P_v4.2_20171012/voxel/host_IterativeRecon_TBCT_voxel.c:1-92). */
 void Reconstruction_3D_ray_driven_CBCT(float* h_volume, float* h_proj_data, float beta_temp);
 /* V63/host_IterativeRecon_CBCT.c:131-204: prints <Ax,Ax> and <x,A^T A x> for view 0. */
 void CheckMatchedJointOperator(float* h_volume);

@@ -1,6 +1,7 @@
 """CTR_SART_REFERENCE_BP: the SART update with the reference backprojector's
-own arithmetic (V63/kernel_IterativeRecon_universal.cu:571-810).  With it a
-FP32 SART pass -- and the SART + FISTA + FGP-TV loop built on it -- equals the
+own arithmetic (V63/kernel_IterativeRecon_universal.cu:571-810; for the
+tetrahedron beam its program's backprojection and update).  With it a FP32
+SART pass -- and the SART + FISTA + FGP-TV loop built on it -- equals the
 reference's bit for bit: against the C restatement (pinned to the reference's
 kernels compiled for the CPU) and against the golden fixtures made by those
 kernels themselves."""
@@ -11,7 +12,7 @@ import pytest
 
 from scan_configs import SMALL, STYLES, TBCT, ctr_desc, og_desc_xyz
 
-CASES = dict(SMALL, **STYLES)
+CASES = dict(SMALL, **STYLES, **TBCT)
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 pytestmark = pytest.mark.gpu
@@ -57,7 +58,7 @@ def test_sart_pass_equals_restatement_from_signed_zeros(name, oracle_built):
     g = gpu_b200.Geometry(ctr_desc(cfg))
     rng = np.random.default_rng(31)
     vol = rng.uniform(0, 0.05, o.vol_shape).astype(np.float32)
-    vol[rng.uniform(size=vol.shape) < 0.2] = -0.0
+    vol[rng.uniform(size=vol.shape) < 0.2] = -0.0     # the tetrahedron beam's update has no "+= 0"
     b = np.stack([o.forward_view(vol * 1.1, j, 0) for j in range(cfg["nviews"])])
     want = o.sart_pass_ref(o.sart_pass_ref(vol, b, 0.8), b, 0.8)
     x = torch.from_numpy(vol).cuda()
@@ -66,7 +67,7 @@ def test_sart_pass_equals_restatement_from_signed_zeros(name, oracle_built):
     np.testing.assert_array_equal(bits(x.cpu().numpy()), bits(want))
 
 
-@pytest.mark.parametrize("name", ["cube16", "odd", "fan_slices_odd", "parallel"])
+@pytest.mark.parametrize("name", ["cube16", "odd", "fan_slices_odd", "parallel", "tbct"])
 def test_every_launch_shape_gives_the_same_result(name, oracle_built):
     import gpu_b200
     cfg = CASES[name]
@@ -85,11 +86,12 @@ def test_every_launch_shape_gives_the_same_result(name, oracle_built):
         np.testing.assert_array_equal(got, ref, err_msg=f"bp shape {bs}")
 
 
-def test_solver_equals_reference_call_sequence(oracle_built):
+@pytest.mark.parametrize("name", ["aniso", "tbct"])
+def test_solver_equals_reference_call_sequence(name, oracle_built):
     """Three SART + FISTA + FGP-TV iterations (graph-captured) with the
     reference backprojector: the reference's loop restated, bit for bit."""
     import gpu_b200
-    cfg = SMALL["aniso"]
+    cfg = CASES[name]
     o = oracle_built.Oracle(og_desc_xyz(cfg))
     g = gpu_b200.Geometry(ctr_desc(cfg))
     truth = o.phantom(np.array([[0, 0, 0, 5, 4, 3, 0.3, 0.2, 0.1, 0.02], [1.5, -1, 0.5, 2, 2, 2, 0, 0, 0, 0.03]]))
@@ -112,12 +114,3 @@ def test_solver_equals_reference_call_sequence(oracle_built):
         t = np.float32(t_k)
     np.testing.assert_array_equal(bits(out.cpu().numpy()), bits(xprev))
 
-
-def test_tetrahedron_beam_is_refused():
-    import gpu_b200
-    cfg = TBCT["tbct"]
-    g = gpu_b200.Geometry(ctr_desc(cfg))
-    x = torch.zeros(g.vol_shape, device="cuda")
-    b = torch.zeros((cfg["nviews"],) + g.view_shape, device="cuda")
-    with pytest.raises(gpu_b200.CtrError):
-        g.sart_pass(x, b, 0.8, flags=flags())
