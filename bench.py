@@ -714,6 +714,22 @@ def run_tbct(args):
     h2d = h_sino.numel() * h_sino.element_size()
     d2h = h_vol.numel() * h_vol.element_size() + 3 * 8
 
+    # T42's own backprojection arithmetic (CTR_SART_REFERENCE_BP: the SART pass
+    # equals the tetrahedron-beam program's bit for bit), FP32 as the reference
+    geom.set_shapes(tuned["f32"]["fp_shape"], tuned["f32"]["bp_shape"])
+    refbp = gpu_b200.Solver(geom, gpu_b200.F32, beta=TBCT_BETA, lambda_tv=0.0, fgp_iters=0, fista=True,
+                            objective=True, use_graph=True, sart_flags=gpu_b200.SART_REFERENCE_BP)
+    refbp.set_sinogram(runs["f32"]["sino"])
+    refbp.set_volume(None)
+    refbp.iterate(1)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    refbp.iterate(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    refbp_ms = e0.elapsed_time(e1) / args.steps
+    refbp.close()
+
     # per-kernel times of the SART projectors (32 views spread over the scan)
     kern = {}
     for mode in ("f32", "f16"):
@@ -750,6 +766,9 @@ def run_tbct(args):
         "f32": {"iter_per_s": 1000.0 / runs["f32"]["ms"], "ms_per_step": runs["f32"]["ms"],
                 "voxel_updates_per_s": 1000.0 / runs["f32"]["ms"] * V * T["n_views"]},
         "f16_over_f32": runs["f32"]["ms"] / runs["f16"]["ms"],
+        "reference_bp_f32": {"iter_per_s": 1000.0 / refbp_ms, "ms_per_step": refbp_ms,
+                             "note": "CTR_SART_REFERENCE_BP: the tetrahedron-beam program's backprojection "
+                                     "arithmetic, SART pass bit-exact with it"},
         "objective_last": {m: runs[m]["objective_last"] for m in runs},
         "e2e": {"value": 1000.0 / e2e_ms, "unit": "iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": "k_sart_walk, tetrahedron beam (SART update, f16 volume, tiled)",

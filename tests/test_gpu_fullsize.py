@@ -104,15 +104,16 @@ def test_dot_product_full_size(cfg, oracle_built):
         assert abs(a - b) <= 1e-6 * max(abs(a), abs(b)), (a, b)
 
 
-def test_sart_view_reference_backprojector_full_size(oracle_built):
+@pytest.mark.parametrize("cfg", [SCAN, TBCT_SCAN], ids=["cone512", "tbct512"])
+def test_sart_view_reference_backprojector_full_size(cfg, oracle_built):
     """CTR_SART_REFERENCE_BP at full size: one SART view from a non-zero volume
     equals the reference's backprojection arithmetic (the C restatement pinned
     to the reference's kernels) bit for bit."""
     import gpu_b200
-    g, o, vol = scan(SCAN, oracle_built)
+    g, o, vol = scan(cfg, oracle_built)
     h = vol.cpu().numpy()
-    j = 701
-    b = torch.zeros((SCAN["nviews"],) + g.view_shape, device="cuda")
+    j = (cfg["nviews"] // 2 + 189) % cfg["nviews"]
+    b = torch.zeros((cfg["nviews"],) + g.view_shape, device="cuda")
     g.forward(vol * 1.05, b[j:j + 1], j, 1)
     x = vol.clone()
     g.sart_views(x, b, 0.8, j, 1, flags=gpu_b200.SART_REFERENCE_BP)
