@@ -42,6 +42,8 @@ def parse():
                    help="profiling mode: set up the scan, run a SART update of this many views, print timings, exit")
     p.add_argument("--profile-iteration", action="store_true",
                    help="with --profile-views: also run two FP16 solver iterations (the second in steady state)")
+    p.add_argument("--profile-refbp", action="store_true",
+                   help="with --profile-views: the SART updates with the reference backprojector's arithmetic")
     p.add_argument("--profile-fdk", type=int, default=0,
                    help="profiling mode: FDK of the 512^3 scan restricted to this many views (weighting, ramp "
                         "and backprojection), print timings, exit")
@@ -352,7 +354,8 @@ def profile_views(args):
         geom.set_shapes(1, 1)
     for name, s in (("f32", sino32), ("f16", sino16)):
         vol = torch.zeros(geom.vol_shape, device="cuda", dtype=s.dtype)
-        fp, bp = geom.sart_views(vol, s, beta, 0, n, flags=gpu_b200.SART_TILED, timed=True)
+        fl = gpu_b200.SART_TILED | (gpu_b200.SART_REFERENCE_BP if args.profile_refbp else 0)
+        fp, bp = geom.sart_views(vol, s, beta, 0, n, flags=fl, timed=True)
         out[name] = {"fp_ms_per_view": fp / n, "bp_ms_per_view": bp / n}
         del vol
     del truth
