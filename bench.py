@@ -952,6 +952,19 @@ def main():
         _, b_ms = geom.sart_views(vtmp, runs["f32"]["sino"], BETA, (j * 97) % SCAN["n_views"], 1,
                                      flags=gpu_b200.SART_TILED | gpu_b200.SART_REFERENCE_BP, timed=True)
         rb_bp += b_ms
+    # the reference's default build (Number_of_Devices 4, its z-slab SART,
+    # bit-exact with its multi-GPU kernels) on this one GPU: per view 4 slab
+    # partial projections, the ordered combination, 4 slab updates
+    slab4 = {}
+    for key, fl in (("reference_bp", gpu_b200.SART_TILED | gpu_b200.SART_REFERENCE_BP),
+                    ("engine", gpu_b200.SART_TILED)):
+        geom.sart_pass_slabs(vtmp, runs["f32"]["sino"], BETA, 4, 0, 4, flags=fl)          # warm-up
+        barrier()
+        e0.record(stream)
+        geom.sart_pass_slabs(vtmp, runs["f32"]["sino"], BETA, 4, 100, 32, flags=fl)
+        e1.record(stream)
+        barrier()
+        slab4[key] = e0.elapsed_time(e1) / 32
     del vtmp
 
     # ray-voxel intersections of one pass over all views (Siddon segments of
@@ -1012,6 +1025,11 @@ def main():
                                  "bp_ms_per_view": rb_bp / 32,
                                  "note": "CTR_SART_REFERENCE_BP: the reference backprojector's arithmetic, "
                                          "SART pass bit-exact with the reference"},
+            "slabs4_f32": {"ms_per_view_reference_bp": slab4["reference_bp"], "ms_per_view_engine": slab4["engine"],
+                           "one_device_ms_per_view": {"f32_fp": kern["f32"]["fp_ms"], "reference_bp": rb_bp / 32},
+                           "note": "the reference's default Number_of_Devices=4 build: z-slab SART views (4 slab "
+                                   "partial projections, the ordered combination, 4 slab updates) on one B200, "
+                                   "views 100-131, FP32, tiled; bit-exact with its multi-GPU kernels"},
             "fdk_ms": fdk_ms,
             "f32": {"iter_per_s": job_rate(ms_f32, world), "ms_per_step": ms_f32,
                     "voxel_updates_per_s": job_rate(ms_f32, world) * V * SCAN["n_views"]},

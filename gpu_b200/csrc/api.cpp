@@ -271,6 +271,187 @@ extern "C" ctr_status ctr_forward_trace(const ctr_geometry* geom, const float* v
 
 // ------------------------------------------------------------- TV and FISTA
 
+// ------------------------------------------------ z-slab SART (multi-GPU build)
+
+namespace {
+
+ctr_status need_slab(const Geometry* g)
+{
+    if (g->dg.slab_n > 1) return set_error(CTR_ERR_UNSUPPORTED, "not for a slab geometry");
+    return CTR_OK;
+}
+
+// the slab geometries of g (a whole-volume geometry) for an n-way split, built on first use
+ctr_status slab_geoms(Geometry* g, int n, std::vector<Geometry*>& out)
+{
+    CTR_TRY(need_slab(g));
+    if ((int)g->slab_geoms.size() != n) {
+        for (Geometry* sg : g->slab_geoms) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(sg));
+        g->slab_geoms.clear();
+        for (int i = 0; i < n; ++i) {
+            ctr_geometry* sg = nullptr;
+            const ctr_status st = ctr_geometry_create_slab(&g->desc, n, i, &sg);
+            if (st != CTR_OK) {
+                for (Geometry* q : g->slab_geoms) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(q));
+                g->slab_geoms.clear();
+                return st;
+            }
+            g->slab_geoms.push_back(GE(sg));
+        }
+    }
+    for (Geometry* sg : g->slab_geoms) {   // the parent's tuned launch shapes
+        sg->fp_shape = g->fp_shape;
+        sg->bp_shape = g->bp_shape;
+    }
+    out = g->slab_geoms;
+    return CTR_OK;
+}
+
+ctr_status ensure_parts(Geometry* g, size_t bytes)
+{
+    if (bytes <= g->parts_cap) return CTR_OK;
+    if (g->d_parts) cudaFree(g->d_parts);
+    g->d_parts = nullptr;
+    g->parts_cap = 0;
+    CTR_CUDA_TRY(cudaMalloc(&g->d_parts, bytes));
+    g->parts_cap = bytes;
+    return CTR_OK;
+}
+
+// views [v0, v0+nv) of the D-slab SART on one GPU; pv the whole volume (linear or tiled)
+ctr_status sart_views_slabs(Geometry* g, const std::vector<Geometry*>& sl, void* pv, ctr_dtype vdt, bool tiled,
+                            const void* sino, ctr_dtype sdt, float beta, unsigned flags, uint32_t seed, int v0, int nv,
+                            cudaStream_t st)
+{
+    const int D = (int)sl.size();
+    const long long P = g->npix();
+    const long long per_slab = tiled ? tiled_count(sl[0]->dg) : sl[0]->nvox();
+    const size_t es = dtype_size(vdt);
+    CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
+    CTR_TRY(ensure_parts(g, (size_t)P * D * sizeof(float2)));
+    float2* parts = (float2*)g->d_parts;
+    for (int j = v0; j < v0 + nv; ++j) {
+        for (int i = 0; i < D; ++i) {                  // multiGPU.c:71-75
+            FpArgs a{};
+            a.vol = (const char*)pv + (size_t)per_slab * i * es; a.vol_dtype = vdt; a.view0 = j; a.nview = 1;
+            a.kind = FP_PARTIAL; a.out = parts + (size_t)P * i; a.tiled = tiled;
+            CTR_TRY(launch_forward(*sl[i], a, st, nullptr));
+        }
+        CTR_TRY(launch_combine(*g, parts, D, j, (const char*)sino + (size_t)j * P * dtype_size(sdt), sdt,
+                               (float2*)g->d_rays, st));   // :82-95
+        for (int i = 0; i < D; ++i) {                  // :103-112
+            BpArgs b{};
+            b.vol = (char*)pv + (size_t)per_slab * i * es; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = j;
+            b.nview = 1; b.sart = 1; b.flags = flags; b.beta = beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j;
+            b.tiled = tiled;
+            CTR_TRY(launch_backproject(*sl[i], b, st));
+        }
+    }
+    return CTR_OK;
+}
+
+}  // namespace
+
+extern "C" ctr_status ctr_forward_partial(const ctr_geometry* geom, const void* vol, ctr_dtype vdt, int view,
+                                          float* part, unsigned flags, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(part, "part"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, view, 1));
+    FpArgs a{};
+    a.vol = vol; a.vol_dtype = vdt; a.view0 = view; a.nview = 1; a.kind = FP_PARTIAL; a.out = part;
+    a.tiled = (flags & CTR_VOLUME_TILED) != 0;
+    return launch_forward(*g, a, S(stream), nullptr);
+}
+
+extern "C" ctr_status ctr_combine_partials(const ctr_geometry* geom, const float* parts, int n_parts, int view,
+                                           const void* b_view, ctr_dtype bdt, float* rays, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(parts, "parts"));
+    CTR_TRY(need(b_view, "b_view"));
+    CTR_TRY(need(rays, "rays"));
+    CTR_TRY(need_dtype(bdt, "b_dtype"));
+    if (n_parts < 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "n_parts must be >= 1");
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, view, 1));
+    return launch_combine(*g, (const float2*)parts, n_parts, view, b_view, bdt, (float2*)rays, S(stream));
+}
+
+extern "C" ctr_status ctr_sart_update(const ctr_geometry* geom, void* vol, ctr_dtype vdt, const float* rays, int view,
+                                      float beta, unsigned flags, uint32_t seed, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(rays, "rays"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    if (!std::isfinite(beta)) return set_error(CTR_ERR_INVALID_ARGUMENT, "beta must be finite");
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, view, 1));
+    BpArgs b{};
+    b.vol = vol; b.vol_dtype = vdt; b.rays = rays; b.view0 = view; b.nview = 1; b.sart = 1;
+    b.flags = flags & (CTR_SART_STOCHASTIC_ROUND | CTR_SART_REFERENCE_BP); b.beta = beta;
+    b.seed = seed * 0x9E3779B9u + (uint32_t)view; b.tiled = (flags & CTR_VOLUME_TILED) != 0;
+    CTR_TRY(launch_backproject(*g, b, S(stream)));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_sart_pass_slabs(const ctr_geometry* geom, int n_slabs, void* vol, ctr_dtype vdt,
+                                          const void* sino, ctr_dtype sdt, float beta, unsigned flags, uint32_t seed,
+                                          int v0, int n, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need_dtype(vdt, "vol_dtype"));
+    CTR_TRY(need_dtype(sdt, "sino_dtype"));
+    if (!std::isfinite(beta)) return set_error(CTR_ERR_INVALID_ARGUMENT, "beta must be finite");
+    if (n_slabs < 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "n_slabs must be >= 1");
+    Geometry* g = GE(geom);
+    CTR_TRY(check_views(g, v0, n));
+    std::vector<Geometry*> sl;
+    CTR_TRY(slab_geoms(g, n_slabs, sl));
+    cudaStream_t st = S(stream);
+    const bool tiled = (flags & CTR_SART_TILED) != 0;
+    void* pv = vol;
+    if (tiled) {
+        CTR_TRY(ensure_tiled(g, (size_t)tiled_count(g->dg) * dtype_size(vdt)));
+        pv = g->d_tiled;
+        CTR_TRY(launch_tiling(*g, vol, pv, vdt, true, st));
+    }
+    CTR_TRY(sart_views_slabs(g, sl, pv, vdt, tiled, sino, sdt, beta, flags & ~CTR_SART_TILED, seed, v0, n, st));
+    if (tiled) CTR_TRY(launch_tiling(*g, pv, vol, vdt, false, st));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_volume_tiling(const ctr_geometry* geom, const void* src, void* dst, ctr_dtype dt,
+                                        int to_tiled, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(src, "src"));
+    CTR_TRY(need(dst, "dst"));
+    CTR_TRY(need_dtype(dt, "dtype"));
+    return launch_tiling(*GE(geom), src, dst, dt, to_tiled != 0, S(stream));
+}
+
+extern "C" ctr_status ctr_volume_tiled_count(const ctr_geometry* geom, int64_t* count)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(count, "count"));
+    *count = tiled_count(GE(geom)->dg);
+    return CTR_OK;
+}
+
+
 extern "C" ctr_status ctr_fgp_tv(const ctr_geometry* geom, void* vol, ctr_dtype dt, float lambda, int n_iter,
                                  void* stream)
 {
@@ -364,6 +545,7 @@ extern "C" ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float
     CTR_TRY(need(geom, "geometry"));
     CTR_TRY(need(sino, "sino"));
     CTR_TRY(need(vol, "vol"));
+    CTR_TRY(need_slab(GE(geom)));
     if (GE(geom)->dg.ct_style != 0) return set_error(CTR_ERR_UNSUPPORTED, "FDK is for the cone-beam geometry");
     return launch_fdk(*GE(geom), sino, vol, S(stream));
 }
@@ -377,6 +559,7 @@ extern "C" ctr_status ctr_fdk_backproject(const ctr_geometry* geom, const float*
     CTR_TRY(need(vol, "vol"));
     Geometry* g = GE(geom);
     CTR_TRY(check_views(g, v0, n));
+    CTR_TRY(need_slab(g));
     if (g->dg.ct_style != 0) return set_error(CTR_ERR_UNSUPPORTED, "FDK is for the cone-beam geometry");
     return launch_fdk_bp(*g, filtered, v0, n, vol, S(stream));
 }
@@ -495,6 +678,7 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
     CTR_TRY(need(out, "out"));
     CTR_TRY(need_dtype(vdt, "vol_dtype"));
     *out = nullptr;
+    CTR_TRY(need_slab(GE(geom)));
     if (!std::isfinite(p->beta) || !std::isfinite(p->lambda_tv) || p->lambda_tv < 0.f || p->fgp_iters < 0)
         return set_error(CTR_ERR_INVALID_ARGUMENT, "bad solver parameters");
     ctr_solver* s = new (std::nothrow) ctr_solver();
@@ -1095,6 +1279,7 @@ extern "C" ctr_status ctr_batch_get_volume(ctr_batch* b, int scan, void* dst, vo
 namespace {
 std::mutex g_default_mu;
 Geometry* g_default = nullptr;
+int g_default_devices = 1;   // Number_of_Devices of the replaced build
 
 // device copy of a host or device buffer
 struct DevBuf {
@@ -1117,6 +1302,15 @@ extern "C" ctr_status ctr_set_default_geometry(const ctr_geometry_desc* desc)
     CTR_TRY(ctr_geometry_create(desc, &g));
     if (g_default) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(g_default));
     g_default = GE(g);
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_set_default_devices(int n)
+{
+    clear_error();
+    if (n < 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "Number_of_Devices must be >= 1");
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    g_default_devices = n;
     return CTR_OK;
 }
 
@@ -1148,10 +1342,14 @@ extern "C" void Reconstruction_3D_ray_driven_CBCT(float* h_volume, float* h_proj
     const size_t vb = g->nvox() * 4, pb = (size_t)g->npix() * g->desc.n_views * 4;
     DevBuf v, p;
     if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, h_proj_data, pb) != CTR_OK) return;
-    // the reference's own backprojection arithmetic: the drop-in returns the reference's numbers
-    if (ctr_sart_pass(reinterpret_cast<ctr_geometry*>(g), v.p, CTR_F32, p.p, CTR_F32, beta, CTR_SART_REFERENCE_BP, 0,
-                      nullptr) != CTR_OK)
-        return;
+    // the reference's own backprojection arithmetic: the drop-in returns the reference's numbers;
+    // for an n-device build its z-slab sequence (V63/host_IterativeRecon_CBCT_multiGPU.c:1-161)
+    ctr_geometry* gg = reinterpret_cast<ctr_geometry*>(g);
+    const ctr_status st = g_default_devices > 1
+                              ? ctr_sart_pass_slabs(gg, g_default_devices, v.p, CTR_F32, p.p, CTR_F32, beta,
+                                                    CTR_SART_REFERENCE_BP, 0, 0, g->desc.n_views, nullptr)
+                              : ctr_sart_pass(gg, v.p, CTR_F32, p.p, CTR_F32, beta, CTR_SART_REFERENCE_BP, 0, nullptr);
+    if (st != CTR_OK) return;
     cudaError_t e = cudaMemcpy(h_volume, v.p, vb, cudaMemcpyDefault);
     if (e != cudaSuccess) { cuda_error(e, "Reconstruction_3D_ray_driven_CBCT"); return; }
     check_device_errors(g, nullptr);
@@ -1166,10 +1364,30 @@ extern "C" void CheckMatchedJointOperator(float* h_volume)
     DevBuf v, p, bp;
     if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, nullptr, pb) != CTR_OK || in_dev(bp, nullptr, vb) != CTR_OK) return;
     ctr_geometry* gg = reinterpret_cast<ctr_geometry*>(g);
-    // view 0: y = A x (command 0), z = A^T y with the reference's masked command-0 BP
-    if (ctr_forward(gg, v.p, CTR_F32, p.p, CTR_F32, 0, 1, nullptr) != CTR_OK) return;
     if (cudaMemset(bp.p, 0, vb) != cudaSuccess) return;
-    if (ctr_backproject(gg, (const float*)p.p, 0, 1, bp.p, CTR_F32, CTR_BP_FOV_MASK, nullptr) != CTR_OK) return;
+    if (g_default_devices > 1) {
+        // the n-device build (V63/host_IterativeRecon_CBCT_multiGPU.c:296-412): y = the slabs'
+        // weighted sums added in order (no threshold), then each slab's command-0 backprojection
+        std::vector<Geometry*> sl;
+        if (slab_geoms(g, g_default_devices, sl) != CTR_OK) return;
+        const int D = (int)sl.size();
+        const long long P = g->npix();
+        if (ensure_parts(g, (size_t)P * D * sizeof(float2)) != CTR_OK) return;
+        for (int i = 0; i < D; ++i)
+            if (ctr_forward_partial(reinterpret_cast<ctr_geometry*>(sl[i]), (const float*)v.p + sl[0]->nvox() * i,
+                                    CTR_F32, 0, (float*)g->d_parts + 2 * P * i, 0, nullptr) != CTR_OK)
+                return;
+        if (launch_combine(*g, (const float2*)g->d_parts, D, 0, nullptr, CTR_F32, (float2*)p.p, nullptr) != CTR_OK)
+            return;
+        for (int i = 0; i < D; ++i)
+            if (ctr_backproject(reinterpret_cast<ctr_geometry*>(sl[i]), (const float*)p.p, 0, 1,
+                                (float*)bp.p + sl[0]->nvox() * i, CTR_F32, CTR_BP_FOV_MASK, nullptr) != CTR_OK)
+                return;
+    } else {
+        // view 0: y = A x (command 0), z = A^T y with the reference's masked command-0 BP
+        if (ctr_forward(gg, v.p, CTR_F32, p.p, CTR_F32, 0, 1, nullptr) != CTR_OK) return;
+        if (ctr_backproject(gg, (const float*)p.p, 0, 1, bp.p, CTR_F32, CTR_BP_FOV_MASK, nullptr) != CTR_OK) return;
+    }
     std::vector<float> hy(g->npix()), hz(g->nvox());
     if (cudaMemcpy(hy.data(), p.p, pb, cudaMemcpyDeviceToHost) != cudaSuccess ||
         cudaMemcpy(hz.data(), bp.p, vb, cudaMemcpyDeviceToHost) != cudaSuccess) return;

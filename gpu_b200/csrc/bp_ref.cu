@@ -42,7 +42,7 @@ __global__ void k_zref(const DevGeom g, float2* __restrict__ zref)
         const int k = (int)(t / g.ZP), v = (int)(t % g.ZP);
         const int src = v / g.nvr;
         const float cz = g.ct_style == 3 ? fa(g.bz, fm(g.vz, fa(0.5f, (float)k)))
-                                         : fa(fa(g.bz, fm(g.vz, 0.5f)), fm((float)k, g.vz));
+                                         : fa(fa(g.bz_ref, g.cz_off), fm((float)k, g.vz));
         const float qz = fa(g.zmin, fm((float)(v - src * g.nvr), g.dv));
         const float sz = g.ct_style == 3 ? fa(g.zsrc0, fm((float)src, g.zsrc_dz)) : (g.ct_style == 0 ? g.srcz : cz);
         const float az0 = fdv(fs(fs(cz, fm(0.5f, g.vz)), qz), fs(sz, qz));
@@ -62,10 +62,11 @@ ctr_status launch_zref(const Geometry& G, float2* zref, cudaStream_t st)
 constexpr int REF_COLS = 4;   // rectangle columns whose x-y alphas a thread keeps in registers
 
 template <typename VT>
-__device__ __forceinline__ void plus_zero(VT* p)
+__device__ __forceinline__ void plus_zero(const DevGeom& g, VT* p)
 {
     // the reference's "d_volumn_kernel[idx] += 0.0f": only a stored -0 changes
-    if (__float_as_uint(Store<VT>::ldw(p)) == 0x80000000u) Store<VT>::st(p, 0.0f);
+    // (the multi-GPU build's slab kernel has the line commented out, multiGPU.cu:1388-1391)
+    if (g.ref_plus0 && __float_as_uint(Store<VT>::ldw(p)) == 0x80000000u) Store<VT>::st(p, 0.0f);
 }
 
 // CONE: CT_style 0 (the source's height fixed; d12 from the ray record)
@@ -88,7 +89,7 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
     const float ey = fs((float)j, g.fov_h_y);
     if (fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2) {
         VT* pv = pv0;
-        for (int k = kb; k < ke; ++k, pv += vstep) plus_zero(pv);
+        for (int k = kb; k < ke; ++k, pv += vstep) plus_zero(g, pv);
         return;
     }
 
@@ -156,7 +157,7 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
     const int R = g.R;
     VT* pv = pv0;
     for (int k = kb; k < ke; ++k, pv += vstep) {
-        const float cz = fa(fa(g.bz, fm(g.vz, 0.5f)), fm((float)k, g.vz));
+        const float cz = fa(fa(g.bz_ref, g.cz_off), fm((float)k, g.vz));   // :594; a slab's, multiGPU.cu:1179
         // detector rows of the rectangle (:655-683)
         float minZ, maxZ;
         if (CONE) {
@@ -210,7 +211,7 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
             }
         }
         if (sl < g.thr_bp) {                                                 // :799-807
-            plus_zero(pv);
+            plus_zero(g, pv);
         } else {
             const float nv = fa(Store<VT>::ldw(pv), fdv(fm(beta, sw), sl));
             if (STOCH) st_sr<VT>(pv, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));

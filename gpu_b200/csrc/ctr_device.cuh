@@ -104,6 +104,35 @@ __device__ __forceinline__ int tile_index(const DevGeom& g, int i, int j, int k)
     return (((k * g.Nt) + (j >> 3)) * g.Mt + (i >> 3)) * 64 + ((j & 7) << 3) + (i & 7);
 }
 
+// Source X2 and detector pixel centre X1 of the ray through pixel (u, v) at
+// view angle (s, c) (V63/kernel_IterativeRecon_universal.cu:21-45): one source
+// (cone beam), the source at the row's height (multi-slice fan beam), or a
+// source opposite each pixel (parallel beam); the tetrahedron beam's row v is
+// row v % nvr of source v / nvr's band (T42/...TBCT_voxel.cu:23-40).
+struct RayEnds {
+    float x1x, x1y, x1z, x2x, x2y, x2z;
+};
+__device__ __forceinline__ RayEnds ray_ends(const DevGeom& g, float s, float c, int u, int v)
+{
+    RayEnds e;
+    const float pu = fa(g.ymin, fm((float)u, g.du));
+    const float sy_ = g.ct_style == 2 ? pu : g.srcy;
+    e.x2x = fs(fm(g.srcx, c), fm(sy_, s));
+    e.x2y = fa(fm(g.srcx, s), fm(sy_, c));
+    e.x1x = fs(fm(g.dod, c), fm(pu, s));
+    e.x1y = fa(fm(g.dod, s), fm(pu, c));
+    const int src = g.ct_style == 3 ? v / g.nvr : 0;
+    e.x1z = fa(g.zmin, fm((float)(v - src * g.nvr), g.dv));
+    e.x2z = g.ct_style == 3 ? fa(g.zsrc0, fm((float)src, g.zsrc_dz)) : (g.ct_style == 0 ? g.srcz : e.x1z);
+    return e;
+}
+// d12 = |X2 - X1| (universal.cu:290)
+__device__ __forceinline__ float ray_d12(const RayEnds& e)
+{
+    const float dx = fs(e.x2x, e.x1x), dy = fs(e.x2y, e.x1y), dz = fs(e.x2z, e.x1z);
+    return __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));
+}
+
 // Dispatch a runtime ctr_dtype to a storage type.
 #define CTR_DISPATCH_DTYPE(dt, T, ...)                      \
     switch (dt) {                                           \

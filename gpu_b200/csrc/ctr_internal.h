@@ -45,6 +45,14 @@ struct DevGeom {
     float fdk_ang;          // us_rate*PI/180.0f        (V63/FDK/kernel_FDK.cu:117)
     float fdk_usn;          // us_rate*Nviews in float  (same line)
     int fdk_full;           // fdk_usn == 360: the FP64 factor 360.0/fdk_usn is exactly 1
+    // z-slab of the multi-GPU build (V63/kernel_IterativeRecon_universal_multiGPU.cu:591-1402):
+    // Z is the slab's ZETA/D slices, bz its BOUNDARY_VOXEL_Z; the whole volume otherwise
+    int slab_n, slab_i;     // D (1: no split) and this slab's index (subVolIdx)
+    int zpar_kr;            // the single-GPU z-parallel k range applies (not T42's, not a slab's)
+    int row_lo, row_hi;     // partial forward: rows traced (a fan-slice / parallel slab: its band)
+    float bz_ref, cz_off;   // reference BP voxel centre z = (bz_ref + cz_off) + k*vz (universal.cu:594,
+                            // multiGPU.cu:1179): bz and vz*0.5f, or the whole volume's bz and vz*(k0+0.5f)
+    int ref_plus0;          // the reference BP's "+= 0.0f" on voxels without rays (not in a slab's)
     const float* px;        // plane coordinates vx*n+bx for n = -1..M+1 at px[n+1]
     const float* py;
     const float* pz;
@@ -81,6 +89,9 @@ struct Geometry {
     float* d_fdk = nullptr; size_t fdk_cap = 0;
     void* d_tiled = nullptr; size_t tiled_bytes = 0;   // tiled copy for CTR_SART_TILED
     float* d_ramp = nullptr;                           // 2R-1 taps
+    // slab geometries of the one-GPU slab SART (ctr_sart_pass_slabs), built on first use
+    std::vector<Geometry*> slab_geoms;
+    void* d_parts = nullptr; size_t parts_cap = 0;     // [D][P] float2 partial ray sums
     // launch shapes (indices into the tuner's tables; results do not depend on them)
     int fp_shape = 1;                                  // FP: see kFpShapes in fp.cu
     int bp_shape = 1;                                  // SART BP: see kBpShapes in bp.cu
@@ -119,7 +130,9 @@ ctr_status check_device_errors(Geometry* g, cudaStream_t st);
 // ---- kernel launchers (implemented in the .cu files) ----
 // FP_SART_OBJ: the SART correction of vol and, in the same traversal, the
 // objective residual (A vol2 - b)^2 of a second volume.
-enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3, FP_DOT = 4, FP_SART_OBJ = 5 };
+// FP_PARTIAL: a slab's (Sum(len*f), Sum(len)) per ray as float2, no threshold.
+enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3, FP_DOT = 4, FP_SART_OBJ = 5,
+              FP_PARTIAL = 6 };
 struct FpArgs {
     const void* vol; ctr_dtype vol_dtype;
     int view0, nview;
@@ -170,6 +183,11 @@ struct __align__(16) AdjRay {
 ctr_status launch_ray_prep(const Geometry& g, const float* y, int view0, int nview, AdjRay* rays,
                            cudaStream_t st);
 
+// slab SART: the slabs' partial sums [n_parts][P] added in slab order, the
+// SART correction of view `view` and the ray's d12 -> rays (slabs.cu); with
+// b == nullptr the weighted sums alone, as floats
+ctr_status launch_combine(const Geometry& g, const float2* parts, int n_parts, int view, const void* b,
+                          ctr_dtype b_dt, float2* rays, cudaStream_t st);
 ctr_status launch_reduce(const double* partial, size_t n, double* out, cudaStream_t st);
 ctr_status launch_dot(const float* a, const float* b, long long n, double* partial, size_t cap,
                       double* out, cudaStream_t st);

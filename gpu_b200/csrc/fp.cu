@@ -97,22 +97,12 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     r.a_lo = 1.0f; r.a_hi = 0.0f;
     r.vi0 = r.vj0 = r.vk0 = -1; r.par = 0;
 
-    // source X2 and detector pixel centre X1 (universal.cu:21-45): one
-    // source (cone beam), the source at the row's height (multi-slice fan
-    // beam), or a source opposite each pixel (parallel beam); the tetrahedron
-    // beam's row v is row v % nvr of source v / nvr's band (T42/...TBCT_voxel.cu:23-40)
-    const float pu = fa(g.ymin, fm((float)u, g.du));
-    const float sy_ = g.ct_style == 2 ? pu : g.srcy;
-    const float x2x = fs(fm(g.srcx, c), fm(sy_, s));
-    const float x2y = fa(fm(g.srcx, s), fm(sy_, c));
-    const float x1x = fs(fm(g.dod, c), fm(pu, s));
-    const float x1y = fa(fm(g.dod, s), fm(pu, c));
-    const int src = g.ct_style == 3 ? v / g.nvr : 0;
-    const float x1z = fa(g.zmin, fm((float)(v - src * g.nvr), g.dv));
-    const float x2z = g.ct_style == 3 ? fa(g.zsrc0, fm((float)src, g.zsrc_dz)) : (g.ct_style == 0 ? g.srcz : x1z);
+    // source X2 and detector pixel centre X1 (universal.cu:21-45)
+    const RayEnds re = ray_ends(g, s, c, u, v);
+    const float x1x = re.x1x, x1y = re.x1y, x1z = re.x1z, x2x = re.x2x, x2y = re.x2y, x2z = re.x2z;
     const float dx = fs(x2x, x1x), dy = fs(x2y, x1y), dz = fs(x2z, x1z);
     const float ix = fdv(1.0f, dx), iy = fdv(1.0f, dy), iz = fdv(1.0f, dz);
-    r.d12 = __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));   // :290
+    r.d12 = ray_d12(re);   // :290
 
     // alpha_min / alpha_max (:77-104); PX[n+1] is plane n
     float a0, a1;
@@ -128,7 +118,10 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
     int i_min, i_max, j_min, j_max, k_min, k_max;
     bool hit;
     const bool zpar = fabsf(fs(x1z, x2z)) < fm(g.vz, 1e-6f);
-    const bool zpar_k = zpar && g.ct_style != 3;   // T42 has no z-parallel k range (T42/...TBCT_voxel.cu:171)
+    // T42 (T42/...TBCT_voxel.cu:171) and the multi-GPU build's slab projector
+    // (V63/kernel_IterativeRecon_universal_multiGPU.cu:775-800) have no
+    // z-parallel k range
+    const bool zpar_k = zpar && g.zpar_kr;
     if (!E64) {
         hit = !(amax <= amin);
         if (!hit) return r;
@@ -385,12 +378,17 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     const long long P = (long long)g.R * g.ZP;
     const long long p = (long long)w * P + (long long)v * g.R + u;
     double e2 = 0.0;
-    if (active) {
+    if (KIND == FP_PARTIAL && active && (v < g.row_lo || v >= g.row_hi)) {
+        // a fan-slice / parallel-beam slab traces only its band's rows (multiGPU.cu:663-667)
+        ((float2*)out)[p] = make_float2(0.0f, 0.0f);
+    } else if (active) {
         const float2 sc = g.trig[view0 + w];
         const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, KIND == FP_SART_OBJ>(
             g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v, vol2);
         const bool zero = rr.len < g.thr_fp;                       // :554
-        if (KIND == FP_FORWARD) {
+        if (KIND == FP_PARTIAL) {
+            ((float2*)out)[p] = make_float2(rr.sum, rr.len);           // multiGPU.cu:1146-1147, no threshold
+        } else if (KIND == FP_FORWARD) {
             st_any(out, p, out_dt, zero ? 0.0f : rr.sum);
         } else if (KIND == FP_SART || KIND == FP_SART_OBJ) {
             const float bv = ld_any(b, p, b_dt);
@@ -441,7 +439,7 @@ static void launch_fp_tl(const Geometry& G, const FpArgs& a, int nview, size_t s
 template <typename VT, int KIND, int BY, int CPM = 0, int MINB = 1>
 static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
-    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ) {
+    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_PARTIAL) {
         if (a.tiled) {
             launch_fp_tl<VT, KIND, BY, CPM, true, MINB>(G, a, nview, smem, st);
             return;
@@ -477,7 +475,7 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
     const DevGeom& g = G.dg;
     if (a.nview <= 0) return CTR_OK;
     if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
-    if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE && a.kind != FP_SART_OBJ)
+    if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE && a.kind != FP_SART_OBJ && a.kind != FP_PARTIAL)
         return set_error(CTR_ERR_UNSUPPORTED, "the tiled layout is for SART and objective projections");
     if (a.kind == FP_SART_OBJ && !a.vol2) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART_OBJ needs vol2");
     // the dot product keeps the fixed shape: its block partial sums, and so
@@ -493,6 +491,7 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
         case FP_SART: launch_fp_shape<VT, FP_SART>(G, a, smem, st); break;
         case FP_OBJECTIVE: launch_fp_shape<VT, FP_OBJECTIVE>(G, a, smem, st); break;
         case FP_SART_OBJ: launch_fp_shape<VT, FP_SART_OBJ>(G, a, smem, st); break;
+        case FP_PARTIAL: launch_fp_shape<VT, FP_PARTIAL>(G, a, smem, st); break;
         case FP_TRACE: launch_fp_t<VT, FP_TRACE, FP_BY>(G, a, a.nview, smem, st); break;
         case FP_DOT: launch_fp_t<VT, FP_DOT, FP_BY>(G, a, a.nview, smem, st); break;
         }

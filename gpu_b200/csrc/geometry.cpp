@@ -157,12 +157,24 @@ static ctr_status validate(const ctr_geometry_desc* d)
 
 using namespace ctr;
 
-extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geometry** out)
+// The whole volume (n_slabs = 1) or slab `slab` of the n_slabs-way z split of
+// the multi-GPU build.
+static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ctr_geometry** out)
 {
     clear_error();
     if (!out) return set_error(CTR_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     CTR_TRY(validate(din));
+    if (n_slabs < 1 || slab < 0 || slab >= n_slabs)
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "slab %d of %d", slab, n_slabs);
+    if (n_slabs > 1) {
+        if (din->flags & CTR_GEOM_TBCT)
+            return set_error(CTR_ERR_UNSUPPORTED, "the slab split is the cone/fan/parallel build's (not CTR_GEOM_TBCT)");
+        // V63/main_recon.cu:24: volume height and detector rows split evenly
+        if (din->nz % n_slabs != 0 || din->nv % n_slabs != 0)
+            return set_error(CTR_ERR_BAD_GEOMETRY, "nz=%d and nv=%d must both split into %d slabs", din->nz, din->nv,
+                             n_slabs);
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return set_error(CTR_ERR_NO_DEVICE, "no CUDA device");
@@ -205,6 +217,33 @@ extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geom
     q.bx = -d.vx * ((float)d.nx / 2.0f + (float)d.m_offset);
     q.by = -d.vy * ((float)d.ny / 2.0f);
     q.bz = -d.vz * ((float)d.nz / 2.0f);
+    // the slab of the multi-GPU build (V63/kernel_IterativeRecon_universal_multiGPU.cu):
+    // BOUNDARY_VOXEL_Z = boundary_voxel_z + volumn_z*ZETA/D*subVolIdx and ZETA/D
+    // slices in the projector (:636-637), the backprojector's voxel centre
+    // boundary_voxel_z + volumn_z*(ZETA/D*subVolIdx + 0.5f) + k*volumn_z (:1179)
+    q.slab_n = n_slabs;
+    q.slab_i = slab;
+    q.bz_ref = q.bz;
+    q.cz_off = d.vz * 0.5f;
+    q.ref_plus0 = 1;
+    q.zpar_kr = tbct ? 0 : 1;
+    q.row_lo = 0;
+    q.row_hi = q.ZP;
+    if (n_slabs > 1) {
+        const int zs = d.nz / n_slabs, k0 = zs * slab;
+        q.bz = q.bz_ref + d.vz * (float)d.nz / (float)n_slabs * (float)slab;
+        q.cz_off = d.vz * ((float)k0 + 0.5f);
+        q.ref_plus0 = 0;   // :1388-1391
+        q.zpar_kr = 0;     // :775-800
+        if (q.ct_style == 1 || q.ct_style == 2) {   // :663
+            q.row_lo = d.nv / n_slabs * slab;
+            q.row_hi = d.nv / n_slabs * (slab + 1);
+        }
+        d.nz = zs;
+        g->desc.nz = zs;
+        q.Z = zs;
+        q.max_steps = d.nx + d.ny + zs + 3;
+    }
     // Detector_Ymin / Detector_Zmin (main_recon.cu:83-84)
     q.ymin = -d.du * ((float)d.nu / 2.0f - 0.5f) + d.offset;
     q.zmin = -d.dv * ((float)d.nv / 2.0f - 0.5f);
@@ -370,6 +409,27 @@ fail:
     return st;
 }
 
+extern "C" ctr_status ctr_geometry_create(const ctr_geometry_desc* din, ctr_geometry** out)
+{
+    return create(din, 1, 0, out);
+}
+
+extern "C" ctr_status ctr_geometry_create_slab(const ctr_geometry_desc* din, int n_slabs, int slab,
+                                               ctr_geometry** out)
+{
+    return create(din, n_slabs, slab, out);
+}
+
+extern "C" ctr_status ctr_geometry_slab(const ctr_geometry* geom, int* n_slabs, int* slab, int* k0)
+{
+    if (!geom) return set_error(CTR_ERR_INVALID_ARGUMENT, "geometry is NULL");
+    const Geometry* g = reinterpret_cast<const Geometry*>(geom);
+    if (n_slabs) *n_slabs = g->dg.slab_n;
+    if (slab) *slab = g->dg.slab_i;
+    if (k0) *k0 = g->dg.Z * g->dg.slab_i;
+    return CTR_OK;
+}
+
 extern "C" ctr_status ctr_geometry_destroy(ctr_geometry* geom)
 {
     if (!geom) return CTR_OK;
@@ -386,6 +446,8 @@ extern "C" ctr_status ctr_geometry_destroy(ctr_geometry* geom)
     cudaFree(g->d_fdk);
     cudaFree(g->d_tiled);
     cudaFree(g->d_ramp);
+    cudaFree(g->d_parts);
+    for (Geometry* sg : g->slab_geoms) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(sg));
     delete g;
     return CTR_OK;
 }

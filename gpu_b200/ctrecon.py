@@ -38,6 +38,7 @@ GEOM_TBCT = 0x8
 SART_STOCHASTIC_ROUND = 0x1
 SART_TILED = 0x2
 SART_REFERENCE_BP = 0x4
+VOLUME_TILED = 0x8
 
 # every symbol include/ctrecon.h declares
 EXPORTED = [
@@ -53,7 +54,9 @@ EXPORTED = [
     "ctr_io_read_raw", "ctr_io_read_views", "ctr_io_write_views",
     "ctr_batch_create", "ctr_batch_destroy", "ctr_batch_set_sinogram", "ctr_batch_reset", "ctr_batch_iterate",
     "ctr_batch_get_volume", "ctr_geometry_set_shapes", "ctr_geometry_get_shapes", "ctr_geometry_autotune",
-    "ctr_solver_objectives",
+    "ctr_solver_objectives", "ctr_geometry_create_slab", "ctr_geometry_slab", "ctr_forward_partial",
+    "ctr_combine_partials", "ctr_sart_update", "ctr_sart_pass_slabs", "ctr_volume_tiling", "ctr_volume_tiled_count",
+    "ctr_set_default_devices",
 ]
 
 
@@ -152,6 +155,15 @@ def load_library(path: str = LIB_PATH):
         "ctr_batch_reset": ([vp, vp], i),
         "ctr_batch_iterate": ([vp, i, vp, vp], i),
         "ctr_batch_get_volume": ([vp, i, vp, vp], i),
+        "ctr_geometry_create_slab": ([C.POINTER(GeometryDesc), i, i, C.POINTER(C.c_void_p)], i),
+        "ctr_geometry_slab": ([G, C.POINTER(i), C.POINTER(i), C.POINTER(i)], i),
+        "ctr_forward_partial": ([G, vp, i, i, vp, u, vp], i),
+        "ctr_combine_partials": ([G, vp, i, i, vp, i, vp, vp], i),
+        "ctr_sart_update": ([G, vp, i, vp, i, f, u, C.c_uint32, vp], i),
+        "ctr_sart_pass_slabs": ([G, i, vp, i, vp, i, f, u, C.c_uint32, i, i, vp], i),
+        "ctr_volume_tiling": ([G, vp, vp, i, i, vp], i),
+        "ctr_volume_tiled_count": ([G, C.POINTER(C.c_int64)], i),
+        "ctr_set_default_devices": ([i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -221,13 +233,21 @@ def make_desc(nx, ny, nz, vx, nu, nv, du, dso, dod, n_views, us_rate=None, initi
 
 
 class Geometry:
-    """A scan geometry on the current CUDA device (``ctr_geometry``)."""
+    """A scan geometry on the current CUDA device (``ctr_geometry``).
 
-    def __init__(self, desc: GeometryDesc):
+    With ``n_slabs`` > 1: slab ``slab`` of the z split of the reference's
+    multi-GPU build (``ctr_geometry_create_slab``); its volumes are that slab's
+    nz/n_slabs slices."""
+
+    def __init__(self, desc: GeometryDesc, n_slabs: int = 1, slab: int = 0):
         self.lib = load_library()
         self.desc = desc
+        self.n_slabs, self.slab = n_slabs, slab
         h = C.c_void_p()
-        check(self.lib.ctr_geometry_create(C.byref(desc), C.byref(h)))
+        if n_slabs > 1:
+            check(self.lib.ctr_geometry_create_slab(C.byref(desc), n_slabs, slab, C.byref(h)))
+        else:
+            check(self.lib.ctr_geometry_create(C.byref(desc), C.byref(h)))
         self.h = h
 
     def close(self):
@@ -244,7 +264,12 @@ class Geometry:
     # shapes
     @property
     def vol_shape(self):
-        return (self.desc.nz, self.desc.ny, self.desc.nx)
+        return (self.desc.nz // self.n_slabs, self.desc.ny, self.desc.nx)
+
+    @property
+    def first_slice(self):
+        """Index in the whole volume of this geometry's first slice."""
+        return self.vol_shape[0] * self.slab
 
     @property
     def view_shape(self):
@@ -286,6 +311,42 @@ class Geometry:
                                       seed, view_begin, view_count, C.byref(fp) if timed else None,
                                       C.byref(bp) if timed else None, _stream(stream)))
         return (fp.value, bp.value) if timed else None
+
+    # z-slab SART of the multi-GPU build
+    def forward_partial(self, vol, view, part, flags=0, stream=None):
+        """part (rows, nu, 2) float32 <- this slab's (Sum(len*f), Sum(len)) per ray."""
+        check(self.lib.ctr_forward_partial(self.h, _ptr(vol), dtype_code(vol), view, _ptr(part), flags,
+                                           _stream(stream)))
+        return part
+
+    def combine_partials(self, parts, view, b_view, rays, stream=None):
+        """rays (rows, nu, 2) float32 <- (correction, d12) from parts (n, rows, nu, 2) in slab order."""
+        check(self.lib.ctr_combine_partials(self.h, _ptr(parts), parts.shape[0], view, _ptr(b_view),
+                                            dtype_code(b_view), _ptr(rays), _stream(stream)))
+        return rays
+
+    def sart_update(self, vol, rays, view, beta, flags=0, seed=0, stream=None):
+        check(self.lib.ctr_sart_update(self.h, _ptr(vol), dtype_code(vol), _ptr(rays), view, beta, flags, seed,
+                                       _stream(stream)))
+        return vol
+
+    def sart_pass_slabs(self, vol, sino, beta, n_slabs, view_begin=0, view_count=None, flags=0, seed=0,
+                        stream=None):
+        """The n_slabs-way slab SART on one GPU (vol: the whole volume)."""
+        n = self.n_views - view_begin if view_count is None else view_count
+        check(self.lib.ctr_sart_pass_slabs(self.h, n_slabs, _ptr(vol), dtype_code(vol), _ptr(sino),
+                                           dtype_code(sino), beta, flags, seed, view_begin, n, _stream(stream)))
+        return vol
+
+    def tiled_count(self):
+        n = C.c_int64()
+        check(self.lib.ctr_volume_tiled_count(self.h, C.byref(n)))
+        return n.value
+
+    def volume_tiling(self, src, dst, to_tiled=True, stream=None):
+        check(self.lib.ctr_volume_tiling(self.h, _ptr(src), _ptr(dst), dtype_code(src), int(to_tiled),
+                                         _stream(stream)))
+        return dst
 
     def forward_trace(self, vol, view, nseg, hsh, length, stream=None):
         check(self.lib.ctr_forward_trace(self.h, _ptr(vol), view, _ptr(nseg), _ptr(hsh), _ptr(length),
@@ -527,6 +588,11 @@ def read_views(directory, nu, nv, n_views, us_rate, initial_angle=0.0, tomo=0, r
 # The reference's host entry points (V63/host_*.c[u|pp]), same names and
 # argument meaning; host numpy arrays are updated in place like the reference.
 # ---------------------------------------------------------------------------
+
+def set_default_devices(n: int):
+    """Number_of_Devices of the reference build the host functions stand in for."""
+    check(load_library().ctr_set_default_devices(n))
+
 
 def set_default_geometry(desc: GeometryDesc):
     check(load_library().ctr_set_default_geometry(C.byref(desc)))

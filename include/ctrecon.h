@@ -201,6 +201,67 @@ ctr_status ctr_sart_views_noalloc(const ctr_geometry* geom, void* vol, ctr_dtype
                                   ctr_dtype sino_dtype, float beta, unsigned flags, uint32_t seed,
                                   int view_begin, int view_count, void* stream);
 
+/* ------------------------------------------- z-slab SART of the multi-GPU build */
+
+/* The reference's default build (V63/main_recon.cu:23, Number_of_Devices 4)
+ * splits the volume into D z-slabs, one per device, and runs each SART view
+ * as (V63/host_IterativeRecon_CBCT_multiGPU.c:1-161, kernels
+ * V63/kernel_IterativeRecon_universal_multiGPU.cu):
+ *   1. every slab projects its own voxels: partial ray sums (Sum(len*f),
+ *      Sum(len)), no threshold (forward_ray_driven_3d_kernel_correction_
+ *      separate, :591-1149), with the slab's own z planes
+ *      boundary_voxel_z + volumn_z*ZETA/D*s + n*volumn_z and ZETA/D slices;
+ *   2. the parts are added in slab order from zero and divided:
+ *      c = (b - Sum(len*f))/Sum(len), 0 below volumn_z*1e-6 (:1-19);
+ *   3. every slab backprojects c into its voxels (:1156-1402).
+ * The rounding differs from the one-device pass (a ray's sum is the sum of
+ * its slabs' sums; the slab planes are computed from the slab's boundary), so
+ * these calls reproduce the D-device build, not the one-device one.  ZETA and
+ * Z_prj must split evenly into D (V63/main_recon.cu:24); not for CTR_GEOM_TBCT.
+ *
+ * Slab s of D of a scan: a geometry of nz/D slices.  Volumes passed with it
+ * are that slab's nx*ny*(nz/D) voxels; its z planes, voxel centres and (for
+ * CTR_GEOM_FAN_SLICES / CTR_GEOM_PARALLEL) traced detector rows are the
+ * multi-GPU build's.  Not for the solver or FDK. */
+ctr_status ctr_geometry_create_slab(const ctr_geometry_desc* desc, int n_slabs, int slab, ctr_geometry** out);
+/* D (1 for a whole-volume geometry), s, and the slab's first slice in the volume. */
+ctr_status ctr_geometry_slab(const ctr_geometry* geom, int* n_slabs, int* slab, int* first_slice);
+
+/* Per-view calls of one slab, for a host that holds one slab per GPU and
+ * exchanges the parts itself (e.g. an all-gather over NCCL):
+ * ctr_forward_partial: part[p] = (Sum(len*f), Sum(len)) of ray p (2 floats per
+ *   ray, rows*nu rays) for view `view` of the slab volume;
+ * ctr_combine_partials: parts = n_parts such arrays back to back, in slab
+ *   order; writes the ray records rays[p] = (c, d12) (2 floats per ray) from
+ *   the view's measured data b_view (rows*nu values of b_dtype); any geometry
+ *   of the scan;
+ * ctr_sart_update: the slab's SART backprojection of those records,
+ *   vol += beta*Sum(w c)/Sum(w) (CTR_SART_REFERENCE_BP: the multi-GPU
+ *   backprojector's arithmetic, bit-exact with it; clear: the gather update
+ *   with the slab projector's own chords).
+ * CTR_VOLUME_TILED: vol is stored in the 8x8-tiled layout (ctr_volume_tiling)
+ * instead of [z][y][x]; the result is the same. */
+#define CTR_VOLUME_TILED 0x8u
+ctr_status ctr_forward_partial(const ctr_geometry* slab_geom, const void* vol, ctr_dtype vol_dtype, int view,
+                               float* part, unsigned flags, void* stream);
+ctr_status ctr_combine_partials(const ctr_geometry* geom, const float* parts, int n_parts, int view,
+                                const void* b_view, ctr_dtype b_dtype, float* rays, void* stream);
+ctr_status ctr_sart_update(const ctr_geometry* slab_geom, void* vol, ctr_dtype vol_dtype, const float* rays,
+                           int view, float beta, unsigned flags, uint32_t seed, void* stream);
+/* The D-slab SART over views [view_begin, view_begin+view_count) on one GPU:
+ * geom is the whole-volume geometry, vol the whole volume ([z][y][x], the D
+ * slabs back to back); flags as ctr_sart_pass.  Its slab geometries are kept
+ * with geom. */
+ctr_status ctr_sart_pass_slabs(const ctr_geometry* geom, int n_slabs, void* vol, ctr_dtype vol_dtype,
+                               const void* sino, ctr_dtype sino_dtype, float beta, unsigned flags, uint32_t seed,
+                               int view_begin, int view_count, void* stream);
+/* Layout conversion between [z][y][x] and the 8x8-tiled layout of the
+ * projectors (to_tiled = 1: src linear, dst tiled); dst holds
+ * ctr_volume_tiled_count elements when tiled. */
+ctr_status ctr_volume_tiling(const ctr_geometry* geom, const void* src, void* dst, ctr_dtype dtype, int to_tiled,
+                             void* stream);
+ctr_status ctr_volume_tiled_count(const ctr_geometry* geom, int64_t* count);
+
 /* Trace one view: per ray, the number of Siddon segments, an FNV-1a hash of
  * the visited voxel index sequence and the summed chord length.  For parity
  * checks of the traversal (the voxel index set of every ray). */
@@ -379,6 +440,12 @@ ctr_status ctr_io_write_views(const char* dir, int nu, int nv, int n_views, floa
  * (pinned or pageable) or device pointers, copy in and out like the reference,
  * and report failures through ctr_last_error_string(). */
 ctr_status ctr_set_default_geometry(const ctr_geometry_desc* desc);
+/* Number_of_Devices of the reference build being replaced (V63/main_recon.cu:23,
+ * default 1).  With n > 1 Reconstruction_3D_ray_driven_CBCT and
+ * CheckMatchedJointOperator compute what the n-device build computes (the
+ * z-slab sequence above, on the current GPU); Forward_3D_ray_driven_siddon's
+ * row split gives the one-device projections already. */
+ctr_status ctr_set_default_devices(int n);
 
 /* V63/host_IterativeRecon_CBCT.c:70-128: A x for all views into h_proj_data. */
 void Forward_3D_ray_driven_siddon(float* h_volume, float* h_proj_data);

@@ -68,6 +68,28 @@ int og_init(og_geom* g, const og_desc* d)
     } else if (e->ct_style < 0 || e->ct_style > 3) {
         return -1;
     }
+    g->k0 = 0;
+    g->bz_ref = g->bz;
+    g->zpar_kr = e->ct_style != 3;
+    g->row_lo = 0;
+    g->row_hi = g->rows;
+    if (e->n_slabs > 1) {
+        /* slab subVolIdx of the multi-GPU build: ZETA/D slices, its own
+         * BOUNDARY_VOXEL_Z and ZETA_new in every z plane of the traversal, no
+         * z-parallel k range (V63/kernel_IterativeRecon_universal_multiGPU.cu:
+         * 636-637,686-687,775-800,891); fan-slice and parallel beams trace only the rows of
+         * the slab's band (:663).  ZETA and Z_prj split evenly (V63/main_recon.cu:24). */
+        const int D = e->n_slabs, sl = e->slab, Z = e->nz;
+        if (e->ct_style == 3 || sl < 0 || sl >= D || Z % D != 0 || e->nv % D != 0) return -1;
+        g->d.nz = Z / D;
+        g->k0 = Z / D * sl;
+        g->bz = g->bz_ref + e->vz * (float)Z / (float)D * (float)sl;
+        g->zpar_kr = 0;
+        if (e->ct_style == 1 || e->ct_style == 2) {
+            g->row_lo = e->nv / D * sl;
+            g->row_hi = e->nv / D * (sl + 1);
+        }
+    }
     return 0;
 }
 
@@ -143,7 +165,7 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
      * no special k range for rays parallel to the z planes (:171) and the
      * loop test alpha_max - alpha_c > 1e-6f (:282) */
     const int tb = g->d.ct_style == 3;
-    const int zpar_k = !tb && fabsf(x1z - x2z) < g->d.vz * 1e-6f;
+    const int zpar_k = g->zpar_kr && fabsf(x1z - x2z) < g->d.vz * 1e-6f;
 
     const float ix = 1.0f / (x2x - x1x);   /* :48-50 */
     const float iy = 1.0f / (x2y - x1y);
@@ -659,7 +681,9 @@ void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float b
                 const long long idx = (long long)M * N * k + (long long)M * j + i;
                 const float cx = g->bx + vx * 0.5f + (float)i * vx;     /* :592-594 */
                 const float cy = g->by + vy * 0.5f + (float)j * vy;
-                const float cz = g->bz + vz * 0.5f + (float)k * vz;
+                /* :592-594; a slab's voxel centre, multiGPU.cu:1179 (k0 = 0,
+                 * bz_ref = bz otherwise: vz*(0.0f+0.5f) = vz*0.5f) */
+                const float cz = g->bz_ref + vz * ((float)g->k0 + 0.5f) + (float)k * vz;
                 float sw = 0.0f, sl = 0.0f;
                 if (!og_fov_masked(g, i, j)) {
                     float minY = INFINITY, minZ = INFINITY, maxY = -INFINITY, maxZ = -INFINITY;
@@ -729,7 +753,9 @@ void og_backproject_ref(const og_geom* g, float* vol, const float* corr, float b
                             }
                     }
                 }
-                if (sl < vx * 1e-6f) vol[idx] += 0.0f;                         /* :799-807 */
+                if (sl < vx * 1e-6f) {                                         /* :799-807 */
+                    if (g->d.n_slabs <= 1) vol[idx] += 0.0f;                   /* none in multiGPU.cu:1388-1391 */
+                }
                 else if (command == 0) vol[idx] = sw;
                 else vol[idx] += beta * sw / sl;
             }
@@ -1423,12 +1449,26 @@ void og_backproject_gather(const og_geom* g, float* vol, const float* corr, floa
                             minZ = fminf(minZ, oz); maxZ = fmaxf(maxZ, oz);
                         }
                 int u0 = (int)floorf((minY - g->ymin) * inv_du + 0.5f), u1 = (int)floorf((maxY - g->ymin) * inv_du + 0.5f);
-                int v0 = (int)floorf((minZ - g->zmin) * inv_dv + 0.5f), v1 = (int)floorf((maxZ - g->zmin) * inv_dv + 0.5f);
+                int v0, v1;
+                if (g->d.ct_style == 0) {
+                    v0 = (int)floorf((minZ - g->zmin) * inv_dv + 0.5f);
+                    v1 = (int)floorf((maxZ - g->zmin) * inv_dv + 0.5f);
+                } else {
+                    /* rays in z planes: the rows of the cell's z span (a row on a
+                     * cell plane belongs to the cell above; the centre alone can
+                     * miss it when the voxel is taller than a row or the row sits
+                     * on the slab's edge) */
+                    v0 = (int)floorf((og_plane(vz, k, g->bz) - g->zmin) * inv_dv + 0.5f);
+                    v1 = (int)floorf((og_plane(vz, k + 1, g->bz) - g->zmin) * inv_dv + 0.5f);
+                }
+                /* widen by one row each side before the range test: the engine's
+                 * row range is any superset of the rows with a positive chord */
+                v0 -= 1;
+                v1 += 1;
                 if ((u0 < 0 && u1 < 0) || (u0 > R - 1 && u1 > R - 1) || (v0 < 0 && v1 < 0) || (v0 > ZP - 1 && v1 > ZP - 1))
                     continue;
-                /* widen by one row each side: the engine's row range is any superset */
-                v0 = v0 - 1 < 0 ? 0 : v0 - 1;
-                v1 = v1 + 1 > ZP - 1 ? ZP - 1 : v1 + 1;
+                v0 = v0 < 0 ? 0 : v0;
+                v1 = v1 > ZP - 1 ? ZP - 1 : v1;
                 u0 = u0 < 0 ? 0 : u0;
                 u1 = u1 > R - 1 ? R - 1 : u1;
                 const float xlo = og_plane(vx, i, g->bx), xhi = og_plane(vx, i + 1, g->bx);
@@ -1469,4 +1509,68 @@ void og_sart_pass_gather(const og_geom* g, float* vol, const float* sino, float 
         og_backproject_gather(g, vol, corr, beta, s, c);
     }
     free(corr);
+}
+
+/* ------------------------------------------------------------------------ */
+/* z-slab SART of the multi-GPU build                                       */
+/* (V63/host_IterativeRecon_CBCT_multiGPU.c:1-161)                          */
+/* ------------------------------------------------------------------------ */
+void og_forward_partial(const og_geom* g, const float* vol, float s, float c, float* wsum, float* lsum)
+{
+    const int R = g->d.nu, ZP = g->rows;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int v = 0; v < ZP; ++v)
+        for (int u = 0; u < R; ++u) {
+            float len = 0.0f, sum = 0.0f;
+            if (v >= g->row_lo && v < g->row_hi) sum = og_fp_ray(g, vol, s, c, u, v, 0, &len, NULL, NULL);
+            wsum[(long long)v * R + u] = sum;                 /* multiGPU.cu:1146-1147 */
+            lsum[(long long)v * R + u] = len;
+        }
+}
+
+void og_combine_partials(const og_geom* g, int n_parts, const float* wsum, const float* lsum, const float* b,
+                         float* corr)
+{
+    const long long P = (long long)g->d.nu * g->rows;
+    const float thr = g->d.vz * 1e-6f;
+    for (long long p = 0; p < P; ++p) {
+        float w = 0.0f, l = 0.0f;                              /* memset, multiGPU.c:82-83 */
+        for (int i = 0; i < n_parts; ++i) {                    /* kernel_add_proj, multiGPU.cu:1-5 */
+            w = w + wsum[(long long)i * P + p];
+            l = l + lsum[(long long)i * P + p];
+        }
+        corr[p] = l < thr ? 0.0f : (b[p] - w) * 1.0f / l;      /* kernel_divide_proj, :7-19 */
+    }
+}
+
+int og_sart_pass_slabs(const og_desc* d, float* vol, const float* sino, float beta, int v0, int nv, int engine)
+{
+    const int D = d->n_slabs < 1 ? 1 : d->n_slabs;
+    og_geom* gs = (og_geom*)calloc((size_t)D, sizeof(og_geom));
+    for (int i = 0; i < D; ++i) {
+        og_desc e = *d;
+        e.n_slabs = D;
+        e.slab = i;
+        if (og_init(&gs[i], &e) != 0) {
+            free(gs);
+            return -1;
+        }
+    }
+    const long long P = (long long)gs[0].d.nu * gs[0].rows;
+    const long long Vs = (long long)gs[0].d.nx * gs[0].d.ny * gs[0].d.nz;
+    float* w = (float*)malloc(sizeof(float) * P * D);
+    float* l = (float*)malloc(sizeof(float) * P * D);
+    float* corr = (float*)malloc(sizeof(float) * P);
+    for (int j = v0; j < v0 + nv; ++j) {
+        float s, c;
+        og_view_trig(&gs[0], j, 0, &s, &c);
+        for (int i = 0; i < D; ++i) og_forward_partial(&gs[i], vol + Vs * i, s, c, w + P * i, l + P * i);
+        og_combine_partials(&gs[0], D, w, l, sino + P * j, corr);
+        for (int i = 0; i < D; ++i) {
+            if (engine) og_backproject_gather(&gs[i], vol + Vs * i, corr, beta, s, c);
+            else og_backproject_ref(&gs[i], vol + Vs * i, corr, beta, s, c, 1);
+        }
+    }
+    free(w); free(l); free(corr); free(gs);
+    return 0;
 }

@@ -51,6 +51,10 @@ typedef struct og_desc {
                              /* 3: tetrahedron beam (TBCT v4.2, below)       */
     int   n_sources;         /* ct_style 3: N_source, sources along z, each  */
                              /* with its own band of nv detector rows        */
+    int   n_slabs;           /* > 1: the z-slab split of the multi-GPU SART  */
+                             /* (V63 Number_of_Devices): this description is */
+    int   slab;              /* slab `slab` (subVolIdx) of n_slabs, nz/n_slabs*/
+                             /* slices of the nz-slice volume; 0/1: no split  */
 } og_desc;
 
 /* Derived constants, computed with the reference's float/double steps. */
@@ -64,6 +68,16 @@ typedef struct og_geom {
     float zsrc0, zsrc_dz;           /* Source_z_min, Source_interval (:95-108) */
     int   rows;                     /* detector rows of one view: nv, or     */
                                     /* nv * n_sources for ct_style 3          */
+    /* Slab geometry (n_slabs > 1): d.nz is the slab's ZETA/D slices, bz its
+     * BOUNDARY_VOXEL_Z = boundary_voxel_z + volumn_z*ZETA/D*subVolIdx
+     * (V63/kernel_IterativeRecon_universal_multiGPU.cu:636-637) and k0 the
+     * whole volume's index of its first slice; otherwise k0 = 0, bz_ref = bz. */
+    int   k0;
+    float bz_ref;                   /* boundary_voxel_z of the whole volume  */
+    int   zpar_kr;                  /* the z-parallel k range of :172-178     */
+                                    /* applies (not T42's, not a slab's)      */
+    int   row_lo, row_hi;           /* CT_style 1/2 slab: rows of its band    */
+                                    /* (multiGPU.cu:663); else 0, rows        */
 } og_geom;
 
 int  og_init(og_geom* g, const og_desc* d);
@@ -124,9 +138,32 @@ void og_sart_pass_matched(const og_geom* g, float* vol, const float* sino, float
 void og_sart_pass_f64(const og_geom* g, double* vol, const double* sino, double beta);
 /* the engine's gather SART update: reference BP semantics (candidate
  * rectangle, FOV mask, thresholds) with every alpha evaluated the Siddon
- * projector's way, float sums in the engine's pair order */
+ * projector's way, float sums in the engine's pair order.  The candidate
+ * rows are a superset of the rows with a positive chord (the cone beam's
+ * rectangle, the fan-slice / parallel beams' rows of the cell's z span, each
+ * widened by a row), so they do not change the sums. */
 void og_backproject_gather(const og_geom* g, float* vol, const float* corr, float beta, float s, float c);
 void og_sart_pass_gather(const og_geom* g, float* vol, const float* sino, float beta);
+
+/* ---- z-slab SART of the multi-GPU build (V63/host_IterativeRecon_CBCT_multiGPU.c:1-161,
+ *      kernels V63/kernel_IterativeRecon_universal_multiGPU.cu:1-19,591-1402) ----
+ * On a slab geometry: the slab's partial ray sums, Sum(len*f) -> wsum and
+ * Sum(len) -> lsum, with no threshold (forward_ray_driven_3d_kernel_
+ * correction_separate); og_backproject_ref on a slab geometry is
+ * backprj_ray_driven_3d_kernel_multiGPU (its voxel centres, no "+= 0"). */
+void og_forward_partial(const og_geom* g, const float* vol, float s, float c, float* wsum, float* lsum);
+/* The host's combination (multiGPU.c:82-95): both sums start from 0 and add
+ * the parts in slab order (kernel_add_proj), then kernel_divide_proj:
+ * corr = 0 where Sum(len) < volumn_z*1e-6f, else (b - Sum(len*f))*1.0f/Sum(len).
+ * wsum, lsum: [n_parts][rows*R]. */
+void og_combine_partials(const og_geom* g, int n_parts, const float* wsum, const float* lsum, const float* b,
+                         float* corr);
+/* Views [v0, v0+nv) of the slab SART pass on the whole volume vol; d is the
+ * whole scan with n_slabs = D (its slab field is ignored).  engine = 0: the
+ * multi-GPU backprojector's arithmetic; 1: the engine's gather update
+ * (og_backproject_gather) on each slab geometry.  Returns -1 if d does not
+ * split into D slabs. */
+int og_sart_pass_slabs(const og_desc* d, float* vol, const float* sino, float beta, int v0, int nv, int engine);
 
 /* ---- FGP TV prox, 7-array GPU form (V63/kernel_FGP_Denoise_GPUx7.cu:2-88,
  *      driver V63/host_FGP_Denoise_GPUx7.c:1-111) ---- */

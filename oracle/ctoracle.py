@@ -39,6 +39,7 @@ class OgDesc(C.Structure):
         ("offset", C.c_float), ("m_offset", C.c_int),
         ("us_rate", C.c_float), ("initial_angle", C.c_float), ("shift_angle", C.c_float),
         ("ct_style", C.c_int), ("n_sources", C.c_int),
+        ("n_slabs", C.c_int), ("slab", C.c_int),
     ]
 
 
@@ -50,6 +51,7 @@ class OgGeom(C.Structure):
         ("ymin", C.c_float), ("zmin", C.c_float),
         ("srcx", C.c_float), ("srcy", C.c_float), ("srcz", C.c_float),
         ("zmax", C.c_float), ("zsrc0", C.c_float), ("zsrc_dz", C.c_float), ("rows", C.c_int),
+        ("k0", C.c_int), ("bz_ref", C.c_float), ("zpar_kr", C.c_int), ("row_lo", C.c_int), ("row_hi", C.c_int),
     ]
 
 
@@ -66,6 +68,16 @@ def make_desc(nx, ny, nz, nu, nv, nviews, vx, du, dso, dod, us_rate=None,
     return OgDesc(nx, ny, nz, nu, nv, nviews, vx, vx, vz, du, du, dso, dod,
                   offset, m_offset, us_rate, initial_angle, shift_angle, ct_style,
                   n_sources if ct_style == 3 else 0)
+
+
+def slab_desc(desc: OgDesc, n_slabs: int, slab: int) -> OgDesc:
+    """The description of slab ``slab`` of the ``n_slabs``-way z split of the
+    multi-GPU build (its kernels take the whole scan's constants plus the
+    device index)."""
+    d = OgDesc()
+    C.pointer(d)[0] = desc
+    d.n_slabs, d.slab = n_slabs, slab
+    return d
 
 
 def build():
@@ -118,6 +130,9 @@ class Oracle:
             "og_fdk": [G, _f32p, _f32p],
             "og_phantom_voxelize": [G, _f64p, i, _f32p],
             "og_phantom_project": [G, _f64p, i, d, d, _f32p],
+            "og_forward_partial": [G, _f32p, f, f, _f32p, _f32p],
+            "og_combine_partials": [G, i, _f32p, _f32p, _f32p, _f32p],
+            "og_sart_pass_slabs": [C.POINTER(OgDesc), _f32p, _f32p, f, i, i, i],
         }
         for name, args in sig.items():
             getattr(lib, name).argtypes = args
@@ -233,6 +248,32 @@ class Oracle:
         self.lib.og_sart_pass_f64(self.gp, vol, np.ascontiguousarray(sino, np.float64), beta)
         return vol
 
+    def forward_partial(self, vol, view):
+        """On a slab description: the slab's (Sum(len*f), Sum(len)) per ray."""
+        s, c = self.trig(view)
+        w = np.zeros(self.view_shape, np.float32)
+        ln = np.zeros(self.view_shape, np.float32)
+        self.lib.og_forward_partial(self.gp, np.ascontiguousarray(vol, np.float32), s, c, w, ln)
+        return w, ln
+
+    def combine_partials(self, wsum, lsum, b):
+        """The SART correction of the parts [n_parts][rows][R], added in order."""
+        wsum = np.ascontiguousarray(wsum, np.float32)
+        out = np.zeros(self.view_shape, np.float32)
+        self.lib.og_combine_partials(self.gp, wsum.shape[0], wsum, np.ascontiguousarray(lsum, np.float32),
+                                     np.ascontiguousarray(b, np.float32), out)
+        return out
+
+    def sart_pass_slabs(self, vol, sino, beta, n_slabs, v0=0, nv=None, engine=False):
+        """Views [v0, v0+nv) of the n_slabs-way slab SART on the whole volume."""
+        nv = self.desc.nviews - v0 if nv is None else nv
+        vol = np.ascontiguousarray(vol, np.float32).copy()
+        d = slab_desc(self.desc, n_slabs, 0)
+        if self.lib.og_sart_pass_slabs(C.byref(d), vol, np.ascontiguousarray(sino, np.float32), beta, v0, nv,
+                                       int(engine)) != 0:
+            raise ValueError("the scan does not split into %d slabs" % n_slabs)
+        return vol
+
     def fgp(self, f, lam, iters):
         d = self.desc
         out = np.zeros(self.vol_shape, np.float32)
@@ -328,6 +369,11 @@ class RefOracle:
             "ref_fdk_weight": [_f32p, _f32p, i],
             "ref_ramp_filter": [_f32p, _f32p, i],
             "ref_fdk_bp_view": [_f32p, _f32p, f, f],
+            "ref_slab_forward_view": [i, i, _f32p, _f32p, _f32p, f, f],
+            "ref_combine_view": [i, _f32p, _f32p, _f32p, _f32p],
+            "ref_slab_backproject_view": [i, i, _f32p, _f32p, f, f, f, i],
+            "ref_sart_views_slabs": [i, _f32p, _f32p, f, i, i],
+            "ref_forward_view_split": [i, _f32p, _f32p, f, f],
         }
         for name, args in sig.items():
             if hasattr(lib, name):   # the tetrahedron-beam build has the projectors only
@@ -378,6 +424,55 @@ class RefOracle:
         vol = np.ascontiguousarray(vol, np.float32).copy()
         self.lib.ref_sart_views(vol, np.ascontiguousarray(sino, np.float32), beta, v0, nv)
         return vol
+
+    # the multi-GPU build with Number_of_Devices = D (volume: the D slabs back to back)
+    def _slab_vol(self, D):
+        d = self.desc
+        return (d.nz // D, d.ny, d.nx)
+
+    def slab_forward_view(self, vol_slab, D, sub, view):
+        """forward_ray_driven_3d_kernel_correction_separate: (weightedLen, sumLen)."""
+        self._set()
+        s, c = self.trig(view)
+        w = np.zeros(self.view_shape, np.float32)
+        ln = np.zeros(self.view_shape, np.float32)
+        if self.lib.ref_slab_forward_view(D, sub, np.ascontiguousarray(vol_slab, np.float32), ln, w, s, c) != 0:
+            raise ValueError("no %d-way split" % D)
+        return w, ln
+
+    def combine_view(self, wsum, lsum, b):
+        self._set()
+        wsum = np.ascontiguousarray(wsum, np.float32)
+        out = np.zeros(self.view_shape, np.float32)
+        if self.lib.ref_combine_view(wsum.shape[0], np.ascontiguousarray(lsum, np.float32), wsum,
+                                     np.ascontiguousarray(b, np.float32), out) != 0:
+            raise ValueError("no split")
+        return out
+
+    def slab_backproject_view(self, vol_slab, corr, D, sub, view, beta=1.0, command=1):
+        self._set()
+        s, c = self.trig(view)
+        vol = np.ascontiguousarray(vol_slab, np.float32).copy()
+        if self.lib.ref_slab_backproject_view(D, sub, vol, np.ascontiguousarray(corr, np.float32), beta, s, c,
+                                              command) != 0:
+            raise ValueError("no %d-way split" % D)
+        return vol
+
+    def sart_slabs(self, vol, sino, beta, D, v0=0, nv=None):
+        self._set()
+        nv = self.desc.nviews - v0 if nv is None else nv
+        vol = np.ascontiguousarray(vol, np.float32).copy()
+        if self.lib.ref_sart_views_slabs(D, vol, np.ascontiguousarray(sino, np.float32), beta, v0, nv) != 0:
+            raise ValueError("no %d-way split" % D)
+        return vol
+
+    def forward_view_split(self, vol, D, view):
+        self._set()
+        s, c = self.trig(view)
+        out = np.zeros(self.view_shape, np.float32)
+        if self.lib.ref_forward_view_split(D, np.ascontiguousarray(vol, np.float32), out, s, c) != 0:
+            raise ValueError("no %d-way split" % D)
+        return out
 
     def fgp(self, f, lam, iters):
         self._set()

@@ -17,6 +17,11 @@
  * abbreviated T42/, read from REF_TBCT_DIR; output oracle/_ref/libctref_tbct.so).
  * Its atomicAdd becomes a plain add: a voxel's sources are launched in
  * ascending order by one thread.
+ *
+ * The CBCT builds also run the multi-GPU build's kernels
+ * (V63/kernel_IterativeRecon_universal_multiGPU.cu) with its host sequence
+ * (V63/host_IterativeRecon_CBCT_multiGPU.c): the devices become a loop over
+ * the slabs in device order, Number_of_Devices a global set per call.
  */
 #include <cmath>
 #include <complex>
@@ -68,7 +73,10 @@ static inline float atomicAdd(float* p, float v)
 }
 #include REF_STR(REF_TBCT_DIR/voxel/kernel_IterativeRecon_TBCT_voxel.cu)
 #else
+/* the multi-GPU build's device count (V63/main_recon.cu:23), set per call */
+static int Number_of_Devices = 1;
 #include REF_STR(REF_DIR/kernel_IterativeRecon_universal.cu)
+#include REF_STR(REF_DIR/kernel_IterativeRecon_universal_multiGPU.cu)
 #include REF_STR(REF_DIR/kernel_FGP_Denoise_GPUx7.cu)
 #include REF_STR(REF_DIR/kernel_tool_functions.cu)
 #include REF_STR(REF_DIR/FDK/kernel_FDK.cu)
@@ -251,6 +259,128 @@ void ref_sart_views(float* vol, const float* sino, float beta, int v0, int nv)
         ref_backproject_view(vol, corr, beta, s, c, 1);
     }
     free(corr);
+}
+
+/* ---- the multi-GPU build (Number_of_Devices = D > 1) ---- */
+static int ref_devices(int D)
+{
+    if (D < 1 || ZETA % D != 0 || Z_prj % D != 0) return -1;
+    Number_of_Devices = D;
+    return 0;
+}
+
+/* forward_ray_driven_3d_kernel_correction_separate over grid (1, Z_prj) x block R
+ * on the slab volume sub (V63/host_IterativeRecon_CBCT_multiGPU.c:71-75) */
+int ref_slab_forward_view(int D, int sub, const float* vol_slab, float* sumLen, float* weightedLen, float s, float c)
+{
+    if (ref_devices(D) != 0) return -1;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int v = 0; v < Z_prj; ++v) {
+        tl_blockDim = {(unsigned)R, 1, 1};
+        tl_gridDim = {1, (unsigned)Z_prj, 1};
+        for (int u = 0; u < R; ++u) {
+            tl_blockIdx = {0, (unsigned)v, 0};
+            tl_threadIdx = {(unsigned)u, 0, 0};
+            forward_ray_driven_3d_kernel_correction_separate((float*)vol_slab, sumLen, weightedLen, s, c, sub);
+        }
+    }
+    return 0;
+}
+
+/* the host's combination of the D parts, [D][Z_prj*R] each
+ * (V63/host_IterativeRecon_CBCT_multiGPU.c:82-95): memset, kernel_add_proj per
+ * device in order (weighted, then lengths), kernel_divide_proj */
+int ref_combine_view(int D, const float* sumLen, const float* weightedLen, const float* b, float* corr)
+{
+    if (ref_devices(D) != 0) return -1;
+    const long long P = (long long)R * Z_prj;
+    float* hs = (float*)calloc(P, sizeof(float));
+    float* hw = (float*)calloc(P, sizeof(float));
+    auto grid = [&](auto&& fn) {
+        tl_blockDim = {(unsigned)R, 1, 1};
+        tl_gridDim = {1, (unsigned)Z_prj, 1};
+        for (int v = 0; v < Z_prj; ++v)
+            for (int u = 0; u < R; ++u) {
+                tl_blockIdx = {0, (unsigned)v, 0};
+                tl_threadIdx = {(unsigned)u, 0, 0};
+                fn();
+            }
+    };
+    for (int i = 0; i < D; ++i) {
+        grid([&] { kernel_add_proj(hw, (float*)weightedLen + P * i); });
+        grid([&] { kernel_add_proj(hs, (float*)sumLen + P * i); });
+    }
+    grid([&] { kernel_divide_proj(corr, (float*)b, hs, hw); });
+    free(hs);
+    free(hw);
+    return 0;
+}
+
+/* backprj_ray_driven_3d_kernel_multiGPU over grid (1, N, ZETA/D) x block M */
+int ref_slab_backproject_view(int D, int sub, float* vol_slab, const float* corr, float beta, float s, float c,
+                              int command)
+{
+    if (ref_devices(D) != 0) return -1;
+    const int Zs = ZETA / D;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = 0; k < Zs; ++k)
+        for (int j = 0; j < N; ++j) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            tl_gridDim = {1, (unsigned)N, (unsigned)Zs};
+            for (int i = 0; i < M; ++i) {
+                tl_blockIdx = {0, (unsigned)j, (unsigned)k};
+                tl_threadIdx = {(unsigned)i, 0, 0};
+                backprj_ray_driven_3d_kernel_multiGPU(vol_slab, (float*)corr, beta, s, c, sub, command);
+            }
+        }
+    return 0;
+}
+
+/* Reconstruction_3D_ray_driven_CBCT of the multi-GPU build
+ * (V63/host_IterativeRecon_CBCT_multiGPU.c:1-161) for the views [v0, v0+nv):
+ * the volume is the D slabs back to back (:40-44) */
+int ref_sart_views_slabs(int D, float* vol, const float* sino, float beta, int v0, int nv)
+{
+    if (ref_devices(D) != 0) return -1;
+    const long long P = (long long)R * Z_prj, Vs = (long long)M * N * (ZETA / D);
+    float* sl = (float*)calloc(P * D, sizeof(float));
+    float* wl = (float*)calloc(P * D, sizeof(float));
+    float* corr = (float*)malloc(sizeof(float) * P);
+    for (int j = v0; j < v0 + nv; ++j) {
+        float s, c;
+        ref_view_trig(j, 0, &s, &c);
+        for (int i = 0; i < D; ++i) ref_slab_forward_view(D, i, vol + Vs * i, sl + P * i, wl + P * i, s, c);
+        ref_combine_view(D, sl, wl, sino + P * j, corr);
+        for (int i = 0; i < D; ++i) ref_slab_backproject_view(D, i, vol + Vs * i, corr, beta, s, c, 1);
+    }
+    free(sl);
+    free(wl);
+    free(corr);
+    return 0;
+}
+
+/* Forward_3D_ray_driven_siddon of the multi-GPU build, one view
+ * (V63/host_IterativeRecon_CBCT_multiGPU.c:171-258): device i projects rows
+ * [Z_prj/D*i, Z_prj/D*(i+1)) of the whole volume with
+ * forward_ray_driven_3d_kernel_correction_multiGPU, command 0 */
+int ref_forward_view_split(int D, const float* vol, float* out, float s, float c)
+{
+    if (ref_devices(D) != 0) return -1;
+    const int rows = Z_prj / D;
+    for (int i = 0; i < D; ++i) {
+        float* part = out + (long long)R * rows * i;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int v = 0; v < rows; ++v) {
+            tl_blockDim = {(unsigned)R, 1, 1};
+            tl_gridDim = {1, (unsigned)rows, 1};
+            for (int u = 0; u < R; ++u) {
+                tl_blockIdx = {0, (unsigned)v, 0};
+                tl_threadIdx = {(unsigned)u, 0, 0};
+                forward_ray_driven_3d_kernel_correction_multiGPU((float*)vol, part, part, s, c, i, 0);
+            }
+        }
+    }
+    return 0;
 }
 
 /* FGP_denoise_GPUx7_exact (V63/host_FGP_Denoise_GPUx7.c:1-111), in place */

@@ -62,6 +62,27 @@ TBCT = {
 }
 
 
+# The multi-GPU build's z split (V63/main_recon.cu:23 Number_of_Devices): nz
+# and nv split into each listed slab count.  "cone_wide": a wide cone
+# (magnification 2, +-8 degrees), so rays cross slab boundaries and a ray's
+# sum is the sum of its slabs' sums; "pitch07": a voxel pitch whose slab
+# planes round differently from the whole volume's, and an odd detector whose
+# central row's rays lie in a z plane; "fan_edges": fan-slice rows lying
+# exactly on slab boundary planes (traced by neither slab); "parallel_slabs":
+# the parallel beam.
+SLABS = {
+    "cube16": dict(SMALL["cube16"], slabs=[2, 4]),
+    "cone_wide": dict(nx=16, ny=16, nz=16, nu=24, nv=24, nviews=10, vx=1.0, du=1.0, dso=40.0, dod=-40.0,
+                      initial_angle=1.0, slabs=[2, 4]),
+    "pitch07": dict(nx=14, ny=14, nz=12, nu=22, nv=15, nviews=8, vx=0.7, du=1.3, dso=1000.0, dod=-500.0,
+                    initial_angle=2.0, slabs=[3]),
+    "fan_edges": dict(nx=12, ny=12, nz=12, nu=17, nv=9, nviews=8, vx=1.0, du=1.6, dso=1000.0, dod=-500.0,
+                      initial_angle=3.5, ct_style=1, slabs=[3]),
+    "parallel_slabs": dict(nx=16, ny=16, nz=12, nu=24, nv=12, nviews=12, vx=1.0, du=1.2, dso=1000.0, dod=-500.0,
+                           ct_style=2, slabs=[2, 4]),
+}
+
+
 def og_desc(cfg):
     from oracle.ctoracle import make_desc
     return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["nu"], cfg["nv"], cfg["nviews"], cfg["vx"], cfg["du"],
