@@ -44,6 +44,9 @@ def parse():
                    help="with --profile-views: also run two FP16 solver iterations (the second in steady state)")
     p.add_argument("--profile-refbp", action="store_true",
                    help="with --profile-views: the SART updates with the reference backprojector's arithmetic")
+    p.add_argument("--profile-slabs", type=int, default=0,
+                   help="short run for ncu: N views of the 4-slab SART (the reference's default 4-device build) "
+                        "on the 512^3 scan, FP32, its backprojection arithmetic, tiled")
     p.add_argument("--profile-fdk", type=int, default=0,
                    help="profiling mode: FDK of the 512^3 scan restricted to this many views (weighting, ramp "
                         "and backprojection), print timings, exit")
@@ -319,6 +322,32 @@ def profile_fdk(args):
     torch.cuda.synchronize()
     print(json.dumps({"profile_fdk": n, "fdk_small_ms": e[0].elapsed_time(e[1]),
                       "backprojection_ms_per_view": e[2].elapsed_time(e[3]) / (2 * n)}), flush=True)
+
+
+def profile_slabs(args):
+    """A short run for ncu: --profile-slabs views of the 4-slab SART pass on the
+    512^3 scan (per view 4 partial projections, the ordered combination, 4
+    slab updates), FP32, the reference backprojector's arithmetic, tiled;
+    after 2 warm-up views."""
+    import torch
+
+    import gpu_b200
+    n = args.profile_slabs
+    geom = gpu_b200.Geometry(gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"],
+                                                SCAN["du"], SCAN["dso"], SCAN["dod"], SCAN["n_views"]))
+    truth = torch.zeros(geom.vol_shape, device="cuda")
+    geom.phantom_voxelize(phantom_params(2024), truth)
+    sino = torch.zeros((n + 2,) + geom.view_shape, device="cuda")
+    geom.forward(truth, sino, 0, n + 2)
+    vol = torch.zeros(geom.vol_shape, device="cuda")
+    fl = gpu_b200.SART_TILED | gpu_b200.SART_REFERENCE_BP
+    geom.sart_pass_slabs(vol, sino, BETA, 4, 0, 2, flags=fl)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    geom.sart_pass_slabs(vol, sino, BETA, 4, 2, n, flags=fl)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_slabs": n, "ms_per_view": e0.elapsed_time(e1) / n}), flush=True)
 
 
 def profile_views(args):
@@ -802,6 +831,8 @@ def main():
         return profile_views(args)
     if args.profile_fdk:
         return profile_fdk(args)
+    if args.profile_slabs:
+        return profile_slabs(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "large":

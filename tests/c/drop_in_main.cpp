@@ -6,7 +6,10 @@
 // ctr_set_default_geometry instead of compile-time constants.
 //
 //   drop_in_main nx ny nz vx nu nv du dso dod n_views iterations step_size
-//                lambda_TV Niter_denoise sinogram.raw out_volume.raw
+//                lambda_TV Niter_denoise sinogram.raw out_volume.raw [Number_of_Devices]
+//
+// Number_of_Devices (default 1) is that of the build being replaced
+// (V63/main_recon.cu:23; the stock file has 4).
 //
 // Prints one line per iteration: "k tv fidelity objective" (%.17g), like the
 // reference's object_func array (V63/main_recon.cu:419-425).
@@ -20,11 +23,12 @@
 
 int main(int argc, char** argv)
 {
-    if (argc != 17) {
-        std::fprintf(stderr, "usage: %s nx ny nz vx nu nv du dso dod n_views iters step lambda_tv niter_fgp sino out\n",
-                     argv[0]);
+    if (argc != 17 && argc != 18) {
+        std::fprintf(stderr, "usage: %s nx ny nz vx nu nv du dso dod n_views iters step lambda_tv niter_fgp sino out "
+                     "[devices]\n", argv[0]);
         return 2;
     }
+    const int Number_of_Devices = argc == 18 ? std::atoi(argv[17]) : 1;
     ctr_geometry_desc d;
     std::memset(&d, 0, sizeof(d));
     d.nx = std::atoi(argv[1]); d.ny = std::atoi(argv[2]); d.nz = std::atoi(argv[3]);
@@ -38,7 +42,7 @@ int main(int argc, char** argv)
     const float step_size = (float)std::atof(argv[12]);
     const float lambda_TV = (float)std::atof(argv[13]);
     const int Niter_denoise = std::atoi(argv[14]);
-    if (ctr_set_default_geometry(&d) != CTR_OK) {
+    if (ctr_set_default_geometry(&d) != CTR_OK || ctr_set_default_devices(Number_of_Devices) != CTR_OK) {
         std::fprintf(stderr, "ctrecon: %s\n", ctr_last_error_string());
         return 1;
     }

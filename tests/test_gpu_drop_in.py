@@ -3,14 +3,17 @@ driver loop (V63/main_recon.cu:286-430) written against the library's
 reference-compatible host functions, compiled with g++ against
 include/ctrecon.h and linked to the in-tree libctrecon.so.  Its reconstruction
 must equal the reference's call sequence restated by the oracle bit for bit,
-and its printed objectives the oracle's."""
+and its printed objectives the oracle's: for the one-device build, and for
+the stock 4-device build (Number_of_Devices 4, whose SART pass is the z-slab
+sequence of V63/host_IterativeRecon_CBCT_multiGPU.c) on a wide-cone scan
+whose rays cross the slab planes."""
 import os
 import subprocess
 
 import numpy as np
 import pytest
 
-from scan_configs import SMALL, og_desc_xyz
+from scan_configs import SLABS, SMALL, og_desc_xyz
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -23,8 +26,10 @@ def _cuda():
         pytest.skip("no CUDA device")
 
 
-def test_cpp_driver_equals_reference_sequence(tmp_path, oracle_built):
-    cfg = SMALL["cube16"]
+# the driver takes no initial angle (the reference's initialAngle is 0 in the stock file)
+@pytest.mark.parametrize("cfg,devices", [(SMALL["cube16"], 1), (dict(SLABS["cone_wide"], initial_angle=0.0), 4)],
+                         ids=["one_device", "four_devices"])
+def test_cpp_driver_equals_reference_sequence(cfg, devices, tmp_path, oracle_built):
     exe = tmp_path / "drop_in_main"
     lib = os.path.join(ROOT, "gpu_b200")
     subprocess.run(["g++", "-O2", "-ffp-contract=off", "-std=c++17", "-I", os.path.join(ROOT, "include"),
@@ -36,7 +41,8 @@ def test_cpp_driver_equals_reference_sequence(tmp_path, oracle_built):
     b.tofile(tmp_path / "sino.raw")
     beta, lam, fgp_iters, iters = np.float32(0.8), np.float32(0.05), 5, 3
     args = [cfg["nx"], cfg["ny"], cfg["nz"], cfg["vx"], cfg["nu"], cfg["nv"], cfg["du"], cfg["dso"], cfg["dod"],
-            cfg["nviews"], iters, float(beta), float(lam), fgp_iters, tmp_path / "sino.raw", tmp_path / "vol.raw"]
+            cfg["nviews"], iters, float(beta), float(lam), fgp_iters, tmp_path / "sino.raw", tmp_path / "vol.raw",
+            devices]
     run = subprocess.run([str(exe)] + [str(a) for a in args], capture_output=True, text=True, timeout=300)
     assert run.returncode == 0, run.stderr
     got = np.fromfile(tmp_path / "vol.raw", np.float32).reshape(o.vol_shape)
@@ -48,7 +54,8 @@ def test_cpp_driver_equals_reference_sequence(tmp_path, oracle_built):
     t = np.float32(1.0)
     want_objs = []
     for _ in range(iters):
-        x = o.fgp(o.sart_pass_ref(y, b, beta), beta * lam, fgp_iters)
+        sart = o.sart_pass_ref(y, b, beta) if devices == 1 else o.sart_pass_slabs(y, b, beta, devices)
+        x = o.fgp(sart, beta * lam, fgp_iters)
         t_k = (np.float32(1.0) + np.sqrt(np.float32(1.0) + np.float32(4.0) * t * t, dtype=np.float32)) / np.float32(2.0)
         y, xprev = o.fista_momentum(y, xprev, x, t, t_k)
         t = np.float32(t_k)
