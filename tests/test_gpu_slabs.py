@@ -6,7 +6,8 @@ against the reference's multi-GPU kernels (golden fixtures,
 tests/golden/make_golden_slabs.py) and the oracle; the whole D-slab pass on
 one GPU (ctr_sart_pass_slabs) and the reference-compatible
 Reconstruction_3D_ray_driven_CBCT with ctr_set_default_devices(D), linear and
-tiled; the 512^3 scan split in 4.  Bit-exact throughout.
+tiled; the 512^3 scan split in 4; the one-slab-per-rank driver
+(gpu_b200/slabs.py) over a one-rank NCCL group.  Bit-exact throughout.
 """
 import os
 
@@ -195,3 +196,44 @@ def test_full_size_four_slabs(oracle_built):
         assert np.count_nonzero(got != h) > 0.05 * h.size
         want = o.sart_pass_slabs(h, bh, 0.8, D, v0=j, nv=1, engine=engine)
         np.testing.assert_array_equal(bits(got), bits(want), err_msg=f"engine={engine}")
+
+
+def test_slab_driver_over_nccl_one_rank(oracle_built):
+    """gpu_b200.slabs.SlabSART on the GPU with a one-rank NCCL group (the only
+    group one GPU allows without ranks waiting on one another): the exchange
+    is all_gather_into_tensor of one part, the combination of one part is the
+    one-device correction, so the driver's pass equals ctr_sart_pass bit for
+    bit (both update arithmetics, linear and tiled slab volume)."""
+    import socket
+    from datetime import timedelta
+
+    import torch.distributed as dist
+
+    import gpu_b200
+    from gpu_b200.slabs import SlabOps, SlabSART
+    cfg = SLABS["cone_wide"]
+    g = load("cone_wide")
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=60))
+    try:
+        ops = SlabOps(ctr_desc(cfg), 1, 0)
+        drv = SlabSART(ops, 0, 1, "cuda")
+        whole = gpu_b200.Geometry(ctr_desc(cfg))
+        b = dev(g["b"])
+        for flags in (gpu_b200.SART_REFERENCE_BP, 0):
+            want = dev(g["vol0"])
+            whole.sart_pass(want, b, 0.8, flags=flags)
+            x = dev(g["vol0"])
+            drv.views(x, b, 0.8, 0, cfg["nviews"], flags=flags)
+            np.testing.assert_array_equal(bits(x.cpu().numpy()), bits(want.cpu().numpy()), err_msg=f"flags={flags}")
+            t = torch.zeros(ops.geom.tiled_count(), device="cuda")
+            ops.geom.volume_tiling(dev(g["vol0"]), t, True)
+            drv.views(t, b, 0.8, 0, cfg["nviews"], flags=flags, tiled=True)
+            x = torch.zeros(ops.vol_shape, device="cuda")
+            ops.geom.volume_tiling(t, x, False)
+            np.testing.assert_array_equal(bits(x.cpu().numpy()), bits(want.cpu().numpy()), err_msg=f"tiled {flags}")
+    finally:
+        dist.destroy_process_group()
