@@ -33,7 +33,7 @@ METRIC = "SART-FISTA-TV iter/s & voxel-updates/s, 512^3 x 1024 views, mixed vs F
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=6)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mixed", choices=["f16", "bf16"], default="f16")
@@ -44,6 +44,9 @@ def parse():
                    help="with --profile-views: also run two FP16 solver iterations (the second in steady state)")
     p.add_argument("--profile-refbp", action="store_true",
                    help="with --profile-views: the SART updates with the reference backprojector's arithmetic")
+    p.add_argument("--profile-obj", action="store_true",
+                   help="short run for ncu: two FP16 solver iterations on an 8-view subset of the 512^3 scan "
+                        "(the second projects the first's objective in its SART traversal)")
     p.add_argument("--profile-slabs", type=int, default=0,
                    help="short run for ncu: N views of the 4-slab SART (the reference's default 4-device build) "
                         "on the 512^3 scan, FP32, its backprojection arithmetic, tiled")
@@ -322,6 +325,38 @@ def profile_fdk(args):
     torch.cuda.synchronize()
     print(json.dumps({"profile_fdk": n, "fdk_small_ms": e[0].elapsed_time(e[1]),
                       "backprojection_ms_per_view": e[2].elapsed_time(e[3]) / (2 * n)}), flush=True)
+
+
+def profile_obj(args):
+    """A short run for ncu: the FP16 solver (FISTA, FGP-TV, objective) on the
+    512^3 scan restricted to its first 8 views (same angles), two
+    iterations: the first's SART forward projections are the plain kind, the
+    second's also project the first's objective (the fused kind)."""
+    import torch
+
+    import gpu_b200
+    n = 8
+    geom = gpu_b200.Geometry(gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"],
+                                                SCAN["du"], SCAN["dso"], SCAN["dod"], n,
+                                                us_rate=360.0 / SCAN["n_views"]))
+    truth = torch.zeros(geom.vol_shape, device="cuda")
+    geom.phantom_voxelize(phantom_params(2024), truth)
+    sino = torch.zeros((n,) + geom.view_shape, device="cuda", dtype=torch.float16)
+    geom.forward(truth, sino, 0, n)
+    del truth
+    solver = gpu_b200.Solver(geom, gpu_b200.F16, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS)
+    solver.set_sinogram(sino)
+    solver.set_volume(None)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    solver.iterate(1, objectives=False)
+    e[1].record()
+    solver.iterate(1, objectives=False)
+    e[2].record()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_obj": n, "first_iteration_ms": e[0].elapsed_time(e[1]),
+                      "second_iteration_ms": e[1].elapsed_time(e[2])}), flush=True)
+    solver.close()
 
 
 def profile_slabs(args):
@@ -833,6 +868,8 @@ def main():
         return profile_fdk(args)
     if args.profile_slabs:
         return profile_slabs(args)
+    if args.profile_obj:
+        return profile_obj(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "large":
