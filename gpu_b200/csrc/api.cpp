@@ -303,6 +303,22 @@ ctr_status slab_geoms(Geometry* g, int n, std::vector<Geometry*>& out)
         sg->fp_shape = g->fp_shape;
         sg->bp_shape = g->bp_shape;
     }
+    if ((int)g->slab_streams.size() != n) {
+        for (cudaStream_t q : g->slab_streams) cudaStreamDestroy(q);
+        for (cudaEvent_t e : g->slab_events) cudaEventDestroy(e);
+        g->slab_streams.clear();
+        g->slab_events.clear();
+        for (int i = 0; i < n; ++i) {
+            cudaStream_t q = nullptr;
+            CTR_CUDA_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+            g->slab_streams.push_back(q);
+        }
+        for (int i = 0; i < n + 2; ++i) {
+            cudaEvent_t e = nullptr;
+            CTR_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            g->slab_events.push_back(e);
+        }
+    }
     out = g->slab_geoms;
     return CTR_OK;
 }
@@ -318,7 +334,16 @@ ctr_status ensure_parts(Geometry* g, size_t bytes)
     return CTR_OK;
 }
 
-// views [v0, v0+nv) of the D-slab SART on one GPU; pv the whole volume (linear or tiled)
+// Views [v0, v0+nv) of the D-slab SART on one GPU; pv the whole volume
+// (linear or tiled).  The slabs are independent between the combinations --
+// slab s's projection reads and its update writes only slab s -- so each
+// slab runs on its own stream: its projection of view j, then (after the
+// combination of view j on st, which waits for every slab's projection) its
+// update, then its projection of view j+1.  A slab's short launches then
+// share the GPU with the others' instead of running one after another.  The
+// ray records and parts are safe to reuse: view j+1's combination waits for
+// every slab's projection of j+1, each of which follows that slab's update
+// of j.
 ctr_status sart_views_slabs(Geometry* g, const std::vector<Geometry*>& sl, void* pv, ctr_dtype vdt, bool tiled,
                             const void* sino, ctr_dtype sdt, float beta, unsigned flags, uint32_t seed, int v0, int nv,
                             cudaStream_t st)
@@ -330,24 +355,44 @@ ctr_status sart_views_slabs(Geometry* g, const std::vector<Geometry*>& sl, void*
     CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
     CTR_TRY(ensure_parts(g, (size_t)P * D * sizeof(float2)));
     float2* parts = (float2*)g->d_parts;
-    for (int j = v0; j < v0 + nv; ++j) {
-        for (int i = 0; i < D; ++i) {                  // multiGPU.c:71-75
+    const std::vector<cudaStream_t>& ss = g->slab_streams;
+    const std::vector<cudaEvent_t>& ev = g->slab_events;
+    cudaEvent_t ev_comb = ev[D], ev_start = ev[D + 1];
+    CTR_CUDA_TRY(cudaEventRecord(ev_start, st));
+    for (int i = 0; i < D; ++i) CTR_CUDA_TRY(cudaStreamWaitEvent(ss[i], ev_start, 0));
+    ctr_status r = CTR_OK;
+    for (int j = v0; j < v0 + nv && r == CTR_OK; ++j) {
+        for (int i = 0; i < D && r == CTR_OK; ++i) {   // multiGPU.c:71-75
             FpArgs a{};
             a.vol = (const char*)pv + (size_t)per_slab * i * es; a.vol_dtype = vdt; a.view0 = j; a.nview = 1;
             a.kind = FP_PARTIAL; a.out = parts + (size_t)P * i; a.tiled = tiled;
-            CTR_TRY(launch_forward(*sl[i], a, st, nullptr));
+            r = launch_forward(*sl[i], a, ss[i], nullptr);
+            if (r == CTR_OK && cudaEventRecord(ev[i], ss[i]) != cudaSuccess) r = set_error(CTR_ERR_CUDA, "cudaEventRecord");
+            if (r == CTR_OK && cudaStreamWaitEvent(st, ev[i], 0) != cudaSuccess)
+                r = set_error(CTR_ERR_CUDA, "cudaStreamWaitEvent");
         }
-        CTR_TRY(launch_combine(*g, parts, D, j, (const char*)sino + (size_t)j * P * dtype_size(sdt), sdt,
-                               (float2*)g->d_rays, st));   // :82-95
-        for (int i = 0; i < D; ++i) {                  // :103-112
+        if (r == CTR_OK)
+            r = launch_combine(*g, parts, D, j, (const char*)sino + (size_t)j * P * dtype_size(sdt), sdt,
+                               (float2*)g->d_rays, st);   // :82-95
+        if (r == CTR_OK && cudaEventRecord(ev_comb, st) != cudaSuccess) r = set_error(CTR_ERR_CUDA, "cudaEventRecord");
+        for (int i = 0; i < D && r == CTR_OK; ++i) {   // :103-112
+            if (cudaStreamWaitEvent(ss[i], ev_comb, 0) != cudaSuccess) {
+                r = set_error(CTR_ERR_CUDA, "cudaStreamWaitEvent");
+                break;
+            }
             BpArgs b{};
             b.vol = (char*)pv + (size_t)per_slab * i * es; b.vol_dtype = vdt; b.rays = g->d_rays; b.view0 = j;
             b.nview = 1; b.sart = 1; b.flags = flags; b.beta = beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j;
             b.tiled = tiled;
-            CTR_TRY(launch_backproject(*sl[i], b, st));
+            r = launch_backproject(*sl[i], b, ss[i]);
         }
     }
-    return CTR_OK;
+    // st resumes after every slab's last launch, also on an error
+    for (int i = 0; i < D; ++i) {
+        cudaEventRecord(ev[i], ss[i]);
+        cudaStreamWaitEvent(st, ev[i], 0);
+    }
+    return r;
 }
 
 }  // namespace

@@ -49,7 +49,8 @@ struct DevGeom {
     // Z is the slab's ZETA/D slices, bz its BOUNDARY_VOXEL_Z; the whole volume otherwise
     int slab_n, slab_i;     // D (1: no split) and this slab's index (subVolIdx)
     int zpar_kr;            // the single-GPU z-parallel k range applies (not T42's, not a slab's)
-    int row_lo, row_hi;     // partial forward: rows traced (a fan-slice / parallel slab: its band)
+    int row_lo, row_hi;     // partial forward: rows traced (a fan-slice / parallel slab: its band; a
+                            // cone-beam slab: a conservative band of the rows that can reach it)
     float bz_ref, cz_off;   // reference BP voxel centre z = (bz_ref + cz_off) + k*vz (universal.cu:594,
                             // multiGPU.cu:1179): bz and vz*0.5f, or the whole volume's bz and vz*(k0+0.5f)
     int ref_plus0;          // the reference BP's "+= 0.0f" on voxels without rays (not in a slab's)
@@ -89,8 +90,11 @@ struct Geometry {
     float* d_fdk = nullptr; size_t fdk_cap = 0;
     void* d_tiled = nullptr; size_t tiled_bytes = 0;   // tiled copy for CTR_SART_TILED
     float* d_ramp = nullptr;                           // 2R-1 taps
-    // slab geometries of the one-GPU slab SART (ctr_sart_pass_slabs), built on first use
+    // slab geometries of the one-GPU slab SART (ctr_sart_pass_slabs), built on first use,
+    // with a stream per slab and the events that order them around the combination
     std::vector<Geometry*> slab_geoms;
+    std::vector<cudaStream_t> slab_streams;
+    std::vector<cudaEvent_t> slab_events;              // [0, D): per slab; D: combination; D+1: start
     void* d_parts = nullptr; size_t parts_cap = 0;     // [D][P] float2 partial ray sums
     // launch shapes (indices into the tuner's tables; results do not depend on them)
     int fp_shape = 1;                                  // FP: see kFpShapes in fp.cu

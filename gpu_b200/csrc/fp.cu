@@ -379,7 +379,8 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     const long long p = (long long)w * P + (long long)v * g.R + u;
     double e2 = 0.0;
     if (KIND == FP_PARTIAL && active && (v < g.row_lo || v >= g.row_hi)) {
-        // a fan-slice / parallel-beam slab traces only its band's rows (multiGPU.cu:663-667)
+        // a fan-slice / parallel-beam slab traces only its band's rows (multiGPU.cu:663-667);
+        // a cone-beam slab's other rows miss it, and their sums are (0, 0)
         ((float2*)out)[p] = make_float2(0.0f, 0.0f);
     } else if (active) {
         const float2 sc = g.trig[view0 + w];

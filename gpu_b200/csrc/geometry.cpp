@@ -238,6 +238,30 @@ static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ct
         if (q.ct_style == 1 || q.ct_style == 2) {   // :663
             q.row_lo = d.nv / n_slabs * slab;
             q.row_hi = d.nv / n_slabs * (slab + 1);
+        } else {
+            // Cone beam: the rows whose rays can reach the slab at any view.  A
+            // point at alpha of a ray lies at DOD + alpha*(DSO-DOD) along the
+            // view's axis and at height x1z*(1-alpha) (the source at z = 0), and
+            // the volume lies within its xy half-diagonal of the axis, so inside
+            // the volume alpha is in [a_lo, a_hi].  Rows whose heights over that
+            // range stay a voxel clear of the slab miss it geometrically and the
+            // projector gives them (0, 0); the band keeps two rows of margin.
+            const double rv = 0.5 * std::sqrt((double)d.nx * d.vx * d.nx * d.vx + (double)d.ny * d.vy * d.ny * d.vy) +
+                              std::fabs((double)d.m_offset * d.vx);
+            const double a_lo = (-rv - d.dod) / ((double)d.dso - d.dod), a_hi = (rv - d.dod) / ((double)d.dso - d.dod);
+            const double zlo = (double)q.bz - d.vz, zhi = (double)q.bz + (double)zs * d.vz + d.vz;
+            const float zmin = -d.dv * ((float)d.nv / 2.0f - 0.5f);   // Detector_Zmin, set below
+            int lo = d.nv, hi = -1;
+            for (int v = 0; v < d.nv; ++v) {
+                const double x1z = (double)zmin + (double)v * d.dv;
+                const double z0 = x1z * (1.0 - a_hi), z1 = x1z * (1.0 - a_lo);
+                if (std::max(z0, z1) >= zlo && std::min(z0, z1) <= zhi) {
+                    lo = std::min(lo, v);
+                    hi = v;
+                }
+            }
+            q.row_lo = lo <= hi ? std::max(0, lo - 2) : 0;
+            q.row_hi = lo <= hi ? std::min(d.nv, hi + 3) : 0;
         }
         d.nz = zs;
         g->desc.nz = zs;
@@ -447,6 +471,8 @@ extern "C" ctr_status ctr_geometry_destroy(ctr_geometry* geom)
     cudaFree(g->d_tiled);
     cudaFree(g->d_ramp);
     cudaFree(g->d_parts);
+    for (cudaStream_t q : g->slab_streams) cudaStreamDestroy(q);
+    for (cudaEvent_t e : g->slab_events) cudaEventDestroy(e);
     for (Geometry* sg : g->slab_geoms) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(sg));
     delete g;
     return CTR_OK;
