@@ -271,6 +271,12 @@ class Geometry:
         """Index in the whole volume of this geometry's first slice."""
         return self.vol_shape[0] * self.slab
 
+    def slab_info(self):
+        """(n_slabs, slab, first slice) as the library holds them (``ctr_geometry_slab``)."""
+        n, s, k0 = C.c_int(), C.c_int(), C.c_int()
+        check(self.lib.ctr_geometry_slab(self.h, C.byref(n), C.byref(s), C.byref(k0)))
+        return n.value, s.value, k0.value
+
     @property
     def view_shape(self):
         """(rows, columns) of one view; the tetrahedron beam's rows are all its sources' bands."""

@@ -56,7 +56,7 @@ def test_per_view_steps_equal_reference(name, D, oracle_built):
     j = int(g["view"])
     zs = cfg["nz"] // D
     gs = slab_geoms(cfg, D)
-    assert [x.first_slice for x in gs] == [zs * s for s in range(D)]
+    assert [x.slab_info() for x in gs] == [(D, s, zs * s) for s in range(D)]
     rows, nu = gs[0].view_shape
     for tiled in (False, True):
         parts = torch.zeros((D, rows, nu, 2), device="cuda")
