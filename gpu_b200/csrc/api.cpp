@@ -303,7 +303,7 @@ ctr_status slab_geoms(Geometry* g, int n, std::vector<Geometry*>& out)
         sg->fp_shape = g->fp_shape;
         sg->bp_shape = g->bp_shape;
     }
-    if ((int)g->slab_streams.size() != n) {
+    if ((int)g->slab_streams.size() != n || (int)g->slab_events.size() != n + 2) {   // also after a failed build
         for (cudaStream_t q : g->slab_streams) cudaStreamDestroy(q);
         for (cudaEvent_t e : g->slab_events) cudaEventDestroy(e);
         g->slab_streams.clear();
@@ -1397,7 +1397,9 @@ extern "C" void Reconstruction_3D_ray_driven_CBCT(float* h_volume, float* h_proj
     if (st != CTR_OK) return;
     cudaError_t e = cudaMemcpy(h_volume, v.p, vb, cudaMemcpyDefault);
     if (e != cudaSuccess) { cuda_error(e, "Reconstruction_3D_ray_driven_CBCT"); return; }
-    check_device_errors(g, nullptr);
+    if (check_device_errors(g, nullptr) != CTR_OK || g_default_devices <= 1) return;
+    for (Geometry* sg : g->slab_geoms)   // the slabs' projectors keep their own error words
+        if (check_device_errors(sg, nullptr) != CTR_OK) return;
 }
 
 extern "C" void CheckMatchedJointOperator(float* h_volume)
