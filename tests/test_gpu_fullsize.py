@@ -1,6 +1,8 @@
 """Parity at the benchmark's full size: the 512^3 volume (0.5 mm), 1024x768
-detector (0.4 mm), 1024 views, DSO 1000 mm, DOD -500 mm, and the
-tetrahedron-beam scan (512^3 x 0.1 mm, 64 sources x 16 x 1024).
+detector (0.4 mm), 1024 views, DSO 1000 mm, DOD -500 mm, the
+tetrahedron-beam scan (512^3 x 0.1 mm, 64 sources x 16 x 1024), and the
+large mixed-precision scan (1024^3 x 0.25 mm, 1024x1024 detector x 0.3 mm,
+1024 views; its FP32 and FP16 projections).
 
 The oracle projects and updates a few whole views of these scans in seconds
 (OpenMP), so the checks are the small scans' checks on spread-out views:
@@ -16,6 +18,7 @@ torch = pytest.importorskip("torch")
 SCAN = dict(nx=512, ny=512, nz=512, vx=0.5, nu=1024, nv=768, du=0.4, dso=1000.0, dod=-500.0, nviews=1024)
 TBCT_SCAN = dict(nx=512, ny=512, nz=512, vx=0.1, nu=1024, nv=16, du=0.12, dso=200.0, dod=-200.0, nviews=360,
                  us_rate=1.0, ct_style=3, n_sources=64)
+LARGE = dict(nx=1024, ny=1024, nz=1024, vx=0.25, nu=1024, nv=1024, du=0.3, dso=1000.0, dod=-500.0, nviews=1024)
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -47,11 +50,11 @@ def scan(cfg, oracle_mod):
     return g, o, vol
 
 
-@pytest.mark.parametrize("cfg", [SCAN, TBCT_SCAN], ids=["cone512", "tbct512"])
+@pytest.mark.parametrize("cfg", [SCAN, TBCT_SCAN, LARGE], ids=["cone512", "tbct512", "cone1024"])
 def test_forward_and_traversal_bit_exact(cfg, oracle_built):
     g, o, vol = scan(cfg, oracle_built)
     h = vol.cpu().numpy()
-    views = [0, cfg["nviews"] // 3 + 1, cfg["nviews"] - 5]
+    views = [0, cfg["nviews"] // 3 + 1, cfg["nviews"] - 5][: 2 if cfg is LARGE else 3]
     nseg = torch.zeros(g.view_shape, dtype=torch.int32, device="cuda")
     hsh = torch.zeros(g.view_shape, dtype=torch.int64, device="cuda")
     ln = torch.zeros(g.view_shape, dtype=torch.float32, device="cuda")
@@ -91,7 +94,7 @@ def test_sart_view_update_bit_exact(cfg, oracle_built):
     np.testing.assert_array_equal(bits(got), bits(want))
 
 
-@pytest.mark.parametrize("cfg", [SCAN, TBCT_SCAN], ids=["cone512", "tbct512"])
+@pytest.mark.parametrize("cfg", [SCAN, TBCT_SCAN, LARGE], ids=["cone512", "tbct512", "cone1024"])
 def test_dot_product_full_size(cfg, oracle_built):
     """<Ax, y> = <x, A^T y> to 1e-6 relative over 8 views spread over the scan
     (x uniform over the voxels, y normal over the detector bins)."""
@@ -123,3 +126,20 @@ def test_sart_view_reference_backprojector_full_size(cfg, oracle_built):
     assert np.count_nonzero(got != h) > 0.05 * h.size
     np.testing.assert_array_equal(bits(got), bits(want))
 
+
+
+def test_large_scan_half_precision_forward(oracle_built):
+    """The 1024^3 scan stored in FP16 and BF16: each projection equals the
+    oracle's FP32 projection of the widened volume, bit for bit (one view
+    each; the storage is widened exactly, the arithmetic is the FP32 one)."""
+    g, o, vol = scan(LARGE, oracle_built)
+    for dt, j in ((torch.float16, 77), (torch.bfloat16, 611)):
+        lo = vol.to(dt)
+        del vol
+        out = torch.zeros((1,) + g.view_shape, device="cuda")
+        g.forward(lo, out, j, 1)
+        want = o.forward_view(lo.float().cpu().numpy(), j, 0)
+        assert np.count_nonzero(want) > 0.1 * want.size
+        np.testing.assert_array_equal(bits(out[0].cpu().numpy()), bits(want), err_msg=str(dt))
+        vol = lo.float()
+        del lo
