@@ -21,7 +21,7 @@ from __future__ import annotations
 import torch
 import torch.distributed as dist
 
-from .ctrecon import F32, Geometry, GeometryDesc, VOLUME_TILED
+from .ctrecon import Geometry, GeometryDesc, VOLUME_TILED
 
 
 class SlabOps:
@@ -82,4 +82,4 @@ def slab_of(vol: torch.Tensor, rank: int, world_size: int) -> torch.Tensor:
     return vol[zs * rank: zs * (rank + 1)]
 
 
-__all__ = ["SlabOps", "SlabSART", "exchange", "slab_of", "F32"]
+__all__ = ["SlabOps", "SlabSART", "exchange", "slab_of"]
