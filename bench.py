@@ -1020,6 +1020,22 @@ def main():
         _, b_ms = geom.sart_views(vtmp, runs["f32"]["sino"], BETA, (j * 97) % SCAN["n_views"], 1,
                                      flags=gpu_b200.SART_TILED | gpu_b200.SART_REFERENCE_BP, timed=True)
         rb_bp += b_ms
+    # the reference's default build's whole loop (Number_of_Devices 4): the
+    # solver with its slab pass and backprojection arithmetic, FP32, every
+    # iteration's objective projected on its own (bit-exact with that build)
+    dflt = gpu_b200.Solver(geom, gpu_b200.F32, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
+                           objective=True, use_graph=True, sart_flags=gpu_b200.SART_REFERENCE_BP)
+    dflt.set_slabs(4)
+    dflt.set_sinogram(runs["f32"]["sino"])
+    dflt.set_volume(None)
+    dflt.iterate(1)
+    barrier()
+    e0.record(stream)
+    dflt.iterate(2)
+    e1.record(stream)
+    barrier()
+    dflt_ms = job_ms(e0.elapsed_time(e1) / 2)
+    dflt.close()
     # the reference's default build (Number_of_Devices 4, its z-slab SART,
     # bit-exact with its multi-GPU kernels) on this one GPU: per view 4 slab
     # partial projections, the ordered combination, 4 slab updates
@@ -1093,6 +1109,11 @@ def main():
                                  "bp_ms_per_view": rb_bp / 32,
                                  "note": "CTR_SART_REFERENCE_BP: the reference backprojector's arithmetic, "
                                          "SART pass bit-exact with the reference"},
+            "reference_default_build_f32": {"iter_per_s": job_rate(dflt_ms, world), "ms_per_step": dflt_ms,
+                                            "note": "the reference's default Number_of_Devices=4 build's SART + "
+                                                    "FISTA + FGP-TV loop, bit-exact with it, on one B200 "
+                                                    "(ctr_solver_set_slabs(4), CTR_SART_REFERENCE_BP, FP32); "
+                                                    "2 timed iterations after 1"},
             "slabs4_f32": {"ms_per_view_reference_bp": slab4["reference_bp"], "ms_per_view_engine": slab4["engine"],
                            "one_device_ms_per_view": {"f32_fp": kern["f32"]["fp_ms"], "reference_bp": rb_bp / 32},
                            "note": "the reference's default Number_of_Devices=4 build: z-slab SART views (4 slab "

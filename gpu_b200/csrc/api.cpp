@@ -712,6 +712,7 @@ struct ctr_solver {
     int hist_cap = 0;
     std::vector<unsigned char> hist_valid;
     bool obj_pending = false;
+    int slabs = 1;           // > 1: the SART pass of the reference's slabs-device build (ctr_solver_set_slabs)
 };
 
 extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt, const ctr_solver_params* p,
@@ -859,6 +860,35 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st, boo
     return CTR_OK;
 }
 
+// The SART pass of the reference's D-device build on the solver's tiled
+// volume: its slab sequence, each slab on its own stream between the
+// combinations (sart_views_slabs), issued directly.
+static ctr_status solver_sart_slabs(ctr_solver* s, uint32_t seed, cudaStream_t st)
+{
+    Geometry* g = s->g;
+    std::vector<Geometry*> sl;
+    CTR_TRY(slab_geoms(g, s->slabs, sl));
+    CTR_TRY(launch_tiling(*g, s->y, s->yt, s->vdt, true, st));
+    CTR_TRY(sart_views_slabs(g, sl, s->yt, s->vdt, true, s->sino, s->sdt, s->p.beta, s->p.sart_flags & ~CTR_SART_TILED,
+                             seed, 0, g->desc.n_views, st));
+    return launch_tiling(*g, s->yt, s->y, s->vdt, false, st);
+}
+
+extern "C" ctr_status ctr_solver_set_slabs(ctr_solver* s, int n_slabs)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    if (n_slabs < 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "n_slabs must be >= 1");
+    if (n_slabs > 1) {
+        std::vector<Geometry*> sl;
+        CTR_TRY(slab_geoms(s->g, n_slabs, sl));   // the slab geometries, streams, events
+        CTR_TRY(ensure_rays(s->g, (size_t)s->g->npix() * sizeof(float2)));
+        CTR_TRY(ensure_parts(s->g, (size_t)s->g->npix() * n_slabs * sizeof(float2)));
+    }
+    s->slabs = n_slabs;
+    return CTR_OK;
+}
+
 // history rows for iterations 1..k (allocated outside any capture)
 static ctr_status hist_reserve(ctr_solver* s, int k, cudaStream_t st)
 {
@@ -931,7 +961,12 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
     for (int it = 0; it < n; ++it) {
         // The objective of x_(k-1), the previous iteration's result (V63/main_recon.cu:390-430),
         // is projected in this iteration's SART traversal: x_(k-1) is xprev with
-        // FISTA and the volume the pass starts from without.
+        // FISTA and the volume the pass starts from without.  With the slab
+        // pass it is projected on its own with the one-device projector, whose
+        // sums the D-device build's row-split projector gives
+        // (V63/host_IterativeRecon_CBCT_multiGPU.c:171-258).
+        const bool slabbed = s->slabs > 1;
+        if (slabbed && s->obj_pending) CTR_TRY(flush_objective(s, st));
         const bool fused = s->obj_pending;
         if (fused) {
             const void* xk1 = s->p.fista ? s->xprev : s->y;
@@ -939,7 +974,8 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
             CTR_TRY(objective_async(g, xk1, s->vdt, s->sino, s->sdt, nullptr, s->d_obj + 1, st));   // TV
         }
         // V63/main_recon.cu:344-386 (FISTA == 1) / :316-341 (FISTA == 0)
-        CTR_TRY(solver_sart(s, (uint32_t)(s->k + 1), st, fused));
+        if (slabbed) CTR_TRY(solver_sart_slabs(s, (uint32_t)(s->k + 1), st));
+        else CTR_TRY(solver_sart(s, (uint32_t)(s->k + 1), st, fused));
         if (fused) {
             CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
             CTR_TRY(hist_store(s, s->k, st));

@@ -56,7 +56,7 @@ EXPORTED = [
     "ctr_batch_get_volume", "ctr_geometry_set_shapes", "ctr_geometry_get_shapes", "ctr_geometry_autotune",
     "ctr_solver_objectives", "ctr_geometry_create_slab", "ctr_geometry_slab", "ctr_forward_partial",
     "ctr_combine_partials", "ctr_sart_update", "ctr_sart_pass_slabs", "ctr_volume_tiling", "ctr_volume_tiled_count",
-    "ctr_set_default_devices",
+    "ctr_set_default_devices", "ctr_solver_set_slabs",
 ]
 
 
@@ -164,6 +164,7 @@ def load_library(path: str = LIB_PATH):
         "ctr_volume_tiling": ([G, vp, vp, i, i, vp], i),
         "ctr_volume_tiled_count": ([G, C.POINTER(C.c_int64)], i),
         "ctr_set_default_devices": ([i], i),
+        "ctr_solver_set_slabs": ([vp, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -475,6 +476,10 @@ class Solver:
         obj = np.zeros(3 * max(n, 1), np.float64)
         check(self.lib.ctr_solver_iterate(self.h, n, obj.ctypes.data, _stream(stream)))
         return obj[: 3 * n].reshape(n, 3)
+
+    def set_slabs(self, n_slabs):
+        """The SART pass of the reference's n_slabs-device build (``ctr_solver_set_slabs``)."""
+        check(self.lib.ctr_solver_set_slabs(self.h, n_slabs))
 
     def objectives(self, first, count, stream=None):
         """Objective history rows of iterations first..first+count-1 (1-based)."""

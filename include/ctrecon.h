@@ -361,6 +361,17 @@ ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* objective_out, void*
 /* Copy the current estimate x_k (vol_dtype) to dst (device or host). */
 ctr_status ctr_solver_get_volume(ctr_solver* s, void* dst, void* stream);
 ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k);
+
+/* The SART pass of the reference's n_slabs-device build (its z-slab sequence,
+ * ctr_sart_pass_slabs) instead of the one-device pass, from the next
+ * ctr_solver_iterate on; 1 restores the one-device pass.  With n_slabs > 1
+ * every iteration's objective is projected on its own with the one-device
+ * projector (the sums the n-device build's row-split projector gives) rather
+ * than inside the next pass, and the pass is issued without a CUDA graph.
+ * With sart_flags = CTR_SART_REFERENCE_BP and FP32 storage the SART + FISTA +
+ * FGP-TV loop and its objectives equal that build's.  ZETA and Z_prj must
+ * split into n_slabs; not for CTR_GEOM_TBCT. */
+ctr_status ctr_solver_set_slabs(ctr_solver* s, int n_slabs);
 /* Objective history [TV, fidelity, objective] of iterations first..first+count-1
  * (1-based, at most the iterations run).  With objective_out == NULL,
  * ctr_solver_iterate leaves the objective of its last x_k pending and projects

@@ -237,3 +237,50 @@ def test_slab_driver_over_nccl_one_rank(oracle_built):
             np.testing.assert_array_equal(bits(x.cpu().numpy()), bits(want.cpu().numpy()), err_msg=f"tiled {flags}")
     finally:
         dist.destroy_process_group()
+
+
+def test_solver_with_slabs_equals_reference_loop(oracle_built):
+    """ctr_solver_set_slabs(4) with the reference's backprojection arithmetic:
+    three SART + FISTA + FGP-TV iterations (V63/main_recon.cu:344-430) equal
+    the reference's 4-device loop restated by the oracle, volume bit for bit
+    and objectives to 1e-12 (the objective projected by the one-device
+    projector, as the 4-device build's row split does); set_slabs(1) then
+    continues with the one-device pass."""
+    import gpu_b200
+    cfg, D = SLABS["cone_wide"], 4
+    o = oracle_built.Oracle(og_desc(cfg))
+    truth = o.phantom(np.array([[0, 0, 0, 5, 4, 3, 0.3, 0.2, 0.1, 0.02], [1.5, -1, 0.5, 2, 2, 2, 0, 0, 0, 0.03]]))
+    b = np.stack([o.forward_view(truth, j, 0) for j in range(cfg["nviews"])])
+    beta, lam, it = np.float32(0.8), np.float32(0.05), 5
+    g = gpu_b200.Geometry(ctr_desc(cfg))
+    s = gpu_b200.Solver(g, gpu_b200.F32, beta=float(beta), lambda_tv=float(lam), fgp_iters=it, fista=True,
+                        objective=True, use_graph=True, sart_flags=gpu_b200.SART_REFERENCE_BP)
+    s.set_slabs(D)
+    s.set_sinogram(dev(b))
+    s.set_volume(None)
+    objs = s.iterate(3)
+    out = torch.zeros(o.vol_shape, device="cuda")
+    s.get_volume(out)
+    y = np.zeros(o.vol_shape, np.float32)
+    xprev = np.zeros_like(y)
+    t = np.float32(1.0)
+    want = []
+    for _ in range(3):
+        x = o.fgp(o.sart_pass_slabs(y, b, beta, D), beta * lam, it)
+        t_k = (np.float32(1.0) + np.sqrt(np.float32(1.0) + np.float32(4.0) * t * t, dtype=np.float32)) / np.float32(2.0)
+        y, xprev = o.fista_momentum(y, xprev, x, t, t_k)
+        t = np.float32(t_k)
+        fid = o.l2_norm(np.stack([o.forward_view(x, j, 0) for j in range(cfg["nviews"])]), b)
+        tv = o.tv_norm(x)
+        want.append((tv, fid, fid + 2.0 * float(lam) * tv))
+    np.testing.assert_array_equal(bits(out.cpu().numpy()), bits(xprev))
+    np.testing.assert_allclose(objs, np.array(want), rtol=1e-12)
+    # back to the one-device pass for the next iteration
+    s.set_slabs(1)
+    s.iterate(1)
+    s.get_volume(out)
+    x = o.fgp(o.sart_pass_ref(y, b, beta), beta * lam, it)
+    t_k = (np.float32(1.0) + np.sqrt(np.float32(1.0) + np.float32(4.0) * t * t, dtype=np.float32)) / np.float32(2.0)
+    _, xprev = o.fista_momentum(y, xprev, x, t, t_k)
+    np.testing.assert_array_equal(bits(out.cpu().numpy()), bits(xprev))
+    s.close()
