@@ -299,9 +299,21 @@ ctr_status slab_geoms(Geometry* g, int n, std::vector<Geometry*>& out)
             g->slab_geoms.push_back(GE(sg));
         }
     }
+    if (g->dg.ct_style == 3 && !g->split_geom) {
+        // the tetrahedron beam's n-device build projects whole views with V63's
+        // traversal rules (T42/voxel/kernel_IterativeRecon_TBCT_voxel_multiGPU.cu:22-576);
+        // for the other scanners its row-split projector is the one-device one
+        ctr_geometry* sg = nullptr;
+        CTR_TRY(ctr_geometry_create_slab(&g->desc, n, -1, &sg));
+        g->split_geom = GE(sg);
+    }
     for (Geometry* sg : g->slab_geoms) {   // the parent's tuned launch shapes
         sg->fp_shape = g->fp_shape;
         sg->bp_shape = g->bp_shape;
+    }
+    if (g->split_geom) {
+        g->split_geom->fp_shape = g->fp_shape;
+        g->split_geom->bp_shape = g->bp_shape;
     }
     if ((int)g->slab_streams.size() != n || (int)g->slab_events.size() != n + 2) {   // also after a failed build
         for (cudaStream_t q : g->slab_streams) cudaStreamDestroy(q);
@@ -923,7 +935,9 @@ static ctr_status flush_objective(ctr_solver* s, cudaStream_t st)
     if (!s->obj_pending) return CTR_OK;
     const void* xk = s->p.fista ? s->xprev : s->y;
     CTR_TRY(hist_reserve(s, s->k, st));
-    CTR_TRY(objective_async(s->g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
+    // with the slab pass, the n-device build's projector (its own for the tetrahedron beam)
+    Geometry* og = (s->slabs > 1 && s->g->split_geom) ? s->g->split_geom : s->g;
+    CTR_TRY(objective_async(og, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
     CTR_TRY(hist_store(s, s->k, st));
     s->obj_pending = false;
     return CTR_OK;
@@ -1409,7 +1423,15 @@ extern "C" void Forward_3D_ray_driven_siddon(float* h_volume, float* h_proj_data
     const size_t vb = g->nvox() * 4, pb = (size_t)g->npix() * g->desc.n_views * 4;
     DevBuf v, p;
     if (in_dev(v, h_volume, vb) != CTR_OK || in_dev(p, nullptr, pb) != CTR_OK) return;
-    ctr_geometry* gg = reinterpret_cast<ctr_geometry*>(g);
+    Geometry* fg = g;
+    if (g_default_devices > 1 && g->dg.ct_style == 3) {
+        // the tetrahedron beam's n-device build projects with its row-split projector
+        // (T42/voxel/host_IterativeRecon_TBCT_voxel_multiGPU.c:185-306)
+        std::vector<Geometry*> sl;
+        if (slab_geoms(g, g_default_devices, sl) != CTR_OK) return;
+        fg = g->split_geom;
+    }
+    ctr_geometry* gg = reinterpret_cast<ctr_geometry*>(fg);
     if (ctr_forward(gg, v.p, CTR_F32, p.p, CTR_F32, 0, g->desc.n_views, nullptr) != CTR_OK) return;
     cudaError_t e = cudaMemcpy(h_proj_data, p.p, pb, cudaMemcpyDefault);
     if (e != cudaSuccess) cuda_error(e, "Forward_3D_ray_driven_siddon");

@@ -347,8 +347,8 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
     // TB: the depth of the column centre as T42 evaluates it (:568-569, :620)
     float tden = 0.f;
     if (TB) {
-        const float cxr = fa(g.bx, fm(g.vx, fa(0.5f, (float)i)));
-        const float cyr = fa(g.by, fm(g.vy, fa(0.5f, (float)j)));
+        const float cxr = tb_centre_xy(g, g.bx, g.vx, i);
+        const float cyr = tb_centre_xy(g, g.by, g.vy, j);
         tden = fs(fa(fm(cxr, c), fm(cyr, s)), g.dod);
     }
     // TB: the range [s0, s1] of sources kept for the current voxel.  Both
@@ -434,7 +434,7 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
             }
         } else {
             // the sources T42 keeps for this voxel (:620-627): source_lower <= z <= source_upper
-            const float czr = fa(g.bz, fm(g.vz, fa(0.5f, (float)k)));
+            const float czr = tb_centre_z(g, k);
             const float upper = fa(fdv(fm(fs(fa(czr, g.vz), g.zmin), g.dsod), tden), g.zmin);
             const float lower = fa(fdv(fm(fs(fs(czr, g.vz), g.zmax), g.dsod), tden), g.zmax);
             auto zsrc = [&](int q) { return fa(g.zsrc0, fm((float)q, g.zsrc_dz)); };

@@ -41,8 +41,7 @@ __global__ void k_zref(const DevGeom g, float2* __restrict__ zref)
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t / g.ZP), v = (int)(t % g.ZP);
         const int src = v / g.nvr;
-        const float cz = g.ct_style == 3 ? fa(g.bz, fm(g.vz, fa(0.5f, (float)k)))
-                                         : fa(fa(g.bz_ref, g.cz_off), fm((float)k, g.vz));
+        const float cz = g.ct_style == 3 ? tb_centre_z(g, k) : fa(fa(g.bz_ref, g.cz_off), fm((float)k, g.vz));
         const float qz = fa(g.zmin, fm((float)(v - src * g.nvr), g.dv));
         const float sz = g.ct_style == 3 ? fa(g.zsrc0, fm((float)src, g.zsrc_dz)) : (g.ct_style == 0 ? g.srcz : cz);
         const float az0 = fdv(fs(fs(cz, fm(0.5f, g.vz)), qz), fs(sz, qz));
@@ -247,8 +246,8 @@ k_sart_ref_tb(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ 
     const float ey = fs((float)j, g.fov_h_y);
     if (fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2) return;
 
-    const float cx = fa(g.bx, fm(g.vx, fa(0.5f, (float)i)));                 // :568-569
-    const float cy = fa(g.by, fm(g.vy, fa(0.5f, (float)j)));
+    const float cx = tb_centre_xy(g, g.bx, g.vx, i);                        // :568-569
+    const float cy = tb_centre_xy(g, g.by, g.vy, j);
     const float2 sc = g.trig[view];
     const float s = sc.x, c = sc.y;
     const float DSO = g.dso, DOD = g.dod;
@@ -306,7 +305,7 @@ k_sart_ref_tb(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ 
     bool s_est = true;
     VT* pv = vol + (TL ? (long long)tile_index(g, i, j, kb) : (long long)kb * MN + (long long)j * g.M + i);
     for (int k = kb; k < ke; ++k, pv += vstep) {
-        const float cz = fa(g.bz, fm(g.vz, fa(0.5f, (float)k)));           // :570
+        const float cz = tb_centre_z(g, k);                                 // :570
         const float upper = fa(fdv(fm(fs(fa(cz, g.vz), g.zmin), g.dsod), tden), g.zmin);   // :623
         const float lower = fa(fdv(fm(fs(fs(cz, g.vz), g.zmax), g.dsod), tden), g.zmax);   // :624
         if (s_est) {   // the kept sources: one range growing with k (see k_sart_walk's TB form)

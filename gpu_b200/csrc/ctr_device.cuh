@@ -133,6 +133,19 @@ __device__ __forceinline__ float ray_d12(const RayEnds& e)
     return __fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz)));
 }
 
+// The tetrahedron-beam backprojector's voxel centre: b + v*(0.5f + i) along x
+// and y, bz + vz*(0.5f + k) (T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:
+// 568-570); in a slab of its multi-GPU build b + v*0.5f + i*v and
+// boundary_voxel_z + vz*(ZETA/D*s + 0.5f) + k*vz (T42/voxel/..._multiGPU.cu:1140-1142).
+__device__ __forceinline__ float tb_centre_xy(const DevGeom& g, float b, float v, int i)
+{
+    return g.slab_n > 1 ? fa(fa(b, fm(v, 0.5f)), fm((float)i, v)) : fa(b, fm(v, fa(0.5f, (float)i)));
+}
+__device__ __forceinline__ float tb_centre_z(const DevGeom& g, int k)
+{
+    return g.slab_n > 1 ? fa(fa(g.bz_ref, g.cz_off), fm((float)k, g.vz)) : fa(g.bz, fm(g.vz, fa(0.5f, (float)k)));
+}
+
 // Dispatch a runtime ctr_dtype to a storage type.
 #define CTR_DISPATCH_DTYPE(dt, T, ...)                      \
     switch (dt) {                                           \

@@ -54,6 +54,8 @@ struct DevGeom {
     float bz_ref, cz_off;   // reference BP voxel centre z = (bz_ref + cz_off) + k*vz (universal.cu:594,
                             // multiGPU.cu:1179): bz and vz*0.5f, or the whole volume's bz and vz*(k0+0.5f)
     int ref_plus0;          // the reference BP's "+= 0.0f" on voxels without rays (not in a slab's)
+    float thr_comb;         // the slab combination's zero-length threshold: volumn_z*1e-6f (V63),
+                            // volumn_z*1e-3f (T42/voxel/kernel_IterativeRecon_TBCT_voxel_multiGPU.cu:14)
     const float* px;        // plane coordinates vx*n+bx for n = -1..M+1 at px[n+1]
     const float* py;
     const float* pz;
@@ -95,6 +97,8 @@ struct Geometry {
     std::vector<Geometry*> slab_geoms;
     std::vector<cudaStream_t> slab_streams;
     std::vector<cudaEvent_t> slab_events;              // [0, D): per slab; D: combination; D+1: start
+    Geometry* split_geom = nullptr;                    // tetrahedron beam: the D-device build's row-split
+                                                       // projector (ctr_geometry_create_slab, slab -1)
     void* d_parts = nullptr; size_t parts_cap = 0;     // [D][P] float2 partial ray sums
     // launch shapes (indices into the tuner's tables; results do not depend on them)
     int fp_shape = 1;                                  // FP: see kFpShapes in fp.cu

@@ -165,12 +165,10 @@ static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ct
     if (!out) return set_error(CTR_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     CTR_TRY(validate(din));
-    if (n_slabs < 1 || slab < 0 || slab >= n_slabs)
+    if (n_slabs < 1 || slab < (n_slabs > 1 ? -1 : 0) || slab >= n_slabs)
         return set_error(CTR_ERR_INVALID_ARGUMENT, "slab %d of %d", slab, n_slabs);
     if (n_slabs > 1) {
-        if (din->flags & CTR_GEOM_TBCT)
-            return set_error(CTR_ERR_UNSUPPORTED, "the slab split is the cone/fan/parallel build's (not CTR_GEOM_TBCT)");
-        // V63/main_recon.cu:24: volume height and detector rows split evenly
+        // V63/main_recon.cu:24, T42/main_recon.cu:18: volume height and detector rows split evenly
         if (din->nz % n_slabs != 0 || din->nv % n_slabs != 0)
             return set_error(CTR_ERR_BAD_GEOMETRY, "nz=%d and nv=%d must both split into %d slabs", din->nz, din->nv,
                              n_slabs);
@@ -202,12 +200,15 @@ static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ct
         // the volume's nearest point is at least -DOD - (half-diagonal) away
         const double half_diag = 0.5 * std::sqrt((double)d.nx * d.vx * d.nx * d.vx + (double)d.ny * d.vy * d.ny * d.vy) +
                                  std::fabs((double)d.m_offset * d.vx);
-        // (the tetrahedron beam's loop test, alpha_max - alpha_c > 1e-6f, has no one-comparison form)
-        q.fast_exit = (!tbct && (-(double)d.dod - half_diag) / ((double)d.dso - (double)d.dod) >= 1e-6) ? 1 : 0;
+        // (the tetrahedron beam's loop test, alpha_max - alpha_c > 1e-6f, has no one-comparison
+        // form; its multi-GPU build's projectors test against 1e-16f, as V63's)
+        const bool inside = (-(double)d.dod - half_diag) / ((double)d.dso - (double)d.dod) >= 1e-6;
+        q.fast_exit = ((!tbct || n_slabs > 1) && inside) ? 1 : 0;
     }
     q.entry64 = (d.flags & CTR_GEOM_ENTRY_F64) ? 1 : 0;
     q.ct_style = tbct ? 3 : ((d.flags & CTR_GEOM_FAN_SLICES) ? 1 : ((d.flags & CTR_GEOM_PARALLEL) ? 2 : 0));
-    q.loop_eps = tbct ? 1e-6f : 1e-16f;   // T42/...TBCT_voxel.cu:282, V63/...universal.cu:291
+    // T42/...TBCT_voxel.cu:282, V63/...universal.cu:291, T42/..._multiGPU.cu:303,853
+    q.loop_eps = (tbct && n_slabs == 1) ? 1e-6f : 1e-16f;
     q.vx = d.vx; q.vy = d.vy; q.vz = d.vz;
     // inv_volumn_x = 1.0/volumn_x (double division stored as float), main_recon.cu:88
     q.inv_vx = (float)(1.0 / (double)d.vx);
@@ -229,7 +230,15 @@ static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ct
     q.zpar_kr = tbct ? 0 : 1;
     q.row_lo = 0;
     q.row_hi = q.ZP;
-    if (n_slabs > 1) {
+    q.thr_comb = tbct ? d.vz * 1e-3f : d.vz * 1e-6f;
+    if (n_slabs > 1 && slab == -1) {
+        // the whole volume as the n-device build's row-split projector traverses it
+        // (V63/..._multiGPU.cu:21-590, T42/voxel/..._multiGPU.cu:22-576): V63's rules,
+        // so the tetrahedron beam gains the z-parallel k range; a whole-volume geometry otherwise
+        q.zpar_kr = 1;
+        q.slab_n = 1;
+        q.slab_i = 0;
+    } else if (n_slabs > 1) {
         const int zs = d.nz / n_slabs, k0 = zs * slab;
         q.bz = q.bz_ref + d.vz * (float)d.nz / (float)n_slabs * (float)slab;
         q.cz_off = d.vz * ((float)k0 + 0.5f);
@@ -238,7 +247,7 @@ static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ct
         if (q.ct_style == 1 || q.ct_style == 2) {   // :663
             q.row_lo = d.nv / n_slabs * slab;
             q.row_hi = d.nv / n_slabs * (slab + 1);
-        } else {
+        } else if (q.ct_style == 0) {
             // Cone beam: the rows whose rays can reach the slab at any view.  A
             // point at alpha of a ray lies at DOD + alpha*(DSO-DOD) along the
             // view's axis and at height x1z*(1-alpha) (the source at z = 0), and
@@ -281,9 +290,10 @@ static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ct
     q.zsrc0 = 0.0f;
     q.zsrc_dz = 0.0f;
     if (tbct && d.n_sources > 1) {                        // T42/main_recon.cu:76, :104-107
-        const float bzu = -d.vz * ((float)d.nz / 2.0f) + (float)d.nz * d.vz;
+        // placed from the whole volume's faces (din->nz, bz_ref), also for a slab
+        const float bzu = -d.vz * ((float)din->nz / 2.0f) + (float)din->nz * d.vz;
         const float zsmax = (bzu - q.zmax) * (d.dso - d.dod) / d.dso + q.zmax;
-        q.zsrc0 = (q.bz - q.zmin) * (d.dso - d.dod) / d.dso + q.zmin;
+        q.zsrc0 = (q.bz_ref - q.zmin) * (d.dso - d.dod) / d.dso + q.zmin;
         q.zsrc_dz = (zsmax - q.zsrc0) / (float)(d.n_sources - 1);
         if (!(q.zsrc_dz > 0.f)) {
             delete g;
@@ -471,6 +481,7 @@ extern "C" ctr_status ctr_geometry_destroy(ctr_geometry* geom)
     cudaFree(g->d_tiled);
     cudaFree(g->d_ramp);
     cudaFree(g->d_parts);
+    if (g->split_geom) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(g->split_geom));
     for (cudaStream_t q : g->slab_streams) cudaStreamDestroy(q);
     for (cudaEvent_t e : g->slab_events) cudaEventDestroy(e);
     for (Geometry* sg : g->slab_geoms) ctr_geometry_destroy(reinterpret_cast<ctr_geometry*>(sg));

@@ -32,8 +32,8 @@ __global__ void k_combine(const DevGeom g, const float2* __restrict__ parts, int
             reinterpret_cast<float*>(rays)[p] = w;
             continue;
         }
-        // kernel_divide_proj: 0 below volumn_z*1e-6f, else (b - w)*1.0f/l (x*1.0f is x)
-        const float corr = l < g.thr_fp ? 0.0f : fdv(fs(ld_any(b, p, b_dt), w), l);
+        // kernel_divide_proj: 0 below volumn_z*1e-6f (T42: 1e-3f), else (b - w)*1.0f/l (x*1.0f is x)
+        const float corr = l < g.thr_comb ? 0.0f : fdv(fs(ld_any(b, p, b_dt), w), l);
         const int v = (int)(p / g.R), u = (int)(p - (long long)v * g.R);
         rays[p] = make_float2(corr, ray_d12(ray_ends(g, sc.x, sc.y, u, v)));
     }

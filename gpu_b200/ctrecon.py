@@ -238,7 +238,8 @@ class Geometry:
 
     With ``n_slabs`` > 1: slab ``slab`` of the z split of the reference's
     multi-GPU build (``ctr_geometry_create_slab``); its volumes are that slab's
-    nz/n_slabs slices."""
+    nz/n_slabs slices; ``slab = -1``: the whole volume as that build's
+    row-split projector traverses it."""
 
     def __init__(self, desc: GeometryDesc, n_slabs: int = 1, slab: int = 0):
         self.lib = load_library()
@@ -265,12 +266,14 @@ class Geometry:
     # shapes
     @property
     def vol_shape(self):
-        return (self.desc.nz // self.n_slabs, self.desc.ny, self.desc.nx)
+        # slab -1: the whole volume (the n-device build's row-split projector)
+        nz = self.desc.nz // self.n_slabs if self.slab >= 0 else self.desc.nz
+        return (nz, self.desc.ny, self.desc.nx)
 
     @property
     def first_slice(self):
         """Index in the whole volume of this geometry's first slice."""
-        return self.vol_shape[0] * self.slab
+        return self.vol_shape[0] * max(self.slab, 0)
 
     def slab_info(self):
         """(n_slabs, slab, first slice) as the library holds them (``ctr_geometry_slab``)."""

@@ -217,14 +217,22 @@ ctr_status ctr_sart_views_noalloc(const ctr_geometry* geom, void* vol, ctr_dtype
  * The rounding differs from the one-device pass (a ray's sum is the sum of
  * its slabs' sums; the slab planes are computed from the slab's boundary), so
  * these calls reproduce the D-device build, not the one-device one.  ZETA and
- * Z_prj must split evenly into D (V63/main_recon.cu:24); not for CTR_GEOM_TBCT.
+ * Z_prj must split evenly into D (V63/main_recon.cu:24).  The tetrahedron-beam
+ * program's default build is its multi-GPU one too (T42/main_recon.cu:17,
+ * T42/voxel/kernel_IterativeRecon_TBCT_voxel_multiGPU.cu): the same sequence with its sources, its
+ * projectors testing alpha_max - alpha_c > 1e-16f (its one-device one: 1e-6f),
+ * its combination zeroing below volumn_z*1e-3f, and its slab backprojector's
+ * voxel centres; CTR_GEOM_TBCT geometries get those.
  *
  * Slab s of D of a scan: a geometry of nz/D slices.  Volumes passed with it
  * are that slab's nx*ny*(nz/D) voxels; its z planes, voxel centres and (for
  * CTR_GEOM_FAN_SLICES / CTR_GEOM_PARALLEL) traced detector rows are the
- * multi-GPU build's.  Not for the solver or FDK. */
+ * multi-GPU build's.  s = -1: the whole volume as the D-device build's
+ * row-split projector (its Forward_3D_ray_driven_siddon) traverses it -- for
+ * the tetrahedron beam V63's traversal rules, otherwise the one-device
+ * projector.  Not for the solver or FDK. */
 ctr_status ctr_geometry_create_slab(const ctr_geometry_desc* desc, int n_slabs, int slab, ctr_geometry** out);
-/* D (1 for a whole-volume geometry), s, and the slab's first slice in the volume. */
+/* D (1 for a whole-volume geometry, s = -1 included), s, and the slab's first slice in the volume. */
 ctr_status ctr_geometry_slab(const ctr_geometry* geom, int* n_slabs, int* slab, int* first_slice);
 
 /* Per-view calls of one slab, for a host that holds one slab per GPU and
@@ -369,8 +377,9 @@ ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k);
  * projector (the sums the n-device build's row-split projector gives) rather
  * than inside the next pass, and the pass is issued without a CUDA graph.
  * With sart_flags = CTR_SART_REFERENCE_BP and FP32 storage the SART + FISTA +
- * FGP-TV loop and its objectives equal that build's.  ZETA and Z_prj must
- * split into n_slabs; not for CTR_GEOM_TBCT. */
+ * FGP-TV loop and its objectives equal that build's (for CTR_GEOM_TBCT the
+ * objective's projector is that build's row-split one).  ZETA and Z_prj must
+ * split into n_slabs. */
 ctr_status ctr_solver_set_slabs(ctr_solver* s, int n_slabs);
 /* Objective history [TV, fidelity, objective] of iterations first..first+count-1
  * (1-based, at most the iterations run).  With objective_out == NULL,
@@ -452,10 +461,11 @@ ctr_status ctr_io_write_views(const char* dir, int nu, int nv, int n_views, floa
  * and report failures through ctr_last_error_string(). */
 ctr_status ctr_set_default_geometry(const ctr_geometry_desc* desc);
 /* Number_of_Devices of the reference build being replaced (V63/main_recon.cu:23,
- * default 1).  With n > 1 Reconstruction_3D_ray_driven_CBCT and
- * CheckMatchedJointOperator compute what the n-device build computes (the
- * z-slab sequence above, on the current GPU); Forward_3D_ray_driven_siddon's
- * row split gives the one-device projections already. */
+ * T42/main_recon.cu:17; default 1).  With n > 1 Reconstruction_3D_ray_driven_CBCT
+ * and CheckMatchedJointOperator compute what the n-device build computes (the
+ * z-slab sequence above, on the current GPU); Forward_3D_ray_driven_siddon
+ * projects as its row-split projector (V63's is the one-device one; the
+ * tetrahedron beam's follows V63's traversal rules). */
 ctr_status ctr_set_default_devices(int n);
 
 /* V63/host_IterativeRecon_CBCT.c:70-128: A x for all views into h_proj_data. */

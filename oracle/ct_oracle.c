@@ -73,6 +73,18 @@ int og_init(og_geom* g, const og_desc* d)
     g->zpar_kr = e->ct_style != 3;
     g->row_lo = 0;
     g->row_hi = g->rows;
+    /* T42's one-device projector stops at alpha_max - alpha_c > 1e-6f
+     * (T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:282); V63's and T42's
+     * multi-GPU projectors at 1e-16f (T42/voxel/..._multiGPU.cu:303,853) */
+    g->loop_eps = e->ct_style == 3 && e->n_slabs <= 1 ? 1e-6f : 1e-16f;
+    if (e->n_slabs > 1 && e->slab == -1) {
+        /* the whole volume as the multi-GPU build's row-split projector
+         * traverses it (V63/..._multiGPU.cu:21-590, T42/voxel/..._multiGPU.cu:22-576):
+         * V63's own rules, so T42's gains the z-parallel k range */
+        if (e->nz % e->n_slabs != 0 || e->nv % e->n_slabs != 0) return -1;
+        g->zpar_kr = 1;
+        return 0;
+    }
     if (e->n_slabs > 1) {
         /* slab subVolIdx of the multi-GPU build: ZETA/D slices, its own
          * BOUNDARY_VOXEL_Z and ZETA_new in every z plane of the traversal, no
@@ -80,7 +92,7 @@ int og_init(og_geom* g, const og_desc* d)
          * 636-637,686-687,775-800,891); fan-slice and parallel beams trace only the rows of
          * the slab's band (:663).  ZETA and Z_prj split evenly (V63/main_recon.cu:24). */
         const int D = e->n_slabs, sl = e->slab, Z = e->nz;
-        if (e->ct_style == 3 || sl < 0 || sl >= D || Z % D != 0 || e->nv % D != 0) return -1;
+        if (sl < 0 || sl >= D || Z % D != 0 || e->nv % D != 0) return -1;
         g->d.nz = Z / D;
         g->k0 = Z / D * sl;
         g->bz = g->bz_ref + e->vz * (float)Z / (float)D * (float)sl;
@@ -306,7 +318,7 @@ static inline float og_traverse(const og_geom* g, float s, float c, int u, int v
          * is the same rule for all non-NaN alphas. */
         const int maxsteps = M + N + Z + 3;
         int steps = 0;
-        const float eps = tb ? 1e-6f : 1e-16f;
+        const float eps = g->loop_eps;
         while (amax - ac > eps) {
             if (vi > M - 1 || vi < 0 || vj > N - 1 || vj < 0 || vk > Z - 1 || vk < 0) break;
             if (++steps > maxsteps) break;   /* unreachable for finite alphas */
@@ -578,6 +590,24 @@ int og_fov_masked(const og_geom* g, int i, int j)
  * two zeroed volumes by atomicAdd; update (:765-775) then adds
  * beta*sum/length where the summed length exceeds volumn_x*1e-3 (a double
  * comparison).  Sources are added in ascending order here. */
+/* The tetrahedron-beam backprojector's voxel centre: bx + vx*(0.5f + i)
+ * (T42/voxel/kernel_IterativeRecon_TBCT_voxel.cu:568-570), or in a slab of its
+ * multi-GPU build bx + vx*0.5f + i*vx and boundary_voxel_z +
+ * vz*(ZETA/D*s + 0.5f) + k*vz (T42/voxel/..._multiGPU.cu:1140-1142). */
+static inline void og_tb_centre(const og_geom* g, int i, int j, int k, float* cx, float* cy, float* cz)
+{
+    const float vx = g->d.vx, vy = g->d.vy, vz = g->d.vz;
+    if (g->d.n_slabs > 1) {
+        *cx = g->bx + vx * 0.5f + (float)i * vx;
+        *cy = g->by + vy * 0.5f + (float)j * vy;
+        *cz = g->bz_ref + vz * ((float)g->k0 + 0.5f) + (float)k * vz;
+    } else {
+        *cx = g->bx + vx * (0.5f + (float)i);
+        *cy = g->by + vy * (0.5f + (float)j);
+        *cz = g->bz + vz * (0.5f + (float)k);
+    }
+}
+
 static void og_backproject_ref_tbct(const og_geom* g, float* vol, const float* corr, float beta, float s, float c)
 {
     const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->d.nv, K = g->d.n_sources;
@@ -592,9 +622,8 @@ static void og_backproject_ref_tbct(const og_geom* g, float* vol, const float* c
                 const long long idx = (long long)M * N * k + (long long)M * j + i;
                 float WS = 0.0f, L = 0.0f;                               /* the zeroed sums */
                 if (!og_fov_masked(g, i, j)) {                           /* :600-608 */
-                    const float cx = g->bx + vx * (0.5f + (float)i);    /* :568-570 */
-                    const float cy = g->by + vy * (0.5f + (float)j);
-                    const float cz = g->bz + vz * (0.5f + (float)k);
+                    float cx, cy, cz;
+                    og_tb_centre(g, i, j, k, &cx, &cy, &cz);
                     const float sx = g->srcx * c - g->srcy * s;          /* :613-614 */
                     const float sy = g->srcx * s + g->srcy * c;
                     const float tc = cx * c + cy * s;                    /* :620 */
@@ -1337,8 +1366,8 @@ static void og_backproject_gather_tbct(const og_geom* g, float* vol, const float
             for (int i = 0; i < M; ++i) {
                 if (og_fov_masked(g, i, j)) continue;
                 /* source exclusion, with the reference's voxel centre */
-                const float cxr = g->bx + vx * (0.5f + (float)i), cyr = g->by + vy * (0.5f + (float)j);
-                const float czr = g->bz + vz * (0.5f + (float)k);
+                float cxr, cyr, czr;
+                og_tb_centre(g, i, j, k, &cxr, &cyr, &czr);
                 const float tc = cxr * c + cyr * s;
                 const float upper = (czr + vz - g->zmin) * (DSO - DOD) / (tc - DOD) + g->zmin;
                 const float lower = (czr - vz - g->zmax) * (DSO - DOD) / (tc - DOD) + g->zmax;
@@ -1532,7 +1561,9 @@ void og_combine_partials(const og_geom* g, int n_parts, const float* wsum, const
                          float* corr)
 {
     const long long P = (long long)g->d.nu * g->rows;
-    const float thr = g->d.vz * 1e-6f;
+    /* V63's kernel_divide_proj zeroes below volumn_z*1e-6f, T42's below
+     * volumn_z*1e-3f (T42/voxel/kernel_IterativeRecon_TBCT_voxel_multiGPU.cu:14) */
+    const float thr = g->d.ct_style == 3 ? g->d.vz * 1e-3f : g->d.vz * 1e-6f;
     for (long long p = 0; p < P; ++p) {
         float w = 0.0f, l = 0.0f;                              /* memset, multiGPU.c:82-83 */
         for (int i = 0; i < n_parts; ++i) {                    /* kernel_add_proj, multiGPU.cu:1-5 */

@@ -54,7 +54,9 @@ typedef struct og_desc {
     int   n_slabs;           /* > 1: the z-slab split of the multi-GPU SART  */
                              /* (V63 Number_of_Devices): this description is */
     int   slab;              /* slab `slab` (subVolIdx) of n_slabs, nz/n_slabs*/
-                             /* slices of the nz-slice volume; 0/1: no split  */
+                             /* slices of the nz-slice volume; 0/1: no split; */
+                             /* -1: the whole volume as the n_slabs-device    */
+                             /* build's row-split projector traverses it      */
 } og_desc;
 
 /* Derived constants, computed with the reference's float/double steps. */
@@ -78,6 +80,9 @@ typedef struct og_geom {
                                     /* applies (not T42's, not a slab's)      */
     int   row_lo, row_hi;           /* CT_style 1/2 slab: rows of its band    */
                                     /* (multiGPU.cu:663); else 0, rows        */
+    float loop_eps;                 /* Siddon loop test alpha_max - alpha_c > */
+                                    /* loop_eps: 1e-6f in T42's one-device     */
+                                    /* projector, 1e-16f everywhere else        */
 } og_geom;
 
 int  og_init(og_geom* g, const og_desc* d);

@@ -20,6 +20,8 @@ REF_SO = os.path.join(HERE, "_ref", "libctref.so")
 # (3: the tetrahedron-beam program's kernels)
 REF_SO_STYLE = {0: REF_SO, 1: os.path.join(HERE, "_ref", "libctref_fbct.so"),
                 2: os.path.join(HERE, "_ref", "libctref_pbct.so"), 3: os.path.join(HERE, "_ref", "libctref_tbct.so")}
+# the tetrahedron-beam program's multi-GPU build (its own kernels)
+REF_SO_TBCT_MULTI = os.path.join(HERE, "_ref", "libctref_tbct_multi.so")
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -52,6 +54,7 @@ class OgGeom(C.Structure):
         ("srcx", C.c_float), ("srcy", C.c_float), ("srcz", C.c_float),
         ("zmax", C.c_float), ("zsrc0", C.c_float), ("zsrc_dz", C.c_float), ("rows", C.c_int),
         ("k0", C.c_int), ("bz_ref", C.c_float), ("zpar_kr", C.c_int), ("row_lo", C.c_int), ("row_hi", C.c_int),
+        ("loop_eps", C.c_float),
     ]
 
 
@@ -73,7 +76,8 @@ def make_desc(nx, ny, nz, nu, nv, nviews, vx, du, dso, dod, us_rate=None,
 def slab_desc(desc: OgDesc, n_slabs: int, slab: int) -> OgDesc:
     """The description of slab ``slab`` of the ``n_slabs``-way z split of the
     multi-GPU build (its kernels take the whole scan's constants plus the
-    device index)."""
+    device index); ``slab = -1``: the whole volume as that build's row-split
+    projector traverses it."""
     d = OgDesc()
     C.pointer(d)[0] = desc
     d.n_slabs, d.slab = n_slabs, slab
@@ -350,8 +354,9 @@ class Oracle:
 class RefOracle:
     """The reference's own kernels compiled for the CPU (``_ref/libctref.so``)."""
 
-    def __init__(self, desc: OgDesc):
-        so = REF_SO_STYLE[desc.ct_style]
+    def __init__(self, desc: OgDesc, multi: bool = False):
+        """multi: the tetrahedron-beam program's multi-GPU build (its slab calls)."""
+        so = REF_SO_TBCT_MULTI if multi and desc.ct_style == 3 else REF_SO_STYLE[desc.ct_style]
         if not os.path.exists(so):
             raise FileNotFoundError(so)
         self.lib = lib = C.CDLL(so)

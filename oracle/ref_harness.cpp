@@ -14,7 +14,11 @@
  * With -DREF_TBCT the same harness runs the tetrahedron-beam program's
  * projector, backprojector and update kernels instead
  * (TBCT/TBCT_1024V_1024P_v4.2_20171012/voxel/kernel_IterativeRecon_TBCT_voxel.cu,
- * abbreviated T42/, read from REF_TBCT_DIR; output oracle/_ref/libctref_tbct.so).
+ * abbreviated T42/, read from REF_TBCT_DIR; output oracle/_ref/libctref_tbct.so);
+ * with -DREF_TBCT -DREF_TBCT_MULTI its multi-GPU build's kernels
+ * (T42/voxel/kernel_IterativeRecon_TBCT_voxel_multiGPU.cu) with its host
+ * sequence (T42/voxel/host_IterativeRecon_TBCT_voxel_multiGPU.c), the devices
+ * a loop over the slabs (oracle/_ref/libctref_tbct_multi.so).
  * Its atomicAdd becomes a plain add: a voxel's sources are launched in
  * ascending order by one thread.
  *
@@ -71,7 +75,13 @@ static inline float atomicAdd(float* p, float v)
     *p = o + v;
     return o;
 }
+#ifdef REF_TBCT_MULTI
+/* the multi-GPU build's device count (T42/main_recon.cu:17), set per call */
+static int Number_of_Devices = 1;
+#include REF_STR(REF_TBCT_DIR/voxel/kernel_IterativeRecon_TBCT_voxel_multiGPU.cu)
+#else
 #include REF_STR(REF_TBCT_DIR/voxel/kernel_IterativeRecon_TBCT_voxel.cu)
+#endif
 #else
 /* the multi-GPU build's device count (V63/main_recon.cu:23), set per call */
 static int Number_of_Devices = 1;
@@ -146,7 +156,152 @@ void ref_view_trig(int j, int fdk, float* s_out, float* c_out)
     *c_out = cos(t_theta);
 }
 
-#ifdef REF_TBCT
+#if defined(REF_TBCT) && defined(REF_TBCT_MULTI)
+static int ref_devices(int D)
+{
+    if (D < 1 || ZETA % D != 0 || Z_prj % D != 0) return -1;
+    Number_of_Devices = D;
+    return 0;
+}
+
+/* forward_ray_driven_3d_kernel_correction_separate over grid (1, Z_prj, N_source) x
+ * block R on slab sub (T42/voxel/host_IterativeRecon_TBCT_voxel_multiGPU.c:78-82) */
+int ref_slab_forward_view(int D, int sub, const float* vol_slab, float* sumLen, float* weightedLen, float s, float c)
+{
+    if (ref_devices(D) != 0) return -1;
+#pragma omp parallel for collapse(2) schedule(dynamic, 1)
+    for (int src = 0; src < N_source; ++src)
+        for (int v = 0; v < Z_prj; ++v) {
+            tl_blockDim = {(unsigned)R, 1, 1};
+            tl_gridDim = {1, (unsigned)Z_prj, (unsigned)N_source};
+            for (int u = 0; u < R; ++u) {
+                tl_blockIdx = {0, (unsigned)v, (unsigned)src};
+                tl_threadIdx = {(unsigned)u, 0, 0};
+                forward_ray_driven_3d_kernel_correction_separate((float*)vol_slab, sumLen, weightedLen, s, c, sub);
+            }
+        }
+    return 0;
+}
+
+/* the host's combination (multiGPU.c:89-101): memset, kernel_add_proj per device
+ * in order (weighted, then lengths), kernel_divide_proj; parts [D][N_source*Z_prj*R] */
+int ref_combine_view(int D, const float* sumLen, const float* weightedLen, const float* b, float* corr)
+{
+    if (ref_devices(D) != 0) return -1;
+    const long long P = (long long)R * Z_prj * N_source;
+    float* hs = (float*)calloc(P, sizeof(float));
+    float* hw = (float*)calloc(P, sizeof(float));
+    auto grid = [&](auto&& fn) {
+        tl_blockDim = {(unsigned)R, 1, 1};
+        tl_gridDim = {1, (unsigned)Z_prj, (unsigned)N_source};
+        for (int src = 0; src < N_source; ++src)
+            for (int v = 0; v < Z_prj; ++v)
+                for (int u = 0; u < R; ++u) {
+                    tl_blockIdx = {0, (unsigned)v, (unsigned)src};
+                    tl_threadIdx = {(unsigned)u, 0, 0};
+                    fn();
+                }
+    };
+    for (int i = 0; i < D; ++i) {
+        grid([&] { kernel_add_proj(hw, (float*)weightedLen + P * i); });
+        grid([&] { kernel_add_proj(hs, (float*)sumLen + P * i); });
+    }
+    grid([&] { kernel_divide_proj(corr, (float*)b, hs, hw); });
+    free(hs);
+    free(hw);
+    return 0;
+}
+
+/* backprj_ray_driven_3d_kernel_multiGPU into zeroed slab volumes (a voxel's
+ * sources in ascending order), then update (multiGPU.c:119-135); command is
+ * ignored, as the kernels have none */
+int ref_slab_backproject_view(int D, int sub, float* vol_slab, const float* corr, float beta, float s, float c,
+                              int command)
+{
+    (void)command;
+    if (ref_devices(D) != 0) return -1;
+    const int Zs = ZETA / D;
+    const long long V = (long long)M * N * Zs;
+    float* ws = (float*)calloc(V, sizeof(float));
+    float* len = (float*)calloc(V, sizeof(float));
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = 0; k < Zs; ++k)
+        for (int j = 0; j < N; ++j) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            tl_gridDim = {(unsigned)N, (unsigned)Zs, (unsigned)N_source};
+            for (int src = 0; src < N_source; ++src)
+                for (int i = 0; i < M; ++i) {
+                    tl_blockIdx = {(unsigned)j, (unsigned)k, (unsigned)src};
+                    tl_threadIdx = {(unsigned)i, 0, 0};
+                    backprj_ray_driven_3d_kernel_multiGPU(ws, len, (float*)corr, s, c, sub);
+                }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Zs; ++k)
+        for (int j = 0; j < N; ++j) {
+            tl_blockDim = {(unsigned)M, 1, 1};
+            for (int i = 0; i < M; ++i) {
+                tl_blockIdx = {(unsigned)j, (unsigned)k, 0};
+                tl_threadIdx = {(unsigned)i, 0, 0};
+                update(vol_slab, ws, len, beta);
+            }
+        }
+    free(ws);
+    free(len);
+    return 0;
+}
+
+/* Reconstruction_3D_ray_driven_TBCT of the multi-GPU build (multiGPU.c:1-183) for
+ * the views [v0, v0+nv); the volume is the D slabs back to back (:44-48) */
+int ref_sart_views_slabs(int D, float* vol, const float* sino, float beta, int v0, int nv)
+{
+    if (ref_devices(D) != 0) return -1;
+    const long long P = (long long)R * Z_prj * N_source, Vs = (long long)M * N * (ZETA / D);
+    float* sl = (float*)calloc(P * D, sizeof(float));
+    float* wl = (float*)calloc(P * D, sizeof(float));
+    float* corr = (float*)malloc(sizeof(float) * P);
+    for (int j = v0; j < v0 + nv; ++j) {
+        float s, c;
+        ref_view_trig(j, 0, &s, &c);
+        for (int i = 0; i < D; ++i) ref_slab_forward_view(D, i, vol + Vs * i, sl + P * i, wl + P * i, s, c);
+        ref_combine_view(D, sl, wl, sino + P * j, corr);
+        for (int i = 0; i < D; ++i) ref_slab_backproject_view(D, i, vol + Vs * i, corr, beta, s, c, 1);
+    }
+    free(sl);
+    free(wl);
+    free(corr);
+    return 0;
+}
+
+/* Forward_3D_ray_driven_siddon_TBCT of the multi-GPU build, one view
+ * (multiGPU.c:185-306): device i projects rows [Z_prj/D*i, Z_prj/D*(i+1)) of
+ * every source's band with forward_ray_driven_3d_kernel_correction_multiGPU,
+ * command 0, into [src][row][col] portions copied back per source (:264-267) */
+int ref_forward_view_split(int D, const float* vol, float* out, float s, float c)
+{
+    if (ref_devices(D) != 0) return -1;
+    const int rows = Z_prj / D;
+    float* part = (float*)malloc(sizeof(float) * (size_t)R * rows * N_source);
+    for (int i = 0; i < D; ++i) {
+#pragma omp parallel for collapse(2) schedule(dynamic, 1)
+        for (int src = 0; src < N_source; ++src)
+            for (int v = 0; v < rows; ++v) {
+                tl_blockDim = {(unsigned)R, 1, 1};
+                tl_gridDim = {1, (unsigned)rows, (unsigned)N_source};
+                for (int u = 0; u < R; ++u) {
+                    tl_blockIdx = {0, (unsigned)v, (unsigned)src};
+                    tl_threadIdx = {(unsigned)u, 0, 0};
+                    forward_ray_driven_3d_kernel_correction_multiGPU((float*)vol, part, part, s, c, i, 0);
+                }
+            }
+        for (int k = 0; k < N_source; ++k)
+            memcpy(out + (size_t)R * Z_prj * k + (size_t)R * rows * i, part + (size_t)R * rows * k,
+                   sizeof(float) * R * rows);
+    }
+    free(part);
+    return 0;
+}
+#elif defined(REF_TBCT)
 /* forward_ray_driven_3d_kernel_correction over grid (1, Z_prj, N_source) x block R
  * (T42/voxel/host_IterativeRecon_TBCT_voxel.c:48-49, one block row per launch here) */
 void ref_forward_view(const float* vol, float* out, const float* b, float s, float c, int command)

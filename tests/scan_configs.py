@@ -80,6 +80,10 @@ SLABS = {
                       initial_angle=3.5, ct_style=1, slabs=[3]),
     "parallel_slabs": dict(nx=16, ny=16, nz=12, nu=24, nv=12, nviews=12, vx=1.0, du=1.2, dso=1000.0, dod=-500.0,
                            ct_style=2, slabs=[2, 4]),
+    # the tetrahedron-beam program's multi-GPU build (its default, T42/main_recon.cu:17)
+    "tbct_slabs": dict(TBCT["tbct"], slabs=[2, 4]),
+    "tbct_slab3": dict(nx=15, ny=17, nz=12, nu=31, nv=6, nviews=8, vx=1.0, du=1.1, dso=50.0, dod=-30.0, offset=0.7,
+                       m_offset=1, shift_angle=3.0, ct_style=3, n_sources=3, slabs=[3]),
 }
 
 

@@ -117,10 +117,11 @@ def test_one_gpu_slab_pass(name, D, oracle_built):
     np.testing.assert_array_equal(bits(x.cpu().numpy()), bits(want))
 
 
-@pytest.mark.parametrize("name,D", [("cone_wide", 4), ("fan_edges", 3), ("parallel_slabs", 2)])
+@pytest.mark.parametrize("name,D", [("cone_wide", 4), ("fan_edges", 3), ("parallel_slabs", 2), ("tbct_slabs", 4)])
 def test_reference_compatible_entry_point_with_devices(name, D, oracle_built, capfd):
-    """Number_of_Devices = D: Reconstruction_3D_ray_driven_CBCT returns the
-    D-device build's numbers; back at 1 device, the one-device build's."""
+    """Number_of_Devices = D: Reconstruction_3D_ray_driven_CBCT and
+    Forward_3D_ray_driven_siddon return the D-device build's numbers; back at
+    1 device, the one-device build's."""
     import gpu_b200
     cfg = SLABS[name]
     g = load(name)
@@ -131,9 +132,14 @@ def test_reference_compatible_entry_point_with_devices(name, D, oracle_built, ca
         gpu_b200.reconstruction_3d_ray_driven_cbct(x, g["b"].copy(), 0.8)
         assert gpu_b200.last_error() == ""
         np.testing.assert_array_equal(bits(x), bits(g[f"sart_{D}"]))
-        gpu_b200.check_matched_joint_operator(g["vol0"].copy())   # the D-device check runs and prints
+        proj = np.zeros_like(g["b"])
+        gpu_b200.forward_3d_ray_driven_siddon(g["vol0"].copy(), proj)
         assert gpu_b200.last_error() == ""
-        assert "inner product" in capfd.readouterr().out
+        np.testing.assert_array_equal(bits(proj[int(g["view"])]), bits(g[f"fwd_split_{D}"]))
+        if cfg.get("ct_style", 0) != 3:   # T42's backprojector has no command 0 for the check
+            gpu_b200.check_matched_joint_operator(g["vol0"].copy())   # the D-device check runs and prints
+            assert gpu_b200.last_error() == ""
+            assert "inner product" in capfd.readouterr().out
     finally:
         gpu_b200.set_default_devices(1)
     x = g["vol0"].copy()
@@ -152,8 +158,9 @@ def test_slab_geometry_errors():
         gpu_b200.Geometry(ctr_desc(cfg), 3, 3)
     tb = dict(nx=16, ny=16, nz=16, nu=32, nv=4, nviews=4, vx=1.0, du=1.2, dso=40.0, dod=-40.0, ct_style=3,
               n_sources=2)
-    with pytest.raises(gpu_b200.CtrError):                     # the tetrahedron beam: not this build's split
-        gpu_b200.Geometry(ctr_desc(tb), 2, 0)
+    with pytest.raises(gpu_b200.CtrError):                     # the tetrahedron beam: 16 slices in 3
+        gpu_b200.Geometry(ctr_desc(tb), 3, 0)
+    assert gpu_b200.Geometry(ctr_desc(tb), 2, 1).slab_info() == (2, 1, 8)   # its multi-GPU build's slab
     sg = gpu_b200.Geometry(ctr_desc(cfg), 3, 1)
     with pytest.raises(gpu_b200.CtrError):                     # the solver needs the whole volume
         gpu_b200.Solver(sg, gpu_b200.F32)
@@ -239,16 +246,18 @@ def test_slab_driver_over_nccl_one_rank(oracle_built):
         dist.destroy_process_group()
 
 
-def test_solver_with_slabs_equals_reference_loop(oracle_built):
-    """ctr_solver_set_slabs(4) with the reference's backprojection arithmetic:
+@pytest.mark.parametrize("name,D", [("cone_wide", 4), ("tbct_slabs", 2)])
+def test_solver_with_slabs_equals_reference_loop(name, D, oracle_built):
+    """ctr_solver_set_slabs(D) with the reference's backprojection arithmetic:
     three SART + FISTA + FGP-TV iterations (V63/main_recon.cu:344-430) equal
-    the reference's 4-device loop restated by the oracle, volume bit for bit
-    and objectives to 1e-12 (the objective projected by the one-device
-    projector, as the 4-device build's row split does); set_slabs(1) then
-    continues with the one-device pass."""
+    the reference's D-device loop restated by the oracle, volume bit for bit
+    and objectives to 1e-12 (the objective projected by the D-device build's
+    row-split projector: V63's one-device projector, for the tetrahedron beam
+    its multi-GPU rules); set_slabs(1) then continues with the one-device pass."""
     import gpu_b200
-    cfg, D = SLABS["cone_wide"], 4
+    cfg = SLABS[name]
     o = oracle_built.Oracle(og_desc(cfg))
+    split = oracle_built.Oracle(oracle_built.slab_desc(og_desc(cfg), D, -1))
     truth = o.phantom(np.array([[0, 0, 0, 5, 4, 3, 0.3, 0.2, 0.1, 0.02], [1.5, -1, 0.5, 2, 2, 2, 0, 0, 0, 0.03]]))
     b = np.stack([o.forward_view(truth, j, 0) for j in range(cfg["nviews"])])
     beta, lam, it = np.float32(0.8), np.float32(0.05), 5
@@ -270,7 +279,7 @@ def test_solver_with_slabs_equals_reference_loop(oracle_built):
         t_k = (np.float32(1.0) + np.sqrt(np.float32(1.0) + np.float32(4.0) * t * t, dtype=np.float32)) / np.float32(2.0)
         y, xprev = o.fista_momentum(y, xprev, x, t, t_k)
         t = np.float32(t_k)
-        fid = o.l2_norm(np.stack([o.forward_view(x, j, 0) for j in range(cfg["nviews"])]), b)
+        fid = o.l2_norm(np.stack([split.forward_view(x, j, 0) for j in range(cfg["nviews"])]), b)
         tv = o.tv_norm(x)
         want.append((tv, fid, fid + 2.0 * float(lam) * tv))
     np.testing.assert_array_equal(bits(out.cpu().numpy()), bits(xprev))
@@ -284,3 +293,17 @@ def test_solver_with_slabs_equals_reference_loop(oracle_built):
     _, xprev = o.fista_momentum(y, xprev, x, t, t_k)
     np.testing.assert_array_equal(bits(out.cpu().numpy()), bits(xprev))
     s.close()
+
+
+@pytest.mark.parametrize("name,D", CASES)
+def test_row_split_projector(name, D):
+    """ctr_geometry_create_slab(desc, D, -1): the whole volume projected as the
+    D-device build's row-split projector does (golden, from its kernels)."""
+    import gpu_b200
+    g = load(name)
+    geom = gpu_b200.Geometry(ctr_desc(SLABS[name]), D, -1)
+    assert geom.vol_shape == g["vol0"].shape and geom.slab_info() == (1, 0, 0)
+    out = torch.zeros((1,) + geom.view_shape, device="cuda")
+    j = int(g["view"])
+    geom.forward(dev(g["vol0"]), out, j, 1)
+    np.testing.assert_array_equal(bits(out[0].cpu().numpy()), bits(g[f"fwd_split_{D}"]))

@@ -3,13 +3,16 @@
 The fixtures (tests/golden/make_golden_slabs.py) come from the reference's
 multi-GPU kernels (V63/kernel_IterativeRecon_universal_multiGPU.cu) run on
 the CPU with its host sequence (V63/host_IterativeRecon_CBCT_multiGPU.c),
-the devices a loop over the slabs.  The restatement must reproduce, bit for
+the devices a loop over the slabs, and from the tetrahedron-beam program's
+own multi-GPU build (T42/voxel/*_multiGPU.*).  The restatement must reproduce, bit for
 bit, each slab's partial ray sums, the ordered combination into the SART
 correction, the slab backprojections (commands 0 and 1) and whole passes.
 Where oracle/_ref is built, the same comparisons also run live on fresh
 inputs, and the reference's row-split forward projection is checked against
-its one-device projection (the reason the one-device projector serves the
-D-device Forward_3D_ray_driven_siddon).
+the oracle's (slab -1) and, for V63, against its one-device projection (the
+reason the one-device projector serves V63's D-device
+Forward_3D_ray_driven_siddon; T42's multi-GPU projectors use V63's
+traversal rules instead of its own).
 """
 import os
 
@@ -71,7 +74,7 @@ def test_slab_pass_is_not_the_one_device_pass(oracle_built):
     at z = +-4 (not the one at z = 0, the source's height), the 0.7 mm slabs'
     planes round differently, and fan-slice rows on a slab plane are traced by
     neither slab."""
-    for name, D in (("cone_wide", 4), ("pitch07", 3), ("fan_edges", 3)):
+    for name, D in (("cone_wide", 4), ("pitch07", 3), ("fan_edges", 3), ("tbct_slabs", 4)):
         cfg = SLABS[name]
         g = load(name)
         o = oracle_built.Oracle(og_desc(cfg))
@@ -87,13 +90,23 @@ def test_slab_geometry_rejects_uneven_splits(oracle_built):
             oracle_built.Oracle(oracle_built.slab_desc(d, D, 0))
     tb = og_desc(dict(nx=16, ny=16, nz=16, nu=32, nv=4, nviews=4, vx=1.0, du=1.2, dso=40.0, dod=-40.0,
                       ct_style=3, n_sources=2))
-    with pytest.raises(ValueError):        # the tetrahedron beam has its own multi-GPU program
-        oracle_built.Oracle(oracle_built.slab_desc(tb, 2, 0))
+    for D in (3, 8):                       # 16 slices / 4 rows per band do not split
+        with pytest.raises(ValueError):
+            oracle_built.Oracle(oracle_built.slab_desc(tb, D, 0))
 
 
-def _ref_or_skip(oracle_built, d):
+@pytest.mark.parametrize("name,D", CASES)
+def test_row_split_forward_equals_reference_golden(name, D, oracle_built):
+    """The D-device build's whole-view projector (slab -1: V63's traversal
+    rules, which T42's multi-GPU build also uses) against its kernels' output."""
+    g = load(name)
+    o = oracle_built.Oracle(oracle_built.slab_desc(og_desc(SLABS[name]), D, -1))
+    np.testing.assert_array_equal(bits(o.forward_view(g["vol0"], int(g["view"]), 0)), bits(g[f"fwd_split_{D}"]))
+
+
+def _ref_or_skip(oracle_built, d, multi=False):
     try:
-        return oracle_built.RefOracle(d)
+        return oracle_built.RefOracle(d, multi=multi)
     except FileNotFoundError:
         pytest.skip("oracle/_ref not built (needs the reference checkout)")
 
@@ -104,7 +117,8 @@ def test_live_against_reference_kernels(name, D, oracle_built):
     the reference's kernels run now."""
     cfg = SLABS[name]
     d = og_desc(cfg)
-    ref = _ref_or_skip(oracle_built, d)
+    ref = _ref_or_skip(oracle_built, d, multi=True)   # the multi-GPU kernels (T42's own for its scans)
+    one = _ref_or_skip(oracle_built, d)
     o = oracle_built.Oracle(d)
     rng = np.random.default_rng(77 + D)
     truth = o.phantom(np.array([[0, 0, 0, 5, 4, 3, 0.3, 0.2, 0.1, 0.02], [1.5, -1, 0.5, 2, 2, 2, 0, 0, 0, 0.03]]))
@@ -112,5 +126,9 @@ def test_live_against_reference_kernels(name, D, oracle_built):
     vol = rng.uniform(0, 0.02, o.vol_shape).astype(np.float32)
     vol[rng.uniform(size=vol.shape) < 0.05] = -0.0
     np.testing.assert_array_equal(bits(o.sart_pass_slabs(vol, b, 0.8, D)), bits(ref.sart_slabs(vol, b, 0.8, D)))
+    split = oracle_built.Oracle(oracle_built.slab_desc(d, D, -1))
     for j in (0, cfg["nviews"] - 1):
-        np.testing.assert_array_equal(bits(ref.forward_view_split(truth, D, j)), bits(ref.forward_view(truth, j, 0)))
+        want = ref.forward_view_split(truth, D, j)
+        np.testing.assert_array_equal(bits(split.forward_view(truth, j, 0)), bits(want))
+        if cfg.get("ct_style", 0) != 3:   # V63's row split is its one-device projector
+            np.testing.assert_array_equal(bits(want), bits(one.forward_view(truth, j, 0)))
