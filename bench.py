@@ -796,6 +796,21 @@ def run_tbct(args):
     torch.cuda.synchronize()
     refbp_ms = e0.elapsed_time(e1) / args.steps
     refbp.close()
+    # the program's default build (Number_of_Devices 4, T42/main_recon.cu:17): its
+    # slab SART and row-split objective projector, bit-exact with it
+    dflt = gpu_b200.Solver(geom, gpu_b200.F32, beta=TBCT_BETA, lambda_tv=0.0, fgp_iters=0, fista=True,
+                           objective=True, use_graph=True, sart_flags=gpu_b200.SART_REFERENCE_BP)
+    dflt.set_slabs(4)
+    dflt.set_sinogram(runs["f32"]["sino"])
+    dflt.set_volume(None)
+    dflt.iterate(1)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    dflt.iterate(2)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dflt_ms = e0.elapsed_time(e1) / 2
+    dflt.close()
 
     # per-kernel times of the SART projectors (32 views spread over the scan)
     kern = {}
@@ -836,6 +851,11 @@ def run_tbct(args):
         "reference_bp_f32": {"iter_per_s": 1000.0 / refbp_ms, "ms_per_step": refbp_ms,
                              "note": "CTR_SART_REFERENCE_BP: the tetrahedron-beam program's backprojection "
                                      "arithmetic, SART pass bit-exact with it"},
+        "reference_default_build_f32": {"iter_per_s": 1000.0 / dflt_ms, "ms_per_step": dflt_ms,
+                                        "note": "the program's default Number_of_Devices=4 build's SART + FISTA "
+                                                "loop with its objective, bit-exact with it, on one B200 "
+                                                "(ctr_solver_set_slabs(4), CTR_SART_REFERENCE_BP, FP32); 2 timed "
+                                                "iterations after 1"},
         "objective_last": {m: runs[m]["objective_last"] for m in runs},
         "e2e": {"value": 1000.0 / e2e_ms, "unit": "iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": "k_sart_walk, tetrahedron beam (SART update, f16 volume, tiled)",
