@@ -26,7 +26,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SCAN = dict(nx=512, ny=512, nz=512, vx=0.5, nu=1024, nv=768, du=0.4, dso=1000.0, dod=-500.0, n_views=1024)
-BETA, LAMBDA_TV, FGP_ITERS = 0.8, 2e-4, 20
+# The SART relaxation of the FISTA loop is the reference's own step,
+# step_size = 2/Lip_con with Lip_con = 32 (V63/main_recon.cu:58,161).  (A
+# relaxation of 0.8, right for plain SART, makes FISTA over SART diverge after
+# a few iterations at these sizes.)
+BETA, LAMBDA_TV, FGP_ITERS = 2.0 / 32.0, 2e-4, 20
 METRIC = "SART-FISTA-TV iter/s & voxel-updates/s, 512^3 x 1024 views, mixed vs FP32, 1 B200"
 
 
@@ -639,7 +643,7 @@ def run_large(args):
 # lambda_TV = 0 (SART + FISTA, no TV prox), the objective every iteration.
 TBCT_SCAN = dict(nx=512, ny=512, nz=512, vx=0.1, nu=1024, nv=16, n_sources=64, du=0.12, dso=200.0, dod=-200.0,
                  n_views=360, us_rate=1.0)
-TBCT_BETA = 2.0 / 32.0
+TBCT_BETA = 2.0 / 32.0   # T42/main_recon.cu's Lip_con = 32, as the cone-beam loop's
 
 
 def tbct_geometry(seed):
