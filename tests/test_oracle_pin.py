@@ -29,12 +29,20 @@ def load(name):
     return dict(np.load(os.path.join(HERE, "golden", f"{name}.npz")))
 
 
+# FGP and the norms are the cone-beam program's (the tetrahedron-beam program
+# shares them); FDK exists for the cone beam (CT_style 0) only.
+FGP_CASES = sorted(n for n in CASES if CASES[n].get("ct_style", 0) != 3)
+FDK_CASES = sorted(n for n in CASES if not CASES[n].get("ct_style", 0))
+
+
+def _case(name, oracle_built):
+    cfg = CASES[name]
+    return name, cfg, oracle_built.Oracle(og_desc_xyz(cfg)), load(name)
+
+
 @pytest.fixture(params=sorted(CASES))
 def case(request, oracle_built):
-    name = request.param
-    cfg = CASES[name]
-    o = oracle_built.Oracle(og_desc_xyz(cfg))
-    return name, cfg, o, load(name)
+    return _case(request.param, oracle_built)
 
 
 def test_forward_bit_exact(case):
@@ -60,19 +68,17 @@ def test_sart_pass_bit_exact(case):
     np.testing.assert_array_equal(bits(out), bits(g["sart"]))
 
 
-def test_fgp_and_norms_bit_exact(case):
-    _, cfg, o, g = case
-    if cfg.get("ct_style", 0) == 3:
-        pytest.skip("the tetrahedron-beam program shares the cone-beam program's FGP")
+@pytest.mark.parametrize("name", FGP_CASES)
+def test_fgp_and_norms_bit_exact(name, oracle_built):
+    _, cfg, o, g = _case(name, oracle_built)
     np.testing.assert_array_equal(bits(o.fgp(g["vol"], float(g["fgp_lambda"]), int(g["fgp_iters"]))), bits(g["fgp"]))
     assert o.tv_norm(g["vol"]) == float(g["tv"])
     assert o.l2_norm(g["fp0"], g["b"]) == float(g["l2"])
 
 
-def test_fdk_stages(case):
-    _, cfg, o, g = case
-    if cfg.get("ct_style", 0):
-        pytest.skip("FDK is the cone beam's only")
+@pytest.mark.parametrize("name", FDK_CASES)
+def test_fdk_stages(name, oracle_built):
+    _, cfg, o, g = _case(name, oracle_built)
     np.testing.assert_array_equal(bits(o.fdk_weight(g["b"])), bits(g["fdkw"]))
     ramp = o.ramp_filter(g["fdkw"][:2])
     # the reference filters with a double-precision FFT; the restatement convolves
