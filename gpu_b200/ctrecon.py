@@ -439,7 +439,13 @@ def convert(src, dst, stream=None):
 
 
 class Solver:
-    """SART + FISTA + FGP-TV outer loop on device buffers (``ctr_solver``)."""
+    """SART + FISTA + FGP-TV outer loop on device buffers (``ctr_solver``).
+
+    ``beta`` is the SART relaxation.  The reference's FISTA loop uses its step
+    2/Lip_con = 2/32 = 0.0625 (V63/main_recon.cu:58,161), and its FGP lambda is
+    beta * lambda_tv.  The default 0.8 suits plain SART (``fista=False``); under
+    FISTA it makes the iteration diverge after a few passes on a 256^3 /
+    360-view scan, so pass the reference's step there."""
 
     def __init__(self, geom: Geometry, vol_dtype=F32, beta=0.8, lambda_tv=0.0, fgp_iters=20, fista=True,
                  objective=True, use_graph=True, sart_flags=0):
