@@ -126,3 +126,8 @@ CONFIG2 = dict(nx=256, ny=256, nz=256, nu=384, nv=384, nviews=360, vx=0.5, du=20
 # offset keeps views off the exact axes.
 MIXED = dict(nx=64, ny=64, nz=64, nu=96, nv=96, nviews=90, vx=2.0, du=3.2, dso=1000.0, dod=-500.0,
              initial_angle=1.0)
+
+# The same field of view at half the sampling, for the FP64 oracle's
+# FISTA-step test on the CPU.
+FISTA32 = dict(nx=32, ny=32, nz=32, nu=48, nv=48, nviews=90, vx=4.0, du=6.4, dso=1000.0, dod=-500.0,
+               initial_angle=1.0)

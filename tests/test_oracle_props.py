@@ -1,12 +1,12 @@
 """Properties of the CPU oracle itself (no GPU): the FP64 twin agrees with the
 FP32 restatement, the scatter adjoint is the projector's transpose, analytic
 line integrals agree with the Siddon projection of the voxelised phantom, the
-spatial ramp kernel equals the padded-DFT filter, and FGP decreases its
-objective."""
+spatial ramp kernel equals the padded-DFT filter, FGP decreases its
+objective, and the reference's FISTA loop is stable at its own step."""
 import numpy as np
 import pytest
 
-from scan_configs import MIXED, SMALL, og_desc_xyz
+from scan_configs import FISTA32, MIXED, SMALL, og_desc_xyz
 
 
 @pytest.fixture(scope="module")
@@ -69,3 +69,38 @@ def test_fgp_decreases_its_objective(oracle_built):
     assert obj(x) < obj(f)
     x2 = o.fgp(f, lam, 40)
     assert obj(x2) <= obj(x) * (1 + 1e-4)
+
+
+def test_fista_step_of_the_reference_is_stable(oracle_built):
+    """The reference's loop (V63/main_recon.cu:344-386) in FP64: SART from y,
+    FGP-TV with lambda = beta * lambda_TV, FISTA momentum.  At its own step
+    beta = 2/Lip_con = 2/32 (:58,161) the error against the phantom stays
+    bounded for 30 iterations; at beta = 0.8, the plain-SART relaxation, the
+    momentum amplifies it geometrically (RMSE ~300x the phantom's maximum by
+    iteration 30 on this scan)."""
+    o = oracle_built.Oracle(og_desc_xyz(FISTA32))
+    rng = np.random.default_rng(100)
+    params = oracle_built.random_ellipsoids(rng, 10, 40.0, (5.0, 40.0), (0.01, 0.03))
+    truth = o.phantom(params)
+    b = o.phantom_sinogram(params)
+    b = (b + 0.005 * b.max() * rng.standard_normal(b.shape)).astype(np.float64)
+    mu = float(truth.max())
+
+    def rmse_history(beta, iters=30):
+        y = np.zeros(o.vol_shape)
+        xprev = np.zeros_like(y)
+        t = 1.0
+        out = []
+        for _ in range(iters):
+            x = o.fgp_f64(o.sart_pass_f64(y, b, beta), beta * 2e-4, 20)
+            tk = (1.0 + np.sqrt(1.0 + 4.0 * t * t)) / 2.0
+            y = x + (t - 1.0) / tk * (x - xprev)
+            xprev = x
+            t = tk
+            out.append(float(np.sqrt(np.mean((x - truth) ** 2))) / mu)
+        return out
+
+    small = rmse_history(2.0 / 32.0)
+    assert max(small) < 0.1 and small[-1] < 0.06
+    large = rmse_history(0.8)
+    assert large[-1] > 10.0 and large[-1] > 4.0 * large[-5]
