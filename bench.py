@@ -961,6 +961,20 @@ def main():
         runs[mode]["solver"] = solver
         runs[mode]["sino"] = sino
 
+    # accuracy of the mixed-precision run against the FP32 run after the same
+    # iterations on the same scan (outside the timed regions)
+    try:
+        v32 = runs["f32"]["solver"].get_volume(torch.empty(vshape, device=dev, dtype=torch.float32))
+        vmx = runs["mixed"]["solver"].get_volume(torch.empty(vshape, device=dev, dtype=mixed_dt)).float()
+        scale = float(v32.abs().max())
+        diff = vmx - v32
+        mixed_acc = {"rmse": float(torch.sqrt(torch.mean(diff * diff))) / scale,
+                     "max_abs": float(diff.abs().max()) / scale,
+                     "relative_to": "the FP32 reconstruction's maximum", "iterations": args.warmup + args.steps}
+        del v32, vmx, diff
+    except Exception as e:  # an accuracy side figure must not hide the timing
+        mixed_acc = {"error": str(e)[:200]}
+
     # end to end through the public API with host buffers: every step copies the
     # measured sinogram in from pinned host memory, runs one iteration and reads
     # the reconstructed volume back; the steps' objectives are read at the end
@@ -1147,6 +1161,7 @@ def main():
             "f32": {"iter_per_s": job_rate(ms_f32, world), "ms_per_step": ms_f32,
                     "voxel_updates_per_s": job_rate(ms_f32, world) * V * SCAN["n_views"]},
             "mixed_over_f32": ms_f32 / ms_mixed,
+            "mixed_vs_f32_accuracy": mixed_acc,
             "objective_last": {"f32": runs["f32"]["objective_last"], "mixed": runs["mixed"]["objective_last"]},
             "e2e": {"value": job_rate(e2e_ms, world), "unit": "iter/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
