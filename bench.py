@@ -1138,7 +1138,8 @@ def main():
             "config": {"workload": "SART+FISTA+FGP-TV (20 inner) iteration with objective, 512^3 x 0.5 mm, "
                                    "1024 views, 1024x768 detector x 0.4 mm, DSO 1000 mm, DOD -500 mm",
                        "phantom": "40 ellipsoids + 200 spheres (seeded), Siddon projections + 0.5% noise",
-                       "parallelism": f"replicas x{world}", "l2": "inputs > L2 (512 MB+ volume)"},
+                       "parallelism": f"replicas x{world}", "l2": "inputs > L2 (512 MB+ volume)",
+                       "relaxation": BETA, "lambda_tv": LAMBDA_TV, "fgp_iters": FGP_ITERS},
             "voxel_updates_per_s": value * V * SCAN["n_views"],
             "ray_voxel_intersections_per_s": value * 3 * segs_per_pass,
             "ray_voxel_intersections_per_pass": segs_per_pass,
