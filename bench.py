@@ -32,6 +32,30 @@ SCAN = dict(nx=512, ny=512, nz=512, vx=0.5, nu=1024, nv=768, du=0.4, dso=1000.0,
 # a few iterations at these sizes.)
 BETA, LAMBDA_TV, FGP_ITERS = 2.0 / 32.0, 2e-4, 20
 METRIC = "SART-FISTA-TV iter/s & voxel-updates/s, 512^3 x 1024 views, mixed vs FP32, 1 B200"
+# 16 views spread evenly over the scan, off the axis-aligned angles (views
+# 0, 256, 512, 768 at 1024 views): the CPU arms time their SART and
+# objective projections on these, and the measurement noise is scaled to
+# their largest ray sum
+SAMPLE_VIEWS = [17 + 64 * k for k in range(16)]
+NOISE = 0.005          # Gaussian noise sigma, relative to the largest ray sum of the sample views
+SCAN_SEED = 2024
+
+
+def scan_config(world):
+    """The workload's description, shared by both arms of the benchmark."""
+    return {"workload": "SART+FISTA+FGP-TV (20 inner) iteration with objective, 512^3 x 0.5 mm, "
+                        "1024 views, 1024x768 detector x 0.4 mm, DSO 1000 mm, DOD -500 mm",
+            "phantom": "40 ellipsoids + 200 spheres (seeded), Siddon projections + 0.5% noise",
+            "parallelism": f"replicas x{world}", "l2": "inputs > L2 (512 MB+ volume)",
+            "relaxation": BETA, "lambda_tv": LAMBDA_TV, "fgp_iters": FGP_ITERS}
+
+
+def view_noise(view, n, seed):
+    """Unit Gaussian noise of one view (CPU generator seeded per view, so the
+    CPU arm can draw its sample views' noise without the others)."""
+    import torch
+    gen = torch.Generator().manual_seed(seed * 1000003 + view)
+    return torch.randn(n, generator=gen, dtype=torch.float32)
 
 
 def parse():
@@ -209,90 +233,132 @@ def issue_roofline(traffic, launch_ms, sm_mhz, dev):
             "instructions_per_launch": traffic["warp_instructions_per_launch"], "sms": sms, "sm_mhz": sm_mhz}
 
 
-def cpu_baseline(steps_hint=1, budget_s=12.0):
-    """The reference's own kernels compiled for the CPU (oracle/_ref), timed on
-    this host's cores on a bounded sample of one iteration, scaled to a full
-    iteration: S views of the SART pass and of the objective forward
-    projection (x 1024/S), 2 of the 20 FGP inner iterations (x 10), TV norm."""
-    import numpy as np
+class CpuScan:
+    """The reference's own kernels compiled for the CPU (oracle/_ref) on the
+    benchmark's scan: the same seeded phantom (the oracle's voxelizer, whose
+    sums are the device voxelizer's), and the measured views of SAMPLE_VIEWS
+    made as the GPU arm makes them (the projector's ray sums plus the seeded
+    noise of each view).  The estimate starts at zero, as the solver's."""
 
-    from oracle import ctoracle
-    d = ctoracle.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["nu"], SCAN["nv"], SCAN["n_views"], SCAN["vx"],
-                           SCAN["du"], SCAN["dso"], SCAN["dod"])
-    ref = ctoracle.RefOracle(d)
-    rng = np.random.default_rng(0)
-    vol = rng.uniform(0.0, 0.02, ref.vol_shape).astype(np.float32)
-    nviews = SCAN["n_views"]
-    b_view = rng.uniform(0.0, 5.0, (1,) + ref.view_shape).astype(np.float32)
-    # calibrate on one SART view, then size the sample to the budget
-    ref._set()
-    out = vol.copy()
-    t0 = time.perf_counter()
-    s, c = ref.trig(0)
-    corr = np.zeros(ref.view_shape, np.float32)
-    ref.lib.ref_forward_view(out, corr, b_view[0].ctypes.data, s, c, 1)
-    ref.lib.ref_backproject_view(out, corr, BETA, s, c, 1)
-    t_one = time.perf_counter() - t0
-    s_views = max(1, min(64, int(0.4 * budget_s / max(t_one, 1e-3))))
-    stride = max(1, nviews // s_views)
-    views = list(range(0, nviews, stride))[:s_views]
-    t0 = time.perf_counter()
-    for j in views:
-        s, c = ref.trig(j)
-        corr = np.zeros(ref.view_shape, np.float32)
-        ref.lib.ref_forward_view(out, corr, b_view[0].ctypes.data, s, c, 1)
-        ref.lib.ref_backproject_view(out, corr, BETA, s, c, 1)
-    t_sart = (time.perf_counter() - t0) / len(views) * nviews
-    t0 = time.perf_counter()
-    for j in views:
-        s, c = ref.trig(j)
-        fp = np.zeros(ref.view_shape, np.float32)
-        ref.lib.ref_forward_view(out, fp, None, s, c, 0)
-    t_obj = (time.perf_counter() - t0) / len(views) * nviews
-    t0 = time.perf_counter()
-    ref.fgp(out, BETA * LAMBDA_TV, 2)
-    t_fgp = (time.perf_counter() - t0) * FGP_ITERS / 2.0
-    t0 = time.perf_counter()
-    ref.tv_norm(out)
-    t_tv = time.perf_counter() - t0
-    t_iter = t_sart + t_obj + t_fgp + t_tv
-    cores = os.cpu_count()
+    def __init__(self, seed=SCAN_SEED):
+        import numpy as np
+
+        from oracle import ctoracle
+        d = ctoracle.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["nu"], SCAN["nv"], SCAN["n_views"],
+                               SCAN["vx"], SCAN["du"], SCAN["dso"], SCAN["dod"])
+        self.ref = ctoracle.RefOracle(d)
+        truth = ctoracle.Oracle(d).phantom(phantom_params(seed))
+        self.ref._set()
+        clean = {}
+        for j in SAMPLE_VIEWS:
+            s, c = self.ref.trig(j)
+            out = np.zeros(self.ref.view_shape, np.float32)
+            self.ref.lib.ref_forward_view(truth, out, None, s, c, 0)
+            clean[j] = out
+        sigma = NOISE * max(float(v.max()) for v in clean.values())
+        P = SCAN["nu"] * SCAN["nv"]
+        self.b = {j: (clean[j] + sigma * view_noise(j, P, seed).numpy().reshape(self.ref.view_shape)).astype(np.float32)
+                  for j in SAMPLE_VIEWS}
+        self.vol = np.zeros(self.ref.vol_shape, np.float32)
+        del truth
+
+    def sart_view(self, j):
+        """Seconds of one SART view: the projection with correction, then the update."""
+        import numpy as np
+        self.ref._set()
+        s, c = self.ref.trig(j)
+        corr = np.zeros(self.ref.view_shape, np.float32)
+        t0 = time.perf_counter()
+        self.ref.lib.ref_forward_view(self.vol, corr, self.b[j].ctypes.data, s, c, 1)
+        self.ref.lib.ref_backproject_view(self.vol, corr, BETA, s, c, 1)
+        return time.perf_counter() - t0
+
+    def objective_view(self, j):
+        """Seconds of the objective's forward projection of one view."""
+        import numpy as np
+        self.ref._set()
+        s, c = self.ref.trig(j)
+        fp = np.zeros(self.ref.view_shape, np.float32)
+        t0 = time.perf_counter()
+        self.ref.lib.ref_forward_view(self.vol, fp, None, s, c, 0)
+        return time.perf_counter() - t0
+
+    def iteration(self, views):
+        """One iteration's time estimated from a sample: the SART pass and the
+        objective's projection from `views` (x n_views/len(views)), FGP from 2
+        of its 20 inner iterations (x 10), the TV norm."""
+        sart = [self.sart_view(j) for j in views]
+        obj = [self.objective_view(j) for j in views]
+        t0 = time.perf_counter()
+        self.ref.fgp(self.vol, BETA * LAMBDA_TV, 2)
+        t_fgp = (time.perf_counter() - t0) * FGP_ITERS / 2.0
+        t0 = time.perf_counter()
+        self.ref.tv_norm(self.vol)
+        t_tv = time.perf_counter() - t0
+        n = SCAN["n_views"]
+        t_sart, t_obj = sum(sart) / len(views) * n, sum(obj) / len(views) * n
+        return {"seconds_per_iter": t_sart + t_obj + t_fgp + t_tv,
+                "parts_s": {"sart": t_sart, "objective_fp": t_obj, "fgp": t_fgp, "tv": t_tv},
+                "per_view_s": {"views": list(views), "sart": sart, "objective_fp": obj}}
+
+
+def host_cores():
     try:
-        cores = len(os.sched_getaffinity(0))
+        return len(os.sched_getaffinity(0))
     except AttributeError:
-        pass
-    return {
-        "value": 1.0 / t_iter, "unit": "iter/s", "cores": cores, "kind": "reference",
-        "sample": (f"reference kernels compiled for the CPU (OpenMP, {cores} threads): SART on {len(views)} of "
-                   f"{nviews} views and the objective forward projection on the same views (scaled x{nviews}/"
-                   f"{len(views)}), 2 of {FGP_ITERS} FGP inner iterations (x{FGP_ITERS // 2}), TV norm; "
-                   f"512^3 volume, 1024x768 detector"),
-        "seconds_per_iter": t_iter,
-        "parts_s": {"sart": t_sart, "objective_fp": t_obj, "fgp": t_fgp, "tv": t_tv},
-    }
+        return os.cpu_count()
+
+
+def cpu_sample_text(cores, per_step):
+    n = SCAN["n_views"]
+    return (f"reference kernels compiled for the CPU (OpenMP, {cores} threads) on the benchmark scan (same seeded "
+            f"phantom and noise): SART and the objective forward projection timed on views 17+64k, k=0..15 "
+            f"(16 of {n}, evenly spaced, off the axis angles; {per_step} per step), scaled x{n}/{per_step}; "
+            f"2 of {FGP_ITERS} FGP inner iterations (x{FGP_ITERS // 2}); TV norm; 512^3 volume, 1024x768 detector")
+
+
+def cpu_baseline():
+    """The CPU reference timed once on all 16 sample views."""
+    scan = CpuScan()
+    r = scan.iteration(SAMPLE_VIEWS)
+    cores = host_cores()
+    sv = r["per_view_s"]["sart"]
+    return {"value": 1.0 / r["seconds_per_iter"], "unit": "iter/s", "cores": cores, "kind": "reference",
+            "sample": cpu_sample_text(cores, len(SAMPLE_VIEWS)), "seconds_per_iter": r["seconds_per_iter"],
+            "parts_s": r["parts_s"], "sart_view_s": {"min": min(sv), "max": max(sv), "mean": sum(sv) / len(sv)}}
 
 
 def run_reference(args):
+    """The reference's CPU implementation on the same scan: each step times 2
+    of the 16 sample views in turn (the steps' samples cycle through all 16),
+    so that the run stays within a few minutes."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    times = []
-    info = None
+    scan = CpuScan()
+    per_step = 2
+    times, sart_view = [], {}
     for it in range(args.warmup + args.steps):
-        info = cpu_baseline()
+        views = [SAMPLE_VIEWS[(per_step * it + i) % len(SAMPLE_VIEWS)] for i in range(per_step)]
+        r = scan.iteration(views)
         if it >= args.warmup:
-            times.append(info["seconds_per_iter"])
+            times.append(r["seconds_per_iter"])
+            for j, t in zip(views, r["per_view_s"]["sart"]):
+                sart_view.setdefault(j, []).append(t)
     ms = 1000.0 * sum(times) / len(times)
     value = 1000.0 / ms
+    cores = host_cores()
+    per_view = {j: sum(t) / len(t) for j, t in sorted(sart_view.items())}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "SART+FISTA+FGP-TV (20 inner) iteration, 512^3 x 0.5 mm, 1024 views, "
-                               "1024x768 detector x 0.4 mm, DSO 1000 mm, DOD -500 mm", "l2": "inputs > L2"},
-        "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")} | {"value": value},
+        "config": scan_config(world),
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": cores, "kind": "reference",
+                         "sample": cpu_sample_text(cores, per_step)},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "voxel_updates_per_s": value * SCAN["nx"] * SCAN["ny"] * SCAN["nz"] * SCAN["n_views"],
+        "sart_view_s": {"per_view": per_view, "min": min(per_view.values()), "max": max(per_view.values())},
     }
     print(json.dumps(line), flush=True)
 
@@ -472,10 +538,13 @@ def batched_scans(n, seed=4):
 
 
 def run_batched(args):
-    """Aggregate voxel-updates/s of a batch of uneven scans stored in BF16,
-    every iteration of every scan one CUDA graph launch; per-scan relative
-    RMSE of the BF16 batch against the FP32 single-scan solver on the same
-    sinogram after the timed iterations."""
+    """Aggregate voxel-updates/s of a batch of uneven scans with BF16 volumes
+    (the refinement solver: BF16 copies for the projectors and a BF16
+    correction per pass with stochastic rounding, FP32 FISTA state; FP16
+    measured data), every iteration of every scan one CUDA graph launch;
+    per-scan RMSE and maximum error against the FP64 reference solver on the
+    same data after the same iterations, relative to the scan's phantom
+    maximum."""
     import torch
 
     import gpu_b200
@@ -483,22 +552,23 @@ def run_batched(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     specs = batched_scans(args.scans, seed=4 + rank)
-    geoms, sinos = [], []
+    geoms, sinos, mus = [], [], []
     for sp in specs:
         g = gpu_b200.Geometry(gpu_b200.make_desc(sp["nx"], sp["ny"], sp["nz"], sp["vx"], sp["nu"], sp["nv"],
                                                  sp["du"], sp["dso"], sp["dod"], sp["n_views"]))
         truth = torch.zeros(g.vol_shape, device=dev)
         g.phantom_voxelize(sp["phantom"], truth)
+        mus.append(float(truth.max()))
         sino = torch.zeros((sp["n_views"],) + g.view_shape, device=dev)
         g.forward(truth, sino)
         geoms.append(g)
-        sinos.append(sino.to(torch.bfloat16))
+        sinos.append(sino.to(torch.float16))
         del truth, sino
         if not args.no_tune:
             g.autotune(gpu_b200.BF16, n_views=2)
     flags = 0 if args.no_sr else gpu_b200.SART_STOCHASTIC_ROUND
     batch = gpu_b200.Batch(geoms, gpu_b200.BF16, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS,
-                           sart_flags=flags)
+                           sart_flags=flags, refine=True)
     for i, s in enumerate(sinos):
         batch.set_sinogram(i, s)
     batch.reset()
@@ -517,36 +587,44 @@ def run_batched(args):
     ms = e0.elapsed_time(e1) / iters
     clk = clocks.stop()
     updates = sum(sp["nx"] * sp["ny"] * sp["nz"] * sp["n_views"] for sp in specs)
-    # accuracy: the same iterations in FP32 through the single-scan solver
-    errs = []
+    # accuracy: the same iterations through the FP64 reference solver on the
+    # same (FP16-stored) data, per scan, relative to the scan's phantom maximum
+    errs, maxs = [], []
     for i, (sp, g) in enumerate(zip(specs, geoms)):
-        got = torch.zeros(g.vol_shape, device=dev, dtype=torch.bfloat16)
-        batch.get_volume(i, got)
-        s32 = gpu_b200.Solver(g, gpu_b200.F32, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS)
-        s32.set_sinogram(sinos[i].float().contiguous())
-        s32.set_volume(None)
-        s32.iterate(iters)
-        want = torch.zeros(g.vol_shape, device=dev)
-        s32.get_volume(want)
-        s32.close()
-        errs.append(float(torch.sqrt(torch.mean((got.float() - want) ** 2)) / want.abs().max().clamp_min(1e-30)))
-    # per scan and step: tile, FP + BP per view, untile, FGP (2 per inner step
-    # + final); from the second step the previous objective fused (tile, TV +
-    # reduce, 2-level reduce); after the last step the objective (tile, FP,
-    # 2 reduce, TV, reduce)
-    launches = sum((2 + 2 * sp["n_views"] + 2 * FGP_ITERS + 1) * iters + 5 * (iters - 1) + 6 for sp in specs)
+        got = torch.zeros(g.vol_shape, device=dev)
+        batch.get_volume_f32(i, got)
+        s64 = gpu_b200.Solver(g, gpu_b200.F64, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, objective=False)
+        s64.set_sinogram(sinos[i])
+        s64.set_volume(None)
+        s64.iterate(iters, objectives=False)
+        want = torch.zeros(g.vol_shape, device=dev, dtype=torch.float64)
+        s64.get_volume(want)
+        s64.close()
+        dlt = got.double() - want
+        errs.append(float(torch.sqrt(torch.mean(dlt * dlt))) / mus[i])
+        maxs.append(float(dlt.abs().max()) / mus[i])
+        del got, want, dlt
+    # per scan and step: the pass's FISTA factor, FP + BP per view, the sum
+    # y_k + d, FGP (2 per inner step), the final prox with the rotation; from
+    # the second step the previous objective fused (TV + reduce, 2-level
+    # reduce); after the last step the objective (FP, 2 reduce, TV, reduce)
+    launches = sum((3 + 2 * sp["n_views"] + 2 * FGP_ITERS) * iters + 4 * (iters - 1) + 5 for sp in specs)
     line = {
         "metric": "batched SART-FISTA-TV voxel-updates/s", "value": updates * 1000.0 / ms,
         "unit": "voxel-updates/s", "n_gpus": 1, "steps": iters, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16 storage, f32 arithmetic" + ("" if args.no_sr else ", stochastic rounding of the SART update"),
+        "dtype": "bf16 storage for the projectors (refinement: FP32 FISTA state, FP16 sinogram), f32 arithmetic"
+                 + ("" if args.no_sr else ", stochastic rounding of the correction's updates"),
         "data": "synthetic",
         "config": {"workload": f"{len(specs)} uneven scans (volumes 64-256^3, 90-720 views, 96^2-384^2 detectors, "
                                f"DSO 600-1200 mm), one CUDA graph launch per iteration of all scans",
                    "scans": [{k: sp[k] for k in ("nx", "n_views", "nu", "dso")} for sp in specs],
                    "l2": "inputs > L2 (sum of the scans' volumes and sinograms)"},
         "iter_per_s": 1000.0 / ms,
-        "rel_rmse_vs_f32": {"max": max(errs), "median": sorted(errs)[len(errs) // 2]},
+        "error_vs_fp64": {"rmse": {"max": max(errs), "median": sorted(errs)[len(errs) // 2]},
+                          "max_abs": {"max": max(maxs), "median": sorted(maxs)[len(maxs) // 2]},
+                          "per_scan_rmse": errs, "iterations": iters,
+                          "relative_to": "each scan's phantom maximum, against the FP64 reference solver"},
         "clocks": clk, "gpu_launches": launches,
         "launch_shapes": [g.shapes() for g in geoms],
     }
@@ -590,12 +668,16 @@ def run_large(args):
     stream = torch.cuda.current_stream()
     out = {}
     vols = {}
+    sino16 = sino32.to(torch.float16)
+    # BF16 and FP16: the refinement solver (16-bit copies and correction,
+    # FP32 FISTA state, FP16 measured data); BF16 with stochastic rounding
     for mode, vdt, tdt in (("f32", gpu_b200.F32, torch.float32), ("bf16", gpu_b200.BF16, torch.bfloat16),
                            ("f16", gpu_b200.F16, torch.float16)):
-        sino = sino32 if tdt == torch.float32 else sino32.to(tdt)
+        sino = sino32 if tdt == torch.float32 else sino16
         tuned = geom.autotune(vdt, n_views=2)
         flags = gpu_b200.SART_STOCHASTIC_ROUND if mode == "bf16" else 0
-        solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, sart_flags=flags)
+        solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, sart_flags=flags,
+                                 refine=(mode != "f32"))
         solver.set_sinogram(sino)
         solver.set_volume(None)
         for _ in range(args.warmup):
@@ -610,29 +692,44 @@ def run_large(args):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
-        vol = torch.zeros(geom.vol_shape, device=dev, dtype=tdt)
-        solver.get_volume(vol)
+        vol = torch.zeros(geom.vol_shape, device=dev)
+        solver.get_volume_f32(vol)
         solver.close()
         vols[mode] = vol
         out[mode] = {"ms_per_step": ms, "iter_per_s": 1000.0 / ms, "clocks": clocks.stop(),
                      "launch_shapes": [tuned["fp_shape"], tuned["bp_shape"]],
                      "voxel_updates_per_s": 1000.0 / ms * L["nx"] * L["ny"] * L["nz"] * L["n_views"]}
-        if sino is not sino32:
-            del sino
-    ref = vols["f32"]
-    for mode in ("bf16", "f16"):
-        dlt = vols[mode].float() - ref
-        out[mode]["rmse_vs_f32"] = float(torch.sqrt(torch.mean(dlt * dlt))) / mu_max
-        out[mode]["max_err_vs_f32"] = float(dlt.abs().max()) / mu_max
+    del sino16
+    # the FP64 reference solver on the same (FP32) data for the same iterations
+    f64 = gpu_b200.Solver(geom, gpu_b200.F64, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, objective=False)
+    f64.set_sinogram(sino32)
+    f64.set_volume(None)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    f64.iterate(args.steps, objectives=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ref = f64.get_volume(torch.zeros(geom.vol_shape, device=dev, dtype=torch.float64))
+    f64.close()
+    for mode in ("f32", "bf16", "f16"):
+        dlt = vols[mode].double() - ref
+        out[mode]["rmse_vs_fp64"] = float(torch.sqrt(torch.mean(dlt * dlt))) / mu_max
+        out[mode]["max_err_vs_fp64"] = float(dlt.abs().max()) / mu_max
         out[mode]["speedup_vs_f32"] = out["f32"]["ms_per_step"] / out[mode]["ms_per_step"]
+        del dlt
     line = {"metric": "SART-FISTA-TV iter/s, 1024^3 x 1024 views, BF16/FP16 vs FP32", "value": out["bf16"]["iter_per_s"],
             "unit": "iter/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": out["bf16"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "bf16 storage (stochastic rounding), f32 arithmetic", "data": "synthetic",
+            "vs_baseline": None,
+            "dtype": "bf16 storage for the projectors (refinement: FP32 FISTA state, FP16 sinogram, stochastic "
+                     "rounding), f32 arithmetic",
+            "data": "synthetic",
             "config": {"workload": "1024^3 x 0.25 mm, 1024 views, 1024x1024 detector x 0.3 mm, DSO 1000 mm, "
                                    "DOD -500 mm, 100 seeded ellipsoids, noiseless Siddon sinogram",
                        "l2": "inputs > L2"},
-            "modes": out, "phantom_max": mu_max}
+            "modes": out, "phantom_max": mu_max, "fp64_ms_per_iteration": e0.elapsed_time(e1) / args.steps,
+            "errors_relative_to": "the phantom's maximum attenuation, against the FP64 reference solver after the "
+                                  "same iterations"}
     print(json.dumps(line), flush=True)
 
 
@@ -916,16 +1013,24 @@ def main():
     V = SCAN["nx"] * SCAN["ny"] * SCAN["nz"]
     P = SCAN["nu"] * SCAN["nv"]
 
-    # synthetic scan: seeded phantom, its Siddon projections + 0.5% Gaussian noise
+    # synthetic scan: seeded phantom, its Siddon projections + Gaussian noise of
+    # 0.5% of the largest ray sum of the sample views, drawn per view from a
+    # seeded CPU generator (the CPU arm draws the same noise for its views)
+    seed = SCAN_SEED + rank
     truth = torch.zeros(vshape, device=dev)
-    geom.phantom_voxelize(phantom_params(2024 + rank), truth)
+    geom.phantom_voxelize(phantom_params(seed), truth)
+    truth_max = float(truth.max())
     sino32 = torch.zeros(sshape, device=dev)
     geom.forward(truth, sino32)
-    gen = torch.Generator(device=dev).manual_seed(77 + rank)
-    sino32 += 0.005 * sino32.max() * torch.randn(sshape, device=dev, generator=gen)
+    sigma = NOISE * float(sino32[SAMPLE_VIEWS].max())
+    for j in range(SCAN["n_views"]):
+        sino32[j] += sigma * view_noise(j, P, seed).to(dev).view(sshape[1:])
     del truth
     mixed_dt = torch.float16 if args.mixed == "f16" else torch.bfloat16
     mixed_code = gpu_b200.F16 if args.mixed == "f16" else gpu_b200.BF16
+    # the measured data are stored in FP16 for either 16-bit volume type (BF16's
+    # 8-bit mantissa would change the data by itself)
+    sino16 = sino32.to(torch.float16)
 
     def barrier():
         torch.cuda.synchronize()
@@ -938,11 +1043,14 @@ def main():
     runs = {}
     stream = torch.cuda.current_stream()
     tuned = {}
-    for mode, vdt, sdt in (("f32", gpu_b200.F32, torch.float32), ("mixed", mixed_code, mixed_dt)):
+    # mixed precision: the refinement solver (FP32 FISTA state, 16-bit copies
+    # for the projectors, each pass accumulated into a 16-bit correction
+    # against the FP32 residual), the form that meets the accuracy bar
+    for mode, vdt, sino in (("f32", gpu_b200.F32, sino32), ("mixed", mixed_code, sino16)):
         tuned[mode] = geom.autotune(vdt, n_views=4)      # launch shapes; results do not depend on them
-        sino = sino32 if sdt == torch.float32 else sino32.to(sdt)
         solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
-                                 objective=True, use_graph=True)
+                                 objective=True, use_graph=True, refine=(mode == "mixed"),
+                                 sart_flags=gpu_b200.SART_STOCHASTIC_ROUND if vdt == gpu_b200.BF16 else 0)
         solver.set_sinogram(sino)
         solver.set_volume(None)
         solver.iterate(args.warmup)
@@ -961,19 +1069,71 @@ def main():
         runs[mode]["solver"] = solver
         runs[mode]["sino"] = sino
 
-    # accuracy of the mixed-precision run against the FP32 run after the same
-    # iterations on the same scan (outside the timed regions)
+    # accuracy (outside the timed regions): the FP64 reference solver on the
+    # same scan (FP32 measured data) for the same number of iterations; the
+    # errors of the mixed-precision estimate (its FP32 x_k) and of the FP32
+    # run, relative to the phantom's maximum attenuation.  The FP64 run's
+    # state after 5 iterations also scores the FP64 ray-box entry variant.
+    n_acc = args.warmup + args.steps
+    n_early = min(5, n_acc)
+    acc, entry64 = {}, {}
     try:
-        v32 = runs["f32"]["solver"].get_volume(torch.empty(vshape, device=dev, dtype=torch.float32))
-        vmx = runs["mixed"]["solver"].get_volume(torch.empty(vshape, device=dev, dtype=mixed_dt)).float()
-        scale = float(v32.abs().max())
-        diff = vmx - v32
-        mixed_acc = {"rmse": float(torch.sqrt(torch.mean(diff * diff))) / scale,
-                     "max_abs": float(diff.abs().max()) / scale,
-                     "relative_to": "the FP32 reconstruction's maximum", "iterations": args.warmup + args.steps}
-        del v32, vmx, diff
+        def err(v, ref):
+            d = v.double() - ref
+            return {"rmse": float(torch.sqrt(torch.mean(d * d))) / truth_max,
+                    "max_abs": float(d.abs().max()) / truth_max}
+
+        f64 = gpu_b200.Solver(geom, gpu_b200.F64, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
+                              objective=False)
+        f64.set_sinogram(sino32)
+        f64.set_volume(None)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f64.iterate(n_early, objectives=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        f64_ms = e0.elapsed_time(e1) / n_early
+        ref_early = f64.get_volume(torch.empty(vshape, device=dev, dtype=torch.float64))
+        if n_acc > n_early:
+            f64.iterate(n_acc - n_early, objectives=False)
+        ref = f64.get_volume(torch.empty(vshape, device=dev, dtype=torch.float64))
+        f64.close()
+        for mode in ("mixed", "f32"):
+            acc[mode] = err(runs[mode]["solver"].get_volume_f32(torch.empty(vshape, device=dev)), ref)
+        mixed_acc = {"rmse": acc["mixed"]["rmse"], "max_abs": acc["mixed"]["max_abs"], "f32": acc["f32"],
+                     "relative_to": "the phantom's maximum attenuation, against the FP64 reference solver",
+                     "iterations": n_acc, "fp64_ms_per_iteration": f64_ms, "bar": 1e-3,
+                     "meets_bar": acc["mixed"]["rmse"] <= 1e-3}
+        del ref
+        # CTR_GEOM_ENTRY_F64: the ray-box entry/exit in FP64 (the traversal in
+        # FP32); kernel times per view and the FP32 solver's error after
+        # n_early iterations, beside the default FP32 entry
+        d64 = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
+                                 SCAN["dso"], SCAN["dod"], SCAN["n_views"], entry64=True)
+        for key, gm in (("entry_f32", geom), ("entry_f64", gpu_b200.Geometry(d64))):
+            gm.set_shapes(tuned["f32"]["fp_shape"], tuned["f32"]["bp_shape"])
+            s = gpu_b200.Solver(gm, gpu_b200.F32, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
+                                objective=False)
+            s.set_sinogram(sino32)
+            s.set_volume(None)
+            s.iterate(n_early, objectives=False)
+            entry64[key] = err(s.get_volume_f32(torch.empty(vshape, device=dev)), ref_early)
+            s.close()
+            vol = torch.zeros(vshape, device=dev)
+            gm.sart_views(vol, sino32, BETA, 0, 4, flags=gpu_b200.SART_TILED)
+            fp_t = bp_t = 0.0
+            for j in range(16):
+                f_ms, b_ms = gm.sart_views(vol, sino32, BETA, (j * 97) % SCAN["n_views"], 1,
+                                           flags=gpu_b200.SART_TILED, timed=True)
+                fp_t += f_ms
+                bp_t += b_ms
+            entry64[key].update({"fp_ms_per_view": fp_t / 16, "bp_ms_per_view": bp_t / 16})
+            del vol
+        entry64["iterations"] = n_early
+        entry64["relative_to"] = "the phantom's maximum attenuation, against the FP64 reference solver"
+        del ref_early
     except Exception as e:  # an accuracy side figure must not hide the timing
-        mixed_acc = {"error": str(e)[:200]}
+        mixed_acc = {"error": str(e)[:300]}
 
     # end to end through the public API with host buffers: every step copies the
     # measured sinogram in from pinned host memory, runs one iteration and reads
@@ -1020,19 +1180,21 @@ def main():
 
     # the iteration without the objective (the reference's loop evaluates it
     # every iteration, so the headline keeps it)
+    # (side figures below: a few timed iterations each)
+    side_steps = min(args.steps, 3)
     geom.set_shapes(tuned["mixed"]["fp_shape"], tuned["mixed"]["bp_shape"])
     noobj = gpu_b200.Solver(geom, mixed_code, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
-                            objective=False, use_graph=True)
+                            objective=False, use_graph=True, refine=True)
     noobj.set_sinogram(runs["mixed"]["sino"])
     noobj.set_volume(None)
     noobj.iterate(1)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    noobj.iterate(args.steps)
+    noobj.iterate(side_steps)
     e1.record(stream)
     barrier()
-    noobj_ms = job_ms(e0.elapsed_time(e1) / args.steps)
+    noobj_ms = job_ms(e0.elapsed_time(e1) / side_steps)
     noobj.close()
 
     # the reference backprojector's arithmetic (CTR_SART_REFERENCE_BP: the
@@ -1046,10 +1208,10 @@ def main():
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    refbp.iterate(args.steps)
+    refbp.iterate(side_steps)
     e1.record(stream)
     barrier()
-    refbp_ms = job_ms(e0.elapsed_time(e1) / args.steps)
+    refbp_ms = job_ms(e0.elapsed_time(e1) / side_steps)
     refbp.close()
     vtmp = torch.zeros(vshape, device=dev)
     geom.sart_views(vtmp, runs["f32"]["sino"], BETA, 0, 4, flags=gpu_b200.SART_TILED | gpu_b200.SART_REFERENCE_BP)
@@ -1125,21 +1287,23 @@ def main():
         ms_mixed = runs["mixed"]["ms"]
         ms_f32 = runs["f32"]["ms"]
         value = job_rate(ms_mixed, world)
-        # every step: SART (tile, FP + BP per view, untile), FGP (2 per inner
-        # step + final); objective of steps 1..K-1 fused into the next SART pass (tile
-        # x, TV + reduce, 2-level reduce of the partials); of step K separate
-        # (tile, FP, 2 reduce, TV, reduce)
-        launches_per_step = 2 + 2 * SCAN["n_views"] + 2 * FGP_ITERS + 1
-        launches_total = launches_per_step * args.steps + 5 * (args.steps - 1) + 6
+        # every step of the refinement solver: the pass's FISTA factor, FP + BP
+        # per view, the sum y_k + d, FGP (2 per inner step), the final prox with
+        # the rotation; objective of steps 1..K-1 fused into the next pass (TV +
+        # reduce, 2-level reduce of the partials); of step K separate (FP of all
+        # views, 2 reduce, TV, reduce)
+        launches_per_step = 1 + 2 * SCAN["n_views"] + 1 + 2 * FGP_ITERS + 1
+        launches_total = launches_per_step * args.steps + 4 * (args.steps - 1) + 5
         line = {
             "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": f"{args.mixed} storage, f32 arithmetic", "data": "synthetic",
-            "config": {"workload": "SART+FISTA+FGP-TV (20 inner) iteration with objective, 512^3 x 0.5 mm, "
-                                   "1024 views, 1024x768 detector x 0.4 mm, DSO 1000 mm, DOD -500 mm",
-                       "phantom": "40 ellipsoids + 200 spheres (seeded), Siddon projections + 0.5% noise",
-                       "parallelism": f"replicas x{world}", "l2": "inputs > L2 (512 MB+ volume)",
-                       "relaxation": BETA, "lambda_tv": LAMBDA_TV, "fgp_iters": FGP_ITERS},
+            "vs_baseline": None,
+            "dtype": f"{args.mixed} storage for the projectors (refinement: FP32 FISTA state, FP16 sinogram), "
+                     f"f32 arithmetic",
+            "data": "synthetic",
+            "config": scan_config(world),
+            "accuracy_vs_fp64": mixed_acc,
+            "entry_f64": entry64,
             "voxel_updates_per_s": value * V * SCAN["n_views"],
             "ray_voxel_intersections_per_s": value * 3 * segs_per_pass,
             "ray_voxel_intersections_per_pass": segs_per_pass,
@@ -1162,7 +1326,6 @@ def main():
             "f32": {"iter_per_s": job_rate(ms_f32, world), "ms_per_step": ms_f32,
                     "voxel_updates_per_s": job_rate(ms_f32, world) * V * SCAN["n_views"]},
             "mixed_over_f32": ms_f32 / ms_mixed,
-            "mixed_vs_f32_accuracy": mixed_acc,
             "objective_last": {"f32": runs["f32"]["objective_last"], "mixed": runs["mixed"]["objective_last"]},
             "e2e": {"value": job_rate(e2e_ms, world), "unit": "iter/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

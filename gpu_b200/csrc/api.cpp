@@ -607,6 +607,25 @@ extern "C" ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float
     return launch_fdk(*GE(geom), sino, vol, S(stream));
 }
 
+extern "C" ctr_status ctr_fdk_projector_frame(const ctr_geometry* geom, const float* sino, float* vol, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(geom, "geometry"));
+    CTR_TRY(need(sino, "sino"));
+    CTR_TRY(need(vol, "vol"));
+    Geometry* g = GE(geom);
+    CTR_TRY(need_slab(g));
+    const ctr_geometry_desc& d = g->desc;
+    if (g->dg.ct_style != 0) return set_error(CTR_ERR_UNSUPPORTED, "FDK is for the cone-beam geometry");
+    if (d.nx != d.ny || g->dg.vx != g->dg.vy || d.m_offset != 0 || d.offset != 0.0f)
+        return set_error(CTR_ERR_UNSUPPORTED, "the projector frame of FDK needs nx == ny, vx == vy and no offsets");
+    // the FDK frame at angle +theta is the projector's frame at -theta with x and y exchanged
+    cudaStream_t st = S(stream);
+    CTR_TRY(launch_swap_xy(*g, vol, st));
+    CTR_TRY(launch_fdk(*g, sino, vol, st));
+    return launch_swap_xy(*g, vol, st);
+}
+
 extern "C" ctr_status ctr_fdk_backproject(const ctr_geometry* geom, const float* filtered, int v0, int n, float* vol,
                                           void* stream)
 {
@@ -713,9 +732,10 @@ struct ctr_solver {
     void* xt = nullptr;      // 8x8-tiled copy of x_(k-1) for the objective fused into the SART pass
     float t = 1.0f;          // t_(k-1) of V63/main_recon.cu:177
     int k = 0;
-    cudaGraph_t graph[2] = {nullptr, nullptr};        // SART pass: plain, with the fused objective
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    const void* graph_ws[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // workspaces captured with
+    // SART pass: plain, with the fused objective, the refinement pass
+    cudaGraph_t graph[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+    const void* graph_ws[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};   // workspaces captured with
     double* d_obj = nullptr; // [2] fid, tv
     // Objective history on the device, row k-1 = (fidelity, TV) of x_k.  The
     // objective of the latest x_k is "pending" until the next SART pass
@@ -725,6 +745,18 @@ struct ctr_solver {
     std::vector<unsigned char> hist_valid;
     bool obj_pending = false;
     int slabs = 1;           // > 1: the SART pass of the reference's slabs-device build (ctr_solver_set_slabs)
+    // Refinement solver (p.refine): FP32 x_k and x_(k-1); xt is the 16-bit
+    // copy of x_k the projectors read (tiled) and yt the correction volume d
+    // (tiled); ax holds A x~ of the previous copy, one FP32 value per ray of
+    // every view; gm is the FISTA factor of the coming pass (device: d_gm).
+    bool refine = false;
+    float* xk32 = nullptr;
+    float* xm32 = nullptr;
+    float* ax = nullptr;
+    float* d_gm = nullptr;
+    float gm = 0.0f;
+    // the FP64 reference solver (vol_dtype CTR_F64, f64.cu)
+    F64Solver* f64 = nullptr;
 };
 
 extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt, const ctr_solver_params* p,
@@ -734,8 +766,8 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
     CTR_TRY(need(geom, "geometry"));
     CTR_TRY(need(p, "params"));
     CTR_TRY(need(out, "out"));
-    CTR_TRY(need_dtype(vdt, "vol_dtype"));
     *out = nullptr;
+    if (vdt != CTR_F64) CTR_TRY(need_dtype(vdt, "vol_dtype"));
     CTR_TRY(need_slab(GE(geom)));
     if (!std::isfinite(p->beta) || !std::isfinite(p->lambda_tv) || p->lambda_tv < 0.f || p->fgp_iters < 0)
         return set_error(CTR_ERR_INVALID_ARGUMENT, "bad solver parameters");
@@ -744,13 +776,36 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
     s->g = GE(geom);
     s->vdt = vdt;
     s->p = *p;
+    if (vdt == CTR_F64) {   // the FP64 reference solver
+        ctr_status st = f64_create(s->g, *p, &s->f64);
+        if (st != CTR_OK) {
+            delete s;
+            return st;
+        }
+        *out = s;
+        return CTR_OK;
+    }
+    s->refine = p->refine != 0;
     const size_t bytes = s->g->nvox() * dtype_size(vdt);
     cudaError_t e;
+    if (s->refine) {
+        const size_t b32 = s->g->nvox() * sizeof(float);
+        const size_t nax = (size_t)s->g->npix() * s->g->desc.n_views * sizeof(float);
+        if ((e = cudaMalloc(&s->xk32, b32)) != cudaSuccess || (e = cudaMalloc(&s->xm32, b32)) != cudaSuccess ||
+            (e = cudaMalloc(&s->ax, nax)) != cudaSuccess || (e = cudaMalloc(&s->d_gm, sizeof(float))) != cudaSuccess ||
+            (e = cudaMemset(s->xk32, 0, b32)) != cudaSuccess || (e = cudaMemset(s->xm32, 0, b32)) != cudaSuccess ||
+            (e = cudaMemset(s->ax, 0, nax)) != cudaSuccess || (e = cudaMemset(s->d_gm, 0, sizeof(float))) != cudaSuccess) {
+            ctr_status st = cuda_error(e, "refinement solver allocation");
+            ctr_solver_destroy(s);
+            return st;
+        }
+    }
     if ((e = cudaMalloc(&s->y, bytes)) != cudaSuccess || (e = cudaMalloc(&s->xprev, bytes)) != cudaSuccess ||
         (e = cudaMalloc(&s->yt, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess ||
         (e = cudaMalloc(&s->xt, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess ||
         (e = cudaMalloc(&s->d_obj, 4 * sizeof(double))) != cudaSuccess || (e = cudaMemset(s->y, 0, bytes)) != cudaSuccess ||
-        (e = cudaMemset(s->xprev, 0, bytes)) != cudaSuccess) {
+        (e = cudaMemset(s->xprev, 0, bytes)) != cudaSuccess ||
+        (e = cudaMemset(s->xt, 0, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess) {
         ctr_status st = cuda_error(e, "solver allocation");
         ctr_solver_destroy(s);
         return st;
@@ -761,7 +816,7 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
 
 static void drop_graph(ctr_solver* s)
 {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 3; ++i) {
         if (s->exec[i]) cudaGraphExecDestroy(s->exec[i]);
         if (s->graph[i]) cudaGraphDestroy(s->graph[i]);
         s->exec[i] = nullptr;
@@ -779,6 +834,11 @@ extern "C" ctr_status ctr_solver_destroy(ctr_solver* s)
     cudaFree(s->xt);
     cudaFree(s->d_obj);
     cudaFree(s->d_hist);
+    cudaFree(s->xk32);
+    cudaFree(s->xm32);
+    cudaFree(s->ax);
+    cudaFree(s->d_gm);
+    if (s->f64) f64_destroy(s->f64);
     delete s;
     return CTR_OK;
 }
@@ -805,6 +865,7 @@ extern "C" ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void
     clear_error();
     CTR_TRY(need(s, "solver"));
     cudaStream_t st = S(stream);
+    if (s->f64) return f64_set_volume(s->f64, (const double*)vol, st);
     const size_t bytes = s->g->nvox() * dtype_size(s->vdt);
     if (vol) {
         CTR_CUDA_TRY(cudaMemcpyAsync(s->y, vol, bytes, cudaMemcpyDefault, st));
@@ -813,11 +874,122 @@ extern "C" ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void
         CTR_CUDA_TRY(cudaMemsetAsync(s->y, 0, bytes, st));
         CTR_CUDA_TRY(cudaMemsetAsync(s->xprev, 0, bytes, st));
     }
+    if (s->refine) {   // x_k = x_(k-1) = the estimate in FP32, its 16-bit copy, no previous projection
+        const size_t b32 = s->g->nvox() * sizeof(float);
+        CTR_TRY(launch_convert(s->y, s->vdt, s->xk32, CTR_F32, s->g->nvox(), st));
+        CTR_CUDA_TRY(cudaMemcpyAsync(s->xm32, s->xk32, b32, cudaMemcpyDeviceToDevice, st));
+        CTR_TRY(launch_tiling(*s->g, s->y, s->xt, s->vdt, true, st));
+        CTR_CUDA_TRY(cudaMemsetAsync(s->ax, 0, (size_t)s->g->npix() * s->g->desc.n_views * sizeof(float), st));
+        s->gm = 0.0f;
+    }
     s->t = 1.0f;
     s->k = 0;
     s->obj_pending = false;
     s->hist_valid.clear();
     return CTR_OK;
+}
+
+// The refinement solver's SART pass: d = 0, then per view the projection of
+// the copy xt and of d (FP_SART_REFINE: the residual against y_k, A x~_k into
+// ax, the objective partials of x~_k) and the SART update of d.
+static ctr_status refine_pass(ctr_solver* s, uint32_t seed, const uint32_t* pass_seed, const float* gdev,
+                              cudaStream_t st)
+{
+    Geometry* g = s->g;
+    const long long P = g->npix();
+    const size_t per_view = objective_partials_per_view(g->dg);
+    CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
+    CTR_CUDA_TRY(cudaMemsetAsync(s->yt, 0, (size_t)tiled_count(g->dg) * dtype_size(s->vdt), st));
+    for (int j = 0; j < g->desc.n_views; ++j) {
+        FpArgs a{};
+        a.vol = s->xt; a.vol_dtype = s->vdt; a.view0 = j; a.nview = 1; a.kind = FP_SART_REFINE; a.tiled = 1;
+        a.out = g->d_rays; a.b = (const char*)s->sino + (size_t)j * P * dtype_size(s->sdt); a.b_dtype = s->sdt;
+        a.vol2 = s->yt; a.ax = s->ax + (size_t)j * P; a.gdev = gdev; a.partial = g->d_partial + (size_t)j * per_view;
+        CTR_TRY(launch_forward(*g, a, st, nullptr));
+        BpArgs b{};
+        b.vol = s->yt; b.vol_dtype = s->vdt; b.rays = g->d_rays; b.view0 = j; b.nview = 1; b.sart = 1;
+        b.flags = s->p.sart_flags; b.beta = s->p.beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j;
+        b.pass_seed = pass_seed; b.tiled = 1;
+        CTR_TRY(launch_backproject(*g, b, st));
+    }
+    return CTR_OK;
+}
+
+// Replay graph gi of the solver, capturing issue(stream) first if it has none
+// or if a workspace it used (ws0, ws1) was reallocated by another call.
+template <typename F>
+static ctr_status solver_graph(ctr_solver* s, int gi, const void* ws0, const void* ws1, cudaStream_t st, F issue)
+{
+    if (s->exec[gi] && (s->graph_ws[gi][0] != ws0 || s->graph_ws[gi][1] != ws1)) {
+        cudaGraphExecDestroy(s->exec[gi]);
+        cudaGraphDestroy(s->graph[gi]);
+        s->exec[gi] = nullptr;
+        s->graph[gi] = nullptr;
+    }
+    if (!s->exec[gi]) {
+        cudaStream_t cs;
+        CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        ctr_status r = CTR_OK;
+        if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
+        if (r == CTR_OK) r = issue(cs);
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(cs, &gr);
+        if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
+        if (r == CTR_OK) {
+            e = cudaGraphInstantiate(&s->exec[gi], gr, 0);
+            if (e != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
+        }
+        s->graph[gi] = gr;
+        s->graph_ws[gi][0] = ws0;
+        s->graph_ws[gi][1] = ws1;
+        cudaStreamDestroy(cs);
+        if (r != CTR_OK) {
+            if (s->exec[gi]) cudaGraphExecDestroy(s->exec[gi]);
+            if (s->graph[gi]) cudaGraphDestroy(s->graph[gi]);
+            s->exec[gi] = nullptr;
+            s->graph[gi] = nullptr;
+            return r;
+        }
+    }
+    CTR_CUDA_TRY(cudaGraphLaunch(s->exec[gi], st));
+    return CTR_OK;
+}
+
+// The refinement pass of ctr_solver_iterate: the FISTA factor of the pass
+// goes to device memory first, so the captured graph reads it.
+static ctr_status solver_refine_pass(ctr_solver* s, uint32_t seed, cudaStream_t st)
+{
+    Geometry* g = s->g;
+    CTR_TRY(ensure_rays(g, (size_t)g->npix() * sizeof(float2)));
+    CTR_TRY(ensure_partial(g, objective_partials_per_view(g->dg) * g->desc.n_views + 2048));
+    CTR_TRY(launch_set_scalar(s->d_gm, s->gm, st));
+    const bool stoch = (s->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
+    if (!s->p.use_graph || stoch) return refine_pass(s, seed, nullptr, s->d_gm, st);
+    return solver_graph(s, 2, g->d_rays, g->d_partial, st,
+                        [&](cudaStream_t cs) { return refine_pass(s, 0, nullptr, s->d_gm, cs); });
+}
+
+// The refinement solver's objective of x_k by its own projection: the
+// fidelity of the copy xt (tiled) that the passes project, the TV of the
+// FP32 x_k, into d_obj.
+static ctr_status refine_objective(ctr_solver* s, cudaStream_t st)
+{
+    Geometry* g = s->g;
+    const size_t per_view = objective_partials_per_view(g->dg);
+    const size_t nblk = per_view * g->desc.n_views;
+    CTR_TRY(ensure_partial(g, std::max(nblk, (size_t)148 * 64) + 2048));
+    const long long P = g->npix();
+    for (int c = 0; c < g->desc.n_views; c += 65535) {
+        FpArgs a{};
+        a.vol = s->xt; a.vol_dtype = s->vdt; a.view0 = c; a.nview = std::min(65535, g->desc.n_views - c);
+        a.kind = FP_OBJECTIVE; a.tiled = 1;
+        a.b = (const char*)s->sino + (size_t)c * P * dtype_size(s->sdt); a.b_dtype = s->sdt;
+        a.partial = g->d_partial + (size_t)c * per_view;
+        CTR_TRY(launch_forward(*g, a, st, nullptr));
+    }
+    CTR_TRY(launch_reduce(g->d_partial, nblk, s->d_obj, st));
+    return launch_tv(*g, s->xk32, CTR_F32, g->d_partial, 148 * 64, s->d_obj + 1, st);
 }
 
 // One SART pass (fused: also the objective partials of xt), captured once per
@@ -833,43 +1005,10 @@ static ctr_status solver_sart(ctr_solver* s, uint32_t seed, cudaStream_t st, boo
     if (!s->p.use_graph || stoch)   // the seed changes every pass: issue directly
         return sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, seed, st, nullptr, s->yt, xt,
                          part);
-    const int gi = fused ? 1 : 0;
-    if (s->exec[gi] && (s->graph_ws[gi][0] != g->d_rays || s->graph_ws[gi][1] != part)) {
-        cudaGraphExecDestroy(s->exec[gi]);   // a workspace was reallocated by another call
-        cudaGraphDestroy(s->graph[gi]);
-        s->exec[gi] = nullptr;
-        s->graph[gi] = nullptr;
-    }
-    if (!s->exec[gi]) {
-        cudaStream_t cs;
-        CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-        ctr_status r = CTR_OK;
-        if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
-        if (r == CTR_OK)
-            r = sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, cs, nullptr, s->yt, xt,
-                          part);
-        cudaGraph_t gr = nullptr;
-        e = cudaStreamEndCapture(cs, &gr);
-        if (r == CTR_OK && e != cudaSuccess) r = cuda_error(e, "cudaStreamEndCapture");
-        if (r == CTR_OK) {
-            e = cudaGraphInstantiate(&s->exec[gi], gr, 0);
-            if (e != cudaSuccess) r = cuda_error(e, "cudaGraphInstantiate");
-        }
-        s->graph[gi] = gr;
-        s->graph_ws[gi][0] = g->d_rays;
-        s->graph_ws[gi][1] = part;
-        cudaStreamDestroy(cs);
-        if (r != CTR_OK) {
-            if (s->exec[gi]) cudaGraphExecDestroy(s->exec[gi]);
-            if (s->graph[gi]) cudaGraphDestroy(s->graph[gi]);
-            s->exec[gi] = nullptr;
-            s->graph[gi] = nullptr;
-            return r;
-        }
-    }
-    CTR_CUDA_TRY(cudaGraphLaunch(s->exec[gi], st));
-    return CTR_OK;
+    return solver_graph(s, fused ? 1 : 0, g->d_rays, part, st, [&](cudaStream_t cs) {
+        return sart_pass(g, s->y, s->vdt, s->sino, s->sdt, s->p.beta, s->p.sart_flags, 0, cs, nullptr, s->yt, xt,
+                         part);
+    });
 }
 
 // The SART pass of the reference's D-device build on the solver's tiled
@@ -891,6 +1030,9 @@ extern "C" ctr_status ctr_solver_set_slabs(ctr_solver* s, int n_slabs)
     clear_error();
     CTR_TRY(need(s, "solver"));
     if (n_slabs < 1) return set_error(CTR_ERR_INVALID_ARGUMENT, "n_slabs must be >= 1");
+    if (n_slabs > 1 && (s->refine || s->f64))
+        return set_error(CTR_ERR_UNSUPPORTED, "the slab pass is not available to the %s solver",
+                         s->f64 ? "FP64" : "refinement");
     if (n_slabs > 1) {
         std::vector<Geometry*> sl;
         CTR_TRY(slab_geoms(s->g, n_slabs, sl));   // the slab geometries, streams, events
@@ -935,6 +1077,12 @@ static ctr_status flush_objective(ctr_solver* s, cudaStream_t st)
     if (!s->obj_pending) return CTR_OK;
     const void* xk = s->p.fista ? s->xprev : s->y;
     CTR_TRY(hist_reserve(s, s->k, st));
+    if (s->refine) {   // the fidelity of the projectors' copy of x_k, the TV of the FP32 x_k
+        CTR_TRY(refine_objective(s, st));
+        CTR_TRY(hist_store(s, s->k, st));
+        s->obj_pending = false;
+        return CTR_OK;
+    }
     // with the slab pass, the n-device build's projector (its own for the tetrahedron beam)
     Geometry* og = (s->slabs > 1 && s->g->split_geom) ? s->g->split_geom : s->g;
     CTR_TRY(objective_async(og, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
@@ -970,8 +1118,40 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
     if (n < 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "n < 0");
     cudaStream_t st = S(stream);
     Geometry* g = s->g;
+    if (s->f64) return f64_iterate(s->f64, s->sino, s->sdt, n, obj_out, st);
     const int k0 = s->k;
     CTR_TRY(hist_reserve(s, k0 + n, st));
+    if (s->refine) {
+        for (int it = 0; it < n; ++it) {
+            // y_k = (1+g) x_k - g x_(k-1) stays implicit: the pass projects the
+            // copy of x_k and the correction d, and the objective of x_k rides
+            // on it (V63/main_recon.cu:344-386, 390-430)
+            const bool pending = s->obj_pending;
+            if (pending) CTR_TRY(launch_tv(*g, s->xk32, CTR_F32, g->d_partial, 148 * 64, s->d_obj + 1, st));
+            CTR_TRY(solver_refine_pass(s, (uint32_t)(s->k + 1), st));
+            if (pending) {
+                CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj,
+                                      st));
+                CTR_TRY(hist_store(s, s->k, st));
+                s->obj_pending = false;
+            }
+            const float lam = s->p.lambda_tv > 0.f ? s->p.beta * s->p.lambda_tv : 0.f;
+            CTR_TRY(launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->xt, s->vdt, lam, s->p.fgp_iters, s->d_gm,
+                                         st));
+            const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // :372
+            if (s->p.fista) {
+                s->gm = (s->t - 1.0f) / t_k;                                     // the next pass's y_k
+                s->t = t_k;
+            }
+            s->k++;
+            s->obj_pending = s->p.objective != 0;
+        }
+        if (obj_out && n > 0) {
+            CTR_TRY(flush_objective(s, st));
+            CTR_TRY(read_history(s, k0 + 1, n, obj_out, st));
+        }
+        return check_device_errors(g, st);
+    }
     for (int it = 0; it < n; ++it) {
         // The objective of x_(k-1), the previous iteration's result (V63/main_recon.cu:390-430),
         // is projected in this iteration's SART traversal: x_(k-1) is xprev with
@@ -1022,6 +1202,8 @@ extern "C" ctr_status ctr_solver_objectives(ctr_solver* s, int first, int count,
     clear_error();
     CTR_TRY(need(s, "solver"));
     CTR_TRY(need(out, "out"));
+    if (s->f64)
+        return set_error(CTR_ERR_UNSUPPORTED, "the FP64 solver returns its objectives from ctr_solver_iterate only");
     if (first < 1 || count < 0 || first + count - 1 > s->k)
         return set_error(CTR_ERR_INVALID_ARGUMENT, "iterations %d..%d not run (k = %d)", first, first + count - 1, s->k);
     if (count == 0) return CTR_OK;
@@ -1036,16 +1218,52 @@ extern "C" ctr_status ctr_solver_get_volume(ctr_solver* s, void* dst, void* stre
     clear_error();
     CTR_TRY(need(s, "solver"));
     CTR_TRY(need(dst, "dst"));
+    if (s->f64) return f64_get_volume(s->f64, dst, false, S(stream));
     const void* xk = (s->p.fista && s->k > 0) ? s->xprev : s->y;
+    if (s->refine) {   // the storage rounding of the FP32 x_k (the projectors' copy, untiled)
+        CTR_TRY(launch_convert(s->xk32, CTR_F32, s->y, s->vdt, s->g->nvox(), S(stream)));
+        xk = s->y;
+    }
     CTR_CUDA_TRY(cudaMemcpyAsync(dst, xk, s->g->nvox() * dtype_size(s->vdt), cudaMemcpyDefault, S(stream)));
     CTR_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_solver_get_volume_f32(ctr_solver* s, float* dst, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(s, "solver"));
+    CTR_TRY(need(dst, "dst"));
+    cudaStream_t st = S(stream);
+    if (s->f64) return f64_get_volume(s->f64, dst, true, st);
+    const size_t b32 = s->g->nvox() * sizeof(float);
+    if (s->refine) {
+        CTR_CUDA_TRY(cudaMemcpyAsync(dst, s->xk32, b32, cudaMemcpyDefault, st));
+        CTR_CUDA_TRY(cudaStreamSynchronize(st));
+        return CTR_OK;
+    }
+    const void* xk = (s->p.fista && s->k > 0) ? s->xprev : s->y;
+    if (s->vdt == CTR_F32) {
+        CTR_CUDA_TRY(cudaMemcpyAsync(dst, xk, b32, cudaMemcpyDefault, st));
+        CTR_CUDA_TRY(cudaStreamSynchronize(st));
+        return CTR_OK;
+    }
+    float* tmp = nullptr;   // widened on the device, then copied to dst (which may be host memory)
+    CTR_CUDA_TRY(cudaMalloc(&tmp, b32));
+    ctr_status r = launch_convert(xk, s->vdt, tmp, CTR_F32, s->g->nvox(), st);
+    cudaError_t e = cudaSuccess;
+    if (r == CTR_OK) e = cudaMemcpyAsync(dst, tmp, b32, cudaMemcpyDefault, st);
+    if (r == CTR_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    if (r != CTR_OK) return r;
+    CTR_CUDA_TRY(e);
     return CTR_OK;
 }
 
 extern "C" ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k)
 {
     if (!s || !k) return set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument");
-    *k = s->k;
+    *k = s->f64 ? f64_iteration(s->f64) : s->k;
     return CTR_OK;
 }
 
@@ -1071,15 +1289,19 @@ extern "C" ctr_status ctr_solver_save(ctr_solver* s, const char* path, void* str
     clear_error();
     CTR_TRY(need(s, "solver"));
     CTR_TRY(need(path, "path"));
-    const size_t bytes = s->g->nvox() * dtype_size(s->vdt);
+    if (s->f64) return set_error(CTR_ERR_UNSUPPORTED, "the FP64 solver has no checkpoint");
+    // refinement solver: the FP32 x_k and x_(k-1) (its copies and A x~_(k-1) are rebuilt on load)
+    const size_t bytes = s->g->nvox() * (s->refine ? sizeof(float) : dtype_size(s->vdt));
     std::vector<char> buf(2 * bytes);
-    CTR_CUDA_TRY(cudaMemcpyAsync(buf.data(), s->y, bytes, cudaMemcpyDeviceToHost, S(stream)));
-    CTR_CUDA_TRY(cudaMemcpyAsync(buf.data() + bytes, s->xprev, bytes, cudaMemcpyDeviceToHost, S(stream)));
+    CTR_CUDA_TRY(cudaMemcpyAsync(buf.data(), s->refine ? (void*)s->xk32 : s->y, bytes, cudaMemcpyDeviceToHost,
+                                 S(stream)));
+    CTR_CUDA_TRY(cudaMemcpyAsync(buf.data() + bytes, s->refine ? (void*)s->xm32 : s->xprev, bytes,
+                                 cudaMemcpyDeviceToHost, S(stream)));
     CTR_CUDA_TRY(cudaStreamSynchronize(S(stream)));
     CkptHeader h{};
     memcpy(h.magic, "CTRCKPT1", 8);
-    h.version = 1; h.dtype = s->vdt; h.geom = geom_hash(s->g->desc); h.k = s->k; h.fista = s->p.fista;
-    h.t = s->t; h.nvox = s->g->nvox();
+    h.version = s->refine ? 2 : 1; h.dtype = s->vdt; h.geom = geom_hash(s->g->desc); h.k = s->k;
+    h.fista = s->p.fista; h.t = s->t; h.pad = s->refine ? s->gm : 0.0f; h.nvox = s->g->nvox();
     FILE* f = fopen(path, "wb");
     if (!f) return set_error(CTR_ERR_IO, "cannot open %s for writing", path);
     const bool ok = fwrite(&h, sizeof(h), 1, f) == 1 && fwrite(buf.data(), 1, buf.size(), f) == buf.size();
@@ -1093,19 +1315,42 @@ extern "C" ctr_status ctr_solver_load(ctr_solver* s, const char* path, void* str
     clear_error();
     CTR_TRY(need(s, "solver"));
     CTR_TRY(need(path, "path"));
+    if (s->f64) return set_error(CTR_ERR_UNSUPPORTED, "the FP64 solver has no checkpoint");
     FILE* f = fopen(path, "rb");
     if (!f) return set_error(CTR_ERR_IO, "cannot open %s", path);
     CkptHeader h{};
-    const size_t bytes = s->g->nvox() * dtype_size(s->vdt);
+    const size_t bytes = s->g->nvox() * (s->refine ? sizeof(float) : dtype_size(s->vdt));
     std::vector<char> buf(2 * bytes);
     const bool ok = fread(&h, sizeof(h), 1, f) == 1 && fread(buf.data(), 1, buf.size(), f) == buf.size();
     fclose(f);
     if (!ok || memcmp(h.magic, "CTRCKPT1", 8) != 0) return set_error(CTR_ERR_IO, "%s is not a solver checkpoint", path);
     if (h.geom != geom_hash(s->g->desc) || h.dtype != (uint32_t)s->vdt || h.nvox != (uint64_t)s->g->nvox())
         return set_error(CTR_ERR_INVALID_ARGUMENT, "checkpoint %s was written for another geometry or dtype", path);
-    CTR_CUDA_TRY(cudaMemcpyAsync(s->y, buf.data(), bytes, cudaMemcpyHostToDevice, S(stream)));
-    CTR_CUDA_TRY(cudaMemcpyAsync(s->xprev, buf.data() + bytes, bytes, cudaMemcpyHostToDevice, S(stream)));
-    CTR_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+    if (h.version != (s->refine ? 2u : 1u))
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "checkpoint %s was written by a %s solver", path,
+                         h.version == 2 ? "refinement" : "non-refinement");
+    cudaStream_t st = S(stream);
+    if (s->refine) {
+        // x_k, x_(k-1) in FP32; the copy of x_k (tiled) and A x~_(k-1) of the
+        // copy of x_(k-1), as the passes left them (a forward projection of
+        // the linear copy gives the same sums, with the same zero rule)
+        Geometry* g = s->g;
+        CTR_CUDA_TRY(cudaMemcpyAsync(s->xk32, buf.data(), bytes, cudaMemcpyHostToDevice, st));
+        CTR_CUDA_TRY(cudaMemcpyAsync(s->xm32, buf.data() + bytes, bytes, cudaMemcpyHostToDevice, st));
+        CTR_TRY(launch_convert(s->xk32, CTR_F32, s->y, s->vdt, g->nvox(), st));
+        CTR_TRY(launch_tiling(*g, s->y, s->xt, s->vdt, true, st));
+        CTR_TRY(launch_convert(s->xm32, CTR_F32, s->xprev, s->vdt, g->nvox(), st));
+        FpArgs a{};
+        a.vol = s->xprev; a.vol_dtype = s->vdt; a.view0 = 0; a.nview = g->desc.n_views; a.kind = FP_FORWARD;
+        a.out = s->ax; a.out_dtype = CTR_F32;
+        CTR_TRY(forward_chunks(g, a, st));
+        CTR_CUDA_TRY(cudaStreamSynchronize(st));
+        s->gm = h.pad;
+    } else {
+        CTR_CUDA_TRY(cudaMemcpyAsync(s->y, buf.data(), bytes, cudaMemcpyHostToDevice, st));
+        CTR_CUDA_TRY(cudaMemcpyAsync(s->xprev, buf.data() + bytes, bytes, cudaMemcpyHostToDevice, st));
+        CTR_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     s->k = h.k;
     s->t = h.t;
     s->obj_pending = false;                       // objectives before the checkpoint are not known here
@@ -1135,6 +1380,14 @@ static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_
                                bool fused)
 {
     Geometry* g = s->g;
+    if (s->refine) {   // as ctr_solver_iterate's refinement iteration, with g from gam_dev
+        if (fused) CTR_TRY(launch_tv(*g, s->xk32, CTR_F32, g->d_partial, 148 * 64, s->d_obj + 1, st));
+        CTR_TRY(refine_pass(s, 0, seed_dev, gam_dev, st));
+        if (fused)
+            CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
+        const float lam = s->p.lambda_tv > 0.f ? s->p.beta * s->p.lambda_tv : 0.f;
+        return launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->xt, s->vdt, lam, s->p.fgp_iters, gam_dev, st);
+    }
     if (fused) {
         const void* xk1 = s->p.fista ? s->xprev : s->y;
         CTR_TRY(launch_tiling(*g, xk1, s->xt, s->vdt, true, st));
@@ -1244,6 +1497,7 @@ extern "C" ctr_status ctr_batch_create(const ctr_geometry* const* geoms, int n, 
     CTR_TRY(need(out, "out"));
     *out = nullptr;
     if (n <= 0) return set_error(CTR_ERR_INVALID_ARGUMENT, "need at least one scan");
+    if (vdt == CTR_F64) return set_error(CTR_ERR_UNSUPPORTED, "the FP64 solver runs one scan at a time");
     for (int i = 0; i < n; ++i) {
         if (!geoms[i]) return set_error(CTR_ERR_INVALID_ARGUMENT, "geometry %d is NULL", i);
         for (int j = 0; j < i; ++j)
@@ -1334,14 +1588,20 @@ extern "C" ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* obj_out, vo
         for (int i = 0; i < ns; ++i) {
             ctr_solver* s = b->scans[i];
             const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // V63/main_recon.cu:372
-            b->h_gam[i] = (s->t - 1.0f) / t_k;
+            // the momentum of this iteration, or for a refinement solver the
+            // factor of y_k that its pass projects (set by the previous iteration)
+            b->h_gam[i] = s->refine ? s->gm : (s->t - 1.0f) / t_k;
             b->h_seed[i] = (uint32_t)(s->k + 1);   // the single-scan solver's seed of this pass
         }
         CTR_CUDA_TRY(cudaMemcpyAsync(b->d_gam, b->h_gam.data(), sizeof(float) * ns, cudaMemcpyHostToDevice, st));
         CTR_CUDA_TRY(cudaMemcpyAsync(b->d_seed, b->h_seed.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice, st));
         CTR_CUDA_TRY(cudaGraphLaunch(b->exec[gi], st));
         for (auto* s : b->scans) {
-            if (s->p.fista) s->t = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;
+            if (s->p.fista) {
+                const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;
+                if (s->refine) s->gm = (s->t - 1.0f) / t_k;
+                s->t = t_k;
+            }
             s->k++;
         }
         if (gi == 1) CTR_TRY(obj_rows(it - 1));
@@ -1350,7 +1610,8 @@ extern "C" ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* obj_out, vo
         if (objective) {
             for (auto* s : b->scans) {
                 const void* xk = s->p.fista ? s->xprev : s->y;
-                CTR_TRY(objective_async(s->g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
+                if (s->refine) CTR_TRY(refine_objective(s, st));
+                else CTR_TRY(objective_async(s->g, xk, s->vdt, s->sino, s->sdt, s->d_obj, s->d_obj + 1, st, s->yt));
             }
             CTR_TRY(obj_rows(n - 1));
         } else if (obj_out) {
@@ -1367,6 +1628,14 @@ extern "C" ctr_status ctr_batch_get_volume(ctr_batch* b, int scan, void* dst, vo
     CTR_TRY(need(b, "batch"));
     if (scan < 0 || scan >= (int)b->scans.size()) return set_error(CTR_ERR_INVALID_ARGUMENT, "scan %d out of range", scan);
     return ctr_solver_get_volume(b->scans[scan], dst, stream);
+}
+
+extern "C" ctr_status ctr_batch_get_volume_f32(ctr_batch* b, int scan, float* dst, void* stream)
+{
+    clear_error();
+    CTR_TRY(need(b, "batch"));
+    if (scan < 0 || scan >= (int)b->scans.size()) return set_error(CTR_ERR_INVALID_ARGUMENT, "scan %d out of range", scan);
+    return ctr_solver_get_volume_f32(b->scans[scan], dst, stream);
 }
 
 // -------------------------------------------- reference-compatible entry points

@@ -139,8 +139,12 @@ ctr_status check_device_errors(Geometry* g, cudaStream_t st);
 // FP_SART_OBJ: the SART correction of vol and, in the same traversal, the
 // objective residual (A vol2 - b)^2 of a second volume.
 // FP_PARTIAL: a slab's (Sum(len*f), Sum(len)) per ray as float2, no threshold.
+// FP_SART_REFINE: the refinement solver's pass.  vol is the 16-bit copy of
+// x_k, vol2 the correction volume d; per ray c = (b - ((1+g)Ax_k - g Ax_(k-1))
+// - Ad)/len with g = *gdev and Ax_(k-1) read from ax[p], which is then
+// overwritten with Ax_k; the objective partials of x_k as FP_SART_OBJ.
 enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3, FP_DOT = 4, FP_SART_OBJ = 5,
-              FP_PARTIAL = 6 };
+              FP_PARTIAL = 6, FP_SART_REFINE = 7 };
 struct FpArgs {
     const void* vol; ctr_dtype vol_dtype;
     int view0, nview;
@@ -152,6 +156,8 @@ struct FpArgs {
     const void* vol2 = nullptr;           // SART_OBJ: the volume of the objective (same dtype, layout)
     int* nseg; uint64_t* hash; float* len;  // TRACE
     int tiled = 0;                        // vol in the 8x8-tiled layout (FORWARD, SART, OBJECTIVE)
+    float* ax = nullptr;                  // SART_REFINE: FP32 ray sums of the previous x copy, this view
+    const float* gdev = nullptr;          // SART_REFINE: the FISTA factor g (device)
 };
 ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, size_t* nblocks_out);
 // objective partials per view: one per warp of 32 rays
@@ -210,9 +216,30 @@ ctr_status launch_fgp(Geometry& g, void* vol, ctr_dtype dt, float lambda, int it
                       const float* gamma_dev = nullptr);
 ctr_status launch_momentum(const Geometry& g, void* y, void* xprev, const void* x, ctr_dtype dt,
                            float gam, cudaStream_t st, const float* gamma_dev = nullptr);
+// Refinement solver, after its SART pass (fgp.cu): xm = (1+g) xk - g xm + d
+// (d tiled, dt storage), then with lam > 0 and iters >= 0 the FGP-TV prox of
+// that FP32 volume (duals in dt storage), and x* (the prox, or the sum when
+// lam == 0) rotated in: xm = xk, xk = x*, xt = the dt copy of x* (tiled).
+ctr_status launch_refine_update(Geometry& g, float* xk, float* xm, const void* d_tiled, void* xt_tiled,
+                                ctr_dtype dt, float lam, int iters, const float* gdev, cudaStream_t st);
+// *p = v on the device (a per-iteration scalar that graphs read)
+ctr_status launch_set_scalar(float* p, float v, cudaStream_t st);
+
+// The FP64 reference solver (f64.cu): the solver's iteration with every step
+// in FP64.  obj_out (host, may be NULL): [TV, fidelity, objective] per
+// iteration, evaluated when params.objective is set (NaN otherwise).
+struct F64Solver;
+ctr_status f64_create(Geometry* g, const ctr_solver_params& p, F64Solver** out);
+void f64_destroy(F64Solver* s);
+ctr_status f64_set_volume(F64Solver* s, const double* vol, cudaStream_t st);
+ctr_status f64_iterate(F64Solver* s, const void* sino, ctr_dtype sdt, int n, double* obj_out, cudaStream_t st);
+ctr_status f64_get_volume(F64Solver* s, void* dst, bool as_f32, cudaStream_t st);
+int f64_iteration(const F64Solver* s);
 ctr_status launch_convert(const void* src, ctr_dtype sdt, void* dst, ctr_dtype ddt, long long n,
                           cudaStream_t st);
 ctr_status launch_fdk(Geometry& g, const float* sino, float* vol, cudaStream_t st);
+// exchange x and y of every z slice in place (nx == ny)
+ctr_status launch_swap_xy(const Geometry& g, float* vol, cudaStream_t st);
 // the backprojection stage: vol += views [view0, view0+nview) of the filtered sinogram (fsino[0] = view0)
 ctr_status launch_fdk_bp(const Geometry& g, const float* fsino, int view0, int nview, float* vol, cudaStream_t st);
 ctr_status launch_phantom(const Geometry& g, const double* dparams, int n, float* vol,

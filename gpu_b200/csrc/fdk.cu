@@ -244,6 +244,25 @@ ctr_status launch_fdk(Geometry& G, const float* sino, float* vol, cudaStream_t s
     return launch_fdk_bp(G, fsino, 0, nv, vol, st);
 }
 
+// In-place exchange of x and y in every z slice of a square (nx == ny) volume.
+__global__ void k_swap_xy(int n, int Z, float* __restrict__ vol)
+{
+    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+    if (i >= n || j >= n || i >= j) return;
+    float* sl = vol + (long long)k * n * n;
+    const float a = sl[(long long)j * n + i];
+    sl[(long long)j * n + i] = sl[(long long)i * n + j];
+    sl[(long long)i * n + j] = a;
+}
+
+ctr_status launch_swap_xy(const Geometry& G, float* vol, cudaStream_t st)
+{
+    const int n = G.desc.nx, Z = G.desc.nz;
+    k_swap_xy<<<dim3((n + 31) / 32, (n + 7) / 8, Z), dim3(32, 8), 0, st>>>(n, Z, vol);
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
 ctr_status launch_fdk_bp(const Geometry& G, const float* fsino, int view0, int nview, float* vol, cudaStream_t st)
 {
     const DevGeom& g = G.dg;

@@ -14,8 +14,10 @@ namespace ctr {
 
 static constexpr int FG_BX = 32, FG_BY = 8;
 
-template <typename T>
-__device__ __forceinline__ float fgp_L(const T* __restrict__ f, const T* __restrict__ r, const T* __restrict__ s,
+// f may be stored in another type than the duals (the refinement solver's
+// FP32 sum y_k + d against 16-bit duals).
+template <typename T, typename TF = T>
+__device__ __forceinline__ float fgp_L(const TF* __restrict__ f, const T* __restrict__ r, const T* __restrict__ s,
                                        const T* __restrict__ t, int x, int y, int z, long long p, int M, long long MN,
                                        float lambda)
 {
@@ -23,7 +25,7 @@ __device__ __forceinline__ float fgp_L(const T* __restrict__ f, const T* __restr
     const float sv = Store<T>::ld(s + p), sm = y > 0 ? Store<T>::ld(s + p - M) : 0.0f;
     const float tv = Store<T>::ld(t + p), tm = z > 0 ? Store<T>::ld(t + p - MN) : 0.0f;
     const float tl = fa(fa(fs(rv, rm), fs(sv, sm)), fs(tv, tm));       // L_Pc :14
-    return fs(Store<T>::ld(f + p), fm(lambda, tl));                    // :17
+    return fs(Store<TF>::ld(f + p), fm(lambda, tl));                   // :17
 }
 
 // One inner iteration in two passes, as the reference's x7 form: k_fgp_L
@@ -32,9 +34,9 @@ __device__ __forceinline__ float fgp_L(const T* __restrict__ f, const T* __restr
 // updates the voxel's own duals in place (no voxel reads another's duals in
 // this pass, so no double buffer is needed).  One thread per voxel, a 3-D
 // grid of 32x8 tiles: both passes stream at close to the copy bandwidth.
-template <typename T>
+template <typename T, typename TF = T>
 __global__ void __launch_bounds__(FG_BX * FG_BY)
-k_fgp_L(int M, int N, int Z, const T* __restrict__ f, const T* __restrict__ r, const T* __restrict__ s,
+k_fgp_L(int M, int N, int Z, const TF* __restrict__ f, const T* __restrict__ r, const T* __restrict__ s,
         const T* __restrict__ t, float* __restrict__ L, float lambda)
 {
     const int x = blockIdx.x * FG_BX + threadIdx.x;
@@ -43,7 +45,7 @@ k_fgp_L(int M, int N, int Z, const T* __restrict__ f, const T* __restrict__ r, c
     if (x >= M || y >= N) return;
     const long long MN = (long long)M * N;
     const long long p = (long long)z * MN + (long long)y * M + x;
-    L[p] = fgp_L(f, r, s, t, x, y, z, p, M, MN, lambda);                 // L_Pc, GPUx7.cu:2-24
+    L[p] = fgp_L<T, TF>(f, r, s, t, x, y, z, p, M, MN, lambda);          // L_Pc, GPUx7.cu:2-24
 }
 
 template <typename T>
@@ -114,6 +116,44 @@ k_fgp_final(int M, int N, int Z, T* __restrict__ vol, const T* __restrict__ o, c
     }
 }
 
+// Refinement solver: the FP32 input of the prox, y_k + d = (1+g) x_k - g x_(k-1) + d,
+// written over x_(k-1) (which is not needed after it).  d is read in the
+// projectors' tiled layout.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_refine_sum(const DevGeom g, const float* __restrict__ xk, float* __restrict__ xm, const T* __restrict__ d,
+             const float* __restrict__ gdev)
+{
+    const float gm = *gdev;
+    const long long MN = (long long)g.M * g.N, n = MN * g.Z;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % g.M), y = (int)((p / g.M) % g.N), z = (int)(p / MN);
+        const float yk = fs(fm(fa(1.0f, gm), xk[p]), fm(gm, xm[p]));
+        xm[p] = fa(yk, Store<T>::ld(d + tile_index(g, x, y, z)));
+    }
+}
+
+// Refinement solver: x* = the prox f - lambda*div(o,p,q) of f = xm (FGP), or
+// f itself; then the rotation x_(k-1) = x_k, x_k = x*, and the projectors'
+// 16-bit copy of x* in the tiled layout (round to nearest).
+template <typename T, bool FGP>
+__global__ void __launch_bounds__(256)
+k_refine_final(const DevGeom g, float* __restrict__ xk, float* __restrict__ xm, const T* __restrict__ o,
+               const T* __restrict__ pd, const T* __restrict__ q, float lambda, T* __restrict__ xt)
+{
+    const int M = g.M;
+    const long long MN = (long long)g.M * g.N, n = MN * g.Z;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % M), y = (int)((p / M) % g.N), z = (int)(p / MN);
+        const float xs = FGP ? fgp_L<T, float>(xm, o, pd, q, x, y, z, p, M, MN, lambda) : xm[p];
+        xm[p] = xk[p];
+        xk[p] = xs;
+        Store<T>::st(xt + tile_index(g, x, y, z), xs);
+    }
+}
+
+__global__ void k_set_scalar(float* p, float v) { *p = v; }
+
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_momentum(long long n, T* __restrict__ y, T* __restrict__ xprev, const T* __restrict__ x, float gam,
@@ -180,6 +220,48 @@ ctr_status launch_momentum(const Geometry& G, void* y, void* xprev, const void* 
     CTR_DISPATCH_DTYPE(dt, T, {
         k_momentum<T><<<grid_for(V, 256), 256, 0, st>>>(V, (T*)y, (T*)xprev, (const T*)x, gam, gamma_dev);
     });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+ctr_status launch_refine_update(Geometry& G, float* xk, float* xm, const void* d_tiled, void* xt_tiled, ctr_dtype dt,
+                                float lam, int iters, const float* gdev, cudaStream_t st)
+{
+    const int M = G.desc.nx, N = G.desc.ny, Z = G.desc.nz;
+    const long long V = G.nvox();
+    const size_t es = dtype_size(dt);
+    const bool fgp = lam > 0.f && iters >= 0;
+    if (fgp) CTR_TRY(ensure_fgp(&G, fgp_workspace_bytes(V, dt)));
+    const int nb = grid_for(V, 256);
+    CTR_DISPATCH_DTYPE(dt, T, {
+        k_refine_sum<T><<<nb, 256, 0, st>>>(G.dg, xk, xm, (const T*)d_tiled, gdev);
+        if (fgp) {
+            CTR_CUDA_TRY(cudaMemsetAsync(G.d_fgp, 0, 6 * (size_t)V * es, st));
+            const float alpha12 = 1.0f / (lam * 12.0f);
+            const dim3 blk(FG_BX, FG_BY), grd((M + FG_BX - 1) / FG_BX, (N + FG_BY - 1) / FG_BY, Z);
+            T* base = (T*)G.d_fgp;
+            T* D[6] = {base, base + V, base + 2 * V, base + 3 * V, base + 4 * V, base + 5 * V};   // r s t o p q
+            float* L = (float*)((char*)G.d_fgp + 6 * (size_t)V * es);
+            float t_k_1 = 1.0f;
+            for (int it = 0; it < iters; ++it) {
+                const float t_k = next_t(t_k_1);
+                const float gam = (t_k_1 - 1.0f) / t_k;
+                k_fgp_L<T, float><<<grd, blk, 0, st>>>(M, N, Z, xm, D[0], D[1], D[2], L, lam);
+                k_fgp_dual<T><<<grd, blk, 0, st>>>(M, N, Z, L, D[0], D[1], D[2], D[3], D[4], D[5], alpha12, gam);
+                t_k_1 = t_k;
+            }
+            k_refine_final<T, true><<<nb, 256, 0, st>>>(G.dg, xk, xm, D[3], D[4], D[5], lam, (T*)xt_tiled);
+        } else {
+            k_refine_final<T, false><<<nb, 256, 0, st>>>(G.dg, xk, xm, nullptr, nullptr, nullptr, 0.f, (T*)xt_tiled);
+        }
+    });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+ctr_status launch_set_scalar(float* p, float v, cudaStream_t st)
+{
+    k_set_scalar<<<1, 1, 0, st>>>(p, v);
     CTR_CUDA_TRY(cudaGetLastError());
     return CTR_OK;
 }

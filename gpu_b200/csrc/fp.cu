@@ -355,9 +355,11 @@ template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false,
 __global__ void __launch_bounds__(FP_BX * BY, MINB)
 k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
           const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
-          uint64_t* __restrict__ hash, float* __restrict__ lens, const VT* __restrict__ vol2)
+          uint64_t* __restrict__ hash, float* __restrict__ lens, const VT* __restrict__ vol2,
+          float* __restrict__ ax, const float* __restrict__ gdev)
 {
     constexpr int NT = FP_BX * BY;
+    constexpr bool DUAL = KIND == FP_SART_OBJ || KIND == FP_SART_REFINE;
     extern __shared__ float sp[];
     float* PX;
     float* PY;
@@ -384,7 +386,7 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
         ((float2*)out)[p] = make_float2(0.0f, 0.0f);
     } else if (active) {
         const float2 sc = g.trig[view0 + w];
-        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, KIND == FP_SART_OBJ>(
+        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, DUAL>(
             g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v, vol2);
         const bool zero = rr.len < g.thr_fp;                       // :554
         if (KIND == FP_PARTIAL) {
@@ -399,6 +401,18 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
                 const float e = fs(zero ? 0.0f : rr.sum2, bv);
                 e2 = (double)fm(e, e);                                 // L2_norm_kernel, tool_functions.cu:35
             }
+        } else if (KIND == FP_SART_REFINE) {
+            // the residual against y_k = (1+g) x_k - g x_(k-1) and the correction d so far
+            const float bv = ld_any(b, p, b_dt);
+            const float sx = zero ? 0.0f : rr.sum;                     // A x_k, the objective's rule
+            const float sp = ax[p];                                    // A x_(k-1), from the previous pass
+            const float gm = *gdev;
+            const float ay = fs(fm(fa(1.0f, gm), sx), fm(gm, sp));
+            const float cv = zero ? 0.0f : fdv(fs(fs(bv, ay), rr.sum2), rr.len);
+            ((float2*)out)[p] = make_float2(cv, rr.d12);
+            ax[p] = sx;
+            const float e = fs(sx, bv);
+            e2 = (double)fm(e, e);
         } else if (KIND == FP_OBJECTIVE) {
             const float ax = zero ? 0.0f : rr.sum;
             const float bv = ld_any(b, p, b_dt);
@@ -412,7 +426,7 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
             lens[p] = rr.len;
         }
     }
-    if (KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ) {
+    if (KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_SART_REFINE) {
         double t = e2;
         for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
         if ((threadIdx.x & 31) == 0 && v < g.ZP) partial[((size_t)w * g.ZP + v) * gridDim.x + tx] = t;
@@ -431,16 +445,19 @@ static void launch_fp_tl(const Geometry& G, const FpArgs& a, int nview, size_t s
     const VT* vol = (const VT*)a.vol;
     if (g.entry64)
         k_forward<VT, KIND, true, BY, CPM, TL, MINB><<<grid, FP_BX * BY, smem, st>>>(
-            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2);
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2,
+            a.ax, a.gdev);
     else
         k_forward<VT, KIND, false, BY, CPM, TL, MINB><<<grid, FP_BX * BY, smem, st>>>(
-            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2);
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2,
+            a.ax, a.gdev);
 }
 
 template <typename VT, int KIND, int BY, int CPM = 0, int MINB = 1>
 static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
-    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_PARTIAL) {
+    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_PARTIAL ||
+                  KIND == FP_SART_REFINE) {
         if (a.tiled) {
             launch_fp_tl<VT, KIND, BY, CPM, true, MINB>(G, a, nview, smem, st);
             return;
@@ -476,13 +493,16 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
     const DevGeom& g = G.dg;
     if (a.nview <= 0) return CTR_OK;
     if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
-    if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE && a.kind != FP_SART_OBJ && a.kind != FP_PARTIAL)
+    if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE && a.kind != FP_SART_OBJ && a.kind != FP_PARTIAL &&
+        a.kind != FP_SART_REFINE)
         return set_error(CTR_ERR_UNSUPPORTED, "the tiled layout is for SART and objective projections");
     if (a.kind == FP_SART_OBJ && !a.vol2) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART_OBJ needs vol2");
+    if (a.kind == FP_SART_REFINE && (!a.vol2 || !a.ax || !a.gdev || !a.partial))
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "SART_REFINE needs vol2, ax, gdev and partial");
     // the dot product keeps the fixed shape: its block partial sums, and so
     // the rounding of the total, do not depend on the tuned shape
     if (nblocks_out)
-        *nblocks_out = (a.kind == FP_OBJECTIVE || a.kind == FP_SART_OBJ)
+        *nblocks_out = (a.kind == FP_OBJECTIVE || a.kind == FP_SART_OBJ || a.kind == FP_SART_REFINE)
                            ? objective_partials_per_view(g) * a.nview
                            : (size_t)((g.R + FP_BX - 1) / FP_BX) * ((g.ZP + FP_BY - 1) / FP_BY) * a.nview;
     const size_t smem = plane_tables_bytes(g);
@@ -492,6 +512,7 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
         case FP_SART: launch_fp_shape<VT, FP_SART>(G, a, smem, st); break;
         case FP_OBJECTIVE: launch_fp_shape<VT, FP_OBJECTIVE>(G, a, smem, st); break;
         case FP_SART_OBJ: launch_fp_shape<VT, FP_SART_OBJ>(G, a, smem, st); break;
+        case FP_SART_REFINE: launch_fp_shape<VT, FP_SART_REFINE>(G, a, smem, st); break;
         case FP_PARTIAL: launch_fp_shape<VT, FP_PARTIAL>(G, a, smem, st); break;
         case FP_TRACE: launch_fp_t<VT, FP_TRACE, FP_BY>(G, a, a.nview, smem, st); break;
         case FP_DOT: launch_fp_t<VT, FP_DOT, FP_BY>(G, a, a.nview, smem, st); break;

@@ -23,23 +23,61 @@ static __device__ __align__(256) float2 g_noalloc_rays[kNoAllocMaxRays];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_addr_mu;
-void* g_addr[kMaxDevices] = {};
+// per device: the array's address and the context it was looked up in
+struct Slot {
+    void* addr;
+    unsigned long long ctx_id;
+};
+Slot g_slot[kMaxDevices] = {};
+
+// Identity of the current CUDA context (the driver's unique context id,
+// through the runtime's driver entry points; nothing is linked against the
+// driver library).  A context created after a device reset, or a
+// non-primary context, has a new id, and the module -- with the array --
+// is loaded afresh in it.  Returns false when the entry points are missing.
+bool current_context_id(unsigned long long* id)
+{
+    typedef int (*GetCurrent)(void**);
+    typedef int (*GetId)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    void* ctx = nullptr;
+    return get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, id) == 0;
+}
 
 // Device address of g_noalloc_rays on the current device.  In host code the
 // array's name is only a stand-in; the address comes from
-// cudaGetSymbolAddress, once per device, with that device current.
+// cudaGetSymbolAddress, with the device current, once per device and
+// context: a new context (after cudaDeviceReset, or another context made
+// current) is looked up again.  Without the context id the lookup runs on
+// every call.
 ctr_status scratch_address(int dev, void** out)
 {
     using namespace ctr;
     if (dev < 0 || dev >= kMaxDevices) return set_error(CTR_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+    unsigned long long id = 0;
+    const bool have_id = current_context_id(&id);
     std::lock_guard<std::mutex> lk(g_addr_mu);
-    if (!g_addr[dev]) {
+    Slot& s = g_slot[dev];
+    if (!have_id || !s.addr || s.ctx_id != id) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_rays);
         if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(no-alloc ray records)");
-        g_addr[dev] = p;
+        s.addr = p;
+        s.ctx_id = have_id ? id : 0;
     }
-    *out = g_addr[dev];
+    *out = s.addr;
     return CTR_OK;
 }
 
@@ -55,6 +93,8 @@ extern "C" ctr_status ctr_sart_views_noalloc(const ctr_geometry* geom, void* vol
     if (!geom || !vol || !sino) return set_error(CTR_ERR_INVALID_ARGUMENT, "NULL argument");
     if (!dtype_ok(vdt) || !dtype_ok(sdt)) return set_error(CTR_ERR_INVALID_ARGUMENT, "unknown dtype");
     if (!std::isfinite(beta)) return set_error(CTR_ERR_INVALID_ARGUMENT, "beta must be finite");
+    if (flags & CTR_SART_TILED)   // the tiled copy is a geometry workspace, which this entry point does not allocate
+        return set_error(CTR_ERR_INVALID_ARGUMENT, "CTR_SART_TILED needs a workspace; use ctr_sart_views");
     const Geometry* g = reinterpret_cast<const Geometry*>(geom);
     if (view_begin < 0 || view_count < 0 || (long long)view_begin + view_count > g->desc.n_views)
         return set_error(CTR_ERR_INVALID_ARGUMENT, "view range [%d, %d) outside [0, %d)", view_begin,

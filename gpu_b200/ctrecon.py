@@ -27,8 +27,8 @@ STATUS_NAMES = {
     4: "CTR_ERR_CUDA", 5: "CTR_ERR_TRAVERSAL_BOUND", 6: "CTR_ERR_TIMEOUT", 7: "CTR_ERR_UNSUPPORTED",
     8: "CTR_ERR_NO_DEVICE", 9: "CTR_ERR_IO",
 }
-# ctr_dtype
-F32, BF16, F16 = 0, 1, 2
+# ctr_dtype (F64: the FP64 reference solver's volumes only)
+F32, BF16, F16, F64 = 0, 1, 2, 3
 GEOM_ENTRY_F64 = 0x1
 BP_ACCUMULATE = 0x1
 BP_FOV_MASK = 0x2
@@ -44,7 +44,8 @@ VOLUME_TILED = 0x8
 EXPORTED = [
     "ctr_geometry_create", "ctr_geometry_destroy", "ctr_geometry_view_trig", "ctr_forward",
     "ctr_backproject", "ctr_sart_pass", "ctr_sart_views", "ctr_sart_views_noalloc", "ctr_forward_trace", "ctr_fgp_tv", "ctr_fista_momentum",
-    "ctr_objective", "ctr_tv_norm", "ctr_l2_norm", "ctr_fdk", "ctr_fdk_backproject", "ctr_dot_test", "ctr_solver_create",
+    "ctr_objective", "ctr_tv_norm", "ctr_l2_norm", "ctr_fdk", "ctr_fdk_projector_frame", "ctr_fdk_backproject",
+    "ctr_dot_test", "ctr_solver_create",
     "ctr_solver_destroy", "ctr_solver_set_sinogram", "ctr_solver_set_volume", "ctr_solver_iterate",
     "ctr_solver_get_volume", "ctr_solver_iteration_count", "ctr_solver_save", "ctr_solver_load",
     "ctr_last_error_string", "ctr_convert", "ctr_phantom_voxelize", "ctr_set_default_geometry",
@@ -56,7 +57,7 @@ EXPORTED = [
     "ctr_batch_get_volume", "ctr_geometry_set_shapes", "ctr_geometry_get_shapes", "ctr_geometry_autotune",
     "ctr_solver_objectives", "ctr_geometry_create_slab", "ctr_geometry_slab", "ctr_forward_partial",
     "ctr_combine_partials", "ctr_sart_update", "ctr_sart_pass_slabs", "ctr_volume_tiling", "ctr_volume_tiled_count",
-    "ctr_set_default_devices", "ctr_solver_set_slabs",
+    "ctr_set_default_devices", "ctr_solver_set_slabs", "ctr_solver_get_volume_f32", "ctr_batch_get_volume_f32",
 ]
 
 
@@ -83,7 +84,7 @@ class GeometryDesc(C.Structure):
 class SolverParams(C.Structure):
     _fields_ = [
         ("beta", C.c_float), ("lambda_tv", C.c_float), ("fgp_iters", C.c_int), ("fista", C.c_int),
-        ("objective", C.c_int), ("use_graph", C.c_int), ("sart_flags", C.c_uint),
+        ("objective", C.c_int), ("use_graph", C.c_int), ("sart_flags", C.c_uint), ("refine", C.c_int),
     ]
 
 
@@ -117,6 +118,7 @@ def load_library(path: str = LIB_PATH):
         "ctr_l2_norm": ([vp, vp, C.c_int64, C.POINTER(d), vp], i),
         "ctr_fdk": ([G, vp, vp, vp], i),
         "ctr_fdk_backproject": ([G, vp, i, i, vp, vp], i),
+        "ctr_fdk_projector_frame": ([G, vp, vp, vp], i),
         "ctr_dot_test": ([G, vp, vp, i, i, C.POINTER(d), C.POINTER(d), vp], i),
         "ctr_solver_create": ([G, i, C.POINTER(SolverParams), C.POINTER(C.c_void_p)], i),
         "ctr_solver_destroy": ([vp], i),
@@ -165,6 +167,8 @@ def load_library(path: str = LIB_PATH):
         "ctr_volume_tiled_count": ([G, C.POINTER(C.c_int64)], i),
         "ctr_set_default_devices": ([i], i),
         "ctr_solver_set_slabs": ([vp, i], i),
+        "ctr_solver_get_volume_f32": ([vp, vp, vp], i),
+        "ctr_batch_get_volume_f32": ([vp, i, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -214,6 +218,8 @@ def dtype_code(t) -> int:
         return BF16
     if dt == torch.float16:
         return F16
+    if dt == torch.float64:
+        return F64
     raise TypeError(f"unsupported dtype {dt}")
 
 
@@ -382,7 +388,13 @@ class Geometry:
         return tv.value
 
     def fdk(self, sino, vol, stream=None):
+        """vol += FDK in the reference's frame (x and y exchanged against ``forward``)."""
         check(self.lib.ctr_fdk(self.h, _ptr(sino), _ptr(vol), _stream(stream)))
+        return vol
+
+    def fdk_projector_frame(self, sino, vol, stream=None):
+        """vol += FDK in the projectors' frame (``ctr_fdk_projector_frame``)."""
+        check(self.lib.ctr_fdk_projector_frame(self.h, _ptr(sino), _ptr(vol), _stream(stream)))
         return vol
 
     def fdk_backproject(self, filtered, vol, view_begin=0, view_count=None, stream=None):
@@ -445,14 +457,20 @@ class Solver:
     2/Lip_con = 2/32 = 0.0625 (V63/main_recon.cu:58,161), and its FGP lambda is
     beta * lambda_tv.  The default 0.8 suits plain SART (``fista=False``); under
     FISTA it makes the iteration diverge after a few passes on a 256^3 /
-    360-view scan, so pass the reference's step there."""
+    360-view scan, so pass the reference's step there.
+
+    ``refine=True`` (with a BF16/F16 ``vol_dtype``): mixed-precision iterative
+    refinement -- FP32 FISTA state, 16-bit copies for the projectors, each
+    SART pass accumulated into a 16-bit correction against the FP32 residual.
+    ``vol_dtype=F64``: the FP64 reference solver (FP64 volumes)."""
 
     def __init__(self, geom: Geometry, vol_dtype=F32, beta=0.8, lambda_tv=0.0, fgp_iters=20, fista=True,
-                 objective=True, use_graph=True, sart_flags=0):
+                 objective=True, use_graph=True, sart_flags=0, refine=False):
         self.geom = geom
         self.lib = geom.lib
+        self.vol_dtype = vol_dtype
         self.params = SolverParams(beta, lambda_tv, fgp_iters, int(fista), int(objective), int(use_graph),
-                                   sart_flags)
+                                   sart_flags, int(refine))
         h = C.c_void_p()
         check(self.lib.ctr_solver_create(geom.h, vol_dtype, C.byref(self.params), C.byref(h)))
         self.h = h
@@ -500,6 +518,11 @@ class Solver:
         check(self.lib.ctr_solver_get_volume(self.h, _ptr(out), _stream(stream)))
         return out
 
+    def get_volume_f32(self, out, stream=None):
+        """The estimate as FP32: a refinement solver's FP32 x_k, otherwise the stored one converted."""
+        check(self.lib.ctr_solver_get_volume_f32(self.h, _ptr(out), _stream(stream)))
+        return out
+
     @property
     def iteration(self):
         k = C.c_int()
@@ -517,10 +540,11 @@ class Batch:
     """Many scans iterated together, one CUDA graph launch per iteration (``ctr_batch``)."""
 
     def __init__(self, geoms, vol_dtype=F32, beta=0.8, lambda_tv=0.0, fgp_iters=20, fista=True, objective=True,
-                 sart_flags=0):
+                 sart_flags=0, refine=False):
         self.geoms = list(geoms)
         self.lib = load_library()
-        self.params = SolverParams(beta, lambda_tv, fgp_iters, int(fista), int(objective), 1, sart_flags)
+        self.params = SolverParams(beta, lambda_tv, fgp_iters, int(fista), int(objective), 1, sart_flags,
+                                   int(refine))
         arr = (C.c_void_p * len(self.geoms))(*[g.h.value for g in self.geoms])
         h = C.c_void_p()
         check(self.lib.ctr_batch_create(arr, len(self.geoms), vol_dtype, C.byref(self.params), C.byref(h)))
@@ -552,6 +576,10 @@ class Batch:
 
     def get_volume(self, scan, out, stream=None):
         check(self.lib.ctr_batch_get_volume(self.h, scan, _ptr(out), _stream(stream)))
+        return out
+
+    def get_volume_f32(self, scan, out, stream=None):
+        check(self.lib.ctr_batch_get_volume_f32(self.h, scan, _ptr(out), _stream(stream)))
         return out
 
 

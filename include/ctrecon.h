@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CTRECON_ABI_VERSION 2
+#define CTRECON_ABI_VERSION 3
 
 typedef enum ctr_status {
     CTR_OK = 0,
@@ -47,8 +47,9 @@ typedef enum ctr_status {
 } ctr_status;
 
 /* storage type of a volume or sinogram buffer; arithmetic is always FP32
- * (FP64 for the norm reductions) */
-typedef enum ctr_dtype { CTR_F32 = 0, CTR_BF16 = 1, CTR_F16 = 2 } ctr_dtype;
+ * (FP64 for the norm reductions).  CTR_F64 is accepted only as the volume
+ * type of ctr_solver_create: the FP64 reference solver. */
+typedef enum ctr_dtype { CTR_F32 = 0, CTR_BF16 = 1, CTR_F16 = 2, CTR_F64 = 3 } ctr_dtype;
 
 /* Scan geometry: the reference's compile-time constants (V63/main_recon.cu:54-111)
  * as a run-time description.  Circular orbit; source at (dso, offset, 0) and
@@ -194,8 +195,11 @@ ctr_status ctr_sart_views(const ctr_geometry* geom, void* vol, ctr_dtype vol_dty
  * on every call).  The ray records live in a fixed 8 MiB device array inside
  * the library, so the detector may have at most 1,048,576 pixels (larger ones
  * are rejected with CTR_ERR_INVALID_ARGUMENT).  The geometry's device must be
- * current.  The first call on a device looks the array up (no allocation);
- * make that first call before any stream capture.  All calls share the
+ * current.  The first call on a device looks the array up (no allocation),
+ * and so does the first call in a new context of that device (after
+ * cudaDeviceReset, or with another context current); make those calls before
+ * any stream capture.  CTR_SART_TILED is refused (its tiled copy would be a
+ * workspace); the other flags act as in ctr_sart_views.  All calls share the
  * array: calls that overlap on the GPU (other streams, other threads) race. */
 ctr_status ctr_sart_views_noalloc(const ctr_geometry* geom, void* vol, ctr_dtype vol_dtype, const void* sino,
                                   ctr_dtype sino_dtype, float beta, unsigned flags, uint32_t seed,
@@ -316,8 +320,20 @@ ctr_status ctr_l2_norm(const float* a, const float* b, int64_t n, double* out, v
  * bilinear backprojection in the +theta frame, accumulated into vol (FP32).
  * Replaces Reconstruction_FDK (V63/host_FDK.cpp:4-57; kernels
  * V63/FDK/kernel_FDK.cu:1-62; ramp V63/FDK/FFT_1d_GPU.h:241-287).
- * Workspace: one FP32 sinogram copy, allocated per call. */
+ * Frame: the reference's FDK rotates its voxels by +theta
+ * (V63/FDK/kernel_FDK.cu:33-34, V63/host_FDK.cpp:37) where the projectors use
+ * -theta, so its volume is the projector frame's volume with x and y
+ * exchanged: vol[k][j][i] here is voxel (x = j, y = i) of ctr_forward's volume.
+ * This call keeps the reference's frame (its output bit for bit);
+ * ctr_fdk_projector_frame returns the projector's frame, e.g. to start the
+ * iterative solver from FDK.  Workspace: two FP32 sinogram copies, allocated
+ * on first use and kept with the geometry. */
 ctr_status ctr_fdk(const ctr_geometry* geom, const float* sino, float* vol, void* stream);
+/* ctr_fdk with the result in the projectors' frame: vol (projector frame) +=
+ * FDK with x and y exchanged, done in place (vol is exchanged, FDK
+ * accumulates, vol is exchanged back).  Needs nx == ny, vx == vy, offset 0
+ * and m_offset 0, where the exchange maps the volume onto itself. */
+ctr_status ctr_fdk_projector_frame(const ctr_geometry* geom, const float* sino, float* vol, void* stream);
 /* The backprojection stage of FDK alone: vol += the bilinear voxel-driven
  * backprojection of the already weighted and filtered views
  * [view_begin, view_begin+view_count) (filtered[w] is view view_begin+w,
@@ -342,7 +358,33 @@ ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, const float* y
 /* SART + FISTA + FGP-TV outer loop of V63/main_recon.cu:286-484 (FISTA == 1)
  * on device buffers.  One iteration: x = SART(y); x = FGP(x, beta*lambda_tv);
  * t_k = (1+sqrt(1+4 t^2))/2; y = x + (t-1)/t_k (x - x_prev); x_prev = x; and,
- * when requested, the objective [TV, fidelity, fidelity + 2 lambda_tv TV]. */
+ * when requested, the objective [TV, fidelity, fidelity + 2 lambda_tv TV].
+ *
+ * refine = 1, mixed-precision iterative refinement (vol_dtype BF16 or F16;
+ * allowed with F32): the FISTA state x_k, x_(k-1) stays in FP32 and is
+ * touched once per iteration.  The projectors read a vol_dtype copy of x_k
+ * and accumulate the SART pass into a vol_dtype correction volume d that
+ * starts at zero: per view j, c = (b_j - A_j y_k - A_j d)/len, where
+ * A_j y_k = (1+g) A_j x_k - g A_j x_(k-1) (g the FISTA factor (t-1)/t_k),
+ * A_j x_k is summed in the same traversal as A_j d, and A_j x_(k-1) is kept
+ * from the previous pass in an FP32 sinogram.  The residual b - A y is thus
+ * formed in FP32 against the estimate itself, and no per-view update is
+ * rounded against the (large) stored estimate, only against d (the
+ * iteration's change).  After the pass x_(k+1) = FGP(y_k + d) in FP32.  In
+ * exact arithmetic this is the same iteration as refine = 0.  The fidelity of
+ * the objective is that of the vol_dtype copy of x_k the pass projects, the TV
+ * that of the FP32 x_k.  Workspace: two FP32 volumes and one FP32 sinogram.
+ * Not with ctr_solver_set_slabs.
+ *
+ * vol_dtype CTR_F64: the FP64 reference solver.  The same iteration with every
+ * step in FP64 on the device: a Siddon traversal per ray with FP64 alphas,
+ * the SART update summing the geometric chord of every (voxel, ray) pair
+ * (gather form), FGP-TV, FISTA (t in FP64) and the objective.  It states the
+ * error of the FP32 and mixed-precision solvers at full size.  Cone beam
+ * only (not CTR_GEOM_FAN_SLICES, CTR_GEOM_PARALLEL or CTR_GEOM_TBCT); the
+ * sinogram may be any storage type (widened); set_volume / get_volume take
+ * FP64 volumes; sart_flags, refine and use_graph are ignored, and
+ * ctr_solver_set_slabs, ctr_solver_save/load and ctr_batch_create refuse it. */
 typedef struct ctr_solver_params {
     float beta;            /* SART relaxation, the reference's 2/Lip_con               */
     float lambda_tv;       /* lambda_TV; the FGP weight is beta*lambda_tv (main:162)     */
@@ -351,6 +393,7 @@ typedef struct ctr_solver_params {
     int   objective;       /* 1: evaluate the objective every iteration                  */
     int   use_graph;       /* 1: capture one iteration as a CUDA graph and replay it     */
     unsigned sart_flags;   /* CTR_SART_*                                                 */
+    int   refine;          /* 1: mixed-precision iterative refinement (above)            */
 } ctr_solver_params;
 
 typedef struct ctr_solver ctr_solver;
@@ -368,6 +411,10 @@ ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void* stream);
 ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* objective_out, void* stream);
 /* Copy the current estimate x_k (vol_dtype) to dst (device or host). */
 ctr_status ctr_solver_get_volume(ctr_solver* s, void* dst, void* stream);
+/* The current estimate as FP32 (device or host): the FP32 x_k of a
+ * refinement solver, the stored x_k widened otherwise, the FP64 x_k rounded
+ * for the FP64 solver.  Synchronises. */
+ctr_status ctr_solver_get_volume_f32(ctr_solver* s, float* dst, void* stream);
 ctr_status ctr_solver_iteration_count(const ctr_solver* s, int* k);
 
 /* The SART pass of the reference's n_slabs-device build (its z-slab sequence,
@@ -414,6 +461,8 @@ ctr_status ctr_batch_reset(ctr_batch* b, void* stream);
  * [scan][iteration][TV, fidelity, objective].  Synchronises. */
 ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* objective_out, void* stream);
 ctr_status ctr_batch_get_volume(ctr_batch* b, int scan, void* dst, void* stream);
+/* ctr_solver_get_volume_f32 of one scan. */
+ctr_status ctr_batch_get_volume_f32(ctr_batch* b, int scan, float* dst, void* stream);
 
 /* ------------------------------------------------------------- utilities */
 

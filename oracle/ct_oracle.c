@@ -1214,31 +1214,70 @@ static void og_rot(const double* e, double Rm[9])
     Rm[6] = st * ss;                Rm[7] = st * cs;                 Rm[8] = ct;
 }
 
+/* Each voxel centre adds the attenuation of every ellipsoid that contains it,
+ * in parameter order.  Ellipsoids whose axis-aligned bounding box (half
+ * extent sqrt(sum_b (R[a][b]*axis_b)^2) along world axis a, widened by a
+ * voxel) misses the voxel's slice, row or centre are skipped: they cannot
+ * contain it, so the sums are those of testing every ellipsoid. */
 void og_phantom_voxelize(const og_geom* g, const double* par, int n, float* vol)
 {
     const int M = g->d.nx, N = g->d.ny, Z = g->d.nz;
     og_geom64 h;
     og_geom_to64(g, &h);
-#pragma omp parallel for collapse(2) schedule(static)
-    for (int k = 0; k < Z; ++k)
-        for (int j = 0; j < N; ++j)
-            for (int i = 0; i < M; ++i) {
-                const double p[3] = {h.bx + h.vx * (i + 0.5), h.by + h.vy * (j + 0.5), h.bz + h.vz * (k + 0.5)};
-                double acc = 0.0;
-                for (int e = 0; e < n; ++e) {
-                    const double* q = par + 10 * e;
-                    double Rm[9];
-                    og_rot(q + 6, Rm);
-                    const double d[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
-                    double r2 = 0.0;
-                    for (int a = 0; a < 3; ++a) {
-                        const double l = (Rm[0 + a] * d[0] + Rm[3 + a] * d[1] + Rm[6 + a] * d[2]) / q[3 + a];
-                        r2 += l * l;
-                    }
-                    if (r2 <= 1.0) acc += q[9];
-                }
-                vol[(long long)M * N * k + (long long)M * j + i] += (float)acc;
+    double* Rm = (double*)malloc(sizeof(double) * 9 * (n > 0 ? n : 1));
+    double* ext = (double*)malloc(sizeof(double) * 3 * (n > 0 ? n : 1));
+    const double pad[3] = {h.vx, h.vy, h.vz};
+    for (int e = 0; e < n; ++e) {
+        og_rot(par + 10 * e + 6, Rm + 9 * e);
+        for (int a = 0; a < 3; ++a) {
+            double s2 = 0.0;
+            for (int b = 0; b < 3; ++b) {
+                const double t = Rm[9 * e + 3 * a + b] * par[10 * e + 3 + b];
+                s2 += t * t;
             }
+            ext[3 * e + a] = sqrt(s2) * (1.0 + 1e-9) + pad[a];
+        }
+    }
+#pragma omp parallel
+    {
+        int* in_k = (int*)malloc(sizeof(int) * (n > 0 ? n : 1));
+        int* in_kj = (int*)malloc(sizeof(int) * (n > 0 ? n : 1));
+#pragma omp for schedule(dynamic, 1)
+        for (int k = 0; k < Z; ++k) {
+            const double pz = h.bz + h.vz * (k + 0.5);
+            int nk = 0;
+            for (int e = 0; e < n; ++e)
+                if (fabs(pz - par[10 * e + 2]) <= ext[3 * e + 2]) in_k[nk++] = e;
+            for (int j = 0; j < N; ++j) {
+                const double py = h.by + h.vy * (j + 0.5);
+                int nkj = 0;
+                for (int t = 0; t < nk; ++t)
+                    if (fabs(py - par[10 * in_k[t] + 1]) <= ext[3 * in_k[t] + 1]) in_kj[nkj++] = in_k[t];
+                for (int i = 0; i < M; ++i) {
+                    const double p[3] = {h.bx + h.vx * (i + 0.5), py, pz};
+                    double acc = 0.0;
+                    for (int t = 0; t < nkj; ++t) {
+                        const int e = in_kj[t];
+                        const double* q = par + 10 * e;
+                        if (fabs(p[0] - q[0]) > ext[3 * e]) continue;
+                        const double* R = Rm + 9 * e;
+                        const double d[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
+                        double r2 = 0.0;
+                        for (int a = 0; a < 3; ++a) {
+                            const double l = (R[0 + a] * d[0] + R[3 + a] * d[1] + R[6 + a] * d[2]) / q[3 + a];
+                            r2 += l * l;
+                        }
+                        if (r2 <= 1.0) acc += q[9];
+                    }
+                    vol[(long long)M * N * k + (long long)M * j + i] += (float)acc;
+                }
+            }
+        }
+        free(in_k);
+        free(in_kj);
+    }
+    free(Rm);
+    free(ext);
 }
 
 void og_phantom_project(const og_geom* g, const double* par, int n, double s, double c, float* out)

@@ -1,14 +1,17 @@
-"""Mixed precision (BF16/FP16 storage, FP32 arithmetic) against the FP64
-oracle: SART + FISTA + FGP-TV iterations on a seeded 10-ellipsoid phantom
-whose sinogram is the FP64 analytic line integrals plus 0.5 % noise.  RMSE is
-stated relative to the phantom's maximum attenuation.
+"""Mixed precision against the FP64 oracle: SART + FISTA + FGP-TV iterations on
+a seeded 10-ellipsoid phantom whose sinogram is the FP64 analytic line
+integrals plus 0.5 % noise.  RMSE and maximum error are stated relative to the
+phantom's maximum attenuation; the bar is an RMSE of at most 1e-3.
 
-Two relaxations: 0.8 (5 iterations) and the reference's FISTA step
-2/Lip_con = 0.0625 (V63/main_recon.cu:58,161; 5 and 20 iterations).  With
-the small step each view's update is small against the stored value, so
-rounding to FP16/BF16 storage loses more of it and the error grows with the
-iteration count; the limits record that.  (0.8 under FISTA diverges after a
-few iterations, the FP64 oracle included, so it is not run longer.)"""
+At the reference's FISTA step 2/Lip_con = 0.0625 (V63/main_recon.cu:58,161)
+each view's update is small against the stored voxel value, so a volume
+stored in FP16/BF16 loses part of every update to rounding and the error
+grows with the iteration count.  The refinement solver (``refine=True``)
+keeps the FISTA state in FP32 and rounds each view's update only against the
+pass's correction volume, which starts at zero; it meets the bar at 20
+iterations with FP16 copies, and with BF16 copies when the correction's
+updates are rounded stochastically.  The plain 16-bit storage form is kept
+for short runs (5 iterations) and is shown to drift at 20."""
 import numpy as np
 import pytest
 
@@ -18,14 +21,14 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 LAM_TV, FGP = 2e-4, 20
+BAR = 1e-3
 
 # (relaxation, iterations, storage mode, RMSE limit relative to max attenuation)
-CASES = [(0.8, 5, "f32", 1e-4), (0.8, 5, "f16", 1e-3), (0.8, 5, "f16_sr", 1e-3), (0.8, 5, "bf16_sr", 4e-3),
-         (0.8, 5, "bf16", 8e-3),
-         (0.0625, 5, "f32", 1e-4), (0.0625, 5, "f16", 1e-3), (0.0625, 5, "f16_sr", 1e-3),
-         (0.0625, 5, "bf16_sr", 8e-3), (0.0625, 5, "bf16", 1.6e-2),
-         (0.0625, 20, "f32", 2e-4), (0.0625, 20, "f16", 6e-3), (0.0625, 20, "f16_sr", 4e-3),
-         (0.0625, 20, "bf16_sr", 2.5e-2), (0.0625, 20, "bf16", 6e-2)]
+CASES = [(0.0625, 20, "f32", 2e-4), (0.0625, 20, "f16_refine", BAR), (0.0625, 20, "f16_sr_refine", BAR),
+         (0.0625, 20, "bf16_sr_refine", BAR),
+         (0.0625, 5, "f32", 1e-4), (0.0625, 5, "f16_refine", BAR), (0.0625, 5, "f16", BAR),
+         (0.8, 5, "f32", 1e-4), (0.8, 5, "f16", BAR), (0.8, 5, "f16_sr", BAR), (0.8, 5, "f16_refine", BAR),
+         (0.8, 5, "bf16_refine", BAR)]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -50,8 +53,10 @@ def fp64_reference(problem, beta, iters):
     `iters` iterations; each relaxation's run continues from its last state."""
     o, _, b, cache = problem
     if beta not in cache:
-        cache[beta] = dict(n=0, y=np.zeros(o.vol_shape), xprev=np.zeros(o.vol_shape), t=1.0)
+        cache[beta] = dict(n=0, y=np.zeros(o.vol_shape), xprev=np.zeros(o.vol_shape), t=1.0, hist={})
     st = cache[beta]
+    if iters in st["hist"]:
+        return st["hist"][iters]
     assert st["n"] <= iters, "iteration counts of one relaxation are requested in increasing order"
     while st["n"] < iters:
         x = o.sart_pass_f64(st["y"], b.astype(np.float64), beta)
@@ -61,36 +66,55 @@ def fp64_reference(problem, beta, iters):
         st["xprev"] = x
         st["t"] = tk
         st["n"] += 1
+        st["hist"][st["n"]] = x
     return st["xprev"]
 
 
-def run(b, vdt, beta, iters, flags=0):
+def run(b, mode, beta, iters):
+    """The solver's FP32 estimate after `iters` iterations.  With a 16-bit
+    volume the sinogram is stored in FP16, as the benchmark stores it (BF16's
+    8-bit mantissa would perturb the measured data by itself: 7e-4 RMSE in
+    the FP64 oracle's reconstruction).  BF16 needs stochastic rounding of the
+    correction volume's updates."""
     import gpu_b200
+    vdt = {"f32": gpu_b200.F32, "f16": gpu_b200.F16, "bf16": gpu_b200.BF16}[mode.split("_")[0]]
+    sdt = torch.float32 if vdt == gpu_b200.F32 else torch.float16
+    flags = gpu_b200.SART_STOCHASTIC_ROUND if "_sr" in mode else 0
     g = gpu_b200.Geometry(ctr_desc(MIXED))
-    tdt = {gpu_b200.F32: torch.float32, gpu_b200.F16: torch.float16, gpu_b200.BF16: torch.bfloat16}[vdt]
     s = gpu_b200.Solver(g, vdt, beta=beta, lambda_tv=LAM_TV, fgp_iters=FGP, fista=True, objective=False,
-                        sart_flags=flags)
-    sino = torch.from_numpy(b).cuda().to(tdt)
-    s.set_sinogram(sino)
+                        sart_flags=flags, refine=mode.endswith("_refine"))
+    s.set_sinogram(torch.from_numpy(b).cuda().to(sdt))
     s.set_volume(None)
     s.iterate(iters)
-    out = torch.zeros(g.vol_shape, device="cuda", dtype=tdt)
-    s.get_volume(out)
-    return out.float().cpu().numpy().astype(np.float64)
+    out = torch.zeros(g.vol_shape, device="cuda")
+    s.get_volume_f32(out)
+    return out.cpu().numpy().astype(np.float64)
+
+
+def errors(got, ref, mu_max):
+    return float(np.sqrt(np.mean((got - ref) ** 2))) / mu_max, float(np.abs(got - ref).max()) / mu_max
 
 
 @pytest.mark.parametrize("beta,iters,mode,limit", CASES)
 def test_rmse_against_fp64_oracle(problem, beta, iters, mode, limit):
-    import gpu_b200
     _, truth, b, _ = problem
     ref = fp64_reference(problem, beta, iters)
-    vdt = {"f32": gpu_b200.F32, "f16": gpu_b200.F16, "f16_sr": gpu_b200.F16, "bf16": gpu_b200.BF16,
-           "bf16_sr": gpu_b200.BF16}[mode]
-    flags = gpu_b200.SART_STOCHASTIC_ROUND if mode.endswith("_sr") else 0
-    got = run(b, vdt, beta, iters, flags)
-    mu_max = float(truth.max())
-    rmse = float(np.sqrt(np.mean((got - ref) ** 2))) / mu_max
-    maxerr = float(np.abs(got - ref).max()) / mu_max
+    got = run(b, mode, beta, iters)
+    rmse, maxerr = errors(got, ref, float(truth.max()))
     print(f"beta {beta}, {iters} iterations, {mode}: RMSE {rmse:.3e}, max abs error {maxerr:.3e} "
-          f"(relative to max attenuation {mu_max:.4f})")
+          f"(relative to max attenuation {truth.max():.4f})")
     assert rmse <= limit
+
+
+def test_plain_16bit_storage_drifts_refinement_does_not(problem):
+    """At the reference's step and 20 iterations the plain FP16 store loses
+    enough of each view's update to miss the bar; the refinement solver with
+    the same 16-bit copies stays within it, at a small fraction of the error."""
+    _, truth, b, _ = problem
+    ref = fp64_reference(problem, 0.0625, 20)
+    mu = float(truth.max())
+    plain, _ = errors(run(b, "f16", 0.0625, 20), ref, mu)
+    refined, _ = errors(run(b, "f16_refine", 0.0625, 20), ref, mu)
+    print(f"20 iterations at 0.0625: plain FP16 storage RMSE {plain:.3e}, refinement {refined:.3e}")
+    assert refined <= BAR < plain
+    assert refined < 0.25 * plain
