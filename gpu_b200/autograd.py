@@ -83,17 +83,25 @@ class _ChunkedFidelity(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, gtotal):
+        """d/dx = A^T (A x - b) and d/db = -(A x - b), each scaled by the
+        incoming gradient; A x is recomputed chunk by chunk."""
         vol, b = ctx.saved_tensors
         g, chunk = ctx.geom, ctx.chunk
-        grad = torch.zeros(g.vol_shape, device=vol.device, dtype=torch.float32)
+        want_x, want_b = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        grad = torch.zeros(g.vol_shape, device=vol.device, dtype=torch.float32) if want_x else None
+        grad_b = torch.empty_like(b, dtype=torch.float32) if want_b else None
         buf = torch.empty((min(chunk, g.n_views),) + g.view_shape, device=vol.device, dtype=torch.float32)
         for v0 in range(0, g.n_views, chunk):
             n = min(chunk, g.n_views - v0)
             ax = buf[:n]
             g.forward(vol, ax, v0, n)                  # recompute this chunk
             r = (ax - b[v0:v0 + n]).contiguous()
-            g.backproject(r, grad, v0, n, flags=ctrecon.BP_ACCUMULATE)
-        return grad * gtotal.float(), None, None, None
+            if want_x:
+                g.backproject(r, grad, v0, n, flags=ctrecon.BP_ACCUMULATE)
+            if want_b:
+                grad_b[v0:v0 + n] = -r
+        gs = gtotal.float()
+        return (grad * gs if want_x else None), (grad_b.to(b.dtype) * gs if want_b else None), None, None
 
 
 def data_fidelity_loss(vol, b, geom, chunk=64):

@@ -162,20 +162,22 @@ k_backproject(const DevGeom g, VT* __restrict__ vol, const REC* __restrict__ ray
                     ub = uu;
                 }
             }
-            for (int uu = ua; uu <= ub; ++uu) {
-                const float4 ct = __ldg(colt + uu);
-                const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
-                const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
-                const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
-                const float bb = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
-                if (!(bb > a)) continue;
+            // per voxel, row by row (rows ascending), the columns of the run
+            // ascending: the walk's and the oracle's order
 #pragma unroll
-                for (int kk = 0; kk < BP_K; ++kk) {
-                    const int kc = min(k0 + kk, g.Z - 1);
-                    const float zl = T.PZ[kc + 1], zh = T.PZ[kc + 2];
-                    for (int vv = vlo[kk]; vv <= vhi[kk]; ++vv) {
-                        const float2 rt = T.RT[vv];
-                        const float az0 = fm(fs(zl, rt.x), rt.y), az1 = fm(fs(zh, rt.x), rt.y);
+            for (int kk = 0; kk < BP_K; ++kk) {
+                const int kc = min(k0 + kk, g.Z - 1);
+                const float zl = T.PZ[kc + 1], zh = T.PZ[kc + 2];
+                for (int vv = vlo[kk]; vv <= vhi[kk]; ++vv) {
+                    const float2 rt = T.RT[vv];
+                    const float az0 = fm(fs(zl, rt.x), rt.y), az1 = fm(fs(zh, rt.x), rt.y);
+                    for (int uu = ua; uu <= ub; ++uu) {
+                        const float4 ct = __ldg(colt + uu);
+                        const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+                        const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+                        const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
+                        const float bb = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+                        if (!(bb > a)) continue;
                         const float lo = fmaxf(a, fminf(az0, az1));
                         const float hi = fminf(bb, fmaxf(az0, az1));
                         const REC rec = rays[(long long)vv * R + uu];
@@ -319,6 +321,7 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         }
     }
     if (ua > ub) return;
+    const int nrun = ub - ua + 1;   // every column of the run crosses the voxel column (bb > a)
     float ra[WALK_RUN], rb[WALK_RUN];
 #pragma unroll
     for (int q = 0; q < WALK_RUN; ++q) {
@@ -373,30 +376,33 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
                 sl = fa(sl, temp);
             }
         };
-        auto pairs = [&](int uu, float a, float bb) {
-            if (!(bb > a)) return;
-            int vv = vlo;
-            if (UNR == 2) {   // two rows' loads in flight, then their pairs in row order
-                for (; vv < vhi; vv += 2) {
-                    const float2 z0c = __ldg(zrow + vv), z1c = __ldg(zrow + vv + 1);
-                    const float2 r0 = __ldg(rays + (long long)vv * R + uu);
-                    const float2 r1 = __ldg(rays + (long long)(vv + 1) * R + uu);
-                    pair(a, bb, z0c, r0);
-                    pair(a, bb, z1c, r1);
-                }
-            }
-            for (; vv <= vhi; ++vv) pair(a, bb, __ldg(zrow + vv), __ldg(rays + (long long)vv * R + uu));
-        };
-        auto all_pairs = [&]() {
+        // the pairs of one detector row: its z-cell interval is loaded once and
+        // met with every column of the run (columns ascending)
+        auto row_pairs = [&](int vv, float2 zc) {
+            const float2* __restrict__ rr = rays + (long long)vv * R + ua;
 #pragma unroll
             for (int q = 0; q < WALK_RUN; ++q)
-                if (ua + q <= ub) pairs(ua + q, ra[q], rb[q]);
-            for (int uu = ua + WALK_RUN; uu <= ub; ++uu) {
-                const float4 ct = __ldg(colt + uu);
+                if (q < nrun) pair(ra[q], rb[q], zc, __ldg(rr + q));
+            for (int q = WALK_RUN; q < nrun; ++q) {   // runs longer than the registers hold
+                const float4 ct = __ldg(colt + ua + q);
                 const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
                 const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
-                pairs(uu, fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)));
+                pair(fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)), zc,
+                     __ldg(rr + q));
             }
+        };
+        // every pair of the voxel, row by row (rows ascending), the order the
+        // oracle's gather sums them
+        auto all_pairs = [&]() {
+            int vv = vlo;
+            if (UNR == 2) {   // two rows' z-cell loads in flight, then their pairs in row order
+                for (; vv < vhi; vv += 2) {
+                    const float2 z0c = __ldg(zrow + vv), z1c = __ldg(zrow + vv + 1);
+                    row_pairs(vv, z0c);
+                    row_pairs(vv + 1, z1c);
+                }
+            }
+            for (; vv <= vhi; ++vv) row_pairs(vv, __ldg(zrow + vv));
         };
         // candidate rows of the band [row0, row0 + nvr) seen from height zs
         // through the cell between planes z0 and z1

@@ -1382,7 +1382,7 @@ static float og_ray_d12(const og_geom* g, float s, float c, int u, int v)
  * there, a source's rays summed apart and the sources added in ascending
  * order, pair threshold vx*1e-6f, update where the summed length exceeds
  * vx*1e-3 in double, :772) with the projector's own chords; a source's pairs
- * in the engine's order (detector column, then row). */
+ * in the engine's order (detector row, then column). */
 static void og_backproject_gather_tbct(const og_geom* g, float* vol, const float* corr, float beta, float s, float c)
 {
     const int M = g->d.nx, N = g->d.ny, Z = g->d.nz, R = g->d.nu, ZP = g->d.nv, K = g->d.n_sources;
@@ -1448,17 +1448,22 @@ static void og_backproject_gather_tbct(const og_geom* g, float* vol, const float
                     if ((v0 < 0 && v1 < 0) || (v0 > ZP - 1 && v1 > ZP - 1)) continue;
                     v0 = v0 - 1 < 0 ? 0 : v0 - 1;
                     v1 = v1 + 1 > ZP - 1 ? ZP - 1 : v1 + 1;
-                    float sw = 0.0f, sl = 0.0f;
+                    /* the band's pairs row by row (rows ascending), columns ascending within a row */
+                    float ca[u1 - u0 + 1], cb[u1 - u0 + 1];
                     for (int u = u0; u <= u1; ++u) {
                         const float* ct = &col[4 * u];
                         const float ax0 = (xlo - ct[0]) * ct[1], ax1 = (xhi - ct[0]) * ct[1];
                         const float ay0 = (ylo - ct[2]) * ct[3], ay1 = (yhi - ct[2]) * ct[3];
-                        const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
-                        const float b = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
-                        if (!(b > a)) continue;
-                        for (int vr = v0; vr <= v1; ++vr) {
-                            const int v = src * ZP + vr;
-                            const float az0 = (zlo - row[2 * v]) * row[2 * v + 1], az1 = (zhi - row[2 * v]) * row[2 * v + 1];
+                        ca[u - u0] = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
+                        cb[u - u0] = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+                    }
+                    float sw = 0.0f, sl = 0.0f;
+                    for (int vr = v0; vr <= v1; ++vr) {
+                        const int v = src * ZP + vr;
+                        const float az0 = (zlo - row[2 * v]) * row[2 * v + 1], az1 = (zhi - row[2 * v]) * row[2 * v + 1];
+                        for (int u = u0; u <= u1; ++u) {
+                            const float a = ca[u - u0], b = cb[u - u0];
+                            if (!(b > a)) continue;
                             const float lo = fmaxf(a, fminf(az0, az1)), hi = fminf(b, fmaxf(az0, az1));
                             const float temp = d12[v * R + u] * (hi - lo);
                             if (temp > thr) {
@@ -1542,16 +1547,21 @@ void og_backproject_gather(const og_geom* g, float* vol, const float* corr, floa
                 const float xlo = og_plane(vx, i, g->bx), xhi = og_plane(vx, i + 1, g->bx);
                 const float ylo = og_plane(vy, j, g->by), yhi = og_plane(vy, j + 1, g->by);
                 const float zlo = og_plane(vz, k, g->bz), zhi = og_plane(vz, k + 1, g->bz);
-                float sw = 0.0f, sl = 0.0f;
+                /* the pairs row by row (rows ascending), columns ascending within a row */
+                float ca[u1 - u0 + 1], cb[u1 - u0 + 1];
                 for (int u = u0; u <= u1; ++u) {
                     const float* ct = &col[4 * u];
                     const float ax0 = (xlo - ct[0]) * ct[1], ax1 = (xhi - ct[0]) * ct[1];
                     const float ay0 = (ylo - ct[2]) * ct[3], ay1 = (yhi - ct[2]) * ct[3];
-                    const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
-                    const float b = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
-                    if (!(b > a)) continue;
-                    for (int v = v0; v <= v1; ++v) {
-                        const float az0 = (zlo - row[2 * v]) * row[2 * v + 1], az1 = (zhi - row[2 * v]) * row[2 * v + 1];
+                    ca[u - u0] = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1));
+                    cb[u - u0] = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+                }
+                float sw = 0.0f, sl = 0.0f;
+                for (int v = v0; v <= v1; ++v) {
+                    const float az0 = (zlo - row[2 * v]) * row[2 * v + 1], az1 = (zhi - row[2 * v]) * row[2 * v + 1];
+                    for (int u = u0; u <= u1; ++u) {
+                        const float a = ca[u - u0], b = cb[u - u0];
+                        if (!(b > a)) continue;
                         const float lo = fmaxf(a, fminf(az0, az1)), hi = fminf(b, fmaxf(az0, az1));
                         const float temp = d12[v * R + u] * (hi - lo);
                         if (temp > thr) {

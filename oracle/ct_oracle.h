@@ -143,7 +143,8 @@ void og_sart_pass_matched(const og_geom* g, float* vol, const float* sino, float
 void og_sart_pass_f64(const og_geom* g, double* vol, const double* sino, double beta);
 /* the engine's gather SART update: reference BP semantics (candidate
  * rectangle, FOV mask, thresholds) with every alpha evaluated the Siddon
- * projector's way, float sums in the engine's pair order.  The candidate
+ * projector's way, float sums in the engine's pair order (detector row by
+ * row, the columns of each row ascending).  The candidate
  * rows are a superset of the rows with a positive chord (the cone beam's
  * rectangle, the fan-slice / parallel beams' rows of the cell's z span, each
  * widened by a row), so they do not change the sums. */

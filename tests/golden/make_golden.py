@@ -1,8 +1,8 @@
 """Generate tests/golden/*.npz from the reference's own kernels.
 
 Runs the reference's CUDA kernel sources compiled for the CPU
-(oracle/_ref/libctref*.so, one per CT_style, built by `make -C oracle` from
-the reference checkout) on seeded inputs for the small scans of
+(oracle/_ref/libctref*.so, one per CT_style, built by
+`make -C oracle REF_ROOT=<reference checkout>`) on seeded inputs for the small scans of
 tests/scan_configs.py (cone beam, and the fan-slice and parallel geometries)
 and the tetrahedron-beam program's (libctref_tbct.so), and stores inputs
 and outputs.  The fixtures pin the C restatement in

@@ -138,3 +138,22 @@ def test_fifty_step_reconstruction(scan2):
     assert losses[-1] < 0.05 * losses[0]
     err0 = truth.norm().item()
     assert (x.detach() - truth).norm().item() < 0.6 * err0
+
+
+def test_fidelity_gradient_of_the_measured_data():
+    """d/db 0.5||Ax - b||^2 = -(Ax - b), alongside the volume's gradient."""
+    import gpu_b200
+    from gpu_b200.autograd import data_fidelity_loss
+    cfg = SMALL["cube16"]
+    g = gpu_b200.Geometry(ctr_desc(cfg))
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.rand(g.vol_shape, device="cuda", generator=gen).requires_grad_(True)
+    b = torch.rand((cfg["nviews"],) + g.view_shape, device="cuda", generator=gen).requires_grad_(True)
+    loss = data_fidelity_loss(x, b, g, chunk=5)
+    (2.0 * loss).backward()
+    ax = torch.zeros_like(b)
+    g.forward(x.detach(), ax)
+    torch.testing.assert_close(b.grad, -2.0 * (ax - b.detach()), rtol=0, atol=0)
+    ref = torch.zeros_like(x)
+    g.backproject((ax - b.detach()).contiguous(), ref)
+    torch.testing.assert_close(x.grad, 2.0 * ref, rtol=1e-6, atol=1e-6 * float(ref.abs().max()))
