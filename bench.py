@@ -65,6 +65,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mixed", choices=["f16", "bf16"], default="f16")
+    p.add_argument("--fast-sums", action="store_true",
+                   help="the mixed-precision run (and --profile-views) with fused ray sums (CTR_GEOM_FAST_SUMS)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-views", type=int, default=0,
                    help="profiling mode: set up the scan, run a SART update of this many views, print timings, exit")
@@ -472,7 +474,7 @@ def profile_views(args):
     else:
         geom = gpu_b200.Geometry(gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"],
                                                     SCAN["nv"], SCAN["du"], SCAN["dso"], SCAN["dod"],
-                                                    SCAN["n_views"]))
+                                                    SCAN["n_views"], fast_sums=args.fast_sums))
         ph = phantom_params(2024)
         n_views, beta, lam = SCAN["n_views"], BETA, LAMBDA_TV
     truth = torch.zeros(geom.vol_shape, device="cuda")
@@ -1009,6 +1011,13 @@ def main():
     desc = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
                               SCAN["dso"], SCAN["dod"], SCAN["n_views"])
     geom = gpu_b200.Geometry(desc)
+    # --fast-sums: the mixed-precision run's projections with fused ray sums
+    # (CTR_GEOM_FAST_SUMS); the FP32 run keeps the reference's sequence
+    geoms = {"f32": geom, "mixed": geom}
+    if args.fast_sums:
+        geoms["mixed"] = gpu_b200.Geometry(gpu_b200.make_desc(
+            SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"], SCAN["dso"],
+            SCAN["dod"], SCAN["n_views"], fast_sums=True))
     vshape, sshape = geom.vol_shape, (SCAN["n_views"],) + geom.view_shape
     V = SCAN["nx"] * SCAN["ny"] * SCAN["nz"]
     P = SCAN["nu"] * SCAN["nv"]
@@ -1047,8 +1056,8 @@ def main():
     # for the projectors, each pass accumulated into a 16-bit correction
     # against the FP32 residual), the form that meets the accuracy bar
     for mode, vdt, sino in (("f32", gpu_b200.F32, sino32), ("mixed", mixed_code, sino16)):
-        tuned[mode] = geom.autotune(vdt, n_views=4)      # launch shapes; results do not depend on them
-        solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
+        tuned[mode] = geoms[mode].autotune(vdt, n_views=4)   # launch shapes; results do not depend on them
+        solver = gpu_b200.Solver(geoms[mode], vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
                                  objective=True, use_graph=True, refine=(mode == "mixed"),
                                  sart_flags=gpu_b200.SART_STOCHASTIC_ROUND if vdt == gpu_b200.BF16 else 0)
         solver.set_sinogram(sino)
@@ -1141,7 +1150,7 @@ def main():
     # (each is projected inside the next step's SART traversal, the last one
     # by that read, all inside the timed region)
     mode = "mixed"
-    geom.set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
+    geoms[mode].set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
     solver, sino = runs[mode]["solver"], runs[mode]["sino"]
     h_sino = sino.cpu().pin_memory()
     h_vol = torch.empty(vshape, dtype=mixed_dt).pin_memory()
@@ -1164,15 +1173,16 @@ def main():
     # library records around each launch on this stream (32 views spread over the scan)
     kern = {}
     for mode in ("f32", "mixed"):
-        geom.set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
+        gk = geoms[mode]
+        gk.set_shapes(tuned[mode]["fp_shape"], tuned[mode]["bp_shape"])
         sino = runs[mode]["sino"]
         vol = torch.zeros(vshape, device=dev, dtype=torch.float32 if mode == "f32" else mixed_dt)
         tl = gpu_b200.SART_TILED                                      # the solver's layout
-        geom.sart_views(vol, sino, BETA, 0, 4, flags=tl)              # warm-up
+        gk.sart_views(vol, sino, BETA, 0, 4, flags=tl)                # warm-up
         fp_t = bp_t = 0.0
         nt = 32
         for j in range(nt):
-            f_ms, b_ms = geom.sart_views(vol, sino, BETA, (j * 97) % SCAN["n_views"], 1, flags=tl, timed=True)
+            f_ms, b_ms = gk.sart_views(vol, sino, BETA, (j * 97) % SCAN["n_views"], 1, flags=tl, timed=True)
             fp_t += f_ms
             bp_t += b_ms
         kern[mode] = {"fp_ms": fp_t / nt, "bp_ms": bp_t / nt}
@@ -1182,9 +1192,9 @@ def main():
     # every iteration, so the headline keeps it)
     # (side figures below: a few timed iterations each)
     side_steps = min(args.steps, 3)
-    geom.set_shapes(tuned["mixed"]["fp_shape"], tuned["mixed"]["bp_shape"])
-    noobj = gpu_b200.Solver(geom, mixed_code, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
-                            objective=False, use_graph=True, refine=True)
+    geoms["mixed"].set_shapes(tuned["mixed"]["fp_shape"], tuned["mixed"]["bp_shape"])
+    noobj = gpu_b200.Solver(geoms["mixed"], mixed_code, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS,
+                            fista=True, objective=False, use_graph=True, refine=True)
     noobj.set_sinogram(runs["mixed"]["sino"])
     noobj.set_volume(None)
     noobj.iterate(1)

@@ -40,10 +40,13 @@ def _deps_mtime():
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    """Compile every source and link the library; returns its path."""
+    """Compile every source (in parallel, one nvcc per source) and link the
+    library; returns its path."""
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(OUT_DIR, exist_ok=True)
     deps = _deps_mtime()
-    objs = []
+    objs, cmds = [], []
     for f in _sources():
         src = os.path.join(SRC, f)
         obj = os.path.join(OUT_DIR, f + ".o")
@@ -55,7 +58,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
+    workers = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
         if verbose:

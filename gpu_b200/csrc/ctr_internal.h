@@ -22,6 +22,7 @@ struct DevGeom {
     int Mt, Nt;             // 8x8 (x, y) tiles per row / column of the tiled layout
     int fast_exit;          // every alpha inside the volume >= 1e-6: the Siddon loop test is one comparison
     int entry64;            // FP64 ray-box entry/exit
+    int fast_sums;          // CTR_GEOM_FAST_SUMS: fused ray-sum accumulation in the solver's projections
     int ct_style;           // 0 cone beam, 1 multi-slice fan beam, 2 parallel beam (the reference's CT_style),
                             // 3 tetrahedron beam (CTR_GEOM_TBCT)
     int nvr;                // detector rows of one source's band (= ZP unless TBCT)

@@ -38,10 +38,13 @@ struct G64 {
     double us, a0, shift;  // degrees
 };
 
-__device__ __forceinline__ void view_sc(const G64& h, int j, double& s, double& c)
+// The projector frame's view angle -(j*us_rate + initial + shift) in radians,
+// evaluated on the host (V63/host_IterativeRecon_CBCT.c:34-41 in FP64).
+static void view_sc(const G64& h, int j, double& s, double& c)
 {
     const double t = -((j * h.us + h.a0) + h.shift) * (3.14159265358979323846 / 180.0);
-    sincos(t, &s, &c);
+    s = std::sin(t);
+    c = std::cos(t);
 }
 
 // Ray of pixel (u, v): detector pixel centre X1 and the direction X2 - X1.
@@ -128,15 +131,13 @@ __device__ double traverse64(const G64& h, const Ray64& r, const double* __restr
 // MODE 1: objective partials, one per warp of 32 rays: Sum((Ax - b)^2).
 template <int MODE>
 __global__ void __launch_bounds__(128)
-k64_forward(const G64 h, const double* __restrict__ vol, int view, const void* __restrict__ b, int b_dt,
+k64_forward(const G64 h, const double* __restrict__ vol, double s, double c, const void* __restrict__ b, int b_dt,
             double2* __restrict__ rays, double* __restrict__ partial)
 {
     const int u = blockIdx.x * 32 + (threadIdx.x & 31);
     const int v = blockIdx.y * 4 + (threadIdx.x >> 5);
     double e2 = 0.0;
     if (u < h.R && v < h.ZP) {
-        double s, c;
-        view_sc(h, view, s, c);
         const Ray64 r = ray64(h, s, c, u, v);
         double len;
         const double sum = traverse64(h, r, vol, &len);
@@ -156,27 +157,68 @@ k64_forward(const G64 h, const double* __restrict__ vol, int view, const void* _
     }
 }
 
-// SART update of one view, one thread per voxel (gather, no atomics).
+// Per detector column u of a view: the pixel centre's x and y and the
+// reciprocals of the ray's x and y extents (0 for an extent below 1e-12 of a
+// voxel: a ray parallel to those planes); per detector row v (the same for
+// every view): the pixel centre's z and 1/(z extent), 0 likewise.
+__global__ void k64_columns(const G64 h, double s, double c, double4* __restrict__ col)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= h.R) return;
+    const double pu = h.ymin + u * h.du;
+    const double x1x = h.dod * c - pu * s, x1y = h.dod * s + pu * c;
+    const double dx = (h.dso * c - h.srcy * s) - x1x, dy = (h.dso * s + h.srcy * c) - x1y;
+    col[u] = make_double4(x1x, x1y, fabs(dx) < h.vx * 1e-12 ? 0.0 : 1.0 / dx, fabs(dy) < h.vy * 1e-12 ? 0.0 : 1.0 / dy);
+}
+__global__ void k64_rows(const G64 h, double2* __restrict__ row)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= h.ZP) return;
+    const double x1z = h.zmin + v * h.dv, dz = 0.0 - x1z;
+    row[v] = make_double2(x1z, fabs(dz) < h.vz * 1e-12 ? 0.0 : 1.0 / dz);
+}
+
+// The alpha interval of a ray inside the slab [lo, hi] of one axis (x1 the
+// ray's start on that axis, inv 1/extent, 0 for a ray parallel to the slab):
+// (-inf, inf) inside, empty (returned false) outside.
+__device__ __forceinline__ bool slab64(double lo, double hi, double x1, double inv, double& a, double& b)
+{
+    if (inv == 0.0) {
+        a = -INFINITY;
+        b = INFINITY;
+        return x1 > lo && x1 < hi;
+    }
+    const double t0 = (lo - x1) * inv, t1 = (hi - x1) * inv;
+    a = fmin(t0, t1);
+    b = fmax(t0, t1);
+    return true;
+}
+
+constexpr int F64_RUN = 4;    // detector columns of a voxel column kept in registers
+constexpr int F64_ZRUN = 16;  // voxels of a column per thread
+
+// SART update of one view (gather, no atomics): a thread walks F64_ZRUN
+// voxels of one (x, y) column.  Per column: the reconstruction cylinder test
+// (the reference's float test, universal.cu:626-628), the detector columns
+// between the corner projections (rounded to the nearest pixel, a superset
+// of the pixel centres the column projects to) and their rays' xy alpha
+// intervals; per voxel: the detector rows between its corner projections
+// (the magnification's extremes over the column) and, per (row, column), the
+// geometric chord d12*(exit - entry).  f += beta*Sum(w c)/Sum(w) where
+// Sum(w) >= vx*1e-6.
 __global__ void __launch_bounds__(128)
-k64_update(const G64 h, const DevGeom g, double* __restrict__ vol, const double2* __restrict__ rays, int view,
-           double beta)
+k64_update(const G64 h, const DevGeom g, double* __restrict__ vol, const double2* __restrict__ rays, double s,
+           double c, const double4* __restrict__ col, const double2* __restrict__ row, double beta)
 {
     const int i = blockIdx.x * 32 + (threadIdx.x & 31);
     const int j = blockIdx.y * 4 + (threadIdx.x >> 5);
-    const int k = blockIdx.z;
     if (i >= h.M || j >= h.N) return;
-    // the reconstruction cylinder, with the reference's float test (universal.cu:626-628)
     const float ex = fs(fs((float)i, g.fov_h_x), g.m_off);
     const float ey = fs((float)j, g.fov_h_y);
     if (fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2) return;
-    double s, c;
-    view_sc(h, view, s, c);
     const double xl = h.bx + i * h.vx, xh = xl + h.vx;
     const double yl = h.by + j * h.vy, yh = yl + h.vy;
-    const double zl = h.bz + k * h.vz, zh = zl + h.vz;
-    // detector rectangle of the voxel's corner projections: a pixel centre
-    // inside it rounds to a pixel inside [floor(lo + 0.5), floor(hi + 0.5)]
-    double umin = INFINITY, umax = -INFINITY, vmin = INFINITY, vmax = -INFINITY;
+    double umin = INFINITY, umax = -INFINITY, mlo = INFINITY, mhi = -INFINITY;
     const double sdd = h.dso - h.dod;
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) {
@@ -185,50 +227,58 @@ k64_update(const G64 h, const DevGeom g, double* __restrict__ vol, const double2
         const double mag = sdd / (h.dso - t);
         const double up = h.srcy + (ss - h.srcy) * mag;
         umin = fmin(umin, up); umax = fmax(umax, up);
-        vmin = fmin(vmin, fmin(zl * mag, zh * mag)); vmax = fmax(vmax, fmax(zl * mag, zh * mag));
+        mlo = fmin(mlo, mag); mhi = fmax(mhi, mag);
     }
     const int ulo = max((int)floor((umin - h.ymin) / h.du + 0.5), 0);
     const int uhi = min((int)floor((umax - h.ymin) / h.du + 0.5), h.R - 1);
-    const int vlo = max((int)floor((vmin - h.zmin) / h.dv + 0.5), 0);
-    const int vhi = min((int)floor((vmax - h.zmin) / h.dv + 0.5), h.ZP - 1);
-    double W = 0.0, L = 0.0;
-    const double x2x = h.dso * c - h.srcy * s, x2y = h.dso * s + h.srcy * c;
-    for (int u = ulo; u <= uhi; ++u) {
-        const double pu = h.ymin + u * h.du;
-        const double x1x = h.dod * c - pu * s, x1y = h.dod * s + pu * c;
-        const double dx = x2x - x1x, dy = x2y - x1y;
-        double lo = -INFINITY, hi = INFINITY;
-        if (fabs(dx) < h.vx * 1e-12) {
-            if (x1x <= xl || x1x >= xh) continue;
-        } else {
-            const double ix = 1.0 / dx, t0 = (xl - x1x) * ix, t1 = (xh - x1x) * ix;
-            lo = fmin(t0, t1); hi = fmax(t0, t1);
-        }
-        if (fabs(dy) < h.vy * 1e-12) {
-            if (x1y <= yl || x1y >= yh) continue;
-        } else {
-            const double iy = 1.0 / dy, t0 = (yl - x1y) * iy, t1 = (yh - x1y) * iy;
-            lo = fmax(lo, fmin(t0, t1)); hi = fmin(hi, fmax(t0, t1));
-        }
-        if (!(hi > lo)) continue;
-        for (int v = vlo; v <= vhi; ++v) {
-            const double x1z = h.zmin + v * h.dv;
-            const double dz = -x1z;
-            double zlo = lo, zhi = hi;
-            if (fabs(dz) < h.vz * 1e-12) {
-                if (x1z <= zl || x1z >= zh) continue;
-            } else {
-                const double iz = 1.0 / dz, t0 = (zl - x1z) * iz, t1 = (zh - x1z) * iz;
-                zlo = fmax(zlo, fmin(t0, t1)); zhi = fmin(zhi, fmax(t0, t1));
-            }
-            if (!(zhi > zlo)) continue;
-            const double2 rc = rays[(long long)v * h.R + u];
-            const double w = rc.y * (zhi - zlo);
-            W += w * rc.x;
-            L += w;
+    if (ulo > uhi) return;
+    const int nrun = uhi - ulo + 1;
+    double ra[F64_RUN], rb[F64_RUN];
+#pragma unroll
+    for (int q = 0; q < F64_RUN; ++q) {
+        ra[q] = 1.0; rb[q] = 0.0;   // empty
+        if (q < nrun) {
+            const double4 ct = col[ulo + q];
+            double a0, b0, a1, b1;
+            const bool in = slab64(xl, xh, ct.x, ct.z, a0, b0) & slab64(yl, yh, ct.y, ct.w, a1, b1);
+            if (in) { ra[q] = fmax(a0, a1); rb[q] = fmin(b0, b1); }
         }
     }
-    if (L >= h.thr) vol[((long long)k * h.N + j) * h.M + i] += beta * W / L;
+    const int kb = blockIdx.z * F64_ZRUN, ke = min(h.Z, kb + F64_ZRUN);
+    const double vscale = 1.0 / h.dv;
+    for (int k = kb; k < ke; ++k) {
+        const double zl = h.bz + k * h.vz, zh = zl + h.vz;
+        const double vmin = fmin(fmin(zl * mlo, zl * mhi), fmin(zh * mlo, zh * mhi));
+        const double vmax = fmax(fmax(zl * mlo, zl * mhi), fmax(zh * mlo, zh * mhi));
+        const int vlo = max((int)floor((vmin - h.zmin) * vscale + 0.5), 0);
+        const int vhi = min((int)floor((vmax - h.zmin) * vscale + 0.5), h.ZP - 1);
+        double W = 0.0, L = 0.0;
+        for (int v = vlo; v <= vhi; ++v) {
+            const double2 rt = row[v];
+            double za, zb;
+            if (!slab64(zl, zh, rt.x, rt.y, za, zb)) continue;
+            const double2* __restrict__ rr = rays + (long long)v * h.R + ulo;
+            for (int q = 0; q < nrun; ++q) {
+                double a, b;
+                if (q < F64_RUN) {
+                    a = ra[q]; b = rb[q];
+                } else {
+                    const double4 ct = col[ulo + q];
+                    double a0, b0, a1, b1;
+                    const bool in = slab64(xl, xh, ct.x, ct.z, a0, b0) & slab64(yl, yh, ct.y, ct.w, a1, b1);
+                    a = in ? fmax(a0, a1) : 1.0;
+                    b = in ? fmin(b0, b1) : 0.0;
+                }
+                const double lo = fmax(a, za), hi = fmin(b, zb);
+                if (!(hi > lo)) continue;
+                const double2 rc = rr[q];
+                const double w = rc.y * (hi - lo);
+                W += w * rc.x;
+                L += w;
+            }
+        }
+        if (L >= h.thr) vol[((long long)k * h.N + j) * h.M + i] += beta * W / L;
+    }
 }
 
 // FGP-TV in FP64 on one-voxel duals (r, s, t, o, p, q): r[p] belongs to the
@@ -328,6 +378,8 @@ struct F64Solver {
     double* xprev = nullptr;   // x_(k-1); after an iteration with FISTA, x_k
     double* work = nullptr;    // FGP: six duals and L (7 volumes)
     double2* rays = nullptr;   // one view's (c, d12)
+    double4* col = nullptr;    // one view's column table (k64_columns)
+    double2* row = nullptr;    // the row table (k64_rows)
     double* partial = nullptr;
     size_t partial_cap = 0;
     double t = 1.0;
@@ -370,11 +422,18 @@ ctr_status f64_create(Geometry* g, const ctr_solver_params& p, F64Solver** out)
     if ((e = cudaMalloc(&s->y, V * sizeof(double))) != cudaSuccess ||
         (e = cudaMalloc(&s->xprev, V * sizeof(double))) != cudaSuccess ||
         (e = cudaMalloc(&s->rays, P * sizeof(double2))) != cudaSuccess ||
+        (e = cudaMalloc(&s->col, (size_t)h.R * sizeof(double4))) != cudaSuccess ||
+        (e = cudaMalloc(&s->row, (size_t)h.ZP * sizeof(double2))) != cudaSuccess ||
         (e = cudaMalloc(&s->partial, s->partial_cap * sizeof(double))) != cudaSuccess ||
         (e = cudaMemset(s->y, 0, V * sizeof(double))) != cudaSuccess ||
         (e = cudaMemset(s->xprev, 0, V * sizeof(double))) != cudaSuccess) {
         f64_destroy(s);
         return cuda_error(e, "FP64 solver allocation");
+    }
+    k64_rows<<<(h.ZP + 127) / 128, 128>>>(h, s->row);
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaDeviceSynchronize()) != cudaSuccess) {
+        f64_destroy(s);
+        return cuda_error(e, "FP64 solver row table");
     }
     *out = s;
     return CTR_OK;
@@ -387,6 +446,8 @@ void f64_destroy(F64Solver* s)
     cudaFree(s->xprev);
     cudaFree(s->work);
     cudaFree(s->rays);
+    cudaFree(s->col);
+    cudaFree(s->row);
     cudaFree(s->partial);
     delete s;
 }
@@ -419,8 +480,10 @@ static ctr_status f64_objective(F64Solver* s, const double* x, const void* sino,
     std::vector<double> part(per_view);
     double f = 0.0;
     for (int j = 0; j < h.nviews; ++j) {
-        k64_forward<1><<<grid, 128, 0, st>>>(h, x, j, (const char*)sino + (size_t)j * P * dtype_size(sdt), sdt, nullptr,
-                                             s->partial);
+        double vs, vc;
+        view_sc(h, j, vs, vc);
+        k64_forward<1><<<grid, 128, 0, st>>>(h, x, vs, vc, (const char*)sino + (size_t)j * P * dtype_size(sdt), sdt,
+                                             nullptr, s->partial);
         CTR_CUDA_TRY(cudaGetLastError());
         CTR_CUDA_TRY(cudaMemcpyAsync(part.data(), s->partial, per_view * sizeof(double), cudaMemcpyDeviceToHost, st));
         CTR_CUDA_TRY(cudaStreamSynchronize(st));
@@ -452,14 +515,17 @@ ctr_status f64_iterate(F64Solver* s, const void* sino, ctr_dtype sdt, int n, dou
     const bool fgp = s->p.lambda_tv > 0.f && s->p.fgp_iters >= 0;
     if (fgp && !s->work) CTR_CUDA_TRY(cudaMalloc(&s->work, 7 * (size_t)V * sizeof(double)));
     const dim3 fgrid((h.R + 31) / 32, (h.ZP + 3) / 4);
-    const dim3 bgrid((h.M + 31) / 32, (h.N + 3) / 4, h.Z);
+    const dim3 bgrid((h.M + 31) / 32, (h.N + 3) / 4, (h.Z + F64_ZRUN - 1) / F64_ZRUN);
     const dim3 vblk(32, 8), vgrid((h.M + 31) / 32, (h.N + 7) / 8, h.Z);
     for (int it = 0; it < n; ++it) {
         // SART pass on y (V63/host_IterativeRecon_CBCT.c:1-67)
         for (int j = 0; j < h.nviews; ++j) {
-            k64_forward<0><<<fgrid, 128, 0, st>>>(h, s->y, j, (const char*)sino + (size_t)j * P * dtype_size(sdt), sdt,
-                                                  s->rays, nullptr);
-            k64_update<<<bgrid, 128, 0, st>>>(h, g->dg, s->y, s->rays, j, beta);
+            double vs, vc;
+            view_sc(h, j, vs, vc);
+            k64_forward<0><<<fgrid, 128, 0, st>>>(h, s->y, vs, vc, (const char*)sino + (size_t)j * P * dtype_size(sdt),
+                                                  sdt, s->rays, nullptr);
+            k64_columns<<<(h.R + 127) / 128, 128, 0, st>>>(h, vs, vc, s->col);
+            k64_update<<<bgrid, 128, 0, st>>>(h, g->dg, s->y, s->rays, vs, vc, s->col, s->row, beta);
         }
         CTR_CUDA_TRY(cudaGetLastError());
         const double t_k = (1.0 + sqrt(1.0 + 4.0 * s->t * s->t)) / 2.0;   // V63/main_recon.cu:372

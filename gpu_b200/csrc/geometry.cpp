@@ -206,6 +206,7 @@ static ctr_status create(const ctr_geometry_desc* din, int n_slabs, int slab, ct
         q.fast_exit = ((!tbct || n_slabs > 1) && inside) ? 1 : 0;
     }
     q.entry64 = (d.flags & CTR_GEOM_ENTRY_F64) ? 1 : 0;
+    q.fast_sums = (d.flags & CTR_GEOM_FAST_SUMS) ? 1 : 0;
     q.ct_style = tbct ? 3 : ((d.flags & CTR_GEOM_FAN_SLICES) ? 1 : ((d.flags & CTR_GEOM_PARALLEL) ? 2 : 0));
     // T42/...TBCT_voxel.cu:282, V63/...universal.cu:291, T42/..._multiGPU.cu:303,853
     q.loop_eps = (tbct && n_slabs == 1) ? 1e-6f : 1e-16f;

@@ -35,6 +35,7 @@ BP_FOV_MASK = 0x2
 GEOM_FAN_SLICES = 0x2
 GEOM_PARALLEL = 0x4
 GEOM_TBCT = 0x8
+GEOM_FAST_SUMS = 0x10
 SART_STOCHASTIC_ROUND = 0x1
 SART_TILED = 0x2
 SART_REFERENCE_BP = 0x4
@@ -225,16 +226,18 @@ def dtype_code(t) -> int:
 
 def make_desc(nx, ny, nz, vx, nu, nv, du, dso, dod, n_views, us_rate=None, initial_angle=0.0,
               shift_angle=0.0, offset=0.0, m_offset=0, entry64=False, vy=0.0, vz=0.0, dv=0.0, ct_style=0,
-              n_sources=0):
+              n_sources=0, fast_sums=False):
     """ct_style: 0 cone beam, 1 multi-slice fan beam, 2 parallel beam (the
     reference's CT_style); styles 1 and 2 default vz to the detector pitch, as
     the reference does.  ct_style 3: the tetrahedron beam with n_sources
-    sources, nv detector rows each (a view has n_sources * nv rows)."""
+    sources, nv detector rows each (a view has n_sources * nv rows).
+    fast_sums: CTR_GEOM_FAST_SUMS (fused ray-sum accumulation)."""
     if us_rate is None:
         us_rate = 360.0 / n_views
     if ct_style in (1, 2) and not vz:
         vz = du
     flags = (GEOM_ENTRY_F64 if entry64 else 0) | {0: 0, 1: GEOM_FAN_SLICES, 2: GEOM_PARALLEL, 3: GEOM_TBCT}[ct_style]
+    flags |= GEOM_FAST_SUMS if fast_sums else 0
     return GeometryDesc(nx, ny, nz, vx, vy, vz, nu, nv, du, dv, dso, dod, offset, m_offset, n_views,
                         us_rate, initial_angle, shift_angle, flags, n_sources if ct_style == 3 else 0)
 

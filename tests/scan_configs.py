@@ -108,13 +108,13 @@ def og_desc_xyz(cfg):
     return d
 
 
-def ctr_desc(cfg, entry64=False):
+def ctr_desc(cfg, entry64=False, fast_sums=False):
     from gpu_b200.ctrecon import make_desc
     return make_desc(cfg["nx"], cfg["ny"], cfg["nz"], cfg["vx"], cfg["nu"], cfg["nv"], cfg["du"], cfg["dso"],
                      cfg["dod"], cfg["nviews"], initial_angle=cfg.get("initial_angle", 0.0),
                      shift_angle=cfg.get("shift_angle", 0.0), offset=cfg.get("offset", 0.0),
                      m_offset=cfg.get("m_offset", 0), entry64=entry64, ct_style=cfg.get("ct_style", 0),
-                     n_sources=cfg.get("n_sources", 0))
+                     n_sources=cfg.get("n_sources", 0), fast_sums=fast_sums)
 
 # Differentiation scan: 256^3, 360 views, 384^2 detector.  "Config-0 geometry
 # scaled by 2" is read as the same physical extents at twice the sampling:
