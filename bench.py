@@ -1309,7 +1309,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
             "dtype": f"{args.mixed} storage for the projectors (refinement: FP32 FISTA state, FP16 sinogram), "
-                     f"f32 arithmetic",
+                     f"f32 arithmetic" + (", fused ray sums" if args.fast_sums else ""),
             "data": "synthetic",
             "config": scan_config(world),
             "accuracy_vs_fp64": mixed_acc,
