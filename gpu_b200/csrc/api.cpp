@@ -1371,6 +1371,23 @@ static ctr_status solver_reserve(ctr_solver* s)
     return CTR_OK;
 }
 
+// FGP-TV with the fused FISTA step (or the momentum alone), the FISTA factor
+// read from device memory (V63/main_recon.cu:360-384).
+static ctr_status solver_prox(ctr_solver* s, cudaStream_t st, const float* gam_dev)
+{
+    Geometry* g = s->g;
+    const float lam = s->p.beta * s->p.lambda_tv;
+    if (s->p.fista) {
+        if (s->p.lambda_tv > 0.f)
+            CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, s->y, s->xprev, 0.f, st, gam_dev));
+        else
+            CTR_TRY(launch_momentum(*g, s->y, s->xprev, s->y, s->vdt, 0.f, st, gam_dev));
+    } else if (s->p.lambda_tv > 0.f) {
+        CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, nullptr, nullptr, 0.f, st));
+    }
+    return CTR_OK;
+}
+
 // One outer iteration of V63/main_recon.cu:344-386 for one scan on stream st;
 // the FISTA factor and the stochastic-rounding seed of the pass are read from
 // device memory so the launches can be replayed.  fused: the SART traversal
@@ -1397,16 +1414,39 @@ static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_
                       fused ? s->xt : nullptr, fused ? g->d_partial : nullptr));
     if (fused)
         CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
-    const float lam = s->p.beta * s->p.lambda_tv;
-    if (s->p.fista) {
-        if (s->p.lambda_tv > 0.f)
-            CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, s->y, s->xprev, 0.f, st, gam_dev));
-        else
-            CTR_TRY(launch_momentum(*g, s->y, s->xprev, s->y, s->vdt, 0.f, st, gam_dev));
-    } else if (s->p.lambda_tv > 0.f) {
-        CTR_TRY(launch_fgp(*g, s->y, s->vdt, lam, s->p.fgp_iters, nullptr, nullptr, 0.f, st));
+    return solver_prox(s, st, gam_dev);
+}
+
+// The batch's persistent form of solver_issue: the steps before and after
+// the SART pass's views, which the persistent pass runs for every scan in
+// one launch between them.
+static ctr_status batch_pre(ctr_solver* s, cudaStream_t st, bool fused)
+{
+    Geometry* g = s->g;
+    if (s->refine) {
+        if (fused) CTR_TRY(launch_tv(*g, s->xk32, CTR_F32, g->d_partial, 148 * 64, s->d_obj + 1, st));
+        CTR_CUDA_TRY(cudaMemsetAsync(s->yt, 0, (size_t)tiled_count(g->dg) * dtype_size(s->vdt), st));
+        return CTR_OK;
     }
-    return CTR_OK;
+    if (fused) {
+        const void* xk1 = s->p.fista ? s->xprev : s->y;
+        CTR_TRY(launch_tiling(*g, xk1, s->xt, s->vdt, true, st));
+        CTR_TRY(objective_async(g, xk1, s->vdt, s->sino, s->sdt, nullptr, s->d_obj + 1, st));   // TV
+    }
+    return launch_tiling(*g, s->y, s->yt, s->vdt, true, st);
+}
+
+static ctr_status batch_post(ctr_solver* s, cudaStream_t st, const float* gam_dev, bool fused)
+{
+    Geometry* g = s->g;
+    if (!s->refine) CTR_TRY(launch_tiling(*g, s->yt, s->y, s->vdt, false, st));
+    if (fused)
+        CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
+    if (s->refine) {
+        const float lam = s->p.lambda_tv > 0.f ? s->p.beta * s->p.lambda_tv : 0.f;
+        return launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->xt, s->vdt, lam, s->p.fgp_iters, gam_dev, st);
+    }
+    return solver_prox(s, st, gam_dev);
 }
 
 struct ctr_batch {
@@ -1422,6 +1462,14 @@ struct ctr_batch {
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     std::vector<const void*> ws[2];         // workspaces each graph was captured with, 3 per scan
+    // the persistent pass (ctr_batch_set_persistent): the SART views of every
+    // scan in one cooperative launch per iteration
+    bool persistent = false;
+    int pass_blocks = 0;                    // CTAs of the launch (all resident)
+    size_t pass_smem = 0;
+    BatchScan* d_scans[2] = {nullptr, nullptr};   // per graph: the scans' pass descriptions
+    unsigned* d_bars = nullptr;             // one barrier counter per scan
+    unsigned* d_err = nullptr;              // ERR_BARRIER
 };
 
 static std::vector<const void*> batch_workspaces(const ctr_batch* b)
@@ -1446,10 +1494,89 @@ static void batch_drop_graph(ctr_batch* b, int which = -1)
     }
 }
 
+// The forward kind of the scans' passes in graph gi (the same for all scans).
+static int batch_pass_kind(const ctr_batch* b, int gi)
+{
+    return b->scans[0]->refine ? FP_SART_REFINE : (gi == 1 ? FP_SART_OBJ : FP_SART);
+}
+
+// The scans' descriptions for the persistent pass of graph gi, and the
+// split of the launch's CTAs: each scan gets CTAs in proportion to the
+// instructions of its pass (ray steps of the forward projections, voxels
+// of the updates), at least one.
+static ctr_status batch_describe(ctr_batch* b, int gi)
+{
+    const int ns = (int)b->scans.size();
+    const int T = b->pass_blocks;
+    if (ns > T) return set_error(CTR_ERR_UNSUPPORTED, "%d scans exceed the persistent pass's %d resident blocks", ns, T);
+    std::vector<double> cost(ns);
+    double total = 0.0;
+    for (int i = 0; i < ns; ++i) {
+        const DevGeom& g = b->scans[i]->g->dg;
+        cost[i] = (double)g.nviews * ((double)g.R * g.ZP * (g.M + g.N + g.Z) * 21.0 + (double)g.M * g.N * g.Z * 170.0);
+        total += cost[i];
+    }
+    std::vector<int> nc(ns);
+    int used = 0;
+    for (int i = 0; i < ns; ++i) {
+        nc[i] = std::max(1, (int)std::floor(T * cost[i] / total));
+        used += nc[i];
+    }
+    while (used > T) {   // trim the scans with the most CTAs per unit of work
+        int k = -1;
+        for (int i = 0; i < ns; ++i)
+            if (nc[i] > 1 && (k < 0 || nc[i] / cost[i] > nc[k] / cost[k])) k = i;
+        --nc[k];
+        --used;
+    }
+    while (used < T) {   // give the rest to the scans with the most work per CTA
+        int k = 0;
+        for (int i = 1; i < ns; ++i)
+            if (cost[i] / nc[i] > cost[k] / nc[k]) k = i;
+        ++nc[k];
+        ++used;
+    }
+    const int kind = batch_pass_kind(b, gi);
+    std::vector<BatchScan> h(ns);
+    int c0 = 0;
+    for (int i = 0; i < ns; ++i) {
+        ctr_solver* s = b->scans[i];
+        Geometry* G = s->g;
+        BatchScan& q = h[i];
+        q.g = G->dg;
+        if (s->refine) {
+            q.fp_vol = s->xt; q.fp_vol2 = s->yt; q.bp_vol = s->yt;
+            q.partial = G->d_partial; q.ax = s->ax; q.gdev = b->d_gam + i;
+        } else {
+            q.fp_vol = s->yt; q.fp_vol2 = kind == FP_SART_OBJ ? s->xt : nullptr; q.bp_vol = s->yt;
+            q.partial = kind == FP_SART_OBJ ? G->d_partial : nullptr; q.ax = nullptr; q.gdev = nullptr;
+        }
+        q.b = s->sino;
+        q.b_dt = s->sdt;
+        q.rays = (float2*)G->d_rays;
+        q.pass_seed = b->d_seed + i;
+        q.beta = s->p.beta;
+        q.nviews = G->desc.n_views;
+        q.c0 = c0;
+        q.nc = nc[i];
+        c0 += nc[i];
+        q.fp_gx = (G->dg.R + 31) / 32;
+        q.fp_gy = (G->dg.ZP + 3) / 4;
+        q.zl = walk_z_run(G->dg);
+        q.bp_gx = (G->dg.M + 31) / 32;
+        q.bp_gy = (G->dg.N + 3) / 4;
+        q.bp_gz = (G->dg.Z + q.zl - 1) / q.zl;
+    }
+    if (!b->d_scans[gi]) CTR_CUDA_TRY(cudaMalloc(&b->d_scans[gi], sizeof(BatchScan) * ns));
+    CTR_CUDA_TRY(cudaMemcpy(b->d_scans[gi], h.data(), sizeof(BatchScan) * ns, cudaMemcpyHostToDevice));
+    return CTR_OK;
+}
+
 static ctr_status batch_capture(ctr_batch* b, int gi)
 {
     const int ns = (int)b->scans.size();
     for (auto* s : b->scans) CTR_TRY(solver_reserve(s));
+    if (b->persistent) CTR_TRY(batch_describe(b, gi));
     CTR_CUDA_TRY(cudaDeviceSynchronize());
     cudaStream_t cs;
     CTR_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -1457,11 +1584,35 @@ static ctr_status batch_capture(ctr_batch* b, int gi)
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) r = cuda_error(e, "cudaStreamBeginCapture");
     if (r == CTR_OK && (e = cudaEventRecord(b->fork, cs)) != cudaSuccess) r = cuda_error(e, "cudaEventRecord");
-    for (int i = 0; i < ns && r == CTR_OK; ++i) {
-        if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
-        r = solver_issue(b->scans[i], b->streams[i], b->d_gam + i, b->d_seed + i, gi == 1);
-        if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
-        if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
+    if (!b->persistent) {
+        for (int i = 0; i < ns && r == CTR_OK; ++i) {
+            if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
+            r = solver_issue(b->scans[i], b->streams[i], b->d_gam + i, b->d_seed + i, gi == 1);
+            if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
+            if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
+        }
+    } else {
+        // every scan's steps before its views (parallel branches), the one
+        // persistent pass, every scan's steps after them
+        for (int i = 0; i < ns && r == CTR_OK; ++i) {
+            if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
+            r = batch_pre(b->scans[i], b->streams[i], gi == 1);
+            if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
+            if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
+        }
+        const bool stoch = (b->scans[0]->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
+        if (r == CTR_OK && (e = cudaMemsetAsync(b->d_bars, 0, sizeof(unsigned) * ns, cs)) != cudaSuccess)
+            r = cuda_error(e, "cudaMemsetAsync");
+        if (r == CTR_OK)
+            r = launch_batch_pass(b->d_scans[gi], ns, b->pass_blocks, b->scans[0]->vdt, batch_pass_kind(b, gi), stoch,
+                                  b->d_bars, b->d_err, b->pass_smem, cs);
+        if (r == CTR_OK && (e = cudaEventRecord(b->fork, cs)) != cudaSuccess) r = cuda_error(e, "cudaEventRecord");
+        for (int i = 0; i < ns && r == CTR_OK; ++i) {
+            if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
+            r = batch_post(b->scans[i], b->streams[i], b->d_gam + i, gi == 1);
+            if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
+            if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
+        }
     }
     cudaGraph_t gr = nullptr;
     e = cudaStreamEndCapture(cs, &gr);
@@ -1484,7 +1635,56 @@ extern "C" ctr_status ctr_batch_destroy(ctr_batch* b)
     if (b->fork) cudaEventDestroy(b->fork);
     cudaFree(b->d_gam);
     cudaFree(b->d_seed);
+    cudaFree(b->d_scans[0]);
+    cudaFree(b->d_scans[1]);
+    cudaFree(b->d_bars);
+    cudaFree(b->d_err);
     delete b;
+    return CTR_OK;
+}
+
+extern "C" ctr_status ctr_batch_set_persistent(ctr_batch* b, int on)
+{
+    clear_error();
+    CTR_TRY(need(b, "batch"));
+    batch_drop_graph(b);
+    if (!on) {
+        b->persistent = false;
+        return CTR_OK;
+    }
+    const int ns = (int)b->scans.size();
+    size_t smem = 0;
+    for (int i = 0; i < ns; ++i) {
+        const ctr_solver* s = b->scans[i];
+        const DevGeom& g = s->g->dg;
+        if ((s->p.sart_flags & CTR_SART_REFERENCE_BP) || s->slabs > 1 || g.entry64 || g.fast_sums || g.slab_n > 1)
+            return set_error(CTR_ERR_UNSUPPORTED,
+                             "scan %d: the persistent pass runs the engine's update with FP32 entry and the "
+                             "reference's sums (no CTR_SART_REFERENCE_BP, slabs, CTR_GEOM_ENTRY_F64 or "
+                             "CTR_GEOM_FAST_SUMS)", i);
+        smem = std::max(smem, batch_pass_smem(g));
+    }
+    if (smem > 227 * 1024) return set_error(CTR_ERR_UNSUPPORTED, "persistent pass: tables exceed shared memory");
+    const ctr_dtype vdt = b->scans[0]->vdt;
+    const bool stoch = (b->scans[0]->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
+    int per_sm = 0;
+    if (b->scans[0]->refine) {
+        per_sm = batch_pass_blocks_per_sm(vdt, FP_SART_REFINE, stoch, smem);
+    } else {
+        per_sm = std::min(batch_pass_blocks_per_sm(vdt, FP_SART, stoch, smem),
+                          batch_pass_blocks_per_sm(vdt, FP_SART_OBJ, stoch, smem));
+    }
+    int dev = 0, sms = 0;
+    CTR_CUDA_TRY(cudaGetDevice(&dev));
+    CTR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm <= 0 || per_sm * sms < ns)
+        return set_error(CTR_ERR_UNSUPPORTED, "persistent pass: %d resident blocks for %d scans", per_sm * sms, ns);
+    if (!b->d_bars) CTR_CUDA_TRY(cudaMalloc(&b->d_bars, sizeof(unsigned) * ns));
+    if (!b->d_err) CTR_CUDA_TRY(cudaMalloc(&b->d_err, sizeof(unsigned)));
+    CTR_CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(unsigned)));
+    b->pass_blocks = per_sm * sms;
+    b->pass_smem = smem;
+    b->persistent = true;
     return CTR_OK;
 }
 
@@ -1619,6 +1819,15 @@ extern "C" ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* obj_out, vo
         }
     }
     for (auto* s : b->scans) CTR_TRY(check_device_errors(s->g, st));
+    if (b->persistent) {   // a barrier wait of the persistent pass that gave up
+        unsigned h = 0;
+        CTR_CUDA_TRY(cudaMemcpyAsync(&h, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        CTR_CUDA_TRY(cudaStreamSynchronize(st));
+        if (h) {
+            CTR_CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(unsigned)));
+            return set_error(CTR_ERR_TIMEOUT, "the persistent pass's barrier wait gave up (error word %u)", h);
+        }
+    }
     return CTR_OK;
 }
 

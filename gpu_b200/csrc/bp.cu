@@ -29,6 +29,7 @@
 // accumulated per pass in FP64 registers (a float*float product is exact in
 // FP64), so the volume is read and written once per batch.
 #include "ctr_device.cuh"
+#include "fp_kernels.cuh"   // the forward blocks of the batch's persistent pass
 
 namespace ctr {
 
@@ -252,27 +253,34 @@ ctr_status launch_zcell(const Geometry& G, float2* zcell, cudaStream_t st)
 // where the summed length exceeds vx*1e-3 (:772).
 constexpr int WALK_RUN = 4;   // detector columns of the run kept in registers
 
-template <typename VT, bool STOCH, int BY, int MINB, bool TL, int UNR, bool TB>
-__global__ void __launch_bounds__(32 * BY, MINB)
-k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
-            uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
+// The walk's plane and row tables in shared memory (the caller syncs).
+__device__ __forceinline__ void walk_tables(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
+                                            float2*& RT)
 {
-    extern __shared__ float sp[];
-    float* PX = sp;
-    float* PY = PX + (g.M + 3);
-    float* PZ = PY + (g.N + 3);
-    float2* RT = reinterpret_cast<float2*>(PZ + ((g.Z + 3 + 1) & ~1));
-    for (int q = threadIdx.x; q < g.M + 3; q += 32 * BY) PX[q] = g.px[q];
-    for (int q = threadIdx.x; q < g.N + 3; q += 32 * BY) PY[q] = g.py[q];
-    for (int q = threadIdx.x; q < g.Z + 3; q += 32 * BY) PZ[q] = g.pz[q];
-    for (int q = threadIdx.x; q < g.ZP; q += 32 * BY) RT[q] = g.rowt[q];
-    __syncthreads();
-    if (STOCH && pass_seed) seed = *pass_seed * 0x9E3779B9u + (uint32_t)view;
+    PX = sp;
+    PY = PX + (g.M + 3);
+    PZ = PY + (g.N + 3);
+    RT = reinterpret_cast<float2*>(PZ + ((g.Z + 3 + 1) & ~1));
+    for (int q = threadIdx.x; q < g.M + 3; q += blockDim.x) PX[q] = g.px[q];
+    for (int q = threadIdx.x; q < g.N + 3; q += blockDim.x) PY[q] = g.py[q];
+    for (int q = threadIdx.x; q < g.Z + 3; q += blockDim.x) PZ[q] = g.pz[q];
+    for (int q = threadIdx.x; q < g.ZP; q += blockDim.x) RT[q] = g.rowt[q];
+}
 
-    const int i = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int j = blockIdx.y * BY + (threadIdx.x >> 5);
+// One block of the walk: voxel rows by*BY.. and x voxels bx*32.. of z run bz
+// (zl voxels).  k_sart_walk runs it as its own block; the batch's persistent
+// pass runs the blocks of every scan's view in turn.
+template <typename VT, bool STOCH, int BY, bool TL, int UNR, bool TB>
+__device__ __forceinline__ void walk_block(const DevGeom& g, const float* __restrict__ PX,
+                                           const float* __restrict__ PY, const float* __restrict__ PZ,
+                                           const float2* __restrict__ RT, int bx, int by, int bz,
+                                           VT* __restrict__ vol, const float2* __restrict__ rays, int view,
+                                           float beta, uint32_t seed, int zl)
+{
+    const int i = bx * 32 + (threadIdx.x & 31);
+    const int j = by * BY + (threadIdx.x >> 5);
     if (i >= g.M || j >= g.N) return;
-    const int kb = blockIdx.z * zl, ke = min(g.Z, kb + zl);
+    const int kb = bz * zl, ke = min(g.Z, kb + zl);
 
     // FOV cylinder (universal.cu:626-628): masked voxels keep their value
     const float ex = fs(fs((float)i, g.fov_h_x), g.m_off);
@@ -393,7 +401,7 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
         };
         // every pair of the voxel, row by row (rows ascending), the order the
         // oracle's gather sums them
-        auto all_pairs = [&]() {
+        auto all_pairs = [&]() {   // vlo <= vhi here
             int vv = vlo;
             if (UNR == 2) {   // two rows' z-cell loads in flight, then their pairs in row order
                 for (; vv < vhi; vv += 2) {
@@ -401,8 +409,16 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
                     row_pairs(vv, z0c);
                     row_pairs(vv + 1, z1c);
                 }
+                for (; vv <= vhi; ++vv) row_pairs(vv, __ldg(zrow + vv));
+            } else {          // the next row's z-cell load issued before this row's pairs
+                float2 zn = __ldg(zrow + vv);
+                for (; vv < vhi; ++vv) {
+                    const float2 zc = zn;
+                    zn = __ldg(zrow + vv + 1);
+                    row_pairs(vv, zc);
+                }
+                row_pairs(vhi, zn);
             }
-            for (; vv <= vhi; ++vv) row_pairs(vv, __ldg(zrow + vv));
         };
         // candidate rows of the band [row0, row0 + nvr) seen from height zs
         // through the cell between planes z0 and z1
@@ -431,10 +447,11 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
             if ((vlo < 0 && vhi < 0) || (vlo > g.ZP - 1 && vhi > g.ZP - 1)) continue;
             vlo = max(vlo, 0);
             vhi = min(vhi, g.ZP - 1);
+            const float old = Store<VT>::ldw(pv);   // loaded ahead: its latency overlaps the pairs
             all_pairs();
             if (!(sl < g.thr_bp)) {                                            // :799-806
                 VT* p = pv;
-                const float nv = fa(Store<VT>::ldw(p), fdv(fm(beta, sw), sl));
+                const float nv = fa(old, fdv(fm(beta, sw), sl));
                 if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
                 else Store<VT>::st(p, nv);
             }
@@ -479,6 +496,21 @@ k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ra
             }
         }
     }
+}
+
+template <typename VT, bool STOCH, int BY, int MINB, bool TL, int UNR, bool TB>
+__global__ void __launch_bounds__(32 * BY, MINB)
+k_sart_walk(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ rays, int view, float beta,
+            uint32_t seed, const uint32_t* __restrict__ pass_seed, int zl)
+{
+    extern __shared__ float sp[];
+    float *PX, *PY, *PZ;
+    float2* RT;
+    walk_tables(g, sp, PX, PY, PZ, RT);
+    __syncthreads();
+    if (STOCH && pass_seed) seed = *pass_seed * 0x9E3779B9u + (uint32_t)view;
+    walk_block<VT, STOCH, BY, TL, UNR, TB>(g, PX, PY, PZ, RT, blockIdx.x, blockIdx.y, blockIdx.z, vol, rays, view,
+                                           beta, seed, zl);
 }
 
 // Linear <-> 8x8-tiled copies of a volume (same storage type).  One thread
@@ -641,6 +673,170 @@ k_adjoint(const DevGeom g, VT* __restrict__ vol, const AdjRay* __restrict__ rays
 static size_t bp_smem(const DevGeom& g)
 {
     return sizeof(float) * (size_t)(g.M + 3 + g.N + 3 + ((g.Z + 3 + 1) & ~1)) + sizeof(float2) * g.ZP;
+}
+
+// ------------------------------------------------- the batch's persistent pass
+
+int walk_z_run(const DevGeom& g)
+{
+    int zl = kBpShapes[1].zl;
+    const long long cols = (long long)g.M * g.N;
+    while (zl > 1 && cols * ((g.Z + zl - 1) / zl) < 148LL * 2048) zl >>= 1;
+    return zl;
+}
+
+// forward tables (rounded to 8 bytes), then the walk's
+__host__ __device__ __forceinline__ size_t fp_table_floats(const DevGeom& g)
+{
+    return ((size_t)(g.M + g.N + g.Z + 16) + 1) & ~(size_t)1;
+}
+size_t batch_pass_smem(const DevGeom& g) { return sizeof(float) * fp_table_floats(g) + bp_smem(g); }
+
+constexpr unsigned kBarrierSpins = 1u << 24;   // x ~100 ns: a wait gives up after about 2 s
+
+// The CTAs of one scan meet: each block arrives once its threads are done
+// with the phase, then waits until all nc blocks of the scan have arrived
+// (target = nc x the number of phases so far).  The wait is bounded: past
+// kBarrierSpins polls, or once any block has flagged an error, it sets
+// ERR_BARRIER and returns false, and the caller leaves.  The launch is
+// cooperative, so all the scan's blocks are resident and a wait only gives
+// up if something else went wrong.
+__device__ __forceinline__ bool scan_barrier(unsigned* bar, unsigned target, unsigned* err)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();   // this block's writes of the phase, before its arrival
+        atomicAdd(bar, 1u);
+        int good = 1;
+        for (unsigned spins = 0;; ++spins) {
+            if (*(volatile unsigned*)bar >= target) break;
+            if (*(volatile unsigned*)err != 0u || spins > kBarrierSpins) {
+                atomicOr(err, ERR_BARRIER);
+                good = 0;
+                break;
+            }
+            __nanosleep(100);
+        }
+        __threadfence();   // the other blocks' writes, after the wait
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The SART pass of every scan of a batch in one launch.  Block b serves the
+// scan whose CTA range holds it; per view its share of the forward blocks,
+// a barrier, its share of the walk's blocks, a barrier.  Each block runs
+// exactly the per-ray and per-voxel code of k_forward (shape 1) and
+// k_sart_walk (shape 1), so every scan's result equals its solver's.
+template <typename VT, int KIND, bool STOCH>
+__global__ void __launch_bounds__(128, 6)
+k_batch_pass(const BatchScan* __restrict__ scans, int nscans, unsigned* __restrict__ bars, unsigned* __restrict__ err)
+{
+    extern __shared__ float sp[];
+    __shared__ int s_idx;
+    if (threadIdx.x == 0) {   // the last scan whose first block is at or before this one
+        int lo = 0, hi = nscans - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (scans[mid].c0 <= (int)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        s_idx = lo;
+    }
+    __syncthreads();
+    const BatchScan& S = scans[s_idx];
+    const DevGeom& g = S.g;
+    float *PX, *PY, *PZ, *PINF;
+    fp_tables(g, sp, PX, PY, PZ, PINF);
+    float *WX, *WY, *WZ;
+    float2* RT;
+    walk_tables(g, sp + fp_table_floats(g), WX, WY, WZ, RT);
+    __syncthreads();
+    const int local = (int)blockIdx.x - S.c0;
+    const int nfp = S.fp_gx * S.fp_gy, nbp = S.bp_gx * S.bp_gy * S.bp_gz;
+    const long long P = (long long)g.R * g.ZP;
+    const size_t per_view = (size_t)g.ZP * S.fp_gx;
+    const size_t bsz = S.b_dt == CTR_F32 ? 4 : 2;
+    unsigned target = 0;
+    for (int j = 0; j < S.nviews; ++j) {
+        for (int vb = local; vb < nfp; vb += S.nc)
+            fp_block<VT, KIND, false, 4, 0, true, false>(
+                g, PX, PY, PZ, PINF, vb % S.fp_gx, vb / S.fp_gx, 0, S.fp_gx, S.fp_gy, (const VT*)S.fp_vol, j, S.rays,
+                0, (const char*)S.b + (size_t)j * P * bsz, S.b_dt,
+                S.partial ? S.partial + (size_t)j * per_view : nullptr, nullptr, nullptr, nullptr,
+                (const VT*)S.fp_vol2, S.ax ? S.ax + (size_t)j * P : nullptr, S.gdev);
+        target += (unsigned)S.nc;
+        if (!scan_barrier(bars + s_idx, target, err)) return;
+        const uint32_t seed = STOCH ? *S.pass_seed * 0x9E3779B9u + (uint32_t)j : 0u;
+        for (int vb = local; vb < nbp; vb += S.nc) {
+            const int bx = vb % S.bp_gx, r = vb / S.bp_gx, by = r % S.bp_gy, bz = r / S.bp_gy;
+            if (g.ct_style == 3)
+                walk_block<VT, STOCH, 4, true, 1, true>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol, S.rays, j,
+                                                        S.beta, seed, S.zl);
+            else
+                walk_block<VT, STOCH, 4, true, 1, false>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol, S.rays, j,
+                                                         S.beta, seed, S.zl);
+        }
+        target += (unsigned)S.nc;
+        if (!scan_barrier(bars + s_idx, target, err)) return;
+    }
+}
+
+template <typename VT, int KIND, bool STOCH>
+static const void* batch_pass_fn()
+{
+    return reinterpret_cast<const void*>(&k_batch_pass<VT, KIND, STOCH>);
+}
+
+static const void* batch_pass_kernel(ctr_dtype vdt, int kind, bool stoch)
+{
+    const void* f = nullptr;
+    auto pick = [&](auto tag) {
+        using VT = decltype(tag);
+        if (kind == FP_SART) f = stoch ? batch_pass_fn<VT, FP_SART, true>() : batch_pass_fn<VT, FP_SART, false>();
+        else if (kind == FP_SART_OBJ)
+            f = stoch ? batch_pass_fn<VT, FP_SART_OBJ, true>() : batch_pass_fn<VT, FP_SART_OBJ, false>();
+        else if (kind == FP_SART_REFINE)
+            f = stoch ? batch_pass_fn<VT, FP_SART_REFINE, true>() : batch_pass_fn<VT, FP_SART_REFINE, false>();
+    };
+    if (vdt == CTR_F32) pick(float());
+    else if (vdt == CTR_BF16) pick(__nv_bfloat16());
+    else if (vdt == CTR_F16) pick(__half());
+    return f;
+}
+
+int batch_pass_blocks_per_sm(ctr_dtype vdt, int kind, bool stoch, size_t smem)
+{
+    const void* f = batch_pass_kernel(vdt, kind, stoch);
+    if (!f) return 0;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, 128, smem) != cudaSuccess) return 0;
+    return n;
+}
+
+ctr_status launch_batch_pass(const BatchScan* d_scans, int nscans, int nblocks, ctr_dtype vdt, int kind, bool stoch,
+                             unsigned* bars, unsigned* err, size_t smem, cudaStream_t st)
+{
+    const void* f = batch_pass_kernel(vdt, kind, stoch);
+    if (!f) return set_error(CTR_ERR_UNSUPPORTED, "persistent pass: storage type or kind not supported");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void* args[] = {(void*)&d_scans, (void*)&nscans, (void*)&bars, (void*)&err};
+    CTR_CUDA_TRY(cudaLaunchKernelExC(&cfg, f, args));
+    return CTR_OK;
 }
 
 ctr_status launch_backproject(const Geometry& G, const BpArgs& a, cudaStream_t st)

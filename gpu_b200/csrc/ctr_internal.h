@@ -226,6 +226,42 @@ ctr_status launch_refine_update(Geometry& g, float* xk, float* xm, const void* d
 // *p = v on the device (a per-iteration scalar that graphs read)
 ctr_status launch_set_scalar(float* p, float v, cudaStream_t st);
 
+// One scan of the batch's persistent SART pass (bp.cu): the scan's CTAs
+// [c0, c0 + nc) run, view after view, the blocks of its forward projection
+// (fp_gx x fp_gy blocks of 32 x 4 rays), a barrier of the scan's CTAs, the
+// blocks of its walk (bp_gx x bp_gy x bp_gz blocks of 32 x 4 voxel columns,
+// z runs of zl), a barrier.
+struct BatchScan {
+    DevGeom g;
+    const void* fp_vol;          // the volume the projection reads (tiled)
+    const void* fp_vol2;         // SART_OBJ: the objective's volume; SART_REFINE: the correction d
+    void* bp_vol;                // the volume the update writes (tiled)
+    const void* b;               // measured sinogram
+    int b_dt;
+    float2* rays;                // the scan's ray records (one view)
+    double* partial;             // SART_OBJ, SART_REFINE: objective partials, [view][row][u/32]
+    float* ax;                   // SART_REFINE
+    const float* gdev;           // SART_REFINE
+    const uint32_t* pass_seed;   // stochastic rounding (device)
+    float beta;
+    int nviews;
+    int c0, nc;
+    int fp_gx, fp_gy;
+    int bp_gx, bp_gy, bp_gz, zl;
+};
+constexpr unsigned ERR_BARRIER = 2u;   // a persistent pass's barrier wait gave up
+// Blocks per SM the persistent pass runs at (its occupancy), or 0.
+int batch_pass_blocks_per_sm(ctr_dtype vdt, int kind, bool stoch, size_t smem);
+// The persistent pass over every scan: one cooperative launch of nblocks
+// CTAs (all resident at once).  bars: one zeroed counter per scan; err: the
+// device error word (ERR_BARRIER when a barrier wait gives up).
+ctr_status launch_batch_pass(const BatchScan* d_scans, int nscans, int nblocks, ctr_dtype vdt, int kind, bool stoch,
+                             unsigned* bars, unsigned* err, size_t smem, cudaStream_t st);
+// shared memory of the persistent pass for one scan's geometry
+size_t batch_pass_smem(const DevGeom& g);
+// the walk's z run for a geometry (launch shape 1, shortened for small volumes)
+int walk_z_run(const DevGeom& g);
+
 // The FP64 reference solver (f64.cu): the solver's iteration with every step
 // in FP64.  obj_out (host, may be NULL): [TV, fidelity, objective] per
 // iteration, evaluated when params.objective is set (NaN otherwise).

@@ -379,31 +379,36 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
 // tree), stored by (view, row, segment), so the totals do not depend on the
 // launch shape or the issue order; the dot product's are per block of the
 // fixed 32x4 shape.
-template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false, int MINB = 1, bool FAST = false>
-__global__ void __launch_bounds__(FP_BX * BY, MINB)
-k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
-          const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
-          uint64_t* __restrict__ hash, float* __restrict__ lens, const VT* __restrict__ vol2,
-          float* __restrict__ ax, const float* __restrict__ gdev)
+// The plane tables of the forward kernels in shared memory (the caller syncs).
+__device__ __forceinline__ void fp_tables(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
+                                          float*& PINF)
 {
-    constexpr int NT = FP_BX * BY;
-    constexpr bool DUAL = KIND == FP_SART_OBJ || KIND == FP_SART_REFINE;
-    extern __shared__ float sp[];
-    float* PX;
-    float* PY;
-    float* PZ;
-    float* PINF;
     plane_tables_layout(g, sp, PX, PY, PZ, PINF);
-    for (int t = threadIdx.x; t < g.M + 3; t += NT) PX[t] = g.px[t];
-    for (int t = threadIdx.x; t < g.N + 3; t += NT) PY[t] = g.py[t];
-    for (int t = threadIdx.x; t < g.Z + 3; t += NT) PZ[t] = g.pz[t];
+    for (int t = threadIdx.x; t < g.M + 3; t += blockDim.x) PX[t] = g.px[t];
+    for (int t = threadIdx.x; t < g.N + 3; t += blockDim.x) PY[t] = g.py[t];
+    for (int t = threadIdx.x; t < g.Z + 3; t += blockDim.x) PZ[t] = g.pz[t];
     if (threadIdx.x == 0) PINF[0] = __int_as_float(0x7f800000);
-    __syncthreads();
+}
 
-    const int tx = centre_out(blockIdx.x, gridDim.x), ty = centre_out(blockIdx.y, gridDim.y);
+// One block of the forward projection: block (bx, by, bz) of a (gx, gy, *)
+// grid of FP_BX x BY rays (bz: the view offset), with the plane tables in
+// shared memory.  k_forward runs it as its own block; the batch's persistent
+// pass runs the blocks of every scan's view in turn.
+template <typename VT, int KIND, bool E64, int BY, int CPM, bool TL, bool FAST>
+__device__ __forceinline__ void fp_block(const DevGeom& g, const float* __restrict__ PX, const float* __restrict__ PY,
+                                         const float* __restrict__ PZ, const float* __restrict__ PINF, int bx, int by,
+                                         int bz, int gx, int gy, const VT* __restrict__ vol, int view0,
+                                         void* __restrict__ out, int out_dt, const void* __restrict__ b, int b_dt,
+                                         double* __restrict__ partial, int* __restrict__ nseg,
+                                         uint64_t* __restrict__ hash, float* __restrict__ lens,
+                                         const VT* __restrict__ vol2, float* __restrict__ ax,
+                                         const float* __restrict__ gdev)
+{
+    constexpr bool DUAL = KIND == FP_SART_OBJ || KIND == FP_SART_REFINE;
+    const int tx = centre_out(bx, gx), ty = centre_out(by, gy);
     const int u = tx * FP_BX + (threadIdx.x % FP_BX);
     const int v = ty * BY + (threadIdx.x / FP_BX);
-    const int w = blockIdx.z;
+    const int w = bz;
     const bool active = (u < g.R) && (v < g.ZP);
     const long long P = (long long)g.R * g.ZP;
     const long long p = (long long)w * P + (long long)v * g.R + u;
@@ -457,12 +462,31 @@ k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restri
     if (KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_SART_REFINE) {
         double t = e2;
         for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-        if ((threadIdx.x & 31) == 0 && v < g.ZP) partial[((size_t)w * g.ZP + v) * gridDim.x + tx] = t;
+        if ((threadIdx.x & 31) == 0 && v < g.ZP) partial[((size_t)w * g.ZP + v) * gx + tx] = t;
     } else if (KIND == FP_DOT) {
         __shared__ double sh[BY];
         const double t = block_sum(e2, sh);
-        if (threadIdx.x == 0) partial[((size_t)blockIdx.z * gridDim.y + ty) * gridDim.x + tx] = t;
+        if (threadIdx.x == 0) partial[((size_t)bz * gy + ty) * gx + tx] = t;
     }
+}
+
+template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false, int MINB = 1, bool FAST = false>
+__global__ void __launch_bounds__(FP_BX * BY, MINB)
+k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
+          const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
+          uint64_t* __restrict__ hash, float* __restrict__ lens, const VT* __restrict__ vol2,
+          float* __restrict__ ax, const float* __restrict__ gdev)
+{
+    extern __shared__ float sp[];
+    float* PX;
+    float* PY;
+    float* PZ;
+    float* PINF;
+    fp_tables(g, sp, PX, PY, PZ, PINF);
+    __syncthreads();
+    fp_block<VT, KIND, E64, BY, CPM, TL, FAST>(g, PX, PY, PZ, PINF, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x,
+                                               gridDim.y, vol, view0, out, out_dt, b, b_dt, partial, nseg, hash,
+                                               lens, vol2, ax, gdev);
 }
 
 template <typename VT, int KIND, int BY, int CPM, bool TL, int MINB, bool FAST = false>

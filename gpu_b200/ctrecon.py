@@ -59,6 +59,7 @@ EXPORTED = [
     "ctr_solver_objectives", "ctr_geometry_create_slab", "ctr_geometry_slab", "ctr_forward_partial",
     "ctr_combine_partials", "ctr_sart_update", "ctr_sart_pass_slabs", "ctr_volume_tiling", "ctr_volume_tiled_count",
     "ctr_set_default_devices", "ctr_solver_set_slabs", "ctr_solver_get_volume_f32", "ctr_batch_get_volume_f32",
+    "ctr_batch_set_persistent",
 ]
 
 
@@ -170,6 +171,7 @@ def load_library(path: str = LIB_PATH):
         "ctr_solver_set_slabs": ([vp, i], i),
         "ctr_solver_get_volume_f32": ([vp, vp, vp], i),
         "ctr_batch_get_volume_f32": ([vp, i, vp, vp], i),
+        "ctr_batch_set_persistent": ([vp, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -584,6 +586,10 @@ class Batch:
     def get_volume_f32(self, scan, out, stream=None):
         check(self.lib.ctr_batch_get_volume_f32(self.h, scan, _ptr(out), _stream(stream)))
         return out
+
+    def set_persistent(self, on=True):
+        """Every scan's SART views in one persistent launch per iteration (``ctr_batch_set_persistent``)."""
+        check(self.lib.ctr_batch_set_persistent(self.h, int(on)))
 
 
 # ---------------------------------------------------------------------------

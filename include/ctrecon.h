@@ -472,6 +472,19 @@ ctr_status ctr_batch_iterate(ctr_batch* b, int n, double* objective_out, void* s
 ctr_status ctr_batch_get_volume(ctr_batch* b, int scan, void* dst, void* stream);
 /* ctr_solver_get_volume_f32 of one scan. */
 ctr_status ctr_batch_get_volume_f32(ctr_batch* b, int scan, float* dst, void* stream);
+/* on = 1: from the next ctr_batch_iterate, the SART views of every scan run
+ * in one persistent launch per iteration: a cooperative grid of as many
+ * blocks as the GPU holds at once, split among the scans in proportion to
+ * their work; each scan's blocks run its views in order, the forward
+ * projection's blocks, a barrier of the scan's blocks, the update's blocks,
+ * a barrier.  The per-ray and per-voxel code is the single-scan kernels'
+ * (launch shape 1), so every scan's result is unchanged.  The barrier waits
+ * are bounded: one that gives up (about 2 s) makes ctr_batch_iterate return
+ * CTR_ERR_TIMEOUT.  Refused (CTR_ERR_UNSUPPORTED) for scans with
+ * CTR_SART_REFERENCE_BP, slabs, CTR_GEOM_ENTRY_F64 or CTR_GEOM_FAST_SUMS, or
+ * more scans than resident blocks.  on = 0: one kernel per view and scan, the
+ * scans as parallel graph branches (the default). */
+ctr_status ctr_batch_set_persistent(ctr_batch* b, int on);
 
 /* ------------------------------------------------------------- utilities */
 

@@ -36,18 +36,24 @@ def bits(t):
     return t.float().cpu().numpy().view(np.uint32)
 
 
-@pytest.mark.parametrize("dtype", ["f32", "f16", "bf16_sr"])
-def test_batch_equals_single_solver(dtype, oracle_built):
+@pytest.mark.parametrize("persistent", [False, True])
+@pytest.mark.parametrize("dtype", ["f32", "f16", "bf16_sr", "f16_refine"])
+def test_batch_equals_single_solver(dtype, persistent, oracle_built):
     """bf16_sr: stochastic rounding, whose per-pass seed the batch reads from
-    device memory; the single-scan solver issues those passes directly."""
+    device memory; the single-scan solver issues those passes directly.
+    persistent: the SART views of all scans in one persistent launch per
+    iteration (ctr_batch_set_persistent), the same per-ray and per-voxel code."""
     import gpu_b200
-    vdt = {"f32": gpu_b200.F32, "f16": gpu_b200.F16, "bf16_sr": gpu_b200.BF16}[dtype]
-    tdt = {"f32": torch.float32, "f16": torch.float16, "bf16_sr": torch.bfloat16}[dtype]
+    vdt = {"f32": gpu_b200.F32, "f16": gpu_b200.F16, "bf16_sr": gpu_b200.BF16, "f16_refine": gpu_b200.F16}[dtype]
+    tdt = {"f32": torch.float32, "f16": torch.float16, "bf16_sr": torch.bfloat16, "f16_refine": torch.float16}[dtype]
     data = scans(oracle_built)
     flags = gpu_b200.SART_STOCHASTIC_ROUND if dtype.endswith("_sr") else 0
-    kw = dict(beta=0.8, lambda_tv=0.05, fgp_iters=4, fista=True, objective=True, sart_flags=flags)
+    kw = dict(beta=0.8, lambda_tv=0.05, fgp_iters=4, fista=True, objective=True, sart_flags=flags,
+              refine=dtype.endswith("_refine"))
     geoms = [gpu_b200.Geometry(ctr_desc(cfg)) for cfg, _ in data]
     batch = gpu_b200.Batch(geoms, vdt, **kw)
+    if persistent:
+        batch.set_persistent(True)
     for i, (_, b) in enumerate(data):
         batch.set_sinogram(i, b)
     batch.reset()
@@ -65,6 +71,19 @@ def test_batch_equals_single_solver(dtype, oracle_built):
         np.testing.assert_array_equal(bits(got), bits(want))
         np.testing.assert_array_equal(objs[i], ref_obj)
         assert objs[i, -1, 1] < objs[i, 0, 1]
+
+
+def test_persistent_batch_refusals(oracle_built):
+    """The persistent pass runs the engine's update with the reference's sums:
+    the reference backprojection arithmetic is refused, and the per-view form
+    comes back with set_persistent(False)."""
+    import gpu_b200
+    data = scans(oracle_built)[:2]
+    geoms = [gpu_b200.Geometry(ctr_desc(cfg)) for cfg, _ in data]
+    batch = gpu_b200.Batch(geoms, gpu_b200.F32, beta=0.8, sart_flags=gpu_b200.SART_REFERENCE_BP)
+    with pytest.raises(gpu_b200.CtrError):
+        batch.set_persistent(True)
+    batch.set_persistent(False)
 
 
 def test_batch_reset_and_workspace_growth(oracle_built):
