@@ -889,9 +889,10 @@ extern "C" ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void
     return CTR_OK;
 }
 
-// The refinement solver's SART pass: d = 0, then per view the projection of
-// the copy xt and of d (FP_SART_REFINE: the residual against y_k, A x~_k into
-// ax, the objective partials of x~_k) and the SART update of d.
+// The refinement solver's SART pass: d = d0 (the copies' rounding of y_k),
+// then per view the projection of the copy xt and of d (FP_SART_REFINE: the
+// residual against y_k, A x~_k into ax, the objective partials of x~_k) and
+// the SART update of d.
 static ctr_status refine_pass(ctr_solver* s, uint32_t seed, const uint32_t* pass_seed, const float* gdev,
                               cudaStream_t st)
 {
@@ -899,7 +900,7 @@ static ctr_status refine_pass(ctr_solver* s, uint32_t seed, const uint32_t* pass
     const long long P = g->npix();
     const size_t per_view = objective_partials_per_view(g->dg);
     CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
-    CTR_CUDA_TRY(cudaMemsetAsync(s->yt, 0, (size_t)tiled_count(g->dg) * dtype_size(s->vdt), st));
+    CTR_TRY(launch_refine_start(*g, s->xk32, s->xm32, s->yt, s->vdt, gdev, st));
     for (int j = 0; j < g->desc.n_views; ++j) {
         FpArgs a{};
         a.vol = s->xt; a.vol_dtype = s->vdt; a.view0 = j; a.nview = 1; a.kind = FP_SART_REFINE; a.tiled = 1;
@@ -1420,13 +1421,12 @@ static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_
 // The batch's persistent form of solver_issue: the steps before and after
 // the SART pass's views, which the persistent pass runs for every scan in
 // one launch between them.
-static ctr_status batch_pre(ctr_solver* s, cudaStream_t st, bool fused)
+static ctr_status batch_pre(ctr_solver* s, cudaStream_t st, bool fused, const float* gam_dev)
 {
     Geometry* g = s->g;
     if (s->refine) {
         if (fused) CTR_TRY(launch_tv(*g, s->xk32, CTR_F32, g->d_partial, 148 * 64, s->d_obj + 1, st));
-        CTR_CUDA_TRY(cudaMemsetAsync(s->yt, 0, (size_t)tiled_count(g->dg) * dtype_size(s->vdt), st));
-        return CTR_OK;
+        return launch_refine_start(*g, s->xk32, s->xm32, s->yt, s->vdt, gam_dev, st);
     }
     if (fused) {
         const void* xk1 = s->p.fista ? s->xprev : s->y;
@@ -1463,12 +1463,12 @@ struct ctr_batch {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     std::vector<const void*> ws[2];         // workspaces each graph was captured with, 3 per scan
     // the persistent pass (ctr_batch_set_persistent): the SART views of every
-    // scan in one cooperative launch per iteration
+    // scan in one launch per iteration
     bool persistent = false;
-    int pass_blocks = 0;                    // CTAs of the launch (all resident)
+    int pass_blocks = 0;                    // CTAs of the launch (its occupancy x SMs)
     size_t pass_smem = 0;
     BatchScan* d_scans[2] = {nullptr, nullptr};   // per graph: the scans' pass descriptions
-    unsigned* d_bars = nullptr;             // one barrier counter per scan
+    void* d_flow = nullptr;                 // the pass's work counters (batch_flow_bytes)
     unsigned* d_err = nullptr;              // ERR_BARRIER
 };
 
@@ -1596,16 +1596,16 @@ static ctr_status batch_capture(ctr_batch* b, int gi)
         // persistent pass, every scan's steps after them
         for (int i = 0; i < ns && r == CTR_OK; ++i) {
             if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
-            r = batch_pre(b->scans[i], b->streams[i], gi == 1);
+            r = batch_pre(b->scans[i], b->streams[i], gi == 1, b->d_gam + i);
             if (r == CTR_OK && (e = cudaEventRecord(b->joins[i], b->streams[i])) != cudaSuccess) r = cuda_error(e, "join");
             if (r == CTR_OK && (e = cudaStreamWaitEvent(cs, b->joins[i], 0)) != cudaSuccess) r = cuda_error(e, "join");
         }
         const bool stoch = (b->scans[0]->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
-        if (r == CTR_OK && (e = cudaMemsetAsync(b->d_bars, 0, sizeof(unsigned) * ns, cs)) != cudaSuccess)
+        if (r == CTR_OK && (e = cudaMemsetAsync(b->d_flow, 0, batch_flow_bytes(ns), cs)) != cudaSuccess)
             r = cuda_error(e, "cudaMemsetAsync");
         if (r == CTR_OK)
             r = launch_batch_pass(b->d_scans[gi], ns, b->pass_blocks, b->scans[0]->vdt, batch_pass_kind(b, gi), stoch,
-                                  b->d_bars, b->d_err, b->pass_smem, cs);
+                                  b->d_flow, b->d_err, b->pass_smem, cs);
         if (r == CTR_OK && (e = cudaEventRecord(b->fork, cs)) != cudaSuccess) r = cuda_error(e, "cudaEventRecord");
         for (int i = 0; i < ns && r == CTR_OK; ++i) {
             if ((e = cudaStreamWaitEvent(b->streams[i], b->fork, 0)) != cudaSuccess) { r = cuda_error(e, "fork"); break; }
@@ -1637,7 +1637,7 @@ extern "C" ctr_status ctr_batch_destroy(ctr_batch* b)
     cudaFree(b->d_seed);
     cudaFree(b->d_scans[0]);
     cudaFree(b->d_scans[1]);
-    cudaFree(b->d_bars);
+    cudaFree(b->d_flow);
     cudaFree(b->d_err);
     delete b;
     return CTR_OK;
@@ -1679,7 +1679,7 @@ extern "C" ctr_status ctr_batch_set_persistent(ctr_batch* b, int on)
     CTR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (per_sm <= 0 || per_sm * sms < ns)
         return set_error(CTR_ERR_UNSUPPORTED, "persistent pass: %d resident blocks for %d scans", per_sm * sms, ns);
-    if (!b->d_bars) CTR_CUDA_TRY(cudaMalloc(&b->d_bars, sizeof(unsigned) * ns));
+    if (!b->d_flow) CTR_CUDA_TRY(cudaMalloc(&b->d_flow, batch_flow_bytes(ns)));
     if (!b->d_err) CTR_CUDA_TRY(cudaMalloc(&b->d_err, sizeof(unsigned)));
     CTR_CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(unsigned)));
     b->pass_blocks = per_sm * sms;

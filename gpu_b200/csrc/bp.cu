@@ -252,15 +252,22 @@ ctr_status launch_zcell(const Geometry& G, float2* zcell, cudaStream_t st)
 // above); the sources are added in ascending order, and the update applies
 // where the summed length exceeds vx*1e-3 (:772).
 constexpr int WALK_RUN = 4;   // detector columns of the run kept in registers
+constexpr float ROW_EPS = 1.0f / 32.0f;   // margin of the alpha-range row estimate, in rows
 
-// The walk's plane and row tables in shared memory (the caller syncs).
-__device__ __forceinline__ void walk_tables(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
-                                            float2*& RT)
+// The walk's plane and row tables in shared memory: their addresses, and the
+// tables themselves (the caller syncs).
+__device__ __forceinline__ void walk_tables_addr(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
+                                                 float2*& RT)
 {
     PX = sp;
     PY = PX + (g.M + 3);
     PZ = PY + (g.N + 3);
     RT = reinterpret_cast<float2*>(PZ + ((g.Z + 3 + 1) & ~1));
+}
+__device__ __forceinline__ void walk_tables(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
+                                            float2*& RT)
+{
+    walk_tables_addr(g, sp, PX, PY, PZ, RT);
     for (int q = threadIdx.x; q < g.M + 3; q += blockDim.x) PX[q] = g.px[q];
     for (int q = threadIdx.x; q < g.N + 3; q += blockDim.x) PY[q] = g.py[q];
     for (int q = threadIdx.x; q < g.Z + 3; q += blockDim.x) PZ[q] = g.pz[q];
@@ -269,8 +276,9 @@ __device__ __forceinline__ void walk_tables(const DevGeom& g, float* sp, float*&
 
 // One block of the walk: voxel rows by*BY.. and x voxels bx*32.. of z run bz
 // (zl voxels).  k_sart_walk runs it as its own block; the batch's persistent
-// pass runs the blocks of every scan's view in turn.
-template <typename VT, bool STOCH, int BY, bool TL, int UNR, bool TB>
+// pass runs the blocks of every scan's view in turn, with coherent loads of
+// the ray records (COH: written by other blocks of that launch).
+template <typename VT, bool STOCH, int BY, bool TL, int UNR, bool TB, bool COH = false>
 __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __restrict__ PX,
                                            const float* __restrict__ PY, const float* __restrict__ PZ,
                                            const float2* __restrict__ RT, int bx, int by, int bz,
@@ -319,21 +327,55 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     // the run of detector columns whose ray column crosses this voxel column
     const float4* __restrict__ colt = g.colt + (long long)view * g.R;
     int ua = uhi + 1, ub = ulo - 1;
+    float amin = 1.0f, bmax = 0.0f;   // the run's alpha range inside the voxel column
     for (int uu = ulo; uu <= uhi; ++uu) {
         const float4 ct = __ldg(colt + uu);
         const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
         const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
-        if (fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)) > fmaxf(fminf(ax0, ax1), fminf(ay0, ay1))) {
+        const float a = fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), bb = fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1));
+        if (bb > a) {
             ua = min(ua, uu);
             ub = uu;
+            amin = fminf(amin, a);
+            bmax = fmaxf(bmax, bb);
         }
     }
     if (ua > ub) return;
     const int nrun = ub - ua + 1;   // every column of the run crosses the voxel column (bb > a)
+
+    // Candidate detector rows.  A cone-beam ray from source height zs meets
+    // height z at alpha where z = x1z + alpha (zs - x1z), so the ray of the
+    // row centred at x1z is inside the cell [z0, z1] at some alpha of the
+    // run's range [amin, bmax] iff x1z lies between the least of
+    // zs + (z0 - zs) / (1 - alpha) and the greatest of zs + (z1 - zs) / (1 - alpha)
+    // over alpha = amin, bmax (both bounds are monotone in alpha).  Written
+    // as z + (z - zs) m, m = alpha / (1 - alpha), it is the corner estimate's
+    // form with the corners' magnifications replaced by the run's alpha
+    // range.  The rows whose centre lies in that span widened by ROW_EPS rows
+    // (the float error of the span is below 1e-3 rows; a row the projector
+    // takes as level, |x1z - zs| < 1e-6 vz, sits inside it) are a superset of
+    // the rows with a positive chord; the corner estimate rounds to the
+    // nearest row instead, half a row of margin each side.  Both are bounds,
+    // not sums: they use fused multiply-adds (their rounding, below 1e-4
+    // rows, is inside either margin), and a detector height z maps to the
+    // row position z * inv_dv - zmin * inv_dv, offset by the margin.
+    float row_off = 0.5f;
+    if ((g.ct_style == 0 || g.ct_style == 3) && amin > 0.0f && bmax < 1.0f) {
+        mlo = __fdividef(amin, fs(1.0f, amin));
+        mhi = __fdividef(bmax, fs(1.0f, bmax));
+        row_off = ROW_EPS;
+    }
+    const float zrow0 = -fm(g.zmin, g.inv_dv);
+    const float zrow_lo = fs(zrow0, row_off), zrow_hi = fa(zrow0, row_off);
+    // the warp's longest run: the pair slots every detector row executes
+    const int nq = __reduce_max_sync(__activemask(), nrun);
+    // the run's alpha intervals; a slot beyond the run gets the empty interval
+    // [1, 0] (no chord with any row: hi - lo <= -1), so every thread of the
+    // warp runs the same pair slots without a test
     float ra[WALK_RUN], rb[WALK_RUN];
 #pragma unroll
     for (int q = 0; q < WALK_RUN; ++q) {
-        ra[q] = 0.f; rb[q] = 0.f;
+        ra[q] = 1.f; rb[q] = 0.f;
         if (ua + q <= ub) {
             const float4 ct = __ldg(colt + ua + q);
             const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
@@ -351,7 +393,7 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     float cmn = 0.f, cmx = 0.f;
     if (!TB) {
         const float z0 = PZ[kb + 1], zlo = fs(z0, g.srcz);
-        const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
+        const float a0 = __fmaf_rn(mlo, zlo, z0), a1 = __fmaf_rn(mhi, zlo, z0);
         cmn = fminf(a0, a1);
         cmx = fmaxf(a0, a1);
     }
@@ -372,6 +414,10 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     const long long vstep = TL ? 64LL * g.Mt * g.Nt : MN;
     VT* pv = vol + (TL ? (long long)tile_index(g, i, j, kb) : (long long)kb * MN + (long long)j * g.M + i);
     const float2* __restrict__ zrow = g.zcell + (long long)kb * g.ZP;
+    // the z run with NQ pair slots per detector row (NQ = the warp's longest
+    // run, at most WALK_RUN; longer runs take the rest from the column table)
+    auto z_run = [&](auto nq_c) {
+    constexpr int NQ = decltype(nq_c)::value;
     for (int k = kb; k < ke; ++k, pv += vstep, zrow += g.ZP) {
         int vlo = 0, vhi = -1;   // candidate rows (absolute row indices)
         float sw = 0.f, sl = 0.f;
@@ -386,18 +432,20 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
         };
         // the pairs of one detector row: its z-cell interval is loaded once and
         // met with every column of the run (columns ascending)
+        auto rec = [&](const float2* p) { return COH ? __ldca(p) : __ldg(p); };
         auto row_pairs = [&](int vv, float2 zc) {
             const float2* __restrict__ rr = rays + (long long)vv * R + ua;
 #pragma unroll
-            for (int q = 0; q < WALK_RUN; ++q)
-                if (q < nrun) pair(ra[q], rb[q], zc, __ldg(rr + q));
-            for (int q = WALK_RUN; q < nrun; ++q) {   // runs longer than the registers hold
-                const float4 ct = __ldg(colt + ua + q);
-                const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
-                const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
-                pair(fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)), zc,
-                     __ldg(rr + q));
-            }
+            for (int q = 0; q < NQ; ++q)   // a slot beyond the run reads the run's last record (no chord)
+                pair(ra[q], rb[q], zc, rec(rr + min(q, nrun - 1)));
+            if (NQ == WALK_RUN)
+                for (int q = WALK_RUN; q < nrun; ++q) {   // runs longer than the registers hold
+                    const float4 ct = __ldg(colt + ua + q);
+                    const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
+                    const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+                    pair(fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)), zc,
+                         rec(rr + q));
+                }
         };
         // every pair of the voxel, row by row (rows ascending), the order the
         // oracle's gather sums them
@@ -424,29 +472,27 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
         // through the cell between planes z0 and z1
         auto band_rows = [&](float z0, float z1, float zs, int row0) -> bool {
             const float zlo = fs(z0, zs), zhi = fs(z1, zs);
-            const float a0 = fa(fm(mlo, zlo), z0), a1 = fa(fm(mhi, zlo), z0);
-            const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
+            const float a0 = __fmaf_rn(mlo, zlo, z0), a1 = __fmaf_rn(mhi, zlo, z0);
+            const float b0 = __fmaf_rn(mlo, zhi, z1), b1 = __fmaf_rn(mhi, zhi, z1);
             const float zmn = fminf(fminf(a0, a1), fminf(b0, b1)), zmx = fmaxf(fmaxf(a0, a1), fmaxf(b0, b1));
-            int lo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
-            int hi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
-            if ((lo < 0 && hi < 0) || (lo > g.nvr - 1 && hi > g.nvr - 1)) return false;
-            vlo = row0 + max(lo, 0);
-            vhi = row0 + min(hi, g.nvr - 1);
+            const int lo = max(__float2int_ru(__fmaf_rn(zmn, g.inv_dv, zrow_lo)), 0);
+            const int hi = min(__float2int_rd(__fmaf_rn(zmx, g.inv_dv, zrow_hi)), g.nvr - 1);
+            if (lo > hi) return false;
+            vlo = row0 + lo;
+            vhi = row0 + hi;
             return true;
         };
         if (!TB) {
             // candidate detector rows of voxel k
             const float z1 = PZ[k + 2], zhi = fs(z1, g.srcz);
-            const float b0 = fa(fm(mlo, zhi), z1), b1 = fa(fm(mhi, zhi), z1);
+            const float b0 = __fmaf_rn(mlo, zhi, z1), b1 = __fmaf_rn(mhi, zhi, z1);
             const float bmn = fminf(b0, b1), bmx = fmaxf(b0, b1);
             const float zmn = fminf(cmn, bmn), zmx = fmaxf(cmx, bmx);
             cmn = bmn;
             cmx = bmx;
-            vlo = __float2int_rd(fa(fm(fs(zmn, g.zmin), g.inv_dv), 0.5f));
-            vhi = __float2int_rd(fa(fm(fs(zmx, g.zmin), g.inv_dv), 0.5f));
-            if ((vlo < 0 && vhi < 0) || (vlo > g.ZP - 1 && vhi > g.ZP - 1)) continue;
-            vlo = max(vlo, 0);
-            vhi = min(vhi, g.ZP - 1);
+            vlo = max(__float2int_ru(__fmaf_rn(zmn, g.inv_dv, zrow_lo)), 0);
+            vhi = min(__float2int_rd(__fmaf_rn(zmx, g.inv_dv, zrow_hi)), g.ZP - 1);
+            if (vlo > vhi) continue;
             const float old = Store<VT>::ldw(pv);   // loaded ahead: its latency overlaps the pairs
             all_pairs();
             if (!(sl < g.thr_bp)) {                                            // :799-806
@@ -495,6 +541,14 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
                 else Store<VT>::st(p, nv);
             }
         }
+    }
+    };
+    if (nq <= 2) {
+        if (nq <= 1) z_run(std::integral_constant<int, 1>());
+        else z_run(std::integral_constant<int, 2>());
+    } else {
+        if (nq == 3) z_run(std::integral_constant<int, 3>());
+        else z_run(std::integral_constant<int, WALK_RUN>());
     }
 }
 
@@ -692,95 +746,150 @@ __host__ __device__ __forceinline__ size_t fp_table_floats(const DevGeom& g)
 }
 size_t batch_pass_smem(const DevGeom& g) { return sizeof(float) * fp_table_floats(g) + bp_smem(g); }
 
-constexpr unsigned kBarrierSpins = 1u << 24;   // x ~100 ns: a wait gives up after about 2 s
+constexpr unsigned long long kIdleNs = 4000000000ull;   // a block idles at most 4 s (by the global timer)
 
-// The CTAs of one scan meet: each block arrives once its threads are done
-// with the phase, then waits until all nc blocks of the scan have arrived
-// (target = nc x the number of phases so far).  The wait is bounded: past
-// kBarrierSpins polls, or once any block has flagged an error, it sets
-// ERR_BARRIER and returns false, and the caller leaves.  The launch is
-// cooperative, so all the scan's blocks are resident and a wait only gives
-// up if something else went wrong.
-__device__ __forceinline__ bool scan_barrier(unsigned* bar, unsigned target, unsigned* err)
+__device__ __forceinline__ unsigned long long global_ns()
 {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();   // this block's writes of the phase, before its arrival
-        atomicAdd(bar, 1u);
-        int good = 1;
-        for (unsigned spins = 0;; ++spins) {
-            if (*(volatile unsigned*)bar >= target) break;
-            if (*(volatile unsigned*)err != 0u || spins > kBarrierSpins) {
-                atomicOr(err, ERR_BARRIER);
-                good = 0;
-                break;
-            }
-            __nanosleep(100);
-        }
-        __threadfence();   // the other blocks' writes, after the wait
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
-// The SART pass of every scan of a batch in one launch.  Block b serves the
-// scan whose CTA range holds it; per view its share of the forward blocks,
-// a barrier, its share of the walk's blocks, a barrier.  Each block runs
-// exactly the per-ray and per-voxel code of k_forward (shape 1) and
-// k_sart_walk (shape 1), so every scan's result equals its solver's.
+// blocks of phase ph of a scan: view ph/2's forward projection (even) or walk (odd)
+__device__ __forceinline__ unsigned flow_blocks(const BatchScan& S, unsigned ph)
+{
+    return (ph & 1u) ? (unsigned)(S.bp_gx * S.bp_gy * S.bp_gz) : (unsigned)(S.fp_gx * S.fp_gy);
+}
+
+// Thread 0 of a block: claim one block of work, from the home scan first,
+// then round the other scans; returns the scan (phase and block in ph, blk),
+// or -1 once every scan is done or an error was flagged.  With nothing to
+// claim (every scan's current phase handed out, its last blocks still
+// running) it polls again after a sleep that doubles up to 4 us; idle past
+// kIdleNs it flags ERR_BARRIER and returns -1.
+__device__ __forceinline__ int flow_claim(const BatchScan* __restrict__ scans, int nscans, int home,
+                                          BatchFlow* flow, unsigned* finished, unsigned* err, unsigned& ph, int& blk)
+{
+    unsigned sleep_ns = 64;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (*(volatile unsigned*)err != 0u || *(volatile unsigned*)finished >= (unsigned)nscans) return -1;
+        for (int t = 0; t < nscans; ++t) {
+            const int s = home + t < nscans ? home + t : home + t - nscans;
+            const BatchScan& S = scans[s];
+            const unsigned last = 2u * (unsigned)S.nviews;
+            const unsigned long long w = *(volatile unsigned long long*)&flow[s].claim;
+            const unsigned p = (unsigned)(w >> 32);
+            if (p >= last || (unsigned)w >= flow_blocks(S, p)) continue;
+            const unsigned long long o = atomicAdd(&flow[s].claim, 1ull);
+            const unsigned p2 = (unsigned)(o >> 32);
+            if (p2 < last && (unsigned)o < flow_blocks(S, p2)) {
+                ph = p2;
+                blk = (int)(unsigned)o;
+                return s;
+            }
+        }
+        if (global_ns() - t0 > kIdleNs) {
+            atomicOr(err, ERR_BARRIER);
+            return -1;
+        }
+        __nanosleep(sleep_ns);
+        sleep_ns = min(2u * sleep_ns, 4096u);
+    }
+}
+
+// The SART pass of every scan of a batch in one launch, scheduled as a data
+// flow.  A scan's phases run in order (view j's forward projection, its
+// walk, view j+1's forward projection, ...); the blocks of a phase run in any
+// order on any CTA.  A CTA takes the next block of its home scan's current
+// phase, else of any other scan's, so no CTA waits while some scan has a
+// block to give.  The phase's last block to finish opens the next phase:
+// each block releases its writes (fence, then its count), the last one
+// resets the count and moves the claim word on (fence first); a CTA that
+// claims a block fences before reading (acquire), and reads the ray records
+// and volumes the launch writes with coherent loads.  Each block runs the
+// per-ray and per-voxel code of k_forward (shape 1) and k_sart_walk (shape
+// 1), every voxel sees its views in order, so every scan's result equals
+// its solver's.  No block waits for a particular other block, so the CTAs
+// need not be co-resident; an idle CTA's wait is bounded (flow_claim).
+// 5 blocks per SM: 96 registers hold the forward and walk code without
+// spills (80, at 6 per SM, spilled 250-400 bytes a thread).
 template <typename VT, int KIND, bool STOCH>
-__global__ void __launch_bounds__(128, 6)
-k_batch_pass(const BatchScan* __restrict__ scans, int nscans, unsigned* __restrict__ bars, unsigned* __restrict__ err)
+__global__ void __launch_bounds__(128, 5)
+k_batch_pass(const BatchScan* __restrict__ scans, int nscans, BatchFlow* __restrict__ flow,
+             unsigned* __restrict__ finished, unsigned* __restrict__ err)
 {
     extern __shared__ float sp[];
-    __shared__ int s_idx;
-    if (threadIdx.x == 0) {   // the last scan whose first block is at or before this one
+    __shared__ int s_scan, s_blk;
+    __shared__ unsigned s_ph;
+    int home = 0;
+    {   // the last scan whose first home CTA is at or before this one
         int lo = 0, hi = nscans - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (scans[mid].c0 <= (int)blockIdx.x) lo = mid;
             else hi = mid - 1;
         }
-        s_idx = lo;
+        home = lo;
     }
-    __syncthreads();
-    const BatchScan& S = scans[s_idx];
-    const DevGeom& g = S.g;
-    float *PX, *PY, *PZ, *PINF;
-    fp_tables(g, sp, PX, PY, PZ, PINF);
-    float *WX, *WY, *WZ;
-    float2* RT;
-    walk_tables(g, sp + fp_table_floats(g), WX, WY, WZ, RT);
-    __syncthreads();
-    const int local = (int)blockIdx.x - S.c0;
-    const int nfp = S.fp_gx * S.fp_gy, nbp = S.bp_gx * S.bp_gy * S.bp_gz;
-    const long long P = (long long)g.R * g.ZP;
-    const size_t per_view = (size_t)g.ZP * S.fp_gx;
-    const size_t bsz = S.b_dt == CTR_F32 ? 4 : 2;
-    unsigned target = 0;
-    for (int j = 0; j < S.nviews; ++j) {
-        for (int vb = local; vb < nfp; vb += S.nc)
-            fp_block<VT, KIND, false, 4, 0, true, false>(
+    int cur = -1;   // the scan whose tables are in shared memory
+    for (;;) {
+        if (threadIdx.x == 0) {
+            unsigned ph = 0;
+            int blk = 0;
+            const int s = flow_claim(scans, nscans, home, flow, finished, err, ph, blk);
+            __threadfence();   // acquire: the phase before ph is complete
+            s_scan = s;
+            s_ph = ph;
+            s_blk = blk;
+        }
+        __syncthreads();
+        const int s = s_scan;
+        if (s < 0) return;
+        const BatchScan& S = scans[s];
+        const DevGeom& g = S.g;
+        float *PX, *PY, *PZ, *PINF, *WX, *WY, *WZ;   // recomputed per block, not kept live across blocks
+        float2* RT;
+        if (s != cur) {   // this scan's plane tables
+            fp_tables(g, sp, PX, PY, PZ, PINF);
+            walk_tables(g, sp + fp_table_floats(g), WX, WY, WZ, RT);
+            __syncthreads();
+            cur = s;
+        }
+        plane_tables_addr(g, sp, PX, PY, PZ, PINF);
+        walk_tables_addr(g, sp + fp_table_floats(g), WX, WY, WZ, RT);
+        const unsigned ph = s_ph;
+        const int vb = s_blk, j = (int)(ph >> 1);
+        if ((ph & 1u) == 0u) {
+            const long long P = (long long)g.R * g.ZP;
+            const size_t per_view = (size_t)g.ZP * S.fp_gx;
+            const size_t bsz = S.b_dt == CTR_F32 ? 4 : 2;
+            fp_block<VT, KIND, false, 4, 0, true, false, true>(
                 g, PX, PY, PZ, PINF, vb % S.fp_gx, vb / S.fp_gx, 0, S.fp_gx, S.fp_gy, (const VT*)S.fp_vol, j, S.rays,
                 0, (const char*)S.b + (size_t)j * P * bsz, S.b_dt,
                 S.partial ? S.partial + (size_t)j * per_view : nullptr, nullptr, nullptr, nullptr,
                 (const VT*)S.fp_vol2, S.ax ? S.ax + (size_t)j * P : nullptr, S.gdev);
-        target += (unsigned)S.nc;
-        if (!scan_barrier(bars + s_idx, target, err)) return;
-        const uint32_t seed = STOCH ? *S.pass_seed * 0x9E3779B9u + (uint32_t)j : 0u;
-        for (int vb = local; vb < nbp; vb += S.nc) {
+        } else {
+            const uint32_t seed = STOCH ? *S.pass_seed * 0x9E3779B9u + (uint32_t)j : 0u;
             const int bx = vb % S.bp_gx, r = vb / S.bp_gx, by = r % S.bp_gy, bz = r / S.bp_gy;
             if (g.ct_style == 3)
-                walk_block<VT, STOCH, 4, true, 1, true>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol, S.rays, j,
-                                                        S.beta, seed, S.zl);
+                walk_block<VT, STOCH, 4, true, 1, true, true>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol, S.rays,
+                                                              j, S.beta, seed, S.zl);
             else
-                walk_block<VT, STOCH, 4, true, 1, false>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol, S.rays, j,
-                                                         S.beta, seed, S.zl);
+                walk_block<VT, STOCH, 4, true, 1, false, true>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol,
+                                                               S.rays, j, S.beta, seed, S.zl);
         }
-        target += (unsigned)S.nc;
-        if (!scan_barrier(bars + s_idx, target, err)) return;
+        __syncthreads();   // the block's writes are issued
+        if (threadIdx.x == 0) {
+            __threadfence();   // release them
+            const unsigned d = atomicAdd(&flow[s].done, 1u) + 1u;
+            if (d == flow_blocks(S, ph)) {   // the phase's last block opens the next
+                atomicExch(&flow[s].done, 0u);
+                __threadfence();
+                atomicExch(&flow[s].claim, (unsigned long long)(ph + 1u) << 32);
+                if (ph + 1u == 2u * (unsigned)S.nviews) atomicAdd(finished, 1u);
+            }
+        }
     }
 }
 
@@ -820,21 +929,18 @@ int batch_pass_blocks_per_sm(ctr_dtype vdt, int kind, bool stoch, size_t smem)
 }
 
 ctr_status launch_batch_pass(const BatchScan* d_scans, int nscans, int nblocks, ctr_dtype vdt, int kind, bool stoch,
-                             unsigned* bars, unsigned* err, size_t smem, cudaStream_t st)
+                             void* flow, unsigned* err, size_t smem, cudaStream_t st)
 {
     const void* f = batch_pass_kernel(vdt, kind, stoch);
     if (!f) return set_error(CTR_ERR_UNSUPPORTED, "persistent pass: storage type or kind not supported");
+    BatchFlow* fl = (BatchFlow*)flow;
+    unsigned* finished = (unsigned*)(fl + nscans);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nblocks);
     cfg.blockDim = dim3(128);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    void* args[] = {(void*)&d_scans, (void*)&nscans, (void*)&bars, (void*)&err};
+    void* args[] = {(void*)&d_scans, (void*)&nscans, (void*)&fl, (void*)&finished, (void*)&err};
     CTR_CUDA_TRY(cudaLaunchKernelExC(&cfg, f, args));
     return CTR_OK;
 }

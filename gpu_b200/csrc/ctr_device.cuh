@@ -18,21 +18,29 @@ __device__ __forceinline__ float fdv(float a, float b) { return __fdiv_rn(a, b);
 
 // storage <-> FP32
 template <typename T> struct Store;
+// ld: the read-only path (data no thread of the launch writes); ldc: a
+// coherent load (ld.global.ca) for data that other blocks of the same launch
+// wrote before an acquire (the batch's persistent pass).
 template <> struct Store<float> {
     static __device__ __forceinline__ float ld(const float* p) { return __ldg(p); }
+    static __device__ __forceinline__ float ldc(const float* p) { return __ldca(p); }
     static __device__ __forceinline__ float ldw(const float* p) { return *p; }
     static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
     static __device__ __forceinline__ float rn(float v) { return v; }
 };
 template <> struct Store<__nv_bfloat16> {
     static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+    static __device__ __forceinline__ float ldc(const __nv_bfloat16* p) { return __bfloat162float(__ldca(p)); }
     static __device__ __forceinline__ float ldw(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+    static __device__ __forceinline__ float rn(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
 };
 template <> struct Store<__half> {
     static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
+    static __device__ __forceinline__ float ldc(const __half* p) { return __half2float(__ldca(p)); }
     static __device__ __forceinline__ float ldw(const __half* p) { return __half2float(*p); }
     static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+    static __device__ __forceinline__ float rn(float v) { return __half2float(__float2half_rn(v)); }
 };
 
 // Stochastic rounding of an FP32 value to the storage type: add uniform random

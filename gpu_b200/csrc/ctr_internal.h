@@ -217,7 +217,12 @@ ctr_status launch_fgp(Geometry& g, void* vol, ctr_dtype dt, float lambda, int it
                       const float* gamma_dev = nullptr);
 ctr_status launch_momentum(const Geometry& g, void* y, void* xprev, const void* x, ctr_dtype dt,
                            float gam, cudaStream_t st, const float* gamma_dev = nullptr);
-// Refinement solver, after its SART pass (fgp.cu): xm = (1+g) xk - g xm + d
+// Refinement solver, before its SART pass (fgp.cu): the correction volume d
+// (tiled, dt storage) = d0, the dt rounding of (1+g)(xk - x~k) - g(xm - x~m)
+// with x~ the round-to-nearest dt copies (zero in FP32 storage).
+ctr_status launch_refine_start(Geometry& g, const float* xk, const float* xm, void* d_tiled, ctr_dtype dt,
+                               const float* gdev, cudaStream_t st);
+// Refinement solver, after its SART pass (fgp.cu): xm = (1+g) xk - g xm + (d - d0)
 // (d tiled, dt storage), then with lam > 0 and iters >= 0 the FGP-TV prox of
 // that FP32 volume (duals in dt storage), and x* (the prox, or the sum when
 // lam == 0) rotated in: xm = xk, xk = x*, xt = the dt copy of x* (tiled).
@@ -226,11 +231,12 @@ ctr_status launch_refine_update(Geometry& g, float* xk, float* xm, const void* d
 // *p = v on the device (a per-iteration scalar that graphs read)
 ctr_status launch_set_scalar(float* p, float v, cudaStream_t st);
 
-// One scan of the batch's persistent SART pass (bp.cu): the scan's CTAs
-// [c0, c0 + nc) run, view after view, the blocks of its forward projection
-// (fp_gx x fp_gy blocks of 32 x 4 rays), a barrier of the scan's CTAs, the
-// blocks of its walk (bp_gx x bp_gy x bp_gz blocks of 32 x 4 voxel columns,
-// z runs of zl), a barrier.
+// One scan of the batch's persistent SART pass (bp.cu): view after view, the
+// blocks of its forward projection (fp_gx x fp_gy blocks of 32 x 4 rays),
+// then the blocks of its walk (bp_gx x bp_gy x bp_gz blocks of 32 x 4 voxel
+// columns, z runs of zl).  CTAs [c0, c0 + nc) take this scan's blocks first
+// (its home CTAs, a share proportional to its work) and any other scan's
+// when it has none to give.
 struct BatchScan {
     DevGeom g;
     const void* fp_vol;          // the volume the projection reads (tiled)
@@ -249,14 +255,25 @@ struct BatchScan {
     int fp_gx, fp_gy;
     int bp_gx, bp_gy, bp_gz, zl;
 };
-constexpr unsigned ERR_BARRIER = 2u;   // a persistent pass's barrier wait gave up
+// The persistent pass's work counters of one scan: claim = (phase << 32) |
+// the next block of the phase to hand out, done = the phase's blocks
+// finished; phase 2j is view j's forward projection, 2j + 1 its walk.
+struct BatchFlow {
+    unsigned long long claim;
+    unsigned done;
+    unsigned pad;
+};
+// bytes of the persistent pass's zeroed state: one BatchFlow per scan and
+// the count of finished scans
+inline size_t batch_flow_bytes(int nscans) { return sizeof(BatchFlow) * (size_t)nscans + 16; }
+constexpr unsigned ERR_BARRIER = 2u;   // a persistent pass's block found no work for too long
 // Blocks per SM the persistent pass runs at (its occupancy), or 0.
 int batch_pass_blocks_per_sm(ctr_dtype vdt, int kind, bool stoch, size_t smem);
-// The persistent pass over every scan: one cooperative launch of nblocks
-// CTAs (all resident at once).  bars: one zeroed counter per scan; err: the
-// device error word (ERR_BARRIER when a barrier wait gives up).
+// The persistent pass over every scan: one launch of nblocks CTAs.  flow:
+// batch_flow_bytes(nscans) zeroed bytes; err: the device error word
+// (ERR_BARRIER when a block idles past its bound).
 ctr_status launch_batch_pass(const BatchScan* d_scans, int nscans, int nblocks, ctr_dtype vdt, int kind, bool stoch,
-                             unsigned* bars, unsigned* err, size_t smem, cudaStream_t st);
+                             void* flow, unsigned* err, size_t smem, cudaStream_t st);
 // shared memory of the persistent pass for one scan's geometry
 size_t batch_pass_smem(const DevGeom& g);
 // the walk's z run for a geometry (launch shape 1, shortened for small volumes)

@@ -119,6 +119,46 @@ k_fgp_final(int M, int N, int Z, T* __restrict__ vol, const T* __restrict__ o, c
 // Refinement solver: the FP32 input of the prox, y_k + d = (1+g) x_k - g x_(k-1) + d,
 // written over x_(k-1) (which is not needed after it).  d is read in the
 // projectors' tiled layout.
+// Refinement solver: the start d0 of the correction volume, the storage
+// rounding of y_k - y~_k = (1+g)(x_k - x~_k) - g (x_(k-1) - x~_(k-1)), where
+// x~ are the projectors' round-to-nearest copies of the FP32 iterates (the
+// pass projects y~_k through the copy of x_k and A x~_(k-1)).  With d
+// starting there, A (y~_k + d) is the projection of the FP32 y_k up to the
+// rounding of that small difference, so the copies' rounding does not bias
+// the fixed point.  Zero for FP32 storage.
+template <typename T>
+__device__ __forceinline__ float refine_d0(float xk, float xm, float gm)
+{
+    const float e = fs(fm(fa(1.0f, gm), fs(xk, Store<T>::rn(xk))), fm(gm, fs(xm, Store<T>::rn(xm))));
+    return Store<T>::rn(e);
+}
+
+// d = d0 in the tiled layout, one thread per tiled element (padding zero).
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_refine_start(const DevGeom g, const float* __restrict__ xk, const float* __restrict__ xm,
+               const float* __restrict__ gdev, T* __restrict__ d)
+{
+    const float gm = *gdev;
+    const long long n = tiled_count(g);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int w = (int)(t & 63);
+        const long long tile = t >> 6;
+        const int tx = (int)(tile % g.Mt);
+        const long long r = tile / g.Mt;
+        const int ty = (int)(r % g.Nt);
+        const int k = (int)(r / g.Nt);
+        const int i = tx * 8 + (w & 7), j = ty * 8 + (w >> 3);
+        float v = 0.0f;
+        if (i < g.M && j < g.N) {
+            const long long p = ((long long)k * g.N + j) * g.M + i;
+            v = refine_d0<T>(xk[p], xm[p], gm);
+        }
+        Store<T>::st(d + t, v);
+    }
+}
+
+// z = y_k + (d - d0) in FP32 into xm (FGP's input).
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_refine_sum(const DevGeom g, const float* __restrict__ xk, float* __restrict__ xm, const T* __restrict__ d,
@@ -128,8 +168,9 @@ k_refine_sum(const DevGeom g, const float* __restrict__ xk, float* __restrict__ 
     const long long MN = (long long)g.M * g.N, n = MN * g.Z;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(p % g.M), y = (int)((p / g.M) % g.N), z = (int)(p / MN);
-        const float yk = fs(fm(fa(1.0f, gm), xk[p]), fm(gm, xm[p]));
-        xm[p] = fa(yk, Store<T>::ld(d + tile_index(g, x, y, z)));
+        const float xkv = xk[p], xmv = xm[p];
+        const float yk = fs(fm(fa(1.0f, gm), xkv), fm(gm, xmv));
+        xm[p] = fa(yk, fs(Store<T>::ld(d + tile_index(g, x, y, z)), refine_d0<T>(xkv, xmv, gm)));
     }
 }
 
@@ -255,6 +296,15 @@ ctr_status launch_refine_update(Geometry& G, float* xk, float* xm, const void* d
             k_refine_final<T, false><<<nb, 256, 0, st>>>(G.dg, xk, xm, nullptr, nullptr, nullptr, 0.f, (T*)xt_tiled);
         }
     });
+    CTR_CUDA_TRY(cudaGetLastError());
+    return CTR_OK;
+}
+
+ctr_status launch_refine_start(Geometry& G, const float* xk, const float* xm, void* d_tiled, ctr_dtype dt,
+                               const float* gdev, cudaStream_t st)
+{
+    const int nb = grid_for(tiled_count(G.dg), 256);
+    CTR_DISPATCH_DTYPE(dt, T, { k_refine_start<T><<<nb, 256, 0, st>>>(G.dg, xk, xm, gdev, (T*)d_tiled); });
     CTR_CUDA_TRY(cudaGetLastError());
     return CTR_OK;
 }

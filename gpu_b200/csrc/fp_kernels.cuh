@@ -54,13 +54,18 @@ struct RayResult {
 
 // Shared plane tables with one padding entry before and after each table,
 // then the +inf slot: 1 + (M+3) + 2 + (N+3) + 2 + (Z+3) + 1 + 1 floats.
-__device__ __forceinline__ void plane_tables_layout(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
-                                                    float*& PINF)
+__device__ __forceinline__ void plane_tables_addr(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
+                                                  float*& PINF)
 {
     PX = sp + 1;
     PY = PX + (g.M + 3) + 2;
     PZ = PY + (g.N + 3) + 2;
     PINF = PZ + (g.Z + 3) + 1;
+}
+__device__ __forceinline__ void plane_tables_layout(const DevGeom& g, float* sp, float*& PX, float*& PY, float*& PZ,
+                                                    float*& PINF)
+{
+    plane_tables_addr(g, sp, PX, PY, PZ, PINF);
     for (int t = threadIdx.x; t < g.M + g.N + g.Z + 16; t += blockDim.x) sp[t] = 0.f;
     __syncthreads();
 }
@@ -94,7 +99,7 @@ __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, 
 // step rule are the same code, so every ray visits the same voxels.  The sums
 // round differently from the reference's sequence (within 1e-5 relative).
 template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false, int CPM = 0, bool TL = false,
-          bool DUAL = false, bool FAST = false>
+          bool DUAL = false, bool FAST = false, bool COH = false>
 __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
                                             const float* __restrict__ PY, const float* __restrict__ PZ,
                                             const float* __restrict__ PINF, const VT* __restrict__ vol, float s,
@@ -281,10 +286,10 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
         const float m = fminf(fminf(ax, ay), az);
         if (FAST && LOAD) {   // alpha steps, d12 applied after the loop
             const float da = fs(m, ac);
-            const float f = Store<VT>::ld(vol + idx);
+            const float f = COH ? Store<VT>::ldc(vol + idx) : Store<VT>::ld(vol + idx);
             sum = __fmaf_rn(seg_p, f_p, sum);                          // +0 on the first step
             if (DUAL) {
-                const float f2 = Store<VT>::ld(vol2 + idx);
+                const float f2 = COH ? Store<VT>::ldc(vol2 + idx) : Store<VT>::ld(vol2 + idx);
                 sum2 = __fmaf_rn(seg_p, f2_p, sum2);
                 f2_p = f2;
             }
@@ -294,11 +299,11 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
             const float seg = fm(d12, fs(m, ac));
             len = fa(len, seg);
             if (LOAD) {
-                const float f = Store<VT>::ld(vol + idx);
+                const float f = COH ? Store<VT>::ldc(vol + idx) : Store<VT>::ld(vol + idx);
                 if (ACC64) dsum = __fma_rn((double)seg_p, (double)f_p, dsum);   // +0 on the first step
                 else sum = fa(sum, fm(seg_p, f_p));
                 if (DUAL) {
-                    const float f2 = Store<VT>::ld(vol2 + idx);
+                    const float f2 = COH ? Store<VT>::ldc(vol2 + idx) : Store<VT>::ld(vol2 + idx);
                     sum2 = fa(sum2, fm(seg_p, f2_p));
                     f2_p = f2;
                 }
@@ -393,8 +398,9 @@ __device__ __forceinline__ void fp_tables(const DevGeom& g, float* sp, float*& P
 // One block of the forward projection: block (bx, by, bz) of a (gx, gy, *)
 // grid of FP_BX x BY rays (bz: the view offset), with the plane tables in
 // shared memory.  k_forward runs it as its own block; the batch's persistent
-// pass runs the blocks of every scan's view in turn.
-template <typename VT, int KIND, bool E64, int BY, int CPM, bool TL, bool FAST>
+// pass runs the blocks of every scan's view in turn, with coherent volume
+// loads (COH: the volumes were written by other blocks of that launch).
+template <typename VT, int KIND, bool E64, int BY, int CPM, bool TL, bool FAST, bool COH = false>
 __device__ __forceinline__ void fp_block(const DevGeom& g, const float* __restrict__ PX, const float* __restrict__ PY,
                                          const float* __restrict__ PZ, const float* __restrict__ PINF, int bx, int by,
                                          int bz, int gx, int gy, const VT* __restrict__ vol, int view0,
@@ -419,7 +425,7 @@ __device__ __forceinline__ void fp_block(const DevGeom& g, const float* __restri
         ((float2*)out)[p] = make_float2(0.0f, 0.0f);
     } else if (active) {
         const float2 sc = g.trig[view0 + w];
-        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, DUAL, FAST>(
+        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, DUAL, FAST, COH>(
             g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v, vol2);
         const bool zero = rr.len < g.thr_fp;                       // :554
         if (KIND == FP_PARTIAL) {

@@ -371,15 +371,18 @@ ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, const float* y
  *
  * refine = 1, mixed-precision iterative refinement (vol_dtype BF16 or F16;
  * allowed with F32): the FISTA state x_k, x_(k-1) stays in FP32 and is
- * touched once per iteration.  The projectors read a vol_dtype copy of x_k
- * and accumulate the SART pass into a vol_dtype correction volume d that
- * starts at zero: per view j, c = (b_j - A_j y_k - A_j d)/len, where
- * A_j y_k = (1+g) A_j x_k - g A_j x_(k-1) (g the FISTA factor (t-1)/t_k),
- * A_j x_k is summed in the same traversal as A_j d, and A_j x_(k-1) is kept
- * from the previous pass in an FP32 sinogram.  The residual b - A y is thus
- * formed in FP32 against the estimate itself, and no per-view update is
- * rounded against the (large) stored estimate, only against d (the
- * iteration's change).  After the pass x_(k+1) = FGP(y_k + d) in FP32.  In
+ * touched once per iteration.  The projectors read the round-to-nearest
+ * vol_dtype copies x~ of the iterates and accumulate the SART pass into a
+ * vol_dtype correction volume d: per view j, c = (b_j - A_j y~_k - A_j d)/len,
+ * where A_j y~_k = (1+g) A_j x~_k - g A_j x~_(k-1) (g the FISTA factor
+ * (t-1)/t_k), A_j x~_k is summed in the same traversal as A_j d, and
+ * A_j x~_(k-1) is kept from the previous pass in an FP32 sinogram.  d starts
+ * at d0, the vol_dtype rounding of y_k - y~_k (the copies' own rounding
+ * errors, each at most half a vol_dtype ulp), so that y~_k + d is the FP32 y_k to
+ * within the rounding of that small difference: the residual is formed in
+ * FP32 against the estimate itself, and no per-view update is rounded
+ * against the (large) stored estimate, only against d (the iteration's
+ * change).  After the pass x_(k+1) = FGP(y_k + (d - d0)) in FP32.  In
  * exact arithmetic this is the same iteration as refine = 0.  The fidelity of
  * the objective is that of the vol_dtype copy of x_k the pass projects, the TV
  * that of the FP32 x_k.  Workspace: two FP32 volumes and one FP32 sinogram.
@@ -473,13 +476,16 @@ ctr_status ctr_batch_get_volume(ctr_batch* b, int scan, void* dst, void* stream)
 /* ctr_solver_get_volume_f32 of one scan. */
 ctr_status ctr_batch_get_volume_f32(ctr_batch* b, int scan, float* dst, void* stream);
 /* on = 1: from the next ctr_batch_iterate, the SART views of every scan run
- * in one persistent launch per iteration: a cooperative grid of as many
- * blocks as the GPU holds at once, split among the scans in proportion to
- * their work; each scan's blocks run its views in order, the forward
- * projection's blocks, a barrier of the scan's blocks, the update's blocks,
- * a barrier.  The per-ray and per-voxel code is the single-scan kernels'
- * (launch shape 1), so every scan's result is unchanged.  The barrier waits
- * are bounded: one that gives up (about 2 s) makes ctr_batch_iterate return
+ * in one persistent launch per iteration, as many blocks as the GPU holds at
+ * once, scheduled as a data flow: each scan's phases (view j's forward
+ * projection, then its update, then view j+1's projection, ...) run in
+ * order, the blocks of a phase on any block of the launch; a block takes
+ * work from its home scan (the blocks are split among the scans in
+ * proportion to their work) and from any other scan when its own has none to
+ * give, and the last block of a phase to finish opens the next.  The per-ray
+ * and per-voxel code is the single-scan kernels' (launch shape 1), so every
+ * scan's result is unchanged.  A block that finds no work for 4 s (nothing
+ * legitimate takes that long) stops the pass, and ctr_batch_iterate returns
  * CTR_ERR_TIMEOUT.  Refused (CTR_ERR_UNSUPPORTED) for scans with
  * CTR_SART_REFERENCE_BP, slabs, CTR_GEOM_ENTRY_F64 or CTR_GEOM_FAST_SUMS, or
  * more scans than resident blocks.  on = 0: one kernel per view and scan, the

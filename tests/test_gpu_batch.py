@@ -42,7 +42,8 @@ def test_batch_equals_single_solver(dtype, persistent, oracle_built):
     """bf16_sr: stochastic rounding, whose per-pass seed the batch reads from
     device memory; the single-scan solver issues those passes directly.
     persistent: the SART views of all scans in one persistent launch per
-    iteration (ctr_batch_set_persistent), the same per-ray and per-voxel code."""
+    iteration (ctr_batch_set_persistent), its blocks handed out as a data
+    flow over the scans' phases, the same per-ray and per-voxel code."""
     import gpu_b200
     vdt = {"f32": gpu_b200.F32, "f16": gpu_b200.F16, "bf16_sr": gpu_b200.BF16, "f16_refine": gpu_b200.F16}[dtype]
     tdt = {"f32": torch.float32, "f16": torch.float16, "bf16_sr": torch.bfloat16, "f16_refine": torch.float16}[dtype]

@@ -8,7 +8,8 @@ each view's update is small against the stored voxel value, so a volume
 stored in FP16/BF16 loses part of every update to rounding and the error
 grows with the iteration count.  The refinement solver (``refine=True``)
 keeps the FISTA state in FP32 and rounds each view's update only against the
-pass's correction volume, which starts at zero; it meets the bar at 20
+pass's correction volume, which starts at the 16-bit copies' own rounding of
+the estimate (so that rounding does not bias the result); it meets the bar at 20
 iterations with FP16 copies, and with BF16 copies when the correction's
 updates are rounded stochastically.  The plain 16-bit storage form is kept
 for short runs (5 iterations) and is shown to drift at 20."""

@@ -46,7 +46,9 @@ def refine_restated(o, b, beta, lam_tv, fgp_iters, n_iter, dtype, fista=True):
     fids = []
     for _ in range(n_iter):
         xc = store(xk, dtype)          # the projectors' copy of x_k
-        d = np.zeros_like(xk)
+        # d starts at the copies' rounding of y_k = (1+g) x_k - g x_(k-1)
+        d0 = store((F(1.0) + gm) * (xk - xc) - gm * (xm - store(xm, dtype)), dtype)
+        d = d0.copy()
         for j in range(nv):
             sx = o.forward_view(xc, j, 0)                    # A x~_k, zero below vz*1e-6
             sd = o.forward_view(d, j, 0)                     # A d (its rays above the threshold)
@@ -57,7 +59,7 @@ def refine_restated(o, b, beta, lam_tv, fgp_iters, n_iter, dtype, fista=True):
             ax[j] = sx
             d = store(o.backproject_gather(d, c, j, beta), dtype)
         fids.append(float(np.sum(((ax - b).astype(F) ** 2).astype(np.float64))))
-        z = ((F(1.0) + gm) * xk - gm * xm + d).astype(F)
+        z = ((F(1.0) + gm) * xk - gm * xm + (d - d0)).astype(F)
         xs = o.fgp(z, F(beta) * F(lam_tv), fgp_iters) if lam_tv > 0 else z
         xm, xk = xk, xs.astype(F)
         t_k = (F(1.0) + np.sqrt(F(1.0) + F(4.0) * t * t, dtype=F)) / F(2.0)
