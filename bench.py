@@ -50,6 +50,11 @@ def scan_config(world):
             "relaxation": BETA, "lambda_tv": LAMBDA_TV, "fgp_iters": FGP_ITERS}
 
 
+def refine_note(args):
+    """The refinement solver's correction volume, as the bench lines name it."""
+    return "FP32 correction volume" if args.refine == 2 else "16-bit correction volume"
+
+
 def view_noise(view, n, seed):
     """Unit Gaussian noise of one view (CPU generator seeded per view, so the
     CPU arm can draw its sample views' noise without the others)."""
@@ -65,6 +70,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mixed", choices=["f16", "bf16"], default="f16")
+    p.add_argument("--refine", type=int, choices=[1, 2], default=2,
+                   help="the 16-bit runs' refinement solver: 1 keeps the correction volume in the 16-bit type, "
+                        "2 in FP32")
     p.add_argument("--fast-sums", action="store_true",
                    help="the mixed-precision run (and --profile-views) with fused ray sums (CTR_GEOM_FAST_SUMS)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -497,7 +505,8 @@ def profile_views(args):
     del truth
     if args.profile_iteration:
         # the benchmark's mixed-precision form: the refinement solver
-        solver = gpu_b200.Solver(geom, gpu_b200.F16, beta=beta, lambda_tv=lam, fgp_iters=FGP_ITERS, refine=True)
+        solver = gpu_b200.Solver(geom, gpu_b200.F16, beta=beta, lambda_tv=lam, fgp_iters=FGP_ITERS,
+                                 refine=args.refine)
         solver.set_sinogram(sino16)
         solver.set_volume(None)
         t0 = time.perf_counter()
@@ -571,7 +580,7 @@ def run_batched(args):
             g.autotune(gpu_b200.BF16, n_views=2)
     flags = 0 if args.no_sr else gpu_b200.SART_STOCHASTIC_ROUND
     batch = gpu_b200.Batch(geoms, gpu_b200.BF16, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS,
-                           sart_flags=flags, refine=True)
+                           sart_flags=flags, refine=args.refine)
     for i, s in enumerate(sinos):
         batch.set_sinogram(i, s)
     iters = args.steps
@@ -630,8 +639,9 @@ def run_batched(args):
         "metric": "batched SART-FISTA-TV voxel-updates/s", "value": updates * 1000.0 / ms,
         "unit": "voxel-updates/s", "n_gpus": 1, "steps": iters, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16 storage for the projectors (refinement: FP32 FISTA state, FP16 sinogram), f32 arithmetic"
-                 + ("" if args.no_sr else ", stochastic rounding of the correction's updates"),
+        "dtype": f"bf16 storage for the projectors (refinement: FP32 FISTA state, {refine_note(args)}, FP16 "
+                 f"sinogram), f32 arithmetic"
+                 + ("" if args.no_sr or args.refine == 2 else ", stochastic rounding of the correction's updates"),
         "data": "synthetic",
         "config": {"workload": f"{len(specs)} uneven scans (volumes 64-256^3, 90-720 views, 96^2-384^2 detectors, "
                                f"DSO 600-1200 mm), one CUDA graph launch per iteration of all scans",
@@ -697,7 +707,7 @@ def run_large(args):
         tuned = geom.autotune(vdt, n_views=2)
         flags = gpu_b200.SART_STOCHASTIC_ROUND if mode == "bf16" else 0
         solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, sart_flags=flags,
-                                 refine=(mode != "f32"))
+                                 refine=0 if mode == "f32" else args.refine)
         solver.set_sinogram(sino)
         solver.set_volume(None)
         for _ in range(args.warmup):
@@ -749,8 +759,8 @@ def run_large(args):
             "unit": "iter/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": out["bf16"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "bf16 storage for the projectors (refinement: FP32 FISTA state, FP16 sinogram, stochastic "
-                     "rounding), f32 arithmetic",
+            "dtype": f"bf16 storage for the projectors (refinement: FP32 FISTA state, {refine_note(args)}, FP16 "
+                     f"sinogram" + (", stochastic rounding" if args.refine == 1 else "") + "), f32 arithmetic",
             "data": "synthetic",
             "config": {"workload": "1024^3 x 0.25 mm, 1024 views, 1024x1024 detector x 0.3 mm, DSO 1000 mm, "
                                    "DOD -500 mm, 100 seeded ellipsoids, noiseless Siddon sinogram",
@@ -1084,7 +1094,7 @@ def main():
     for mode, vdt, sino in (("f32", gpu_b200.F32, sino32), ("mixed", mixed_code, sino16)):
         tuned[mode] = geoms[mode].autotune(vdt, n_views=4)   # launch shapes; results do not depend on them
         solver = gpu_b200.Solver(geoms[mode], vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, fista=True,
-                                 objective=True, use_graph=True, refine=(mode == "mixed"),
+                                 objective=True, use_graph=True, refine=args.refine if mode == "mixed" else 0,
                                  sart_flags=gpu_b200.SART_STOCHASTIC_ROUND if vdt == gpu_b200.BF16 else 0)
         solver.set_sinogram(sino)
         solver.set_volume(None)
@@ -1220,7 +1230,7 @@ def main():
     side_steps = min(args.steps, 3)
     geoms["mixed"].set_shapes(tuned["mixed"]["fp_shape"], tuned["mixed"]["bp_shape"])
     noobj = gpu_b200.Solver(geoms["mixed"], mixed_code, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS,
-                            fista=True, objective=False, use_graph=True, refine=True)
+                            fista=True, objective=False, use_graph=True, refine=args.refine)
     noobj.set_sinogram(runs["mixed"]["sino"])
     noobj.set_volume(None)
     noobj.iterate(1)
@@ -1334,8 +1344,8 @@ def main():
             "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": f"{args.mixed} storage for the projectors (refinement: FP32 FISTA state, FP16 sinogram), "
-                     f"f32 arithmetic" + (", fused ray sums" if args.fast_sums else ""),
+            "dtype": f"{args.mixed} storage for the projectors (refinement: FP32 FISTA state, {refine_note(args)}, "
+                     f"FP16 sinogram), f32 arithmetic" + (", fused ray sums" if args.fast_sums else ""),
             "data": "synthetic",
             "config": scan_config(world),
             "accuracy_vs_fp64": mixed_acc,

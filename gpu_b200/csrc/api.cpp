@@ -750,6 +750,7 @@ struct ctr_solver {
     // (tiled); ax holds A x~ of the previous copy, one FP32 value per ray of
     // every view; gm is the FISTA factor of the coming pass (device: d_gm).
     bool refine = false;
+    ctr_dtype ddt = CTR_F32;   // the correction volume's type: vol_dtype, or FP32 (refine = 2)
     float* xk32 = nullptr;
     float* xm32 = nullptr;
     float* ax = nullptr;
@@ -771,6 +772,7 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
     CTR_TRY(need_slab(GE(geom)));
     if (!std::isfinite(p->beta) || !std::isfinite(p->lambda_tv) || p->lambda_tv < 0.f || p->fgp_iters < 0)
         return set_error(CTR_ERR_INVALID_ARGUMENT, "bad solver parameters");
+    if (p->refine < 0 || p->refine > 2) return set_error(CTR_ERR_INVALID_ARGUMENT, "refine must be 0, 1 or 2");
     ctr_solver* s = new (std::nothrow) ctr_solver();
     if (!s) return set_error(CTR_ERR_OUT_OF_MEMORY, "host allocation");
     s->g = GE(geom);
@@ -786,6 +788,7 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
         return CTR_OK;
     }
     s->refine = p->refine != 0;
+    s->ddt = p->refine == 2 ? CTR_F32 : vdt;
     const size_t bytes = s->g->nvox() * dtype_size(vdt);
     cudaError_t e;
     if (s->refine) {
@@ -801,7 +804,7 @@ extern "C" ctr_status ctr_solver_create(const ctr_geometry* geom, ctr_dtype vdt,
         }
     }
     if ((e = cudaMalloc(&s->y, bytes)) != cudaSuccess || (e = cudaMalloc(&s->xprev, bytes)) != cudaSuccess ||
-        (e = cudaMalloc(&s->yt, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess ||
+        (e = cudaMalloc(&s->yt, (size_t)tiled_count(s->g->dg) * dtype_size(s->refine ? s->ddt : vdt))) != cudaSuccess ||
         (e = cudaMalloc(&s->xt, (size_t)tiled_count(s->g->dg) * dtype_size(vdt))) != cudaSuccess ||
         (e = cudaMalloc(&s->d_obj, 4 * sizeof(double))) != cudaSuccess || (e = cudaMemset(s->y, 0, bytes)) != cudaSuccess ||
         (e = cudaMemset(s->xprev, 0, bytes)) != cudaSuccess ||
@@ -889,10 +892,17 @@ extern "C" ctr_status ctr_solver_set_volume(ctr_solver* s, const void* vol, void
     return CTR_OK;
 }
 
+// The refinement projection kind: the correction in the copies' type, or in
+// FP32 (refine = 2) while the copies are 16-bit.
+static FpKind refine_kind(const ctr_solver* s)
+{
+    return (s->ddt == CTR_F32 && s->vdt != CTR_F32) ? FP_SART_REFINE32 : FP_SART_REFINE;
+}
+
 // The refinement solver's SART pass: d = d0 (the copies' rounding of y_k),
 // then per view the projection of the copy xt and of d (FP_SART_REFINE: the
 // residual against y_k, A x~_k into ax, the objective partials of x~_k) and
-// the SART update of d.
+// the SART update of d (in its own type: FP32 d takes no stochastic rounding).
 static ctr_status refine_pass(ctr_solver* s, uint32_t seed, const uint32_t* pass_seed, const float* gdev,
                               cudaStream_t st)
 {
@@ -900,16 +910,17 @@ static ctr_status refine_pass(ctr_solver* s, uint32_t seed, const uint32_t* pass
     const long long P = g->npix();
     const size_t per_view = objective_partials_per_view(g->dg);
     CTR_TRY(ensure_rays(g, (size_t)P * sizeof(float2)));
-    CTR_TRY(launch_refine_start(*g, s->xk32, s->xm32, s->yt, s->vdt, gdev, st));
+    CTR_TRY(launch_refine_start(*g, s->xk32, s->xm32, s->yt, s->ddt, s->vdt, gdev, st));
+    const unsigned flags = s->ddt == CTR_F32 ? (s->p.sart_flags & ~CTR_SART_STOCHASTIC_ROUND) : s->p.sart_flags;
     for (int j = 0; j < g->desc.n_views; ++j) {
         FpArgs a{};
-        a.vol = s->xt; a.vol_dtype = s->vdt; a.view0 = j; a.nview = 1; a.kind = FP_SART_REFINE; a.tiled = 1;
+        a.vol = s->xt; a.vol_dtype = s->vdt; a.view0 = j; a.nview = 1; a.kind = refine_kind(s); a.tiled = 1;
         a.out = g->d_rays; a.b = (const char*)s->sino + (size_t)j * P * dtype_size(s->sdt); a.b_dtype = s->sdt;
         a.vol2 = s->yt; a.ax = s->ax + (size_t)j * P; a.gdev = gdev; a.partial = g->d_partial + (size_t)j * per_view;
         CTR_TRY(launch_forward(*g, a, st, nullptr));
         BpArgs b{};
-        b.vol = s->yt; b.vol_dtype = s->vdt; b.rays = g->d_rays; b.view0 = j; b.nview = 1; b.sart = 1;
-        b.flags = s->p.sart_flags; b.beta = s->p.beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j;
+        b.vol = s->yt; b.vol_dtype = s->ddt; b.rays = g->d_rays; b.view0 = j; b.nview = 1; b.sart = 1;
+        b.flags = flags; b.beta = s->p.beta; b.seed = seed * 0x9E3779B9u + (uint32_t)j;
         b.pass_seed = pass_seed; b.tiled = 1;
         CTR_TRY(launch_backproject(*g, b, st));
     }
@@ -1137,7 +1148,7 @@ extern "C" ctr_status ctr_solver_iterate(ctr_solver* s, int n, double* obj_out, 
                 s->obj_pending = false;
             }
             const float lam = s->p.lambda_tv > 0.f ? s->p.beta * s->p.lambda_tv : 0.f;
-            CTR_TRY(launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->xt, s->vdt, lam, s->p.fgp_iters, s->d_gm,
+            CTR_TRY(launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->ddt, s->xt, s->vdt, lam, s->p.fgp_iters, s->d_gm,
                                          st));
             const float t_k = (1.0f + sqrtf(1.0f + 4.0f * s->t * s->t)) / 2.0f;   // :372
             if (s->p.fista) {
@@ -1404,7 +1415,7 @@ static ctr_status solver_issue(ctr_solver* s, cudaStream_t st, const float* gam_
         if (fused)
             CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
         const float lam = s->p.lambda_tv > 0.f ? s->p.beta * s->p.lambda_tv : 0.f;
-        return launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->xt, s->vdt, lam, s->p.fgp_iters, gam_dev, st);
+        return launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->ddt, s->xt, s->vdt, lam, s->p.fgp_iters, gam_dev, st);
     }
     if (fused) {
         const void* xk1 = s->p.fista ? s->xprev : s->y;
@@ -1426,7 +1437,7 @@ static ctr_status batch_pre(ctr_solver* s, cudaStream_t st, bool fused, const fl
     Geometry* g = s->g;
     if (s->refine) {
         if (fused) CTR_TRY(launch_tv(*g, s->xk32, CTR_F32, g->d_partial, 148 * 64, s->d_obj + 1, st));
-        return launch_refine_start(*g, s->xk32, s->xm32, s->yt, s->vdt, gam_dev, st);
+        return launch_refine_start(*g, s->xk32, s->xm32, s->yt, s->ddt, s->vdt, gam_dev, st);
     }
     if (fused) {
         const void* xk1 = s->p.fista ? s->xprev : s->y;
@@ -1444,7 +1455,7 @@ static ctr_status batch_post(ctr_solver* s, cudaStream_t st, const float* gam_de
         CTR_TRY(launch_reduce(g->d_partial, objective_partials_per_view(g->dg) * g->desc.n_views, s->d_obj, st));
     if (s->refine) {
         const float lam = s->p.lambda_tv > 0.f ? s->p.beta * s->p.lambda_tv : 0.f;
-        return launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->xt, s->vdt, lam, s->p.fgp_iters, gam_dev, st);
+        return launch_refine_update(*g, s->xk32, s->xm32, s->yt, s->ddt, s->xt, s->vdt, lam, s->p.fgp_iters, gam_dev, st);
     }
     return solver_prox(s, st, gam_dev);
 }
@@ -1497,7 +1508,7 @@ static void batch_drop_graph(ctr_batch* b, int which = -1)
 // The forward kind of the scans' passes in graph gi (the same for all scans).
 static int batch_pass_kind(const ctr_batch* b, int gi)
 {
-    return b->scans[0]->refine ? FP_SART_REFINE : (gi == 1 ? FP_SART_OBJ : FP_SART);
+    return b->scans[0]->refine ? refine_kind(b->scans[0]) : (gi == 1 ? FP_SART_OBJ : FP_SART);
 }
 
 // The scans' descriptions for the persistent pass of graph gi, and the
@@ -1562,7 +1573,10 @@ static ctr_status batch_describe(ctr_batch* b, int gi)
         c0 += nc[i];
         q.fp_gx = (G->dg.R + 31) / 32;
         q.fp_gy = (G->dg.ZP + 3) / 4;
-        q.zl = walk_z_run(G->dg);
+        // the full z run of 32 voxels: the scans fill the GPU together, so a
+        // small scan's run is not shortened to make blocks (fewer blocks to
+        // hand out, each column's setup shared by more voxels)
+        q.zl = std::min(32, G->dg.Z);
         q.bp_gx = (G->dg.M + 31) / 32;
         q.bp_gy = (G->dg.N + 3) / 4;
         q.bp_gz = (G->dg.Z + q.zl - 1) / q.zl;
@@ -1669,7 +1683,8 @@ extern "C" ctr_status ctr_batch_set_persistent(ctr_batch* b, int on)
     const bool stoch = (b->scans[0]->p.sart_flags & CTR_SART_STOCHASTIC_ROUND) != 0;
     int per_sm = 0;
     if (b->scans[0]->refine) {
-        per_sm = batch_pass_blocks_per_sm(vdt, FP_SART_REFINE, stoch, smem);
+        const FpKind k = refine_kind(b->scans[0]);
+        per_sm = batch_pass_blocks_per_sm(vdt, k, stoch && k == FP_SART_REFINE, smem);
     } else {
         per_sm = std::min(batch_pass_blocks_per_sm(vdt, FP_SART, stoch, smem),
                           batch_pass_blocks_per_sm(vdt, FP_SART_OBJ, stoch, smem));

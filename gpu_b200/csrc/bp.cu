@@ -867,17 +867,20 @@ k_batch_pass(const BatchScan* __restrict__ scans, int nscans, BatchFlow* __restr
             fp_block<VT, KIND, false, 4, 0, true, false, true>(
                 g, PX, PY, PZ, PINF, vb % S.fp_gx, vb / S.fp_gx, 0, S.fp_gx, S.fp_gy, (const VT*)S.fp_vol, j, S.rays,
                 0, (const char*)S.b + (size_t)j * P * bsz, S.b_dt,
-                S.partial ? S.partial + (size_t)j * per_view : nullptr, nullptr, nullptr, nullptr,
-                (const VT*)S.fp_vol2, S.ax ? S.ax + (size_t)j * P : nullptr, S.gdev);
+                S.partial ? S.partial + (size_t)j * per_view : nullptr, nullptr, nullptr, nullptr, S.fp_vol2,
+                S.ax ? S.ax + (size_t)j * P : nullptr, S.gdev);
         } else {
-            const uint32_t seed = STOCH ? *S.pass_seed * 0x9E3779B9u + (uint32_t)j : 0u;
+            // the updated volume: the FP32 correction of FP_SART_REFINE32, else the storage type
+            using WT = typename std::conditional<KIND == FP_SART_REFINE32, float, VT>::type;
+            constexpr bool WSTOCH = STOCH && !std::is_same<WT, float>::value;
+            const uint32_t seed = WSTOCH ? *S.pass_seed * 0x9E3779B9u + (uint32_t)j : 0u;
             const int bx = vb % S.bp_gx, r = vb / S.bp_gx, by = r % S.bp_gy, bz = r / S.bp_gy;
             if (g.ct_style == 3)
-                walk_block<VT, STOCH, 4, true, 1, true, true>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol, S.rays,
-                                                              j, S.beta, seed, S.zl);
+                walk_block<WT, WSTOCH, 4, true, 1, true, true>(g, WX, WY, WZ, RT, bx, by, bz, (WT*)S.bp_vol, S.rays,
+                                                               j, S.beta, seed, S.zl);
             else
-                walk_block<VT, STOCH, 4, true, 1, false, true>(g, WX, WY, WZ, RT, bx, by, bz, (VT*)S.bp_vol,
-                                                               S.rays, j, S.beta, seed, S.zl);
+                walk_block<WT, WSTOCH, 4, true, 1, false, true>(g, WX, WY, WZ, RT, bx, by, bz, (WT*)S.bp_vol,
+                                                                S.rays, j, S.beta, seed, S.zl);
         }
         __syncthreads();   // the block's writes are issued
         if (threadIdx.x == 0) {
@@ -909,6 +912,10 @@ static const void* batch_pass_kernel(ctr_dtype vdt, int kind, bool stoch)
             f = stoch ? batch_pass_fn<VT, FP_SART_OBJ, true>() : batch_pass_fn<VT, FP_SART_OBJ, false>();
         else if (kind == FP_SART_REFINE)
             f = stoch ? batch_pass_fn<VT, FP_SART_REFINE, true>() : batch_pass_fn<VT, FP_SART_REFINE, false>();
+        else if (kind == FP_SART_REFINE32) {   // FP32 correction: no stochastic rounding
+            if constexpr (std::is_same<VT, float>::value) f = batch_pass_fn<VT, FP_SART_REFINE, false>();
+            else f = batch_pass_fn<VT, FP_SART_REFINE32, false>();
+        }
     };
     if (vdt == CTR_F32) pick(float());
     else if (vdt == CTR_BF16) pick(__nv_bfloat16());

@@ -144,8 +144,10 @@ ctr_status check_device_errors(Geometry* g, cudaStream_t st);
 // x_k, vol2 the correction volume d; per ray c = (b - ((1+g)Ax_k - g Ax_(k-1))
 // - Ad)/len with g = *gdev and Ax_(k-1) read from ax[p], which is then
 // overwritten with Ax_k; the objective partials of x_k as FP_SART_OBJ.
+// FP_SART_REFINE32: FP_SART_REFINE with the correction volume (vol2) in FP32
+// while vol is a 16-bit copy.
 enum FpKind { FP_FORWARD = 0, FP_SART = 1, FP_OBJECTIVE = 2, FP_TRACE = 3, FP_DOT = 4, FP_SART_OBJ = 5,
-              FP_PARTIAL = 6, FP_SART_REFINE = 7 };
+              FP_PARTIAL = 6, FP_SART_REFINE = 7, FP_SART_REFINE32 = 8 };
 struct FpArgs {
     const void* vol; ctr_dtype vol_dtype;
     int view0, nview;
@@ -154,7 +156,8 @@ struct FpArgs {
     const void* b; ctr_dtype b_dtype;     // SART/OBJECTIVE: measured sinogram; DOT: y (offset to view0)
     double* partial;                      // OBJECTIVE, SART_OBJ: one double per warp (32 rays of a row),
                                           // [view - view0][v][u/32]; DOT: one per block
-    const void* vol2 = nullptr;           // SART_OBJ: the volume of the objective (same dtype, layout)
+    const void* vol2 = nullptr;           // SART_OBJ: the volume of the objective (same dtype, layout);
+                                          // SART_REFINE: the correction d (vol_dtype; FP32 for SART_REFINE32)
     int* nseg; uint64_t* hash; float* len;  // TRACE
     int tiled = 0;                        // vol in the 8x8-tiled layout (FORWARD, SART, OBJECTIVE)
     float* ax = nullptr;                  // SART_REFINE: FP32 ray sums of the previous x copy, this view
@@ -218,15 +221,16 @@ ctr_status launch_fgp(Geometry& g, void* vol, ctr_dtype dt, float lambda, int it
 ctr_status launch_momentum(const Geometry& g, void* y, void* xprev, const void* x, ctr_dtype dt,
                            float gam, cudaStream_t st, const float* gamma_dev = nullptr);
 // Refinement solver, before its SART pass (fgp.cu): the correction volume d
-// (tiled, dt storage) = d0, the dt rounding of (1+g)(xk - x~k) - g(xm - x~m)
-// with x~ the round-to-nearest dt copies (zero in FP32 storage).
-ctr_status launch_refine_start(Geometry& g, const float* xk, const float* xm, void* d_tiled, ctr_dtype dt,
-                               const float* gdev, cudaStream_t st);
+// (tiled, ddt storage: dt or FP32) = d0, the ddt rounding of
+// (1+g)(xk - x~k) - g(xm - x~m) with x~ the round-to-nearest dt copies (zero
+// for FP32 copies).
+ctr_status launch_refine_start(Geometry& g, const float* xk, const float* xm, void* d_tiled, ctr_dtype ddt,
+                               ctr_dtype dt, const float* gdev, cudaStream_t st);
 // Refinement solver, after its SART pass (fgp.cu): xm = (1+g) xk - g xm + (d - d0)
-// (d tiled, dt storage), then with lam > 0 and iters >= 0 the FGP-TV prox of
+// (d tiled, ddt storage), then with lam > 0 and iters >= 0 the FGP-TV prox of
 // that FP32 volume (duals in dt storage), and x* (the prox, or the sum when
 // lam == 0) rotated in: xm = xk, xk = x*, xt = the dt copy of x* (tiled).
-ctr_status launch_refine_update(Geometry& g, float* xk, float* xm, const void* d_tiled, void* xt_tiled,
+ctr_status launch_refine_update(Geometry& g, float* xk, float* xm, const void* d_tiled, ctr_dtype ddt, void* xt_tiled,
                                 ctr_dtype dt, float lam, int iters, const float* gdev, cudaStream_t st);
 // *p = v on the device (a per-iteration scalar that graphs read)
 ctr_status launch_set_scalar(float* p, float v, cudaStream_t st);

@@ -125,19 +125,20 @@ k_fgp_final(int M, int N, int Z, T* __restrict__ vol, const T* __restrict__ o, c
 // pass projects y~_k through the copy of x_k and A x~_(k-1)).  With d
 // starting there, A (y~_k + d) is the projection of the FP32 y_k up to the
 // rounding of that small difference, so the copies' rounding does not bias
-// the fixed point.  Zero for FP32 storage.
-template <typename T>
+// the fixed point.  T: the copies' type; TD: the correction's (T, or FP32).
+// Zero for FP32 copies.
+template <typename T, typename TD>
 __device__ __forceinline__ float refine_d0(float xk, float xm, float gm)
 {
     const float e = fs(fm(fa(1.0f, gm), fs(xk, Store<T>::rn(xk))), fm(gm, fs(xm, Store<T>::rn(xm))));
-    return Store<T>::rn(e);
+    return Store<TD>::rn(e);
 }
 
 // d = d0 in the tiled layout, one thread per tiled element (padding zero).
-template <typename T>
+template <typename T, typename TD>
 __global__ void __launch_bounds__(256)
 k_refine_start(const DevGeom g, const float* __restrict__ xk, const float* __restrict__ xm,
-               const float* __restrict__ gdev, T* __restrict__ d)
+               const float* __restrict__ gdev, TD* __restrict__ d)
 {
     const float gm = *gdev;
     const long long n = tiled_count(g);
@@ -152,16 +153,16 @@ k_refine_start(const DevGeom g, const float* __restrict__ xk, const float* __res
         float v = 0.0f;
         if (i < g.M && j < g.N) {
             const long long p = ((long long)k * g.N + j) * g.M + i;
-            v = refine_d0<T>(xk[p], xm[p], gm);
+            v = refine_d0<T, TD>(xk[p], xm[p], gm);
         }
-        Store<T>::st(d + t, v);
+        Store<TD>::st(d + t, v);
     }
 }
 
 // z = y_k + (d - d0) in FP32 into xm (FGP's input).
-template <typename T>
+template <typename T, typename TD>
 __global__ void __launch_bounds__(256)
-k_refine_sum(const DevGeom g, const float* __restrict__ xk, float* __restrict__ xm, const T* __restrict__ d,
+k_refine_sum(const DevGeom g, const float* __restrict__ xk, float* __restrict__ xm, const TD* __restrict__ d,
              const float* __restrict__ gdev)
 {
     const float gm = *gdev;
@@ -170,7 +171,7 @@ k_refine_sum(const DevGeom g, const float* __restrict__ xk, float* __restrict__ 
         const int x = (int)(p % g.M), y = (int)((p / g.M) % g.N), z = (int)(p / MN);
         const float xkv = xk[p], xmv = xm[p];
         const float yk = fs(fm(fa(1.0f, gm), xkv), fm(gm, xmv));
-        xm[p] = fa(yk, fs(Store<T>::ld(d + tile_index(g, x, y, z)), refine_d0<T>(xkv, xmv, gm)));
+        xm[p] = fa(yk, fs(Store<TD>::ld(d + tile_index(g, x, y, z)), refine_d0<T, TD>(xkv, xmv, gm)));
     }
 }
 
@@ -265,17 +266,19 @@ ctr_status launch_momentum(const Geometry& G, void* y, void* xprev, const void* 
     return CTR_OK;
 }
 
-ctr_status launch_refine_update(Geometry& G, float* xk, float* xm, const void* d_tiled, void* xt_tiled, ctr_dtype dt,
-                                float lam, int iters, const float* gdev, cudaStream_t st)
+ctr_status launch_refine_update(Geometry& G, float* xk, float* xm, const void* d_tiled, ctr_dtype ddt, void* xt_tiled,
+                                ctr_dtype dt, float lam, int iters, const float* gdev, cudaStream_t st)
 {
     const int M = G.desc.nx, N = G.desc.ny, Z = G.desc.nz;
     const long long V = G.nvox();
     const size_t es = dtype_size(dt);
     const bool fgp = lam > 0.f && iters >= 0;
+    if (ddt != dt && ddt != CTR_F32) return set_error(CTR_ERR_INVALID_ARGUMENT, "correction type");
     if (fgp) CTR_TRY(ensure_fgp(&G, fgp_workspace_bytes(V, dt)));
     const int nb = grid_for(V, 256);
     CTR_DISPATCH_DTYPE(dt, T, {
-        k_refine_sum<T><<<nb, 256, 0, st>>>(G.dg, xk, xm, (const T*)d_tiled, gdev);
+        if (ddt == CTR_F32) k_refine_sum<T, float><<<nb, 256, 0, st>>>(G.dg, xk, xm, (const float*)d_tiled, gdev);
+        else k_refine_sum<T, T><<<nb, 256, 0, st>>>(G.dg, xk, xm, (const T*)d_tiled, gdev);
         if (fgp) {
             CTR_CUDA_TRY(cudaMemsetAsync(G.d_fgp, 0, 6 * (size_t)V * es, st));
             const float alpha12 = 1.0f / (lam * 12.0f);
@@ -300,11 +303,15 @@ ctr_status launch_refine_update(Geometry& G, float* xk, float* xm, const void* d
     return CTR_OK;
 }
 
-ctr_status launch_refine_start(Geometry& G, const float* xk, const float* xm, void* d_tiled, ctr_dtype dt,
-                               const float* gdev, cudaStream_t st)
+ctr_status launch_refine_start(Geometry& G, const float* xk, const float* xm, void* d_tiled, ctr_dtype ddt,
+                               ctr_dtype dt, const float* gdev, cudaStream_t st)
 {
+    if (ddt != dt && ddt != CTR_F32) return set_error(CTR_ERR_INVALID_ARGUMENT, "correction type");
     const int nb = grid_for(tiled_count(G.dg), 256);
-    CTR_DISPATCH_DTYPE(dt, T, { k_refine_start<T><<<nb, 256, 0, st>>>(G.dg, xk, xm, gdev, (T*)d_tiled); });
+    CTR_DISPATCH_DTYPE(dt, T, {
+        if (ddt == CTR_F32) k_refine_start<T, float><<<nb, 256, 0, st>>>(G.dg, xk, xm, gdev, (float*)d_tiled);
+        else k_refine_start<T, T><<<nb, 256, 0, st>>>(G.dg, xk, xm, gdev, (T*)d_tiled);
+    });
     CTR_CUDA_TRY(cudaGetLastError());
     return CTR_OK;
 }

@@ -11,16 +11,19 @@ ctr_status launch_forward(const Geometry& G, const FpArgs& a, cudaStream_t st, s
     const DevGeom& g = G.dg;
     if (a.nview <= 0) return CTR_OK;
     if (a.nview > 65535) return set_error(CTR_ERR_INVALID_ARGUMENT, "too many views in one launch");
+    const bool refine = a.kind == FP_SART_REFINE || a.kind == FP_SART_REFINE32;
     if (a.tiled && a.kind != FP_SART && a.kind != FP_OBJECTIVE && a.kind != FP_SART_OBJ && a.kind != FP_PARTIAL &&
-        a.kind != FP_SART_REFINE)
+        !refine)
         return set_error(CTR_ERR_UNSUPPORTED, "the tiled layout is for SART and objective projections");
+    if (a.kind == FP_SART_REFINE32 && !a.tiled)
+        return set_error(CTR_ERR_UNSUPPORTED, "SART_REFINE32 takes tiled volumes");
     if (a.kind == FP_SART_OBJ && !a.vol2) return set_error(CTR_ERR_INVALID_ARGUMENT, "SART_OBJ needs vol2");
-    if (a.kind == FP_SART_REFINE && (!a.vol2 || !a.ax || !a.gdev || !a.partial))
+    if (refine && (!a.vol2 || !a.ax || !a.gdev || !a.partial))
         return set_error(CTR_ERR_INVALID_ARGUMENT, "SART_REFINE needs vol2, ax, gdev and partial");
     // the dot product keeps the fixed shape: its block partial sums, and so
     // the rounding of the total, do not depend on the tuned shape
     if (nblocks_out)
-        *nblocks_out = (a.kind == FP_OBJECTIVE || a.kind == FP_SART_OBJ || a.kind == FP_SART_REFINE)
+        *nblocks_out = (a.kind == FP_OBJECTIVE || a.kind == FP_SART_OBJ || refine)
                            ? objective_partials_per_view(g) * a.nview
                            : (size_t)((g.R + FP_BX - 1) / FP_BX) * ((g.ZP + FP_BY - 1) / FP_BY) * a.nview;
     const size_t smem = plane_tables_bytes(g);

@@ -23,6 +23,8 @@
 //     backprojector), or reduces the squared residual in FP64 (objective).
 #pragma once
 
+#include <type_traits>
+
 #include "ctr_device.cuh"
 
 namespace ctr {
@@ -99,11 +101,11 @@ __device__ __forceinline__ float pos_floor(float a, float d, float x1, float b, 
 // step rule are the same code, so every ray visits the same voxels.  The sums
 // round differently from the reference's sequence (within 1e-5 relative).
 template <typename VT, bool E64, bool TRACE, bool LOAD = true, bool ACC64 = false, int CPM = 0, bool TL = false,
-          bool DUAL = false, bool FAST = false, bool COH = false>
+          bool DUAL = false, bool FAST = false, bool COH = false, typename VT2 = VT>
 __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __restrict__ PX,
                                             const float* __restrict__ PY, const float* __restrict__ PZ,
                                             const float* __restrict__ PINF, const VT* __restrict__ vol, float s,
-                                            float c, int u, int v, const VT* __restrict__ vol2 = nullptr)
+                                            float c, int u, int v, const VT2* __restrict__ vol2 = nullptr)
 {
     const int M = g.M, N = g.N, Z = g.Z;
     RayResult r;
@@ -289,7 +291,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
             const float f = COH ? Store<VT>::ldc(vol + idx) : Store<VT>::ld(vol + idx);
             sum = __fmaf_rn(seg_p, f_p, sum);                          // +0 on the first step
             if (DUAL) {
-                const float f2 = COH ? Store<VT>::ldc(vol2 + idx) : Store<VT>::ld(vol2 + idx);
+                const float f2 = COH ? Store<VT2>::ldc(vol2 + idx) : Store<VT2>::ld(vol2 + idx);
                 sum2 = __fmaf_rn(seg_p, f2_p, sum2);
                 f2_p = f2;
             }
@@ -303,7 +305,7 @@ __device__ __forceinline__ RayResult siddon(const DevGeom& g, const float* __res
                 if (ACC64) dsum = __fma_rn((double)seg_p, (double)f_p, dsum);   // +0 on the first step
                 else sum = fa(sum, fm(seg_p, f_p));
                 if (DUAL) {
-                    const float f2 = COH ? Store<VT>::ldc(vol2 + idx) : Store<VT>::ld(vol2 + idx);
+                    const float f2 = COH ? Store<VT2>::ldc(vol2 + idx) : Store<VT2>::ld(vol2 + idx);
                     sum2 = fa(sum2, fm(seg_p, f2_p));
                     f2_p = f2;
                 }
@@ -407,10 +409,13 @@ __device__ __forceinline__ void fp_block(const DevGeom& g, const float* __restri
                                          void* __restrict__ out, int out_dt, const void* __restrict__ b, int b_dt,
                                          double* __restrict__ partial, int* __restrict__ nseg,
                                          uint64_t* __restrict__ hash, float* __restrict__ lens,
-                                         const VT* __restrict__ vol2, float* __restrict__ ax,
+                                         const void* __restrict__ vol2_any, float* __restrict__ ax,
                                          const float* __restrict__ gdev)
 {
-    constexpr bool DUAL = KIND == FP_SART_OBJ || KIND == FP_SART_REFINE;
+    constexpr bool REFINE = KIND == FP_SART_REFINE || KIND == FP_SART_REFINE32;
+    constexpr bool DUAL = KIND == FP_SART_OBJ || REFINE;
+    using VT2 = typename std::conditional<KIND == FP_SART_REFINE32, float, VT>::type;   // the second volume's type
+    const VT2* __restrict__ vol2 = (const VT2*)vol2_any;
     const int tx = centre_out(bx, gx), ty = centre_out(by, gy);
     const int u = tx * FP_BX + (threadIdx.x % FP_BX);
     const int v = ty * BY + (threadIdx.x / FP_BX);
@@ -425,7 +430,7 @@ __device__ __forceinline__ void fp_block(const DevGeom& g, const float* __restri
         ((float2*)out)[p] = make_float2(0.0f, 0.0f);
     } else if (active) {
         const float2 sc = g.trig[view0 + w];
-        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, DUAL, FAST, COH>(
+        const RayResult rr = siddon<VT, E64, KIND == FP_TRACE, true, KIND == FP_DOT, CPM, TL, DUAL, FAST, COH, VT2>(
             g, PX, PY, PZ, PINF, vol, sc.x, sc.y, u, v, vol2);
         const bool zero = rr.len < g.thr_fp;                       // :554
         if (KIND == FP_PARTIAL) {
@@ -440,7 +445,7 @@ __device__ __forceinline__ void fp_block(const DevGeom& g, const float* __restri
                 const float e = fs(zero ? 0.0f : rr.sum2, bv);
                 e2 = (double)fm(e, e);                                 // L2_norm_kernel, tool_functions.cu:35
             }
-        } else if (KIND == FP_SART_REFINE) {
+        } else if (REFINE) {
             // the residual against y_k = (1+g) x_k - g x_(k-1) and the correction d so far
             const float bv = ld_any(b, p, b_dt);
             const float sx = zero ? 0.0f : rr.sum;                     // A x_k, the objective's rule
@@ -465,7 +470,7 @@ __device__ __forceinline__ void fp_block(const DevGeom& g, const float* __restri
             lens[p] = rr.len;
         }
     }
-    if (KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_SART_REFINE) {
+    if (KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || REFINE) {
         double t = e2;
         for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
         if ((threadIdx.x & 31) == 0 && v < g.ZP) partial[((size_t)w * g.ZP + v) * gx + tx] = t;
@@ -480,7 +485,7 @@ template <typename VT, int KIND, bool E64, int BY, int CPM = 0, bool TL = false,
 __global__ void __launch_bounds__(FP_BX * BY, MINB)
 k_forward(const DevGeom g, const VT* __restrict__ vol, int view0, void* __restrict__ out, int out_dt,
           const void* __restrict__ b, int b_dt, double* __restrict__ partial, int* __restrict__ nseg,
-          uint64_t* __restrict__ hash, float* __restrict__ lens, const VT* __restrict__ vol2,
+          uint64_t* __restrict__ hash, float* __restrict__ lens, const void* __restrict__ vol2,
           float* __restrict__ ax, const float* __restrict__ gdev)
 {
     extern __shared__ float sp[];
@@ -503,25 +508,29 @@ static void launch_fp_tl(const Geometry& G, const FpArgs& a, int nview, size_t s
     const VT* vol = (const VT*)a.vol;
     if (g.entry64)
         k_forward<VT, KIND, true, BY, CPM, TL, MINB, FAST><<<grid, FP_BX * BY, smem, st>>>(
-            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2,
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, a.vol2,
             a.ax, a.gdev);
     else
         k_forward<VT, KIND, false, BY, CPM, TL, MINB, FAST><<<grid, FP_BX * BY, smem, st>>>(
-            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, (const VT*)a.vol2,
+            g, vol, a.view0, a.out, a.out_dtype, a.b, a.b_dtype, a.partial, a.nseg, a.hash, a.len, a.vol2,
             a.ax, a.gdev);
 }
 
 template <typename VT, int KIND, int BY, int CPM = 0, int MINB = 1, bool FAST = false>
 static void launch_fp_t(const Geometry& G, const FpArgs& a, int nview, size_t smem, cudaStream_t st)
 {
-    if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_PARTIAL ||
-                  KIND == FP_SART_REFINE) {
-        if (a.tiled) {
-            launch_fp_tl<VT, KIND, BY, CPM, true, MINB, FAST>(G, a, nview, smem, st);
-            return;
+    if constexpr (KIND == FP_SART_REFINE32) {   // the refinement solver's volumes are always tiled
+        launch_fp_tl<VT, KIND, BY, CPM, true, MINB, FAST>(G, a, nview, smem, st);
+    } else {
+        if constexpr (KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ || KIND == FP_PARTIAL ||
+                      KIND == FP_SART_REFINE) {
+            if (a.tiled) {
+                launch_fp_tl<VT, KIND, BY, CPM, true, MINB, FAST>(G, a, nview, smem, st);
+                return;
+            }
         }
+        launch_fp_tl<VT, KIND, BY, CPM, false, MINB, FAST>(G, a, nview, smem, st);
     }
-    launch_fp_tl<VT, KIND, BY, CPM, false, MINB, FAST>(G, a, nview, smem, st);
 }
 
 // Projector shapes the tuner chooses from: (rows per block, plane mode --
@@ -552,7 +561,7 @@ template <typename VT, int KIND>
 static void launch_fp_shape(const Geometry& G, const FpArgs& a, size_t smem, cudaStream_t st)
 {
     if constexpr (KIND == FP_FORWARD || KIND == FP_SART || KIND == FP_OBJECTIVE || KIND == FP_SART_OBJ ||
-                  KIND == FP_SART_REFINE) {
+                  KIND == FP_SART_REFINE || KIND == FP_SART_REFINE32) {
         if (G.dg.fast_sums) {
             launch_fp_shape_t<VT, KIND, true>(G, a, smem, st);
             return;
@@ -572,6 +581,10 @@ void launch_forward_kinds(const Geometry& G, const FpArgs& a, size_t smem, cudaS
     case FP_OBJECTIVE: launch_fp_shape<VT, FP_OBJECTIVE>(G, a, smem, st); break;
     case FP_SART_OBJ: launch_fp_shape<VT, FP_SART_OBJ>(G, a, smem, st); break;
     case FP_SART_REFINE: launch_fp_shape<VT, FP_SART_REFINE>(G, a, smem, st); break;
+    case FP_SART_REFINE32:   // an FP32 copy with an FP32 correction is FP_SART_REFINE
+        if constexpr (std::is_same<VT, float>::value) launch_fp_shape<VT, FP_SART_REFINE>(G, a, smem, st);
+        else launch_fp_shape<VT, FP_SART_REFINE32>(G, a, smem, st);
+        break;
     case FP_PARTIAL: launch_fp_shape<VT, FP_PARTIAL>(G, a, smem, st); break;
     case FP_TRACE: launch_fp_t<VT, FP_TRACE, FP_BY>(G, a, a.nview, smem, st); break;
     case FP_DOT: launch_fp_t<VT, FP_DOT, FP_BY>(G, a, a.nview, smem, st); break;

@@ -464,9 +464,10 @@ class Solver:
     FISTA it makes the iteration diverge after a few passes on a 256^3 /
     360-view scan, so pass the reference's step there.
 
-    ``refine=True`` (with a BF16/F16 ``vol_dtype``): mixed-precision iterative
-    refinement -- FP32 FISTA state, 16-bit copies for the projectors, each
-    SART pass accumulated into a 16-bit correction against the FP32 residual.
+    ``refine=True`` (or 1, with a BF16/F16 ``vol_dtype``): mixed-precision
+    iterative refinement -- FP32 FISTA state, 16-bit copies for the
+    projectors, each SART pass accumulated into a 16-bit correction against
+    the FP32 residual.  ``refine=2``: the same with the correction in FP32.
     ``vol_dtype=F64``: the FP64 reference solver (FP64 volumes)."""
 
     def __init__(self, geom: Geometry, vol_dtype=F32, beta=0.8, lambda_tv=0.0, fgp_iters=20, fista=True,

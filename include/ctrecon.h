@@ -386,7 +386,11 @@ ctr_status ctr_dot_test(const ctr_geometry* geom, const float* x, const float* y
  * exact arithmetic this is the same iteration as refine = 0.  The fidelity of
  * the objective is that of the vol_dtype copy of x_k the pass projects, the TV
  * that of the FP32 x_k.  Workspace: two FP32 volumes and one FP32 sinogram.
- * Not with ctr_solver_set_slabs.
+ * Not with ctr_solver_set_slabs.  refine = 2 keeps d in FP32 (its per-view
+ * updates are then not rounded to 16 bits; a 16-bit d's rounding noise is
+ * the error floor of refine = 1, about 2e-3 of the maximum with BF16 at
+ * 1024^3): the projectors read the 16-bit copy and the FP32 d, the update
+ * writes FP32 d, stochastic rounding does not apply to it.
  *
  * vol_dtype CTR_F64: the FP64 reference solver.  The same iteration with every
  * step in FP64 on the device: a Siddon traversal per ray with FP64 alphas,
@@ -405,7 +409,8 @@ typedef struct ctr_solver_params {
     int   objective;       /* 1: evaluate the objective every iteration                  */
     int   use_graph;       /* 1: capture one iteration as a CUDA graph and replay it     */
     unsigned sart_flags;   /* CTR_SART_*                                                 */
-    int   refine;          /* 1: mixed-precision iterative refinement (above)            */
+    int   refine;          /* 1: mixed-precision iterative refinement (above); 2: the    */
+                           /* same with the correction volume d in FP32                  */
 } ctr_solver_params;
 
 typedef struct ctr_solver ctr_solver;

@@ -11,8 +11,11 @@ keeps the FISTA state in FP32 and rounds each view's update only against the
 pass's correction volume, which starts at the 16-bit copies' own rounding of
 the estimate (so that rounding does not bias the result); it meets the bar at 20
 iterations with FP16 copies, and with BF16 copies when the correction's
-updates are rounded stochastically.  The plain 16-bit storage form is kept
-for short runs (5 iterations) and is shown to drift at 20."""
+updates are rounded stochastically.  ``refine=2`` keeps the correction in
+FP32 (its per-view updates are then not rounded at all; a 16-bit
+correction's rounding noise is refine=1's error floor).  The plain 16-bit
+storage form is kept for short runs (5 iterations) and is shown to drift at
+20."""
 import numpy as np
 import pytest
 
@@ -26,7 +29,7 @@ BAR = 1e-3
 
 # (relaxation, iterations, storage mode, RMSE limit relative to max attenuation)
 CASES = [(0.0625, 20, "f32", 2e-4), (0.0625, 20, "f16_refine", BAR), (0.0625, 20, "f16_sr_refine", BAR),
-         (0.0625, 20, "bf16_sr_refine", BAR),
+         (0.0625, 20, "bf16_sr_refine", BAR), (0.0625, 20, "f16_refine2", BAR), (0.0625, 20, "bf16_refine2", BAR),
          (0.0625, 5, "f32", 1e-4), (0.0625, 5, "f16_refine", BAR), (0.0625, 5, "f16", BAR),
          (0.8, 5, "f32", 1e-4), (0.8, 5, "f16", BAR), (0.8, 5, "f16_sr", BAR), (0.8, 5, "f16_refine", BAR),
          (0.8, 5, "bf16_refine", BAR)]
@@ -82,8 +85,9 @@ def run(b, mode, beta, iters):
     sdt = torch.float32 if vdt == gpu_b200.F32 else torch.float16
     flags = gpu_b200.SART_STOCHASTIC_ROUND if "_sr" in mode else 0
     g = gpu_b200.Geometry(ctr_desc(MIXED))
+    refine = 2 if mode.endswith("_refine2") else int(mode.endswith("_refine"))   # 2: FP32 correction
     s = gpu_b200.Solver(g, vdt, beta=beta, lambda_tv=LAM_TV, fgp_iters=FGP, fista=True, objective=False,
-                        sart_flags=flags, refine=mode.endswith("_refine"))
+                        sart_flags=flags, refine=refine)
     s.set_sinogram(torch.from_numpy(b).cuda().to(sdt))
     s.set_volume(None)
     s.iterate(iters)

@@ -35,9 +35,11 @@ def store(x, dtype):
     return x.astype(np.float16).astype(np.float32) if dtype == "f16" else x.astype(np.float32)
 
 
-def refine_restated(o, b, beta, lam_tv, fgp_iters, n_iter, dtype, fista=True):
+def refine_restated(o, b, beta, lam_tv, fgp_iters, n_iter, dtype, fista=True, d32=False):
     """The refinement iteration in float32 from oracle primitives; returns the
-    FP32 x_k and the fidelity of each iteration's 16-bit copy."""
+    FP32 x_k and the fidelity of each iteration's 16-bit copy.  d32: the
+    correction volume kept in FP32 (refine=2)."""
+    dstore = (lambda x: x.astype(np.float32)) if d32 else (lambda x: store(x, dtype))
     nv = b.shape[0]
     xk = np.zeros(o.vol_shape, F)
     xm = np.zeros_like(xk)
@@ -47,7 +49,7 @@ def refine_restated(o, b, beta, lam_tv, fgp_iters, n_iter, dtype, fista=True):
     for _ in range(n_iter):
         xc = store(xk, dtype)          # the projectors' copy of x_k
         # d starts at the copies' rounding of y_k = (1+g) x_k - g x_(k-1)
-        d0 = store((F(1.0) + gm) * (xk - xc) - gm * (xm - store(xm, dtype)), dtype)
+        d0 = dstore((F(1.0) + gm) * (xk - xc) - gm * (xm - store(xm, dtype)))
         d = d0.copy()
         for j in range(nv):
             sx = o.forward_view(xc, j, 0)                    # A x~_k, zero below vz*1e-6
@@ -57,7 +59,7 @@ def refine_restated(o, b, beta, lam_tv, fgp_iters, n_iter, dtype, fista=True):
             zero = ln < F(o.desc.vz) * F(1e-6)
             c = np.where(zero, F(0.0), ((b[j] - ay) - sd) / np.where(zero, F(1.0), ln)).astype(F)
             ax[j] = sx
-            d = store(o.backproject_gather(d, c, j, beta), dtype)
+            d = dstore(o.backproject_gather(d, c, j, beta))
         fids.append(float(np.sum(((ax - b).astype(F) ** 2).astype(np.float64))))
         z = ((F(1.0) + gm) * xk - gm * xm + (d - d0)).astype(F)
         xs = o.fgp(z, F(beta) * F(lam_tv), fgp_iters) if lam_tv > 0 else z
@@ -77,24 +79,25 @@ def problem(oracle_mod, name):
 
 
 @pytest.mark.parametrize("name", ["cube16", "aniso", "tbct"])
-@pytest.mark.parametrize("dtype,lam", [("f32", 0.05), ("f16", 0.0)])
-def test_refine_matches_restatement(name, dtype, lam, oracle_built):
+@pytest.mark.parametrize("dtype,lam,refine", [("f32", 0.05, 1), ("f16", 0.0, 1), ("f16", 0.0, 2)])
+def test_refine_matches_restatement(name, dtype, lam, refine, oracle_built):
+    """refine=2: the correction volume in FP32 while the copies are FP16."""
     import gpu_b200
     cfg, o, b = problem(oracle_built, name)
     beta, fgp_iters, n = 0.3, 4, 3
     vdt, tdt = {"f32": (gpu_b200.F32, torch.float32), "f16": (gpu_b200.F16, torch.float16)}[dtype]
     g = gpu_b200.Geometry(ctr_desc(cfg))
     s = gpu_b200.Solver(g, vdt, beta=beta, lambda_tv=lam, fgp_iters=fgp_iters, fista=True, objective=True,
-                        refine=True)
+                        refine=refine)
     s.set_sinogram(torch.from_numpy(b).cuda().to(tdt))
     s.set_volume(None)
     objs = s.iterate(n)
     got = torch.zeros(o.vol_shape, device="cuda")
     s.get_volume_f32(got)
     bq = store(b, dtype)
-    want, fids = refine_restated(o, bq, beta, lam, fgp_iters, n + 1, dtype)
+    want, fids = refine_restated(o, bq, beta, lam, fgp_iters, n + 1, dtype, d32=refine == 2)
     # n + 1 restated passes: the last one's fidelity is the objective of x_n
-    want_n, _ = refine_restated(o, bq, beta, lam, fgp_iters, n, dtype)
+    want_n, _ = refine_restated(o, bq, beta, lam, fgp_iters, n, dtype, d32=refine == 2)
     np.testing.assert_array_equal(bits(got.cpu().numpy()), bits(want_n))
     np.testing.assert_allclose(objs[:, 1], fids[1:], rtol=1e-12)
     copy = torch.zeros(o.vol_shape, device="cuda", dtype=tdt)
@@ -102,15 +105,21 @@ def test_refine_matches_restatement(name, dtype, lam, oracle_built):
     np.testing.assert_array_equal(bits(copy.float().cpu().numpy()), bits(store(want_n, dtype)))
 
 
-@pytest.mark.parametrize("dtype", ["f16", "bf16_sr"])
-def test_refine_batch_equals_single(dtype, oracle_built):
+@pytest.mark.parametrize("persistent", [False, True])
+@pytest.mark.parametrize("dtype", ["f16", "bf16_sr", "bf16_d32"])
+def test_refine_batch_equals_single(dtype, persistent, oracle_built):
+    """bf16_d32: BF16 copies with the FP32 correction (refine=2)."""
     import gpu_b200
-    vdt, tdt = {"f16": (gpu_b200.F16, torch.float16), "bf16_sr": (gpu_b200.BF16, torch.bfloat16)}[dtype]
+    vdt, tdt = {"f16": (gpu_b200.F16, torch.float16), "bf16_sr": (gpu_b200.BF16, torch.bfloat16),
+                "bf16_d32": (gpu_b200.BF16, torch.bfloat16)}[dtype]
     flags = gpu_b200.SART_STOCHASTIC_ROUND if dtype.endswith("_sr") else 0
-    kw = dict(beta=0.3, lambda_tv=0.05, fgp_iters=4, fista=True, objective=True, sart_flags=flags, refine=True)
+    kw = dict(beta=0.3, lambda_tv=0.05, fgp_iters=4, fista=True, objective=True, sart_flags=flags,
+              refine=2 if dtype.endswith("_d32") else 1)
     data = [problem(oracle_built, n) for n in ["cube16", "odd", "aniso", "tbct"]]
     geoms = [gpu_b200.Geometry(ctr_desc(cfg)) for cfg, _, _ in data]
     batch = gpu_b200.Batch(geoms, vdt, **kw)
+    if persistent:
+        batch.set_persistent(True)
     sinos = [torch.from_numpy(b).cuda().to(tdt) for _, _, b in data]
     for i, sb in enumerate(sinos):
         batch.set_sinogram(i, sb)
