@@ -70,6 +70,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mixed", choices=["f16", "bf16"], default="f16")
+    p.add_argument("--large-plain", action="store_true",
+                   help="large: also run plain FP16 storage (no refinement) against the FP64 reference")
     p.add_argument("--refine", type=int, choices=[1, 2], default=2,
                    help="the 16-bit runs' refinement solver: 1 keeps the correction volume in the 16-bit type, "
                         "2 in FP32")
@@ -600,7 +602,7 @@ def run_batched(args):
         clocks.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        batch.iterate(iters)
+        objs = batch.iterate(iters)
         e1.record(stream)
         torch.cuda.synchronize()
         timed[mode] = (e0.elapsed_time(e1) / iters, clocks.stop())
@@ -609,14 +611,20 @@ def run_batched(args):
     updates = sum(sp["nx"] * sp["ny"] * sp["nz"] * sp["n_views"] for sp in specs)
     # accuracy: the same iterations through the FP64 reference solver on the
     # same (FP16-stored) data, per scan, relative to the scan's phantom maximum
-    errs, maxs = [], []
+    # The fidelity's trend over the timed iterations (last / first) of this
+    # run and of the FP64 solver: a scan whose fidelity grows in FP64 too is
+    # one where FISTA over SART diverges at this step, and its error against
+    # the FP64 run measures that divergence, not the arithmetic.
+    errs, maxs, trend, trend64 = [], [], [], []
     for i, (sp, g) in enumerate(zip(specs, geoms)):
         got = torch.zeros(g.vol_shape, device=dev)
         batch.get_volume_f32(i, got)
-        s64 = gpu_b200.Solver(g, gpu_b200.F64, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, objective=False)
+        s64 = gpu_b200.Solver(g, gpu_b200.F64, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, objective=True)
         s64.set_sinogram(sinos[i])
         s64.set_volume(None)
-        s64.iterate(iters, objectives=False)
+        o64 = s64.iterate(iters)
+        trend.append(float(objs[i][-1][1] / objs[i][0][1]))
+        trend64.append(float(o64[-1][1] / o64[0][1]))
         want = torch.zeros(g.vol_shape, device=dev, dtype=torch.float64)
         s64.get_volume(want)
         s64.close()
@@ -654,7 +662,9 @@ def run_batched(args):
         "error_vs_fp64": {"rmse": {"max": max(errs), "median": sorted(errs)[len(errs) // 2]},
                           "max_abs": {"max": max(maxs), "median": sorted(maxs)[len(maxs) // 2]},
                           "per_scan_rmse": errs, "iterations": iters,
-                          "relative_to": "each scan's phantom maximum, against the FP64 reference solver"},
+                          "relative_to": "each scan's phantom maximum, against the FP64 reference solver",
+                          "fidelity_last_over_first": {"this_run": trend, "fp64": trend64},
+                          "diverging_in_fp64": [i for i, t in enumerate(trend64) if t > 1.0]},
         "clocks": clk, "gpu_launches": launches,
         "launch_shapes": [g.shapes() for g in geoms],
     }
@@ -667,9 +677,11 @@ LARGE = dict(nx=1024, ny=1024, nz=1024, vx=0.25, nu=1024, nv=1024, du=0.3, dso=1
 
 def run_large(args):
     """1024^3 (0.25 mm) / 1024 views / 1024x1024 detector (0.3 mm): iterations/s
-    of FP32, BF16 and FP16 storage on a seeded 100-ellipsoid phantom, and the
-    RMSE and maximum error of the BF16/FP16 reconstructions against the FP32
-    one after the same iterations (relative to the phantom's maximum)."""
+    of FP32 and of the BF16 / FP16 refinement solver on a seeded 100-ellipsoid
+    phantom, and the RMSE and maximum error of every reconstruction against
+    the FP64 reference solver after the same iterations (relative to the
+    phantom's maximum).  --large-plain adds plain FP16 storage (no
+    refinement), whose error grows with the iterations."""
     import numpy as np
     import torch
 
@@ -699,15 +711,19 @@ def run_large(args):
     out = {}
     vols = {}
     sino16 = sino32.to(torch.float16)
-    # BF16 and FP16: the refinement solver (16-bit copies and correction,
-    # FP32 FISTA state, FP16 measured data); BF16 with stochastic rounding
-    for mode, vdt, tdt in (("f32", gpu_b200.F32, torch.float32), ("bf16", gpu_b200.BF16, torch.bfloat16),
-                           ("f16", gpu_b200.F16, torch.float16)):
+    # BF16 and FP16: the refinement solver (16-bit copies, FP32 FISTA state,
+    # FP16 measured data); a 16-bit correction takes stochastic rounding in
+    # BF16.  f16_plain: FP16 storage without refinement.
+    modes = [("f32", gpu_b200.F32, torch.float32), ("bf16", gpu_b200.BF16, torch.bfloat16),
+             ("f16", gpu_b200.F16, torch.float16)]
+    if args.large_plain:
+        modes.append(("f16_plain", gpu_b200.F16, torch.float16))
+    for mode, vdt, tdt in modes:
         sino = sino32 if tdt == torch.float32 else sino16
         tuned = geom.autotune(vdt, n_views=2)
         flags = gpu_b200.SART_STOCHASTIC_ROUND if mode == "bf16" else 0
         solver = gpu_b200.Solver(geom, vdt, beta=BETA, lambda_tv=LAMBDA_TV, fgp_iters=FGP_ITERS, sart_flags=flags,
-                                 refine=0 if mode == "f32" else args.refine)
+                                 refine=0 if mode in ("f32", "f16_plain") else args.refine)
         solver.set_sinogram(sino)
         solver.set_volume(None)
         for _ in range(args.warmup):
@@ -741,7 +757,7 @@ def run_large(args):
     torch.cuda.synchronize()
     ref = f64.get_volume(torch.zeros(geom.vol_shape, device=dev, dtype=torch.float64))
     f64.close()
-    for mode in ("f32", "bf16", "f16"):
+    for mode in vols:
         dlt = vols[mode].double() - ref
         out[mode]["rmse_vs_fp64"] = float(torch.sqrt(torch.mean(dlt * dlt))) / mu_max
         out[mode]["max_err_vs_fp64"] = float(dlt.abs().max()) / mu_max

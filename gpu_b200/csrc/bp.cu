@@ -768,7 +768,8 @@ __device__ __forceinline__ unsigned flow_blocks(const BatchScan& S, unsigned ph)
 // running) it polls again after a sleep that doubles up to 4 us; idle past
 // kIdleNs it flags ERR_BARRIER and returns -1.
 __device__ __forceinline__ int flow_claim(const BatchScan* __restrict__ scans, int nscans, int home,
-                                          BatchFlow* flow, unsigned* finished, unsigned* err, unsigned& ph, int& blk)
+                                          BatchFlow* flow, unsigned* finished, unsigned* err, unsigned& ph, int& blk,
+                                          int& cnt)
 {
     unsigned sleep_ns = 64;
     const unsigned long long t0 = global_ns();
@@ -779,13 +780,17 @@ __device__ __forceinline__ int flow_claim(const BatchScan* __restrict__ scans, i
             const BatchScan& S = scans[s];
             const unsigned last = 2u * (unsigned)S.nviews;
             const unsigned long long w = *(volatile unsigned long long*)&flow[s].claim;
-            const unsigned p = (unsigned)(w >> 32);
-            if (p >= last || (unsigned)w >= flow_blocks(S, p)) continue;
-            const unsigned long long o = atomicAdd(&flow[s].claim, 1ull);
-            const unsigned p2 = (unsigned)(o >> 32);
-            if (p2 < last && (unsigned)o < flow_blocks(S, p2)) {
+            const unsigned p = (unsigned)(w >> 32), nb = flow_blocks(S, p);
+            if (p >= last || (unsigned)w >= nb) continue;
+            // a chunk of up to 8 blocks per claim (1 per 128 of the phase):
+            // one claim's latency serves several blocks
+            const unsigned k = max(1u, min(8u, nb / 128u));
+            const unsigned long long o = atomicAdd(&flow[s].claim, (unsigned long long)k);
+            const unsigned p2 = (unsigned)(o >> 32), nb2 = flow_blocks(S, p2), c2 = (unsigned)o;
+            if (p2 < last && c2 < nb2) {
                 ph = p2;
-                blk = (int)(unsigned)o;
+                blk = (int)c2;
+                cnt = (int)min(k, nb2 - c2);
                 return s;
             }
         }
@@ -801,12 +806,12 @@ __device__ __forceinline__ int flow_claim(const BatchScan* __restrict__ scans, i
 // The SART pass of every scan of a batch in one launch, scheduled as a data
 // flow.  A scan's phases run in order (view j's forward projection, its
 // walk, view j+1's forward projection, ...); the blocks of a phase run in any
-// order on any CTA.  A CTA takes the next block of its home scan's current
-// phase, else of any other scan's, so no CTA waits while some scan has a
-// block to give.  The phase's last block to finish opens the next phase:
-// each block releases its writes (fence, then its count), the last one
-// resets the count and moves the claim word on (fence first); a CTA that
-// claims a block fences before reading (acquire), and reads the ray records
+// order on any CTA.  A CTA takes the next chunk of blocks (1-8) of its home
+// scan's current phase, else of any other scan's, so no CTA waits while some
+// scan has a block to give.  The phase's last chunk to finish opens the next
+// phase: each chunk releases its writes (fence, then its count), the last
+// one resets the count and moves the claim word on (fence first); a CTA that
+// claims a chunk fences before reading (acquire), and reads the ray records
 // and volumes the launch writes with coherent loads.  Each block runs the
 // per-ray and per-voxel code of k_forward (shape 1) and k_sart_walk (shape
 // 1), every voxel sees its views in order, so every scan's result equals
@@ -820,7 +825,7 @@ k_batch_pass(const BatchScan* __restrict__ scans, int nscans, BatchFlow* __restr
              unsigned* __restrict__ finished, unsigned* __restrict__ err)
 {
     extern __shared__ float sp[];
-    __shared__ int s_scan, s_blk;
+    __shared__ int s_scan, s_blk, s_cnt;
     __shared__ unsigned s_ph;
     int home = 0;
     {   // the last scan whose first home CTA is at or before this one
@@ -836,12 +841,13 @@ k_batch_pass(const BatchScan* __restrict__ scans, int nscans, BatchFlow* __restr
     for (;;) {
         if (threadIdx.x == 0) {
             unsigned ph = 0;
-            int blk = 0;
-            const int s = flow_claim(scans, nscans, home, flow, finished, err, ph, blk);
+            int blk = 0, cnt = 0;
+            const int s = flow_claim(scans, nscans, home, flow, finished, err, ph, blk, cnt);
             __threadfence();   // acquire: the phase before ph is complete
             s_scan = s;
             s_ph = ph;
             s_blk = blk;
+            s_cnt = cnt;
         }
         __syncthreads();
         const int s = s_scan;
@@ -859,34 +865,36 @@ k_batch_pass(const BatchScan* __restrict__ scans, int nscans, BatchFlow* __restr
         plane_tables_addr(g, sp, PX, PY, PZ, PINF);
         walk_tables_addr(g, sp + fp_table_floats(g), WX, WY, WZ, RT);
         const unsigned ph = s_ph;
-        const int vb = s_blk, j = (int)(ph >> 1);
-        if ((ph & 1u) == 0u) {
-            const long long P = (long long)g.R * g.ZP;
-            const size_t per_view = (size_t)g.ZP * S.fp_gx;
-            const size_t bsz = S.b_dt == CTR_F32 ? 4 : 2;
-            fp_block<VT, KIND, false, 4, 0, true, false, true>(
-                g, PX, PY, PZ, PINF, vb % S.fp_gx, vb / S.fp_gx, 0, S.fp_gx, S.fp_gy, (const VT*)S.fp_vol, j, S.rays,
-                0, (const char*)S.b + (size_t)j * P * bsz, S.b_dt,
-                S.partial ? S.partial + (size_t)j * per_view : nullptr, nullptr, nullptr, nullptr, S.fp_vol2,
-                S.ax ? S.ax + (size_t)j * P : nullptr, S.gdev);
-        } else {
-            // the updated volume: the FP32 correction of FP_SART_REFINE32, else the storage type
-            using WT = typename std::conditional<KIND == FP_SART_REFINE32, float, VT>::type;
-            constexpr bool WSTOCH = STOCH && !std::is_same<WT, float>::value;
-            const uint32_t seed = WSTOCH ? *S.pass_seed * 0x9E3779B9u + (uint32_t)j : 0u;
-            const int bx = vb % S.bp_gx, r = vb / S.bp_gx, by = r % S.bp_gy, bz = r / S.bp_gy;
-            if (g.ct_style == 3)
-                walk_block<WT, WSTOCH, 4, true, 1, true, true>(g, WX, WY, WZ, RT, bx, by, bz, (WT*)S.bp_vol, S.rays,
-                                                               j, S.beta, seed, S.zl);
-            else
-                walk_block<WT, WSTOCH, 4, true, 1, false, true>(g, WX, WY, WZ, RT, bx, by, bz, (WT*)S.bp_vol,
-                                                                S.rays, j, S.beta, seed, S.zl);
+        const int j = (int)(ph >> 1), cnt = s_cnt;
+        for (int vb = s_blk; vb < s_blk + cnt; ++vb) {   // the claimed chunk of the phase
+            if ((ph & 1u) == 0u) {
+                const long long P = (long long)g.R * g.ZP;
+                const size_t per_view = (size_t)g.ZP * S.fp_gx;
+                const size_t bsz = S.b_dt == CTR_F32 ? 4 : 2;
+                fp_block<VT, KIND, false, 4, 0, true, false, true>(
+                    g, PX, PY, PZ, PINF, vb % S.fp_gx, vb / S.fp_gx, 0, S.fp_gx, S.fp_gy, (const VT*)S.fp_vol, j,
+                    S.rays, 0, (const char*)S.b + (size_t)j * P * bsz, S.b_dt,
+                    S.partial ? S.partial + (size_t)j * per_view : nullptr, nullptr, nullptr, nullptr, S.fp_vol2,
+                    S.ax ? S.ax + (size_t)j * P : nullptr, S.gdev);
+            } else {
+                // the updated volume: the FP32 correction of FP_SART_REFINE32, else the storage type
+                using WT = typename std::conditional<KIND == FP_SART_REFINE32, float, VT>::type;
+                constexpr bool WSTOCH = STOCH && !std::is_same<WT, float>::value;
+                const uint32_t seed = WSTOCH ? *S.pass_seed * 0x9E3779B9u + (uint32_t)j : 0u;
+                const int bx = vb % S.bp_gx, r = vb / S.bp_gx, by = r % S.bp_gy, bz = r / S.bp_gy;
+                if (g.ct_style == 3)
+                    walk_block<WT, WSTOCH, 4, true, 1, true, true>(g, WX, WY, WZ, RT, bx, by, bz, (WT*)S.bp_vol,
+                                                                   S.rays, j, S.beta, seed, S.zl);
+                else
+                    walk_block<WT, WSTOCH, 4, true, 1, false, true>(g, WX, WY, WZ, RT, bx, by, bz, (WT*)S.bp_vol,
+                                                                    S.rays, j, S.beta, seed, S.zl);
+            }
         }
-        __syncthreads();   // the block's writes are issued
+        __syncthreads();   // the chunk's writes are issued
         if (threadIdx.x == 0) {
             __threadfence();   // release them
-            const unsigned d = atomicAdd(&flow[s].done, 1u) + 1u;
-            if (d == flow_blocks(S, ph)) {   // the phase's last block opens the next
+            const unsigned d = atomicAdd(&flow[s].done, (unsigned)cnt) + (unsigned)cnt;
+            if (d == flow_blocks(S, ph)) {   // the phase's last chunk opens the next
                 atomicExch(&flow[s].done, 0u);
                 __threadfence();
                 atomicExch(&flow[s].claim, (unsigned long long)(ph + 1u) << 32);
