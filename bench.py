@@ -551,6 +551,21 @@ def batched_scans(n, seed=4):
     return out
 
 
+def sampling_split(specs, errs):
+    """The per-scan errors split by the detector pixel's width at the
+    isocentre in voxels: at most one voxel (every voxel met by rays of
+    positive chord in every view) or wider (a voxel may meet one ray of a view
+    at a grazing chord, and whether the voxel-driven update takes it depends
+    on the chord's last bits)."""
+    fine, coarse = [], []
+    for sp, e in zip(specs, errs):
+        pixel_at_iso = sp["du"] * sp["dso"] / (sp["dso"] - sp["dod"])
+        (fine if pixel_at_iso <= sp["vx"] else coarse).append(e)
+    summ = lambda v: {"scans": len(v), "rmse_max": max(v) if v else None,
+                      "rmse_median": sorted(v)[len(v) // 2] if v else None}
+    return {"pixel_at_most_one_voxel": summ(fine), "pixel_wider_than_a_voxel": summ(coarse)}
+
+
 def run_batched(args):
     """Aggregate voxel-updates/s of a batch of uneven scans with BF16 volumes
     (the refinement solver: BF16 copies for the projectors and a BF16
@@ -664,7 +679,8 @@ def run_batched(args):
                           "per_scan_rmse": errs, "iterations": iters,
                           "relative_to": "each scan's phantom maximum, against the FP64 reference solver",
                           "fidelity_last_over_first": {"this_run": trend, "fp64": trend64},
-                          "diverging_in_fp64": [i for i, t in enumerate(trend64) if t > 1.0]},
+                          "diverging_in_fp64": [i for i, t in enumerate(trend64) if t > 1.0],
+                          "by_sampling": sampling_split(specs, errs)},
         "clocks": clk, "gpu_launches": launches,
         "launch_shapes": [g.shapes() for g in geoms],
     }
