@@ -421,14 +421,16 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     for (int k = kb; k < ke; ++k, pv += vstep, zrow += g.ZP) {
         int vlo = 0, vhi = -1;   // candidate rows (absolute row indices)
         float sw = 0.f, sl = 0.f;
+        // selects, not a branch: the sums take the pair only above the
+        // threshold (:785-791); the product is formed either way
         auto pair = [&](float a, float bb, float2 zc, float2 rec) {
             const float lo = fmaxf(a, zc.x);
             const float hi = fminf(bb, zc.y);
             const float temp = fm(rec.y, fs(hi, lo));
-            if (temp > g.thr_bp) {                                             // :785-791
-                sw = fa(sw, fm(temp, rec.x));
-                sl = fa(sl, temp);
-            }
+            const bool on = temp > g.thr_bp;
+            const float w = fa(sw, fm(temp, rec.x)), l = fa(sl, temp);
+            sw = on ? w : sw;
+            sl = on ? l : sl;
         };
         // the pairs of one detector row: its z-cell interval is loaded once and
         // met with every column of the run (columns ascending)
@@ -440,9 +442,11 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
                 pair(ra[q], rb[q], zc, rec(rr + min(q, nrun - 1)));
             if (NQ == WALK_RUN)
                 for (int q = WALK_RUN; q < nrun; ++q) {   // runs longer than the registers hold
+                    // the column's planes re-read from the shared tables (rare: not kept live)
                     const float4 ct = __ldg(colt + ua + q);
-                    const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
-                    const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
+                    const float x0 = PX[i + 1], x1 = PX[i + 2], y0 = PY[j + 1], y1 = PY[j + 2];
+                    const float ax0 = fm(fs(x0, ct.x), ct.y), ax1 = fm(fs(x1, ct.x), ct.y);
+                    const float ay0 = fm(fs(y0, ct.z), ct.w), ay1 = fm(fs(y1, ct.z), ct.w);
                     pair(fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)), zc,
                          rec(rr + q));
                 }
