@@ -76,7 +76,11 @@ def parse():
                    help="the 16-bit runs' refinement solver: 1 keeps the correction volume in the 16-bit type, "
                         "2 in FP32")
     p.add_argument("--fast-sums", action="store_true",
-                   help="the mixed-precision run (and --profile-views) with fused ray sums (CTR_GEOM_FAST_SUMS)")
+                   help="the mixed-precision run (and --profile-views) with fused ray sums (CTR_GEOM_FAST_SUMS); "
+                        "the default")
+    p.add_argument("--exact-sums", action="store_true",
+                   help="the mixed-precision run (and --profile-views) with the reference's ray-sum sequence "
+                        "instead of fused ray sums")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-views", type=int, default=0,
                    help="profiling mode: set up the scan, run a SART update of this many views, print timings, exit")
@@ -103,7 +107,14 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="batched: keep the default launch shapes")
     p.add_argument("--no-sr", action="store_true", help="batched: BF16 updates rounded to nearest instead of "
                                                         "stochastically")
-    return p.parse_args()
+    args = p.parse_args()
+    # the mixed-precision run is not the reference's sum sequence in any case
+    # (refinement), so it takes the fused sums unless asked otherwise; the
+    # FP32 run always keeps the reference's sequence, and --profile-views
+    # takes the fused sums only when --fast-sums is given
+    args.profile_fast_sums = args.fast_sums
+    args.fast_sums = not args.exact_sums
+    return args
 
 
 def dist_env():
@@ -484,7 +495,7 @@ def profile_views(args):
     else:
         geom = gpu_b200.Geometry(gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"],
                                                     SCAN["nv"], SCAN["du"], SCAN["dso"], SCAN["dod"],
-                                                    SCAN["n_views"], fast_sums=args.fast_sums))
+                                                    SCAN["n_views"], fast_sums=args.profile_fast_sums))
         ph = phantom_params(2024)
         n_views, beta, lam = SCAN["n_views"], BETA, LAMBDA_TV
     truth = torch.zeros(geom.vol_shape, device="cuda")
@@ -1079,8 +1090,9 @@ def main():
     desc = gpu_b200.make_desc(SCAN["nx"], SCAN["ny"], SCAN["nz"], SCAN["vx"], SCAN["nu"], SCAN["nv"], SCAN["du"],
                               SCAN["dso"], SCAN["dod"], SCAN["n_views"])
     geom = gpu_b200.Geometry(desc)
-    # --fast-sums: the mixed-precision run's projections with fused ray sums
-    # (CTR_GEOM_FAST_SUMS); the FP32 run keeps the reference's sequence
+    # the mixed-precision run's projections with fused ray sums
+    # (CTR_GEOM_FAST_SUMS) unless --exact-sums; the FP32 run keeps the
+    # reference's sequence
     geoms = {"f32": geom, "mixed": geom}
     if args.fast_sums:
         geoms["mixed"] = gpu_b200.Geometry(gpu_b200.make_desc(
