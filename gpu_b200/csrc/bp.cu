@@ -453,16 +453,14 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
         };
         // every pair of the voxel, row by row (rows ascending), the order the
         // oracle's gather sums them
-        auto all_pairs = [&]() {   // vlo <= vhi here
-            int vv = vlo;
-            if (UNR == 2) {   // two rows' z-cell loads in flight, then their pairs in row order
-                for (; vv < vhi; vv += 2) {
-                    const float2 z0c = __ldg(zrow + vv), z1c = __ldg(zrow + vv + 1);
-                    row_pairs(vv, z0c);
-                    row_pairs(vv + 1, z1c);
-                }
-                for (; vv <= vhi; ++vv) row_pairs(vv, __ldg(zrow + vv));
-            } else {          // the next row's z-cell load issued before this row's pairs
+        // Every lane runs the warp's largest row count (no divergent loop):
+        // a lane past its own rows meets the empty z interval [1, 0] (no
+        // chord with any column) at a row clamped into the table.  (The
+        // tetrahedron beam calls this per source, inside a loop whose trip
+        // count differs across lanes; there each lane runs its own rows.)
+        auto all_pairs = [&]() {   // vlo..vhi: this lane's rows (none when vlo > vhi)
+            if constexpr (TB) {   // this lane's rows, the next row's z-cell load ahead (vlo <= vhi here)
+                int vv = vlo;
                 float2 zn = __ldg(zrow + vv);
                 for (; vv < vhi; ++vv) {
                     const float2 zc = zn;
@@ -470,6 +468,25 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
                     row_pairs(vv, zc);
                 }
                 row_pairs(vhi, zn);
+                return;
+            }
+            const int nrows = max(vhi - vlo + 1, 0);
+            const int wrows = __reduce_max_sync(__activemask(), nrows);
+            const float2 none = make_float2(1.0f, 0.0f);
+            auto row = [&](int r) { return min(max(vlo + r, 0), g.ZP - 1); };
+            if (UNR == 2) {   // two rows' z-cell loads in flight, then their pairs in row order
+                for (int r = 0; r < wrows; r += 2) {
+                    const float2 z0c = __ldg(zrow + row(r)), z1c = __ldg(zrow + row(r + 1));
+                    row_pairs(row(r), r < nrows ? z0c : none);
+                    if (r + 1 < wrows) row_pairs(row(r + 1), r + 1 < nrows ? z1c : none);
+                }
+            } else {          // the next row's z-cell load issued before this row's pairs
+                float2 zn = __ldg(zrow + row(0));
+                for (int r = 0; r < wrows; ++r) {
+                    const float2 zc = r < nrows ? zn : none;
+                    zn = __ldg(zrow + row(r + 1));
+                    row_pairs(row(r), zc);
+                }
             }
         };
         // candidate rows of the band [row0, row0 + nvr) seen from height zs
@@ -496,7 +513,7 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
             cmx = bmx;
             vlo = max(__float2int_ru(__fmaf_rn(zmn, g.inv_dv, zrow_lo)), 0);
             vhi = min(__float2int_rd(__fmaf_rn(zmx, g.inv_dv, zrow_hi)), g.ZP - 1);
-            if (vlo > vhi) continue;
+            // (a voxel with no rows stays in step with the warp: its sums stay 0, no update)
             const float old = Store<VT>::ldw(pv);   // loaded ahead: its latency overlaps the pairs
             all_pairs();
             if (!(sl < g.thr_bp)) {                                            // :799-806
