@@ -456,9 +456,20 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
         // Every lane runs the warp's largest row count (no divergent loop):
         // a lane past its own rows meets the empty z interval [1, 0] (no
         // chord with any column) at a row clamped into the table.  (The
-        // tetrahedron beam calls this once per source of the warp's union
-        // of kept sources, so every lane of the warp gets here together.)
+        // tetrahedron beam calls this per source, inside a loop whose trip
+        // count differs across lanes; there each lane runs its own rows.)
         auto all_pairs = [&]() {   // vlo..vhi: this lane's rows (none when vlo > vhi)
+            if constexpr (TB) {   // this lane's rows, the next row's z-cell load ahead (vlo <= vhi here)
+                int vv = vlo;
+                float2 zn = __ldg(zrow + vv);
+                for (; vv < vhi; ++vv) {
+                    const float2 zc = zn;
+                    zn = __ldg(zrow + vv + 1);
+                    row_pairs(vv, zc);
+                }
+                row_pairs(vhi, zn);
+                return;
+            }
             const int nrows = max(vhi - vlo + 1, 0);
             const int wrows = __reduce_max_sync(__activemask(), nrows);
             const float2 none = make_float2(1.0f, 0.0f);
@@ -536,20 +547,13 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
             while (s1 >= 0 && zsrc(s1) > upper) --s1;
             const float z0 = PZ[k + 1], z1 = PZ[k + 2];
             float WS = 0.f, L = 0.f;
-            // every lane runs the warp's union of kept sources; a source a
-            // lane does not keep, or whose band it misses, has no rows there
-            // and leaves its sums untouched
-            const unsigned am = __activemask();
-            const int qlo = __reduce_min_sync(am, s0 <= s1 ? s0 : g.nsrc);
-            const int qhi = __reduce_max_sync(am, s0 <= s1 ? s1 : -1);
-            for (int q = qlo; q <= qhi; ++q) {
-                const bool keep = q >= s0 && q <= s1 && band_rows(z0, z1, zsrc(q), q * g.nvr);
-                if (!keep) { vlo = 1; vhi = 0; }
+            for (int q = s0; q <= s1; ++q) {
+                if (!band_rows(z0, z1, zsrc(q), q * g.nvr)) continue;
                 sw = 0.f;
                 sl = 0.f;
                 all_pairs();
-                WS = keep ? fa(WS, sw) : WS;                                   // :754-755
-                L = keep ? fa(L, sl) : L;
+                WS = fa(WS, sw);                                               // :754-755
+                L = fa(L, sl);
             }
             if (L > g.thr_upd) {                                               // :772-773
                 VT* p = pv;
