@@ -1725,7 +1725,10 @@ extern "C" ctr_status ctr_batch_create(const ctr_geometry* const* geoms, int n, 
     for (int i = 0; i < n && st == CTR_OK; ++i) {
         ctr_solver* s = nullptr;
         st = ctr_solver_create(geoms[i], vdt, p, &s);
-        if (st == CTR_OK) b->scans.push_back(s);
+        if (st == CTR_OK) {
+            s->p.sart_flags |= BP_FULL_RUNS;   // the scans fill the GPU together
+            b->scans.push_back(s);
+        }
         cudaStream_t cs = nullptr;
         cudaEvent_t ev = nullptr;
         if (st == CTR_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)

@@ -636,7 +636,8 @@ static ctr_status launch_sart_walk(const Geometry& G, const BpArgs& a, cudaStrea
     const BpShape sh = kBpShapes[(G.bp_shape >= 0 && G.bp_shape < BP_SHAPES) ? G.bp_shape : 1];
     int zl = sh.zl;
     const long long cols = (long long)g.M * g.N;
-    while (zl > 1 && cols * ((g.Z + zl - 1) / zl) < 148LL * 2048) zl >>= 1;   // about two waves at least
+    if (!(a.flags & BP_FULL_RUNS))
+        while (zl > 1 && cols * ((g.Z + zl - 1) / zl) < 148LL * 2048) zl >>= 1;   // about two waves at least
     const dim3 grid((g.M + 31) / 32, (g.N + sh.rows - 1) / sh.rows, (g.Z + zl - 1) / zl);
     if (grid.z > 65535) return set_error(CTR_ERR_UNSUPPORTED, "too many z runs");
     const float2* rays = (const float2*)a.rays;

@@ -167,6 +167,10 @@ ctr_status launch_forward(const Geometry& g, const FpArgs& a, cudaStream_t st, s
 // objective partials per view: one per warp of 32 rays
 inline size_t objective_partials_per_view(const DevGeom& g) { return (size_t)g.ZP * ((g.R + 31) / 32); }
 
+// Internal SART flag (not in the public header): the walk keeps its full z
+// runs instead of shortening them to fill the GPU with one scan's blocks (a
+// batch's scans fill it together).  The sums do not depend on the runs.
+constexpr unsigned BP_FULL_RUNS = 0x40000000u;
 struct BpArgs {
     void* vol; ctr_dtype vol_dtype;
     const void* rays;                     // [nview][ZP][R]: float2 (c, d12) for SART and the
