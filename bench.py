@@ -668,7 +668,8 @@ def run_batched(args):
     launches += iters if form == "persistent" else sum(2 * sp["n_views"] * iters for sp in specs)
     other = "graph_branches" if form == "persistent" else "persistent"
     notes = {"graph_branches": "one kernel per view and scan, the scans as parallel graph branches",
-             "persistent": "every scan's SART views in one persistent cooperative launch per iteration"}
+             "persistent": "every scan's SART views in one persistent launch per iteration, its blocks handed "
+                           "out as a data flow over the scans' phases"}
     line = {
         "metric": "batched SART-FISTA-TV voxel-updates/s", "value": updates * 1000.0 / ms,
         "unit": "voxel-updates/s", "n_gpus": 1, "steps": iters, "warmup": args.warmup, "ms_per_step": ms,
