@@ -144,35 +144,14 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
     float clo[REF_COLS], chi[REF_COLS], cq2[REF_COLS];
     unsigned live = 0;
     const int ncol = maxYi - minYi + 1;
-    float amin = 1.0f, bmax = 0.0f;   // the live columns' alpha range inside the voxel column
 #pragma unroll
     for (int q = 0; q < REF_COLS; ++q) {
         clo[q] = 0.f; chi[q] = 0.f; cq2[q] = 0.f;
         if (!u_out && q < ncol) {
             column(minYi + q, clo[q], chi[q], cq2[q]);
-            if (chi[q] > clo[q]) {   // an empty x-y interval is empty for every z
-                live |= 1u << q;
-                amin = fminf(amin, clo[q]);
-                bmax = fmaxf(bmax, chi[q]);
-            }
+            if (chi[q] > clo[q]) live |= 1u << q;   // an empty x-y interval is empty for every z
         }
     }
-    for (int q = REF_COLS; !u_out && q < ncol; ++q) {   // wide rectangles
-        float lo, hi, q2;
-        column(minYi + q, lo, hi, q2);
-        if (hi > lo) { amin = fminf(amin, lo); bmax = fmaxf(bmax, hi); }
-    }
-    // Cone beam: the rows whose ray meets the cell within the live columns'
-    // alpha range, as the SART walk derives them (the row centred at qz is
-    // inside [z0, z1] at some alpha of [amin, bmax] iff qz lies between the
-    // least of z0 + (z0 - zs) m and the greatest of z1 + (z1 - zs) m over
-    // m = alpha / (1 - alpha), alpha = amin, bmax), widened by 1/32 row: a
-    // superset of the rows with a positive chord, so the sums are the
-    // rectangle's (its other rows add nothing).  Otherwise the rectangle's rows.
-    const bool tight = CONE && amin > 0.0f && bmax < 1.0f;
-    const float m_lo = tight ? __fdividef(amin, fs(1.0f, amin)) : 0.0f;
-    const float m_hi = tight ? __fdividef(bmax, fs(1.0f, bmax)) : 0.0f;
-    const float row_pos = -fm(g.zmin, g.inv_dv);
 
     const int R = g.R;
     VT* pv = pv0;
@@ -187,9 +166,8 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
             for (int kk = 0; kk < 2; ++kk) {
                 const float pz = fs(fa(cz, fm((float)kk, g.vz)), fm(0.5f, g.vz));
                 const float dz = fs(pz, g.srcz);
-                const float ml = tight ? m_lo : mlo, mh = tight ? m_hi : mhi;
-                const float a0 = fa(fm(dz >= 0.f ? ml : mh, dz), pz);   // the smallest of the 4 corners
-                const float a1 = fa(fm(dz >= 0.f ? mh : ml, dz), pz);   // and the largest
+                const float a0 = fa(fm(dz >= 0.f ? mlo : mhi, dz), pz);   // the smallest of the 4 corners
+                const float a1 = fa(fm(dz >= 0.f ? mhi : mlo, dz), pz);   // and the largest
                 minZ = fminf(minZ, a0);
                 maxZ = fmaxf(maxZ, a1);
             }
@@ -197,25 +175,12 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
             minZ = cz;
             maxZ = cz;
         }
-        int minZi, maxZi;
-        if (tight) {
-            minZi = __float2int_ru(__fmaf_rn(minZ, g.inv_dv, fs(row_pos, 1.0f / 32.0f)));
-            maxZi = __float2int_rd(__fmaf_rn(maxZ, g.inv_dv, fa(row_pos, 1.0f / 32.0f)));
-        } else {
-            minZi = __float2int_rd(fa(fm(fs(minZ, g.zmin), g.inv_dv), 0.5f));
-            maxZi = __float2int_rd(fa(fm(fs(maxZ, g.zmin), g.inv_dv), 0.5f));
-        }
+        int minZi = __float2int_rd(fa(fm(fs(minZ, g.zmin), g.inv_dv), 0.5f));
+        int maxZi = __float2int_rd(fa(fm(fs(maxZ, g.zmin), g.inv_dv), 0.5f));
         float sw = 0.f, sl = 0.f;
-        // this lane's rows [minZi, maxZi] (none when out of the detector)
-        const bool rows_out = u_out || (minZi < 0 && maxZi < 0) || (minZi > g.ZP - 1 && maxZi > g.ZP - 1);
-        minZi = max(minZi, 0);
-        maxZi = min(maxZi, g.ZP - 1);
-        const int nrows = rows_out ? 0 : max(maxZi - minZi + 1, 0);
-        // every lane runs the warp's largest row count; a lane past its own
-        // rows meets the empty z interval [1, 0] (no chord) at a row clamped
-        // into the table
-        const int wrows = __reduce_max_sync(__activemask(), nrows);
-        if (wrows > 0) {
+        if (!(u_out || (minZi < 0 && maxZi < 0) || (minZi > g.ZP - 1 && maxZi > g.ZP - 1))) {
+            minZi = max(minZi, 0);
+            maxZi = min(maxZi, g.ZP - 1);
             const float2* __restrict__ zr = g.zref + (long long)k * g.ZP;
             auto pair = [&](float lo, float hi, float q2, float2 zc, float qzd, float2 rec) {
                 const float amin = fmaxf(lo, zc.x), amax = fminf(hi, zc.y);
@@ -230,9 +195,8 @@ k_sart_ref(const DevGeom g, VT* __restrict__ vol, const float2* __restrict__ ray
                     }
                 }
             };
-            for (int r = 0; r < wrows; ++r) {
-                const int jr = min(max(minZi + r, 0), g.ZP - 1);
-                const float2 zc = r < nrows ? __ldg(zr + jr) : make_float2(1.0f, 0.0f);
+            for (int jr = minZi; jr <= maxZi; ++jr) {
+                const float2 zc = __ldg(zr + jr);
                 const float qzd = CONE ? 0.f : fs(cz, fa(g.zmin, fm((float)jr, g.dv)));   // sz - qz, sz = cz
                 const float2* __restrict__ rrow = rays + (long long)jr * R + minYi;
 #pragma unroll
