@@ -285,19 +285,25 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
                                            VT* __restrict__ vol, const float2* __restrict__ rays, int view,
                                            float beta, uint32_t seed, int zl)
 {
+    // A warp leaves together or not at all: the lanes of a warp that stays
+    // and have nothing to do (past the volume's x edge, outside the FOV
+    // cylinder, missing the detector) run on as idle lanes with no columns
+    // and no rows, so that the warp-wide reductions below always have all
+    // 32 lanes.  Idle lanes read only in-range addresses and store nothing.
     const int i = bx * 32 + (threadIdx.x & 31);
     const int j = by * BY + (threadIdx.x >> 5);
-    if (i >= g.M || j >= g.N) return;
+    if (j >= g.N) return;   // the whole warp
+    const int ic = min(i, g.M - 1);
     const int kb = bz * zl, ke = min(g.Z, kb + zl);
 
     // FOV cylinder (universal.cu:626-628): masked voxels keep their value
     const float ex = fs(fs((float)i, g.fov_h_x), g.m_off);
     const float ey = fs((float)j, g.fov_h_y);
-    if (fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) >= g.fov_r2) return;
+    bool live = i < g.M && fa(fm(fm(fm(ex, g.vx), ex), g.vx), fm(fm(fm(ey, g.vy), ey), g.vy)) < g.fov_r2;
 
-    const float cx = fa(fa(g.bx, fm(g.vx, 0.5f)), fm((float)i, g.vx));   // :592-594
+    const float cx = fa(fa(g.bx, fm(g.vx, 0.5f)), fm((float)ic, g.vx));   // :592-594
     const float cy = fa(fa(g.by, fm(g.vy, 0.5f)), fm((float)j, g.vy));
-    const float xlo = PX[i + 1], xhi = PX[i + 2];
+    const float xlo = PX[ic + 1], xhi = PX[ic + 2];
     const float ylo = PY[j + 1], yhi = PY[j + 2];
     const float2 sc = g.trig[view];
     const float s = sc.x, c = sc.y;
@@ -320,9 +326,10 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     if (g.ct_style == 1 || g.ct_style == 2) { mlo = 0.0f; mhi = 0.0f; }
     int ulo = __float2int_rd(fa(fm(fs(umin, g.ymin), g.inv_du), 0.5f));
     int uhi = __float2int_rd(fa(fm(fs(umax, g.ymin), g.inv_du), 0.5f));
-    if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) return;
+    if ((ulo < 0 && uhi < 0) || (ulo > g.R - 1 && uhi > g.R - 1)) live = false;
     ulo = max(ulo, 0);
     uhi = min(uhi, g.R - 1);
+    if (!live) { ulo = 1; uhi = 0; }   // an idle lane searches no column
 
     // the run of detector columns whose ray column crosses this voxel column
     const float4* __restrict__ colt = g.colt + (long long)view * g.R;
@@ -340,8 +347,12 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
             bmax = fmaxf(bmax, bb);
         }
     }
-    if (ua > ub) return;
-    const int nrun = ub - ua + 1;   // every column of the run crosses the voxel column (bb > a)
+    if (ua > ub) live = false;
+    if (__all_sync(0xffffffffu, !live)) return;   // the whole warp is idle
+    if (!live) { ua = 0; ub = -1; }
+    // every column of the run crosses the voxel column (bb > a); none for an idle lane
+    const int nrun = ub - ua + 1;
+    const int nrun_ld = max(nrun, 1);   // records are read at ua .. ua + nrun_ld - 1 (in range)
 
     // Candidate detector rows.  A cone-beam ray from source height zs meets
     // height z at alpha where z = x1z + alpha (zs - x1z), so the ray of the
@@ -368,7 +379,7 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     const float zrow0 = -fm(g.zmin, g.inv_dv);
     const float zrow_lo = fs(zrow0, row_off), zrow_hi = fa(zrow0, row_off);
     // the warp's longest run: the pair slots every detector row executes
-    const int nq = __reduce_max_sync(__activemask(), nrun);
+    const int nq = __reduce_max_sync(0xffffffffu, nrun);
     // the run's alpha intervals; a slot beyond the run gets the empty interval
     // [1, 0] (no chord with any row: hi - lo <= -1), so every thread of the
     // warp runs the same pair slots without a test
@@ -412,7 +423,8 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     bool s_est = TB;
     // voxel and z-cell row addresses advance by a constant per z step
     const long long vstep = TL ? 64LL * g.Mt * g.Nt : MN;
-    VT* pv = vol + (TL ? (long long)tile_index(g, i, j, kb) : (long long)kb * MN + (long long)j * g.M + i);
+    // (ic: an idle lane past the x edge loads its neighbour's value and stores nothing)
+    VT* pv = vol + (TL ? (long long)tile_index(g, ic, j, kb) : (long long)kb * MN + (long long)j * g.M + ic);
     const float2* __restrict__ zrow = g.zcell + (long long)kb * g.ZP;
     // the z run with NQ pair slots per detector row (NQ = the warp's longest
     // run, at most WALK_RUN; longer runs take the rest from the column table)
@@ -439,7 +451,7 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
             const float2* __restrict__ rr = rays + (long long)vv * R + ua;
 #pragma unroll
             for (int q = 0; q < NQ; ++q)   // a slot beyond the run reads the run's last record (no chord)
-                pair(ra[q], rb[q], zc, rec(rr + min(q, nrun - 1)));
+                pair(ra[q], rb[q], zc, rec(rr + min(q, nrun_ld - 1)));
             if (NQ == WALK_RUN)
                 for (int q = WALK_RUN; q < nrun; ++q) {   // runs longer than the registers hold
                     // the column's planes re-read from the shared tables (rare: not kept live)
@@ -470,8 +482,8 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
                 row_pairs(vhi, zn);
                 return;
             }
-            const int nrows = max(vhi - vlo + 1, 0);
-            const int wrows = __reduce_max_sync(__activemask(), nrows);
+            const int nrows = live ? max(vhi - vlo + 1, 0) : 0;   // an idle lane has none
+            const int wrows = __reduce_max_sync(0xffffffffu, nrows);
             const float2 none = make_float2(1.0f, 0.0f);
             auto row = [&](int r) { return min(max(vlo + r, 0), g.ZP - 1); };
             if (UNR == 2) {   // two rows' z-cell loads in flight, then their pairs in row order
@@ -516,13 +528,13 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
             // (a voxel with no rows stays in step with the warp: its sums stay 0, no update)
             const float old = Store<VT>::ldw(pv);   // loaded ahead: its latency overlaps the pairs
             all_pairs();
-            if (!(sl < g.thr_bp)) {                                            // :799-806
+            if (live && !(sl < g.thr_bp)) {                                    // :799-806
                 VT* p = pv;
                 const float nv = fa(old, fdv(fm(beta, sw), sl));
                 if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
                 else Store<VT>::st(p, nv);
             }
-        } else {
+        } else if (live) {   // no warp-wide step here: an idle lane skips the voxel
             // the sources T42 keeps for this voxel (:620-627): source_lower <= z <= source_upper
             const float czr = tb_centre_z(g, k);
             const float upper = fa(fdv(fm(fs(fa(czr, g.vz), g.zmin), g.dsod), tden), g.zmin);
