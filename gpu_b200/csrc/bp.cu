@@ -349,10 +349,10 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     }
     if (ua > ub) live = false;
     if (__all_sync(0xffffffffu, !live)) return;   // the whole warp is idle
-    if (!live) { ua = 0; ub = -1; }
-    // every column of the run crosses the voxel column (bb > a); none for an idle lane
+    // every column of the run crosses the voxel column (bb > a); an idle lane
+    // keeps a run of one column (0) whose alpha interval is empty (below)
+    if (!live) { ua = 0; ub = 0; }
     const int nrun = ub - ua + 1;
-    const int nrun_ld = max(nrun, 1);   // records are read at ua .. ua + nrun_ld - 1 (in range)
 
     // Candidate detector rows.  A cone-beam ray from source height zs meets
     // height z at alpha where z = x1z + alpha (zs - x1z), so the ray of the
@@ -371,13 +371,15 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
     // rows, is inside either margin), and a detector height z maps to the
     // row position z * inv_dv - zmin * inv_dv, offset by the margin.
     float row_off = 0.5f;
-    if ((g.ct_style == 0 || g.ct_style == 3) && amin > 0.0f && bmax < 1.0f) {
+    if ((g.ct_style == 0 || g.ct_style == 3) && live && amin > 0.0f && bmax < 1.0f) {
         mlo = __fdividef(amin, fs(1.0f, amin));
         mhi = __fdividef(bmax, fs(1.0f, bmax));
         row_off = ROW_EPS;
     }
     const float zrow0 = -fm(g.zmin, g.inv_dv);
-    const float zrow_lo = fs(zrow0, row_off), zrow_hi = fa(zrow0, row_off);
+    // an idle lane's lowest row lies far above the table (its corner bounds
+    // are finite, for a column of the volume): it has no rows
+    const float zrow_lo = live ? fs(zrow0, row_off) : 1e7f, zrow_hi = fa(zrow0, row_off);
     // the warp's longest run: the pair slots every detector row executes
     const int nq = __reduce_max_sync(0xffffffffu, nrun);
     // the run's alpha intervals; a slot beyond the run gets the empty interval
@@ -387,7 +389,7 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
 #pragma unroll
     for (int q = 0; q < WALK_RUN; ++q) {
         ra[q] = 1.f; rb[q] = 0.f;
-        if (ua + q <= ub) {
+        if (live && ua + q <= ub) {
             const float4 ct = __ldg(colt + ua + q);
             const float ax0 = fm(fs(xlo, ct.x), ct.y), ax1 = fm(fs(xhi, ct.x), ct.y);
             const float ay0 = fm(fs(ylo, ct.z), ct.w), ay1 = fm(fs(yhi, ct.z), ct.w);
@@ -451,7 +453,7 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
             const float2* __restrict__ rr = rays + (long long)vv * R + ua;
 #pragma unroll
             for (int q = 0; q < NQ; ++q)   // a slot beyond the run reads the run's last record (no chord)
-                pair(ra[q], rb[q], zc, rec(rr + min(q, nrun_ld - 1)));
+                pair(ra[q], rb[q], zc, rec(rr + min(q, nrun - 1)));
             if (NQ == WALK_RUN)
                 for (int q = WALK_RUN; q < nrun; ++q) {   // runs longer than the registers hold
                     // the column's planes re-read from the shared tables (rare: not kept live)
@@ -482,7 +484,7 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
                 row_pairs(vhi, zn);
                 return;
             }
-            const int nrows = live ? max(vhi - vlo + 1, 0) : 0;   // an idle lane has none
+            const int nrows = max(vhi - vlo + 1, 0);
             const int wrows = __reduce_max_sync(0xffffffffu, nrows);
             const float2 none = make_float2(1.0f, 0.0f);
             auto row = [&](int r) { return min(max(vlo + r, 0), g.ZP - 1); };
@@ -525,10 +527,11 @@ __device__ __forceinline__ void walk_block(const DevGeom& g, const float* __rest
             cmx = bmx;
             vlo = max(__float2int_ru(__fmaf_rn(zmn, g.inv_dv, zrow_lo)), 0);
             vhi = min(__float2int_rd(__fmaf_rn(zmx, g.inv_dv, zrow_hi)), g.ZP - 1);
-            // (a voxel with no rows stays in step with the warp: its sums stay 0, no update)
+            // (a voxel with no rows, an idle lane's included, stays in step with
+            // the warp: its sums stay 0, below thr_bp > 0, so it is not updated)
             const float old = Store<VT>::ldw(pv);   // loaded ahead: its latency overlaps the pairs
             all_pairs();
-            if (live && !(sl < g.thr_bp)) {                                    // :799-806
+            if (!(sl < g.thr_bp)) {                                            // :799-806
                 VT* p = pv;
                 const float nv = fa(old, fdv(fm(beta, sw), sl));
                 if (STOCH) st_sr<VT>(p, nv, hash32(seed ^ hash32((uint32_t)(k * MN + j * g.M + i))));
