@@ -131,6 +131,15 @@ static ctr_status validate(const ctr_geometry_desc* d)
         return set_error(CTR_ERR_BAD_GEOMETRY, "detector too large");
     if (!(d->vx > 0.f) || !(d->du > 0.f) || !std::isfinite(d->vx) || !std::isfinite(d->du))
         return set_error(CTR_ERR_BAD_GEOMETRY, "voxel and detector pitch must be positive and finite");
+    // vy, vz, dv: 0 or below selects the x / u pitch; a given one must be finite
+    if (!std::isfinite(d->vy) || !std::isfinite(d->vz) || !std::isfinite(d->dv))
+        return set_error(CTR_ERR_BAD_GEOMETRY, "vy, vz and dv must be finite (0 selects the x or u pitch)");
+    // the projector's and the update's thresholds are 1e-6 of a voxel pitch
+    // (universal.cu:554, :785, :799); a pitch whose threshold rounds to 0 in
+    // float would let a ray or a voxel with no chord divide by zero
+    const float vz_used = d->vz > 0.f ? d->vz : d->vx;
+    if (!(d->vx * 1e-6f > 0.f) || !(vz_used * 1e-6f > 0.f))
+        return set_error(CTR_ERR_BAD_GEOMETRY, "voxel pitch too small: 1e-6 of it rounds to 0 in float");
     if (!(d->dso > 0.f) || !std::isfinite(d->dso) || !std::isfinite(d->dod) || !(d->dod < d->dso))
         return set_error(CTR_ERR_BAD_GEOMETRY, "need 0 < dso and dod < dso (detector opposite the source)");
     if (!std::isfinite(d->us_rate) || !std::isfinite(d->initial_angle) || !std::isfinite(d->shift_angle) ||

@@ -96,6 +96,10 @@ def _desc_variant(name):
         return ctrecon.make_desc(**dict(base, dso=0.0))
     if name == "zero detector pitch":
         return ctrecon.make_desc(**dict(base, du=0.0))
+    if name == "infinite z pitch":
+        return ctrecon.make_desc(**base, vz=float("inf"))
+    if name == "voxel pitch below the thresholds' range":
+        return ctrecon.make_desc(**dict(base, vx=1e-40))   # 1e-6 of it is below the least float
     raise KeyError(name)
 
 
@@ -111,6 +115,8 @@ REJECTIONS = {
     "non-finite angle": "must be finite",
     "source at the isocentre": "0 < dso",
     "zero detector pitch": "pitch must be positive",
+    "infinite z pitch": "must be finite",
+    "voxel pitch below the thresholds' range": "rounds to 0",
 }
 
 
